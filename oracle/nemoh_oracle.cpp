@@ -1,0 +1,2057 @@
+// =============================================================================
+// TEST INFRASTRUCTURE ONLY -- not part of the nemoh_b200 product.
+//
+// CPU FP64 restatement of the reference Nemoh Solver's per-frequency BEM solve
+// (Fortran 90, default REAL promoted to double). Only tests/, the smoke check
+// and bench.py's CPU-baseline leg may load or run this code, as the checker
+// and as the timed CPU baseline; the product never links it.
+//
+// Parity status: the reference cannot be compiled here (no Fortran compiler),
+// so this restatement is pinned (a) function by function against independent
+// mathematics (exponential-integral kernel GG, Rankine panel integrals by
+// quadrature, the dispersion root) and (b) at solve level against the
+// reference's own verification data (Verification/Cylinder Aquaplus results,
+// a few percent). At the 1e-9 level parity with the Fortran is unpinned.
+//
+// Every routine follows the named reference routine line by line, 1-based
+// arrays, same expression order and branch structure (goto where the Fortran
+// uses arithmetic IF / GOTO). Files cited relative to the Nemoh tree:
+//   Solver/NEMOH.f90                  Main (30-176), CREK/VNS/COFINT (179-274)
+//   Solver/Core/PREPARE_MESH.f90      PRE_PROC_MESH / GOMG (30-180)
+//   Solver/Core/ELEMENTARY_FNS.f90    GG, CIH, SIH (31-106)
+//   Solver/Core/COMPUTE_GREEN_INFD.f90 VAVINFD, VNSINFD, CINT_INFD, PL2
+//   Solver/Core/COMPUTE_GREEN_FD.f90  VAVFD, VNSFD, CINT_FD, LISC, EXPORS,
+//                                     MCAS, SPRBM, SPQFB, HOUSRS, VSD, FF, X0
+//   Solver/Core/M_SOLVER.f90          GAUSSZ (31-104)
+//   Solver/Core/SOLVE_BEM_INFD_DIRECT.f90, SOLVE_BEM_FD_DIRECT.f90, SOLVE_BEM.f90
+//
+// Deliberate differences, all documented:
+//  * STOP becomes a C++ exception turned into a status code at the C API.
+//  * COMPLEX*8 locals of VNSINFD (COMPUTE_GREEN_INFD.f90:237-238) are double.
+//  * The wave term left undefined by the reference when AKZ > -1.5e-6
+//    (COMPUTE_GREEN_INFD.f90:284-289, COMPUTE_GREEN_FD.f90:307-311) is an error.
+// Build: g++ -O2 -ffp-contract=off -fcx-fortran-rules (see oracle/Makefile).
+// =============================================================================
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <fstream>
+#include <sstream>
+#include <chrono>
+
+typedef double R;
+typedef std::complex<double> C;
+
+namespace {
+
+struct Stop : std::runtime_error {
+  int code;
+  Stop(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// status codes shared with the product's C-ABI (include/nemoh_b200.h)
+enum {
+  ST_OK = 0, ST_INVALID = 1, ST_PANEL_AREA = 2, ST_PIVOT = 3, ST_OMEGA = 4,
+  ST_LISC = 5, ST_SPRBM = 6, ST_DISPERSION = 7, ST_AKZ_UNDEFINED = 8,
+  ST_IO = 9, ST_HOUSRS = 10
+};
+
+inline R sgn(R a, R b) { return std::copysign(std::fabs(a), b); }  // Fortran SIGN
+inline R sq(R x) { return x * x; }
+inline R cube(R x) { return x * x * x; }
+
+// ---------------------------------------------------------------------------
+// ELEMENTARY_FNS.f90:31-81  GG(Z,CEX)
+// ---------------------------------------------------------------------------
+C GG(C Z, C CEX) {
+  const C IPI(0., 3.14159265);
+  C Y, G;
+  R T;
+  if (Z.real() + 16. <= 0.) {               // case 1
+    Y = 1. / Z;
+    return Y * (1. + Y * (-1. + Y * (2. + Y * (-6. + Y * (24. + Y * (-120.))))));
+  }
+  T = Z.imag();
+  if (std::fabs(T) - 10. > 0.) {             // case 3
+    G = 0.711093 / (Z + 0.415775) + 0.278518 / (Z + 2.29428) + 0.010389 / (Z + 6.2900);
+    if (T < 0.) return G - IPI * CEX;
+    return G + IPI * CEX;
+  }
+  if (Z.real() + 0.5 > 0.) {                 // case 2
+    G = -(std::log(Z) * (.1E+01 + Z * (0.23721365E+00 + Z * (0.206543E-01 + Z * (0.763297E-03 +
+          Z * 0.97087007E-05)))) + 0.5772156649E+00 * (0.99999207E+00 +
+          Z * (-0.149545886E+01 + Z * (0.41806426E-01 + Z * (-0.3000591E-01 +
+          Z * (0.19387339E-02 + Z * (-0.51801555E-03))))))) / (0.1E+01 +
+          Z * (-0.76273617E+00 + Z * (0.28388363E+00 + Z * (-0.66786033E-01 + Z * (0.12982719E-01
+          + Z * (-0.8700861E-03 + Z * 0.2989204E-03))))));
+    if (T < 0.) return G - IPI * CEX;
+    return G + IPI * CEX;
+  }
+  if (T < 0.) {                              // case 4, lower half plane
+    return ((((((( C(1.000000, 1.3935496E-06) * Z + C(15.82958, -20.14222))
+      * Z + C(-70.52863, -227.9511)) * Z + C(-985.4221, -226.6272)) * Z
+      + C(-1202.318, 1580.907)) * Z + C(953.2441, 1342.447)) * Z
+      + C(417.3716, -196.6665)) * Z + C(-9.881266, -24.24952)) /
+      (((((((( C(1.000000, 0.0000000E+00) * Z + C(16.83184, -20.14481)) * Z
+      + C(-55.66969, -248.1167)) * Z + C(-1068.640, -434.4707)) * Z
+      + C(-2082.250, 1522.471)) * Z + C(383.3455, 2730.378)) * Z
+      + C(1216.791, 351.7189)) * Z + C(115.3926, -161.2647)) * Z
+      + C(-3.777369, -4.510900)) - IPI * CEX;
+  }
+  return ((((((( C(1.000000, -1.3935496E-06) * Z + C(15.82958, 20.14222))
+    * Z + C(-70.52863, 227.9511)) * Z + C(-985.4221, 226.6272)) * Z
+    + C(-1202.318, -1580.907)) * Z + C(953.2441, -1342.447)) * Z
+    + C(417.3716, 196.6665)) * Z + C(-9.881266, 24.24952)) /
+    (((((((( C(1.000000, 0.0000000E+00) * Z + C(16.83184, 20.14481)) * Z
+    + C(-55.66969, 248.1167)) * Z + C(-1068.640, 434.4707)) * Z
+    + C(-2082.250, -1522.471)) * Z + C(383.3455, -2730.378)) * Z
+    + C(1216.791, -351.7189)) * Z + C(115.3926, 161.2647)) * Z
+    + C(-3.777369, 4.510900)) + IPI * CEX;
+}
+
+// COMPUTE_GREEN_INFD.f90:641-645
+inline R PL2(R U1, R U2, R U3, R XU) { return ((XU - U1) * (XU - U2)) / ((U3 - U1) * (U3 - U2)); }
+
+// Gauss-Legendre half-rules of CINT_INFD / CINT_FD (COMPUTE_GREEN_INFD.f90:509-531)
+const R Q8d[4] = {.4801449, .3983332, .2627662, .09171732};
+const R CQ8d[4] = {.05061427, .1111905, .1568533, .1813419};
+const R Q12d[6] = {.4907803, .4520586, .3849513, .2936589, .1839157, .06261670};
+const R CQ12d[6] = {.2358766E-1, .5346966E-1, .8003916E-1, .1015837, .1167462, .1245735};
+const R Q16d[8] = {.4947004, .4722875, .4328156, .3777022, .3089381, .2290084, .1408017, .04750625};
+const R CQ16d[8] = {.01357622, .03112676, .04757925, .06231448, .07479799, .08457826, .09130170, .09472530};
+const R Q24d[12] = {.4975936, .4873642, .469137, .4432077, .4100009, .3700621, .3240468, .2727107,
+                    .2168967, .1575213, .09555943, .032028446};
+const R CQ24d[12] = {.6170615E-2, .1426569E-1, .2213872E-1, .2964929E-1, .366732E-1, .4309508E-1,
+                     .4880932E-1, .5372213E-1, .5775283E-1, .6083523E-1, .6291873E-1, .6396909E-1};
+const R Q32d[16] = {.4986319, .4928057, .4823811, .4674530, .4481605, .4246838, .3972418, .3660910,
+                    .3315221, .2938578, .2534499, .2106756, .1659343, .1196436, .07223598, .02415383};
+const R CQ32d[16] = {.350930E-2, .8137197E-2, .1269603E-1, .1713693E-1, .2141794E-1, .2549903E-1,
+                     .2934204E-1, .3291111E-1, .3617289E-1, .3909694E-1, .4165596E-1, .4382604E-1,
+                     .4558693E-1, .4692219E-1, .4781936E-1, .4827004E-1};
+
+// CINT_INFD / CINT_FD body: fills QQ(1..N), CQ(1..N) (1-based arrays of >=102)
+void cint(R AKK, int& N, R* QQ, R* CQ) {
+  const int NPIN = 101;
+  const R PI = 4. * std::atan(1.);
+  const R *q = nullptr, *c = nullptr;
+  int h = 0;
+  if (AKK - .4 <= 0) { N = 8; q = Q8d; c = CQ8d; h = 4; }
+  else if (AKK - 2.5 <= 0) { N = 12; q = Q12d; c = CQ12d; h = 6; }
+  else if (AKK - 4. <= 0) { N = 16; q = Q16d; c = CQ16d; h = 8; }
+  else if (AKK - 8. <= 0) { N = 24; q = Q24d; c = CQ24d; h = 12; }
+  else if (AKK - 25. <= 0) { N = 32; q = Q32d; c = CQ32d; h = 16; }
+  if (q) {
+    R QF[33], CF[33];
+    for (int I = 1; I <= h; ++I) {
+      QF[I] = q[I - 1]; QF[N + 1 - I] = -q[I - 1];
+      CF[I] = c[I - 1]; CF[N + 1 - I] = c[I - 1];
+    }
+    for (int J = 1; J <= N; ++J) { QQ[J] = QF[J] * PI; CQ[J] = CF[J] * PI; }
+    return;
+  }
+  N = 51;
+  if (AKK > 40.) N = NPIN;
+  for (int J = 1; J <= N; ++J) {
+    QQ[J] = -PI / 2. + (J - 1.) / (N - 1.) * PI;
+    if (J == 1 || J == N) CQ[J] = PI / (3. * (N - 1.));
+    else if (J % 2 != 0) CQ[J] = 2. / (3. * (N - 1.)) * PI;
+    else CQ[J] = 4. / (3. * (N - 1.)) * PI;
+  }
+}
+
+// COMPUTE_GREEN_FD.f90:1612-1632
+R FF(R XTT, R AK, R AM) {
+  R COEF = sq(AM + AK) / (sq(AM) - sq(AK) + AK);
+  R H = XTT - AM;
+  R TOL = std::fmax(0.1, 0.1 * AM);
+  if (std::fabs(H) > TOL)
+    return (XTT + AK) * std::exp(XTT) / (XTT * std::sinh(XTT) - AK * std::cosh(XTT)) - COEF / (XTT - AM) - 2.;
+  R A = AM - TOL, B = AM, Cc = AM + TOL;
+  R D = (A + AK) * std::exp(A) / (A * std::sinh(A) - AK * std::cosh(A)) - COEF / (A - AM) - 2;
+  R E = COEF / (AM + AK) * (AM + AK + 1) - sq(COEF / (AM + AK)) * AM - 2;
+  R F = (Cc + AK) * std::exp(Cc) / (Cc * std::sinh(Cc) - AK * std::cosh(Cc)) - COEF / (Cc - AM) - 2;
+  return (XTT - B) * (XTT - Cc) * D / ((A - B) * (A - Cc)) + (XTT - Cc) * (XTT - A) * E / ((B - Cc) * (B - A)) +
+         (XTT - A) * (XTT - B) * F / ((Cc - A) * (Cc - B));
+}
+
+// COMPUTE_GREEN_FD.f90:1635-1680
+R X0(R AK) {
+  const R EPS = 5.E-6;
+  int ITOUR = 0, IITER = 0;
+  R XI = 0., XS = XI, XM, VAL1, VAL2;
+  R PAS = std::fmax(AK, std::sqrt(AK));
+L30:
+  XS = XS + PAS;
+  ITOUR = ITOUR + 1;
+  if (ITOUR <= 1000) {
+    VAL1 = AK - XS * std::tanh(XS);
+    VAL2 = AK - XI * std::tanh(XI);
+    if (VAL1 * VAL2 > 0) goto L30;
+  }
+  IITER = 0;
+L10:
+  XM = (XI + XS) * 0.5;
+  IITER = IITER + 1;
+  if (IITER > 1000 || ITOUR > 1000) throw Stop(ST_DISPERSION, "ERREUR DANS LA RECHERCHE DE LA RACINE (X0)");
+  if (std::fabs((XS - XI) / XM) > EPS) {
+    VAL1 = AK - XM * std::tanh(XM);
+    VAL2 = AK - XI * std::tanh(XI);
+    if (std::fabs(VAL1 * VAL2) <= 1.E-12) VAL1 = 0.;
+    if (VAL1 * VAL2 < 0) XS = XM; else XI = XM;
+    goto L10;
+  }
+  return XM;
+}
+
+// ---------------------------------------------------------------------------
+// LISC and its helpers (COMPUTE_GREEN_FD.f90:1007-1511). 1-based arrays.
+// S is S(4*(31-1), 31+1) column-major with leading dimension NMAX=120.
+// ---------------------------------------------------------------------------
+const int LD = 120;
+inline R& At(R* A, int i, int j) { return A[(i - 1) + LD * (j - 1)]; }
+
+// HOUSRS (COMPUTE_GREEN_FD.f90:1454-1511)
+void HOUSRS(R* A, int NL, int NCC, int NS, R EPS) {
+  int NTC = NCC + NS;
+  if (NCC > NL) throw Stop(ST_HOUSRS, "NBRE DE COLONNES > NBRES DE LIGNES");
+  for (int K = 1; K <= NCC; ++K) {
+    R E = 0;
+    for (int I = K; I <= NL; ++I) E = E + sq(At(A, I, K));
+    R E0 = std::sqrt(E);
+    if (E0 < EPS) throw Stop(ST_HOUSRS, "NORME INFERIEURE A EPS (HOUSRS)");
+    R AR;
+    if (At(A, K, K) == 0) AR = -E0; else AR = -sgn(E0, At(A, K, K));
+    R ETA = AR * (AR - At(A, K, K));
+    int KP1 = K + 1;
+    for (int J = KP1; J <= NTC; ++J) {
+      R BA = (At(A, K, K) - AR) * At(A, K, J);
+      for (int I = KP1; I <= NL; ++I) BA = BA + At(A, I, K) * At(A, I, J);
+      At(A, K, J) = At(A, K, J) + BA / AR;
+      for (int I = KP1; I <= NL; ++I) At(A, I, J) = At(A, I, J) - At(A, I, K) * BA / ETA;
+    }
+    At(A, K, K) = AR;
+    for (int I = KP1; I <= NL; ++I) At(A, I, K) = 0;
+  }
+  for (int J = 1; J <= NS; ++J) {
+    int NCJ = NCC + J;
+    At(A, NCC, NCJ) = At(A, NCC, NCJ) / At(A, NCC, NCC);
+    for (int L = 2; L <= NCC; ++L) {
+      int I1 = NCC + 1 - L;
+      int M = I1 + 1;
+      for (int I = M; I <= NCC; ++I) At(A, I1, NCJ) = At(A, I1, NCJ) - At(A, I1, I) * At(A, I, NCJ);
+      At(A, I1, NCJ) = At(A, I1, NCJ) / At(A, I1, I1);
+    }
+  }
+}
+
+// SPQFB (COMPUTE_GREEN_FD.f90:1354-1451): quadratic factor by Bairstow iteration
+void SPQFB(R* Cc, int IC, R* Q, int LIM, int& IER) {
+  int I, J, L, LL;
+  R H = 0., HH = 0., A, A1, AA, B, BB, B1, C1 = 0., CA, CB, CC, CD, DQ1, DQ2, EPS, EPS1;
+  R Q1, Q2, QQ1, QQ2, QQQ1, QQQ2;
+  IER = 0;
+  J = IC + 1;
+L1:
+  J = J - 1;
+  if (J - 1 <= 0) goto L40;
+  if (Cc[J] == 0) goto L1;
+  A = Cc[J];
+  if (A - 1. == 0) goto L6;
+  for (I = 1; I <= J; ++I) {
+    Cc[I] = Cc[I] / A;
+    if (std::fabs(Cc[I]) - 1.E27 >= 0) goto L40;
+  }
+L6:
+  if (J - 3 < 0) goto L41;
+  if (J - 3 == 0) goto L38;
+L7:
+  EPS = 1.E-14;
+  EPS1 = 1.E-6;
+  L = 0;
+  LL = 0;
+  Q1 = Q[1];
+  Q2 = Q[2];
+  QQ1 = 0.;
+  QQ2 = 0.;
+  AA = Cc[1];
+  BB = Cc[2];
+  CB = std::fabs(AA);
+  CA = std::fabs(BB);
+  if (CB - CA < 0) { CC = CB + CB; CB = CB / CA; CA = 1.; }
+  else if (CB - CA == 0) { CC = CA + CA; CA = 1.; CB = 1.; }
+  else { CC = CA + CA; CA = CA / CB; CB = 1.; }
+  CD = CC * .1;
+L12:
+  A = 0.;
+  B = A;
+  A1 = A;
+  B1 = A;
+  I = J;
+  QQQ1 = Q1;
+  QQQ2 = Q2;
+  DQ1 = HH;
+  DQ2 = H;
+L13:
+  H = -Q1 * B - Q2 * A + Cc[I];
+  if (std::fabs(H) - 1.E27 >= 0) goto L42;
+  B = A;
+  A = H;
+  I = I - 1;
+  if (I - 1 < 0) goto L18;
+  if (I - 1 == 0) H = 0.;
+  H = -Q1 * B1 - Q2 * A1 + H;
+  if (std::fabs(H) - 1.E27 >= 0) goto L42;
+  C1 = B1;
+  B1 = A1;
+  A1 = H;
+  goto L13;
+L18:
+  H = CA * std::fabs(A) + CB * std::fabs(B);
+  if (LL > 0) goto L39;
+  L = L + 1;
+  if (std::fabs(A) - EPS * std::fabs(Cc[1]) > 0) goto L21;
+  if (std::fabs(B) - EPS * std::fabs(Cc[2]) <= 0) goto L39;
+L21:
+  if (H - CC <= 0) {
+    AA = A;
+    BB = B;
+    CC = H;
+    QQ1 = Q1;
+    QQ2 = Q2;
+  }
+  if (L - LIM <= 0) goto L28;
+  if (H - CD <= 0) goto L43;
+  if (Q[1] != 0) goto L27;
+  if (Q[2] == 0) goto L42;
+L27:
+  Q[1] = 0.;
+  Q[2] = 0.;
+  goto L7;
+L28:
+  HH = std::fmax(std::fmax(std::fabs(A1), std::fabs(B1)), std::fabs(C1));
+  if (HH <= 0) goto L42;
+  A1 = A1 / HH;
+  B1 = B1 / HH;
+  C1 = C1 / HH;
+  H = A1 * C1 - B1 * B1;
+  if (H == 0) goto L42;
+  A = A / HH;
+  B = B / HH;
+  HH = (B * A1 - A * B1) / H;
+  H = (A * C1 - B * B1) / H;
+  Q1 = Q1 + HH;
+  Q2 = Q2 + H;
+  if (std::fabs(HH) - EPS * std::fabs(Q1) > 0) goto L33;
+  if (std::fabs(H) - EPS * std::fabs(Q2) > 0) goto L33;
+  LL = 1;
+  goto L12;
+L33:
+  if (L - 1 <= 0) goto L12;
+  if (std::fabs(HH) - EPS1 * std::fabs(Q1) > 0) goto L12;
+  if (std::fabs(H) - EPS1 * std::fabs(Q2) > 0) goto L12;
+  if (std::fabs(QQQ1 * HH) - std::fabs(Q1 * DQ1) >= 0) goto L44;
+  if (std::fabs(QQQ2 * H) - std::fabs(Q2 * DQ2) < 0) goto L12;
+  goto L44;
+L38:
+  Q[1] = Cc[1];
+  Q[2] = Cc[2];
+  Q[3] = 0.;
+  Q[4] = 0.;
+  return;
+L39:
+  Q[1] = Q1;
+  Q[2] = Q2;
+  Q[3] = A;
+  Q[4] = B;
+  return;
+L40:
+  IER = -1;
+  return;
+L41:
+  IER = -2;
+  return;
+L42:
+  IER = -3;
+  goto L44;
+L43:
+  IER = 1;
+L44:
+  Q[1] = QQ1;
+  Q[2] = QQ2;
+  Q[3] = AA;
+  Q[4] = BB;
+}
+
+// SPRBM (COMPUTE_GREEN_FD.f90:1182-1351): all roots of a real polynomial
+void SPRBM(R* Cc, int IC, R* RR, R* RC, R* POL, int& IR, int& IER) {
+  int I, J, L, N, LIM, IST = 1;
+  R A, B, H, EPS, Q1, Q2, Q[5];
+  EPS = 1.E-6;
+  LIM = 100;
+  IR = IC + 1;
+L1:
+  IR = IR - 1;
+  if (IR - 1 <= 0) goto L42;
+  if (Cc[IR] == 0) goto L1;
+  IER = 0;
+  J = IR;
+  L = 0;
+  A = Cc[IR];
+  for (I = 1; I <= IR; ++I) {
+    if (L <= 0) {
+      if (Cc[I] == 0) {
+        RR[I] = 0.;
+        RC[I] = 0.;
+        POL[J] = 0.;
+        J = J - 1;
+        continue;
+      }
+      L = 1;
+      IST = I;
+      J = 0;
+    }
+    J = J + 1;
+    Cc[I] = Cc[I] / A;
+    POL[J] = Cc[I];
+    if (std::fabs(POL[J]) - 1.E27 >= 0) goto L42;
+  }
+  Q1 = 0.;
+  Q2 = 0.;
+L9:
+  if (J - 2 < 0) goto L33;
+  if (J - 2 > 0) goto L14;
+  A = POL[1];
+  RR[IST] = -A;
+  RC[IST] = 0.;
+  IR = IR - 1;
+  Q2 = 0.;
+  if (IR - 1 > 0) {
+    for (I = 2; I <= IR; ++I) {
+      Q1 = Q2;
+      Q2 = POL[I + 1];
+      POL[I] = A * Q2 + Q1;
+    }
+  }
+  POL[IR + 1] = A + Q2;
+  goto L34;
+L14:
+  for (L = 1; L <= 10; ++L) {
+    N = 1;
+  L15:
+    Q[1] = Q1;
+    Q[2] = Q2;
+    SPQFB(POL, J, Q, LIM, I);
+    if (I == 0) goto L24;
+    if (I > 0) goto L23;
+    if (Q1 != 0) goto L18;
+    if (Q2 == 0) goto L21;
+  L18:
+    if (N == 1 || N == 3) { Q1 = -Q1; N = N + 1; goto L15; }
+    if (N == 2) { Q2 = -Q2; N = N + 1; goto L15; }
+  L21:
+    Q1 = 1. + Q1;
+    Q2 = 1. - Q2;
+  }
+  IER = 3;
+  IR = IR - J;
+  goto L45;
+L23:
+  IER = 1;
+L24:
+  Q1 = Q[1];
+  Q2 = Q[2];
+  B = 0.;
+  A = 0.;
+  I = J;
+L25:
+  H = -Q1 * B - Q2 * A + POL[I];
+  POL[I] = B;
+  B = A;
+  A = H;
+  I = I - 1;
+  if (I - 2 > 0) goto L25;
+  POL[2] = B;
+  POL[1] = A;
+  L = IR - 1;
+  if (J - L <= 0) {
+    for (I = J; I <= L; ++I) POL[I - 1] = POL[I - 1] + POL[I] * Q2 + POL[I + 1] * Q1;
+  }
+  POL[L] = POL[L] + POL[L + 1] * Q2 + Q1;
+  POL[IR] = POL[IR] + Q2;
+  H = -.5 * Q2;
+  A = H * H - Q1;
+  B = std::sqrt(std::fabs(A));
+  if (A <= 0) {
+    RR[IST] = H;
+    RC[IST] = B;
+    IST = IST + 1;
+    RR[IST] = H;
+    RC[IST] = -B;
+  } else {
+    B = H + sgn(B, H);
+    RR[IST] = Q1 / B;
+    RC[IST] = 0.;
+    IST = IST + 1;
+    RR[IST] = B;
+    RC[IST] = 0.;
+  }
+  IST = IST + 1;
+  J = J - 2;
+  goto L9;
+L33:
+  IR = IR - 1;
+L34:
+  A = 0.;
+  for (I = 1; I <= IR; ++I) {
+    Q1 = Cc[I];
+    Q2 = POL[I + 1];
+    POL[I] = Q2;
+    if (Q1 != 0) Q2 = (Q1 - Q2) / Q1;
+    Q2 = std::fabs(Q2);
+    if (Q2 - A > 0) A = Q2;
+  }
+  I = IR + 1;
+  POL[I] = 1.;
+  RR[I] = A;
+  RC[I] = 0.;
+  if (IER <= 0) {
+    if (A - EPS > 0) IER = -1;
+  }
+  goto L45;
+L42:
+  IER = 2;
+  IR = 0;
+L45:
+  if (IER == 2) throw Stop(ST_SPRBM, "IER = 2 ERREUR DANS SPRBM");
+}
+
+// MCAS (COMPUTE_GREEN_FD.f90:1146-1179)
+void MCAS(int NEXP, const R* TEXP, const R* XT, const R* YT, int NPP, R* AR, R* A) {
+  const R EPS = 1.E-20;
+  for (int I = 1; I <= NEXP; ++I)
+    for (int J = 1; J <= NEXP; ++J) {
+      R S = 0;
+      for (int L = 1; L <= NPP; ++L) {
+        R TT = (TEXP[I] + TEXP[J]) * XT[L];
+        if (TT + 30 >= 0) S = S + std::exp(TT);
+      }
+      At(A, I, J) = S;
+    }
+  for (int I = 1; I <= NEXP; ++I) {
+    R S = 0;
+    for (int L = 1; L <= NPP; ++L) {
+      R TTT = TEXP[I] * XT[L];
+      if (TTT + 30 >= 0) S = S + std::exp(TTT) * YT[L];
+    }
+    At(A, I, NEXP + 1) = S;
+  }
+  HOUSRS(A, NEXP, NEXP, 1, EPS);
+  for (int I = 1; I <= NEXP; ++I) AR[I] = At(A, I, NEXP + 1);
+}
+
+// EXPORS (COMPUTE_GREEN_FD.f90:1080-1143): Prony fit of exponentials
+void EXPORS(const R* XT, const R* YT, int NJ, int& NM, R* VCOM, R* S, R* SC, R* VR, R* VC, R* POL, R* AR) {
+  int NPP = NJ + 1;
+  R H = (XT[NPP] - XT[1]) / NJ;
+  int K = NPP - NM;
+  for (int I = 1; I <= K; ++I) {
+    for (int J = 1; J <= NM; ++J) {
+      int JJ = NM - J + I;
+      At(S, I, J) = YT[JJ];
+    }
+    int II = NM + I;
+    At(S, I, NM + 1) = -YT[II];
+  }
+  R EPS = 1.E-20;
+  HOUSRS(S, K, NM, 1, EPS);
+  for (int I = 1; I <= NM; ++I) {
+    int IJ = NM - I + 1;
+    SC[IJ] = At(S, I, NM + 1);
+  }
+  int MN = NM + 1;
+  SC[MN] = 1.;
+  int IS, IER;
+  SPRBM(SC, MN, VR, VC, POL, IS, IER);
+  for (int I = 1; I <= NM; ++I) {
+    C COM(VR[I], VC[I]);
+    COM = std::log(COM) / H;
+    VR[I] = COM.real();
+    VC[I] = COM.imag();
+  }
+  int I = 1, J = 0;
+L100:
+  if (VC[I] == 0) {
+    J = J + 1;
+    VCOM[J] = VR[I];
+    I = I + 1;
+  } else if (std::fabs(VR[I] - VR[I + 1]) - 1.E-5 <= 0) {
+    J = J + 1;
+    VCOM[J] = VR[I];
+    I = I + 2;
+  } else {
+    J = J + 1;
+    VCOM[J] = VR[I];
+    I = I + 1;
+  }
+  if (I - NM <= 0) goto L100;
+  int NEXP = J;
+  J = 0;
+  for (I = 1; I <= NEXP; ++I) {
+    J = J + 1;
+    if (VCOM[I] >= 0. || VCOM[I] + 20. <= 0) { J = J - 1; continue; }
+    VCOM[J] = VCOM[I];
+  }
+  NEXP = J;
+  NM = NEXP;
+  MCAS(NEXP, VCOM, XT, YT, NPP, AR, S);
+}
+
+// LISC (COMPUTE_GREEN_FD.f90:1007-1077). AMBDA, AR are 1-based (size >= 32).
+void LISC(R AK0, R AM0, int& NM, R* AMBDA, R* AR) {
+  static thread_local std::vector<R> Sbuf;
+  Sbuf.assign(LD * 32, 0.);
+  R* S = Sbuf.data();
+  R SC[33] = {0}, VR[33] = {0}, VC[33] = {0}, POL[33] = {0};
+  R XT[122] = {0}, YT[122] = {0};
+  for (int i = 0; i < 32; ++i) AR[i] = 0.;
+  const R NEXR = 31;
+  const R PRECI = 1.E-02;
+  const int ISTIR = 0;
+  int NK = 4;
+  const R A = -0.1, B = 20.;
+L62:
+  NM = NK;
+  {
+    int NJ = 4 * NM;
+    int NPP = NJ + 1;
+    R H = (B - A) / NJ;
+    for (int I = 1; I <= NPP; ++I) {
+      XT[I] = A + (I - 1) * H;
+      YT[I] = FF(XT[I], AK0, AM0);
+    }
+    int ISOR = 0;
+    EXPORS(XT, YT, NJ, NM, AMBDA, S, SC, VR, VC, POL, AR);
+    int NPI = 2;
+    int NMO = NPI * NPP - NPI + 1;
+    R ERMAX = 0., ERMOY = 0.;
+    for (int I = 1; I <= NMO; ++I) {
+      R XX = (I - 1) * B / (NMO - 1);
+      R YY = FF(XX, AK0, AM0);
+      R TT = 0.;
+      for (int J = 1; J <= NM; ++J) {
+        R RT = AMBDA[J] * XX;
+        if (RT > -20.) TT = TT + AR[J] * std::exp(RT);
+      }
+      R DIF = YY - TT;
+      ERMOY = ERMOY + DIF;
+      ERMAX = std::fmax(ERMAX, std::fabs(DIF));
+      if (std::fabs(DIF) > PRECI) ISOR = 1;
+    }
+    ERMOY = ERMOY / NMO;
+    if (ISTIR == 1) goto L61;
+    if (ISOR == 0) goto L61;
+    NK = NK + 2;
+    if (NK - (NEXR - 1) <= 0) goto L62;
+  }
+L61:
+  for (int J = 1; J <= NM; ++J)
+    if (AMBDA[J] > 0.) throw Stop(ST_LISC, "LISC: positive exponent AMBDA");
+}
+
+// ---------------------------------------------------------------------------
+// Solver state (COM_VAR.f90) and the routines that use it
+// ---------------------------------------------------------------------------
+struct Oracle {
+  // environment
+  R RHO = 0, G = 0, Depth = 0, ZER = 0, T = 0;
+  int NP = 0, NFA = 0, IMX = 0, IXX = 0, NSYMY = 0;
+  std::vector<R> X, Y, Z;                   // 1..NP
+  std::vector<int> M1, M2, M3, M4;          // 1..NFA
+  std::vector<R> XN, YN, ZN, XG, YG, ZG, AIRE, TDIS, DIST;
+  std::vector<C> ZPB, ZPS, ZIGB, ZIGS;
+  std::vector<C> ZIJ;                       // (NFA, 2NFA) column-major
+  std::vector<C> AInv;                      // (NFA, NFA, 2^NSYMY)
+  R w_previous = -1.;
+  R FSP = 0, FSM = 0, VSXP = 0, VSYP = 0, VSZP = 0, VSXM = 0, VSYM = 0, VSZM = 0;
+  R SP1 = 0, SM1 = 0, SP2 = 0, SM2 = 0;
+  R VSXP1 = 0, VSXP2 = 0, VSYP1 = 0, VSYP2 = 0, VSZP1 = 0, VSZP2 = 0;
+  R VSXM1 = 0, VSXM2 = 0, VSYM1 = 0, VSYM2 = 0, VSZM1 = 0, VSZM2 = 0;
+  static const int NPINTE = 251;
+  R XR[329], XZ[47];
+  std::vector<R> APD1X, APD1Z, APD2X, APD2Z;  // (328,46) 1-based via apd()
+  int NQ = 0;
+  R CQ[NPINTE + 1], QQ[NPINTE + 1], AMBDA[32], AR[32];
+  bool cache_s = false;                     // store S per omega (bit-identical to recomputing)
+  std::vector<C> Sp, Sm;                    // cached S+ and S- (NFA,NFA) col-major
+  R s_cache_w = -1.;
+  std::string err;
+
+  Oracle() {
+    APD1X.assign(329 * 47, 0.); APD1Z = APD1X; APD2X = APD1X; APD2Z = APD1X;
+    std::memset(CQ, 0, sizeof CQ); std::memset(QQ, 0, sizeof QQ);
+    std::memset(AMBDA, 0, sizeof AMBDA); std::memset(AR, 0, sizeof AR);
+  }
+  static inline int ti(int I, int J) { return I + 329 * J; }
+  C& zij(int i, int j) { return ZIJ[(i - 1) + (size_t)NFA * (j - 1)]; }
+  C& ainv(int i, int j, int k) { return AInv[(i - 1) + (size_t)NFA * ((j - 1) + (size_t)NFA * (k - 1))]; }
+
+  // ---- NEMOH.f90:179-274  CREK / VNS / COFINT ------------------------------
+  void COFINT(R* CQT, R* QQT) {
+    const R PI = 4. * std::atan(1.);
+    for (int J = 1; J <= NPINTE; ++J) {
+      QQT[J] = -PI / 2. + (J - 1.) / (NPINTE - 1.) * PI;
+      if (J == 1 || J == NPINTE) CQT[J] = PI / (3. * (NPINTE - 1.));
+      else if (J % 2 != 0) CQT[J] = 2. / (3. * (NPINTE - 1.)) * PI;
+      else CQT[J] = 4. / (3. * (NPINTE - 1.)) * PI;
+    }
+  }
+  void VNS(R AKZ, R AKR, int I, int J) {
+    R QQT[NPINTE + 1], CQT[NPINTE + 1];
+    const C IM(0., 1.);
+    COFINT(CQT, QQT);
+    R FD1JX = 0., FD1JZ = 0., FD2JX = 0., FD2JZ = 0.;
+    for (int IT = 1; IT <= NPINTE; ++IT) {
+      R TETA = QQT[IT];
+      R CQIT = CQT[IT];
+      R CT = std::cos(TETA);
+      C ZIK = AKZ + IM * (AKR * CT);
+      C CEX = (ZIK.real() + 30. <= 0) ? C(0., 0.) : std::exp(ZIK);
+      C GZ = GG(ZIK, CEX);
+      C C1 = CQIT * (GZ - 1. / ZIK);
+      C C2 = CQIT * CEX;
+      FD1JX = FD1JX + CT * C1.imag();
+      FD1JZ = FD1JZ + C1.real();
+      FD2JX = FD2JX + CT * C2.imag();
+      FD2JZ = FD2JZ + C2.real();
+    }
+    APD1X[ti(I, J)] = FD1JX;
+    APD1Z[ti(I, J)] = FD1JZ;
+    APD2X[ti(I, J)] = FD2JX;
+    APD2Z[ti(I, J)] = FD2JZ;
+  }
+  void CREK() {
+    const int JZ = 46, IR = 328;
+    for (int J = 1; J <= JZ; ++J) {
+      R AKZ = std::fmin(std::fmin(std::pow(10., J / 5. - 6), std::pow(10., J / 8. - 4.5)), 16.);
+      XZ[J] = -AKZ;
+    }
+    XR[1] = 0.;
+    for (int I = 2; I <= IR; ++I) {
+      R AKR;
+      if (I < 40) AKR = std::fmin(std::pow(10., (I - 1.) / 5 - 6), 4. / 3. + std::fabs((I - 32.) / 3.));
+      else AKR = 4. / 3. + std::fabs((I - 32.) / 3.);
+      XR[I] = AKR;
+    }
+    for (int J = 1; J <= JZ; ++J)
+      for (int I = 1; I <= IR; ++I) VNS(XZ[J], XR[I], I, J);
+  }
+
+  // ---- PREPARE_MESH.f90:30-180 ---------------------------------------------
+  void PRE_PROC_MESH() {
+    IMX = NFA;
+    R GL = 0., BL = 0.;
+    for (int I = 1; I <= NP; ++I)
+      for (int J = I + 1; J <= NP; ++J) {
+        GL = std::fmax(std::fabs(X[J] - X[I]), GL);
+        if (NSYMY == 0) BL = std::fmax(std::fabs(Y[J] - Y[I]), BL);
+        if (NSYMY == 1) BL = std::fmax(std::fmax(std::fabs(Y[J]), std::fabs(Y[I])), BL);
+      }
+    if (NSYMY == 1) BL = 2. * BL;
+    GL = std::fmax(GL, BL);
+    ZER = -1.E-5 * GL;
+    IXX = IMX;
+    GOMG();
+  }
+  void GOMG() {
+    int NSYM = NSYMY + 1;
+    const R EPPM = 1.E-25;
+    for (int I = 1; I <= IMX; ++I) {
+      int K = M1[I], L = M2[I], M = M3[I], N = M4[I];
+      R T1X = X[M] - X[K], T1Y = Y[M] - Y[K], T1Z = Z[M] - Z[K];
+      R T2X = X[N] - X[L], T2Y = Y[N] - Y[L], T2Z = Z[N] - Z[L];
+      R XNX = T1Y * T2Z - T2Y * T1Z;
+      R XNY = T1Z * T2X - T2Z * T1X;
+      R XNZ = T1X * T2Y - T2X * T1Y;
+      R XNQ = std::sqrt(sq(XNX) + sq(XNY) + sq(XNZ));
+      if (XNQ <= EPPM) throw Stop(ST_PANEL_AREA, "Error: area of panel " + std::to_string(I) + " is too small");
+      XN[I] = XNX / XNQ;
+      YN[I] = XNY / XNQ;
+      ZN[I] = XNZ / XNQ;
+      R XAVER = (X[K] + X[M] + X[L] + X[N]) * 0.25;
+      R YAVER = (Y[K] + Y[M] + Y[N] + Y[L]) * 0.25;
+      R ZAVER = (Z[K] + Z[M] + Z[N] + Z[L]) * 0.25;
+      R T1 = std::sqrt(sq(T1X) + sq(T1Y) + sq(T1Z));
+      R T1UNX = T1X / T1, T1UNY = T1Y / T1, T1UNZ = T1Z / T1;
+      R T2UNX = YN[I] * T1UNZ - ZN[I] * T1UNY;
+      R T2UNY = ZN[I] * T1UNX - XN[I] * T1UNZ;
+      R T2UNZ = XN[I] * T1UNY - YN[I] * T1UNX;
+      R XI1 = T1UNX * (X[K] - XAVER) + T1UNY * (Y[K] - YAVER) + T1UNZ * (Z[K] - ZAVER);
+      R XI2 = T1UNX * (X[L] - XAVER) + T1UNY * (Y[L] - YAVER) + T1UNZ * (Z[L] - ZAVER);
+      R XI3 = T1UNX * (X[M] - XAVER) + T1UNY * (Y[M] - YAVER) + T1UNZ * (Z[M] - ZAVER);
+      R XI4 = T1UNX * (X[N] - XAVER) + T1UNY * (Y[N] - YAVER) + T1UNZ * (Z[N] - ZAVER);
+      R ETA1 = T2UNX * (X[K] - XAVER) + T2UNY * (Y[K] - YAVER) + T2UNZ * (Z[K] - ZAVER);
+      R ETA2 = T2UNX * (X[L] - XAVER) + T2UNY * (Y[L] - YAVER) + T2UNZ * (Z[L] - ZAVER);
+      R ETA3 = T2UNX * (X[M] - XAVER) + T2UNY * (Y[M] - YAVER) + T2UNZ * (Z[M] - ZAVER);
+      R ETA4 = T2UNX * (X[N] - XAVER) + T2UNY * (Y[N] - YAVER) + T2UNZ * (Z[N] - ZAVER);
+      R XIO = (XI4 * (ETA1 - ETA2) + XI2 * (ETA4 - ETA1)) / (3. * (ETA2 - ETA4));
+      R ETAO = -ETA1 / 3.;
+      R ETAN1 = ETA1 - ETAO, ETAN2 = ETA2 - ETAO, ETAN3 = ETA3 - ETAO, ETAN4 = ETA4 - ETAO;
+      R XIN1 = XI1 - XIO, XIN2 = XI2 - XIO, XIN3 = XI3 - XIO, XIN4 = XI4 - XIO;
+      XG[I] = XAVER + T1UNX * XIO + T2UNX * ETAO;
+      YG[I] = YAVER + T1UNY * XIO + T2UNY * ETAO;
+      ZG[I] = ZAVER + T1UNZ * XIO + T2UNZ * ETAO;
+      DIST[I] = 0.;
+      for (int IJJ = 1; IJJ <= NSYM; ++IJJ) {
+        int NJJ = (IJJ % 2 == 1) ? 1 : -1;   // (-1)**(IJJ+1)
+        for (int KK = 1; KK <= NP; ++KK) {
+          R DPOINT = std::fmax(std::fabs(XG[I] - X[KK]), std::fabs(YG[I] - Y[KK] * NJJ));
+          DIST[I] = std::fmax(DIST[I], DPOINT);
+        }
+      }
+      R T1b = (XIN3 - XIN1) * (XIN3 - XIN1);
+      R T2b = (XIN4 - XIN2) * (XIN4 - XIN2) + (ETAN4 - ETAN2) * (ETAN4 - ETAN2);
+      (void)T1b; (void)T2b;  // TI1 is computed but unused by the reference
+      AIRE[I] = (XIN3 - XIN1) * (ETAN4 - ETAN2) * 0.5;
+      R TT1 = std::sqrt(XIN1 * XIN1 + ETAN1 * ETAN1);
+      R TT2 = std::sqrt(XIN2 * XIN2 + ETAN2 * ETAN2);
+      R TT3 = std::sqrt(XIN3 * XIN3 + ETAN3 * ETAN3);
+      R TT4 = std::sqrt(XIN4 * XIN4 + ETAN4 * ETAN4);
+      TDIS[I] = std::fmax(std::fmax(TT1, TT2), std::fmax(TT3, TT4));
+    }
+  }
+
+  // ---- INITIALIZATION.f90:28-69 (mesh part) --------------------------------
+  void initialize(int np, int nfa, int isym, const R* xyz, const int* m1234, R rho, R g, R depth) {
+    RHO = rho; G = g; Depth = depth;
+    NFA = nfa; NP = np;
+    NSYMY = (isym == 1) ? 1 : 0;
+    X.assign(NP + 1, 0.); Y = X; Z = X;
+    for (int i = 1; i <= NP; ++i) {
+      X[i] = xyz[3 * (i - 1)]; Y[i] = xyz[3 * (i - 1) + 1]; Z[i] = xyz[3 * (i - 1) + 2];
+    }
+    M1.assign(NFA + 1, 0); M2 = M1; M3 = M1; M4 = M1;
+    for (int i = 1; i <= NFA; ++i) {
+      M1[i] = m1234[4 * (i - 1)]; M2[i] = m1234[4 * (i - 1) + 1];
+      M3[i] = m1234[4 * (i - 1) + 2]; M4[i] = m1234[4 * (i - 1) + 3];
+      for (int k = 0; k < 4; ++k)
+        if (m1234[4 * (i - 1) + k] < 1 || m1234[4 * (i - 1) + k] > NP)
+          throw Stop(ST_INVALID, "panel node index out of range");
+    }
+    XG.assign(2 * NFA + 1, 0.); YG = XG; ZG = XG;
+    AIRE.assign(NFA + 1, 0.); XN = AIRE; YN = AIRE; ZN = AIRE; DIST = AIRE; TDIS = AIRE;
+    ZIGB.assign(NFA + 1, C(0, 0)); ZIGS = ZIGB; ZPB = ZIGB; ZPS = ZIGB;
+    ZIJ.assign((size_t)NFA * 2 * NFA, C(0, 0));
+    AInv.assign((size_t)NFA * NFA * (NSYMY + 1), C(0, 0));
+    w_previous = -1.;
+    PRE_PROC_MESH();
+    CREK();
+  }
+
+  // ---- COMPUTE_GREEN_INFD.f90:33-220 VAVINFD / COMPUTE_GREEN_FD.f90:32-219 VAVFD
+  // The two differ only in DH (0 vs 2*Depth); KKK selects the ZER clip.
+  void VAV(int KKK, R DH, R XGI, R YGI, R ZGI, int ISP, int IFP) {
+    int KK[6];
+    R RR[6], DRX[6], DRY[6], DRZ[6], TXN[6], TYN[6], TZN[6], AIJS[5], VXS[5], VYS[5], VZS[5];
+    const R PI4 = std::atan(1.), PI = 4. * PI4, DPI = 2. * PI, QPI = 4. * PI;
+    int NJJ = 2 * (NSYMY + 1);
+    int MK = (KKK % 2 == 1) ? 1 : -1;     // (-1)**(KKK+1)
+    int I = ISP, J = IFP;
+    R XOI = XGI, YOI = YGI, ZOI = ZGI;
+    if (KKK == 1) {
+      if (I <= IMX) ZOI = (ZGI > ZER) ? ZER : ZGI;
+    } else {
+      if (I <= IMX) ZOI = (ZGI > ZER) ? 20 * ZER : ZGI;
+    }
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
+      int MJJ = (JJ % 2 == 1) ? 1 : -1;
+      int MY = ((JJ / 3 + 2) % 2 == 0) ? 1 : -1;
+      int MZ = ((JJ / 2 + 2) % 2 == 0) ? 1 : -1;
+      int MH = (1 - MZ) / 2;
+      R XOJ = XG[J];
+      R YOJ = YG[J] * MY;
+      R ZOJ = ZG[J] * MZ - DH * MH;
+      R A3J = XN[J];
+      R A6J = YN[J] * MY;
+      R A9J = ZN[J] * MZ;
+      R RO = std::sqrt(sq(XOI - XOJ) + sq(YOI - YOJ) + sq(ZOI - ZOJ));
+      if (RO > 7. * TDIS[J]) {
+        AIJS[JJ] = AIRE[J] / RO;
+        R ASRO = AIJS[JJ] / sq(RO);
+        VXS[JJ] = -(XOI - XOJ) * ASRO;
+        VYS[JJ] = -(YOI - YOJ) * ASRO;
+        VZS[JJ] = -(ZOI - ZOJ) * ASRO;
+      } else {
+        AIJS[JJ] = 0.; VXS[JJ] = 0.; VYS[JJ] = 0.; VZS[JJ] = 0.;
+        KK[1] = M1[J]; KK[2] = M2[J]; KK[3] = M3[J]; KK[4] = M4[J]; KK[5] = KK[1];
+        for (int L = 1; L <= 4; ++L) {
+          TXN[L] = X[KK[L]];
+          TYN[L] = Y[KK[L]] * MY;
+          TZN[L] = Z[KK[L]] * MZ - DH * MH;
+        }
+        TXN[5] = TXN[1]; TYN[5] = TYN[1]; TZN[5] = TZN[1];
+        for (int L = 1; L <= 4; ++L) {
+          RR[L] = std::sqrt(sq(XOI - TXN[L]) + sq(YOI - TYN[L]) + sq(ZOI - TZN[L]));
+          DRX[L] = (XOI - TXN[L]) / RR[L];
+          DRY[L] = (YOI - TYN[L]) / RR[L];
+          DRZ[L] = (ZOI - TZN[L]) / RR[L];
+        }
+        RR[5] = RR[1]; DRX[5] = DRX[1]; DRY[5] = DRY[1]; DRZ[5] = DRZ[1];
+        R GZ = (XOI - XOJ) * A3J + (YOI - YOJ) * A6J + (ZOI - ZOJ) * A9J;
+        for (int L = 1; L <= 4; ++L) {
+          R DK = std::sqrt(sq(TXN[L + 1] - TXN[L]) + sq(TYN[L + 1] - TYN[L]) + sq(TZN[L + 1] - TZN[L]));
+          if (DK >= 1.E-3 * TDIS[J]) {
+            R PJ = (TXN[L + 1] - TXN[L]) / DK;
+            R QJ = (TYN[L + 1] - TYN[L]) / DK;
+            R RJ = (TZN[L + 1] - TZN[L]) / DK;
+            R GYX = A6J * RJ - A9J * QJ;
+            R GYY = A9J * PJ - A3J * RJ;
+            R GYZ = A3J * QJ - A6J * PJ;
+            R GY = (XOI - TXN[L]) * GYX + (YOI - TYN[L]) * GYY + (ZOI - TZN[L]) * GYZ;
+            R SGN = sgn(1., GZ);
+            R DDK = 2. * DK;
+            R ANT = GY * DDK;
+            R DNT = sq(RR[L + 1] + RR[L]) - DK * DK + 2. * std::fabs(GZ) * (RR[L + 1] + RR[L]);
+            R ARG = ANT / DNT;
+            R ANL = RR[L + 1] + RR[L] + DK;
+            R DNL = RR[L + 1] + RR[L] - DK;
+            R DEN = ANL / DNL;
+            R ALDEN = std::log(DEN);
+            R AT = (std::fabs(GZ) >= 1.E-4 * TDIS[J]) ? std::atan(ARG) : 0.;
+            AIJS[JJ] = AIJS[JJ] + GY * ALDEN - 2. * std::fabs(GZ) * AT;
+            R DAT = 2. * AT * SGN;
+            R ANTX = GYX * DDK, ANTY = GYY * DDK, ANTZ = GYZ * DDK;
+            R ANLX = DRX[L + 1] + DRX[L], ANLY = DRY[L + 1] + DRY[L], ANLZ = DRZ[L + 1] + DRZ[L];
+            R DR = 2. * (RR[L + 1] + RR[L] + std::fabs(GZ));
+            R DS = 2. * (RR[L + 1] + RR[L]) * SGN;
+            R DNTX = DR * ANLX + A3J * DS;
+            R DNTY = DR * ANLY + A6J * DS;
+            R DNTZ = DR * ANLZ + A9J * DS;
+            R DENL = ANL * DNL;
+            R DENT = ANT * ANT + DNT * DNT;
+            R ATX = (ANTX * DNT - DNTX * ANT) / DENT;
+            R ATY = (ANTY * DNT - DNTY * ANT) / DENT;
+            R ATZ = (ANTZ * DNT - DNTZ * ANT) / DENT;
+            R DLOGG = (DNL - ANL) / DENL;
+            VXS[JJ] = VXS[JJ] + GYX * ALDEN + GY * ANLX * DLOGG - 2. * std::fabs(GZ) * ATX - DAT * A3J;
+            VYS[JJ] = VYS[JJ] + GYY * ALDEN + GY * ANLY * DLOGG - 2. * std::fabs(GZ) * ATY - DAT * A6J;
+            VZS[JJ] = VZS[JJ] + GYZ * ALDEN + GY * ANLZ * DLOGG - 2. * std::fabs(GZ) * ATZ - DAT * A9J;
+          }
+        }
+        if (I == J && JJ == 1) {
+          VXS[1] = VXS[1] - DPI * A3J;
+          VYS[1] = VYS[1] - DPI * A6J;
+          VZS[1] = VZS[1] - DPI * A9J;
+        } else {
+          AIJS[JJ] = AIJS[JJ] * MJJ;
+          VXS[JJ] = VXS[JJ] * MJJ;
+          VYS[JJ] = VYS[JJ] * MJJ;
+          VZS[JJ] = VZS[JJ] * MJJ;
+        }
+      }
+    }
+    R W;
+    if (NSYMY == 1) {
+      W = AIJS[1] - MK * (AIJS[2] + AIJS[3]) + AIJS[4]; FSP = -W / QPI;
+      W = AIJS[1] - MK * (AIJS[2] - AIJS[3]) - AIJS[4]; FSM = -W / QPI;
+      W = VXS[1] - MK * (VXS[2] + VXS[3]) + VXS[4]; VSXP = -W / QPI;
+      W = VYS[1] - MK * (VYS[2] + VYS[3]) + VYS[4]; VSYP = -W / QPI;
+      W = VZS[1] - MK * (VZS[2] + VZS[3]) + VZS[4]; VSZP = -W / QPI;
+      W = VXS[1] - MK * (VXS[2] - VXS[3]) - VXS[4]; VSXM = -W / QPI;
+      W = VYS[1] - MK * (VYS[2] - VYS[3]) - VYS[4]; VSYM = -W / QPI;
+      W = VZS[1] - MK * (VZS[2] - VZS[3]) - VZS[4]; VSZM = -W / QPI;
+    } else {
+      W = AIJS[1] - MK * AIJS[2]; FSP = -W / QPI; FSM = FSP;
+      W = VXS[1] - MK * VXS[2]; VSXP = -W / QPI; VSXM = VSXP;
+      W = VYS[1] - MK * VYS[2]; VSYP = -W / QPI; VSYM = VSYP;
+      W = VZS[1] - MK * VZS[2]; VSZP = -W / QPI; VSZM = VSZP;
+    }
+  }
+
+  // table interpolation shared by VNSINFD / VNSFD (same stencil code in both)
+  void stencil_kj(R AKZ, int& KJ) {
+    if (AKZ < -1.E-2) KJ = (int)(8 * (std::log10(-AKZ) + 4.5));
+    else KJ = (int)(5 * (std::log10(-AKZ) + 6));
+    KJ = std::max(KJ, 2);
+    KJ = std::min(KJ, 45);
+  }
+  void stencil_ki(R AKR, int& KI) {
+    if (AKR < 1.) KI = (int)(5 * (std::log10(AKR + 1.E-20) + 6) + 1);
+    else KI = (int)(3 * AKR + 28);
+    KI = std::max(KI, 2);
+    KI = std::min(KI, 327);
+  }
+  R interp(const std::vector<R>& T, int KI, int KJ, R XL1, R XL2, R XL3, R ZL1, R ZL2, R ZL3) {
+    R F1 = XL1 * T[ti(KI - 1, KJ - 1)] + XL2 * T[ti(KI, KJ - 1)] + XL3 * T[ti(KI + 1, KJ - 1)];
+    R F2 = XL1 * T[ti(KI - 1, KJ)] + XL2 * T[ti(KI, KJ)] + XL3 * T[ti(KI + 1, KJ)];
+    R F3 = XL1 * T[ti(KI - 1, KJ + 1)] + XL2 * T[ti(KI, KJ + 1)] + XL3 * T[ti(KI + 1, KJ + 1)];
+    return ZL1 * F1 + ZL2 * F2 + ZL3 * F3;
+  }
+
+  // ---- COMPUTE_GREEN_INFD.f90:223-503 VNSINFD ------------------------------
+  void VNSINFD(int KKK, int ISP, int IFP, R XGI, R YGI, R ZGI) {
+    (void)KKK;
+    R FS1[3], FS2[3], VSX1[3], VSY1[3], VSZ1[3], VSX2[3], VSY2[3], VSZ2[3];
+    const R PI4 = std::atan(1.), PI = 4. * PI4, DPI = 2. * PI;
+    const C ZI(0., 1.);
+    const R DPI2 = 2. * PI * PI;
+    const R EPS = 0.0001;
+    R WH = DPI / T, WR = WH;
+    if (std::fabs(WR) < 1.E-4) throw Stop(ST_OMEGA, "ABS(WR) < 1.E-4");
+    R AK0 = WR * WR / G;
+    int NJJ = NSYMY + 1;
+    int I = ISP, J = IFP;
+    R ZMIII = 0.;
+    if (I <= IMX) { ZMIII = ZGI; if (ZGI > ZER) ZMIII = ZER; }
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
+      int BX = (JJ % 2 == 1) ? 1 : -1;
+      if (ZGI < ZER && ZG[J] < ZER) {
+        R YMJJJ = YG[J] * BX;
+        R RRR = std::sqrt(sq(XGI - XG[J]) + sq(YGI - YMJJJ));
+        R AKR = AK0 * RRR;
+        R ZZZ = ZMIII + ZG[J];
+        R AKZ = AK0 * ZZZ;
+        R DD = std::sqrt(sq(RRR) + sq(ZZZ));
+        R PSURR = (DD > EPS) ? PI / cube(AK0 * DD) : 0.;
+        R PD1Z = 0, PD2Z = 0, VZ1 = 0, VZ2 = 0, PD1X = 0, PD2X = 0, VR1 = 0, VR2 = 0;
+        R XL1 = 0, XL2 = 0, XL3 = 0, ZL1 = 0, ZL2 = 0, ZL3 = 0, EPZ = 0, SQ = 0, CSK = 0, SIK = 0;
+        int KI = 0, KJ = 0;
+        if (AKZ > -1.5E-6) {
+          throw Stop(ST_AKZ_UNDEFINED, "AKZ > -1.5E-6: wave term undefined in the reference");
+        } else {
+          if (AKZ > -16.) {
+            if (AKR < 99.7) {
+              stencil_kj(AKZ, KJ);
+              stencil_ki(AKR, KI);
+              XL1 = PL2(XR[KI], XR[KI + 1], XR[KI - 1], AKR);
+              XL2 = PL2(XR[KI + 1], XR[KI - 1], XR[KI], AKR);
+              XL3 = PL2(XR[KI - 1], XR[KI], XR[KI + 1], AKR);
+              ZL1 = PL2(XZ[KJ], XZ[KJ + 1], XZ[KJ - 1], AKZ);
+              ZL2 = PL2(XZ[KJ + 1], XZ[KJ - 1], XZ[KJ], AKZ);
+              ZL3 = PL2(XZ[KJ - 1], XZ[KJ], XZ[KJ + 1], AKZ);
+              PD1Z = interp(APD1Z, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+              PD2Z = interp(APD2Z, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+            } else {
+              EPZ = std::exp(AKZ);
+              R AKP4 = AKR - PI4;
+              SQ = std::sqrt(DPI / AKR);
+              CSK = std::cos(AKP4);
+              SIK = std::sin(AKP4);
+              PD1Z = PSURR * AKZ - PI * EPZ * SQ * SIK;
+              PD2Z = EPZ * SQ * CSK;
+            }
+            VZ1 = PD1Z - PSURR * AKZ;
+            VZ2 = PD2Z;
+          } else {
+            PD1Z = PSURR * AKZ;
+            PD2Z = 0.;
+            VZ1 = 0.;
+            VZ2 = 0.;
+          }
+        }
+        FS1[JJ] = PD1Z;
+        FS2[JJ] = PD2Z;
+        if (RRR > EPS) {
+          if (AKZ <= -1.5E-6) {
+            if (AKZ > -16.) {
+              if (AKR < 99.7) {
+                PD1X = interp(APD1X, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+                PD2X = interp(APD2X, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+              } else {
+                R DSK = 0.5 / AKR;
+                PD1X = -PSURR * AKR + PI * EPZ * SQ * (CSK - DSK * SIK);
+                PD2X = EPZ * SQ * (SIK + DSK * CSK);
+              }
+              VR1 = -PD1X - PSURR * AKR;
+              VR2 = -PD2X;
+            } else {
+              PD1X = -PSURR * AKR;
+              PD2X = 0.;
+              VR1 = 0.;
+              VR2 = 0.;
+            }
+          }
+          R CVX = (XGI - XG[J]) / RRR;
+          R CVY = (YGI - YMJJJ) / RRR;
+          VSX1[JJ] = VR1 * CVX;
+          VSX2[JJ] = VR2 * CVX;
+          VSY1[JJ] = VR1 * CVY;
+          VSY2[JJ] = VR2 * CVY;
+          VSZ1[JJ] = VZ1;
+          VSZ2[JJ] = VZ2;
+        } else {
+          VSX1[JJ] = 0.; VSX2[JJ] = 0.; VSY1[JJ] = 0.; VSY2[JJ] = 0.;
+          VSZ1[JJ] = VZ1; VSZ2[JJ] = VZ2;
+        }
+      } else {
+        // free-surface panel branch (COMPUTE_GREEN_INFD.f90:385-453)
+        FS1[JJ] = 0.; FS2[JJ] = 0.; VSX1[JJ] = 0.; VSX2[JJ] = 0.;
+        VSY1[JJ] = 0.; VSY2[JJ] = 0.; VSZ1[JJ] = 0.; VSZ2[JJ] = 0.;
+        int KK[6] = {0, M1[J], M2[J], M3[J], M4[J], M1[J]};
+        C ZIJv[6], CEX[6], GZ[6];
+        for (int IT = 1; IT <= NQ; ++IT) {
+          R TETA = QQ[IT];
+          R CT = std::cos(TETA);
+          R ST = std::sin(TETA);
+          for (int L = 1; L <= 4; ++L) {
+            ZIJv[L] = AK0 * (ZMIII + Z[KK[L]] + ZI * ((XGI - X[KK[L]]) * CT + (YGI - Y[KK[L]] * BX) * ST));
+            CEX[L] = (ZIJv[L].real() > -25.) ? std::exp(ZIJv[L]) : C(0., 0.);
+            GZ[L] = GG(ZIJv[L], CEX[L]);
+          }
+          ZIJv[5] = ZIJv[1]; CEX[5] = CEX[1]; GZ[5] = GZ[1];
+          C ZA(0., 0.), ZB(0., 0.), ZVS(0., 0.);
+          for (int L = 1; L <= 4; ++L) {
+            C C1 = ZIJv[L + 1] - ZIJv[L];
+            C ASD, BSD, CSD;
+            if (std::fabs(C1.imag()) < EPS && std::fabs(C1.real()) < EPS) {
+              ASD = (GZ[L + 1] + GZ[L]) * 0.5;
+              BSD = (CEX[L + 1] + CEX[L]) * 0.5;
+              CSD = ASD - (0.5 / ZIJv[L + 1] + 0.5 / ZIJv[L]);
+            } else {
+              CSD = (GZ[L + 1] - GZ[L]) / C1;
+              ASD = (GZ[L + 1] - GZ[L] + std::log(ZIJv[L + 1] / ZIJv[L])) / C1;
+              BSD = (CEX[L + 1] - CEX[L]) / C1;
+            }
+            C C2 = (YN[J] * BX - ZI * ZN[J] * ST) * (X[KK[L + 1]] - X[KK[L]]) -
+                   (XN[J] - ZI * ZN[J] * CT) * (Y[KK[L + 1]] - Y[KK[L]]) * (R)BX;
+            ZA = ZA + ASD * C2;
+            ZB = ZB + BSD * C2;
+            ZVS = ZVS + CSD * C2;
+          }
+          FS1[JJ] = FS1[JJ] + CQ[IT] * ZA.real();
+          FS2[JJ] = FS2[JJ] + CQ[IT] * ZB.real();
+          VSX1[JJ] = VSX1[JJ] - CQ[IT] * CT * ZVS.imag();
+          VSX2[JJ] = VSX2[JJ] - CQ[IT] * CT * ZB.imag();
+          VSY1[JJ] = VSY1[JJ] - CQ[IT] * ST * ZVS.imag();
+          VSY2[JJ] = VSY2[JJ] - CQ[IT] * ST * ZB.imag();
+          VSZ1[JJ] = VSZ1[JJ] + CQ[IT] * ZVS.real();
+          VSZ2[JJ] = VSZ2[JJ] + CQ[IT] * ZB.real();
+        }
+        R AKAIR = AK0 * AIRE[J];
+        FS1[JJ] = FS1[JJ] * BX / AKAIR;
+        FS2[JJ] = FS2[JJ] * BX / AKAIR;
+        VSX1[JJ] = VSX1[JJ] * BX / AKAIR;
+        VSX2[JJ] = VSX2[JJ] * BX / AKAIR;
+        VSY1[JJ] = VSY1[JJ] * BX / AKAIR;
+        VSY2[JJ] = VSY2[JJ] * BX / AKAIR;
+        VSZ1[JJ] = VSZ1[JJ] * BX / AKAIR;
+        VSZ2[JJ] = VSZ2[JJ] * BX / AKAIR;
+      }
+    }
+    R AKAIR = AK0 * AIRE[J];
+    R ADPI2 = AKAIR / DPI2;
+    R ADPI = AKAIR / DPI;
+    R AKDPI2 = ADPI2 * AK0;
+    R AKDPI = ADPI * AK0;
+    if (NSYMY == 1) {
+      SM1 = FSM - (FS1[1] - FS1[2]) * ADPI2;
+      SP1 = FSP - (FS1[1] + FS1[2]) * ADPI2;
+      SM2 = -(FS2[1] - FS2[2]) * ADPI;
+      SP2 = -(FS2[1] + FS2[2]) * ADPI;
+      VSXP1 = VSXP - (VSX1[1] + VSX1[2]) * AKDPI2;
+      VSXM1 = VSXM - (VSX1[1] - VSX1[2]) * AKDPI2;
+      VSYP1 = VSYP - (VSY1[1] + VSY1[2]) * AKDPI2;
+      VSYM1 = VSYM - (VSY1[1] - VSY1[2]) * AKDPI2;
+      VSZP1 = VSZP - (VSZ1[1] + VSZ1[2]) * AKDPI2;
+      VSZM1 = VSZM - (VSZ1[1] - VSZ1[2]) * AKDPI2;
+      VSXP2 = -(VSX2[1] + VSX2[2]) * AKDPI;
+      VSXM2 = -(VSX2[1] - VSX2[2]) * AKDPI;
+      VSYP2 = -(VSY2[1] + VSY2[2]) * AKDPI;
+      VSYM2 = -(VSY2[1] - VSY2[2]) * AKDPI;
+      VSZP2 = -(VSZ2[1] + VSZ2[2]) * AKDPI;
+      VSZM2 = -(VSZ2[1] - VSZ2[2]) * AKDPI;
+    } else {
+      SP1 = FSP - FS1[1] * ADPI2;
+      SM1 = SP1;
+      SP2 = -FS2[1] * ADPI;
+      SM2 = SP2;
+      VSXP1 = VSXP - VSX1[1] * AKDPI2; VSXM1 = VSXP1;
+      VSYP1 = VSYP - VSY1[1] * AKDPI2; VSYM1 = VSYP1;
+      VSZP1 = VSZP - VSZ1[1] * AKDPI2; VSZM1 = VSZP1;
+      VSXP2 = -VSX2[1] * AKDPI; VSXM2 = VSXP2;
+      VSYP2 = -VSY2[1] * AKDPI; VSYM2 = VSYP2;
+      VSZP2 = -VSZ2[1] * AKDPI; VSZM2 = VSZP2;
+    }
+  }
+
+  // ---- COMPUTE_GREEN_FD.f90:1514-1609 VSD ----------------------------------
+  void VSD(const R* XFT, const R* YFT, const R* ZFT, int JJ, R XNF, R YNF, R ZNF, R A, R TD, R XGJ, R YGJ,
+           R ZGJ, R XGI, R YGI, R ZIG, R& FS, R& VX, R& VY, R& VZ) {
+    const R QPI = 4. * 4. * std::atan(1.);
+    int MJJ = (JJ % 2 == 1) ? 1 : -1;
+    R QMP = MJJ / (2 * QPI);
+    R RR[6], DRX[6], DRY[6], DRZ[6];
+    R RO = std::sqrt(sq(XGI - XGJ) + sq(YGI - YGJ * MJJ) + sq(ZIG - ZGJ));
+    R GZ = (XGI - XGJ) * XNF + (YGI - YGJ * MJJ) * YNF * MJJ + (ZIG - ZGJ) * ZNF;
+    if (RO > 7 * TD) {
+      FS = -A / (RO * 2 * QPI);
+      R ASRO = FS / sq(RO);
+      VX = -(XGI - XGJ) * ASRO;
+      VY = -(YGI - YGJ * MJJ) * ASRO;
+      VZ = -(ZIG - ZGJ) * ASRO;
+      return;
+    }
+    for (int L = 1; L <= 4; ++L) {
+      RR[L] = std::sqrt(sq(XGI - XFT[L]) + sq(YGI - YFT[L] * MJJ) + sq(ZIG - ZFT[L]));
+      DRX[L] = (XGI - XFT[L]) / RR[L];
+      DRY[L] = (YGI - YFT[L] * MJJ) / RR[L];
+      DRZ[L] = (ZIG - ZFT[L]) / RR[L];
+    }
+    RR[5] = RR[1]; DRX[5] = DRX[1]; DRY[5] = DRY[1]; DRZ[5] = DRZ[1];
+    R AIJS = 0., VXS = 0., VYS = 0., VZS = 0.;
+    for (int L = 1; L <= 4; ++L) {
+      R DK = std::sqrt(sq(XFT[L + 1] - XFT[L]) + sq(YFT[L + 1] - YFT[L]) + sq(ZFT[L + 1] - ZFT[L]));
+      if (DK >= 1.E-3 * TD) {
+        R PJ = (XFT[L + 1] - XFT[L]) / DK;
+        R QJ = (YFT[L + 1] - YFT[L]) * MJJ / DK;
+        R RJ = (ZFT[L + 1] - ZFT[L]) / DK;
+        R GYX = YNF * MJJ * RJ - ZNF * QJ;
+        R GYY = ZNF * PJ - XNF * RJ;
+        R GYZ = XNF * QJ - YNF * MJJ * PJ;
+        R GY = (XGI - XFT[L]) * GYX + (YGI - YFT[L] * MJJ) * GYY + (ZIG - ZFT[L]) * GYZ;
+        R SGN = sgn(1., GZ);
+        R DDK = 2. * DK;
+        R ANT = GY * DDK;
+        R DNT = sq(RR[L + 1] + RR[L]) - DK * DK + 2. * std::fabs(GZ) * (RR[L + 1] + RR[L]);
+        R ANL = RR[L + 1] + RR[L] + DK;
+        R DNL = RR[L + 1] + RR[L] - DK;
+        R DEN = ANL / DNL;
+        R ALDEN = std::log(DEN);
+        R AT;
+        if (std::fabs(GZ) > 1.E-4 * TD) {
+          R ARG = ANT / DNT;
+          AT = std::atan(ARG);
+        } else {
+          AT = 0.;
+        }
+        AIJS = AIJS + GY * ALDEN - 2. * std::fabs(GZ) * AT;
+        R DAT = 2. * AT * SGN;
+        R ANTX = GYX * DDK, ANTY = GYY * DDK, ANTZ = GYZ * DDK;
+        R ANLX = DRX[L + 1] + DRX[L], ANLY = DRY[L + 1] + DRY[L], ANLZ = DRZ[L + 1] + DRZ[L];
+        R DR = 2. * (RR[L + 1] + RR[L] + std::fabs(GZ));
+        R DS = 2. * (RR[L + 1] + RR[L]) * SGN;
+        R DNTX = DR * ANLX + XNF * DS;
+        R DNTY = DR * ANLY + YNF * MJJ * DS;
+        R DNTZ = DR * ANLZ + ZNF * DS;
+        R DENL = ANL * DNL;
+        R DENT = ANT * ANT + DNT * DNT;
+        R ATX = (ANTX * DNT - DNTX * ANT) / DENT;
+        R ATY = (ANTY * DNT - DNTY * ANT) / DENT;
+        R ATZ = (ANTZ * DNT - DNTZ * ANT) / DENT;
+        R DLG = (DNL - ANL) / DENL;
+        VXS = VXS + GYX * ALDEN + GY * ANLX * DLG - 2. * std::fabs(GZ) * ATX - DAT * XNF;
+        VYS = VYS + GYY * ALDEN + GY * ANLY * DLG - 2. * std::fabs(GZ) * ATY - DAT * YNF * MJJ;
+        VZS = VZS + GYZ * ALDEN + GY * ANLZ * DLG - 2. * std::fabs(GZ) * ATZ - DAT * ZNF;
+      }
+    }
+    FS = -AIJS * QMP;
+    VX = -VXS * QMP;
+    VY = -VYS * QMP;
+    VZ = -VZS * QMP;
+  }
+
+  // ---- COMPUTE_GREEN_FD.f90:222-868 VNSFD ----------------------------------
+  // one tabulated image: wave value PD1Z/PD2Z, VZ (the 0001-0012 blocks)
+  struct Img { R ZZZ, AKZ, DD, RR, PSR, PSURR, PD1Z, PD2Z, VZ1, VZ2, PD1X, PD2X, VR2, EPZ, ZL1, ZL2, ZL3; int KJ; };
+
+  void VNSFD(R AM0, R AMH, int NEXP, int ISP, int IFP, R XGI, R YGI, R ZGI) {
+    R FS1[3], FS2[3], VSX1[3], VSY1[3], VSZ1[3], VSX2[3], VSY2[3], VSZ2[3];
+    const R PI4 = std::atan(1.), PI = 4. * std::atan(1.), DPI = 2. * PI, QPI = 4. * PI;
+    const C ZI(0., 1.);
+    R H = Depth;
+    R AKH = AMH * std::tanh(AMH);
+    R A = sq(AMH + AKH) / (H * (sq(AMH) - sq(AKH) + AKH));
+    int NEXP1 = NEXP + 1;
+    AMBDA[NEXP1] = 0.;
+    AR[NEXP1] = 2.;
+    R ADPI2 = -A / (8. * sq(PI));
+    R ADPI = -A / (8 * PI);
+    R COE1 = ADPI2 / AM0, COE2 = ADPI / AM0, COE3 = ADPI2, COE4 = ADPI;
+    const R EPS = 0.0001;
+    int NJJ = NSYMY + 1;
+    int I = ISP, J = IFP;
+    R ZMIII;
+    if (I <= IMX) {
+      ZMIII = ZGI;
+      if (ZGI > ZER) ZMIII = 20 * ZER;
+    } else {
+      ZMIII = 20 * ZER;
+    }
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
+      int BX = (JJ % 2 == 1) ? 1 : -1;
+      if (ZGI < ZER && ZG[J] < ZER) {
+        R YMJJJ = BX * YG[J];
+        R COF1 = COE3 * AIRE[J], COF2 = COE4 * AIRE[J];
+        R COF3 = AM0 * COF1, COF4 = AM0 * COF2;
+        R RRR = std::sqrt(sq(XGI - XG[J]) + sq(YGI - YMJJJ));
+        R AKR = AM0 * RRR;
+        Img im[5];
+        im[1].ZZZ = ZMIII + ZG[J];
+        im[2].ZZZ = ZG[J] - ZMIII - 2 * H;
+        im[3].ZZZ = ZMIII - ZG[J] - 2 * H;
+        im[4].ZZZ = -ZG[J] - ZMIII - 4 * H;
+        R XL1 = 0, XL2 = 0, XL3 = 0, SQ = 0, CSK = 0, SIK = 0, PSK = 0, SCK = 0, SCDS = 0, SSDS = 0;
+        int KI = 0;
+        for (int k = 1; k <= 4; ++k) {
+          Img& m = im[k];
+          m.AKZ = AM0 * m.ZZZ;
+          m.DD = std::sqrt(sq(RRR) + sq(m.ZZZ));
+          if (m.DD > EPS) {
+            m.RR = AM0 * m.DD;
+            m.PSR = PI / m.RR;
+            m.PSURR = PI / cube(m.RR);
+          } else {
+            m.PSR = 0.;
+            m.PSURR = 0.;
+          }
+          if (m.AKZ > -1.5E-6) {
+            throw Stop(ST_AKZ_UNDEFINED, "AKZ > -1.5E-6: wave term undefined in the reference");
+          }
+          if (m.AKZ > -16.) {
+            if (AKR < 99.7) {
+              stencil_kj(m.AKZ, m.KJ);
+              if (k == 1) {
+                stencil_ki(AKR, KI);
+                XL1 = PL2(XR[KI], XR[KI + 1], XR[KI - 1], AKR);
+                XL2 = PL2(XR[KI + 1], XR[KI - 1], XR[KI], AKR);
+                XL3 = PL2(XR[KI - 1], XR[KI], XR[KI + 1], AKR);
+              }
+              m.ZL1 = PL2(XZ[m.KJ], XZ[m.KJ + 1], XZ[m.KJ - 1], m.AKZ);
+              m.ZL2 = PL2(XZ[m.KJ + 1], XZ[m.KJ - 1], XZ[m.KJ], m.AKZ);
+              m.ZL3 = PL2(XZ[m.KJ - 1], XZ[m.KJ], XZ[m.KJ + 1], m.AKZ);
+              m.PD1Z = interp(APD1Z, KI, m.KJ, XL1, XL2, XL3, m.ZL1, m.ZL2, m.ZL3);
+              m.PD2Z = interp(APD2Z, KI, m.KJ, XL1, XL2, XL3, m.ZL1, m.ZL2, m.ZL3);
+            } else {
+              m.EPZ = std::exp(m.AKZ);
+              if (k == 1) {
+                R AKP4 = AKR - PI4;
+                SQ = std::sqrt(DPI / AKR);
+                CSK = std::cos(AKP4);
+                SIK = std::sin(AKP4);
+                PSK = PI * SQ * SIK;
+                SCK = SQ * CSK;
+              }
+              m.PD1Z = m.PSURR * m.AKZ - PSK * m.EPZ;
+              m.PD2Z = m.EPZ * SCK;
+            }
+            m.VZ1 = m.PD1Z - m.PSURR * m.AKZ;
+            m.VZ2 = m.PD2Z;
+          } else {
+            m.PD1Z = m.PSURR * m.AKZ;
+            m.PD2Z = 0.;
+            m.VZ1 = 0.;
+            m.VZ2 = 0.;
+          }
+        }
+        R QTQQ = im[1].PD1Z + im[2].PD1Z + im[3].PD1Z + im[4].PD1Z;
+        FS1[JJ] = COF1 * (QTQQ - im[1].PSR - im[2].PSR - im[3].PSR - im[4].PSR);
+        R STSS = im[1].PD2Z + im[2].PD2Z + im[3].PD2Z + im[4].PD2Z;
+        FS2[JJ] = COF2 * STSS;
+        if (I <= IMX) {
+          if (RRR > EPS) {
+            for (int k = 1; k <= 4; ++k) {
+              Img& m = im[k];
+              if (m.AKZ <= -1.5E-6) {
+                if (m.AKZ > -16.) {
+                  if (AKR < 99.7) {
+                    m.PD1X = interp(APD1X, KI, m.KJ, XL1, XL2, XL3, m.ZL1, m.ZL2, m.ZL3);
+                    m.PD2X = interp(APD2X, KI, m.KJ, XL1, XL2, XL3, m.ZL1, m.ZL2, m.ZL3);
+                  } else {
+                    if (k == 1) {
+                      R DSK = 0.5 / AKR;
+                      SCDS = PI * SQ * (CSK - DSK * SIK);
+                      SSDS = SQ * (SIK + DSK * CSK);
+                    }
+                    m.PD1X = -m.PSURR * AKR - m.EPZ * SCDS;
+                    m.PD2X = m.EPZ * SSDS;
+                  }
+                  m.VR2 = -m.PD2X;
+                } else {
+                  m.PD1X = -m.PSURR * AKR;
+                  m.PD2X = 0.;
+                  m.VR2 = 0.;
+                }
+              }
+            }
+            R C1V3 = -COF3 * (im[1].PD1X + im[2].PD1X + im[3].PD1X + im[4].PD1X);
+            R C2V3 = COF4 * (im[1].VR2 + im[2].VR2 + im[3].VR2 + im[4].VR2);
+            R CVX = (XGI - XG[J]) / RRR;
+            R CVY = (YGI - YMJJJ) / RRR;
+            VSX1[JJ] = C1V3 * CVX;
+            VSX2[JJ] = C2V3 * CVX;
+            VSY1[JJ] = C1V3 * CVY;
+            VSY2[JJ] = C2V3 * CVY;
+          } else {
+            VSX1[JJ] = 0.; VSX2[JJ] = 0.; VSY1[JJ] = 0.; VSY2[JJ] = 0.;
+          }
+          VSZ1[JJ] = COF3 * (im[1].PD1Z - im[2].PD1Z + im[3].PD1Z - im[4].PD1Z);
+          VSZ2[JJ] = COF4 * (im[1].VZ2 - im[2].VZ2 + im[3].VZ2 - im[4].VZ2);
+        }
+        R XPG = XGI - XG[J];
+        R YPG = YGI - YMJJJ;
+        R ACT = -0.5 * AIRE[J] / QPI;
+        for (int KE = 1; KE <= NEXP1; ++KE) {
+          R AQT = ACT * AR[KE];
+          R ZPG[5];
+          ZPG[1] = ZMIII - 2. * H + H * AMBDA[KE] - ZG[J];
+          ZPG[2] = -ZMIII - H * AMBDA[KE] - ZG[J];
+          ZPG[3] = -ZMIII - 4. * H + H * AMBDA[KE] - ZG[J];
+          ZPG[4] = ZMIII + 2. * H - H * AMBDA[KE] - ZG[J];
+          R FTS[5], VXSk[5], VYSk[5], VZSk[5];
+          for (int k = 1; k <= 4; ++k) {
+            R RRk = sq(RRR) + sq(ZPG[k]);
+            R ROk = std::sqrt(RRk);
+            R ASRO;
+            if (ROk > EPS) {
+              FTS[k] = AQT / ROk;
+              ASRO = FTS[k] / RRk;
+            } else {
+              FTS[k] = 0.;
+              ASRO = 0.;
+            }
+            VXSk[k] = -XPG * ASRO;
+            VYSk[k] = -YPG * ASRO;
+            VZSk[k] = -ZPG[k] * ASRO;
+          }
+          FS1[JJ] = FS1[JJ] + FTS[1] + FTS[2] + FTS[3] + FTS[4];
+          if (I <= IMX) {
+            VSX1[JJ] = VSX1[JJ] + (VXSk[1] + VXSk[2] + VXSk[3] + VXSk[4]);
+            VSY1[JJ] = VSY1[JJ] + (VYSk[1] + VYSk[2] + VYSk[3] + VYSk[4]);
+            VSZ1[JJ] = VSZ1[JJ] + (VZSk[1] - VZSk[2] - VZSk[3] + VZSk[4]);
+          }
+        }
+      } else {
+        // free-surface panel branch (COMPUTE_GREEN_FD.f90:707-826)
+        FS1[JJ] = 0.; FS2[JJ] = 0.; VSX1[JJ] = 0.; VSX2[JJ] = 0.;
+        VSY1[JJ] = 0.; VSY2[JJ] = 0.; VSZ1[JJ] = 0.; VSZ2[JJ] = 0.;
+        int KK[6] = {0, M1[J], M2[J], M3[J], M4[J], M1[J]};
+        C ZIJv[5][6], CEX[5][6], GZv[5][6], CL[5][6];
+        for (int IT = 1; IT <= NQ; ++IT) {
+          R TETA = QQ[IT];
+          R CT = std::cos(TETA);
+          R ST = std::sin(TETA);
+          for (int L = 1; L <= 4; ++L) {
+            R OM = (XGI - X[KK[L]]) * CT + (YGI - BX * Y[KK[L]]) * ST;
+            ZIJv[1][L] = AM0 * (Z[KK[L]] + ZMIII + ZI * OM);
+            ZIJv[2][L] = AM0 * (Z[KK[L]] - ZMIII - 2 * H + ZI * OM);
+            ZIJv[3][L] = AM0 * (ZMIII - Z[KK[L]] - 2 * H + ZI * OM);
+            ZIJv[4][L] = AM0 * (-Z[KK[L]] - ZMIII - 4 * H + ZI * OM);
+            for (int KL = 1; KL <= 4; ++KL) {
+              CEX[KL][L] = (ZIJv[KL][L].real() > -25.) ? std::exp(ZIJv[KL][L]) : C(0., 0.);
+              GZv[KL][L] = GG(ZIJv[KL][L], CEX[KL][L]);
+              CL[KL][L] = std::log(-ZIJv[KL][L]);
+            }
+          }
+          for (int KL = 1; KL <= 4; ++KL) {
+            ZIJv[KL][5] = ZIJv[KL][1]; CEX[KL][5] = CEX[KL][1];
+            GZv[KL][5] = GZv[KL][1]; CL[KL][5] = CL[KL][1];
+          }
+          C S1(0, 0), S2(0, 0), ZV1(0, 0), ZV2(0, 0), ZV3(0, 0), ZV4(0, 0);
+          C ZIRS = ZI * ZN[J] * ST;
+          C ZIRC = ZI * ZN[J] * CT;
+          for (int L = 1; L <= 4; ++L) {
+            R DXL = (X[KK[L + 1]] - X[KK[L]]);
+            R DYL = (Y[KK[L + 1]] - Y[KK[L]]) * BX;
+            for (int KL = 1; KL <= 4; ++KL) {
+              int BKL = (KL % 2 == 1) ? 1 : -1;
+              C AUX;
+              if (KL < 3) AUX = DXL * (YN[J] * BX - ZIRS) - DYL * (XN[J] - ZIRC);
+              else AUX = DXL * (-YN[J] * BX - ZIRS) - DYL * (-XN[J] - ZIRC);
+              C Z1 = ZIJv[KL][L + 1], Z0 = ZIJv[KL][L];
+              C CL1 = CL[KL][L + 1], CL0 = CL[KL][L];
+              C G1 = GZv[KL][L + 1], G0 = GZv[KL][L];
+              C CEX1 = CEX[KL][L + 1], CEX0 = CEX[KL][L];
+              C ZAM = Z1 - Z0;
+              if (std::fabs(ZAM.imag()) < EPS && std::fabs(ZAM.real()) < EPS) {
+                S1 = S1 + AUX * (G1 + G0 + CL1 + CL0) * 0.5;
+                ZV1 = ZV1 + AUX * (R)BKL * (G1 + G0) * 0.5;
+                ZV3 = ZV3 + AUX * (G1 + G0) * 0.5;
+                S2 = S2 + AUX * (CEX1 + CEX0) * 0.5;
+                ZV2 = ZV2 + AUX * (R)BKL * (CEX1 + CEX0) * 0.5;
+                ZV4 = ZV4 + AUX * (CEX1 + CEX0) * 0.5;
+              } else {
+                S1 = S1 + AUX * (G1 - G0 + CL1 - CL0 + Z1 * CL1 - Z0 * CL0 - ZAM) / ZAM;
+                ZV1 = ZV1 + AUX * (R)BKL * (G1 - G0 + CL1 - CL0) / ZAM;
+                ZV3 = ZV3 + AUX * (G1 - G0 + CL1 - CL0) / ZAM;
+                S2 = S2 + AUX * (CEX1 - CEX0) / ZAM;
+                ZV2 = ZV2 + AUX * (R)BKL * (CEX1 - CEX0) / ZAM;
+                ZV4 = ZV4 + AUX * (CEX1 - CEX0) / ZAM;
+              }
+            }
+          }
+          FS1[JJ] = FS1[JJ] + CQ[IT] * S1.real() * COE1 * BX;
+          FS2[JJ] = FS2[JJ] + CQ[IT] * S2.real() * COE2 * BX;
+          VSX1[JJ] = VSX1[JJ] - CQ[IT] * CT * ZV3.imag() * COE3 * BX;
+          VSX2[JJ] = VSX2[JJ] - CQ[IT] * CT * ZV4.imag() * COE4 * BX;
+          VSY1[JJ] = VSY1[JJ] - CQ[IT] * ST * ZV3.imag() * COE3 * BX;
+          VSY2[JJ] = VSY2[JJ] - CQ[IT] * ST * ZV4.imag() * COE4 * BX;
+          VSZ1[JJ] = VSZ1[JJ] + CQ[IT] * ZV1.real() * COE3 * BX;
+          VSZ2[JJ] = VSZ2[JJ] + CQ[IT] * ZV2.real() * COE4 * BX;
+        }
+        R ZP[5];
+        ZP[1] = -ZMIII;
+        ZP[2] = ZMIII + 2 * H;
+        ZP[3] = ZMIII - 2. * H;
+        ZP[4] = -ZMIII - 4 * H;
+        R XFT[6], YFT[6], ZFT[6];
+        for (int L = 1; L <= 5; ++L) { XFT[L] = X[KK[L]]; YFT[L] = Y[KK[L]]; ZFT[L] = Z[KK[L]]; }
+        for (int KE = 1; KE <= NEXP1; ++KE) {
+          R FFS1, FFS2, FFS3, FFS4, VX1, VX2, VX3, VX4, VY1, VY2, VY3, VY4, VZ1, VZ2, VZ3, VZ4;
+          VSD(XFT, YFT, ZFT, JJ, XN[J], YN[J], ZN[J], AIRE[J], TDIS[J], XG[J], YG[J], ZG[J], XGI, YGI,
+              ZP[1] - H * AMBDA[KE], FFS1, VX1, VY1, VZ1);
+          VSD(XFT, YFT, ZFT, JJ, XN[J], YN[J], ZN[J], AIRE[J], TDIS[J], XG[J], YG[J], ZG[J], XGI, YGI,
+              ZP[2] - H * AMBDA[KE], FFS2, VX2, VY2, VZ2);
+          VSD(XFT, YFT, ZFT, JJ, XN[J], YN[J], ZN[J], AIRE[J], TDIS[J], XG[J], YG[J], ZG[J], XGI, YGI,
+              ZP[3] + H * AMBDA[KE], FFS3, VX3, VY3, VZ3);
+          VSD(XFT, YFT, ZFT, JJ, XN[J], YN[J], ZN[J], AIRE[J], TDIS[J], XG[J], YG[J], ZG[J], XGI, YGI,
+              ZP[4] + H * AMBDA[KE], FFS4, VX4, VY4, VZ4);
+          FS1[JJ] = FS1[JJ] + (FFS1 + FFS2 + FFS3 + FFS4) * AR[KE];
+          if (I <= IMX) {
+            VSX1[JJ] = VSX1[JJ] + (VX1 + VX2 + VX3 + VX4) * AR[KE];
+            VSY1[JJ] = VSY1[JJ] + (VY1 + VY2 + VY3 + VY4) * AR[KE];
+            VSZ1[JJ] = VSZ1[JJ] + (-VZ1 + VZ2 + VZ3 - VZ4) * AR[KE];
+          }
+        }
+      }
+    }
+    if (NSYMY == 1) {
+      SM1 = FSM + FS1[1] - FS1[2];
+      SP1 = FSP + FS1[1] + FS1[2];
+      SM2 = FS2[1] - FS2[2];
+      SP2 = FS2[1] + FS2[2];
+      VSXP1 = VSXP + VSX1[1] + VSX1[2];
+      VSXM1 = VSXM + VSX1[1] - VSX1[2];
+      VSYP1 = VSYP + VSY1[1] + VSY1[2];
+      VSYM1 = VSYM + VSY1[1] - VSY1[2];
+      VSZP1 = VSZP + VSZ1[1] + VSZ1[2];
+      VSZM1 = VSZM + VSZ1[1] - VSZ1[2];
+      VSXP2 = VSX2[1] + VSX2[2];
+      VSXM2 = VSX2[1] - VSX2[2];
+      VSYP2 = VSY2[1] + VSY2[2];
+      VSYM2 = VSY2[1] - VSY2[2];
+      VSZP2 = VSZ2[1] + VSZ2[2];
+      VSZM2 = VSZ2[1] - VSZ2[2];
+    } else {
+      SP1 = FSP + FS1[1];
+      SM1 = SP1;
+      SP2 = FS2[1];
+      SM2 = SP2;
+      VSXP1 = VSXP + VSX1[1]; VSXM1 = VSXP1;
+      VSYP1 = VSYP + VSY1[1]; VSYM1 = VSYP1;
+      VSZP1 = VSZP + VSZ1[1]; VSZM1 = VSZP1;
+      VSXP2 = VSX2[1]; VSXM2 = VSXP2;
+      VSYP2 = VSY2[1]; VSYM2 = VSYP2;
+      VSZP2 = VSZ2[1]; VSZM2 = VSZP2;
+    }
+  }
+
+  // ---- M_SOLVER.f90:31-104 GAUSSZ on ZIJ (leading dim NFA) -----------------
+  void GAUSSZ(int N, int M) {
+    const R EPS = 1.E-20;
+    for (int J = 1; J <= N - 1; ++J) {
+      int K = J;
+      for (int I = J + 1; I <= N; ++I)
+        if ((std::abs(zij(K, J)) - std::abs(zij(I, J))) <= 0.) K = I;
+      if ((K - J) <= 0) {
+        for (int L = J; L <= M; ++L) {
+          C Cc = zij(J, L);
+          zij(J, L) = zij(K, L);
+          zij(K, L) = Cc;
+        }
+      } else {
+        if ((std::abs(zij(J, J)) - EPS) <= 0.) throw Stop(ST_PIVOT, "PIVOT INFERIEUR A 1.E-20");
+      }
+      for (int Kc = J + 1; Kc <= M; ++Kc) {
+        C P = zij(J, Kc) / zij(J, J);
+        C* colK = &zij(1, Kc);
+        C* colJ = &zij(1, J);
+        for (int I = J + 1; I <= N; ++I) colK[I - 1] = colK[I - 1] - colJ[I - 1] * P;
+      }
+    }
+    if ((std::abs(zij(N, N)) - EPS) <= 0.) throw Stop(ST_PIVOT, "PIVOT INFERIEUR A 1.E-20");
+    for (int IL = N + 1; IL <= M; ++IL) {
+      C* colIL = &zij(1, IL);
+      for (int J = N; J >= 1; --J) {
+        colIL[J - 1] = colIL[J - 1] / zij(J, J);
+        C* colJ = &zij(1, J);
+        for (int I = 1; I <= J - 1; ++I) colIL[I - 1] = colIL[I - 1] - colJ[I - 1] * colIL[J - 1];
+      }
+    }
+  }
+
+  // ---- SOLVE_BEM_{INFD,FD}_DIRECT.f90 (shared structure) -------------------
+  R compute_GM() {
+    int NJJ = NSYMY + 1;
+    R GM = 0.;
+    for (int I = 1; I <= NP - 1; ++I)
+      for (int JJ = 1; JJ <= NJJ; ++JJ) {
+        R BJ = (JJ % 2 == 1) ? 1. : -1.;
+        for (int J = I + 1; J <= NP; ++J) {
+          R DIJ = std::sqrt(sq(X[J] - X[I]) + sq(Y[I] - Y[J] * BJ));
+          GM = std::fmax(DIJ, GM);
+        }
+      }
+    return GM;
+  }
+  // green(): one pair, both symmetry classes, as the INFD/FD routines
+  void green(bool fd, R AM0, R AMH, int NEXP, int I, int J) {
+    if (!fd) {
+      VAV(1, 0., XG[I], YG[I], ZG[I], I, J);
+      VNSINFD(1, I, J, XG[I], YG[I], ZG[I]);
+    } else {
+      VAV(2, 2 * Depth, XG[I], YG[I], ZG[I], I, J);
+      VNSFD(AM0, AMH, NEXP, I, J, XG[I], YG[I], ZG[I]);
+    }
+  }
+
+  // Returns NEXP (0 for infinite depth).
+  int solve_potential(bool fd, const C* NVEL, R AMH_in) {
+    int NJJ = NSYMY + 1;
+    const R PI = 4. * std::atan(1.), DPI = 2. * PI;
+    R W = DPI / T;
+    R AM0, AMH = AMH_in;
+    int NEXP = 0, N = 0;
+    if (!fd) {
+      AM0 = W * W / G;
+    } else {
+      R AKH = W * W * Depth / G;
+      AKH = AMH * std::tanh(AMH);
+      AM0 = AMH / Depth;
+      (void)AKH;
+      if (std::fabs(W) < 1.E-4) throw Stop(ST_OMEGA, "ABS(WR) < 1.E-4");
+    }
+    for (int i = 0; i <= NPINTE; ++i) { CQ[i] = 0.; QQ[i] = 0.; }
+    if (fd) for (int i = 0; i < 32; ++i) { AMBDA[i] = 0.; AR[i] = 0.; }
+    VSXP = 0.; VSXM = 0.; VSYP = 0.; VSYM = 0.; VSZP = 0.; VSZM = 0.;
+    R GM = compute_GM();
+    R AKK = AM0 * GM;
+    if (!fd) {
+      cint(AKK, N, QQ, CQ);       // CINT_INFD writes the module CQ, QQ
+      N = NQ;                     // SOLVE_BEM_INFD_DIRECT.f90:79 (NQ not set)
+    } else {
+      R lq[NPINTE + 1], lc[NPINTE + 1];
+      cint(AKK, N, lq, lc);       // CINT_FD fills local arrays only
+      NQ = N;
+      R AKH = AMH * std::tanh(AMH);
+      LISC(AKH, AMH, NEXP, AMBDA, AR);
+    }
+    std::vector<C> ZOL((size_t)IMX * 2, C(0, 0));
+    std::vector<C> B(IMX + 1);
+    if (W != w_previous) {
+      w_previous = W;
+      bool keep = cache_s;
+      if (keep) { Sp.assign((size_t)IMX * IMX, C(0, 0)); Sm = Sp; s_cache_w = W; }
+      for (int ISYM = 1; ISYM <= NJJ; ++ISYM) {
+        for (size_t q = 0; q < ZIJ.size(); ++q) ZIJ[q] = C(0, 0);
+        for (int ISP = 1; ISP <= IMX; ++ISP)
+          for (int IFP = 1; IFP <= IMX; ++IFP) {
+            green(fd, AM0, AMH, NEXP, ISP, IFP);
+            R PCOS, PSIN;
+            if (ISYM == 1) {
+              PCOS = VSXP1 * XN[ISP] + VSYP1 * YN[ISP] + VSZP1 * ZN[ISP];
+              PSIN = VSXP2 * XN[ISP] + VSYP2 * YN[ISP] + VSZP2 * ZN[ISP];
+              if (keep) {
+                Sp[(ISP - 1) + (size_t)IMX * (IFP - 1)] = C(SP1, SP2);
+                Sm[(ISP - 1) + (size_t)IMX * (IFP - 1)] = C(SM1, SM2);
+              }
+            } else {
+              PCOS = VSXM1 * XN[ISP] + VSYM1 * YN[ISP] + VSZM1 * ZN[ISP];
+              PSIN = VSXM2 * XN[ISP] + VSYM2 * YN[ISP] + VSZM2 * ZN[ISP];
+            }
+            zij(ISP, IFP) = C(PCOS, PSIN);
+          }
+        for (int I = 1; I <= IMX; ++I) {
+          for (int Jc = 1; Jc <= IMX; ++Jc) zij(I, Jc + IMX) = C(0., 0.);
+          zij(I, I + IMX) = C(1., 0.);
+        }
+        GAUSSZ(IMX, 2 * IMX);
+        for (int I = 1; I <= IMX; ++I)
+          for (int Jc = 1; Jc <= IMX; ++Jc) ainv(I, Jc, ISYM) = zij(I, IMX + Jc);
+      }
+    }
+    for (int ISYM = 1; ISYM <= NJJ; ++ISYM) {
+      R BX = (ISYM % 2 == 1) ? 1. : -1.;
+      for (int I = 1; I <= IMX; ++I) {
+        if (NSYMY == 1) B[I] = (NVEL[I - 1] + BX * NVEL[I - 1 + NFA]) * 0.5;
+        else B[I] = NVEL[I - 1];
+      }
+      for (int I = 1; I <= IMX; ++I) {
+        C acc(0., 0.);
+        for (int K = 1; K <= IMX; ++K) acc = acc + ainv(I, K, ISYM) * B[K];
+        ZOL[(I - 1) + (size_t)IMX * (ISYM - 1)] = acc;
+      }
+    }
+    for (int I = 1; I <= IMX; ++I) {
+      if (NSYMY == 0) {
+        ZIGB[I] = ZOL[I - 1];
+        ZIGS[I] = 0.0;
+      } else {
+        ZIGB[I] = (ZOL[I - 1] + ZOL[I - 1 + IMX]);
+        ZIGS[I] = (ZOL[I - 1] - ZOL[I - 1 + IMX]);
+      }
+    }
+    bool use_cache = cache_s && s_cache_w == W && !Sp.empty();
+    for (int I = 1; I <= IMX; ++I) {
+      ZPB[I] = C(0, 0);
+      ZPS[I] = C(0, 0);
+    }
+    for (int I = 1; I <= IMX; ++I)
+      for (int J = 1; J <= IMX; ++J) {
+        R sp1, sp2, sm1, sm2;
+        if (use_cache) {
+          C a = Sp[(I - 1) + (size_t)IMX * (J - 1)], b = Sm[(I - 1) + (size_t)IMX * (J - 1)];
+          sp1 = a.real(); sp2 = a.imag(); sm1 = b.real(); sm2 = b.imag();
+        } else {
+          green(fd, AM0, AMH, NEXP, I, J);
+          sp1 = SP1; sp2 = SP2; sm1 = SM1; sm2 = SM2;
+        }
+        ZPB[I] = ZPB[I] + 0.5 * (ZIGB[J] * C(sp1 + sm1, sp2 + sm2) + ZIGS[J] * C(sp1 - sm1, sp2 - sm2));
+        ZPS[I] = ZPS[I] + 0.5 * (ZIGS[J] * C(sp1 + sm1, sp2 + sm2) + ZIGB[J] * C(sp1 - sm1, sp2 - sm2));
+      }
+    return NEXP;
+  }
+
+  // ---- SOLVE_BEM.f90:28-96 SOLVE_BVP (solve part and pressure) ------------
+  // Returns NEXP; fills PRESSURE (2^s*NFA) if non-null.
+  int solve_bvp(R Period, const C* NVEL, C* PRESSURE, bool* used_fd) {
+    const R PI = 4. * std::atan(1.);
+    const C II(0., 1.);
+    T = Period;
+    R W = 2. * PI / T;
+    R kwave = W * W / G;
+    int NEXP = 0;
+    bool fd = !((Depth == 0.) || (kwave * Depth >= 20));
+    if (!fd) {
+      solve_potential(false, NVEL, 0.);
+    } else {
+      R AKH = W * W * Depth / G;
+      R AMH = X0(AKH);
+      NEXP = solve_potential(true, NVEL, AMH);
+    }
+    if (used_fd) *used_fd = fd;
+    if (PRESSURE) {
+      for (int i = 1; i <= NFA; ++i) {
+        PRESSURE[i - 1] = RHO * II * W * ZPB[i];
+        if (NSYMY == 1) PRESSURE[i - 1 + NFA] = RHO * II * W * ZPS[i];
+      }
+    }
+    return NEXP;
+  }
+
+  // matrices of one omega (no solve): D+, D-, S+, S- column-major NFA x NFA
+  void assemble(R omega, C* dp, C* dm, C* sp, C* sm, int* depth_mode, int* nexp_out) {
+    const R PI = 4. * std::atan(1.);
+    R Period = 2. * PI / omega;
+    T = Period;
+    R W = 2. * PI / T;
+    R kwave = W * W / G;
+    bool fd = !((Depth == 0.) || (kwave * Depth >= 20));
+    R AM0, AMH = 0.;
+    int NEXP = 0, N = 0;
+    for (int i = 0; i <= NPINTE; ++i) { CQ[i] = 0.; QQ[i] = 0.; }
+    VSXP = 0.; VSXM = 0.; VSYP = 0.; VSYM = 0.; VSZP = 0.; VSZM = 0.;
+    R GM = compute_GM();
+    if (!fd) {
+      AM0 = W * W / G;
+      cint(AM0 * GM, N, QQ, CQ);
+    } else {
+      R AKH = W * W * Depth / G;
+      AMH = X0(AKH);
+      AM0 = AMH / Depth;
+      for (int i = 0; i < 32; ++i) { AMBDA[i] = 0.; AR[i] = 0.; }
+      R lq[NPINTE + 1], lc[NPINTE + 1];
+      cint(AM0 * GM, N, lq, lc);
+      NQ = N;
+      LISC(AMH * std::tanh(AMH), AMH, NEXP, AMBDA, AR);
+    }
+    for (int I = 1; I <= IMX; ++I)
+      for (int J = 1; J <= IMX; ++J) {
+        green(fd, AM0, AMH, NEXP, I, J);
+        size_t q = (I - 1) + (size_t)IMX * (J - 1);
+        dp[q] = C(VSXP1 * XN[I] + VSYP1 * YN[I] + VSZP1 * ZN[I], VSXP2 * XN[I] + VSYP2 * YN[I] + VSZP2 * ZN[I]);
+        dm[q] = C(VSXM1 * XN[I] + VSYM1 * YN[I] + VSZM1 * ZN[I], VSXM2 * XN[I] + VSYM2 * YN[I] + VSZM2 * ZN[I]);
+        sp[q] = C(SP1, SP2);
+        sm[q] = C(SM1, SM2);
+      }
+    if (depth_mode) *depth_mode = fd ? 1 : 0;
+    if (nexp_out) *nexp_out = NEXP;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// list-directed reader (each READ starts a new record, values may span lines)
+// ---------------------------------------------------------------------------
+struct ListReader {
+  std::vector<std::string> lines;
+  size_t pos = 0;
+  explicit ListReader(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) throw Stop(ST_IO, "cannot open " + path);
+    std::string s;
+    while (std::getline(f, s)) lines.push_back(s);
+  }
+  void skip() { ++pos; }
+  std::vector<std::string> read(size_t n) {
+    std::vector<std::string> v;
+    while (v.size() < n) {
+      if (pos >= lines.size()) throw Stop(ST_IO, "unexpected end of file");
+      std::string s = lines[pos++];
+      size_t bang = s.find('!');
+      if (bang != std::string::npos) s = s.substr(0, bang);
+      for (char& ch : s) if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      std::istringstream is(s);
+      std::string t;
+      while (is >> t) v.push_back(t);
+    }
+    v.resize(n);
+    return v;
+  }
+  double d() { return std::stod(read(1)[0]); }
+};
+
+// NEMOH.f90:30-176 main program, on the case named by <root>/ID.dat
+int run_case(const std::string& root, bool cache_s, double* seconds) {
+  auto t0 = std::chrono::steady_clock::now();
+  std::string pre = root.empty() ? "" : root + "/";
+  ListReader idr(pre + "ID.dat");
+  int lid = std::stoi(idr.read(1)[0]);
+  std::string id = idr.read(1)[0].substr(0, lid);
+  std::string dir = pre + id;
+  ListReader l10(dir + "/mesh/L10.dat");
+  l10.skip();
+  auto h = l10.read(4);
+  int np = std::stoi(h[1]), nfa = std::stoi(h[2]);
+  ListReader l12(dir + "/mesh/L12.dat");
+  auto h2 = l12.read(2);
+  if (std::stoi(h2[0]) != 2) throw Stop(ST_IO, "The mesh file format is not correct.");
+  int isym = std::stoi(h2[1]);
+  std::vector<double> xyz(3 * np);
+  for (int i = 0; i < np; ++i) {
+    auto v = l12.read(4);
+    for (int k = 0; k < 3; ++k) xyz[3 * i + k] = std::stod(v[1 + k]);
+  }
+  l12.skip();
+  std::vector<int> m(4 * nfa);
+  for (int i = 0; i < nfa; ++i) {
+    auto v = l12.read(4);
+    for (int k = 0; k < 4; ++k) m[4 * i + k] = std::stoi(v[k]);
+  }
+  int nc = nfa * (isym == 1 ? 2 : 1);
+  ListReader bc(dir + "/Normalvelocities.dat");
+  int npb = std::stoi(bc.read(1)[0]);
+  std::vector<double> omega(npb), stype(npb);
+  auto vo = bc.read(npb);
+  for (int j = 0; j < npb; ++j) omega[j] = std::stod(vo[j]);
+  auto vt = bc.read(npb);
+  for (int j = 0; j < npb; ++j) stype[j] = std::stod(vt[j]);
+  for (int k = 0; k < 3; ++k) bc.read(npb);
+  std::vector<C> nvel((size_t)nc * npb);
+  for (int c = 0; c < nc; ++c) {
+    auto v = bc.read(2 * npb);
+    for (int j = 0; j < npb; ++j) nvel[c + (size_t)nc * j] = C(std::stod(v[2 * j]), std::stod(v[2 * j + 1]));
+  }
+  ListReader cal(dir + "/Nemoh.cal");
+  cal.skip();
+  double rho = cal.d(), g = cal.d(), depth = cal.d();
+  { ListReader inp(dir + "/input.txt"); inp.skip(); }
+  ListReader ig(dir + "/mesh/Integration.dat");
+  int nint = std::stoi(ig.read(1)[0]);
+  std::vector<double> nds((size_t)nint * nc);
+  for (int i = 0; i < nint; ++i) {
+    auto v = ig.read(nc);
+    for (int c = 0; c < nc; ++c) nds[i + (size_t)nint * c] = std::stod(v[c]);
+  }
+  { ListReader kr(dir + "/mesh/Kochin.dat"); kr.read(1); }
+  { ListReader fr(dir + "/mesh/Freesurface.dat"); fr.read(2); }
+  Oracle o;
+  o.cache_s = cache_s;
+  o.initialize(np, nfa, isym, xyz.data(), m.data(), rho, g, depth);
+  const double PI = 4. * std::atan(1.);
+  std::vector<C> force((size_t)nint * npb, C(0, 0)), pressure(nc);
+  for (int j = 0; j < npb; ++j) {
+    o.solve_bvp(2. * PI / omega[j], &nvel[(size_t)nc * j], pressure.data(), nullptr);
+    for (int i = 0; i < nint; ++i)
+      for (int c = 0; c < nc; ++c)
+        force[i + (size_t)nint * j] = force[i + (size_t)nint * j] - pressure[c] * nds[i + (size_t)nint * c];
+  }
+  std::ofstream out(dir + "/results/Forces.dat");
+  if (!out) throw Stop(ST_IO, "cannot write " + dir + "/results/Forces.dat");
+  char buf[64];
+  for (int c = 0; c < nint; ++c) {
+    for (int j = 0; j < npb; ++j) {
+      C F = force[c + (size_t)nint * j];
+      double a, b;
+      if (stype[j] != -1.) { a = std::abs(F); b = std::atan2(F.imag(), F.real()); }
+      else { a = F.imag() / omega[j]; b = -F.real(); }
+      std::snprintf(buf, sizeof buf, " %.17E %.17E", a, b);
+      out << buf;
+    }
+    out << "\n";
+  }
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return 0;
+}
+
+thread_local std::string g_last_error;
+
+}  // namespace
+
+// =============================================================================
+// C API used by the tests (ctypes) and by bench.py's CPU-baseline leg
+// =============================================================================
+extern "C" {
+
+const char* nemoh_oracle_last_error() { return g_last_error.c_str(); }
+
+#define ORACLE_TRY(...)                                            \
+  try {                                                            \
+    __VA_ARGS__;                                                          \
+    return 0;                                                      \
+  } catch (const Stop& e) {                                        \
+    g_last_error = e.what();                                       \
+    return e.code;                                                 \
+  } catch (const std::exception& e) {                              \
+    g_last_error = e.what();                                       \
+    return ST_INVALID;                                             \
+  }
+
+int nemoh_oracle_create(void** h, int np, int nfa, int isym, const double* xyz, const int* m1234, double rho,
+                        double g, double depth) {
+  ORACLE_TRY({
+    Oracle* o = new Oracle();
+    try {
+      o->initialize(np, nfa, isym, xyz, m1234, rho, g, depth);
+    } catch (...) {
+      delete o;
+      throw;
+    }
+    *h = o;
+  })
+}
+
+void nemoh_oracle_destroy(void* h) { delete static_cast<Oracle*>(h); }
+
+void nemoh_oracle_set_cache_s(void* h, int on) { static_cast<Oracle*>(h)->cache_s = on != 0; }
+
+// geometry: out[8*NFA] = XN, YN, ZN, XG, YG, ZG, AIRE, TDIS (each NFA); zer
+int nemoh_oracle_geometry(void* h, double* out, double* zer) {
+  Oracle* o = static_cast<Oracle*>(h);
+  int n = o->NFA;
+  for (int i = 1; i <= n; ++i) {
+    out[0 * n + i - 1] = o->XN[i]; out[1 * n + i - 1] = o->YN[i]; out[2 * n + i - 1] = o->ZN[i];
+    out[3 * n + i - 1] = o->XG[i]; out[4 * n + i - 1] = o->YG[i]; out[5 * n + i - 1] = o->ZG[i];
+    out[6 * n + i - 1] = o->AIRE[i]; out[7 * n + i - 1] = o->TDIS[i];
+  }
+  *zer = o->ZER;
+  return 0;
+}
+
+// tables: xr[328], xz[46], apd[4*328*46] = APD1X, APD1Z, APD2X, APD2Z column-major (I,J)
+int nemoh_oracle_tables(void* h, double* xr, double* xz, double* apd) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int i = 1; i <= 328; ++i) xr[i - 1] = o->XR[i];
+  for (int j = 1; j <= 46; ++j) xz[j - 1] = o->XZ[j];
+  const std::vector<R>* t[4] = {&o->APD1X, &o->APD1Z, &o->APD2X, &o->APD2Z};
+  for (int k = 0; k < 4; ++k)
+    for (int j = 1; j <= 46; ++j)
+      for (int i = 1; i <= 328; ++i) apd[k * 328 * 46 + (i - 1) + 328 * (j - 1)] = (*t[k])[Oracle::ti(i, j)];
+  return 0;
+}
+
+int nemoh_oracle_assemble(void* h, double omega, double* dp, double* dm, double* sp, double* sm, int* depth_mode,
+                          int* nexp) {
+  ORACLE_TRY(static_cast<Oracle*>(h)->assemble(omega, (C*)dp, (C*)dm, (C*)sp, (C*)sm, depth_mode, nexp))
+}
+
+// SOLVE_BVP for one problem; pressure may be null. nq_state in/out mirrors NQ.
+int nemoh_oracle_solve_problem(void* h, double period, const double* nvel, double* zigb, double* zigs,
+                               double* zpb, double* zps, double* pressure, int* nexp, int* used_fd) {
+  ORACLE_TRY({
+    Oracle* o = static_cast<Oracle*>(h);
+    bool fd = false;
+    int ne = o->solve_bvp(period, (const C*)nvel, (C*)pressure, &fd);
+    for (int i = 1; i <= o->NFA; ++i) {
+      if (zigb) ((C*)zigb)[i - 1] = o->ZIGB[i];
+      if (zigs) ((C*)zigs)[i - 1] = o->ZIGS[i];
+      if (zpb) ((C*)zpb)[i - 1] = o->ZPB[i];
+      if (zps) ((C*)zps)[i - 1] = o->ZPS[i];
+    }
+    if (nexp) *nexp = ne;
+    if (used_fd) *used_fd = fd ? 1 : 0;
+  })
+}
+
+int nemoh_oracle_get_nq(void* h) { return static_cast<Oracle*>(h)->NQ; }
+void nemoh_oracle_set_nq(void* h, int nq) { static_cast<Oracle*>(h)->NQ = nq; }
+
+int nemoh_oracle_run_case(const char* root, int cache_s, double* seconds) {
+  ORACLE_TRY(run_case(root ? root : "", cache_s != 0, seconds))
+}
+
+void nemoh_oracle_gg(double zr, double zi, double cr, double ci, double* out) {
+  C g = GG(C(zr, zi), C(cr, ci));
+  out[0] = g.real();
+  out[1] = g.imag();
+}
+
+double nemoh_oracle_x0(double ak) {
+  try { return X0(ak); } catch (const Stop& e) { g_last_error = e.what(); return -1.; }
+}
+
+// LISC for given (AKH, AMH): ambda[31], ar[31] (0-based copies of AMBDA(1..), AR(1..))
+int nemoh_oracle_lisc(double akh, double amh, int* nexp, double* ambda, double* ar) {
+  ORACLE_TRY({
+    R A[32] = {0}, B[32] = {0};
+    int nm = 0;
+    LISC(akh, amh, nm, A, B);
+    *nexp = nm;
+    for (int i = 1; i <= 31; ++i) { ambda[i - 1] = A[i]; ar[i - 1] = B[i]; }
+  })
+}
+
+// cint: N and the nodes/weights (1..N) for a given AKK
+int nemoh_oracle_cint(double akk, double* qq, double* cq) {
+  R q[102], c[102];
+  int n = 0;
+  cint(akk, n, q, c);
+  for (int i = 1; i <= n; ++i) { qq[i - 1] = q[i]; cq[i - 1] = c[i]; }
+  return n;
+}
+
+// GAUSSZ-based inverse of an n x n complex matrix (column-major), for tests
+int nemoh_oracle_gaussz_inverse(int n, const double* a, double* ainv) {
+  ORACLE_TRY({
+    Oracle o;
+    o.NFA = n;
+    o.ZIJ.assign((size_t)n * 2 * n, C(0, 0));
+    const C* A = (const C*)a;
+    for (int j = 1; j <= n; ++j)
+      for (int i = 1; i <= n; ++i) o.zij(i, j) = A[(i - 1) + (size_t)n * (j - 1)];
+    for (int i = 1; i <= n; ++i) o.zij(i, i + n) = C(1, 0);
+    o.GAUSSZ(n, 2 * n);
+    C* out = (C*)ainv;
+    for (int j = 1; j <= n; ++j)
+      for (int i = 1; i <= n; ++i) out[(i - 1) + (size_t)n * (j - 1)] = o.zij(i, n + j);
+  })
+}
+
+}  // extern "C"
+
+#ifdef NEMOH_ORACLE_MAIN
+int main(int argc, char** argv) {
+  const char* root = argc > 1 ? argv[1] : "";
+  double secs = 0;
+  int st = nemoh_oracle_run_case(root, 1, &secs);
+  if (st) {
+    std::fprintf(stderr, "nemoh_oracle: error %d: %s\n", st, nemoh_oracle_last_error());
+    return st;
+  }
+  std::printf("Forces.dat written in %.3f s\n", secs);
+  return 0;
+}
+#endif
