@@ -1,0 +1,106 @@
+/*
+ * nemoh_b200 C-ABI: the per-frequency BEM solve of Nemoh on an NVIDIA B200.
+ *
+ * Drop-in for the reference Solver's direct BEM solve:
+ *   SOLVE_POTENTIAL_INFD_DIRECT(NVEL)          Solver/Core/SOLVE_BEM_INFD_DIRECT.f90:34
+ *   SOLVE_POTENTIAL_FD_DIRECT(NVEL,AMH,NEXP)   Solver/Core/SOLVE_BEM_FD_DIRECT.f90:33
+ * as dispatched by SOLVE_BVP (Solver/Core/SOLVE_BEM.f90:28-117), with the mesh
+ * and environment set up as INITIALIZE does (Solver/Core/INITIALIZATION.f90:28-69).
+ *
+ * Conventions
+ *  - Arrays are caller-owned host buffers unless a name ends in _device.
+ *  - Complex numbers are interleaved (re, im) doubles; matrices column-major.
+ *  - Every call returns a status: 0 = OK, otherwise one of NEMOH_B200_E*;
+ *    nemoh_b200_last_error() gives the message. Each STOP of the reference
+ *    maps to a status (no process exit).
+ *  - A context is used by one host thread at a time. Separate contexts may
+ *    run concurrently on separate host threads.
+ */
+#ifndef NEMOH_B200_H
+#define NEMOH_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nemoh_ctx nemoh_ctx;
+
+/* status codes */
+#define NEMOH_B200_OK 0
+#define NEMOH_B200_EINVAL 1          /* bad argument */
+#define NEMOH_B200_EPANEL_AREA 2     /* PREPARE_MESH.f90:112-120 "area of panel is too small" */
+#define NEMOH_B200_EPIVOT 3          /* M_SOLVER.f90:49-52,61-64 "PIVOT INFERIEUR A 1e-20" */
+#define NEMOH_B200_EOMEGA 4          /* COMPUTE_GREEN_INFD.f90:252-255 |W| < 1e-4 */
+#define NEMOH_B200_ELISC 5           /* COMPUTE_GREEN_FD.f90:1073 positive exponent */
+#define NEMOH_B200_ESPRBM 6          /* COMPUTE_GREEN_FD.f90:1311-1314 root finder failure */
+#define NEMOH_B200_EDISPERSION 7     /* COMPUTE_GREEN_FD.f90:1656-1660 no dispersion root */
+#define NEMOH_B200_EAKZ 8            /* COMPUTE_GREEN_INFD.f90:284-289 wave term undefined */
+#define NEMOH_B200_EIO 9             /* file format / IO (drop-in driver) */
+#define NEMOH_B200_EHOUSRS 10        /* COMPUTE_GREEN_FD.f90:1461-1477 least squares */
+#define NEMOH_B200_ECUDA 20          /* CUDA runtime error */
+#define NEMOH_B200_ENOMEM 21         /* device memory exhausted / admission refused */
+#define NEMOH_B200_ENODEV 22         /* no CUDA device */
+#define NEMOH_B200_ECAPACITY 23      /* size beyond a documented limit */
+
+/* precision modes */
+#define NEMOH_B200_FP64 0            /* FP64 assembly, FP64 LU */
+#define NEMOH_B200_MIXED 1           /* FP64 assembly, FP32 LU with split-BF16 tensor-core updates,
+                                        FP64 iterative refinement */
+
+/* Create a context on a CUDA device; builds the Green-function tables
+ * (CREK, Solver/NEMOH.f90:179-274) on that device. */
+int nemoh_b200_create(nemoh_ctx** ctx, int device, int precision_mode);
+int nemoh_b200_destroy(nemoh_ctx* ctx);
+const char* nemoh_b200_last_error(const nemoh_ctx* ctx);
+
+/* Mesh and environment: INITIALIZE + PRE_PROC_MESH (INITIALIZATION.f90:44-67,
+ * PREPARE_MESH.f90:30-180). xyz is 3 x np (x,y,z per node); m1234 is
+ * 4 x nfa 1-based node ids; nsymy = 1 for a y-symmetric half mesh.
+ * depth = 0 means infinite depth. Resets the factor cache. */
+int nemoh_b200_set_mesh(nemoh_ctx* ctx, int np, int nfa, int nsymy, const double* xyz, const int* m1234,
+                        double rho, double g, double depth);
+
+/* One problem, the reference's boundary exactly (SOLVE_BEM.f90:62-96 with
+ * SOLVE_POTENTIAL_*_DIRECT): period T, normal velocities nvel (2^nsymy * nfa
+ * complex). Outputs (nfa complex each, any may be NULL): source strengths
+ * zigb, zigs and boundary potentials zpb, zps; nexp (finite depth exponential
+ * count, 0 in deep water). The factorization is cached while 2*pi/T equals
+ * the previous call's (the reference's w_previous, SOLVE_BEM_INFD_DIRECT.f90:82). */
+int nemoh_b200_solve_problem(nemoh_ctx* ctx, double period, const double* nvel, double* zigb, double* zigs,
+                             double* zpb, double* zps, int* nexp);
+
+/* Batched fast path: nomega frequencies, each with nrhs problems (nrhs <= 16).
+ * nvel: (2^s nfa) x nrhs x nomega complex; nds: nint x (2^s nfa) real
+ * (mesh/Integration.dat, NEMOH.f90:88-94); force: nint x nrhs x nomega
+ * complex, Force = -sum_c PRESSURE(c) NDS(i,c) with PRESSURE = rho i W phi
+ * (NEMOH.f90:137-141, SOLVE_BEM.f90:91-96). Frequencies are processed in the
+ * given order (the order matters only for the reference's free-surface-panel
+ * quadrature state, see DESIGN). */
+int nemoh_b200_solve_frequencies(nemoh_ctx* ctx, int nomega, const double* omegas, int nrhs, const double* nvel,
+                                 int nint, const double* nds, double* force);
+
+/* Same with device-resident inputs/outputs (pointers from cudaMalloc on the
+ * context's device) on the given CUDA stream (cudaStream_t as void*). */
+int nemoh_b200_solve_frequencies_device(nemoh_ctx* ctx, int nomega, const double* omegas, int nrhs,
+                                        const double* nvel_device, int nint, const double* nds_device,
+                                        double* force_device, void* stream);
+
+/* Diagnostics used by the parity tests. */
+/* influence matrices of one frequency (each nfa x nfa complex, column-major):
+ * dp/dm = ZIJ of symmetry class +/-, sp/sm = single-layer S+/S- (SP1+i SP2, SM1+i SM2);
+ * depth_mode = 1 if the finite-depth Green function was used. */
+int nemoh_b200_assemble(nemoh_ctx* ctx, double omega, double* dp, double* dm, double* sp, double* sm,
+                        int* depth_mode);
+/* xr[328], xz[46], apd[4*328*46] = APD1X, APD1Z, APD2X, APD2Z column-major (I,J) */
+int nemoh_b200_get_tables(nemoh_ctx* ctx, double* xr, double* xz, double* apd);
+/* out[8*nfa] = XN,YN,ZN,XG,YG,ZG,AIRE,TDIS; zer = ZER */
+int nemoh_b200_get_geometry(nemoh_ctx* ctx, double* out, double* zer);
+/* timing of the last solve_frequencies call: assembly, factorization, solve+potential+forces (ms) */
+int nemoh_b200_last_timings(nemoh_ctx* ctx, double* assemble_ms, double* factor_ms, double* solve_ms);
+/* number of CUDA kernel launches issued by this context since creation */
+long long nemoh_b200_launch_count(const nemoh_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEMOH_B200_H */

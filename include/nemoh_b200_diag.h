@@ -1,0 +1,25 @@
+/*
+ * nemoh_b200 diagnostics: the host-side scalar setup of one frequency,
+ * exported so that it can be checked against an independent restatement of
+ * the reference routines without a GPU. Not needed to run a solve.
+ */
+#ifndef NEMOH_B200_DIAG_H
+#define NEMOH_B200_DIAG_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* X0: root of x tanh x = ak (Solver/Core/COMPUTE_GREEN_FD.f90:1635-1680) */
+int nemoh_b200_diag_dispersion_root(double ak, double* root);
+/* LISC: finite-depth exponential fit (COMPUTE_GREEN_FD.f90:1007-1077);
+ * ambda[31], ar[31] receive AMBDA(1..31), AR(1..31) */
+int nemoh_b200_diag_exponential_fit(double akh, double amh, int* nexp, double* ambda, double* ar);
+/* CINT_INFD / CINT_FD: returns the node count; qq, cq hold >= 101 entries */
+int nemoh_b200_diag_theta_quadrature(double akk, double* qq, double* cq);
+/* thresholds of the table-stencil indices, 48 each (see DESIGN) */
+int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,246 @@
+"""nemoh_b200: Nemoh's per-frequency BEM solve on an NVIDIA B200 (sm_100a).
+
+Python access to the C-ABI of libnemoh_b200.so (include/nemoh_b200.h). The
+interface mirrors the reference Solver's routines:
+
+    Solver.set_mesh(...)            INITIALIZE + PRE_PROC_MESH
+                                    (Solver/Core/INITIALIZATION.f90:28-69)
+    Solver.solve_potential(T, nvel) SOLVE_POTENTIAL_INFD_DIRECT / _FD_DIRECT
+                                    (SOLVE_BEM_INFD_DIRECT.f90:34, SOLVE_BEM_FD_DIRECT.f90:33)
+                                    -> ZIGB, ZIGS, ZPB, ZPS, NEXP
+    Solver.solve_bvp(T, nvel)       SOLVE_BVP pressure (SOLVE_BEM.f90:28-96)
+    Solver.solve_frequencies(...)   all problems of many frequencies at once, with
+                                    the force integration of Solver/NEMOH.f90:137-141
+
+There is no CPU fallback: without the built library or a CUDA device every
+call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Solver", "NemohError", "FP64", "MIXED", "load_library", "library_path"]
+
+FP64 = 0
+MIXED = 1
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libnemoh_b200.so")
+_lib = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+_ERRNAMES = {1: "EINVAL", 2: "EPANEL_AREA", 3: "EPIVOT", 4: "EOMEGA", 5: "ELISC", 6: "ESPRBM",
+             7: "EDISPERSION", 8: "EAKZ", 9: "EIO", 10: "EHOUSRS", 20: "ECUDA", 21: "ENOMEM",
+             22: "ENODEV", 23: "ECAPACITY"}
+
+
+class NemohError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("nemoh_b200 %s (%d): %s" % (_ERRNAMES.get(code, "?"), code, msg))
+        self.code = code
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def load_library():
+    """Load libnemoh_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise RuntimeError("libnemoh_b200.so is not built (run python -m nemoh_b200.build)")
+    L = ctypes.CDLL(_LIB_PATH)
+    L.nemoh_b200_last_error.restype = ctypes.c_char_p
+    L.nemoh_b200_last_error.argtypes = [_vp]
+    L.nemoh_b200_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int]
+    L.nemoh_b200_destroy.argtypes = [_vp]
+    L.nemoh_b200_set_mesh.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _i,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.nemoh_b200_solve_problem.argtypes = [_vp, ctypes.c_double, _d, _d, _d, _d, _d, _i]
+    L.nemoh_b200_solve_frequencies.argtypes = [_vp, ctypes.c_int, _d, ctypes.c_int, _d, ctypes.c_int, _d, _d]
+    L.nemoh_b200_solve_frequencies_device.argtypes = [_vp, ctypes.c_int, _d, ctypes.c_int, _vp, ctypes.c_int,
+                                                      _vp, _vp, _vp]
+    L.nemoh_b200_assemble.argtypes = [_vp, ctypes.c_double, _d, _d, _d, _d, _i]
+    L.nemoh_b200_get_tables.argtypes = [_vp, _d, _d, _d]
+    L.nemoh_b200_get_geometry.argtypes = [_vp, _d, _d]
+    L.nemoh_b200_last_timings.argtypes = [_vp, _d, _d, _d]
+    L.nemoh_b200_launch_count.argtypes = [_vp]
+    L.nemoh_b200_launch_count.restype = ctypes.c_longlong
+    L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
+    L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
+    L.nemoh_b200_diag_theta_quadrature.argtypes = [ctypes.c_double, _d, _d]
+    L.nemoh_b200_diag_stencil_thresholds.argtypes = [_d, _d, _d]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(_d)
+
+
+def _cplx(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    if n is not None and a.size != n:
+        raise ValueError("expected %d complex values, got %d" % (n, a.size))
+    return a
+
+
+class Solver:
+    """One solver context on one GPU (the reference's COM_VAR state)."""
+
+    def __init__(self, device=0, precision=FP64):
+        L = load_library()
+        h = _vp()
+        st = L.nemoh_b200_create(ctypes.byref(h), int(device), int(precision))
+        if st:
+            raise NemohError(st, "nemoh_b200_create failed (no CUDA device?)")
+        self._h = h
+        self.precision = precision
+        self.nfa = 0
+        self.isym = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().nemoh_b200_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        if st:
+            raise NemohError(st, load_library().nemoh_b200_last_error(self._h).decode())
+
+    @property
+    def launches(self):
+        return int(load_library().nemoh_b200_launch_count(self._h))
+
+    # -- INITIALIZE -----------------------------------------------------------
+    def set_mesh(self, nodes, panels, isym, rho, g, depth):
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        panels = np.ascontiguousarray(panels, dtype=np.int32)
+        self._check(load_library().nemoh_b200_set_mesh(self._h, len(nodes), len(panels), int(isym), _p(nodes),
+                                                       panels.ctypes.data_as(_i), rho, g, depth))
+        self.nfa = len(panels)
+        self.isym = 1 if isym == 1 else 0
+        self.rho = rho
+
+    def set_case(self, case):
+        """Mesh and environment of a nemoh_b200.cases.Case or CaseArrays."""
+        mesh = getattr(case, "mesh", None)
+        if mesh is not None:
+            self.set_mesh(mesh.nodes, mesh.panels, mesh.isym, case.rho, case.g, case.depth)
+        else:
+            self.set_mesh(case.nodes, case.panels, case.isym, case.rho, case.g, case.depth)
+
+    # -- SOLVE_POTENTIAL_*_DIRECT ---------------------------------------------
+    def solve_potential(self, period, nvel):
+        n = self.nfa
+        nvel = _cplx(nvel, n * 2 ** self.isym)
+        out = [np.zeros(n, dtype=np.complex128) for _ in range(4)]
+        nexp = ctypes.c_int()
+        self._check(load_library().nemoh_b200_solve_problem(self._h, float(period), _p(nvel),
+                                                            *[_p(a) for a in out], ctypes.byref(nexp)))
+        zigb, zigs, zpb, zps = out
+        return dict(zigb=zigb, zigs=zigs, zpb=zpb, zps=zps, nexp=nexp.value)
+
+    def solve_bvp(self, period, nvel):
+        """PRESSURE = RHO*i*W*[ZPB; ZPS] (SOLVE_BEM.f90:91-96)."""
+        r = self.solve_potential(period, nvel)
+        w = 2.0 * np.pi / period
+        p = self.rho * 1j * w * r["zpb"]
+        if self.isym:
+            p = np.concatenate([p, self.rho * 1j * w * r["zps"]])
+        return p
+
+    # -- batched frequencies ----------------------------------------------------
+    def solve_frequencies(self, omegas, nvel, nds):
+        """nvel: (2^s N, nrhs, nomega) complex; nds: (nint, 2^s N). Returns force (nint, nrhs, nomega)."""
+        omegas = np.ascontiguousarray(omegas, dtype=np.float64)
+        nvel = np.asfortranarray(nvel, dtype=np.complex128)
+        nds = np.asfortranarray(nds, dtype=np.float64)
+        nc, nrhs, nw = nvel.shape
+        nint = nds.shape[0]
+        if nc != self.nfa * 2 ** self.isym or nw != len(omegas) or nds.shape[1] != nc:
+            raise ValueError("shape mismatch")
+        force = np.zeros((nint, nrhs, nw), dtype=np.complex128, order="F")
+        self._check(load_library().nemoh_b200_solve_frequencies(self._h, nw, _p(omegas), nrhs,
+                                                                nvel.ctypes.data_as(_d), nint,
+                                                                nds.ctypes.data_as(_d), force.ctypes.data_as(_d)))
+        return force
+
+    def solve_frequencies_device(self, omegas, nvel_ptr, nrhs, nint, nds_ptr, force_ptr, stream=0):
+        omegas = np.ascontiguousarray(omegas, dtype=np.float64)
+        self._check(load_library().nemoh_b200_solve_frequencies_device(
+            self._h, len(omegas), _p(omegas), int(nrhs), _vp(nvel_ptr), int(nint), _vp(nds_ptr),
+            _vp(force_ptr), _vp(stream)))
+
+    def last_timings(self):
+        a, f, s = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        load_library().nemoh_b200_last_timings(self._h, ctypes.byref(a), ctypes.byref(f), ctypes.byref(s))
+        return dict(assemble_ms=a.value, factor_ms=f.value, solve_ms=s.value)
+
+    # -- diagnostics -----------------------------------------------------------
+    def assemble(self, omega):
+        n = self.nfa
+        mats = [np.zeros((n, n), dtype=np.complex128, order="F") for _ in range(4)]
+        mode = ctypes.c_int()
+        self._check(load_library().nemoh_b200_assemble(self._h, float(omega), *[m.ctypes.data_as(_d) for m in mats],
+                                                       ctypes.byref(mode)))
+        return mats, mode.value
+
+    def tables(self):
+        xr, xz, apd = np.zeros(328), np.zeros(46), np.zeros(4 * 328 * 46)
+        self._check(load_library().nemoh_b200_get_tables(self._h, _p(xr), _p(xz), _p(apd)))
+        return xr, xz, apd.reshape(4, 46, 328).transpose(0, 2, 1)
+
+    def geometry(self):
+        out = np.zeros(8 * self.nfa)
+        zer = ctypes.c_double()
+        self._check(load_library().nemoh_b200_get_geometry(self._h, _p(out), ctypes.byref(zer)))
+        return out.reshape(8, self.nfa), zer.value
+
+
+# host-side setup checks (no device needed)
+def dispersion_root(ak):
+    r = ctypes.c_double()
+    st = load_library().nemoh_b200_diag_dispersion_root(float(ak), ctypes.byref(r))
+    if st:
+        raise NemohError(st, "dispersion root")
+    return r.value
+
+
+def exponential_fit(akh, amh):
+    n = ctypes.c_int()
+    a, r = np.zeros(31), np.zeros(31)
+    st = load_library().nemoh_b200_diag_exponential_fit(float(akh), float(amh), ctypes.byref(n), _p(a), _p(r))
+    if st:
+        raise NemohError(st, "exponential fit")
+    return n.value, a, r
+
+
+def theta_quadrature(akk):
+    q, c = np.zeros(101), np.zeros(101)
+    n = load_library().nemoh_b200_diag_theta_quadrature(float(akk), _p(q), _p(c))
+    return q[:n], c[:n]
+
+
+def stencil_thresholds():
+    a, b, c = np.zeros(48), np.zeros(48), np.zeros(48)
+    load_library().nemoh_b200_diag_stencil_thresholds(_p(a), _p(b), _p(c))
+    return a, b, c

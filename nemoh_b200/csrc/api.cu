@@ -1,0 +1,687 @@
+// C-ABI of nemoh_b200 (include/nemoh_b200.h): context, device memory, and the
+// per-frequency pipeline  assembly -> LU -> triangular solves -> S*sigma ->
+// pressure/force integration, batched over frequencies and symmetry classes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <functional>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/nemoh_b200.h"
+#include "assembly.cuh"
+#include "fd_setup.h"
+#include "linalg.cuh"
+#include "mixed.cuh"
+
+using namespace nb200;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    else p = nullptr;
+    return e;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct Fail {
+  int code;
+  std::string msg;
+};
+
+}  // namespace
+
+struct nemoh_ctx {
+  int device = 0;
+  int mode = NEMOH_B200_FP64;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+  // tables
+  double h_xr[TAB_IR + 2], h_xz[TAB_JZ + 2];
+  DevBuf d_xr, d_xz, d_apd, d_thr, d_status, d_gm;
+  // mesh
+  int np = 0, nfa = 0, nsymy = 0;
+  double rho = 0, g = 0, depth = 0, zer = 0, gm = 0;
+  DevBuf d_xyz, d_m, d_rec, d_rows;
+  // per-call workspace
+  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_oms, d_slots, d_nvel, d_nds, d_force;
+  MixedWork mixed;
+  int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
+  double w_previous = -1.;   // factor cache key of solve_problem
+  int cached_fd = 0, cached_nexp = 0;
+  float t_asm = 0, t_fac = 0, t_sol = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      throw Fail{e_ == cudaErrorMemoryAllocation ? NEMOH_B200_ENOMEM : NEMOH_B200_ECUDA,         \
+                 std::string(#call) + ": " + cudaGetErrorString(e_)};                            \
+  } while (0)
+
+#define LAUNCHED(ctx)                        \
+  do {                                       \
+    ++(ctx)->launches;                       \
+    CK(cudaGetLastError());                  \
+  } while (0)
+
+static int guarded(nemoh_ctx* ctx, const std::function<void()>& f);
+
+namespace {
+
+const double kPI = 4. * std::atan(1.);
+
+int ncls(const nemoh_ctx* c) { return c->nsymy ? 2 : 1; }
+
+void check_status(nemoh_ctx* c) {
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st) {
+    CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
+    const char* m = st == ST_PIVOT ? "PIVOT INFERIEUR A 1.E-20 (GAUSSZ)"
+                    : st == ST_PANEL_AREA ? "area of a panel is too small (GOMG)"
+                    : st == ST_AKZ_UNDEFINED ? "AKZ > -1.5E-6: wave term undefined in the reference"
+                                              : "device error";
+    throw Fail{st, m};
+  }
+}
+
+// Host-side setup of one frequency (SOLVE_BEM.f90:62-84 and the preambles of
+// SOLVE_POTENTIAL_*_DIRECT). W is the reference's 2*PI/T.
+void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
+  std::memset(&om, 0, sizeof om);
+  om.w = W;
+  om.h = c->depth;
+  const double kwave = W * W / c->g;
+  const bool fd = !((c->depth == 0.) || (kwave * c->depth >= 20));
+  if (std::fabs(W) < 1.E-4) throw Fail{NEMOH_B200_EOMEGA, "ABS(WR) < 1.E-4"};
+  double qq[MAX_NQ + 2], cq[MAX_NQ + 2];
+  if (!fd) {
+    om.fd = 0;
+    om.k0 = W * W / c->g;
+    const int n = theta_quadrature(om.k0 * c->gm, qq, cq);
+    // NQ is not set on this path (SOLVE_BEM_INFD_DIRECT.f90:79): the
+    // free-surface-panel theta sum runs NQ (left by the last finite-depth
+    // solve) times over this path's weights, which are zero past n.
+    om.nq = std::min(c->nq_state, n);
+    for (int i = 1; i <= om.nq; ++i) {
+      om.cq[i] = cq[i];
+      om.ct[i] = std::cos(qq[i]);
+      om.st[i] = std::sin(qq[i]);
+    }
+  } else {
+    om.fd = 1;
+    const double AKH0 = W * W * c->depth / c->g;
+    double AMH;
+    int st = finite_depth_root(AKH0, &AMH);
+    if (st) throw Fail{st, "ERREUR DANS LA RECHERCHE DE LA RACINE (X0)"};
+    const double AKH = AMH * std::tanh(AMH);
+    const double AM0 = AMH / c->depth;
+    om.k0 = AM0;
+    om.amh = AMH;
+    const int n = theta_quadrature(AM0 * c->gm, qq, cq);
+    if (advance_nq) c->nq_state = n;   // NQ=N (SOLVE_BEM_FD_DIRECT.f90:99)
+    om.nq = 0;                         // CQ is zero on this path (COMPUTE_GREEN_FD.f90:874)
+    int nexp = 0;
+    st = exponential_fit(AKH, AMH, &nexp, om.ambda, om.ar);
+    if (st) throw Fail{st, st == ST_LISC ? "LISC: positive exponent" : "exponential fit failed"};
+    om.nexp = nexp;
+    om.ambda[nexp + 1] = 0.;
+    om.ar[nexp + 1] = 2.;
+    const double A = (AMH + AKH) * (AMH + AKH) / (c->depth * (AMH * AMH - AKH * AKH + AKH));
+    const double ADPI2 = -A / (8. * kPI * kPI), ADPI = -A / (8 * kPI);
+    om.coe1 = ADPI2 / AM0;
+    om.coe2 = ADPI / AM0;
+    om.coe3 = ADPI2;
+    om.coe4 = ADPI;
+  }
+}
+
+// capacity: frequencies per device batch
+int batch_capacity(nemoh_ctx* c, int nrhs, int want) {
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t N = c->nfa, cls = ncls(c);
+  size_t per = (2 * cls * N * N + 2 * cls * N * (size_t)std::max(nrhs, 1)) * sizeof(double2) + sizeof(OmegaParams) +
+               cls * LU_NB * LU_NB * sizeof(double2);
+  if (c->mode == NEMOH_B200_MIXED) per += mixed_bytes_per_system(N) * cls;
+  // existing buffers count as available
+  size_t have = c->d_D.bytes + c->d_S.bytes + c->d_X.bytes + c->d_Y.bytes + c->mixed.bytes();
+  size_t budget = (size_t)((fr + have) * 0.8);
+  int cap = (int)std::max<size_t>(1, budget / per);
+  return std::min(cap, want);
+}
+
+void ensure_batch(nemoh_ctx* c, int slots, int nrhs) {
+  const size_t N = c->nfa, cls = ncls(c);
+  const size_t mats = (size_t)slots * cls * N * N * sizeof(double2);
+  CK(c->d_D.ensure(mats));
+  CK(c->d_S.ensure(mats));
+  const size_t rhs = (size_t)slots * cls * N * std::max(nrhs, 1) * sizeof(double2);
+  CK(c->d_X.ensure(rhs));
+  CK(c->d_Y.ensure(rhs));
+  CK(c->d_diag.ensure((size_t)slots * cls * LU_NB * LU_NB * sizeof(double2)));
+  CK(c->d_oms.ensure((size_t)slots * sizeof(OmegaParams)));
+  CK(c->d_slots.ensure((size_t)slots * sizeof(int)));
+  if (c->mode == NEMOH_B200_MIXED) CK(c->mixed.ensure(slots * (int)cls, (int)N, std::max(nrhs, 1)));
+}
+
+GreenCtx green_ctx(nemoh_ctx* c) {
+  GreenCtx g;
+  g.xr = c->d_xr.as<double>();
+  g.xz = c->d_xz.as<double>();
+  g.apd = c->d_apd.as<double4>();
+  g.thr = c->d_thr.as<StencilThresholds>();
+  g.zer = c->zer;
+  g.nsymy = c->nsymy;
+  g.status = c->d_status.as<int>();
+  return g;
+}
+
+// assemble the frequencies held in slots [0, nslots) (params already uploaded)
+void assemble(nemoh_ctx* c, const std::vector<OmegaParams>& oms) {
+  const int N = c->nfa, cls = ncls(c);
+  std::vector<int> infd, fd;
+  for (int s = 0; s < (int)oms.size(); ++s) (oms[s].fd ? fd : infd).push_back(s);
+  std::vector<int> all(infd);
+  all.insert(all.end(), fd.begin(), fd.end());
+  CK(cudaMemcpyAsync(c->d_slots.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  GreenCtx g = green_ctx(c);
+  const long long NN = (long long)N * N;
+  AsmOut o{c->d_D.as<double2>(), c->d_S.as<double2>(), cls * NN};
+  dim3 blk(ASM_ROWS);
+  if (!infd.empty()) {
+    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)infd.size());
+    assemble_kernel<false><<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(), c->d_slots.as<int>(),
+                                                        c->d_rec.as<PanelRec>(), c->d_rows.as<double>(), N, o);
+    LAUNCHED(c);
+  }
+  if (!fd.empty()) {
+    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)fd.size());
+    assemble_kernel<true><<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(),
+                                                       c->d_slots.as<int>() + infd.size(), c->d_rec.as<PanelRec>(),
+                                                       c->d_rows.as<double>(), N, o);
+    LAUNCHED(c);
+  }
+}
+
+Batch dbatch(nemoh_ctx* c) {
+  const long long NN = (long long)c->nfa * c->nfa;
+  return Batch{c->d_D.as<double2>(), NN, c->nfa, c->d_diag.as<double2>()};
+}
+
+void factor_fp64(nemoh_ctx* c, int nsys) {
+  Batch b = dbatch(c);
+  const int N = c->nfa;
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            2 * LU_NB * GM_T * (int)sizeof(double2)));
+    attr = true;
+  }
+  for (int k = 0; k < N; k += LU_NB) {
+    const int nb = std::min(LU_NB, N - k), rest = N - k - nb;
+    const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
+    lu_panel_kernel<double2><<<dim3(1 + nrb + ncb, 1, nsys), LU_RB, 0, c->stream>>>(b, k, c->d_status.as<int>());
+    LAUNCHED(c);
+    if (rest > 0) {
+      const int t = (rest + GM_T - 1) / GM_T;
+      zgemm_update_kernel<double2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(double2), c->stream>>>(b, k, nb);
+    } else {
+      lu_diag_store_kernel<double2><<<dim3(1, 1, nsys), 256, 0, c->stream>>>(b, k, nb);
+    }
+    LAUNCHED(c);
+  }
+}
+
+// solve the factored systems for the right-hand sides in X (result in X)
+void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
+  Batch b = dbatch(c);
+  const int N = c->nfa;
+  const long long xs = (long long)N * nrhs;
+  const int nblk = (N + TS_NB - 1) / TS_NB;
+  for (int blk = 0; blk < nblk; ++blk) {
+    const int below = std::max(0, N - (blk + 1) * TS_NB);
+    trsm_step_kernel<double2, true><<<dim3(std::max(1, (below + 127) / 128), 1, nsys), 128, 0, c->stream>>>(
+        b, c->d_X.as<double2>(), c->d_Y.as<double2>(), xs, nrhs, blk);
+    LAUNCHED(c);
+  }
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int above = blk * TS_NB;
+    trsm_step_kernel<double2, false><<<dim3(std::max(1, (above + 127) / 128), 1, nsys), 128, 0, c->stream>>>(
+        b, c->d_Y.as<double2>(), c->d_X.as<double2>(), xs, nrhs, blk);
+    LAUNCHED(c);
+  }
+}
+
+void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs) {
+  if (c->mode == NEMOH_B200_MIXED) {
+    mixed_factor(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_status.as<int>(), c->stream, c->launches);
+    CK(cudaGetLastError());
+    if (have_rhs) {
+      mixed_solve_refine(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(),
+                         nrhs, c->stream, c->launches);
+      CK(cudaGetLastError());
+    }
+  } else {
+    factor_fp64(c, nsys);
+    if (have_rhs) trsm_fp64(c, nsys, nrhs);
+  }
+}
+
+void potential(nemoh_ctx* c, int nsys, int nrhs) {
+  const int N = c->nfa;
+  const long long NN = (long long)N * N, xs = (long long)N * nrhs;
+  Batch s{c->d_S.as<double2>(), NN, N, nullptr};
+  matmul_rhs_kernel<<<dim3((N + 127) / 128, 1, nsys), 128, 0, c->stream>>>(s, c->d_X.as<double2>(), xs,
+                                                                          c->d_Y.as<double2>(), xs, nrhs);
+  LAUNCHED(c);
+}
+
+void upload_params(nemoh_ctx* c, const std::vector<OmegaParams>& oms) {
+  CK(cudaMemcpyAsync(c->d_oms.p, oms.data(), oms.size() * sizeof(OmegaParams), cudaMemcpyHostToDevice, c->stream));
+}
+
+// shared by the host and device-pointer batched entry points
+void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int nrhs, const double2* nvel_d, int nint,
+                            const double* nds_d, double2* force_d) {
+  if (!c->nfa) throw Fail{NEMOH_B200_EINVAL, "no mesh"};
+  if (nrhs < 1 || nrhs > MAX_RHS) throw Fail{NEMOH_B200_ECAPACITY, "nrhs must be in 1..16"};
+  const int N = c->nfa, cls = ncls(c);
+  const int cap = batch_capacity(c, nrhs, nomega);
+  ensure_batch(c, cap, nrhs);
+  c->t_asm = c->t_fac = c->t_sol = 0;
+  for (int w0 = 0; w0 < nomega; w0 += cap) {
+    const int nw = std::min(cap, nomega - w0);
+    std::vector<OmegaParams> oms(nw);
+    for (int i = 0; i < nw; ++i) {
+      const double T = 2. * kPI / omegas[w0 + i];
+      omega_params(c, 2. * kPI / T, oms[i], true);
+    }
+    upload_params(c, oms);
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    assemble(c, oms);
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    fold_rhs_kernel<<<dim3((N + 127) / 128, nrhs, nw), 128, 0, c->stream>>>(
+        nvel_d + (long long)w0 * nrhs * cls * N, N, c->nsymy, nrhs, c->d_X.as<double2>());
+    LAUNCHED(c);
+    factor_and_solve(c, nw * cls, nrhs, true);
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    potential(c, nw * cls, nrhs);
+    force_kernel<<<dim3(nint, nrhs, nw), 256, 0, c->stream>>>(c->d_Y.as<double2>(), c->d_oms.as<OmegaParams>(), N,
+                                                              c->nsymy, nrhs, nint, nds_d, c->rho,
+                                                              force_d + (long long)w0 * nrhs * nint);
+    LAUNCHED(c);
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    check_status(c);
+    float a, f, s;
+    CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+    CK(cudaEventElapsedTime(&f, c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&s, c->ev[2], c->ev[3]));
+    c->t_asm += a;
+    c->t_fac += f;
+    c->t_sol += s;
+  }
+  c->w_previous = -1.;  // the batch reused the cached-factor slot
+}
+
+}  // namespace
+
+static int guarded(nemoh_ctx* ctx, const std::function<void()>& f) {
+  try {
+    if (ctx) CK(cudaSetDevice(ctx->device));
+    f();
+    return NEMOH_B200_OK;
+  } catch (const Fail& e) {
+    if (ctx) ctx->err = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    if (ctx) ctx->err = e.what();
+    return NEMOH_B200_EINVAL;
+  }
+}
+
+extern "C" {
+
+int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
+  if (!out) return NEMOH_B200_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NEMOH_B200_ENODEV;
+  if (device < 0 || device >= ndev) return NEMOH_B200_EINVAL;
+  if (precision_mode != NEMOH_B200_FP64 && precision_mode != NEMOH_B200_MIXED) return NEMOH_B200_EINVAL;
+  nemoh_ctx* c = new nemoh_ctx();
+  c->device = device;
+  c->mode = precision_mode;
+  int st = guarded(c, [&] {
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& e : c->ev) CK(cudaEventCreate(&e));
+    CK(c->d_status.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
+    CK(c->d_gm.ensure(sizeof(unsigned long long)));
+    // Green tables (CREK): nodes on the host, 251-point theta integrals on the device
+    table_nodes(c->h_xr, c->h_xz);
+    double cqt[NPINTE + 2], qqt[NPINTE + 2], ctt[NPINTE + 2];
+    simpson_251(cqt, qqt);
+    for (int i = 1; i <= NPINTE; ++i) ctt[i] = std::cos(qqt[i]);
+    DevBuf dq, dc;
+    CK(dq.ensure(sizeof cqt));
+    CK(dc.ensure(sizeof ctt));
+    CK(c->d_xr.ensure(sizeof c->h_xr));
+    CK(c->d_xz.ensure(sizeof c->h_xz));
+    CK(c->d_apd.ensure(sizeof(double4) * TAB_IR * TAB_JZ));
+    CK(cudaMemcpyAsync(c->d_xr.p, c->h_xr, sizeof c->h_xr, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_xz.p, c->h_xz, sizeof c->h_xz, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dq.p, cqt, sizeof cqt, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dc.p, ctt, sizeof ctt, cudaMemcpyHostToDevice, c->stream));
+    crek_kernel<<<(TAB_IR * TAB_JZ + 127) / 128, 128, 0, c->stream>>>(c->d_xr.as<double>(), c->d_xz.as<double>(),
+                                                                     dq.as<double>(), dc.as<double>(),
+                                                                     c->d_apd.as<double4>());
+    LAUNCHED(c);
+    StencilThresholds thr;
+    stencil_thresholds(&thr);
+    CK(c->d_thr.ensure(sizeof thr));
+    CK(cudaMemcpyAsync(c->d_thr.p, &thr, sizeof thr, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+  if (st) {
+    nemoh_b200_destroy(c);
+    return st;
+  }
+  *out = c;
+  return NEMOH_B200_OK;
+}
+
+int nemoh_b200_destroy(nemoh_ctx* c) {
+  if (!c) return NEMOH_B200_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NEMOH_B200_OK;
+}
+
+const char* nemoh_b200_last_error(const nemoh_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+long long nemoh_b200_launch_count(const nemoh_ctx* c) { return c ? c->launches : 0; }
+
+int nemoh_b200_set_mesh(nemoh_ctx* c, int np, int nfa, int nsymy, const double* xyz, const int* m1234, double rho,
+                        double g, double depth) {
+  if (!c || np < 2 || nfa < 1 || !xyz || !m1234 || !(g > 0)) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    for (int i = 0; i < 4 * nfa; ++i)
+      if (m1234[i] < 1 || m1234[i] > np) throw Fail{NEMOH_B200_EINVAL, "panel node index out of range"};
+    c->np = np;
+    c->nfa = nfa;
+    c->nsymy = (nsymy == 1) ? 1 : 0;
+    c->rho = rho;
+    c->g = g;
+    c->depth = depth;
+    c->w_previous = -1.;
+    c->nq_state = 0;
+    // ZER (PREPARE_MESH.f90:58-69): the largest pairwise |dx| is max-min
+    double xmin = xyz[0], xmax = xyz[0], ymin = xyz[1], ymax = xyz[1], yabs = 0;
+    for (int i = 0; i < np; ++i) {
+      xmin = std::min(xmin, xyz[3 * i]);
+      xmax = std::max(xmax, xyz[3 * i]);
+      ymin = std::min(ymin, xyz[3 * i + 1]);
+      ymax = std::max(ymax, xyz[3 * i + 1]);
+      yabs = std::max(yabs, std::fabs(xyz[3 * i + 1]));
+    }
+    const double GL0 = xmax - xmin;
+    const double BL = c->nsymy ? 2. * yabs : ymax - ymin;
+    c->zer = -1.E-5 * std::max(GL0, BL);
+    CK(c->d_xyz.ensure(sizeof(double) * 3 * np));
+    CK(c->d_m.ensure(sizeof(int) * 4 * nfa));
+    CK(c->d_rec.ensure(sizeof(PanelRec) * nfa));
+    CK(c->d_rows.ensure(sizeof(double) * 6 * nfa));
+    CK(cudaMemcpyAsync(c->d_xyz.p, xyz, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_m.p, m1234, sizeof(int) * 4 * nfa, cudaMemcpyHostToDevice, c->stream));
+    gomg_kernel<<<(nfa + 127) / 128, 128, 0, c->stream>>>(nfa, c->d_xyz.as<double>(), c->d_m.as<int>(),
+                                                         c->d_rec.as<PanelRec>(), c->d_rows.as<double>(),
+                                                         c->d_status.as<int>());
+    LAUNCHED(c);
+    CK(cudaMemsetAsync(c->d_gm.p, 0, sizeof(unsigned long long), c->stream));
+    gm_kernel<<<592, 256, 0, c->stream>>>(np, c->nsymy, c->d_xyz.as<double>(), c->d_gm.as<unsigned long long>());
+    LAUNCHED(c);
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, c->d_gm.p, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+    check_status(c);
+    std::memcpy(&c->gm, &bits, sizeof bits);
+  });
+}
+
+int nemoh_b200_get_geometry(nemoh_ctx* c, double* out, double* zer) {
+  if (!c || !out || !c->nfa) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    std::vector<PanelRec> r(c->nfa);
+    CK(cudaMemcpyAsync(r.data(), c->d_rec.p, sizeof(PanelRec) * c->nfa, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int n = c->nfa;
+    for (int i = 0; i < n; ++i) {
+      out[i] = r[i].xn; out[n + i] = r[i].yn; out[2 * n + i] = r[i].zn;
+      out[3 * n + i] = r[i].xg; out[4 * n + i] = r[i].yg; out[5 * n + i] = r[i].zg;
+      out[6 * n + i] = r[i].aire; out[7 * n + i] = r[i].tdis;
+    }
+    if (zer) *zer = c->zer;
+  });
+}
+
+int nemoh_b200_get_tables(nemoh_ctx* c, double* xr, double* xz, double* apd) {
+  if (!c) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    std::vector<double4> t(TAB_IR * TAB_JZ);
+    CK(cudaMemcpyAsync(t.data(), c->d_apd.p, sizeof(double4) * t.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (xr) for (int i = 1; i <= TAB_IR; ++i) xr[i - 1] = c->h_xr[i];
+    if (xz) for (int j = 1; j <= TAB_JZ; ++j) xz[j - 1] = c->h_xz[j];
+    if (apd)
+      for (size_t q = 0; q < t.size(); ++q) {
+        apd[q] = t[q].x;
+        apd[TAB_IR * TAB_JZ + q] = t[q].y;
+        apd[2 * TAB_IR * TAB_JZ + q] = t[q].z;
+        apd[3 * TAB_IR * TAB_JZ + q] = t[q].w;
+      }
+  });
+}
+
+int nemoh_b200_assemble(nemoh_ctx* c, double omega, double* dp, double* dm, double* sp, double* sm,
+                        int* depth_mode) {
+  if (!c || !c->nfa || !(omega > 0)) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    ensure_batch(c, 1, 1);
+    std::vector<OmegaParams> oms(1);
+    const double T = 2. * kPI / omega;
+    omega_params(c, 2. * kPI / T, oms[0], true);
+    upload_params(c, oms);
+    assemble(c, oms);
+    check_status(c);
+    const size_t NN = (size_t)c->nfa * c->nfa, b = NN * sizeof(double2);
+    const bool two = c->nsymy == 1;
+    if (dp) CK(cudaMemcpyAsync(dp, c->d_D.p, b, cudaMemcpyDeviceToHost, c->stream));
+    if (dm) CK(cudaMemcpyAsync(dm, c->d_D.as<double2>() + (two ? NN : 0), b, cudaMemcpyDeviceToHost, c->stream));
+    if (sp) CK(cudaMemcpyAsync(sp, c->d_S.p, b, cudaMemcpyDeviceToHost, c->stream));
+    if (sm) CK(cudaMemcpyAsync(sm, c->d_S.as<double2>() + (two ? NN : 0), b, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (depth_mode) *depth_mode = oms[0].fd;
+    c->w_previous = -1.;
+  });
+}
+
+int nemoh_b200_solve_problem(nemoh_ctx* c, double period, const double* nvel, double* zigb, double* zigs,
+                             double* zpb, double* zps, int* nexp) {
+  if (!c || !c->nfa || !nvel || !(period > 0)) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    const int N = c->nfa, cls = ncls(c);
+    const double W = 2. * kPI / period;
+    ensure_batch(c, 1, 1);
+    if (W != c->w_previous) {
+      std::vector<OmegaParams> oms(1);
+      omega_params(c, W, oms[0], true);
+      upload_params(c, oms);
+      assemble(c, oms);
+      factor_and_solve(c, cls, 1, false);
+      check_status(c);
+      c->w_previous = W;
+      c->cached_fd = oms[0].fd;
+      c->cached_nexp = oms[0].nexp;
+    } else if (c->cached_fd) {
+      OmegaParams tmp;
+      omega_params(c, W, tmp, true);  // NQ/LISC side state of a repeated call
+    }
+    // right-hand sides B = (NVEL(I) +- NVEL(I+NFA))/2 (SOLVE_BEM_INFD_DIRECT.f90:123-131)
+    const std::complex<double>* v = reinterpret_cast<const std::complex<double>*>(nvel);
+    std::vector<std::complex<double>> B((size_t)cls * N);
+    for (int s = 0; s < cls; ++s) {
+      const double BX = s == 0 ? 1. : -1.;
+      for (int i = 0; i < N; ++i) B[(size_t)s * N + i] = c->nsymy ? (v[i] + BX * v[i + N]) * 0.5 : v[i];
+    }
+    CK(cudaMemcpyAsync(c->d_X.p, B.data(), B.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (c->mode == NEMOH_B200_MIXED) {
+      mixed_solve_refine(c->mixed, c->d_D.as<double2>(), N, cls, c->d_X.as<double2>(), c->d_Y.as<double2>(), 1,
+                         c->stream, c->launches);
+      CK(cudaGetLastError());
+    } else {
+      trsm_fp64(c, cls, 1);
+    }
+    std::vector<std::complex<double>> zol((size_t)cls * N), phi((size_t)cls * N);
+    CK(cudaMemcpyAsync(zol.data(), c->d_X.p, zol.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    potential(c, cls, 1);
+    CK(cudaMemcpyAsync(phi.data(), c->d_Y.p, phi.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    check_status(c);
+    auto put = [](double* o, int i, std::complex<double> z) {
+      if (o) { o[2 * i] = z.real(); o[2 * i + 1] = z.imag(); }
+    };
+    for (int i = 0; i < N; ++i) {
+      if (c->nsymy) {
+        put(zigb, i, zol[i] + zol[N + i]);
+        put(zigs, i, zol[i] - zol[N + i]);
+        put(zpb, i, phi[i] + phi[N + i]);
+        put(zps, i, phi[i] - phi[N + i]);
+      } else {
+        put(zigb, i, zol[i]);
+        put(zigs, i, 0.);
+        put(zpb, i, phi[i]);
+        put(zps, i, 0.);
+      }
+    }
+    if (nexp) *nexp = c->cached_fd ? c->cached_nexp : 0;
+  });
+}
+
+int nemoh_b200_solve_frequencies(nemoh_ctx* c, int nomega, const double* omegas, int nrhs, const double* nvel,
+                                 int nint, const double* nds, double* force) {
+  if (!c || nomega < 1 || !omegas || !nvel || nint < 0 || (nint > 0 && (!nds || !force))) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    const int N = c->nfa, cls = ncls(c);
+    const size_t nv = (size_t)cls * N * nrhs * nomega;
+    CK(c->d_nvel.ensure(nv * sizeof(double2)));
+    CK(c->d_nds.ensure(std::max<size_t>(1, (size_t)nint * cls * N) * sizeof(double)));
+    CK(c->d_force.ensure(std::max<size_t>(1, (size_t)nint * nrhs * nomega) * sizeof(double2)));
+    CK(cudaMemcpyAsync(c->d_nvel.p, nvel, nv * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (nint)
+      CK(cudaMemcpyAsync(c->d_nds.p, nds, (size_t)nint * cls * N * sizeof(double), cudaMemcpyHostToDevice,
+                         c->stream));
+    solve_frequencies_impl(c, nomega, omegas, nrhs, c->d_nvel.as<double2>(), nint, c->d_nds.as<double>(),
+                           c->d_force.as<double2>());
+    if (nint)
+      CK(cudaMemcpyAsync(force, c->d_force.p, (size_t)nint * nrhs * nomega * sizeof(double2),
+                         cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int nemoh_b200_solve_frequencies_device(nemoh_ctx* c, int nomega, const double* omegas, int nrhs,
+                                        const double* nvel_device, int nint, const double* nds_device,
+                                        double* force_device, void* stream) {
+  if (!c || nomega < 1 || !omegas || !nvel_device) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CK(cudaEventRecord(e, user));
+    CK(cudaStreamWaitEvent(c->stream, e, 0));
+    solve_frequencies_impl(c, nomega, omegas, nrhs, reinterpret_cast<const double2*>(nvel_device), nint, nds_device,
+                           reinterpret_cast<double2*>(force_device));
+    CK(cudaEventRecord(e, c->stream));
+    CK(cudaStreamWaitEvent(user, e, 0));
+    CK(cudaEventDestroy(e));
+  });
+}
+
+int nemoh_b200_last_timings(nemoh_ctx* c, double* a, double* f, double* s) {
+  if (!c) return NEMOH_B200_EINVAL;
+  if (a) *a = c->t_asm;
+  if (f) *f = c->t_fac;
+  if (s) *s = c->t_sol;
+  return NEMOH_B200_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// diagnostics (include/nemoh_b200_diag.h): host setup only, no device needed
+// ---------------------------------------------------------------------------
+#include "../../include/nemoh_b200_diag.h"
+
+extern "C" {
+
+int nemoh_b200_diag_dispersion_root(double ak, double* root) { return finite_depth_root(ak, root); }
+
+int nemoh_b200_diag_exponential_fit(double akh, double amh, int* nexp, double* ambda, double* ar) {
+  double a[MAX_NEXP + 1] = {0}, r[MAX_NEXP + 1] = {0};
+  int st = exponential_fit(akh, amh, nexp, a, r);
+  for (int i = 1; i <= MAX_NEXP; ++i) {
+    ambda[i - 1] = a[i];
+    ar[i - 1] = r[i];
+  }
+  return st;
+}
+
+int nemoh_b200_diag_theta_quadrature(double akk, double* qq, double* cq) {
+  double q[MAX_NQ + 2], c[MAX_NQ + 2];
+  const int n = theta_quadrature(akk, q, c);
+  for (int i = 1; i <= n; ++i) {
+    qq[i - 1] = q[i];
+    cq[i - 1] = c[i];
+  }
+  return n;
+}
+
+int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5) {
+  StencilThresholds t;
+  stencil_thresholds(&t);
+  for (int k = 0; k < 48; ++k) {
+    kj8[k] = t.kj8[k];
+    kj5[k] = t.kj5[k];
+    ki5[k] = t.ki5[k];
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+// Geometry, Green-table and influence-matrix assembly kernels (sm_100a, FP64).
+#pragma once
+#include "green.cuh"
+
+namespace nb200 {
+
+// ---------------------------------------------------------------------------
+// GOMG (Solver/Core/PREPARE_MESH.f90:80-180): one thread per panel.
+// Every operation is exactly rounded so that the panel geometry matches an
+// FP64 CPU run of the reference bit for bit (it feeds every branch later).
+// Writes the source-panel records and the collocation SoA rows
+// (XG, YG, ZG, XN, YN, ZN) and flags degenerate panels.
+// ---------------------------------------------------------------------------
+__global__ void gomg_kernel(int nfa, const double* __restrict__ xyz, const int* __restrict__ m1234,
+                            PanelRec* __restrict__ rec, double* __restrict__ rows, int* status) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nfa) return;
+  const int K = m1234[4 * I] - 1, L = m1234[4 * I + 1] - 1, M = m1234[4 * I + 2] - 1, N = m1234[4 * I + 3] - 1;
+  const double xk = xyz[3 * K], yk = xyz[3 * K + 1], zk = xyz[3 * K + 2];
+  const double xl = xyz[3 * L], yl = xyz[3 * L + 1], zl = xyz[3 * L + 2];
+  const double xm = xyz[3 * M], ym = xyz[3 * M + 1], zm = xyz[3 * M + 2];
+  const double xn = xyz[3 * N], yn = xyz[3 * N + 1], zn = xyz[3 * N + 2];
+  const double T1X = XSUB(xm, xk), T1Y = XSUB(ym, yk), T1Z = XSUB(zm, zk);
+  const double T2X = XSUB(xn, xl), T2Y = XSUB(yn, yl), T2Z = XSUB(zn, zl);
+  const double XNX = XSUB(XMUL(T1Y, T2Z), XMUL(T2Y, T1Z));
+  const double XNY = XSUB(XMUL(T1Z, T2X), XMUL(T2Z, T1X));
+  const double XNZ = XSUB(XMUL(T1X, T2Y), XMUL(T2X, T1Y));
+  const double XNQ = XSQRT(XADD(XADD(XMUL(XNX, XNX), XMUL(XNY, XNY)), XMUL(XNZ, XNZ)));
+  if (XNQ <= 1.E-25) {
+    set_status(status, ST_PANEL_AREA);
+    return;
+  }
+  const double NX = XDIV(XNX, XNQ), NY = XDIV(XNY, XNQ), NZ = XDIV(XNZ, XNQ);
+  const double XAV = XMUL(XADD(XADD(XADD(xk, xm), xl), xn), 0.25);
+  const double YAV = XMUL(XADD(XADD(XADD(yk, ym), yn), yl), 0.25);
+  const double ZAV = XMUL(XADD(XADD(XADD(zk, zm), zn), zl), 0.25);
+  const double T1 = XSQRT(XADD(XADD(XMUL(T1X, T1X), XMUL(T1Y, T1Y)), XMUL(T1Z, T1Z)));
+  const double U1X = XDIV(T1X, T1), U1Y = XDIV(T1Y, T1), U1Z = XDIV(T1Z, T1);
+  const double U2X = XSUB(XMUL(NY, U1Z), XMUL(NZ, U1Y));
+  const double U2Y = XSUB(XMUL(NZ, U1X), XMUL(NX, U1Z));
+  const double U2Z = XSUB(XMUL(NX, U1Y), XMUL(NY, U1X));
+  auto proj = [&](double ux, double uy, double uz, double px, double py, double pz) {
+    return XADD(XADD(XMUL(ux, XSUB(px, XAV)), XMUL(uy, XSUB(py, YAV))), XMUL(uz, XSUB(pz, ZAV)));
+  };
+  const double XI1 = proj(U1X, U1Y, U1Z, xk, yk, zk), XI2 = proj(U1X, U1Y, U1Z, xl, yl, zl);
+  const double XI3 = proj(U1X, U1Y, U1Z, xm, ym, zm), XI4 = proj(U1X, U1Y, U1Z, xn, yn, zn);
+  const double ETA1 = proj(U2X, U2Y, U2Z, xk, yk, zk), ETA2 = proj(U2X, U2Y, U2Z, xl, yl, zl);
+  const double ETA3 = proj(U2X, U2Y, U2Z, xm, ym, zm), ETA4 = proj(U2X, U2Y, U2Z, xn, yn, zn);
+  const double XIO = XDIV(XADD(XMUL(XI4, XSUB(ETA1, ETA2)), XMUL(XI2, XSUB(ETA4, ETA1))),
+                          XMUL(3., XSUB(ETA2, ETA4)));
+  const double ETAO = XDIV(-ETA1, 3.);
+  const double EN1 = XSUB(ETA1, ETAO), EN2 = XSUB(ETA2, ETAO), EN3 = XSUB(ETA3, ETAO), EN4 = XSUB(ETA4, ETAO);
+  const double XN1 = XSUB(XI1, XIO), XN2 = XSUB(XI2, XIO), XN3 = XSUB(XI3, XIO), XN4 = XSUB(XI4, XIO);
+  PanelRec p;
+  p.xg = XADD(XADD(XAV, XMUL(U1X, XIO)), XMUL(U2X, ETAO));
+  p.yg = XADD(XADD(YAV, XMUL(U1Y, XIO)), XMUL(U2Y, ETAO));
+  p.zg = XADD(XADD(ZAV, XMUL(U1Z, XIO)), XMUL(U2Z, ETAO));
+  p.xn = NX;
+  p.yn = NY;
+  p.zn = NZ;
+  p.aire = XMUL(XMUL(XSUB(XN3, XN1), XSUB(EN4, EN2)), 0.5);
+  const double TT1 = XSQRT(XADD(XMUL(XN1, XN1), XMUL(EN1, EN1)));
+  const double TT2 = XSQRT(XADD(XMUL(XN2, XN2), XMUL(EN2, EN2)));
+  const double TT3 = XSQRT(XADD(XMUL(XN3, XN3), XMUL(EN3, EN3)));
+  const double TT4 = XSQRT(XADD(XMUL(XN4, XN4), XMUL(EN4, EN4)));
+  p.tdis = fmax(fmax(TT1, TT2), fmax(TT3, TT4));
+  p.vx[0] = xk; p.vy[0] = yk; p.vz[0] = zk;
+  p.vx[1] = xl; p.vy[1] = yl; p.vz[1] = zl;
+  p.vx[2] = xm; p.vy[2] = ym; p.vz[2] = zm;
+  p.vx[3] = xn; p.vy[3] = yn; p.vz[3] = zn;
+  rec[I] = p;
+  rows[0 * nfa + I] = p.xg;
+  rows[1 * nfa + I] = p.yg;
+  rows[2 * nfa + I] = p.zg;
+  rows[3 * nfa + I] = p.xn;
+  rows[4 * nfa + I] = p.yn;
+  rows[5 * nfa + I] = p.zn;
+}
+
+// GM: largest horizontal node-pair distance including the y-mirror
+// (SOLVE_BEM_INFD_DIRECT.f90:66-76). Non-negative doubles order like their
+// bit patterns, so an unsigned atomicMax reduces them exactly.
+__global__ void gm_kernel(int np, int nsymy, const double* __restrict__ xyz, unsigned long long* gm_bits) {
+  double best = 0.;
+  const long long total = (long long)np * np;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / np), j = (int)(q % np);
+    if (j <= i) continue;
+    const double dx = XSUB(xyz[3 * j], xyz[3 * i]);
+    for (int jj = 0; jj <= nsymy; ++jj) {
+      const double bj = jj ? -1. : 1.;
+      const double dy = XSUB(xyz[3 * i + 1], xyz[3 * j + 1] * bj);
+      best = fmax(best, XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy))));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(gm_bits, (unsigned long long)__double_as_longlong(best));
+}
+
+// ---------------------------------------------------------------------------
+// CREK / VNS (Solver/NEMOH.f90:179-251): one thread per table node,
+// 251-point Simpson rule in theta. cos(theta) comes from the host.
+// ---------------------------------------------------------------------------
+__global__ void crek_kernel(const double* __restrict__ xr, const double* __restrict__ xz,
+                            const double* __restrict__ cqt, const double* __restrict__ ctt, double4* __restrict__ apd) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= TAB_IR * TAB_JZ) return;
+  const int I = q % TAB_IR + 1, J = q / TAB_IR + 1;
+  const double AKZ = xz[J], AKR = xr[I];
+  double f1x = 0., f1z = 0., f2x = 0., f2z = 0.;
+  for (int it = 1; it <= NPINTE; ++it) {
+    const double CT = ctt[it], CQ = cqt[it];
+    const cplx Z = mk(AKZ, XMUL(AKR, CT));
+    const cplx CEX = (AKZ + 30. <= 0.) ? mk(0., 0.) : cexp_(Z);
+    const cplx G = GG(Z, CEX);
+    const cplx C1 = CQ * (G - 1. / Z);
+    const cplx C2 = CQ * CEX;
+    f1x += CT * C1.im;
+    f1z += C1.re;
+    f2x += CT * C2.im;
+    f2z += C2.re;
+  }
+  apd[(I - 1) + TAB_IR * (J - 1)] = make_double4(f1x, f1z, f2x, f2z);
+}
+
+// ---------------------------------------------------------------------------
+// Influence-matrix assembly. Thread = collocation row I, block = 128 rows;
+// the block stages ASM_TJ source panels J in shared memory and walks them.
+// Output per frequency (column-major, leading dimension N): D+ then D- in
+// out.d, S+ then S- in out.s (nsymy=0: one D and one S).
+// Column-major writes by consecutive rows are coalesced 16-byte stores.
+// ---------------------------------------------------------------------------
+constexpr int ASM_ROWS = 128;
+constexpr int ASM_TJ = 32;
+
+struct AsmOut {
+  double2* d;           // D+ (and D-) of frequency slot s at d + s * slot_stride
+  double2* s;           // S+ (and S-) likewise
+  long long slot_stride;
+};
+
+template <bool FD>
+__global__ void __launch_bounds__(ASM_ROWS) assemble_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
+                                                            const int* __restrict__ slots, const PanelRec* __restrict__ rec,
+                                                            const double* __restrict__ rows, int N, AsmOut out) {
+  __shared__ PanelRec sp[ASM_TJ];
+  __shared__ OmegaParams som;
+  const int slot = slots[blockIdx.z];
+  {
+    const double* src = reinterpret_cast<const double*>(oms + slot);
+    double* dst = reinterpret_cast<double*>(&som);
+    for (int i = threadIdx.x; i < (int)(sizeof(OmegaParams) / 8); i += blockDim.x) dst[i] = src[i];
+  }
+  const int j0 = blockIdx.y * ASM_TJ;
+  const int nj = min(ASM_TJ, N - j0);
+  {
+    const double* src = reinterpret_cast<const double*>(rec + j0);
+    double* dst = reinterpret_cast<double*>(sp);
+    const int nw = nj * (int)(sizeof(PanelRec) / 8);
+    for (int i = threadIdx.x; i < nw; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int I = blockIdx.x * ASM_ROWS + threadIdx.x;
+  if (I >= N) return;
+  const double XGI = rows[I], YGI = rows[N + I], ZGI = rows[2 * N + I];
+  const double XNI = rows[3 * N + I], YNI = rows[4 * N + I], ZNI = rows[5 * N + I];
+  const long long NN = (long long)N * N;
+  double2* od = out.d + slot * out.slot_stride;
+  double2* os = out.s + slot * out.slot_stride;
+  for (int jj = 0; jj < nj; ++jj) {
+    const int J = j0 + jj;
+    PairOut r;
+    pair_green<FD>(g, som, XGI, YGI, ZGI, XNI, YNI, ZNI, I == J, sp[jj], r);
+    const long long q = I + (long long)N * J;
+    od[q] = make_double2(r.dp_re, r.dp_im);
+    os[q] = make_double2(r.sp_re, r.sp_im);
+    if (g.nsymy == 1) {
+      od[NN + q] = make_double2(r.dm_re, r.dm_im);
+      os[NN + q] = make_double2(r.sm_re, r.sm_im);
+    }
+  }
+}
+
+}  // namespace nb200

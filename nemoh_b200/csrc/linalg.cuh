@@ -1,0 +1,392 @@
+// Dense complex FP64 linear algebra for the BEM systems (sm_100a).
+//
+// The reference inverts each influence matrix with GAUSSZ (Gauss elimination
+// on [A|I] without effective row pivoting, Solver/Core/M_SOLVER.f90:31-104).
+// Here each matrix is factored once as A = L U (L unit lower, U upper) with a
+// blocked right-looking algorithm and the same no-pivot semantics, including
+// the "pivot below 1e-20" stop (M_SOLVER.f90:49-52, 61-64) as a status code.
+// Without pivoting the panel reduces to the small diagonal block plus two
+// triangular solves, so every step is two launches over the whole batch of
+// systems (blockIdx.z = system):
+//   lu_panel_kernel   factor A11 (redundantly per CTA, in shared memory),
+//                     L21 <- A21 U11^-1 and U12 <- L11^-1 A12
+//   zgemm_update      A22 <- A22 - L21 U12
+#pragma once
+#include "common.cuh"
+
+namespace nb200 {
+
+constexpr int LU_NB = 32;     // panel width
+constexpr int LU_RB = 128;    // rows per L21 CTA
+constexpr int LU_CB = 64;     // columns per U12 CTA
+
+template <class C2>
+struct BatchT {
+  C2* base;               // system s at base + s * stride
+  long long stride;       // elements between systems
+  int n;                  // order (leading dimension = n)
+  C2* diag;               // LU_NB*LU_NB scratch per system for the factored diagonal block
+};
+using Batch = BatchT<double2>;
+
+template <class C2> __device__ __forceinline__ C2 mkc(double x, double y);
+template <> __device__ __forceinline__ double2 mkc<double2>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 mkc<float2>(double x, double y) { return make_float2((float)x, (float)y); }
+
+template <class C2>
+__device__ __forceinline__ C2 cfms(C2 c, C2 a, C2 b) {  // c - a*b
+  C2 r;
+  r.x = c.x - (a.x * b.x - a.y * b.y);
+  r.y = c.y - (a.x * b.y + a.y * b.x);
+  return r;
+}
+__device__ __forceinline__ double2 cdv(double2 a, double2 b) {
+  cplx r = mk(a.x, a.y) / mk(b.x, b.y);
+  return make_double2(r.re, r.im);
+}
+__device__ __forceinline__ float2 cdv(float2 a, float2 b) {
+  if (fabsf(b.x) >= fabsf(b.y)) {
+    float r = b.y / b.x, d = b.x + b.y * r;
+    return make_float2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  float r = b.x / b.y, d = b.y + b.x * r;
+  return make_float2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+__device__ __forceinline__ double cabs2(double2 a) { return hypot(a.x, a.y); }
+__device__ __forceinline__ double cabs2(float2 a) { return hypotf(a.x, a.y); }
+
+// Factor the nb x nb block held column-major in shared memory (ld = nb).
+template <class C2>
+__device__ void factor_block(C2* s, int nb, int* status, bool report) {
+  for (int j = 0; j < nb; ++j) {
+    const C2 piv = s[j + nb * j];
+    if (report && threadIdx.x == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+    __syncthreads();
+    // multipliers of column j
+    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) s[i + nb * j] = cdv(s[i + nb * j], piv);
+    __syncthreads();
+    const int m = nb - j - 1;
+    for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+      const int i = j + 1 + q % m, c = j + 1 + q / m;
+      s[i + nb * c] = cfms(s[i + nb * c], s[i + nb * j], s[j + nb * c]);
+    }
+    __syncthreads();
+  }
+}
+
+template <class C2>
+__global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k, int* status) {
+  __shared__ C2 diag[LU_NB * LU_NB];
+  __shared__ C2 work[LU_NB * LU_CB];
+  const int n = b.n;
+  const int nb = min(LU_NB, n - k);
+  C2* A = b.base + blockIdx.z * b.stride;
+  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
+    const int i = q % nb, c = q / nb;
+    diag[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
+  }
+  __syncthreads();
+  const int rest = n - k - nb;
+  const int nrb = (rest + LU_RB - 1) / LU_RB;
+  factor_block(diag, nb, status, blockIdx.x == 0);
+  if (blockIdx.x == 0) {
+    // the other CTAs of this launch still read A11 from A: park the factored
+    // block in scratch; the next launch of this step stores it (diag_store)
+    C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
+    for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
+    return;
+  }
+  if (blockIdx.x <= nrb) {
+    // L21 rows: x U11 = a, one thread per row
+    const int r = k + nb + (blockIdx.x - 1) * LU_RB + threadIdx.x;
+    if (r >= n) return;
+    C2 x[LU_NB];
+#pragma unroll
+    for (int c = 0; c < LU_NB; ++c)
+      if (c < nb) x[c] = A[r + (long long)n * (k + c)];
+#pragma unroll
+    for (int c = 0; c < LU_NB; ++c) {
+      if (c < nb) {
+        C2 v = x[c];
+#pragma unroll
+        for (int i = 0; i < LU_NB; ++i)
+          if (i < c) v = cfms(v, x[i], diag[i + nb * c]);
+        x[c] = cdv(v, diag[c + nb * c]);
+        A[r + (long long)n * (k + c)] = x[c];
+      }
+    }
+    return;
+  }
+  // U12 columns: L11 y = a (unit lower), one thread per column
+  const int c0 = k + nb + (blockIdx.x - 1 - nrb) * LU_CB;
+  const int ncol = min(LU_CB, n - c0);
+  for (int q = threadIdx.x; q < nb * ncol; q += blockDim.x) {
+    const int i = q % nb, c = q / nb;
+    work[i + nb * c] = A[(k + i) + (long long)n * (c0 + c)];
+  }
+  __syncthreads();
+  if (threadIdx.x < ncol) {
+    C2* y = work + nb * threadIdx.x;
+    for (int i = 1; i < nb; ++i) {
+      C2 v = y[i];
+      for (int j = 0; j < i; ++j) v = cfms(v, diag[i + nb * j], y[j]);
+      y[i] = v;
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nb * ncol; q += blockDim.x) {
+    const int i = q % nb, c = q / nb;
+    A[(k + i) + (long long)n * (c0 + c)] = work[i + nb * c];
+  }
+}
+
+// A22 -= L21 * U12: 64 x 64 output tile per CTA, 16 x 16 threads, 4 x 4 each.
+constexpr int GM_T = 64;
+template <class C2>
+__global__ void __launch_bounds__(256) zgemm_update_kernel(BatchT<C2> b, int k, int kb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2* As = reinterpret_cast<C2*>(smem_raw);   // [kb][64]
+  C2* Bs = As + LU_NB * GM_T;                 // [kb][64]
+  const int n = b.n;
+  const int r0 = k + kb + blockIdx.y * GM_T;
+  const int c0 = k + kb + blockIdx.x * GM_T;
+  C2* A = b.base + blockIdx.z * b.stride;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  if (blockIdx.x == 0 && blockIdx.y == 0) {
+    // store the factored diagonal block of this step (not read by this kernel)
+    const C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
+    for (int q = threadIdx.x; q < kb * kb; q += 256) A[(k + q % kb) + (long long)n * (k + q / kb)] = D[q];
+  }
+  for (int q = threadIdx.x; q < kb * GM_T; q += 256) {
+    const int m = q % GM_T, kk = q / GM_T;
+    const int r = r0 + m;
+    As[kk * GM_T + m] = (r < n) ? A[r + (long long)n * (k + kk)] : mkc<C2>(0., 0.);
+    const int kk2 = q % kb, nn = q / kb;
+    const int c = c0 + nn;
+    Bs[kk2 * GM_T + nn] = (c < n) ? A[(k + kk2) + (long long)n * c] : mkc<C2>(0., 0.);
+  }
+  __syncthreads();
+  C2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = mkc<C2>(0., 0.);
+#pragma unroll 4
+  for (int kk = 0; kk < kb; ++kk) {
+    C2 a[4], bb[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = As[kk * GM_T + ty + 16 * i];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bb[j] = Bs[kk * GM_T + tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acc[i][j].x += a[i].x * bb[j].x - a[i].y * bb[j].y;
+        acc[i][j].y += a[i].x * bb[j].y + a[i].y * bb[j].x;
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = c0 + tx + 16 * j;
+    if (c >= n) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = r0 + ty + 16 * i;
+      if (r >= n) continue;
+      C2* p = A + r + (long long)n * c;
+      C2 v = *p;
+      v.x -= acc[i][j].x;
+      v.y -= acc[i][j].y;
+      *p = v;
+    }
+  }
+}
+
+// last step of the factorization has no trailing update: store A11 here
+template <class C2>
+__global__ void lu_diag_store_kernel(BatchT<C2> b, int k, int kb) {
+  C2* A = b.base + blockIdx.z * b.stride;
+  const C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
+  for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) A[(k + q % kb) + (long long)b.n * (k + q / kb)] = D[q];
+}
+
+// ---------------------------------------------------------------------------
+// Multi-RHS triangular solves on the factored systems. X is n x nrhs per
+// system (ld = n) at xbase + s * xstride. One launch per block of TS_NB rows:
+// every CTA solves the diagonal block in shared memory (CTA 0 stores it) and
+// then applies the block to its slice of the remaining rows.
+// ---------------------------------------------------------------------------
+constexpr int TS_NB = 32;
+constexpr int MAX_RHS = 16;
+
+template <class C2, bool LOWER>
+__global__ void __launch_bounds__(128) trsm_step_kernel(BatchT<C2> b, C2* xbase, C2* ybase, long long xstride,
+                                                        int nrhs, int blk) {
+  // X: running right-hand sides (rows outside the block updated in place),
+  // Y: solution (the block's rows written by CTA 0). X and Y never alias, so
+  // every CTA reads the block's right-hand side before anyone changes it.
+  __shared__ C2 T[TS_NB * TS_NB];
+  __shared__ C2 Xs[TS_NB * MAX_RHS];
+  const int n = b.n;
+  const C2* A = b.base + blockIdx.z * b.stride;
+  C2* X = xbase + blockIdx.z * xstride;
+  C2* Y = ybase + blockIdx.z * xstride;
+  const int k = blk * TS_NB;
+  const int nb = min(TS_NB, n - k);
+  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
+    const int i = q % nb, c = q / nb;
+    T[i + TS_NB * c] = A[(k + i) + (long long)n * (k + c)];
+  }
+  for (int q = threadIdx.x; q < nb * nrhs; q += blockDim.x) {
+    const int i = q % nb, p = q / nb;
+    Xs[i + TS_NB * p] = X[(k + i) + (long long)n * p];
+  }
+  __syncthreads();
+  if (threadIdx.x < nrhs) {
+    C2* x = Xs + TS_NB * threadIdx.x;
+    if (LOWER) {
+      for (int i = 1; i < nb; ++i) {
+        C2 v = x[i];
+        for (int j = 0; j < i; ++j) v = cfms(v, T[i + TS_NB * j], x[j]);
+        x[i] = v;
+      }
+    } else {
+      for (int i = nb - 1; i >= 0; --i) {
+        C2 v = x[i];
+        for (int j = i + 1; j < nb; ++j) v = cfms(v, T[i + TS_NB * j], x[j]);
+        x[i] = cdv(v, T[i + TS_NB * i]);
+      }
+    }
+  }
+  __syncthreads();
+  if (blockIdx.x == 0) {
+    for (int q = threadIdx.x; q < nb * nrhs; q += blockDim.x) {
+      const int i = q % nb, p = q / nb;
+      Y[(k + i) + (long long)n * p] = Xs[i + TS_NB * p];
+    }
+  }
+  // rows to update: below the block (lower) or above it (upper)
+  const int lo = LOWER ? k + nb : 0;
+  const int hi = LOWER ? n : k;
+  const int r = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= hi) return;
+  C2 acc[MAX_RHS];
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p) acc[p] = mkc<C2>(0., 0.);
+  for (int c = 0; c < nb; ++c) {
+    const C2 a = A[r + (long long)n * (k + c)];
+#pragma unroll
+    for (int p = 0; p < MAX_RHS; ++p)
+      if (p < nrhs) {
+        const C2 xv = Xs[c + TS_NB * p];
+        acc[p].x += a.x * xv.x - a.y * xv.y;
+        acc[p].y += a.x * xv.y + a.y * xv.x;
+      }
+  }
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p)
+    if (p < nrhs) {
+      C2* q = X + r + (long long)n * p;
+      C2 v = *q;
+      v.x -= acc[p].x;
+      v.y -= acc[p].y;
+      *q = v;
+    }
+}
+
+// Y = M X for n x n M (ld n) and n x nrhs X: the boundary potential S*sigma.
+__global__ void __launch_bounds__(128) matmul_rhs_kernel(Batch m, const double2* xbase, long long xstride,
+                                                         double2* ybase, long long ystride, int nrhs) {
+  __shared__ double2 Xs[64 * MAX_RHS];
+  const int n = m.n;
+  const double2* M = m.base + blockIdx.z * m.stride;
+  const double2* X = xbase + blockIdx.z * xstride;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double2 acc[MAX_RHS];
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p) acc[p] = make_double2(0., 0.);
+  for (int c0 = 0; c0 < n; c0 += 64) {
+    const int nc = min(64, n - c0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < nc * nrhs; q += blockDim.x) {
+      const int c = q % nc, p = q / nc;
+      Xs[c + 64 * p] = X[(c0 + c) + (long long)n * p];
+    }
+    __syncthreads();
+    if (r < n) {
+      for (int c = 0; c < nc; ++c) {
+        const double2 a = M[r + (long long)n * (c0 + c)];
+#pragma unroll
+        for (int p = 0; p < MAX_RHS; ++p)
+          if (p < nrhs) {
+            const double2 xv = Xs[c + 64 * p];
+            acc[p].x += a.x * xv.x - a.y * xv.y;
+            acc[p].y += a.x * xv.y + a.y * xv.x;
+          }
+      }
+    }
+  }
+  if (r >= n) return;
+  double2* Y = ybase + blockIdx.z * ystride;
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p)
+    if (p < nrhs) Y[r + (long long)n * p] = acc[p];
+}
+
+// B = (NVEL(I) +- NVEL(I+NFA))/2 per symmetry class (SOLVE_BEM_INFD_DIRECT.f90:123-131)
+// nvel: (2^s n) x nrhs per frequency; X: system (w, class) at (w*cls+class)*n*nrhs
+__global__ void fold_rhs_kernel(const double2* __restrict__ nvel, int n, int nsymy, int nrhs, double2* __restrict__ X) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = blockIdx.y, w = blockIdx.z;
+  const int cls = nsymy ? 2 : 1;
+  const double2* v = nvel + ((long long)w * nrhs + p) * cls * n;
+  if (nsymy) {
+    const double2 a = v[i], b = v[i + n];
+    X[((long long)w * 2 + 0) * n * nrhs + (long long)p * n + i] = make_double2((a.x + b.x) * 0.5, (a.y + b.y) * 0.5);
+    X[((long long)w * 2 + 1) * n * nrhs + (long long)p * n + i] = make_double2((a.x - b.x) * 0.5, (a.y - b.y) * 0.5);
+  } else {
+    X[(long long)w * n * nrhs + (long long)p * n + i] = v[i];
+  }
+}
+
+// Force(i,p) = -sum_c PRESSURE(c) NDS(i,c), PRESSURE = RHO*i*W*ZP with
+// ZP = phi+ + phi- on the meshed half and phi+ - phi- on its mirror
+// (SOLVE_BEM.f90:91-96, NEMOH.f90:137-141). phi: system (w,class) n x nrhs.
+__global__ void __launch_bounds__(256) force_kernel(const double2* __restrict__ phi, const OmegaParams* __restrict__ oms,
+                                                    int n, int nsymy, int nrhs, int nint, const double* __restrict__ nds,
+                                                    double rho, double2* __restrict__ force) {
+  const int i = blockIdx.x, p = blockIdx.y, w = blockIdx.z;
+  const int cls = nsymy ? 2 : 1;
+  const double2* pp = phi + ((long long)w * cls + 0) * n * nrhs + (long long)p * n;
+  const double2* pm = phi + ((long long)w * cls + (cls - 1)) * n * nrhs + (long long)p * n;
+  double sr = 0., si = 0.;
+  for (int c = threadIdx.x; c < cls * n; c += blockDim.x) {
+    double2 z;
+    if (!nsymy) z = pp[c];
+    else if (c < n) z = make_double2(pp[c].x + pm[c].x, pp[c].y + pm[c].y);
+    else z = make_double2(pp[c - n].x - pm[c - n].x, pp[c - n].y - pm[c - n].y);
+    const double f = nds[i + (long long)nint * c];
+    sr += z.x * f;
+    si += z.y * f;
+  }
+  __shared__ double red[2][256];
+  red[0][threadIdx.x] = sr;
+  red[1][threadIdx.x] = si;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double rw = rho * oms[w].w;
+    // -(i rho W) * sum(ZP * NDS)
+    force[((long long)w * nrhs + p) * nint + i] = make_double2(rw * red[1][0], -rw * red[0][0]);
+  }
+}
+
+}  // namespace nb200

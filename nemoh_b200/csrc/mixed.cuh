@@ -1,0 +1,229 @@
+// Mixed-precision solve: low-precision LU of the influence matrix, FP64
+// iterative refinement against the FP64 matrix.
+//
+// x0 = LU32^-1 b;  repeat  r = b - D x (FP64 residual, FP64 matrix D),
+//                          x += LU32^-1 r   until |r|inf <= tol |b|inf.
+// The FP32 factorization reuses the blocked no-pivot LU of linalg.cuh; its
+// trailing updates run on the tensor cores (split-BF16 operands, FP32
+// accumulation) when the tcgen05 path is enabled, else as FP32 SIMT GEMMs.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "linalg.cuh"
+#include "tc_gemm.cuh"
+
+namespace nb200 {
+
+constexpr int REFINE_MAX_IT = 30;
+constexpr double REFINE_TOL = 1e-13;
+
+struct MixedWork {
+  float2* lu = nullptr;      // FP32 factors, nsys x n x n
+  float2* diag = nullptr;    // panel scratch
+  double2* b = nullptr;      // right-hand sides (FP64)
+  double2* r = nullptr;      // residual (FP64)
+  float2* rf = nullptr;      // residual/correction (FP32)
+  float2* yf = nullptr;      // forward-solve scratch (FP32)
+  unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
+  TcWork tc;                 // tensor-core GEMM operand buffers
+  int cap_sys = 0, cap_n = 0, cap_rhs = 0;
+  size_t total = 0;
+  int last_iterations = 0;
+  double last_residual = 0.;
+
+  size_t bytes() const { return total; }
+  void release() {
+    cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms);
+    tc.release();
+    lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr;
+    cap_sys = cap_n = cap_rhs = 0;
+    total = 0;
+  }
+  ~MixedWork() { release(); }
+  cudaError_t ensure(int nsys, int n, int nrhs) {
+    if (nsys <= cap_sys && n == cap_n && nrhs <= cap_rhs) return cudaSuccess;
+    release();
+    const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
+    cudaError_t e;
+    if ((e = cudaMalloc(&lu, nsys * NN * sizeof(float2)))) return e;
+    if ((e = cudaMalloc(&diag, (size_t)nsys * LU_NB * LU_NB * sizeof(float2)))) return e;
+    if ((e = cudaMalloc(&b, V * sizeof(double2)))) return e;
+    if ((e = cudaMalloc(&r, V * sizeof(double2)))) return e;
+    if ((e = cudaMalloc(&rf, V * sizeof(float2)))) return e;
+    if ((e = cudaMalloc(&yf, V * sizeof(float2)))) return e;
+    if ((e = cudaMalloc(&norms, (size_t)2 * nsys * nrhs * sizeof(unsigned long long)))) return e;
+    if ((e = tc.ensure(nsys, n))) return e;
+    cap_sys = nsys;
+    cap_n = n;
+    cap_rhs = nrhs;
+    total = nsys * NN * sizeof(float2) + V * (2 * sizeof(double2) + 2 * sizeof(float2)) + tc.bytes();
+    return cudaSuccess;
+  }
+};
+
+inline size_t mixed_bytes_per_system(size_t n) { return n * n * sizeof(float2) + tc_bytes_per_system(n); }
+
+__global__ void d2f_kernel(const double2* __restrict__ a, float2* __restrict__ b, long long count) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count; q += (long long)gridDim.x * blockDim.x) {
+    const double2 v = a[q];
+    b[q] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// x += correction (FP32 -> FP64); on the first pass x = correction
+__global__ void accumulate_kernel(double2* __restrict__ x, const float2* __restrict__ d, long long count, int first) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count; q += (long long)gridDim.x * blockDim.x) {
+    const float2 v = d[q];
+    if (first) x[q] = make_double2(v.x, v.y);
+    else {
+      double2 o = x[q];
+      o.x += v.x;
+      o.y += v.y;
+      x[q] = o;
+    }
+  }
+}
+
+// |b|inf per (system, rhs)
+__global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsigned long long* out) {
+  const int p = blockIdx.y, s = blockIdx.z;
+  const double2* x = v + ((long long)s * nrhs + p) * n;
+  double m = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = fmax(m, fmax(fabs(x[i].x), fabs(x[i].y)));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
+}
+
+// r = b - D x in FP64, rf = (float) r, and |r|inf per (system, rhs)
+__global__ void __launch_bounds__(128) residual_kernel(Batch m, const double2* __restrict__ x, const double2* __restrict__ b,
+                                                       double2* __restrict__ r, float2* __restrict__ rf, int nrhs,
+                                                       unsigned long long* __restrict__ rnorm) {
+  __shared__ double2 Xs[64 * MAX_RHS];
+  const int n = m.n;
+  const double2* M = m.base + blockIdx.z * m.stride;
+  const long long vs = (long long)blockIdx.z * n * nrhs;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double2 acc[MAX_RHS];
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p) acc[p] = make_double2(0., 0.);
+  for (int c0 = 0; c0 < n; c0 += 64) {
+    const int nc = min(64, n - c0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < nc * nrhs; q += blockDim.x) {
+      const int c = q % nc, p = q / nc;
+      Xs[c + 64 * p] = x[vs + (c0 + c) + (long long)n * p];
+    }
+    __syncthreads();
+    if (row < n) {
+      for (int c = 0; c < nc; ++c) {
+        const double2 a = M[row + (long long)n * (c0 + c)];
+#pragma unroll
+        for (int p = 0; p < MAX_RHS; ++p)
+          if (p < nrhs) {
+            const double2 xv = Xs[c + 64 * p];
+            acc[p].x += a.x * xv.x - a.y * xv.y;
+            acc[p].y += a.x * xv.y + a.y * xv.x;
+          }
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p) {
+    if (p >= nrhs) break;
+    double mx = 0.;
+    if (row < n) {
+      const long long q = vs + row + (long long)n * p;
+      const double2 bb = b[q];
+      const double2 rr = make_double2(bb.x - acc[p].x, bb.y - acc[p].y);
+      r[q] = rr;
+      rf[q] = make_float2((float)rr.x, (float)rr.y);
+      mx = fmax(fabs(rr.x), fabs(rr.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0)
+      atomicMax(rnorm + (long long)blockIdx.z * nrhs + p, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches) {
+  const long long total = (long long)nsys * n * n;
+  d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
+  ++launches;
+  BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
+  for (int k = 0; k < n; k += LU_NB) {
+    const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
+    const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
+    lu_panel_kernel<float2><<<dim3(1 + nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k, status);
+    ++launches;
+    if (rest > 0) {
+      if (!tc_update(w.tc, b, k, nb, nsys, st, launches)) {
+        const int t = (rest + GM_T - 1) / GM_T;
+        zgemm_update_kernel<float2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(float2), st>>>(b, k, nb);
+        ++launches;
+      }
+    } else {
+      lu_diag_store_kernel<float2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, nb);
+      ++launches;
+    }
+  }
+}
+
+inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches) {
+  BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
+  const long long xs = (long long)n * nrhs;
+  const int nblk = (n + TS_NB - 1) / TS_NB;
+  for (int blk = 0; blk < nblk; ++blk) {
+    const int below = std::max(0, n - (blk + 1) * TS_NB);
+    trsm_step_kernel<float2, true><<<dim3(std::max(1, (below + 127) / 128), 1, nsys), 128, 0, st>>>(b, w.rf, w.yf, xs,
+                                                                                                   nrhs, blk);
+    ++launches;
+  }
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int above = blk * TS_NB;
+    trsm_step_kernel<float2, false><<<dim3(std::max(1, (above + 127) / 128), 1, nsys), 128, 0, st>>>(b, w.yf, w.rf, xs,
+                                                                                                    nrhs, blk);
+    ++launches;
+  }
+}
+
+// X: right-hand sides in, solution out (FP64); Y unused scratch
+inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double2* X, double2* /*Y*/, int nrhs,
+                               cudaStream_t st, long long& launches) {
+  const long long V = (long long)nsys * n * nrhs;
+  const int nv = nsys * nrhs;
+  cudaMemcpyAsync(w.b, X, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+  cudaMemsetAsync(w.norms, 0, 2 * (size_t)nv * sizeof(unsigned long long), st);
+  norm_kernel<<<dim3(4, nrhs, nsys), 256, 0, st>>>(w.b, n, nrhs, w.norms + nv);
+  ++launches;
+  d2f_kernel<<<1184, 256, 0, st>>>(w.b, w.rf, V);
+  ++launches;
+  std::vector<unsigned long long> h(2 * (size_t)nv);
+  Batch dm{D, (long long)n * n, n, nullptr};
+  w.last_iterations = 0;
+  for (int it = 0; it < REFINE_MAX_IT; ++it) {
+    trsm_f32(w, n, nsys, nrhs, st, launches);
+    accumulate_kernel<<<1184, 256, 0, st>>>(X, w.rf, V, it == 0);
+    ++launches;
+    cudaMemsetAsync(w.norms, 0, (size_t)nv * sizeof(unsigned long long), st);
+    residual_kernel<<<dim3((n + 127) / 128, 1, nsys), 128, 0, st>>>(dm, X, w.b, w.r, w.rf, nrhs, w.norms);
+    ++launches;
+    cudaMemcpyAsync(h.data(), w.norms, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    double worst = 0.;
+    for (int q = 0; q < nv; ++q) {
+      double rn, bn;
+      std::memcpy(&rn, &h[q], 8);
+      std::memcpy(&bn, &h[nv + q], 8);
+      worst = std::max(worst, bn > 0 ? rn / bn : rn);
+    }
+    w.last_iterations = it + 1;
+    w.last_residual = worst;
+    if (worst <= REFINE_TOL || !(worst == worst)) break;
+  }
+}
+
+}  // namespace nb200

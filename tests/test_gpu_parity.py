@@ -1,0 +1,164 @@
+"""Parity of the CUDA path with the CPU FP64 oracle, through the C-ABI.
+
+Tolerances (FP64 path): panel geometry bit-exact (it decides every branch);
+Green tables 1e-13 of the table's magnitude; influence matrices 1e-12 of each
+row's largest entry; source strengths and potentials 1e-10; forces (added
+mass, damping, excitation) 1e-9 relative to the largest force of the same
+integration case. Mixed precision (FP32 LU + FP64 refinement): 1e-6 of FP64.
+"""
+import numpy as np
+import pytest
+
+import gpu_cases as G
+import nemoh_b200 as nb
+import oracle_lib as O
+import verification as V
+from nemoh_b200 import build as B
+from nemoh_b200 import cases as C
+
+pytestmark = pytest.mark.gpu
+
+CASES = G.small_cases()
+IDS = [c.name for c in CASES]
+
+
+@pytest.fixture(scope="module")
+def solver():
+    B.build()
+    s = nb.Solver(0, nb.FP64)
+    yield s
+    s.close()
+
+
+def _mesh(s, case):
+    m = case.mesh
+    s.set_mesh(m.nodes, m.panels, m.isym, case.rho, case.g, case.depth)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_geometry_bit_exact(solver, case):
+    _mesh(solver, case)
+    g, zer = solver.geometry()
+    o = G.oracle_for(case)
+    go, zo = o.geometry()
+    assert zer == zo
+    assert np.array_equal(g, go), np.abs(g - go).max()
+
+
+def test_tables_match_oracle(solver):
+    xr, xz, apd = solver.tables()
+    case = CASES[0]
+    o = G.oracle_for(case)
+    xr2, xz2, apd2 = o.tables()
+    assert np.array_equal(xr, xr2) and np.array_equal(xz, xz2)
+    scale = np.abs(apd2).max(axis=(1, 2), keepdims=True)
+    assert np.max(np.abs(apd - apd2) / scale) < 1e-13
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_assembly_matches_oracle(solver, case):
+    _mesh(solver, case)
+    o = G.oracle_for(case)
+    for w in case.omegas:
+        gm, mode = solver.assemble(w)
+        om, mode_o, _ = o.assemble(w)
+        assert mode == mode_o
+        for a, b in zip(gm, om):
+            row = np.abs(b).max(axis=1, keepdims=True)
+            err = np.abs(a - b) / row
+            assert err.max() < 1e-12, (case.name, w, err.max(), np.unravel_index(err.argmax(), err.shape))
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_solve_problem_matches_oracle(solver, case):
+    """The reference boundary, problem by problem in the pre-processor's order."""
+    _mesh(solver, case)
+    o = G.oracle_for(case)
+    nv = C.body_conditions(case)
+    npb = len(case.betas_deg) + len(case.rad)
+    for j in range(nv.shape[1]):
+        w = case.omegas[j // npb]
+        T = 2 * np.pi / w
+        g = solver.solve_potential(T, nv[:, j])
+        r = O.Oracle.solve_problem(o, T, nv[:, j])
+        assert g["nexp"] == r["nexp"]
+        for k in ("zigb", "zpb") + (("zigs", "zps") if case.mesh.isym else ()):
+            scale = np.abs(r[k]).max()
+            assert np.abs(g[k] - r[k]).max() <= 1e-10 * scale, (case.name, j, k)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_forces_match_oracle(solver, case, tmp_path):
+    _mesh(solver, case)
+    nvel, nds, npb = G.problems(case)
+    F = solver.solve_frequencies(case.omegas, nvel, nds)
+    Fo = G.oracle_forces(case, str(tmp_path))
+    assert G.rel_err(F, Fo) < 1e-9
+
+
+def test_two_body_finite_depth_verification_case(solver, tmp_path):
+    fx = V.load("2Bodies")
+    case = V.case_from_fixture(fx, omegas=fx["omegas"][4:7])
+    _mesh(solver, case)
+    nvel, nds, npb = G.problems(case)
+    F = solver.solve_frequencies(case.omegas, nvel, nds)
+    Fo = G.oracle_forces(case, str(tmp_path))
+    assert G.rel_err(F, Fo) < 1e-9
+
+
+def test_cylinder_verification_against_reference_results(solver):
+    fx = V.load("Cylinder")
+    case = V.case_from_fixture(fx)
+    _mesh(solver, case)
+    nvel, nds, npb = G.problems(case)
+    F = solver.solve_frequencies(case.omegas, nvel, nds)
+    nb_ = len(case.betas_deg)
+    A = np.zeros((len(case.omegas), F.shape[0], len(case.rad)))
+    Bd = np.zeros_like(A)
+    for iw, w in enumerate(case.omegas):
+        A[iw] = F[:, nb_:, iw].imag / w
+        Bd[iw] = -F[:, nb_:, iw].real
+    errs = V.compare_cw(fx, A, Bd)
+    assert max(errs)[0] < 1e-4
+
+
+def test_repeated_frequency_reuses_factorization(solver):
+    case = CASES[0]
+    _mesh(solver, case)
+    nv = C.body_conditions(case)
+    T = 2 * np.pi / case.omegas[0]
+    n0 = solver.launches
+    solver.solve_potential(T, nv[:, 0])
+    n1 = solver.launches
+    solver.solve_potential(T, nv[:, 1])
+    n2 = solver.launches
+    assert (n2 - n1) < (n1 - n0) / 2   # no assembly or factorization on the second call
+
+
+def test_degenerate_panel_reports_status(solver):
+    case = CASES[0]
+    panels = case.mesh.panels.copy()
+    panels[5] = [panels[5][0]] * 4
+    with pytest.raises(nb.NemohError) as e:
+        solver.set_mesh(case.mesh.nodes, panels, 0, 1025.0, 9.81, 0.0)
+    assert e.value.code == 2
+
+
+def test_tiny_frequency_reports_status(solver):
+    case = CASES[0]
+    _mesh(solver, case)
+    nv = C.body_conditions(case)
+    with pytest.raises(nb.NemohError) as e:
+        solver.solve_potential(2 * np.pi / 5e-5, nv[:, 0])
+    assert e.value.code == 4
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_mixed_precision_matches_fp64(case):
+    with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
+        for s in (s64, smx):
+            _mesh(s, case)
+        nvel, nds, npb = G.problems(case)
+        F64 = s64.solve_frequencies(case.omegas, nvel, nds)
+        Fmx = smx.solve_frequencies(case.omegas, nvel, nds)
+        assert G.rel_err(Fmx, F64) < 1e-6
