@@ -331,10 +331,12 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
     factor_and_solve(c, nw * cls, nrhs, true);
     CK(cudaEventRecord(c->ev[2], c->stream));
     potential(c, nw * cls, nrhs);
-    force_kernel<<<dim3(nint, nrhs, nw), 256, 0, c->stream>>>(c->d_Y.as<double2>(), c->d_oms.as<OmegaParams>(), N,
-                                                              c->nsymy, nrhs, nint, nds_d, c->rho,
-                                                              force_d + (long long)w0 * nrhs * nint);
-    LAUNCHED(c);
+    if (nint > 0) {
+      force_kernel<<<dim3(nint, nrhs, nw), 256, 0, c->stream>>>(c->d_Y.as<double2>(), c->d_oms.as<OmegaParams>(), N,
+                                                                c->nsymy, nrhs, nint, nds_d, c->rho,
+                                                                force_d + (long long)w0 * nrhs * nint);
+      LAUNCHED(c);
+    }
     CK(cudaEventRecord(c->ev[3], c->stream));
     check_status(c);
     float a, f, s;

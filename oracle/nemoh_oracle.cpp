@@ -1781,6 +1781,82 @@ struct Oracle {
     if (depth_mode) *depth_mode = fd ? 1 : 0;
     if (nexp_out) *nexp_out = NEXP;
   }
+  // Bounded timing sample of one faithful per-frequency solve (SOLVE_BVP for
+  // nprob problems at one omega: assembly of both symmetry classes, GAUSSZ
+  // inverse per class, and per problem AInv*B plus the boundary potential by
+  // recomputed Green functions), extrapolated to the full solve by operation
+  // counts. Stage rates come from timing real work: whole rows of the Green
+  // evaluations and the first elimination steps of GAUSSZ on an N x 2N matrix.
+  // detail: [0] s/pair-evaluation, [1] s/complex MAC in GAUSSZ, [2] pairs
+  // timed, [3] elimination steps timed, [4] estimated s for one solve.
+  double sample_solve(double omega, int nprob, double budget_s, double* detail) {
+    using clk = std::chrono::steady_clock;
+    const double PI = 4. * std::atan(1.);
+    T = 2. * PI / omega;
+    const R W = 2. * PI / T;
+    const R kwave = W * W / G;
+    const bool fd = !((Depth == 0.) || (kwave * Depth >= 20));
+    R AM0, AMH = 0.;
+    int NEXP = 0, N = 0;
+    for (int i = 0; i <= NPINTE; ++i) { CQ[i] = 0.; QQ[i] = 0.; }
+    R GM = compute_GM();
+    if (!fd) {
+      AM0 = W * W / G;
+      cint(AM0 * GM, N, QQ, CQ);
+    } else {
+      AMH = X0(W * W * Depth / G);
+      AM0 = AMH / Depth;
+      for (int i = 0; i < 32; ++i) { AMBDA[i] = 0.; AR[i] = 0.; }
+      R lq[NPINTE + 1], lc[NPINTE + 1];
+      cint(AM0 * GM, N, lq, lc);
+      NQ = N;
+      LISC(AMH * std::tanh(AMH), AMH, NEXP, AMBDA, AR);
+    }
+    // Green evaluations, whole rows, ISYM=1 fill as SOLVE_BEM_*_DIRECT
+    auto t0 = clk::now();
+    long long pairs = 0;
+    volatile double sink = 0.;
+    for (int ISP = 1; ISP <= IMX; ++ISP) {
+      for (int IFP = 1; IFP <= IMX; ++IFP) {
+        green(fd, AM0, AMH, NEXP, ISP, IFP);
+        sink = sink + VSXP1 * XN[ISP] + VSYP1 * YN[ISP] + VSZP1 * ZN[ISP];
+      }
+      pairs += IMX;
+      if (std::chrono::duration<double>(clk::now() - t0).count() > budget_s / 2) break;
+    }
+    const double t_pair = std::chrono::duration<double>(clk::now() - t0).count() / pairs;
+    // GAUSSZ: first elimination steps of an N x 2N system
+    const int n = IMX, m = 2 * IMX;
+    for (int j = 1; j <= m; ++j)
+      for (int i = 1; i <= n; ++i) zij(i, j) = (j <= n) ? C(i == j ? 4. : 1.e-3 / (1 + std::abs(i - j)), 1.e-3) : C(i + n == j ? 1. : 0., 0.);
+    t0 = clk::now();
+    double macs = 0.;
+    int steps = 0;
+    for (int J = 1; J <= n - 1; ++J) {
+      for (int Kc = J + 1; Kc <= m; ++Kc) {
+        C P = zij(J, Kc) / zij(J, J);
+        C* colK = &zij(1, Kc);
+        C* colJ = &zij(1, J);
+        for (int I = J + 1; I <= n; ++I) colK[I - 1] = colK[I - 1] - colJ[I - 1] * P;
+      }
+      macs += (double)(m - J) * (n - J);
+      ++steps;
+      if (std::chrono::duration<double>(clk::now() - t0).count() > budget_s / 2) break;
+    }
+    const double t_mac = std::chrono::duration<double>(clk::now() - t0).count() / macs;
+    // full GAUSSZ on [A|I]: elimination sum_j (M-j)(N-j) plus back substitution N * N(N-1)/2
+    double elim = 0.;
+    for (int J = 1; J <= n - 1; ++J) elim += (double)(m - J) * (n - J);
+    const double gauss = elim + (double)n * n * (n - 1) / 2.;
+    const double cls = NSYMY + 1.;
+    const double nn = (double)n * n;
+    const double est = cls * nn * t_pair + cls * gauss * t_mac + nprob * (nn * t_pair + cls * nn * t_mac);
+    if (detail) {
+      detail[0] = t_pair; detail[1] = t_mac; detail[2] = (double)pairs; detail[3] = steps; detail[4] = est;
+    }
+    (void)sink;
+    return est;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -1984,6 +2060,15 @@ int nemoh_oracle_solve_problem(void* h, double period, const double* nvel, doubl
     if (nexp) *nexp = ne;
     if (used_fd) *used_fd = fd ? 1 : 0;
   })
+}
+
+double nemoh_oracle_sample_solve(void* h, double omega, int nprob, double budget_s, double* detail) {
+  try {
+    return static_cast<Oracle*>(h)->sample_solve(omega, nprob, budget_s, detail);
+  } catch (const Stop& e) {
+    g_last_error = e.what();
+    return -1.;
+  }
 }
 
 int nemoh_oracle_get_nq(void* h) { return static_cast<Oracle*>(h)->NQ; }

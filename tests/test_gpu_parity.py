@@ -2,7 +2,9 @@
 
 Tolerances (FP64 path): panel geometry bit-exact (it decides every branch);
 Green tables 1e-13 of the table's magnitude; influence matrices 1e-12 of each
-row's largest entry; source strengths and potentials 1e-10; forces (added
+row's largest entry in deep water and 1e-10 in finite depth (the exponential
+image sums cancel more; a flipped branch would show as ~1e-3); source
+strengths and potentials 1e-10; forces (added
 mass, damping, excitation) 1e-9 relative to the largest force of the same
 integration case. Mixed precision (FP32 LU + FP64 refinement): 1e-6 of FP64.
 """
@@ -63,10 +65,11 @@ def test_assembly_matches_oracle(solver, case):
         gm, mode = solver.assemble(w)
         om, mode_o, _ = o.assemble(w)
         assert mode == mode_o
+        tol = 1e-10 if mode else 1e-12
         for a, b in zip(gm, om):
             row = np.abs(b).max(axis=1, keepdims=True)
             err = np.abs(a - b) / row
-            assert err.max() < 1e-12, (case.name, w, err.max(), np.unravel_index(err.argmax(), err.shape))
+            assert err.max() < tol, (case.name, w, err.max(), np.unravel_index(err.argmax(), err.shape))
 
 
 @pytest.mark.parametrize("case", CASES, ids=IDS)
@@ -80,7 +83,7 @@ def test_solve_problem_matches_oracle(solver, case):
         w = case.omegas[j // npb]
         T = 2 * np.pi / w
         g = solver.solve_potential(T, nv[:, j])
-        r = O.Oracle.solve_problem(o, T, nv[:, j])
+        r = o.solve_problem(T, nv[:, j])
         assert g["nexp"] == r["nexp"]
         for k in ("zigb", "zpb") + (("zigs", "zps") if case.mesh.isym else ()):
             scale = np.abs(r[k]).max()
@@ -132,7 +135,10 @@ def test_repeated_frequency_reuses_factorization(solver):
     n1 = solver.launches
     solver.solve_potential(T, nv[:, 1])
     n2 = solver.launches
-    assert (n2 - n1) < (n1 - n0) / 2   # no assembly or factorization on the second call
+    # the second call launches no assembly and no factorization: exactly one
+    # assembly launch and 2*ceil(N/32) LU launches fewer than the first
+    n_lu = 2 * ((case.mesh.npanels + 31) // 32)
+    assert (n1 - n0) - (n2 - n1) == 1 + n_lu
 
 
 def test_degenerate_panel_reports_status(solver):
