@@ -41,6 +41,7 @@ typedef struct nemoh_ctx nemoh_ctx;
 #define NEMOH_B200_ENOMEM 21         /* device memory exhausted / admission refused */
 #define NEMOH_B200_ENODEV 22         /* no CUDA device */
 #define NEMOH_B200_ECAPACITY 23      /* size beyond a documented limit */
+#define NEMOH_B200_ETIMEOUT 30       /* a bounded device-side wait gave up */
 
 /* precision modes */
 #define NEMOH_B200_FP64 0            /* FP64 assembly, FP64 LU */
@@ -97,6 +98,8 @@ int nemoh_b200_get_tables(nemoh_ctx* ctx, double* xr, double* xz, double* apd);
 int nemoh_b200_get_geometry(nemoh_ctx* ctx, double* out, double* zer);
 /* timing of the last solve_frequencies call: assembly, factorization, solve+potential+forces (ms) */
 int nemoh_b200_last_timings(nemoh_ctx* ctx, double* assemble_ms, double* factor_ms, double* solve_ms);
+/* mixed precision: refinement iterations and final max relative residual of the last solve */
+int nemoh_b200_last_refinement(nemoh_ctx* ctx, int* iterations, double* residual);
 /* number of CUDA kernel launches issued by this context since creation */
 long long nemoh_b200_launch_count(const nemoh_ctx* ctx);
 

@@ -35,7 +35,7 @@ _vp = ctypes.c_void_p
 
 _ERRNAMES = {1: "EINVAL", 2: "EPANEL_AREA", 3: "EPIVOT", 4: "EOMEGA", 5: "ELISC", 6: "ESPRBM",
              7: "EDISPERSION", 8: "EAKZ", 9: "EIO", 10: "EHOUSRS", 20: "ECUDA", 21: "ENOMEM",
-             22: "ENODEV", 23: "ECAPACITY"}
+             22: "ENODEV", 23: "ECAPACITY", 30: "ETIMEOUT"}
 
 
 class NemohError(RuntimeError):
@@ -70,6 +70,7 @@ def load_library():
     L.nemoh_b200_get_tables.argtypes = [_vp, _d, _d, _d]
     L.nemoh_b200_get_geometry.argtypes = [_vp, _d, _d]
     L.nemoh_b200_last_timings.argtypes = [_vp, _d, _d, _d]
+    L.nemoh_b200_last_refinement.argtypes = [_vp, _i, _d]
     L.nemoh_b200_launch_count.argtypes = [_vp]
     L.nemoh_b200_launch_count.restype = ctypes.c_longlong
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
@@ -194,6 +195,11 @@ class Solver:
         a, f, s = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         load_library().nemoh_b200_last_timings(self._h, ctypes.byref(a), ctypes.byref(f), ctypes.byref(s))
         return dict(assemble_ms=a.value, factor_ms=f.value, solve_ms=s.value)
+
+    def last_refinement(self):
+        it, res = ctypes.c_int(), ctypes.c_double()
+        load_library().nemoh_b200_last_refinement(self._h, ctypes.byref(it), ctypes.byref(res))
+        return it.value, res.value
 
     # -- diagnostics -----------------------------------------------------------
     def assemble(self, omega):

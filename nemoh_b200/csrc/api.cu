@@ -101,7 +101,8 @@ void check_status(nemoh_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
   if (st) {
     CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
-    const char* m = st == ST_PIVOT ? "PIVOT INFERIEUR A 1.E-20 (GAUSSZ)"
+    const char* m = st == ST_TC_TIMEOUT ? "tensor-core update timed out waiting on its operands"
+                    : st == ST_PIVOT ? "PIVOT INFERIEUR A 1.E-20 (GAUSSZ)"
                     : st == ST_PANEL_AREA ? "area of a panel is too small (GOMG)"
                     : st == ST_AKZ_UNDEFINED ? "AKZ > -1.5E-6: wave term undefined in the reference"
                                               : "device error";
@@ -634,6 +635,13 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* c, int nomega, const double* 
     CK(cudaStreamWaitEvent(user, e, 0));
     CK(cudaEventDestroy(e));
   });
+}
+
+int nemoh_b200_last_refinement(nemoh_ctx* c, int* iterations, double* residual) {
+  if (!c) return NEMOH_B200_EINVAL;
+  if (iterations) *iterations = c->mixed.last_iterations;
+  if (residual) *residual = c->mixed.last_residual;
+  return NEMOH_B200_OK;
 }
 
 int nemoh_b200_last_timings(nemoh_ctx* c, double* a, double* f, double* s) {

@@ -160,7 +160,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
     lu_panel_kernel<float2><<<dim3(1 + nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k, status);
     ++launches;
     if (rest > 0) {
-      if (!tc_update(w.tc, b, k, nb, nsys, st, launches)) {
+      if (!tc_update(w.tc, b, k, nb, nsys, st, launches, status)) {
         const int t = (rest + GM_T - 1) / GM_T;
         zgemm_update_kernel<float2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(float2), st>>>(b, k, nb);
         ++launches;

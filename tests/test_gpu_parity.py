@@ -168,3 +168,6 @@ def test_mixed_precision_matches_fp64(case):
         F64 = s64.solve_frequencies(case.omegas, nvel, nds)
         Fmx = smx.solve_frequencies(case.omegas, nvel, nds)
         assert G.rel_err(Fmx, F64) < 1e-6
+        # a good low-precision factorization converges in a few refinement steps
+        it, res = smx.last_refinement()
+        assert it <= 6 and res <= 1e-13, (it, res)
