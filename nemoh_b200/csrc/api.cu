@@ -62,9 +62,10 @@ struct nemoh_ctx {
   // mesh
   int np = 0, nfa = 0, nsymy = 0;
   double rho = 0, g = 0, depth = 0, zer = 0, gm = 0;
+  double ro_eps2 = 0;   // largest x with sqrt(x) <= 1e-4
   DevBuf d_xyz, d_m, d_rec, d_rows;
   // per-call workspace
-  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_oms, d_slots, d_nvel, d_nds, d_force;
+  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force;
   MixedWork mixed;
   int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
   double w_previous = -1.;   // factor cache key of solve_problem
@@ -167,10 +168,10 @@ int batch_capacity(nemoh_ctx* c, int nrhs, int want) {
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t N = c->nfa, cls = ncls(c);
   size_t per = (2 * cls * N * N + 2 * cls * N * (size_t)std::max(nrhs, 1)) * sizeof(double2) + sizeof(OmegaParams) +
-               cls * LU_NB * LU_NB * sizeof(double2);
+               cls * LU_NB * LU_NB * sizeof(double2) + cls * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2);
   if (c->mode == NEMOH_B200_MIXED) per += mixed_bytes_per_system(N) * cls;
   // existing buffers count as available
-  size_t have = c->d_D.bytes + c->d_S.bytes + c->d_X.bytes + c->d_Y.bytes + c->mixed.bytes();
+  size_t have = c->d_D.bytes + c->d_S.bytes + c->d_X.bytes + c->d_Y.bytes + c->d_inv.bytes + c->mixed.bytes();
   size_t budget = (size_t)((fr + have) * 0.8);
   int cap = (int)std::max<size_t>(1, budget / per);
   return std::min(cap, want);
@@ -185,6 +186,8 @@ void ensure_batch(nemoh_ctx* c, int slots, int nrhs) {
   CK(c->d_X.ensure(rhs));
   CK(c->d_Y.ensure(rhs));
   CK(c->d_diag.ensure((size_t)slots * cls * LU_NB * LU_NB * sizeof(double2)));
+  if (c->mode == NEMOH_B200_FP64)
+    CK(c->d_inv.ensure((size_t)slots * cls * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
   CK(c->d_oms.ensure((size_t)slots * sizeof(OmegaParams)));
   CK(c->d_slots.ensure((size_t)slots * sizeof(int)));
   if (c->mode == NEMOH_B200_MIXED) CK(c->mixed.ensure(slots * (int)cls, (int)N, std::max(nrhs, 1)));
@@ -199,6 +202,7 @@ GreenCtx green_ctx(nemoh_ctx* c) {
   g.zer = c->zer;
   g.nsymy = c->nsymy;
   g.status = c->d_status.as<int>();
+  g.ro_eps2 = c->ro_eps2;
   return g;
 }
 
@@ -225,6 +229,9 @@ void assemble(nemoh_ctx* c, const std::vector<OmegaParams>& oms) {
     assemble_kernel<true><<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(),
                                                        c->d_slots.as<int>() + infd.size(), c->d_rec.as<PanelRec>(),
                                                        c->d_rows.as<double>(), N, o);
+    LAUNCHED(c);
+    fd_images_kernel<<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(), c->d_slots.as<int>() + infd.size(),
+                                                  c->d_rec.as<PanelRec>(), c->d_rows.as<double>(), N, o);
     LAUNCHED(c);
   }
 }
@@ -256,6 +263,16 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
     }
     LAUNCHED(c);
   }
+  static bool attr2 = false;
+  if (!attr2) {
+    CK(cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            2 * TB * TB * (int)sizeof(double2)));
+    attr2 = true;
+  }
+  const int nblk = (N + TB - 1) / TB;
+  inv_diag_kernel<double2><<<dim3(nblk, 1, nsys), TB, 2 * TB * TB * sizeof(double2), c->stream>>>(
+      b, c->d_inv.as<double2>(), nblk);
+  LAUNCHED(c);
 }
 
 // solve the factored systems for the right-hand sides in X (result in X)
@@ -263,17 +280,25 @@ void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
   Batch b = dbatch(c);
   const int N = c->nfa;
   const long long xs = (long long)N * nrhs;
-  const int nblk = (N + TS_NB - 1) / TS_NB;
+  const int nblk = (N + TB - 1) / TB;
+  const int smem = (TB * TB + 2 * TB * MAX_RHS) * (int)sizeof(double2);
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(trsm_blk_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(trsm_blk_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const double2* inv = c->d_inv.as<double2>();
   for (int blk = 0; blk < nblk; ++blk) {
-    const int below = std::max(0, N - (blk + 1) * TS_NB);
-    trsm_step_kernel<double2, true><<<dim3(std::max(1, (below + 127) / 128), 1, nsys), 128, 0, c->stream>>>(
-        b, c->d_X.as<double2>(), c->d_Y.as<double2>(), xs, nrhs, blk);
+    const int below = std::max(0, N - (blk + 1) * TB);
+    trsm_blk_kernel<double2, true><<<dim3(std::max(1, (below + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, c->stream>>>(
+        b, inv, nblk, c->d_X.as<double2>(), c->d_Y.as<double2>(), xs, nrhs, blk);
     LAUNCHED(c);
   }
   for (int blk = nblk - 1; blk >= 0; --blk) {
-    const int above = blk * TS_NB;
-    trsm_step_kernel<double2, false><<<dim3(std::max(1, (above + 127) / 128), 1, nsys), 128, 0, c->stream>>>(
-        b, c->d_Y.as<double2>(), c->d_X.as<double2>(), xs, nrhs, blk);
+    const int above = blk * TB;
+    trsm_blk_kernel<double2, false><<<dim3(std::max(1, (above + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, c->stream>>>(
+        b, inv, nblk, c->d_Y.as<double2>(), c->d_X.as<double2>(), xs, nrhs, blk);
     LAUNCHED(c);
   }
 }
@@ -297,8 +322,9 @@ void potential(nemoh_ctx* c, int nsys, int nrhs) {
   const int N = c->nfa;
   const long long NN = (long long)N * N, xs = (long long)N * nrhs;
   Batch s{c->d_S.as<double2>(), NN, N, nullptr};
-  matmul_rhs_kernel<<<dim3((N + 127) / 128, 1, nsys), 128, 0, c->stream>>>(s, c->d_X.as<double2>(), xs,
-                                                                          c->d_Y.as<double2>(), xs, nrhs);
+  CK(cudaMemsetAsync(c->d_Y.p, 0, (size_t)nsys * xs * sizeof(double2), c->stream));
+  matvec_acc_kernel<<<dim3((N + 127) / 128, (N + MV_COLS - 1) / MV_COLS, nsys), 128, 0, c->stream>>>(
+      s, c->d_X.as<double2>(), xs, c->d_Y.as<double2>(), xs, nrhs, 1.0);
   LAUNCHED(c);
 }
 
@@ -404,6 +430,12 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
                                                                      dq.as<double>(), dc.as<double>(),
                                                                      c->d_apd.as<double4>());
     LAUNCHED(c);
+    // RO > 1e-4 (VNSFD exponential images) decided on RO^2: the largest
+    // double whose correctly rounded square root is still <= 1e-4
+    double t = 1.E-8;
+    while (std::sqrt(std::nextafter(t, 1.)) <= 1.E-4) t = std::nextafter(t, 1.);
+    while (std::sqrt(t) > 1.E-4) t = std::nextafter(t, 0.);
+    c->ro_eps2 = t;
     StencilThresholds thr;
     stencil_thresholds(&thr);
     CK(c->d_thr.ensure(sizeof thr));

@@ -182,4 +182,108 @@ __global__ void __launch_bounds__(ASM_ROWS) assemble_kernel(GreenCtx g, const Om
   }
 }
 
+// ---------------------------------------------------------------------------
+// Finite depth: the exponential images of VNSFD (COMPUTE_GREEN_FD.f90:635-706),
+//   sum_KE AR(KE) (-A/8pi) sum_4 1/rho  and their gradients,
+// added to D+/-, S+/- after assemble_kernel<true>. The reference adds them to
+// FS1, VSX1, VSY1, VSZ1 of each reflection, and those enter SP1/SM1 and the
+// real parts of D+/- linearly (:830-865), so the sums can be accumulated
+// separately. Image depths are shared by both reflections; RO > EPS is
+// decided exactly on RO^2 against a precomputed threshold.
+// ---------------------------------------------------------------------------
+struct ImgPanel {
+  double xg, yg, zg, aire;
+};
+
+__global__ void __launch_bounds__(ASM_ROWS) fd_images_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
+                                                             const int* __restrict__ slots,
+                                                             const PanelRec* __restrict__ rec,
+                                                             const double* __restrict__ rows, int N, AsmOut out) {
+  __shared__ ImgPanel sp[ASM_TJ];
+  __shared__ double s_ambda[MAX_NEXP + 1], s_ar[MAX_NEXP + 1];
+  const int slot = slots[blockIdx.z];
+  const OmegaParams* om = oms + slot;
+  const int nexp1 = om->nexp + 1;
+  for (int i = threadIdx.x; i <= MAX_NEXP; i += blockDim.x) {
+    s_ambda[i] = om->ambda[i];
+    s_ar[i] = om->ar[i];
+  }
+  const int j0 = blockIdx.y * ASM_TJ;
+  const int nj = min(ASM_TJ, N - j0);
+  for (int i = threadIdx.x; i < nj; i += blockDim.x) {
+    const PanelRec& p = rec[j0 + i];
+    sp[i] = ImgPanel{p.xg, p.yg, p.zg, p.aire};
+  }
+  __syncthreads();
+  const int I = blockIdx.x * ASM_ROWS + threadIdx.x;
+  if (I >= N) return;
+  const double XGI = rows[I], YGI = rows[N + I], ZGI = rows[2 * N + I];
+  const double XNI = rows[3 * N + I], YNI = rows[4 * N + I], ZNI = rows[5 * N + I];
+  if (!(ZGI < g.zer)) return;   // free-surface collocation rows use the panel branch
+  const double ZMIII = ZGI;
+  const double H = om->h, H2 = XMUL(2., H), H4 = XMUL(4., H);
+  const double QPI = 4. * 3.141592653589793;
+  const double T2 = g.ro_eps2;
+  const int NJJ = g.nsymy + 1;
+  const long long NN = (long long)N * N;
+  double2* od = out.d + slot * out.slot_stride;
+  double2* os = out.s + slot * out.slot_stride;
+  for (int jj = 0; jj < nj; ++jj) {
+    const ImgPanel P = sp[jj];
+    if (!(P.zg < g.zer)) continue;
+    double dx[2], dy[2], r2[2], fs[2] = {0., 0.}, vx[2] = {0., 0.}, vy[2] = {0., 0.}, vz[2] = {0., 0.};
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      dx[b] = XSUB(XGI, P.xg);
+      dy[b] = XSUB(YGI, P.yg * (b ? -1. : 1.));
+      const double R = XSQRT(XADD(XMUL(dx[b], dx[b]), XMUL(dy[b], dy[b])));
+      r2[b] = XMUL(R, R);
+    }
+    const double ACT = -0.5 * P.aire / QPI;
+#pragma unroll 1
+    for (int KE = 1; KE <= nexp1; ++KE) {
+      const double AQT = ACT * s_ar[KE];
+      const double HA = XMUL(H, s_ambda[KE]);
+      double zp[4], z2[4];
+      zp[0] = XSUB(XADD(XSUB(ZMIII, H2), HA), P.zg);
+      zp[1] = XSUB(XSUB(-ZMIII, HA), P.zg);
+      zp[2] = XSUB(XADD(XSUB(-ZMIII, H4), HA), P.zg);
+      zp[3] = XSUB(XSUB(XADD(ZMIII, H2), HA), P.zg);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) z2[k] = XMUL(zp[k], zp[k]);
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (b >= NJJ) break;
+        double a[4], sa = 0.;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double RRk = XADD(r2[b], z2[k]);
+          if (RRk > T2) {
+            const double ri = rsqrt(RRk);
+            const double FT = AQT * ri;
+            fs[b] += FT;
+            a[k] = FT * ri * ri;
+          } else {
+            a[k] = 0.;
+          }
+          sa += a[k];
+        }
+        vx[b] -= dx[b] * sa;
+        vy[b] -= dy[b] * sa;
+        vz[b] -= zp[0] * a[0] - zp[1] * a[1] - zp[2] * a[2] + zp[3] * a[3];
+      }
+    }
+    const long long q = I + (long long)N * (j0 + jj);
+    if (NJJ == 2) {
+      od[q].x += (vx[0] + vx[1]) * XNI + (vy[0] + vy[1]) * YNI + (vz[0] + vz[1]) * ZNI;
+      od[NN + q].x += (vx[0] - vx[1]) * XNI + (vy[0] - vy[1]) * YNI + (vz[0] - vz[1]) * ZNI;
+      os[q].x += fs[0] + fs[1];
+      os[NN + q].x += fs[0] - fs[1];
+    } else {
+      od[q].x += vx[0] * XNI + vy[0] * YNI + vz[0] * ZNI;
+      os[q].x += fs[0];
+    }
+  }
+}
+
 }  // namespace nb200

@@ -18,6 +18,7 @@
 namespace nb200 {
 
 struct GreenCtx {
+  double ro_eps2;                   // largest x with sqrt(x) <= 1e-4 (exact RO > EPS test on RO^2)
   const double* xr;                 // XR(1..328) at [1..328]
   const double* xz;                 // XZ(1..46) at [1..46]
   const double4* apd;               // {APD1X, APD1Z, APD2X, APD2Z}(I,J) at (I-1)+328*(J-1)
@@ -608,40 +609,7 @@ __device__ __forceinline__ void wave_fd_jj(const GreenCtx& g, const OmegaParams&
   }
   w.VSZ1 = COF3 * (m1.PD1Z - m2.PD1Z + m3.PD1Z - m4.PD1Z);
   w.VSZ2 = COF4 * (m1.VZ2 - m2.VZ2 + m3.VZ2 - m4.VZ2);
-  // exponential images (:635-706)
-  const double ACT = -0.5 * P.aire / QPI;
-  const double RRR2 = XMUL(RRR, RRR);
-  double fs = 0., vx = 0., vy = 0., vz = 0.;
-#pragma unroll 1
-  for (int KE = 1; KE <= om.nexp + 1; ++KE) {
-    const double AQT = ACT * om.ar[KE];
-    const double HA = XMUL(H, om.ambda[KE]);
-    double zp[4];
-    zp[0] = XSUB(XADD(XSUB(ZMIII, H2), HA), P.zg);
-    zp[1] = XSUB(XSUB(-ZMIII, HA), P.zg);
-    zp[2] = XSUB(XADD(XSUB(-ZMIII, H4), HA), P.zg);
-    zp[3] = XSUB(XSUB(XADD(ZMIII, H2), HA), P.zg);
-    double a[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const double RRk = XADD(RRR2, XMUL(zp[k], zp[k]));
-      const double ROk = XSQRT(RRk);
-      if (ROk > EPS) {
-        const double FT = AQT / ROk;
-        fs += FT;
-        a[k] = FT / RRk;
-      } else {
-        a[k] = 0.;
-      }
-    }
-    vx -= dx * (a[0] + a[1] + a[2] + a[3]);
-    vy -= dy * (a[0] + a[1] + a[2] + a[3]);
-    vz -= zp[0] * a[0] - zp[1] * a[1] - zp[2] * a[2] + zp[3] * a[3];
-  }
-  w.FS1 += fs;
-  w.VSX1 += vx;
-  w.VSY1 += vy;
-  w.VSZ1 += vz;
+  // the exponential images (:635-706) are added by fd_images_kernel
 }
 
 // --- one pair, both symmetry classes --------------------------------------

@@ -211,128 +211,7 @@ __global__ void lu_diag_store_kernel(BatchT<C2> b, int k, int kb) {
   for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) A[(k + q % kb) + (long long)b.n * (k + q / kb)] = D[q];
 }
 
-// ---------------------------------------------------------------------------
-// Multi-RHS triangular solves on the factored systems. X is n x nrhs per
-// system (ld = n) at xbase + s * xstride. One launch per block of TS_NB rows:
-// every CTA solves the diagonal block in shared memory (CTA 0 stores it) and
-// then applies the block to its slice of the remaining rows.
-// ---------------------------------------------------------------------------
-constexpr int TS_NB = 32;
 constexpr int MAX_RHS = 16;
-
-template <class C2, bool LOWER>
-__global__ void __launch_bounds__(128) trsm_step_kernel(BatchT<C2> b, C2* xbase, C2* ybase, long long xstride,
-                                                        int nrhs, int blk) {
-  // X: running right-hand sides (rows outside the block updated in place),
-  // Y: solution (the block's rows written by CTA 0). X and Y never alias, so
-  // every CTA reads the block's right-hand side before anyone changes it.
-  __shared__ C2 T[TS_NB * TS_NB];
-  __shared__ C2 Xs[TS_NB * MAX_RHS];
-  const int n = b.n;
-  const C2* A = b.base + blockIdx.z * b.stride;
-  C2* X = xbase + blockIdx.z * xstride;
-  C2* Y = ybase + blockIdx.z * xstride;
-  const int k = blk * TS_NB;
-  const int nb = min(TS_NB, n - k);
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
-    const int i = q % nb, c = q / nb;
-    T[i + TS_NB * c] = A[(k + i) + (long long)n * (k + c)];
-  }
-  for (int q = threadIdx.x; q < nb * nrhs; q += blockDim.x) {
-    const int i = q % nb, p = q / nb;
-    Xs[i + TS_NB * p] = X[(k + i) + (long long)n * p];
-  }
-  __syncthreads();
-  if (threadIdx.x < nrhs) {
-    C2* x = Xs + TS_NB * threadIdx.x;
-    if (LOWER) {
-      for (int i = 1; i < nb; ++i) {
-        C2 v = x[i];
-        for (int j = 0; j < i; ++j) v = cfms(v, T[i + TS_NB * j], x[j]);
-        x[i] = v;
-      }
-    } else {
-      for (int i = nb - 1; i >= 0; --i) {
-        C2 v = x[i];
-        for (int j = i + 1; j < nb; ++j) v = cfms(v, T[i + TS_NB * j], x[j]);
-        x[i] = cdv(v, T[i + TS_NB * i]);
-      }
-    }
-  }
-  __syncthreads();
-  if (blockIdx.x == 0) {
-    for (int q = threadIdx.x; q < nb * nrhs; q += blockDim.x) {
-      const int i = q % nb, p = q / nb;
-      Y[(k + i) + (long long)n * p] = Xs[i + TS_NB * p];
-    }
-  }
-  // rows to update: below the block (lower) or above it (upper)
-  const int lo = LOWER ? k + nb : 0;
-  const int hi = LOWER ? n : k;
-  const int r = lo + blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= hi) return;
-  C2 acc[MAX_RHS];
-#pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p) acc[p] = mkc<C2>(0., 0.);
-  for (int c = 0; c < nb; ++c) {
-    const C2 a = A[r + (long long)n * (k + c)];
-#pragma unroll
-    for (int p = 0; p < MAX_RHS; ++p)
-      if (p < nrhs) {
-        const C2 xv = Xs[c + TS_NB * p];
-        acc[p].x += a.x * xv.x - a.y * xv.y;
-        acc[p].y += a.x * xv.y + a.y * xv.x;
-      }
-  }
-#pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p)
-    if (p < nrhs) {
-      C2* q = X + r + (long long)n * p;
-      C2 v = *q;
-      v.x -= acc[p].x;
-      v.y -= acc[p].y;
-      *q = v;
-    }
-}
-
-// Y = M X for n x n M (ld n) and n x nrhs X: the boundary potential S*sigma.
-__global__ void __launch_bounds__(128) matmul_rhs_kernel(Batch m, const double2* xbase, long long xstride,
-                                                         double2* ybase, long long ystride, int nrhs) {
-  __shared__ double2 Xs[64 * MAX_RHS];
-  const int n = m.n;
-  const double2* M = m.base + blockIdx.z * m.stride;
-  const double2* X = xbase + blockIdx.z * xstride;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double2 acc[MAX_RHS];
-#pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p) acc[p] = make_double2(0., 0.);
-  for (int c0 = 0; c0 < n; c0 += 64) {
-    const int nc = min(64, n - c0);
-    __syncthreads();
-    for (int q = threadIdx.x; q < nc * nrhs; q += blockDim.x) {
-      const int c = q % nc, p = q / nc;
-      Xs[c + 64 * p] = X[(c0 + c) + (long long)n * p];
-    }
-    __syncthreads();
-    if (r < n) {
-      for (int c = 0; c < nc; ++c) {
-        const double2 a = M[r + (long long)n * (c0 + c)];
-#pragma unroll
-        for (int p = 0; p < MAX_RHS; ++p)
-          if (p < nrhs) {
-            const double2 xv = Xs[c + 64 * p];
-            acc[p].x += a.x * xv.x - a.y * xv.y;
-            acc[p].y += a.x * xv.y + a.y * xv.x;
-          }
-      }
-    }
-  }
-  if (r >= n) return;
-  double2* Y = ybase + blockIdx.z * ystride;
-#pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p)
-    if (p < nrhs) Y[r + (long long)n * p] = acc[p];
-}
 
 // B = (NVEL(I) +- NVEL(I+NFA))/2 per symmetry class (SOLVE_BEM_INFD_DIRECT.f90:123-131)
 // nvel: (2^s n) x nrhs per frequency; X: system (w, class) at (w*cls+class)*n*nrhs
@@ -387,6 +266,170 @@ __global__ void __launch_bounds__(256) force_kernel(const double2* __restrict__ 
     // -(i rho W) * sum(ZP * NDS)
     force[((long long)w * nrhs + p) * nint + i] = make_double2(rw * red[1][0], -rw * red[0][0]);
   }
+}
+
+}  // namespace nb200
+
+namespace nb200 {
+
+// ---------------------------------------------------------------------------
+// Blocked triangular solves with precomputed inverses of the diagonal blocks.
+// After the factorization, inv_diag_kernel stores inv(L_bb) and inv(U_bb) for
+// every TB x TB diagonal block; a solve step is then a small block product
+// x_b = inv(T_bb) r_b plus the update of the remaining rows.
+// ---------------------------------------------------------------------------
+constexpr int TB = 64;
+constexpr int TRSM_ROWS = 32;   // rows updated per CTA of a solve step
+
+template <class C2>
+__device__ __forceinline__ void cmad(C2& acc, C2 a, C2 b) {
+  acc.x += a.x * b.x - a.y * b.y;
+  acc.y += a.x * b.y + a.y * b.x;
+}
+
+// inv layout: ((sys * nblk + blk) * 2 + {0: inv L, 1: inv U}) * TB * TB, column-major
+template <class C2>
+__global__ void __launch_bounds__(TB) inv_diag_kernel(BatchT<C2> b, C2* __restrict__ inv, int nblk) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  C2* T = reinterpret_cast<C2*>(dsm);   // [TB][TB]
+  C2* W = T + TB * TB;                  // work columns [TB][TB]
+  const int n = b.n, blk = blockIdx.x, k = blk * TB, nb = min(TB, n - k);
+  const C2* A = b.base + blockIdx.z * b.stride;
+  for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) {
+    const int i = q % TB, c = q / TB;
+    T[q] = (i < nb && c < nb) ? A[(k + i) + (long long)n * (k + c)] : mkc<C2>(i == c ? 1. : 0., 0.);
+  }
+  __syncthreads();
+  const int c = threadIdx.x;
+  C2* out = inv + ((long long)(blockIdx.z * nblk + blk) * 2) * TB * TB;
+  // inv(L): unit lower, column c
+  C2* y = W + TB * c;
+  for (int i = 0; i < TB; ++i) {
+    C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
+    if (i > c)
+      for (int j = c; j < i; ++j) v = cfms(v, T[i + TB * j], y[j]);
+    else if (i < c)
+      v = mkc<C2>(0., 0.);
+    y[i] = v;
+  }
+  for (int i = 0; i < TB; ++i) out[i + TB * c] = y[i];
+  // inv(U): upper, column c
+  for (int i = TB - 1; i >= 0; --i) {
+    C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
+    if (i <= c) {
+      for (int j = i + 1; j <= c; ++j) v = cfms(v, T[i + TB * j], y[j]);
+      v = cdv(v, T[i + TB * i]);
+    } else {
+      v = mkc<C2>(0., 0.);
+    }
+    y[i] = v;
+  }
+  for (int i = 0; i < TB; ++i) out[TB * TB + i + TB * c] = y[i];
+}
+
+// One block step of the forward (LOWER) or backward solve. X holds the
+// running right-hand sides (rows outside the block updated in place), Y the
+// solution; every CTA forms x_b = inv(T_bb) X_b itself from the untouched X_b,
+// CTA 0 stores it, all CTAs update their rows.
+template <class C2, bool LOWER>
+__global__ void __launch_bounds__(128) trsm_blk_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk,
+                                                       C2* xbase, C2* ybase, long long xstride, int nrhs, int blk) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  C2* Ti = reinterpret_cast<C2*>(dsm);   // [TB][TB]
+  C2* Xb = Ti + TB * TB;                 // [TB][MAX_RHS] right-hand side block
+  C2* Sb = Xb + TB * MAX_RHS;            // [TB][MAX_RHS] solved block
+  const int n = b.n, k = blk * TB, nb = min(TB, n - k);
+  const C2* A = b.base + blockIdx.z * b.stride;
+  C2* X = xbase + blockIdx.z * xstride;
+  C2* Y = ybase + blockIdx.z * xstride;
+  const C2* src = inv + ((long long)(blockIdx.z * nblk + blk) * 2 + (LOWER ? 0 : 1)) * TB * TB;
+  for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) Ti[q] = src[q];
+  for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
+    const int i = q % TB, p = q / TB;
+    Xb[i + TB * p] = (i < nb) ? X[(k + i) + (long long)n * p] : mkc<C2>(0., 0.);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
+    const int i = q % TB, p = q / TB;
+    C2 acc = mkc<C2>(0., 0.);
+    for (int j = 0; j < TB; ++j) cmad(acc, Ti[i + TB * j], Xb[j + TB * p]);
+    Sb[i + TB * p] = acc;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int q = threadIdx.x; q < nb * nrhs; q += blockDim.x) {
+      const int i = q % nb, p = q / nb;
+      Y[(k + i) + (long long)n * p] = Sb[i + TB * p];
+    }
+  // update: 32 rows per CTA, 4 threads per row, 16 block columns each; the
+  // 16 loads of a thread are issued back to back, partials meet by shuffles
+  const int lo = LOWER ? k + nb : 0;
+  const int hi = LOWER ? n : k;
+  const int part = threadIdx.x & 3;
+  const int r = lo + blockIdx.x * TRSM_ROWS + (threadIdx.x >> 2);
+  const bool live = r < hi;
+  C2 a[TB / 4];
+#pragma unroll
+  for (int j = 0; j < TB / 4; ++j) {
+    const int c = part * (TB / 4) + j;
+    a[j] = (live && c < nb) ? A[r + (long long)n * (k + c)] : mkc<C2>(0., 0.);
+  }
+#pragma unroll 1
+  for (int p = 0; p < nrhs; ++p) {
+    C2 acc = mkc<C2>(0., 0.);
+#pragma unroll
+    for (int j = 0; j < TB / 4; ++j) cmad(acc, a[j], Sb[part * (TB / 4) + j + TB * p]);
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
+    if (live && part == 0) {
+      C2* q = X + r + (long long)n * p;
+      C2 v = *q;
+      v.x -= acc.x;
+      v.y -= acc.y;
+      *q = v;
+    }
+  }
+}
+
+// Y += sign * M X (FP64) with the columns split over blockIdx.y; partial sums
+// are added with atomics, so Y must hold its initial value (0 or the RHS).
+constexpr int MV_COLS = 128;
+__global__ void __launch_bounds__(128) matvec_acc_kernel(Batch m, const double2* __restrict__ xbase, long long xstride,
+                                                         double2* ybase, long long ystride, int nrhs, double sign) {
+  __shared__ double2 Xs[MV_COLS * MAX_RHS];
+  const int n = m.n;
+  const double2* M = m.base + blockIdx.z * m.stride;
+  const double2* X = xbase + blockIdx.z * xstride;
+  const int c0 = blockIdx.y * MV_COLS, nc = min(MV_COLS, n - c0);
+  for (int q = threadIdx.x; q < MV_COLS * nrhs; q += blockDim.x) {
+    const int c = q % MV_COLS, p = q / MV_COLS;
+    Xs[c + MV_COLS * p] = (c < nc) ? X[(c0 + c) + (long long)n * p] : make_double2(0., 0.);
+  }
+  __syncthreads();
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double2 acc[MAX_RHS];
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p) acc[p] = make_double2(0., 0.);
+  for (int c8 = 0; c8 < nc; c8 += 8) {
+    double2 a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = (c8 + j < nc) ? M[r + (long long)n * (c0 + c8 + j)] : make_double2(0., 0.);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int p = 0; p < MAX_RHS; ++p)
+        if (p < nrhs) cmad(acc[p], a[j], Xs[c8 + j + MV_COLS * p]);
+  }
+  double2* Y = ybase + blockIdx.z * ystride;
+#pragma unroll
+  for (int p = 0; p < MAX_RHS; ++p)
+    if (p < nrhs) {
+      atomicAdd(&Y[r + (long long)n * p].x, sign * acc[p].x);
+      atomicAdd(&Y[r + (long long)n * p].y, sign * acc[p].y);
+    }
 }
 
 }  // namespace nb200

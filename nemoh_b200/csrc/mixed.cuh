@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "linalg.cuh"
@@ -18,7 +19,7 @@
 namespace nb200 {
 
 constexpr int REFINE_MAX_IT = 30;
-constexpr double REFINE_TOL = 1e-13;
+constexpr double REFINE_TOL = 1e-12;
 
 struct MixedWork {
   float2* lu = nullptr;      // FP32 factors, nsys x n x n
@@ -27,6 +28,7 @@ struct MixedWork {
   double2* r = nullptr;      // residual (FP64)
   float2* rf = nullptr;      // residual/correction (FP32)
   float2* yf = nullptr;      // forward-solve scratch (FP32)
+  float2* inv = nullptr;     // inverses of the diagonal blocks of L and U (FP32)
   unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
   TcWork tc;                 // tensor-core GEMM operand buffers
   int cap_sys = 0, cap_n = 0, cap_rhs = 0;
@@ -36,9 +38,9 @@ struct MixedWork {
 
   size_t bytes() const { return total; }
   void release() {
-    cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms);
+    cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms); cudaFree(inv);
     tc.release();
-    lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr;
+    lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr; inv = nullptr;
     cap_sys = cap_n = cap_rhs = 0;
     total = 0;
   }
@@ -55,16 +57,20 @@ struct MixedWork {
     if ((e = cudaMalloc(&rf, V * sizeof(float2)))) return e;
     if ((e = cudaMalloc(&yf, V * sizeof(float2)))) return e;
     if ((e = cudaMalloc(&norms, (size_t)2 * nsys * nrhs * sizeof(unsigned long long)))) return e;
+    const size_t ninv = (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB;
+    if ((e = cudaMalloc(&inv, ninv * sizeof(float2)))) return e;
     if ((e = tc.ensure(nsys, n))) return e;
     cap_sys = nsys;
     cap_n = n;
     cap_rhs = nrhs;
-    total = nsys * NN * sizeof(float2) + V * (2 * sizeof(double2) + 2 * sizeof(float2)) + tc.bytes();
+    total = nsys * NN * sizeof(float2) + V * (2 * sizeof(double2) + 2 * sizeof(float2)) + tc.bytes() + ninv * sizeof(float2);
     return cudaSuccess;
   }
 };
 
-inline size_t mixed_bytes_per_system(size_t n) { return n * n * sizeof(float2) + tc_bytes_per_system(n); }
+inline size_t mixed_bytes_per_system(size_t n) {
+  return n * n * sizeof(float2) + tc_bytes_per_system(n) + ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2);
+}
 
 __global__ void d2f_kernel(const double2* __restrict__ a, float2* __restrict__ b, long long count) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count; q += (long long)gridDim.x * blockDim.x) {
@@ -98,55 +104,19 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
   if ((threadIdx.x & 31) == 0) atomicMax(out + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
-// r = b - D x in FP64, rf = (float) r, and |r|inf per (system, rhs)
-__global__ void __launch_bounds__(128) residual_kernel(Batch m, const double2* __restrict__ x, const double2* __restrict__ b,
-                                                       double2* __restrict__ r, float2* __restrict__ rf, int nrhs,
-                                                       unsigned long long* __restrict__ rnorm) {
-  __shared__ double2 Xs[64 * MAX_RHS];
-  const int n = m.n;
-  const double2* M = m.base + blockIdx.z * m.stride;
-  const long long vs = (long long)blockIdx.z * n * nrhs;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  double2 acc[MAX_RHS];
-#pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p) acc[p] = make_double2(0., 0.);
-  for (int c0 = 0; c0 < n; c0 += 64) {
-    const int nc = min(64, n - c0);
-    __syncthreads();
-    for (int q = threadIdx.x; q < nc * nrhs; q += blockDim.x) {
-      const int c = q % nc, p = q / nc;
-      Xs[c + 64 * p] = x[vs + (c0 + c) + (long long)n * p];
-    }
-    __syncthreads();
-    if (row < n) {
-      for (int c = 0; c < nc; ++c) {
-        const double2 a = M[row + (long long)n * (c0 + c)];
-#pragma unroll
-        for (int p = 0; p < MAX_RHS; ++p)
-          if (p < nrhs) {
-            const double2 xv = Xs[c + 64 * p];
-            acc[p].x += a.x * xv.x - a.y * xv.y;
-            acc[p].y += a.x * xv.y + a.y * xv.x;
-          }
-      }
-    }
+// rf = (float) r and |r|inf per (system, rhs), r = b - D x formed beforehand
+__global__ void residual_finish_kernel(const double2* __restrict__ r, float2* __restrict__ rf, int n, int nrhs,
+                                       unsigned long long* __restrict__ rnorm) {
+  const int p = blockIdx.y, s = blockIdx.z;
+  const long long base = ((long long)s * nrhs + p) * n;
+  double m = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 v = r[base + i];
+    rf[base + i] = make_float2((float)v.x, (float)v.y);
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
   }
-#pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p) {
-    if (p >= nrhs) break;
-    double mx = 0.;
-    if (row < n) {
-      const long long q = vs + row + (long long)n * p;
-      const double2 bb = b[q];
-      const double2 rr = make_double2(bb.x - acc[p].x, bb.y - acc[p].y);
-      r[q] = rr;
-      rf[q] = make_float2((float)rr.x, (float)rr.y);
-      mx = fmax(fabs(rr.x), fabs(rr.y));
-    }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0)
-      atomicMax(rnorm + (long long)blockIdx.z * nrhs + p, (unsigned long long)__double_as_longlong(mx));
-  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(rnorm + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
 inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches) {
@@ -170,22 +140,38 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
       ++launches;
     }
   }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * TB * TB * (int)sizeof(float2));
+    attr = true;
+  }
+  const int nblk = (n + TB - 1) / TB;
+  inv_diag_kernel<float2><<<dim3(nblk, 1, nsys), TB, 2 * TB * TB * sizeof(float2), st>>>(b, w.inv, nblk);
+  ++launches;
 }
 
 inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches) {
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
   const long long xs = (long long)n * nrhs;
-  const int nblk = (n + TS_NB - 1) / TS_NB;
+  const int nblk = (n + TB - 1) / TB;
+  const int smem = (TB * TB + 2 * TB * MAX_RHS) * (int)sizeof(float2);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(trsm_blk_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(trsm_blk_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
   for (int blk = 0; blk < nblk; ++blk) {
-    const int below = std::max(0, n - (blk + 1) * TS_NB);
-    trsm_step_kernel<float2, true><<<dim3(std::max(1, (below + 127) / 128), 1, nsys), 128, 0, st>>>(b, w.rf, w.yf, xs,
-                                                                                                   nrhs, blk);
+    const int below = std::max(0, n - (blk + 1) * TB);
+    trsm_blk_kernel<float2, true><<<dim3(std::max(1, (below + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, st>>>(
+        b, w.inv, nblk, w.rf, w.yf, xs, nrhs, blk);
     ++launches;
   }
   for (int blk = nblk - 1; blk >= 0; --blk) {
-    const int above = blk * TS_NB;
-    trsm_step_kernel<float2, false><<<dim3(std::max(1, (above + 127) / 128), 1, nsys), 128, 0, st>>>(b, w.yf, w.rf, xs,
-                                                                                                    nrhs, blk);
+    const int above = blk * TB;
+    trsm_blk_kernel<float2, false><<<dim3(std::max(1, (above + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, st>>>(
+        b, w.inv, nblk, w.yf, w.rf, xs, nrhs, blk);
     ++launches;
   }
 }
@@ -209,7 +195,11 @@ inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double
     accumulate_kernel<<<1184, 256, 0, st>>>(X, w.rf, V, it == 0);
     ++launches;
     cudaMemsetAsync(w.norms, 0, (size_t)nv * sizeof(unsigned long long), st);
-    residual_kernel<<<dim3((n + 127) / 128, 1, nsys), 128, 0, st>>>(dm, X, w.b, w.r, w.rf, nrhs, w.norms);
+    cudaMemcpyAsync(w.r, w.b, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+    matvec_acc_kernel<<<dim3((n + 127) / 128, (n + MV_COLS - 1) / MV_COLS, nsys), 128, 0, st>>>(
+        dm, X, (long long)n * nrhs, w.r, (long long)n * nrhs, nrhs, -1.0);
+    ++launches;
+    residual_finish_kernel<<<dim3(8, nrhs, nsys), 256, 0, st>>>(w.r, w.rf, n, nrhs, w.norms);
     ++launches;
     cudaMemcpyAsync(h.data(), w.norms, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);

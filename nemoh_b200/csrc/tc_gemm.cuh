@@ -12,8 +12,8 @@
 // A prep kernel writes A'' and B'' as ready-made shared-memory images
 // (K-major, no swizzle, 8x8 core matrices of 128 bytes), so each CTA moves its
 // operands with two bulk async copies (cp.async.bulk, no tensor map). One CTA
-// computes a 64-complex-row x 256-column tile: one thread issues 12
-// tcgen05.mma (M=128, N=256, K=16, BF16 -> FP32 in TMEM), the accumulator is
+// computes a 64-complex-row x 128-column tile: one thread issues 12
+// tcgen05.mma (M=128, N=128, K=16, BF16 -> FP32 in TMEM), the accumulator is
 // read back with tcgen05.ld, staged in shared memory as complex values and
 // subtracted from A22 with coalesced read-modify-writes.
 // Every wait on an mbarrier is bounded; on timeout the kernel raises a status
@@ -30,17 +30,17 @@
 namespace nb200 {
 
 constexpr int TC_ROWS = 64;                     // complex rows per tile (128 real rows)
-constexpr int TC_COLS = 256;                    // columns per tile (MMA N)
+constexpr int TC_COLS = 128;                    // columns per tile (MMA N); 2 CTAs per SM
 constexpr int TC_K = 192;                       // K'' = 3 * 2 * LU_NB
 constexpr int TC_SBO = (TC_K / 8) * 128;        // bytes between 8-row core-matrix groups
 constexpr int TC_A_BYTES = 128 * TC_K * 2;      // 48 KB
-constexpr int TC_B_BYTES = TC_COLS * TC_K * 2;  // 96 KB
+constexpr int TC_B_BYTES = TC_COLS * TC_K * 2;  // 48 KB
 constexpr int TC_SMEM = TC_A_BYTES + TC_B_BYTES + 64;
 constexpr int ST_TC_TIMEOUT = 30;
 
 struct TcWork {
   unsigned char* a = nullptr;   // A'' tiles, nsys x ceil(n/64) x 48 KB
-  unsigned char* b = nullptr;   // B'' tiles, nsys x ceil(n/256) x 96 KB
+  unsigned char* b = nullptr;   // B'' tiles, nsys x ceil(n/128) x 48 KB
   int cap_sys = 0, cap_n = 0;
   size_t total = 0;
   size_t bytes() const { return total; }
@@ -183,7 +183,7 @@ __host__ __device__ constexpr uint32_t tc_idesc() {
          | ((uint32_t)(128 >> 4) << 24);
 }
 
-__global__ void __launch_bounds__(128, 1) tc_update_kernel(BatchT<float2> b, int k, const unsigned char* __restrict__ abuf,
+__global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int k, const unsigned char* __restrict__ abuf,
                                                            const unsigned char* __restrict__ bbuf, long long a_sys,
                                                            long long b_sys, int* status) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -259,11 +259,13 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(BatchT<float2> b, int
   if (ok) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    // TMEM -> registers -> shared memory as complex [col][row] (reusing the operand area)
-    float2* stage = reinterpret_cast<float2*>(smem);
+    // TMEM -> registers -> shared memory, real and imaginary parts as separate
+    // [col][row] float planes (reusing the operand area; conflict-free stores)
+    float* sre = reinterpret_cast<float*>(smem);
+    float* sim = sre + TC_COLS * TC_ROWS;
     const int trow_l = warp * 32 + (threadIdx.x & 31);  // accumulator row of this thread
-    const bool imag = trow_l >= TC_ROWS;
-    const int crow = imag ? trow_l - TC_ROWS : trow_l;
+    float* plane = trow_l >= TC_ROWS ? sim : sre;
+    const int crow = trow_l & (TC_ROWS - 1);
     __syncthreads();
 #pragma unroll 1
     for (int chunk = 0; chunk < TC_COLS / 32; ++chunk) {
@@ -280,27 +282,53 @@ __global__ void __launch_bounds__(128, 1) tc_update_kernel(BatchT<float2> b, int
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        float* dst = reinterpret_cast<float*>(stage + (chunk * 32 + j) * TC_ROWS + crow) + (imag ? 1 : 0);
-        *dst = __uint_as_float(v[j]);
-      }
+      for (int j = 0; j < 32; ++j) plane[(chunk * 32 + j) * TC_ROWS + crow] = __uint_as_float(v[j]);
     }
     __syncthreads();
-    // coalesced complex read-modify-write of the 64 x 256 tile of A22
+    // read-modify-write of the 64 x 128 tile of A22: warp w takes columns
+    // w, w+4, ...; lane l takes rows 2l, 2l+1 (one 16-byte access when the
+    // order n is even, so that every column starts 16-byte aligned). Sixteen
+    // columns' loads are issued before any is used, to keep memory busy.
     float2* A = b.base + blockIdx.z * b.stride;
-    const int row = threadIdx.x & 63, half = threadIdx.x >> 6;
-    const int gr = trow * TC_ROWS + row;
-    if (gr < rest) {
-#pragma unroll 4
-      for (int c = half; c < TC_COLS; c += 2) {
-        const int gc = tcol * TC_COLS + c;
-        if (gc >= rest) break;
-        float2* p = A + (r0 + gr) + (long long)n * (r0 + gc);
-        const float2 d = stage[c * TC_ROWS + row];
-        float2 o = *p;
-        o.x -= d.x;
-        o.y -= d.y;
-        *p = o;
+    const int lane = threadIdx.x & 31;
+    const int gr = trow * TC_ROWS + 2 * lane;
+    const int ncol = min(TC_COLS, rest - tcol * TC_COLS);
+    const bool pair = (gr + 1 < rest) && ((n & 1) == 0);
+    constexpr int UNR = 16;
+    for (int c0 = warp; c0 < ncol; c0 += 4 * UNR) {
+      float4 cur[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int c = c0 + 4 * u;
+        if (c < ncol && gr < rest) {
+          float2* p = A + (r0 + gr) + (long long)n * (r0 + tcol * TC_COLS + c);
+          if (pair) cur[u] = *reinterpret_cast<const float4*>(p);
+          else cur[u] = make_float4(p[0].x, p[0].y, 0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int c = c0 + 4 * u;
+        if (c < ncol && gr < rest) {
+          float2* p = A + (r0 + gr) + (long long)n * (r0 + tcol * TC_COLS + c);
+          const int q = c * TC_ROWS + 2 * lane;
+          float4 o = cur[u];
+          o.x -= sre[q];
+          o.y -= sim[q];
+          if (pair) {
+            o.z -= sre[q + 1];
+            o.w -= sim[q + 1];
+            *reinterpret_cast<float4*>(p) = o;
+          } else {
+            p[0] = make_float2(o.x, o.y);
+            if (gr + 1 < rest) {
+              float2 t = p[1];
+              t.x -= sre[q + 1];
+              t.y -= sim[q + 1];
+              p[1] = t;
+            }
+          }
+        }
       }
     }
   }
