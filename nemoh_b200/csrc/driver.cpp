@@ -1,0 +1,199 @@
+// nemoh_solver_b200: drop-in for the reference Solver executable
+// (Solver/NEMOH.f90:30-176). Reads the case named by ID.dat exactly as the
+// reference does -- ID.dat (Common/Identification.f90:30-37), mesh/L10.dat and
+// mesh/L12.dat (Common/Mesh.f90:81-132), Normalvelocities.dat
+// (Solver/Core/Bodyconditions.f90:65-89), Nemoh.cal lines 2-5 and input.txt
+// (Solver/Core/INITIALIZATION.f90:44-53), mesh/Integration.dat, mesh/Kochin.dat,
+// mesh/Freesurface.dat (NEMOH.f90:88-118) -- solves every problem on the GPU
+// through the C-ABI and writes results/Forces.dat in the reference's layout
+// (NEMOH.f90:152-166).
+//
+// Problems are solved a frequency at a time: consecutive problems that share
+// a frequency go to one nemoh_b200_solve_frequencies call (one assembly and
+// one factorization for all of them, as the reference's w_previous cache).
+// Kochin, free-surface and pressure outputs are not produced.
+//
+// usage: nemoh_solver_b200 [case-root] [--mixed] [--device N]
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nemoh_b200.h"
+
+namespace {
+
+struct IoError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+// Fortran list-directed READ: every READ starts a new record; values may span lines
+class Records {
+ public:
+  explicit Records(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) throw IoError("cannot open " + path);
+    std::string s;
+    while (std::getline(f, s)) lines_.push_back(s);
+  }
+  void skip() { ++pos_; }
+  std::vector<std::string> read(size_t n) {
+    std::vector<std::string> v;
+    while (v.size() < n) {
+      if (pos_ >= lines_.size()) throw IoError("unexpected end of file");
+      std::string s = lines_[pos_++];
+      const size_t bang = s.find('!');
+      if (bang != std::string::npos) s.resize(bang);
+      for (char& ch : s)
+        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      std::istringstream is(s);
+      std::string t;
+      while (is >> t) v.push_back(t);
+    }
+    v.resize(n);
+    return v;
+  }
+  double real() { return std::stod(read(1)[0]); }
+  int integer() { return std::stoi(read(1)[0]); }
+
+ private:
+  std::vector<std::string> lines_;
+  size_t pos_ = 0;
+};
+
+void check(nemoh_ctx* ctx, int st, const char* what) {
+  if (st) {
+    std::fprintf(stderr, "nemoh_solver_b200: %s failed (status %d): %s\n", what, st,
+                 ctx ? nemoh_b200_last_error(ctx) : "");
+    std::exit(st);
+  }
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  std::string root;
+  int mode = NEMOH_B200_FP64, device = 0;
+  for (int a = 1; a < argc; ++a) {
+    if (!std::strcmp(argv[a], "--mixed")) mode = NEMOH_B200_MIXED;
+    else if (!std::strcmp(argv[a], "--device") && a + 1 < argc) device = std::atoi(argv[++a]);
+    else root = argv[a];
+  }
+  const std::string pre = root.empty() ? "" : root + "/";
+  try {
+    Records idr(pre + "ID.dat");
+    const int lid = idr.integer();
+    const std::string dir = pre + idr.read(1)[0].substr(0, lid);
+    Records l10(dir + "/mesh/L10.dat");
+    l10.skip();
+    const auto h = l10.read(4);
+    const int np = std::stoi(h[1]), nfa = std::stoi(h[2]);
+    Records l12(dir + "/mesh/L12.dat");
+    const auto h2 = l12.read(2);
+    if (std::stoi(h2[0]) != 2) throw IoError("The mesh file format is not correct.");
+    const int isym = std::stoi(h2[1]) == 1 ? 1 : 0;
+    std::vector<double> xyz(3 * (size_t)np);
+    for (int i = 0; i < np; ++i) {
+      const auto v = l12.read(4);
+      for (int k = 0; k < 3; ++k) xyz[3 * i + k] = std::stod(v[1 + k]);
+    }
+    l12.skip();
+    std::vector<int> m(4 * (size_t)nfa);
+    for (int i = 0; i < nfa; ++i) {
+      const auto v = l12.read(4);
+      for (int k = 0; k < 4; ++k) m[4 * i + k] = std::stoi(v[k]);
+    }
+    const int nc = nfa * (isym ? 2 : 1);
+    Records bc(dir + "/Normalvelocities.dat");
+    const int npb = bc.integer();
+    std::vector<double> omega(npb), stype(npb);
+    auto vo = bc.read(npb);
+    for (int j = 0; j < npb; ++j) omega[j] = std::stod(vo[j]);
+    auto vt = bc.read(npb);
+    for (int j = 0; j < npb; ++j) stype[j] = std::stod(vt[j]);
+    bool extra_outputs = false;
+    for (int k = 0; k < 3; ++k) {
+      for (const auto& t : bc.read(npb)) extra_outputs |= std::stoi(t) != 0;
+    }
+    std::vector<std::complex<double>> nvel((size_t)nc * npb);
+    for (int c = 0; c < nc; ++c) {
+      const auto v = bc.read(2 * (size_t)npb);
+      for (int j = 0; j < npb; ++j) nvel[c + (size_t)nc * j] = {std::stod(v[2 * j]), std::stod(v[2 * j + 1])};
+    }
+    Records cal(dir + "/Nemoh.cal");
+    cal.skip();
+    const double rho = cal.real(), g = cal.real(), depth = cal.real();
+    {
+      Records inp(dir + "/input.txt");
+      inp.skip();
+    }
+    Records ig(dir + "/mesh/Integration.dat");
+    const int nint = ig.integer();
+    std::vector<double> nds((size_t)nint * nc);   // column-major nint x nc
+    for (int i = 0; i < nint; ++i) {
+      const auto v = ig.read(nc);
+      for (int c = 0; c < nc; ++c) nds[i + (size_t)nint * c] = std::stod(v[c]);
+    }
+    {
+      Records kr(dir + "/mesh/Kochin.dat");
+      extra_outputs |= kr.integer() > 0;
+    }
+    {
+      Records fr(dir + "/mesh/Freesurface.dat");
+      extra_outputs |= std::stoi(fr.read(2)[0]) > 0;
+    }
+    if (extra_outputs)
+      std::fprintf(stderr, "nemoh_solver_b200: Kochin / free-surface / pressure outputs are not produced\n");
+
+    nemoh_ctx* ctx = nullptr;
+    check(nullptr, nemoh_b200_create(&ctx, device, mode), "create");
+    check(ctx, nemoh_b200_set_mesh(ctx, np, nfa, isym, xyz.data(), m.data(), rho, g, depth), "set_mesh");
+
+    std::vector<std::complex<double>> force((size_t)nint * npb);
+    int j = 0;
+    while (j < npb) {
+      int e = j;
+      while (e < npb && omega[e] == omega[j] && e - j < 16) ++e;
+      const int nrhs = e - j;
+      std::vector<std::complex<double>> f((size_t)nint * nrhs);
+      check(ctx,
+            nemoh_b200_solve_frequencies(ctx, 1, &omega[j], nrhs, reinterpret_cast<const double*>(&nvel[(size_t)nc * j]),
+                                         nint, nds.data(), reinterpret_cast<double*>(f.data())),
+            "solve_frequencies");
+      for (int p = 0; p < nrhs; ++p)
+        for (int i = 0; i < nint; ++i) force[i + (size_t)nint * (j + p)] = f[i + (size_t)nint * p];
+      j = e;
+    }
+    nemoh_b200_destroy(ctx);
+
+    std::ofstream out(dir + "/results/Forces.dat");
+    if (!out) throw IoError("cannot write " + dir + "/results/Forces.dat");
+    char buf[80];
+    for (int c = 0; c < nint; ++c) {
+      for (int q = 0; q < npb; ++q) {
+        const std::complex<double> F = force[c + (size_t)nint * q];
+        double a, b;
+        if (stype[q] != -1.) {
+          a = std::abs(F);
+          b = std::atan2(F.imag(), F.real());
+        } else {
+          a = F.imag() / omega[q];
+          b = -F.real();
+        }
+        std::snprintf(buf, sizeof buf, " %.17E %.17E", a, b);
+        out << buf;
+      }
+      out << "\n";
+    }
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "nemoh_solver_b200: %s\n", e.what());
+    return NEMOH_B200_EIO;
+  }
+  return 0;
+}

@@ -1,0 +1,48 @@
+"""GPU: the serving layer (results alone == in the mix) and the drop-in driver."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gpu_cases as G
+import nemoh_b200 as nb
+from nemoh_b200 import build as B
+from nemoh_b200 import cases as C
+from nemoh_b200 import serving as S
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("precision", [nb.FP64, nb.MIXED])
+def test_serving_result_same_alone_and_in_the_mix(precision):
+    B.build()
+    bodies = S.make_bodies(4, seed=11, n_min=150, n_max=400)
+    srv = S.SolveServer(bodies, precision=precision, workers=2)
+    try:
+        reqs = S.make_requests(48, rate=0, n_bodies=4, seed=12)
+        done, wall = srv.run(reqs, realtime=False)
+        assert sorted(r.rid for r in done) == list(range(48))
+        assert max(b[2] for b in srv.batches) > 1
+        by = {r.rid: r for r in done}
+        for rid in (0, 17, 33):
+            r0 = reqs[rid]
+            alone, _ = srv.run([S.Request(1000 + rid, r0.body, r0.omega, r0.beta_deg)], realtime=False)
+            a, m = alone[0].force, by[rid].force
+            tol = 1e-9 if precision == nb.FP64 else 1e-6
+            assert np.abs(a - m).max() <= tol * np.abs(a).max()
+    finally:
+        srv.close()
+
+
+def test_dropin_driver_matches_oracle(tmp_path):
+    B.build()
+    case = G.small_cases()[1]   # symmetric barge, finite depth
+    ref = G.oracle_forces(case, str(tmp_path / "ref"))
+    C.write_case(case, str(tmp_path / "gpu"))
+    exe = os.path.join(ROOT, "nemoh_b200", "_build", "nemoh_solver_b200")
+    subprocess.run([exe, str(tmp_path / "gpu")], check=True)
+    F = np.loadtxt(str(tmp_path / "gpu" / "case" / "results" / "Forces.dat"), ndmin=2)
+    got = G.decode_forces(case, F)
+    assert G.rel_err(got, ref) < 1e-9

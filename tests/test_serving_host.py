@@ -1,0 +1,67 @@
+"""Scheduling logic of the serving layer, with a fake solver (no GPU)."""
+import threading
+import time
+
+import numpy as np
+
+from nemoh_b200 import cases as C
+from nemoh_b200 import serving as S
+
+
+class FakeSolver:
+    """Returns force = sum of the RHS columns scaled by omega; records batches."""
+    calls = []
+    lock = threading.Lock()
+
+    def __init__(self):
+        self.mesh = None
+
+    def set_case(self, case):
+        self.mesh = case.mesh
+
+    def solve_frequencies(self, omegas, nvel, nds):
+        time.sleep(0.002)
+        with FakeSolver.lock:
+            FakeSolver.calls.append(len(omegas))
+        f = np.einsum("cpw,ic->ipw", nvel, nds) * omegas[None, None, :]
+        return f
+
+    def close(self):
+        pass
+
+
+def _bodies():
+    return [S.Body(C.cylinder_mesh(3.0, 4.0, 8, 3, 2, 4), 0.0), S.Body(C.box_mesh(10, 6, 3, 4, 3, 2), 30.0)]
+
+
+def test_every_request_served_once_and_batched():
+    FakeSolver.calls = []
+    bodies = _bodies()
+    srv = S.SolveServer(bodies, workers=2, solver_factory=FakeSolver, memory_bytes=1 << 30)
+    reqs = S.make_requests(60, rate=0, n_bodies=2, seed=1)
+    done, wall = srv.run(reqs, realtime=False)
+    assert sorted(r.rid for r in done) == list(range(60))
+    assert max(FakeSolver.calls) > 1          # requests were batched
+    for r in done:
+        assert r.done >= r.start >= r.arrival
+
+
+def test_result_same_alone_and_in_the_mix():
+    bodies = _bodies()
+    srv = S.SolveServer(bodies, workers=2, solver_factory=FakeSolver, memory_bytes=1 << 30)
+    reqs = S.make_requests(40, rate=0, n_bodies=2, seed=2)
+    done, _ = srv.run(reqs, realtime=False)
+    alone, _ = srv.run([S.Request(99, reqs[7].body, reqs[7].omega, reqs[7].beta_deg)], realtime=False)
+    mixed = {r.rid: r for r in done}[7]
+    assert np.allclose(alone[0].force, mixed.force, rtol=1e-12, atol=0)
+
+
+def test_admission_limits_batch_by_memory():
+    FakeSolver.calls = []
+    bodies = _bodies()
+    budget = bodies[0].bytes_per_frequency() * 3 * 2 / 0.6   # 3 frequencies per worker
+    srv = S.SolveServer(bodies[:1], workers=2, solver_factory=FakeSolver, memory_bytes=budget)
+    assert srv.admission(bodies[0]) == 3
+    reqs = [S.Request(i, 0, 0.5 + 0.01 * i, 0.0) for i in range(20)]
+    done, _ = srv.run(reqs, realtime=False)
+    assert len(done) == 20 and max(FakeSolver.calls) <= 3
