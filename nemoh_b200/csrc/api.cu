@@ -253,8 +253,12 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
   for (int k = 0; k < N; k += LU_NB) {
     const int nb = std::min(LU_NB, N - k), rest = N - k - nb;
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-    lu_panel_kernel<double2><<<dim3(1 + nrb + ncb, 1, nsys), LU_RB, 0, c->stream>>>(b, k, c->d_status.as<int>());
+    lu_diag_kernel<double2><<<dim3(1, 1, nsys), 256, 0, c->stream>>>(b, k, c->d_status.as<int>());
     LAUNCHED(c);
+    if (nrb + ncb > 0) {
+      lu_panel_kernel<double2><<<dim3(nrb + ncb, 1, nsys), LU_RB, 0, c->stream>>>(b, k);
+      LAUNCHED(c);
+    }
     if (rest > 0) {
       const int t = (rest + GM_T - 1) / GM_T;
       zgemm_update_kernel<double2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(double2), c->stream>>>(b, k, nb);
@@ -277,30 +281,9 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
 
 // solve the factored systems for the right-hand sides in X (result in X)
 void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
-  Batch b = dbatch(c);
-  const int N = c->nfa;
-  const long long xs = (long long)N * nrhs;
-  const int nblk = (N + TB - 1) / TB;
-  const int smem = (TB * TB + 2 * TB * MAX_RHS) * (int)sizeof(double2);
-  static bool attr = false;
-  if (!attr) {
-    CK(cudaFuncSetAttribute(trsm_blk_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(trsm_blk_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
-  }
-  const double2* inv = c->d_inv.as<double2>();
-  for (int blk = 0; blk < nblk; ++blk) {
-    const int below = std::max(0, N - (blk + 1) * TB);
-    trsm_blk_kernel<double2, true><<<dim3(std::max(1, (below + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, c->stream>>>(
-        b, inv, nblk, c->d_X.as<double2>(), c->d_Y.as<double2>(), xs, nrhs, blk);
-    LAUNCHED(c);
-  }
-  for (int blk = nblk - 1; blk >= 0; --blk) {
-    const int above = blk * TB;
-    trsm_blk_kernel<double2, false><<<dim3(std::max(1, (above + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, c->stream>>>(
-        b, inv, nblk, c->d_Y.as<double2>(), c->d_X.as<double2>(), xs, nrhs, blk);
-    LAUNCHED(c);
-  }
+  trsm_launch<double2>(dbatch(c), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys, nrhs,
+                       c->stream, c->launches);
+  CK(cudaGetLastError());
 }
 
 void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs) {

@@ -74,31 +74,42 @@ __device__ void factor_block(C2* s, int nb, int* status, bool report) {
   }
 }
 
+// Factor the diagonal block A11 of step k once per system (grid.z = system)
+// into the per-system scratch b.diag; the update kernel of the step stores it
+// back into A (the panel kernel of the same step still reads A11 from there).
 template <class C2>
-__global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k, int* status) {
+__global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
   __shared__ C2 diag[LU_NB * LU_NB];
-  __shared__ C2 work[LU_NB * LU_CB];
   const int n = b.n;
   const int nb = min(LU_NB, n - k);
-  C2* A = b.base + blockIdx.z * b.stride;
+  const C2* A = b.base + blockIdx.z * b.stride;
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
     const int i = q % nb, c = q / nb;
     diag[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
   }
   __syncthreads();
+  factor_block(diag, nb, status, true);
+  C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
+  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
+}
+
+// L21 <- A21 U11^-1 (CTAs [0, nrb)) and U12 <- L11^-1 A12 (CTAs [nrb, nrb+ncb))
+// with the factored A11 taken from the scratch written by lu_diag_kernel.
+template <class C2>
+__global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
+  __shared__ C2 diag[LU_NB * LU_NB];
+  __shared__ C2 work[LU_NB * LU_CB];
+  const int n = b.n;
+  const int nb = min(LU_NB, n - k);
+  C2* A = b.base + blockIdx.z * b.stride;
+  const C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
+  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) diag[q] = D[q];
+  __syncthreads();
   const int rest = n - k - nb;
   const int nrb = (rest + LU_RB - 1) / LU_RB;
-  factor_block(diag, nb, status, blockIdx.x == 0);
-  if (blockIdx.x == 0) {
-    // the other CTAs of this launch still read A11 from A: park the factored
-    // block in scratch; the next launch of this step stores it (diag_store)
-    C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
-    for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
-    return;
-  }
-  if (blockIdx.x <= nrb) {
+  if (blockIdx.x < nrb) {
     // L21 rows: x U11 = a, one thread per row
-    const int r = k + nb + (blockIdx.x - 1) * LU_RB + threadIdx.x;
+    const int r = k + nb + blockIdx.x * LU_RB + threadIdx.x;
     if (r >= n) return;
     C2 x[LU_NB];
 #pragma unroll
@@ -118,7 +129,7 @@ __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k, in
     return;
   }
   // U12 columns: L11 y = a (unit lower), one thread per column
-  const int c0 = k + nb + (blockIdx.x - 1 - nrb) * LU_CB;
+  const int c0 = k + nb + (blockIdx.x - nrb) * LU_CB;
   const int ncol = min(LU_CB, n - c0);
   for (int q = threadIdx.x; q < nb * ncol; q += blockDim.x) {
     const int i = q % nb, c = q / nb;
@@ -327,69 +338,118 @@ __global__ void __launch_bounds__(TB) inv_diag_kernel(BatchT<C2> b, C2* __restri
   for (int i = 0; i < TB; ++i) out[TB * TB + i + TB * c] = y[i];
 }
 
-// One block step of the forward (LOWER) or backward solve. X holds the
-// running right-hand sides (rows outside the block updated in place), Y the
-// solution; every CTA forms x_b = inv(T_bb) X_b itself from the untouched X_b,
-// CTA 0 stores it, all CTAs update their rows.
+// Triangular solves, one launch per diagonal block. X holds the running
+// right-hand sides, Y receives the solution. A launch for block b applies the
+// solved block (already in Y) to the rows still to come, 64 rows per CTA;
+// the CTA holding block b+1 (forward) or b-1 (backward) then solves it with
+// the inverted diagonal block and stores it in Y for the next launch.
+// With apply = false the launch only solves block b (the first step).
 template <class C2, bool LOWER>
-__global__ void __launch_bounds__(128) trsm_blk_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk,
-                                                       C2* xbase, C2* ybase, long long xstride, int nrhs, int blk) {
+__global__ void __launch_bounds__(128) trsm_fused_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk, C2* xbase,
+                                                         C2* ybase, long long xstride, int nrhs, int blk, int apply) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  C2* Ti = reinterpret_cast<C2*>(dsm);   // [TB][TB]
-  C2* Xb = Ti + TB * TB;                 // [TB][MAX_RHS] right-hand side block
-  C2* Sb = Xb + TB * MAX_RHS;            // [TB][MAX_RHS] solved block
-  const int n = b.n, k = blk * TB, nb = min(TB, n - k);
+  C2* Sb = reinterpret_cast<C2*>(dsm);   // [TB][MAX_RHS] solved block blk
+  C2* Xn = Sb + TB * MAX_RHS;            // [TB][MAX_RHS] next block, updated
+  C2* Ti = Xn + TB * MAX_RHS;            // [TB][TB] inverse of the next diagonal block
+  const int n = b.n;
   const C2* A = b.base + blockIdx.z * b.stride;
   C2* X = xbase + blockIdx.z * xstride;
   C2* Y = ybase + blockIdx.z * xstride;
-  const C2* src = inv + ((long long)(blockIdx.z * nblk + blk) * 2 + (LOWER ? 0 : 1)) * TB * TB;
+  int nxt = blk;            // block solved by CTA 0 at the end
+  if (apply) {
+    const int k = blk * TB, nb = min(TB, n - k);
+    for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
+      const int i = q % TB, p = q / TB;
+      Sb[i + TB * p] = (i < nb) ? Y[(k + i) + (long long)n * p] : mkc<C2>(0., 0.);
+    }
+    __syncthreads();
+    // rows of this CTA: forward [k+nb+64c, ...), backward [k-64(c+1), k-64c)
+    const int r0 = LOWER ? k + nb + (int)blockIdx.x * TB : k - ((int)blockIdx.x + 1) * TB;
+    const int row = threadIdx.x & (TB - 1), part = threadIdx.x >> 6;   // two halves of the 64 columns
+    const int r = r0 + row;
+    const bool live = LOWER ? (r < n) : (r >= 0);
+    C2 a[TB / 2];
+#pragma unroll
+    for (int j = 0; j < TB / 2; ++j) {
+      const int c = part * (TB / 2) + j;
+      a[j] = (live && c < nb) ? A[r + (long long)n * (k + c)] : mkc<C2>(0., 0.);
+    }
+    // partials of the second half go through shared memory (reuse Ti)
+    for (int p = 0; p < nrhs; ++p) {
+      C2 acc = mkc<C2>(0., 0.);
+#pragma unroll
+      for (int j = 0; j < TB / 2; ++j) cmad(acc, a[j], Sb[part * (TB / 2) + j + TB * p]);
+      if (part == 1) Ti[row + TB * p] = acc;
+      __syncthreads();
+      if (part == 0 && live) {
+        const C2 o = Ti[row + TB * p];
+        C2* q = X + r + (long long)n * p;
+        C2 v = *q;
+        v.x -= acc.x + o.x;
+        v.y -= acc.y + o.y;
+        *q = v;
+        if (blockIdx.x == 0) Xn[row + TB * p] = v;
+      }
+      __syncthreads();
+    }
+    if (blockIdx.x != 0) return;
+    nxt = LOWER ? blk + 1 : blk - 1;
+    if (nxt < 0 || nxt >= nblk) return;
+  } else {
+    if (blockIdx.x != 0) return;
+    const int k = nxt * TB, nb = min(TB, n - k);
+    for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
+      const int i = q % TB, p = q / TB;
+      Xn[i + TB * p] = (i < nb) ? X[(k + i) + (long long)n * p] : mkc<C2>(0., 0.);
+    }
+  }
+  // CTA 0: solve block nxt from Xn (rows beyond n are zero)
+  const int kn = nxt * TB, nbn = min(TB, n - kn);
+  const C2* src = inv + ((long long)(blockIdx.z * nblk + nxt) * 2 + (LOWER ? 0 : 1)) * TB * TB;
   for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) Ti[q] = src[q];
-  for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
-    const int i = q % TB, p = q / TB;
-    Xb[i + TB * p] = (i < nb) ? X[(k + i) + (long long)n * p] : mkc<C2>(0., 0.);
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
-    const int i = q % TB, p = q / TB;
-    C2 acc = mkc<C2>(0., 0.);
-    for (int j = 0; j < TB; ++j) cmad(acc, Ti[i + TB * j], Xb[j + TB * p]);
-    Sb[i + TB * p] = acc;
-  }
-  __syncthreads();
-  if (blockIdx.x == 0)
-    for (int q = threadIdx.x; q < nb * nrhs; q += blockDim.x) {
-      const int i = q % nb, p = q / nb;
-      Y[(k + i) + (long long)n * p] = Sb[i + TB * p];
+  if (apply)
+    for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
+      const int i = q % TB, p = q / TB;
+      if (i >= nbn) Xn[i + TB * p] = mkc<C2>(0., 0.);
     }
-  // update: 32 rows per CTA, 4 threads per row, 16 block columns each; the
-  // 16 loads of a thread are issued back to back, partials meet by shuffles
-  const int lo = LOWER ? k + nb : 0;
-  const int hi = LOWER ? n : k;
-  const int part = threadIdx.x & 3;
-  const int r = lo + blockIdx.x * TRSM_ROWS + (threadIdx.x >> 2);
-  const bool live = r < hi;
-  C2 a[TB / 4];
-#pragma unroll
-  for (int j = 0; j < TB / 4; ++j) {
-    const int c = part * (TB / 4) + j;
-    a[j] = (live && c < nb) ? A[r + (long long)n * (k + c)] : mkc<C2>(0., 0.);
-  }
-#pragma unroll 1
-  for (int p = 0; p < nrhs; ++p) {
+  __syncthreads();
+  for (int q = threadIdx.x; q < nbn * nrhs; q += blockDim.x) {
+    const int i = q % nbn, p = q / nbn;
     C2 acc = mkc<C2>(0., 0.);
-#pragma unroll
-    for (int j = 0; j < TB / 4; ++j) cmad(acc, a[j], Sb[part * (TB / 4) + j + TB * p]);
-    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
-    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
-    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
-    if (live && part == 0) {
-      C2* q = X + r + (long long)n * p;
-      C2 v = *q;
-      v.x -= acc.x;
-      v.y -= acc.y;
-      *q = v;
-    }
+    for (int j = 0; j < TB; ++j) cmad(acc, Ti[i + TB * j], Xn[j + TB * p]);
+    Y[(kn + i) + (long long)n * p] = acc;
+  }
+}
+
+// Forward then backward solve of the factored systems: X holds the right-hand
+// sides and receives the solution, Y is scratch of the same size.
+template <class C2>
+void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st, long long& launches) {
+  const int N = b.n;
+  const long long xs = (long long)N * nrhs;
+  const int nblk = (N + TB - 1) / TB;
+  const int smem = (2 * TB * MAX_RHS + TB * TB) * (int)sizeof(C2);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(trsm_fused_kernel<C2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(trsm_fused_kernel<C2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr = true;
+  }
+  // forward: X -> Y
+  trsm_fused_kernel<C2, true><<<dim3(1, 1, nsys), 128, smem, st>>>(b, inv, nblk, X, Y, xs, nrhs, 0, 0);
+  ++launches;
+  for (int blk = 0; blk + 1 < nblk; ++blk) {
+    const int below = N - std::min(N, (blk + 1) * TB);
+    trsm_fused_kernel<C2, true><<<dim3(std::max(1, (below + TB - 1) / TB), 1, nsys), 128, smem, st>>>(
+        b, inv, nblk, X, Y, xs, nrhs, blk, 1);
+    ++launches;
+  }
+  // backward: Y -> X
+  trsm_fused_kernel<C2, false><<<dim3(1, 1, nsys), 128, smem, st>>>(b, inv, nblk, Y, X, xs, nrhs, nblk - 1, 0);
+  ++launches;
+  for (int blk = nblk - 1; blk >= 1; --blk) {
+    trsm_fused_kernel<C2, false><<<dim3(blk, 1, nsys), 128, smem, st>>>(b, inv, nblk, Y, X, xs, nrhs, blk, 1);
+    ++launches;
   }
 }
 

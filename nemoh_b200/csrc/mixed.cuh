@@ -127,8 +127,12 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   for (int k = 0; k < n; k += LU_NB) {
     const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-    lu_panel_kernel<float2><<<dim3(1 + nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k, status);
+    lu_diag_kernel<float2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
     ++launches;
+    if (nrb + ncb > 0) {
+      lu_panel_kernel<float2><<<dim3(nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k);
+      ++launches;
+    }
     if (rest > 0) {
       if (!tc_update(w.tc, b, k, nb, nsys, st, launches, status)) {
         const int t = (rest + GM_T - 1) / GM_T;
@@ -153,27 +157,8 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
 
 inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches) {
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
-  const long long xs = (long long)n * nrhs;
-  const int nblk = (n + TB - 1) / TB;
-  const int smem = (TB * TB + 2 * TB * MAX_RHS) * (int)sizeof(float2);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(trsm_blk_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(trsm_blk_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
-  for (int blk = 0; blk < nblk; ++blk) {
-    const int below = std::max(0, n - (blk + 1) * TB);
-    trsm_blk_kernel<float2, true><<<dim3(std::max(1, (below + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, st>>>(
-        b, w.inv, nblk, w.rf, w.yf, xs, nrhs, blk);
-    ++launches;
-  }
-  for (int blk = nblk - 1; blk >= 0; --blk) {
-    const int above = blk * TB;
-    trsm_blk_kernel<float2, false><<<dim3(std::max(1, (above + TRSM_ROWS - 1) / TRSM_ROWS), 1, nsys), 128, smem, st>>>(
-        b, w.inv, nblk, w.yf, w.rf, xs, nrhs, blk);
-    ++launches;
-  }
+  trsm_launch<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches);
+  // the solution is left in w.rf (forward into yf, backward back into rf)
 }
 
 // X: right-hand sides in, solution out (FP64); Y unused scratch

@@ -136,8 +136,10 @@ def test_repeated_frequency_reuses_factorization(solver):
     solver.solve_potential(T, nv[:, 1])
     n2 = solver.launches
     # the second call launches no assembly and no factorization: one assembly
-    # launch, 2*ceil(N/32) LU launches and one diagonal-block inversion fewer
-    n_lu = 2 * ((case.mesh.npanels + 31) // 32)
+    # launch, the LU launches (diagonal block, panel and update per 32-column
+    # step; no panel on the last step) and one diagonal-block inversion fewer
+    steps = (case.mesh.npanels + 31) // 32
+    n_lu = 3 * steps - 1
     assert (n1 - n0) - (n2 - n1) == 2 + n_lu
 
 
