@@ -86,6 +86,27 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* ctx, int nomega, const double
                                         const double* nvel_device, int nint, const double* nds_device,
                                         double* force_device, void* stream);
 
+/* No counterpart in the reference: an entry point that allocates nothing, for
+ * hosts whose device memory is held by their own allocator (a PyTorch caching
+ * allocator, a batching server that admits work by free HBM) and for hosts
+ * whose other streams must not be stalled by cudaFree's device-wide sync.
+ * Factors in place (FP64 LU without pivoting, as the context path) and solves
+ * nsys dense complex systems resident on `device`:
+ *   a_device: nsys x (n x n) complex, column-major, overwritten by L\U;
+ *   x_device: nsys x nrhs x n complex, right-hand sides in, solutions out;
+ *   1 <= nrhs <= 16; both pointers 16-byte aligned; stream = cudaStream_t.
+ * Scratch comes from one static device array of NEMOH_B200_NOALLOC_SCRATCH_BYTES
+ * (16 MiB) per device: a call needing more (about
+ * nsys*(16 KiB + ceil(n/64)*128 KiB + 16*n*nrhs) bytes) returns
+ * NEMOH_B200_ECAPACITY. The first call on a device does a one-time set-up
+ * (symbol lookup, kernel attributes) and should come before any stream
+ * capture. All calls on a device share the scratch, so calls that overlap on
+ * the GPU race. The call returns after its work on `stream` has finished;
+ * msg (may be NULL) receives the error text. */
+#define NEMOH_B200_NOALLOC_SCRATCH_BYTES (16u << 20)
+int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsys, double* a_device, int nrhs, double* x_device,
+                                           void* stream, char* msg, int msg_len);
+
 /* Diagnostics used by the parity tests. */
 /* influence matrices of one frequency (each nfa x nfa complex, column-major):
  * dp/dm = ZIJ of symmetry class +/-, sp/sm = single-layer S+/S- (SP1+i SP2, SM1+i SM2);

@@ -6,7 +6,9 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdint>
 #include <functional>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -710,3 +712,155 @@ int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Factor-and-solve of device-resident systems that allocates nothing.
+//
+// Callers that cannot allocate: hosts that keep the device's memory under
+// their own allocator -- a PyTorch process whose caching allocator holds the
+// free HBM, or a batching server that sized its batches to the memory left
+// (nemoh_b200.serving admits frequencies by HBM footprint) -- where a
+// cudaMalloc inside the call could fail after admission, or force the host's
+// pool to give memory back; and hosts running several solves side by side on
+// one device, where the device-wide synchronisation of cudaFree would stall
+// the other streams. This entry point therefore takes every buffer from the
+// caller and keeps its scratch in one static device array of fixed size.
+//
+// Scratch layout (offsets rounded to 256 bytes):
+//   status word (int)                    must be 0 when the factorization starts:
+//                                        the call clears it on its stream first
+//   nsys x 32x32 complex                 factored diagonal block of the current
+//                                        LU step (written before it is read)
+//   nsys x nblk x 2 x 64x64 complex      inverses of the 64x64 diagonal blocks
+//                                        of L and U (written before read)
+//   nsys x n x nrhs complex              intermediate vector of the triangular
+//                                        solves (written before read)
+// Only the status word has to start at zero. Every call on a device shares
+// the one array: calls whose work overlaps on the GPU (other streams, other
+// host threads) race on it and give wrong results; serialise them.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NEMOH_B200_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+size_t noalloc_align(size_t x) { return (x + 255) & ~size_t(255); }
+
+// scratch bytes needed for nsys systems of order n with nrhs right-hand sides
+size_t noalloc_bytes(long long n, long long nsys, long long nrhs) {
+  const long long nblk = (n + TB - 1) / TB;
+  return noalloc_align(sizeof(int)) + noalloc_align((size_t)nsys * LU_NB * LU_NB * sizeof(double2)) +
+         noalloc_align((size_t)(nsys * nblk * 2) * TB * TB * sizeof(double2)) +
+         noalloc_align((size_t)(nsys * n * nrhs) * sizeof(double2));
+}
+
+void noalloc_message(char* msg, int len, const std::string& s) {
+  if (msg && len > 0) {
+    std::snprintf(msg, (size_t)len, "%s", s.c_str());
+  }
+}
+
+}  // namespace
+
+extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsys, double* a_device, int nrhs,
+                                                      double* x_device, void* stream, char* msg, int msg_len) {
+  noalloc_message(msg, msg_len, "");
+  if (device < 0 || device >= kNoallocMaxDevices || n < 1 || nsys < 1 || nrhs < 1 || nrhs > MAX_RHS || !a_device ||
+      !x_device || (reinterpret_cast<uintptr_t>(a_device) & 15) || (reinterpret_cast<uintptr_t>(x_device) & 15)) {
+    noalloc_message(msg, msg_len, "invalid argument (device, n >= 1, nsys >= 1, 1 <= nrhs <= 16, 16-byte aligned "
+                                  "device pointers)");
+    return NEMOH_B200_EINVAL;
+  }
+  const size_t need = noalloc_bytes(n, nsys, nrhs);
+  if (need > (size_t)NEMOH_B200_NOALLOC_SCRATCH_BYTES) {
+    noalloc_message(msg, msg_len,
+                    "scratch of " + std::to_string(need) + " bytes needed for n=" + std::to_string(n) +
+                        ", nsys=" + std::to_string(nsys) + ", nrhs=" + std::to_string(nrhs) + " exceeds the fixed " +
+                        std::to_string((size_t)NEMOH_B200_NOALLOC_SCRATCH_BYTES) + "-byte scratch");
+    return NEMOH_B200_ECAPACITY;
+  }
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  auto fail = [&](cudaError_t e, const char* what) {
+    noalloc_message(msg, msg_len, std::string(what) + ": " + cudaGetErrorString(e));
+    if (prev >= 0) cudaSetDevice(prev);
+    return NEMOH_B200_ECUDA;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+  unsigned char* base = nullptr;
+  {
+    // set-up, once per device (the first call on the device): look up the
+    // scratch array's address and raise the dynamic shared-memory limits
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return fail(e, "cudaGetSymbolAddress");
+      const int trsm_smem = (2 * TB * MAX_RHS + TB * TB) * (int)sizeof(double2);
+      const cudaError_t a[4] = {
+          cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               2 * LU_NB * GM_T * (int)sizeof(double2)),
+          cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               2 * TB * TB * (int)sizeof(double2)),
+          cudaFuncSetAttribute(trsm_fused_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               trsm_smem),
+          cudaFuncSetAttribute(trsm_fused_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               trsm_smem)};
+      for (cudaError_t x : a)
+        if (x != cudaSuccess) return fail(x, "cudaFuncSetAttribute");
+      g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+    }
+    base = g_noalloc_ptr[device];
+  }
+  const long long nblk = (n + TB - 1) / TB;
+  int* status = reinterpret_cast<int*>(base);
+  size_t off = noalloc_align(sizeof(int));
+  double2* diag = reinterpret_cast<double2*>(base + off);
+  off += noalloc_align((size_t)nsys * LU_NB * LU_NB * sizeof(double2));
+  double2* inv = reinterpret_cast<double2*>(base + off);
+  off += noalloc_align((size_t)(nsys * nblk * 2) * TB * TB * sizeof(double2));
+  double2* y = reinterpret_cast<double2*>(base + off);
+
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  BatchT<double2> b{reinterpret_cast<double2*>(a_device), (long long)n * n, n, diag};
+  e = cudaMemsetAsync(status, 0, sizeof(int), st);
+  if (e != cudaSuccess) return fail(e, "cudaMemsetAsync");
+  // the FP64 no-pivot blocked LU of the context path, step by step
+  for (int k = 0; k < n; k += LU_NB) {
+    const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
+    const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
+    lu_diag_kernel<double2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
+    if (nrb + ncb > 0) lu_panel_kernel<double2><<<dim3(nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k);
+    if (rest > 0) {
+      const int t = (rest + GM_T - 1) / GM_T;
+      zgemm_update_kernel<double2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(double2), st>>>(b, k, nb);
+    } else {
+      lu_diag_store_kernel<double2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, nb);
+    }
+  }
+  inv_diag_kernel<double2><<<dim3((unsigned)nblk, 1, nsys), TB, 2 * TB * TB * sizeof(double2), st>>>(b, inv,
+                                                                                                      (int)nblk);
+  long long launches = 0;
+  trsm_launch<double2>(b, inv, reinterpret_cast<double2*>(x_device), y, nsys, nrhs, st, launches);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(e, "kernel launch");
+  int h_status = 0;
+  e = cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return fail(e, "cudaMemcpyAsync");
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(e, "cudaStreamSynchronize");
+  if (prev >= 0) cudaSetDevice(prev);
+  if (h_status == ST_PIVOT) {
+    noalloc_message(msg, msg_len, "PIVOT INFERIEUR A 1.E-20 (GAUSSZ)");
+    return NEMOH_B200_EPIVOT;
+  }
+  if (h_status) {
+    noalloc_message(msg, msg_len, "device error " + std::to_string(h_status));
+    return NEMOH_B200_ECUDA;
+  }
+  return NEMOH_B200_OK;
+}
