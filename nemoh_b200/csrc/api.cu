@@ -45,6 +45,28 @@ struct DevBuf {
   T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// pinned host staging (parameters and slot lists uploaded per assembly group)
+struct HostBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~HostBuf() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMallocHost(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    else p = nullptr;
+    return e;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
 struct Fail {
   int code;
   std::string msg;
@@ -60,7 +82,7 @@ struct nemoh_ctx {
   long long launches = 0;
   // tables
   double h_xr[TAB_IR + 2], h_xz[TAB_JZ + 2];
-  DevBuf d_xr, d_xz, d_apd, d_thr, d_status, d_gm;
+  DevBuf d_xr, d_xz, d_apd, d_lag, d_thr, d_status, d_gm;
   // mesh
   int np = 0, nfa = 0, nsymy = 0;
   double rho = 0, g = 0, depth = 0, zer = 0, gm = 0;
@@ -68,6 +90,8 @@ struct nemoh_ctx {
   DevBuf d_xyz, d_m, d_rec, d_rows;
   // per-call workspace
   DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force;
+  HostBuf h_oms, h_slots;
+  int cap_slots = 0, cap_nrhs = 0;   // what ensure_batch last provided
   MixedWork mixed;
   int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
   double w_previous = -1.;   // factor cache key of solve_problem
@@ -166,6 +190,7 @@ void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
 
 // capacity: frequencies per device batch
 int batch_capacity(nemoh_ctx* c, int nrhs, int want) {
+  if (want <= c->cap_slots && nrhs <= c->cap_nrhs) return want;   // buffers already fit
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t N = c->nfa, cls = ncls(c);
@@ -192,7 +217,11 @@ void ensure_batch(nemoh_ctx* c, int slots, int nrhs) {
     CK(c->d_inv.ensure((size_t)slots * cls * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
   CK(c->d_oms.ensure((size_t)slots * sizeof(OmegaParams)));
   CK(c->d_slots.ensure((size_t)slots * sizeof(int)));
+  CK(c->h_oms.ensure((size_t)slots * sizeof(OmegaParams)));
+  CK(c->h_slots.ensure((size_t)slots * sizeof(int)));
   if (c->mode == NEMOH_B200_MIXED) CK(c->mixed.ensure(slots * (int)cls, (int)N, std::max(nrhs, 1)));
+  c->cap_slots = std::max(c->cap_slots, slots);
+  c->cap_nrhs = std::max(c->cap_nrhs, std::max(nrhs, 1));
 }
 
 GreenCtx green_ctx(nemoh_ctx* c) {
@@ -200,6 +229,8 @@ GreenCtx green_ctx(nemoh_ctx* c) {
   g.xr = c->d_xr.as<double>();
   g.xz = c->d_xz.as<double>();
   g.apd = c->d_apd.as<double4>();
+  g.xlag = c->d_lag.as<double4>();
+  g.zlag = c->d_lag.as<double4>() + 2 * (TAB_IR + 2);
   g.thr = c->d_thr.as<StencilThresholds>();
   g.zer = c->zer;
   g.nsymy = c->nsymy;
@@ -208,32 +239,42 @@ GreenCtx green_ctx(nemoh_ctx* c) {
   return g;
 }
 
-// assemble the frequencies held in slots [0, nslots) (params already uploaded)
-void assemble(nemoh_ctx* c, const std::vector<OmegaParams>& oms) {
+// Upload the parameters of slots [s0, s1) (already in c->h_oms) and assemble
+// those frequencies: deep-water slots first, then finite-depth ones.
+void assemble_range(nemoh_ctx* c, int s0, int s1) {
   const int N = c->nfa, cls = ncls(c);
-  std::vector<int> infd, fd;
-  for (int s = 0; s < (int)oms.size(); ++s) (oms[s].fd ? fd : infd).push_back(s);
-  std::vector<int> all(infd);
-  all.insert(all.end(), fd.begin(), fd.end());
-  CK(cudaMemcpyAsync(c->d_slots.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  const OmegaParams* hom = c->h_oms.as<OmegaParams>();
+  int* hs = c->h_slots.as<int>() + s0;
+  int ninfd = 0;
+  for (int s = s0; s < s1; ++s)
+    if (!hom[s].fd) hs[ninfd++] = s;
+  int nfd = 0;
+  for (int s = s0; s < s1; ++s)
+    if (hom[s].fd) hs[ninfd + nfd++] = s;
+  CK(cudaMemcpyAsync(c->d_oms.as<OmegaParams>() + s0, hom + s0, (size_t)(s1 - s0) * sizeof(OmegaParams),
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_slots.as<int>() + s0, hs, (size_t)(s1 - s0) * sizeof(int), cudaMemcpyHostToDevice,
+                     c->stream));
   GreenCtx g = green_ctx(c);
   const long long NN = (long long)N * N;
   AsmOut o{c->d_D.as<double2>(), c->d_S.as<double2>(), cls * NN};
   dim3 blk(ASM_ROWS);
-  if (!infd.empty()) {
-    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)infd.size());
-    assemble_kernel<false><<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(), c->d_slots.as<int>(),
-                                                        c->d_rec.as<PanelRec>(), c->d_rows.as<double>(), N, o);
+  const OmegaParams* dom = c->d_oms.as<OmegaParams>();
+  const PanelRec* rec = c->d_rec.as<PanelRec>();
+  const double* rows = c->d_rows.as<double>();
+  const int* ds = c->d_slots.as<int>() + s0;
+  if (ninfd) {
+    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)ninfd);
+    rankine_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, N, o);
+    LAUNCHED(c);
+    wave_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, N, o);
     LAUNCHED(c);
   }
-  if (!fd.empty()) {
-    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)fd.size());
-    assemble_kernel<true><<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(),
-                                                       c->d_slots.as<int>() + infd.size(), c->d_rec.as<PanelRec>(),
-                                                       c->d_rows.as<double>(), N, o);
+  if (nfd) {
+    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
+    rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
     LAUNCHED(c);
-    fd_images_kernel<<<grid, blk, 0, c->stream>>>(g, c->d_oms.as<OmegaParams>(), c->d_slots.as<int>() + infd.size(),
-                                                  c->d_rec.as<PanelRec>(), c->d_rows.as<double>(), N, o);
+    wave_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
     LAUNCHED(c);
   }
 }
@@ -313,9 +354,8 @@ void potential(nemoh_ctx* c, int nsys, int nrhs) {
   LAUNCHED(c);
 }
 
-void upload_params(nemoh_ctx* c, const std::vector<OmegaParams>& oms) {
-  CK(cudaMemcpyAsync(c->d_oms.p, oms.data(), oms.size() * sizeof(OmegaParams), cudaMemcpyHostToDevice, c->stream));
-}
+// frequencies whose host setup is done before their assembly is launched
+constexpr int ASM_GROUP = 8;
 
 // shared by the host and device-pointer batched entry points
 void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int nrhs, const double2* nvel_d, int nint,
@@ -328,14 +368,19 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
   c->t_asm = c->t_fac = c->t_sol = 0;
   for (int w0 = 0; w0 < nomega; w0 += cap) {
     const int nw = std::min(cap, nomega - w0);
-    std::vector<OmegaParams> oms(nw);
+    // host setup of each frequency (in the caller's order, which the NQ state
+    // follows) overlapped with the assembly of the groups set up before it
+    OmegaParams* hom = c->h_oms.as<OmegaParams>();
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    int done = 0;
     for (int i = 0; i < nw; ++i) {
       const double T = 2. * kPI / omegas[w0 + i];
-      omega_params(c, 2. * kPI / T, oms[i], true);
+      omega_params(c, 2. * kPI / T, hom[i], true);
+      if (i + 1 == nw || i + 1 - done >= ASM_GROUP) {
+        assemble_range(c, done, i + 1);
+        done = i + 1;
+      }
     }
-    upload_params(c, oms);
-    CK(cudaEventRecord(c->ev[0], c->stream));
-    assemble(c, oms);
     CK(cudaEventRecord(c->ev[1], c->stream));
     fold_rhs_kernel<<<dim3((N + 127) / 128, nrhs, nw), 128, 0, c->stream>>>(
         nvel_d + (long long)w0 * nrhs * cls * N, N, c->nsymy, nrhs, c->d_X.as<double2>());
@@ -409,6 +454,22 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
     CK(c->d_apd.ensure(sizeof(double4) * TAB_IR * TAB_JZ));
     CK(cudaMemcpyAsync(c->d_xr.p, c->h_xr, sizeof c->h_xr, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_xz.p, c->h_xz, sizeof c->h_xz, cudaMemcpyHostToDevice, c->stream));
+    // 3-node Lagrange stencils of both axes: nodes and reciprocal denominators
+    std::vector<double> lag(8 * (size_t)(TAB_IR + 2 + TAB_JZ + 2), 0.);
+    auto stencils = [&](const double* x, int n, double* out) {
+      for (int k = 2; k < n; ++k) {
+        const double a = x[k - 1], b = x[k], cc = x[k + 1];
+        double* q = out + 8 * k;
+        q[0] = a; q[1] = b; q[2] = cc;
+        q[3] = 1. / ((a - b) * (a - cc));
+        q[4] = 1. / ((b - cc) * (b - a));
+        q[5] = 1. / ((cc - a) * (cc - b));
+      }
+    };
+    stencils(c->h_xr, TAB_IR, lag.data());
+    stencils(c->h_xz, TAB_JZ, lag.data() + 8 * (TAB_IR + 2));
+    CK(c->d_lag.ensure(lag.size() * sizeof(double)));
+    CK(cudaMemcpyAsync(c->d_lag.p, lag.data(), lag.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(dq.p, cqt, sizeof cqt, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(dc.p, ctt, sizeof ctt, cudaMemcpyHostToDevice, c->stream));
     crek_kernel<<<(TAB_IR * TAB_JZ + 127) / 128, 128, 0, c->stream>>>(c->d_xr.as<double>(), c->d_xz.as<double>(),
@@ -535,11 +596,10 @@ int nemoh_b200_assemble(nemoh_ctx* c, double omega, double* dp, double* dm, doub
   if (!c || !c->nfa || !(omega > 0)) return NEMOH_B200_EINVAL;
   return guarded(c, [&] {
     ensure_batch(c, 1, 1);
-    std::vector<OmegaParams> oms(1);
+    OmegaParams& om = c->h_oms.as<OmegaParams>()[0];
     const double T = 2. * kPI / omega;
-    omega_params(c, 2. * kPI / T, oms[0], true);
-    upload_params(c, oms);
-    assemble(c, oms);
+    omega_params(c, 2. * kPI / T, om, true);
+    assemble_range(c, 0, 1);
     check_status(c);
     const size_t NN = (size_t)c->nfa * c->nfa, b = NN * sizeof(double2);
     const bool two = c->nsymy == 1;
@@ -548,7 +608,7 @@ int nemoh_b200_assemble(nemoh_ctx* c, double omega, double* dp, double* dm, doub
     if (sp) CK(cudaMemcpyAsync(sp, c->d_S.p, b, cudaMemcpyDeviceToHost, c->stream));
     if (sm) CK(cudaMemcpyAsync(sm, c->d_S.as<double2>() + (two ? NN : 0), b, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (depth_mode) *depth_mode = oms[0].fd;
+    if (depth_mode) *depth_mode = om.fd;
     c->w_previous = -1.;
   });
 }
@@ -561,15 +621,14 @@ int nemoh_b200_solve_problem(nemoh_ctx* c, double period, const double* nvel, do
     const double W = 2. * kPI / period;
     ensure_batch(c, 1, 1);
     if (W != c->w_previous) {
-      std::vector<OmegaParams> oms(1);
-      omega_params(c, W, oms[0], true);
-      upload_params(c, oms);
-      assemble(c, oms);
+      OmegaParams& om = c->h_oms.as<OmegaParams>()[0];
+      omega_params(c, W, om, true);
+      assemble_range(c, 0, 1);
       factor_and_solve(c, cls, 1, false);
       check_status(c);
       c->w_previous = W;
-      c->cached_fd = oms[0].fd;
-      c->cached_nexp = oms[0].nexp;
+      c->cached_fd = om.fd;
+      c->cached_nexp = om.nexp;
     } else if (c->cached_fd) {
       OmegaParams tmp;
       omega_params(c, W, tmp, true);  // NQ/LISC side state of a repeated call

@@ -125,14 +125,31 @@ __global__ void crek_kernel(const double* __restrict__ xr, const double* __restr
 }
 
 // ---------------------------------------------------------------------------
-// Influence-matrix assembly. Thread = collocation row I, block = 128 rows;
-// the block stages ASM_TJ source panels J in shared memory and walks them.
-// Output per frequency (column-major, leading dimension N): D+ then D- in
-// out.d, S+ then S- in out.s (nsymy=0: one D and one S).
-// Column-major writes by consecutive rows are coalesced 16-byte stores.
+// Influence-matrix assembly, two passes per frequency. Thread = collocation
+// row I, block = 128 rows; the block stages ASM_TJ source panels J in shared
+// memory and walks them. Output per frequency (column-major, leading
+// dimension N): D+ then D- in out.d, S+ then S- in out.s (nsymy=0: one D and
+// one S). Column-major writes by consecutive rows are coalesced 16-byte
+// stores.
+//   rankine_kernel: Rankine part (VAVINFD / VAVFD, plus the exponential images
+//                   of VNSFD in finite depth) -> real parts, imaginary = 0;
+//   wave_kernel:    wave part (VNSINFD / VNSFD) added to the real parts and
+//                   written to the imaginary parts.
+// Splitting the pair evaluation keeps each kernel's registers and code small
+// enough for several CTAs per SM; the extra read of the matrices is 64 bytes
+// per pair and symmetry class pair.
 // ---------------------------------------------------------------------------
 constexpr int ASM_ROWS = 128;
 constexpr int ASM_TJ = 32;
+#ifndef ASM_MINB_RANKINE
+#define ASM_MINB_RANKINE 4
+#endif
+#ifndef ASM_MINB_WAVE_FD
+#define ASM_MINB_WAVE_FD 3
+#endif
+#ifndef ASM_MINB_WAVE_INFD
+#define ASM_MINB_WAVE_INFD 4
+#endif
 
 struct AsmOut {
   double2* d;           // D+ (and D-) of frequency slot s at d + s * slot_stride
@@ -140,26 +157,31 @@ struct AsmOut {
   long long slot_stride;
 };
 
+__device__ __forceinline__ void stage_panels(const PanelRec* __restrict__ rec, int j0, int nj, PanelRec* sp) {
+  const double* src = reinterpret_cast<const double*>(rec + j0);
+  double* dst = reinterpret_cast<double*>(sp);
+  const int nw = nj * (int)(sizeof(PanelRec) / 8);
+  for (int i = threadIdx.x; i < nw; i += blockDim.x) dst[i] = src[i];
+}
+
+__device__ __forceinline__ void stage_params(const OmegaParams* __restrict__ om, OmegaParams* som) {
+  const double* src = reinterpret_cast<const double*>(om);
+  double* dst = reinterpret_cast<double*>(som);
+  for (int i = threadIdx.x; i < (int)(sizeof(OmegaParams) / 8); i += blockDim.x) dst[i] = src[i];
+}
+
 template <bool FD>
-__global__ void __launch_bounds__(ASM_ROWS) assemble_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
-                                                            const int* __restrict__ slots, const PanelRec* __restrict__ rec,
-                                                            const double* __restrict__ rows, int N, AsmOut out) {
+__global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
+                                                           const int* __restrict__ slots,
+                                                           const PanelRec* __restrict__ rec,
+                                                           const double* __restrict__ rows, int N, AsmOut out) {
   __shared__ PanelRec sp[ASM_TJ];
   __shared__ OmegaParams som;
   const int slot = slots[blockIdx.z];
-  {
-    const double* src = reinterpret_cast<const double*>(oms + slot);
-    double* dst = reinterpret_cast<double*>(&som);
-    for (int i = threadIdx.x; i < (int)(sizeof(OmegaParams) / 8); i += blockDim.x) dst[i] = src[i];
-  }
+  stage_params(oms + slot, &som);
   const int j0 = blockIdx.y * ASM_TJ;
   const int nj = min(ASM_TJ, N - j0);
-  {
-    const double* src = reinterpret_cast<const double*>(rec + j0);
-    double* dst = reinterpret_cast<double*>(sp);
-    const int nw = nj * (int)(sizeof(PanelRec) / 8);
-    for (int i = threadIdx.x; i < nw; i += blockDim.x) dst[i] = src[i];
-  }
+  stage_panels(rec, j0, nj, sp);
   __syncthreads();
   const int I = blockIdx.x * ASM_ROWS + threadIdx.x;
   if (I >= N) return;
@@ -168,120 +190,53 @@ __global__ void __launch_bounds__(ASM_ROWS) assemble_kernel(GreenCtx g, const Om
   const long long NN = (long long)N * N;
   double2* od = out.d + slot * out.slot_stride;
   double2* os = out.s + slot * out.slot_stride;
+#pragma unroll 1
   for (int jj = 0; jj < nj; ++jj) {
     const int J = j0 + jj;
-    PairOut r;
-    pair_green<FD>(g, som, XGI, YGI, ZGI, XNI, YNI, ZNI, I == J, sp[jj], r);
+    RealOut r;
+    pair_rankine<FD>(g, som, som.ambda, som.ar, XGI, YGI, ZGI, XNI, YNI, ZNI, I == J, sp[jj], r);
     const long long q = I + (long long)N * J;
-    od[q] = make_double2(r.dp_re, r.dp_im);
-    os[q] = make_double2(r.sp_re, r.sp_im);
+    od[q] = make_double2(r.dp, 0.);
+    os[q] = make_double2(r.sp, 0.);
     if (g.nsymy == 1) {
-      od[NN + q] = make_double2(r.dm_re, r.dm_im);
-      os[NN + q] = make_double2(r.sm_re, r.sm_im);
+      od[NN + q] = make_double2(r.dm, 0.);
+      os[NN + q] = make_double2(r.sm, 0.);
     }
   }
 }
 
-// ---------------------------------------------------------------------------
-// Finite depth: the exponential images of VNSFD (COMPUTE_GREEN_FD.f90:635-706),
-//   sum_KE AR(KE) (-A/8pi) sum_4 1/rho  and their gradients,
-// added to D+/-, S+/- after assemble_kernel<true>. The reference adds them to
-// FS1, VSX1, VSY1, VSZ1 of each reflection, and those enter SP1/SM1 and the
-// real parts of D+/- linearly (:830-865), so the sums can be accumulated
-// separately. Image depths are shared by both reflections; RO > EPS is
-// decided exactly on RO^2 against a precomputed threshold.
-// ---------------------------------------------------------------------------
-struct ImgPanel {
-  double xg, yg, zg, aire;
-};
-
-__global__ void __launch_bounds__(ASM_ROWS) fd_images_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
-                                                             const int* __restrict__ slots,
-                                                             const PanelRec* __restrict__ rec,
-                                                             const double* __restrict__ rows, int N, AsmOut out) {
-  __shared__ ImgPanel sp[ASM_TJ];
-  __shared__ double s_ambda[MAX_NEXP + 1], s_ar[MAX_NEXP + 1];
+template <bool FD>
+__global__ void __launch_bounds__(ASM_ROWS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_WAVE_INFD) wave_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
+                                                        const int* __restrict__ slots, const PanelRec* __restrict__ rec,
+                                                        const double* __restrict__ rows, int N, AsmOut out) {
+  __shared__ PanelRec sp[ASM_TJ];
+  __shared__ OmegaParams som;
   const int slot = slots[blockIdx.z];
-  const OmegaParams* om = oms + slot;
-  const int nexp1 = om->nexp + 1;
-  for (int i = threadIdx.x; i <= MAX_NEXP; i += blockDim.x) {
-    s_ambda[i] = om->ambda[i];
-    s_ar[i] = om->ar[i];
-  }
+  stage_params(oms + slot, &som);
   const int j0 = blockIdx.y * ASM_TJ;
   const int nj = min(ASM_TJ, N - j0);
-  for (int i = threadIdx.x; i < nj; i += blockDim.x) {
-    const PanelRec& p = rec[j0 + i];
-    sp[i] = ImgPanel{p.xg, p.yg, p.zg, p.aire};
-  }
+  stage_panels(rec, j0, nj, sp);
   __syncthreads();
   const int I = blockIdx.x * ASM_ROWS + threadIdx.x;
   if (I >= N) return;
   const double XGI = rows[I], YGI = rows[N + I], ZGI = rows[2 * N + I];
   const double XNI = rows[3 * N + I], YNI = rows[4 * N + I], ZNI = rows[5 * N + I];
-  if (!(ZGI < g.zer)) return;   // free-surface collocation rows use the panel branch
-  const double ZMIII = ZGI;
-  const double H = om->h, H2 = XMUL(2., H), H4 = XMUL(4., H);
-  const double QPI = 4. * 3.141592653589793;
-  const double T2 = g.ro_eps2;
-  const int NJJ = g.nsymy + 1;
   const long long NN = (long long)N * N;
   double2* od = out.d + slot * out.slot_stride;
   double2* os = out.s + slot * out.slot_stride;
-  for (int jj = 0; jj < nj; ++jj) {
-    const ImgPanel P = sp[jj];
-    if (!(P.zg < g.zer)) continue;
-    double dx[2], dy[2], r2[2], fs[2] = {0., 0.}, vx[2] = {0., 0.}, vy[2] = {0., 0.}, vz[2] = {0., 0.};
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      dx[b] = XSUB(XGI, P.xg);
-      dy[b] = XSUB(YGI, P.yg * (b ? -1. : 1.));
-      const double R = XSQRT(XADD(XMUL(dx[b], dx[b]), XMUL(dy[b], dy[b])));
-      r2[b] = XMUL(R, R);
-    }
-    const double ACT = -0.5 * P.aire / QPI;
 #pragma unroll 1
-    for (int KE = 1; KE <= nexp1; ++KE) {
-      const double AQT = ACT * s_ar[KE];
-      const double HA = XMUL(H, s_ambda[KE]);
-      double zp[4], z2[4];
-      zp[0] = XSUB(XADD(XSUB(ZMIII, H2), HA), P.zg);
-      zp[1] = XSUB(XSUB(-ZMIII, HA), P.zg);
-      zp[2] = XSUB(XADD(XSUB(-ZMIII, H4), HA), P.zg);
-      zp[3] = XSUB(XSUB(XADD(ZMIII, H2), HA), P.zg);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) z2[k] = XMUL(zp[k], zp[k]);
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        if (b >= NJJ) break;
-        double a[4], sa = 0.;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const double RRk = XADD(r2[b], z2[k]);
-          if (RRk > T2) {
-            const double ri = rsqrt(RRk);
-            const double FT = AQT * ri;
-            fs[b] += FT;
-            a[k] = FT * ri * ri;
-          } else {
-            a[k] = 0.;
-          }
-          sa += a[k];
-        }
-        vx[b] -= dx[b] * sa;
-        vy[b] -= dy[b] * sa;
-        vz[b] -= zp[0] * a[0] - zp[1] * a[1] - zp[2] * a[2] + zp[3] * a[3];
-      }
-    }
+  for (int jj = 0; jj < nj; ++jj) {
+    PairOut r;
+    pair_wave<FD>(g, som, XGI, YGI, ZGI, XNI, YNI, ZNI, sp[jj], r);
     const long long q = I + (long long)N * (j0 + jj);
-    if (NJJ == 2) {
-      od[q].x += (vx[0] + vx[1]) * XNI + (vy[0] + vy[1]) * YNI + (vz[0] + vz[1]) * ZNI;
-      od[NN + q].x += (vx[0] - vx[1]) * XNI + (vy[0] - vy[1]) * YNI + (vz[0] - vz[1]) * ZNI;
-      os[q].x += fs[0] + fs[1];
-      os[NN + q].x += fs[0] - fs[1];
-    } else {
-      od[q].x += vx[0] * XNI + vy[0] * YNI + vz[0] * ZNI;
-      os[q].x += fs[0];
+    double2 d = od[q], s = os[q];
+    od[q] = make_double2(d.x + r.dp_re, r.dp_im);
+    os[q] = make_double2(s.x + r.sp_re, r.sp_im);
+    if (g.nsymy == 1) {
+      d = od[NN + q];
+      s = os[NN + q];
+      od[NN + q] = make_double2(d.x + r.dm_re, r.dm_im);
+      os[NN + q] = make_double2(s.x + r.sm_re, r.sm_im);
     }
   }
 }

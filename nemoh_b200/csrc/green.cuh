@@ -22,6 +22,8 @@ struct GreenCtx {
   const double* xr;                 // XR(1..328) at [1..328]
   const double* xz;                 // XZ(1..46) at [1..46]
   const double4* apd;               // {APD1X, APD1Z, APD2X, APD2Z}(I,J) at (I-1)+328*(J-1)
+  const double4* xlag;              // 3-node Lagrange stencils of XR, two double4 per centre node K
+  const double4* zlag;              // same for XZ
   const StencilThresholds* thr;
   double zer;                       // ZER (PREPARE_MESH.f90:58-69)
   int nsymy;
@@ -71,11 +73,6 @@ __device__ __noinline__ cplx GG(cplx Z, cplx CEX) {
   return (T < 0.) ? num / den - IPI * CEX : num / den + IPI * CEX;
 }
 
-// COMPUTE_GREEN_INFD.f90:641-645
-__device__ __forceinline__ double PL2(double U1, double U2, double U3, double XU) {
-  return ((XU - U1) * (XU - U2)) / ((U3 - U1) * (U3 - U2));
-}
-
 // integer part of a monotone log10 expression, made exact by thresholds
 __device__ __forceinline__ int stencil_adjust(double x, const double* thr, int k) {
   k = max(0, min(k, 47));
@@ -109,25 +106,16 @@ __device__ __forceinline__ int stencil_ki(double AKR, const StencilThresholds* T
   return min(k, 327);
 }
 
-struct Lagrange {
-  int KI, KJ;
-  double XL1, XL2, XL3, ZL1, ZL2, ZL3;
+// Three-node Lagrange stencil around node K of a table axis: the reference
+// evaluates PL2(U1,U2,U3,XU) = (XU-U1)(XU-U2)/((U3-U1)(U3-U2)) on the nodes
+// K-1, K, K+1 (COMPUTE_GREEN_INFD.f90:306-311, :641-645). The nodes and the
+// reciprocals of the three denominators are tabulated per K (two double4:
+// {a, b, c, 1/((a-b)(a-c))}, {1/((b-c)(b-a)), 1/((c-a)(c-b)), 0, 0}), so a
+// coefficient is two products instead of a division.
+struct Stencil {
+  int K;
+  double L1, L2, L3;
 };
-
-__device__ __forceinline__ void lagrange_x(const GreenCtx& g, double AKR, Lagrange& L) {
-  L.KI = stencil_ki(AKR, g.thr);
-  double a = __ldg(g.xr + L.KI - 1), b = __ldg(g.xr + L.KI), c = __ldg(g.xr + L.KI + 1);
-  L.XL1 = PL2(b, c, a, AKR);
-  L.XL2 = PL2(c, a, b, AKR);
-  L.XL3 = PL2(a, b, c, AKR);
-}
-__device__ __forceinline__ void lagrange_z(const GreenCtx& g, double AKZ, Lagrange& L) {
-  L.KJ = stencil_kj(AKZ, g.thr);
-  double a = __ldg(g.xz + L.KJ - 1), b = __ldg(g.xz + L.KJ), c = __ldg(g.xz + L.KJ + 1);
-  L.ZL1 = PL2(b, c, a, AKZ);
-  L.ZL2 = PL2(c, a, b, AKZ);
-  L.ZL3 = PL2(a, b, c, AKZ);
-}
 
 __device__ __forceinline__ double4 ldg4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);
@@ -135,19 +123,34 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+__device__ __forceinline__ void stencil_coeffs(const double4* lag, int K, double u, Stencil& s) {
+  const double4 p = ldg4(lag + 2 * K), q = ldg4(lag + 2 * K + 1);
+  s.K = K;
+  s.L1 = ((u - p.y) * (u - p.z)) * p.w;
+  s.L2 = ((u - p.z) * (u - p.x)) * q.x;
+  s.L3 = ((u - p.x) * (u - p.y)) * q.y;
+}
+
+__device__ __forceinline__ void stencil_x(const GreenCtx& g, double AKR, Stencil& s) {
+  stencil_coeffs(g.xlag, stencil_ki(AKR, g.thr), AKR, s);
+}
+__device__ __forceinline__ void stencil_z(const GreenCtx& g, double AKZ, Stencil& s) {
+  stencil_coeffs(g.zlag, stencil_kj(AKZ, g.thr), AKZ, s);
+}
+
 // 3x3 Lagrange interpolation of the four tables (:306-319, :345-352)
-__device__ __forceinline__ double4 interp4(const GreenCtx& g, const Lagrange& L) {
+__device__ __forceinline__ double4 interp4(const GreenCtx& g, const Stencil& sx, const Stencil& sz) {
   double4 r = make_double4(0., 0., 0., 0.);
-  const double zl[3] = {L.ZL1, L.ZL2, L.ZL3};
+  const double zl[3] = {sz.L1, sz.L2, sz.L3};
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
-    const double4* row = g.apd + (L.KI - 2) + TAB_IR * (L.KJ - 2 + b);
+    const double4* row = g.apd + (sx.K - 2) + TAB_IR * (sz.K - 2 + b);
     double4 t1 = ldg4(row), t2 = ldg4(row + 1), t3 = ldg4(row + 2);
     double4 F;
-    F.x = L.XL1 * t1.x + L.XL2 * t2.x + L.XL3 * t3.x;
-    F.y = L.XL1 * t1.y + L.XL2 * t2.y + L.XL3 * t3.y;
-    F.z = L.XL1 * t1.z + L.XL2 * t2.z + L.XL3 * t3.z;
-    F.w = L.XL1 * t1.w + L.XL2 * t2.w + L.XL3 * t3.w;
+    F.x = sx.L1 * t1.x + sx.L2 * t2.x + sx.L3 * t3.x;
+    F.y = sx.L1 * t1.y + sx.L2 * t2.y + sx.L3 * t3.y;
+    F.z = sx.L1 * t1.z + sx.L2 * t2.z + sx.L3 * t3.z;
+    F.w = sx.L1 * t1.w + sx.L2 * t2.w + sx.L3 * t3.w;
     r.x += zl[b] * F.x;
     r.y += zl[b] * F.y;
     r.z += zl[b] * F.z;
@@ -227,6 +230,10 @@ __device__ __noinline__ void rankine_near(double XOI, double YOI, double ZOI, co
   }
 }
 
+// Images JJ = 1..4 (direct, sea-bottom / free-surface image, and their
+// y-mirrors) are combined into the two symmetry classes as they are computed:
+// class + takes (1, -MK, -MK, 1), class - takes (1, -MK, MK, -1) of the four
+// (VAVINFD/VAVFD combination, COMPUTE_GREEN_INFD.f90:176-216).
 template <bool FD>
 __device__ __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI, double YGI, double ZGI, bool self,
                                         const PanelRec& P, RankineOut& o) {
@@ -236,11 +243,10 @@ __device__ __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI
   const double MK = FD ? -1. : 1.;
   double XOI = XGI, YOI = YGI, ZOI = ZGI;
   if (ZGI > g.zer) ZOI = FD ? XMUL(20., g.zer) : g.zer;
-  double AIJS[4], VXS[4], VYS[4], VZS[4];
   const double lim7 = XMUL(7., P.tdis);
-#pragma unroll
-  for (int JJ = 1; JJ <= 4; ++JJ) {
-    if (JJ > NJJ) break;
+  o = RankineOut{0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+  for (int JJ = 1; JJ <= NJJ; ++JJ) {
     const int MJJ = (JJ & 1) ? 1 : -1;
     const int MY = (JJ >= 3) ? -1 : 1;
     const int MZ = (JJ == 2 || JJ == 3) ? -1 : 1;
@@ -250,8 +256,9 @@ __device__ __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI
     const double RO = XSQRT(XADD(XADD(XMUL(dx, dx), XMUL(dy, dy)), XMUL(dz, dz)));
     double a, vx, vy, vz;
     if (RO > lim7) {
-      a = P.aire / RO;
-      double ASRO = a / (RO * RO);
+      const double iRO = 1. / RO;
+      a = P.aire * iRO;
+      const double ASRO = a * iRO * iRO;
       vx = -dx * ASRO;
       vy = -dy * ASRO;
       vz = -dz * ASRO;
@@ -265,23 +272,18 @@ __device__ __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI
         a *= MJJ; vx *= MJJ; vy *= MJJ; vz *= MJJ;
       }
     }
-    AIJS[JJ - 1] = a; VXS[JJ - 1] = vx; VYS[JJ - 1] = vy; VZS[JJ - 1] = vz;
+    const double cp = (JJ == 1 || JJ == 4) ? 1. : -MK;
+    const double cm = (JJ == 1) ? 1. : (JJ == 2) ? -MK : (JJ == 3) ? MK : -1.;
+    o.FSP += cp * a; o.VSXP += cp * vx; o.VSYP += cp * vy; o.VSZP += cp * vz;
+    o.FSM += cm * a; o.VSXM += cm * vx; o.VSYM += cm * vy; o.VSZM += cm * vz;
   }
   const double iq = -1. / QPI;
   if (g.nsymy == 1) {
-    o.FSP = (AIJS[0] - MK * (AIJS[1] + AIJS[2]) + AIJS[3]) * iq;
-    o.FSM = (AIJS[0] - MK * (AIJS[1] - AIJS[2]) - AIJS[3]) * iq;
-    o.VSXP = (VXS[0] - MK * (VXS[1] + VXS[2]) + VXS[3]) * iq;
-    o.VSYP = (VYS[0] - MK * (VYS[1] + VYS[2]) + VYS[3]) * iq;
-    o.VSZP = (VZS[0] - MK * (VZS[1] + VZS[2]) + VZS[3]) * iq;
-    o.VSXM = (VXS[0] - MK * (VXS[1] - VXS[2]) - VXS[3]) * iq;
-    o.VSYM = (VYS[0] - MK * (VYS[1] - VYS[2]) - VYS[3]) * iq;
-    o.VSZM = (VZS[0] - MK * (VZS[1] - VZS[2]) - VZS[3]) * iq;
+    o.FSP *= iq; o.VSXP *= iq; o.VSYP *= iq; o.VSZP *= iq;
+    o.FSM *= iq; o.VSXM *= iq; o.VSYM *= iq; o.VSZM *= iq;
   } else {
-    o.FSP = o.FSM = (AIJS[0] - MK * AIJS[1]) * iq;
-    o.VSXP = o.VSXM = (VXS[0] - MK * VXS[1]) * iq;
-    o.VSYP = o.VSYM = (VYS[0] - MK * VYS[1]) * iq;
-    o.VSZP = o.VSZM = (VZS[0] - MK * VZS[1]) * iq;
+    o.FSP *= iq; o.VSXP *= iq; o.VSYP *= iq; o.VSZP *= iq;
+    o.FSM = o.FSP; o.VSXM = o.VSXP; o.VSYM = o.VSYP; o.VSZM = o.VSZP;
   }
 }
 
@@ -340,71 +342,81 @@ __device__ __noinline__ void wave_infd_fs(const OmegaParams& om, double XGI, dou
   w.FS1 *= s; w.FS2 *= s; w.VSX1 *= s; w.VSX2 *= s; w.VSY1 *= s; w.VSY2 *= s; w.VSZ1 *= s; w.VSZ2 *= s;
 }
 
-// --- VNSINFD tabulated branch for one reflection BX (:271-382) -------------
-__device__ __forceinline__ void wave_infd_jj(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
-                                             double ZMIII, int BX, const PanelRec& P, WaveJJ& w) {
+// --- VNSINFD tabulated branch, both reflections (:271-382) ----------------
+// AKZ depends on the depths only, so its stencil is shared by BX = +1 and -1.
+__device__ __forceinline__ void wave_infd_pair(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
+                                               double ZMIII, const PanelRec& P, int NJJ, WaveJJ* w) {
   const double PI = 3.141592653589793, PI4 = 0.7853981633974483, DPI = 2. * PI, EPS = 0.0001;
   const double AK0 = om.k0;
-  const double YMJJJ = P.yg * BX;
-  const double dx = XSUB(XGI, P.xg), dy = XSUB(YGI, YMJJJ);
-  const double RRR = XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy)));
-  const double AKR = XMUL(AK0, RRR);
   const double ZZZ = XADD(ZMIII, P.zg);
   const double AKZ = XMUL(AK0, ZZZ);
-  const double DD = XSQRT(XADD(XMUL(RRR, RRR), XMUL(ZZZ, ZZZ)));
-  double PSURR = 0.;
-  if (DD > EPS) {
-    double t = AK0 * DD;
-    PSURR = PI / (t * t * t);
-  }
-  double PD1Z, PD2Z, VZ1, VZ2, PD1X = 0., PD2X = 0., VR1 = 0., VR2 = 0.;
   if (AKZ > -1.5E-6) {
     set_status(g.status, ST_AKZ_UNDEFINED);
-    w = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
+    w[0] = w[1] = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
     return;
   }
-  if (AKZ > -16.) {
-    if (AKR < 99.7) {
-      Lagrange L;
-      lagrange_x(g, AKR, L);
-      lagrange_z(g, AKZ, L);
-      double4 t = interp4(g, L);
-      PD1X = t.x; PD1Z = t.y; PD2X = t.z; PD2Z = t.w;
-    } else {
-      double EPZ = exp(AKZ);
-      double SQ = sqrt(DPI / AKR);
-      double SIK, CSK;
-      sincos(AKR - PI4, &SIK, &CSK);
-      PD1Z = PSURR * AKZ - PI * EPZ * SQ * SIK;
-      PD2Z = EPZ * SQ * CSK;
-      double DSK = 0.5 / AKR;
-      PD1X = -PSURR * AKR + PI * EPZ * SQ * (CSK - DSK * SIK);
-      PD2X = EPZ * SQ * (SIK + DSK * CSK);
+  Stencil sz;
+  bool have_sz = false;
+#pragma unroll 1
+  for (int b = 0; b < NJJ; ++b) {
+    const double YMJJJ = b ? -P.yg : P.yg;
+    const double dx = XSUB(XGI, P.xg), dy = XSUB(YGI, YMJJJ);
+    const double RRR = XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy)));
+    const double AKR = XMUL(AK0, RRR);
+    const double DD = XSQRT(XADD(XMUL(RRR, RRR), XMUL(ZZZ, ZZZ)));
+    double PSURR = 0.;
+    if (DD > EPS) {
+      const double it = 1. / (AK0 * DD);
+      PSURR = PI * it * it * it;
     }
-    VZ1 = PD1Z - PSURR * AKZ;
-    VZ2 = PD2Z;
-    VR1 = -PD1X - PSURR * AKR;
-    VR2 = -PD2X;
-  } else {
-    PD1Z = PSURR * AKZ;
-    PD2Z = 0.;
-    VZ1 = 0.;
-    VZ2 = 0.;
+    double PD1Z, PD2Z, VZ1, VZ2, PD1X = 0., PD2X = 0., VR1 = 0., VR2 = 0.;
+    if (AKZ > -16.) {
+      if (AKR < 99.7) {
+        if (!have_sz) {
+          stencil_z(g, AKZ, sz);
+          have_sz = true;
+        }
+        Stencil sx;
+        stencil_x(g, AKR, sx);
+        const double4 t = interp4(g, sx, sz);
+        PD1X = t.x; PD1Z = t.y; PD2X = t.z; PD2Z = t.w;
+      } else {
+        const double EPZ = exp(AKZ);
+        const double SQ = sqrt(DPI / AKR);
+        double SIK, CSK;
+        sincos(AKR - PI4, &SIK, &CSK);
+        PD1Z = PSURR * AKZ - PI * EPZ * SQ * SIK;
+        PD2Z = EPZ * SQ * CSK;
+        const double DSK = 0.5 / AKR;
+        PD1X = -PSURR * AKR + PI * EPZ * SQ * (CSK - DSK * SIK);
+        PD2X = EPZ * SQ * (SIK + DSK * CSK);
+      }
+      VZ1 = PD1Z - PSURR * AKZ;
+      VZ2 = PD2Z;
+      VR1 = -PD1X - PSURR * AKR;
+      VR2 = -PD2X;
+    } else {
+      PD1Z = PSURR * AKZ;
+      PD2Z = 0.;
+      VZ1 = 0.;
+      VZ2 = 0.;
+    }
+    WaveJJ& o = w[b];
+    o.FS1 = PD1Z;
+    o.FS2 = PD2Z;
+    if (RRR > EPS) {
+      const double iR = 1. / RRR;
+      const double CVX = dx * iR, CVY = dy * iR;
+      o.VSX1 = VR1 * CVX;
+      o.VSX2 = VR2 * CVX;
+      o.VSY1 = VR1 * CVY;
+      o.VSY2 = VR2 * CVY;
+    } else {
+      o.VSX1 = o.VSX2 = o.VSY1 = o.VSY2 = 0.;
+    }
+    o.VSZ1 = VZ1;
+    o.VSZ2 = VZ2;
   }
-  w.FS1 = PD1Z;
-  w.FS2 = PD2Z;
-  if (RRR > EPS) {
-    const double iR = 1. / RRR;
-    const double CVX = dx * iR, CVY = dy * iR;
-    w.VSX1 = VR1 * CVX;
-    w.VSX2 = VR2 * CVX;
-    w.VSY1 = VR1 * CVY;
-    w.VSY2 = VR2 * CVY;
-  } else {
-    w.VSX1 = w.VSX2 = w.VSY1 = w.VSY2 = 0.;
-  }
-  w.VSZ1 = VZ1;
-  w.VSZ2 = VZ2;
 }
 
 // --- VSD: exact Rankine panel integral used by the FD free-surface branch --
@@ -504,33 +516,25 @@ struct FdImage {
   double PD1Z, PD2Z, VZ2, PD1X, VR2, PSR;
 };
 
-__device__ __forceinline__ void fd_image(const GreenCtx& g, double AM0, double AKR, double RRR, double ZZZ,
-                                         const Lagrange& LX, bool tab, double PSK, double SCK, double SCDS,
-                                         double SSDS, FdImage& m, bool& bad) {
+__device__ __forceinline__ void fd_image(const GreenCtx& g, double AM0, double AKR, double RRR, double ZZZ, double AKZ,
+                                         const Stencil& sx, const Stencil& sz, bool tab, double PSK, double SCK,
+                                         double SCDS, double SSDS, FdImage& m) {
   const double PI = 3.141592653589793, EPS = 0.0001;
-  const double AKZ = XMUL(AM0, ZZZ);
   const double DD = XSQRT(XADD(XMUL(RRR, RRR), XMUL(ZZZ, ZZZ)));
   double PSURR = 0.;
   m.PSR = 0.;
   if (DD > EPS) {
-    double RRv = AM0 * DD;
-    m.PSR = PI / RRv;
-    PSURR = PI / (RRv * RRv * RRv);
-  }
-  if (AKZ > -1.5E-6) {
-    bad = true;
-    m = FdImage{0, 0, 0, 0, 0, 0};
-    return;
+    const double it = 1. / (AM0 * DD);
+    m.PSR = PI * it;
+    PSURR = m.PSR * it * it;
   }
   if (AKZ > -16.) {
     double PD1X, PD2X;
     if (tab) {
-      Lagrange L = LX;
-      lagrange_z(g, AKZ, L);
-      double4 t = interp4(g, L);
+      const double4 t = interp4(g, sx, sz);
       PD1X = t.x; m.PD1Z = t.y; PD2X = t.z; m.PD2Z = t.w;
     } else {
-      double EPZ = exp(AKZ);
+      const double EPZ = exp(AKZ);
       m.PD1Z = PSURR * AKZ - PSK * EPZ;
       m.PD2Z = EPZ * SCK;
       PD1X = -PSURR * AKR - EPZ * SCDS;
@@ -548,158 +552,224 @@ __device__ __forceinline__ void fd_image(const GreenCtx& g, double AM0, double A
   }
 }
 
-// --- VNSFD for one reflection BX ------------------------------------------
-__device__ __forceinline__ void wave_fd_jj(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
-                                           double ZMIII, int BX, const PanelRec& P, WaveJJ& w) {
+// --- VNSFD tabulated branch, both reflections ------------------------------
+// The four image depths Z1..Z4 (and their AKZ stencils) depend on the depths
+// only and are shared by BX = +1 and -1. |Z1| is the smallest of the four,
+// so AKZ1 <= -16 puts every image in the far branch.
+__device__ __forceinline__ void wave_fd_pair(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
+                                             double ZMIII, const PanelRec& P, int NJJ, WaveJJ* w) {
   const double PI = 3.141592653589793, PI4 = 0.7853981633974483, DPI = 2. * PI, EPS = 0.0001;
-  const double QPI = 4. * PI;
   const double AM0 = om.k0, H = om.h;
-  const double YMJJJ = P.yg * BX;
   const double COF1 = om.coe3 * P.aire, COF2 = om.coe4 * P.aire;
   const double COF3 = AM0 * COF1, COF4 = AM0 * COF2;
-  const double dx = XSUB(XGI, P.xg), dy = XSUB(YGI, YMJJJ);
-  const double RRR = XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy)));
-  const double AKR = XMUL(AM0, RRR);
   const double H2 = XMUL(2., H), H4 = XMUL(4., H);
-  const double Z1 = XADD(ZMIII, P.zg);
-  const double Z2 = XSUB(XSUB(P.zg, ZMIII), H2);
-  const double Z3 = XSUB(XSUB(ZMIII, P.zg), H2);
-  const double Z4 = XSUB(XSUB(-P.zg, ZMIII), H4);
-  const bool tab = AKR < 99.7;
-  Lagrange LX{};
-  double PSK = 0., SCK = 0., SCDS = 0., SSDS = 0.;
-  const double AKZ1 = XMUL(AM0, Z1);
-  if (AKZ1 > -16. && AKZ1 <= -1.5E-6) {
-    if (tab) {
-      lagrange_x(g, AKR, LX);
-    } else {
-      double SQ = sqrt(DPI / AKR), SIK, CSK;
-      sincos(AKR - PI4, &SIK, &CSK);
-      PSK = PI * SQ * SIK;
-      SCK = SQ * CSK;
-      double DSK = 0.5 / AKR;
-      SCDS = PI * SQ * (CSK - DSK * SIK);
-      SSDS = SQ * (SIK + DSK * CSK);
-    }
-  }
+  double Z[4], AKZ[4];
+  Z[0] = XADD(ZMIII, P.zg);
+  Z[1] = XSUB(XSUB(P.zg, ZMIII), H2);
+  Z[2] = XSUB(XSUB(ZMIII, P.zg), H2);
+  Z[3] = XSUB(XSUB(-P.zg, ZMIII), H4);
   bool bad = false;
-  FdImage m1, m2, m3, m4;
-  fd_image(g, AM0, AKR, RRR, Z1, LX, tab, PSK, SCK, SCDS, SSDS, m1, bad);
-  fd_image(g, AM0, AKR, RRR, Z2, LX, tab, PSK, SCK, SCDS, SSDS, m2, bad);
-  fd_image(g, AM0, AKR, RRR, Z3, LX, tab, PSK, SCK, SCDS, SSDS, m3, bad);
-  fd_image(g, AM0, AKR, RRR, Z4, LX, tab, PSK, SCK, SCDS, SSDS, m4, bad);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    AKZ[k] = XMUL(AM0, Z[k]);
+    bad |= AKZ[k] > -1.5E-6;
+  }
   if (bad) {
     set_status(g.status, ST_AKZ_UNDEFINED);
-    w = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
+    w[0] = w[1] = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
     return;
   }
-  w.FS1 = COF1 * ((m1.PD1Z + m2.PD1Z + m3.PD1Z + m4.PD1Z) - m1.PSR - m2.PSR - m3.PSR - m4.PSR);
-  w.FS2 = COF2 * (m1.PD2Z + m2.PD2Z + m3.PD2Z + m4.PD2Z);
-  if (RRR > EPS) {
-    const double C1V3 = -COF3 * (m1.PD1X + m2.PD1X + m3.PD1X + m4.PD1X);
-    const double C2V3 = COF4 * (m1.VR2 + m2.VR2 + m3.VR2 + m4.VR2);
-    const double iR = 1. / RRR;
-    const double CVX = dx * iR, CVY = dy * iR;
-    w.VSX1 = C1V3 * CVX;
-    w.VSX2 = C2V3 * CVX;
-    w.VSY1 = C1V3 * CVY;
-    w.VSY2 = C2V3 * CVY;
-  } else {
-    w.VSX1 = w.VSX2 = w.VSY1 = w.VSY2 = 0.;
+  const bool near = AKZ[0] > -16.;
+  Stencil sz[4];
+  bool have_sz = false;
+#pragma unroll 1
+  for (int b = 0; b < NJJ; ++b) {
+    const double YMJJJ = b ? -P.yg : P.yg;
+    const double dx = XSUB(XGI, P.xg), dy = XSUB(YGI, YMJJJ);
+    const double RRR = XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy)));
+    const double AKR = XMUL(AM0, RRR);
+    const bool tab = AKR < 99.7;
+    Stencil sx{2, 0., 0., 0.};
+    double PSK = 0., SCK = 0., SCDS = 0., SSDS = 0.;
+    if (near) {
+      if (tab) {
+        stencil_x(g, AKR, sx);
+        if (!have_sz) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (AKZ[k] > -16.) stencil_z(g, AKZ[k], sz[k]);
+          have_sz = true;
+        }
+      } else {
+        const double SQ = sqrt(DPI / AKR);
+        double SIK, CSK;
+        sincos(AKR - PI4, &SIK, &CSK);
+        PSK = PI * SQ * SIK;
+        SCK = SQ * CSK;
+        const double DSK = 0.5 / AKR;
+        SCDS = PI * SQ * (CSK - DSK * SIK);
+        SSDS = SQ * (SIK + DSK * CSK);
+      }
+    }
+    FdImage m[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) fd_image(g, AM0, AKR, RRR, Z[k], AKZ[k], sx, sz[k], tab, PSK, SCK, SCDS, SSDS, m[k]);
+    WaveJJ& o = w[b];
+    o.FS1 = COF1 * ((m[0].PD1Z + m[1].PD1Z + m[2].PD1Z + m[3].PD1Z) - m[0].PSR - m[1].PSR - m[2].PSR - m[3].PSR);
+    o.FS2 = COF2 * (m[0].PD2Z + m[1].PD2Z + m[2].PD2Z + m[3].PD2Z);
+    if (RRR > EPS) {
+      const double C1V3 = -COF3 * (m[0].PD1X + m[1].PD1X + m[2].PD1X + m[3].PD1X);
+      const double C2V3 = COF4 * (m[0].VR2 + m[1].VR2 + m[2].VR2 + m[3].VR2);
+      const double iR = 1. / RRR;
+      const double CVX = dx * iR, CVY = dy * iR;
+      o.VSX1 = C1V3 * CVX;
+      o.VSX2 = C2V3 * CVX;
+      o.VSY1 = C1V3 * CVY;
+      o.VSY2 = C2V3 * CVY;
+    } else {
+      o.VSX1 = o.VSX2 = o.VSY1 = o.VSY2 = 0.;
+    }
+    o.VSZ1 = COF3 * (m[0].PD1Z - m[1].PD1Z + m[2].PD1Z - m[3].PD1Z);
+    o.VSZ2 = COF4 * (m[0].VZ2 - m[1].VZ2 + m[2].VZ2 - m[3].VZ2);
   }
-  w.VSZ1 = COF3 * (m1.PD1Z - m2.PD1Z + m3.PD1Z - m4.PD1Z);
-  w.VSZ2 = COF4 * (m1.VZ2 - m2.VZ2 + m3.VZ2 - m4.VZ2);
-  // the exponential images (:635-706) are added by fd_images_kernel
 }
 
-// --- one pair, both symmetry classes --------------------------------------
+// --- VNSFD exponential images (COMPUTE_GREEN_FD.f90:635-706) ----------------
+//   sum_KE AR(KE) (-A/8pi) sum_4 1/rho  and their gradients, per reflection.
+// The reference adds them to FS1, VSX1, VSY1, VSZ1 of each reflection, and
+// those enter SP1/SM1 and the real parts of D+/- linearly (:830-865). Image
+// depths are shared by both reflections; RO > EPS is decided exactly on RO^2
+// against a precomputed threshold.
+__device__ __forceinline__ void fd_exp_images(const GreenCtx& g, double H, const double* ambda, const double* ar,
+                                              int nexp1, double XGI, double YGI, double ZMIII, const PanelRec& P,
+                                              int NJJ, double* fs, double* vx, double* vy, double* vz) {
+  const double QPI = 4. * 3.141592653589793;
+  const double H2 = XMUL(2., H), H4 = XMUL(4., H);
+  const double T2 = g.ro_eps2;
+  double dx[2], dy[2], r2[2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    fs[b] = vx[b] = vy[b] = vz[b] = 0.;
+    dx[b] = XSUB(XGI, P.xg);
+    dy[b] = XSUB(YGI, P.yg * (b ? -1. : 1.));
+    const double R = XSQRT(XADD(XMUL(dx[b], dx[b]), XMUL(dy[b], dy[b])));
+    r2[b] = XMUL(R, R);
+  }
+  const double ACT = -0.5 * P.aire / QPI;
+#pragma unroll 1
+  for (int KE = 1; KE <= nexp1; ++KE) {
+    const double AQT = ACT * ar[KE];
+    const double HA = XMUL(H, ambda[KE]);
+    double zp[4], z2[4];
+    zp[0] = XSUB(XADD(XSUB(ZMIII, H2), HA), P.zg);
+    zp[1] = XSUB(XSUB(-ZMIII, HA), P.zg);
+    zp[2] = XSUB(XADD(XSUB(-ZMIII, H4), HA), P.zg);
+    zp[3] = XSUB(XSUB(XADD(ZMIII, H2), HA), P.zg);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) z2[k] = XMUL(zp[k], zp[k]);
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      if (b >= NJJ) break;
+      double a[4], sa = 0.;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double RRk = XADD(r2[b], z2[k]);
+        if (RRk > T2) {
+          const double ri = rsqrt(RRk);
+          const double FT = AQT * ri;
+          fs[b] += FT;
+          a[k] = FT * ri * ri;
+        } else {
+          a[k] = 0.;
+        }
+        sa += a[k];
+      }
+      vx[b] -= dx[b] * sa;
+      vy[b] -= dy[b] * sa;
+      vz[b] -= zp[0] * a[0] - zp[1] * a[1] - zp[2] * a[2] + zp[3] * a[3];
+    }
+  }
+}
+
+// --- Rankine part of one pair, both symmetry classes -------------------------
+// Real parts of D+/- and S+/- (the wave pass adds the rest). In finite depth
+// this also carries the exponential images of the submerged-panel branch.
+struct RealOut {
+  double dp, dm, sp, sm;
+};
+
 template <bool FD>
-__device__ __forceinline__ void pair_green(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI, double ZGI,
-                                           double XNI, double YNI, double ZNI, bool self, const PanelRec& P,
-                                           PairOut& out) {
+__device__ __forceinline__ void pair_rankine(const GreenCtx& g, const OmegaParams& om, const double* ambda,
+                                             const double* ar, double XGI, double YGI, double ZGI, double XNI,
+                                             double YNI, double ZNI, bool self, const PanelRec& P, RealOut& out) {
   RankineOut r;
   rankine<FD>(g, FD ? XMUL(2., om.h) : 0., XGI, YGI, ZGI, self, P, r);
+  if (FD && ZGI < g.zer && P.zg < g.zer) {
+    const int NJJ = g.nsymy + 1;
+    double fs[2], vx[2], vy[2], vz[2];
+    fd_exp_images(g, om.h, ambda, ar, om.nexp + 1, XGI, YGI, ZGI, P, NJJ, fs, vx, vy, vz);
+    if (NJJ == 2) {
+      r.FSP += fs[0] + fs[1];
+      r.FSM += fs[0] - fs[1];
+      r.VSXP += vx[0] + vx[1];
+      r.VSXM += vx[0] - vx[1];
+      r.VSYP += vy[0] + vy[1];
+      r.VSYM += vy[0] - vy[1];
+      r.VSZP += vz[0] + vz[1];
+      r.VSZM += vz[0] - vz[1];
+    } else {
+      r.FSP += fs[0];
+      r.VSXP += vx[0];
+      r.VSYP += vy[0];
+      r.VSZP += vz[0];
+    }
+  }
+  out.dp = r.VSXP * XNI + r.VSYP * YNI + r.VSZP * ZNI;
+  out.dm = r.VSXM * XNI + r.VSYM * YNI + r.VSZM * ZNI;
+  out.sp = r.FSP;
+  out.sm = r.FSM;
+}
+
+// --- wave part of one pair, both symmetry classes ----------------------------
+template <bool FD>
+__device__ __forceinline__ void pair_wave(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI, double ZGI,
+                                          double XNI, double YNI, double ZNI, const PanelRec& P, PairOut& out) {
   const int NJJ = g.nsymy + 1;
   double ZMIII = ZGI;
   if (ZGI > g.zer) ZMIII = FD ? XMUL(20., g.zer) : g.zer;
-  const bool tabulated = (ZGI < g.zer) && (P.zg < g.zer);
   WaveJJ w[2];
-#pragma unroll
-  for (int JJ = 1; JJ <= 2; ++JJ) {
-    if (JJ > NJJ) break;
-    const int BX = (JJ == 1) ? 1 : -1;
-    if (tabulated) {
-      if (FD) wave_fd_jj(g, om, XGI, YGI, ZMIII, BX, P, w[JJ - 1]);
-      else wave_infd_jj(g, om, XGI, YGI, ZMIII, BX, P, w[JJ - 1]);
-    } else {
+  if ((ZGI < g.zer) && (P.zg < g.zer)) {
+    if (FD) wave_fd_pair(g, om, XGI, YGI, ZMIII, P, NJJ, w);
+    else wave_infd_pair(g, om, XGI, YGI, ZMIII, P, NJJ, w);
+  } else {
+#pragma unroll 1
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
       if (FD) wave_fd_fs(om, XGI, YGI, ZMIII, JJ, P, w[JJ - 1]);
-      else wave_infd_fs(om, XGI, YGI, ZMIII, BX, P, w[JJ - 1]);
+      else wave_infd_fs(om, XGI, YGI, ZMIII, JJ == 1 ? 1 : -1, P, w[JJ - 1]);
     }
   }
-  double SP1, SM1, SP2, SM2, VXP1, VXM1, VYP1, VYM1, VZP1, VZM1, VXP2, VXM2, VYP2, VYM2, VZP2, VZM2;
+  if (NJJ == 1) w[1] = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
+  // VNSINFD (:456-500) scales the wave sums by K A / 2pi^2, K A / 2pi (and K
+  // again for gradients) with a minus sign; VNSFD (:830-865) adds them as they are
+  double s1 = 1., s2 = 1., v1 = 1., v2 = 1.;
   if (!FD) {
-    // VNSINFD combination (:456-500)
     const double DPI = 2. * 3.141592653589793, DPI2 = 2. * 3.141592653589793 * 3.141592653589793;
     const double AKAIR = om.k0 * P.aire;
     const double ADPI2 = AKAIR / DPI2, ADPI = AKAIR / DPI;
-    const double AKDPI2 = ADPI2 * om.k0, AKDPI = ADPI * om.k0;
-    if (NJJ == 2) {
-      SM1 = r.FSM - (w[0].FS1 - w[1].FS1) * ADPI2;
-      SP1 = r.FSP - (w[0].FS1 + w[1].FS1) * ADPI2;
-      SM2 = -(w[0].FS2 - w[1].FS2) * ADPI;
-      SP2 = -(w[0].FS2 + w[1].FS2) * ADPI;
-      VXP1 = r.VSXP - (w[0].VSX1 + w[1].VSX1) * AKDPI2;
-      VXM1 = r.VSXM - (w[0].VSX1 - w[1].VSX1) * AKDPI2;
-      VYP1 = r.VSYP - (w[0].VSY1 + w[1].VSY1) * AKDPI2;
-      VYM1 = r.VSYM - (w[0].VSY1 - w[1].VSY1) * AKDPI2;
-      VZP1 = r.VSZP - (w[0].VSZ1 + w[1].VSZ1) * AKDPI2;
-      VZM1 = r.VSZM - (w[0].VSZ1 - w[1].VSZ1) * AKDPI2;
-      VXP2 = -(w[0].VSX2 + w[1].VSX2) * AKDPI;
-      VXM2 = -(w[0].VSX2 - w[1].VSX2) * AKDPI;
-      VYP2 = -(w[0].VSY2 + w[1].VSY2) * AKDPI;
-      VYM2 = -(w[0].VSY2 - w[1].VSY2) * AKDPI;
-      VZP2 = -(w[0].VSZ2 + w[1].VSZ2) * AKDPI;
-      VZM2 = -(w[0].VSZ2 - w[1].VSZ2) * AKDPI;
-    } else {
-      SP1 = SM1 = r.FSP - w[0].FS1 * ADPI2;
-      SP2 = SM2 = -w[0].FS2 * ADPI;
-      VXP1 = VXM1 = r.VSXP - w[0].VSX1 * AKDPI2;
-      VYP1 = VYM1 = r.VSYP - w[0].VSY1 * AKDPI2;
-      VZP1 = VZM1 = r.VSZP - w[0].VSZ1 * AKDPI2;
-      VXP2 = VXM2 = -w[0].VSX2 * AKDPI;
-      VYP2 = VYM2 = -w[0].VSY2 * AKDPI;
-      VZP2 = VZM2 = -w[0].VSZ2 * AKDPI;
-    }
-  } else {
-    // VNSFD combination (:830-865)
-    if (NJJ == 2) {
-      SM1 = r.FSM + w[0].FS1 - w[1].FS1;
-      SP1 = r.FSP + w[0].FS1 + w[1].FS1;
-      SM2 = w[0].FS2 - w[1].FS2;
-      SP2 = w[0].FS2 + w[1].FS2;
-      VXP1 = r.VSXP + w[0].VSX1 + w[1].VSX1;
-      VXM1 = r.VSXM + w[0].VSX1 - w[1].VSX1;
-      VYP1 = r.VSYP + w[0].VSY1 + w[1].VSY1;
-      VYM1 = r.VSYM + w[0].VSY1 - w[1].VSY1;
-      VZP1 = r.VSZP + w[0].VSZ1 + w[1].VSZ1;
-      VZM1 = r.VSZM + w[0].VSZ1 - w[1].VSZ1;
-      VXP2 = w[0].VSX2 + w[1].VSX2;
-      VXM2 = w[0].VSX2 - w[1].VSX2;
-      VYP2 = w[0].VSY2 + w[1].VSY2;
-      VYM2 = w[0].VSY2 - w[1].VSY2;
-      VZP2 = w[0].VSZ2 + w[1].VSZ2;
-      VZM2 = w[0].VSZ2 - w[1].VSZ2;
-    } else {
-      SP1 = SM1 = r.FSP + w[0].FS1;
-      SP2 = SM2 = w[0].FS2;
-      VXP1 = VXM1 = r.VSXP + w[0].VSX1;
-      VYP1 = VYM1 = r.VSYP + w[0].VSY1;
-      VZP1 = VZM1 = r.VSZP + w[0].VSZ1;
-      VXP2 = VXM2 = w[0].VSX2;
-      VYP2 = VYM2 = w[0].VSY2;
-      VZP2 = VZM2 = w[0].VSZ2;
-    }
+    s1 = -ADPI2;
+    s2 = -ADPI;
+    v1 = -ADPI2 * om.k0;
+    v2 = -ADPI * om.k0;
   }
+  const double BM = (NJJ == 2) ? -1. : 1.;   // minus class: w0 - w1 (w1 = 0 without symmetry)
+  const double SP1 = (w[0].FS1 + w[1].FS1) * s1, SM1 = (w[0].FS1 + BM * w[1].FS1) * s1;
+  const double SP2 = (w[0].FS2 + w[1].FS2) * s2, SM2 = (w[0].FS2 + BM * w[1].FS2) * s2;
+  const double VXP1 = (w[0].VSX1 + w[1].VSX1) * v1, VXM1 = (w[0].VSX1 + BM * w[1].VSX1) * v1;
+  const double VYP1 = (w[0].VSY1 + w[1].VSY1) * v1, VYM1 = (w[0].VSY1 + BM * w[1].VSY1) * v1;
+  const double VZP1 = (w[0].VSZ1 + w[1].VSZ1) * v1, VZM1 = (w[0].VSZ1 + BM * w[1].VSZ1) * v1;
+  const double VXP2 = (w[0].VSX2 + w[1].VSX2) * v2, VXM2 = (w[0].VSX2 + BM * w[1].VSX2) * v2;
+  const double VYP2 = (w[0].VSY2 + w[1].VSY2) * v2, VYM2 = (w[0].VSY2 + BM * w[1].VSY2) * v2;
+  const double VZP2 = (w[0].VSZ2 + w[1].VSZ2) * v2, VZM2 = (w[0].VSZ2 + BM * w[1].VSZ2) * v2;
   out.dp_re = VXP1 * XNI + VYP1 * YNI + VZP1 * ZNI;
   out.dp_im = VXP2 * XNI + VYP2 * YNI + VZP2 * ZNI;
   out.dm_re = VXM1 * XNI + VYM1 * YNI + VZM1 * ZNI;

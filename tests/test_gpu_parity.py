@@ -135,12 +135,12 @@ def test_repeated_frequency_reuses_factorization(solver):
     n1 = solver.launches
     solver.solve_potential(T, nv[:, 1])
     n2 = solver.launches
-    # the second call launches no assembly and no factorization: one assembly
-    # launch, the LU launches (diagonal block, panel and update per 32-column
+    # the second call launches no assembly and no factorization: two assembly
+    # launches (Rankine and wave passes), the LU launches (diagonal block, panel and update per 32-column
     # step; no panel on the last step) and one diagonal-block inversion fewer
     steps = (case.mesh.npanels + 31) // 32
     n_lu = 3 * steps - 1
-    assert (n1 - n0) - (n2 - n1) == 2 + n_lu
+    assert (n1 - n0) - (n2 - n1) == 3 + n_lu
 
 
 def test_degenerate_panel_reports_status(solver):
