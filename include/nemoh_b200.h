@@ -97,7 +97,7 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* ctx, int nomega, const double
  *   1 <= nrhs <= 16; both pointers 16-byte aligned; stream = cudaStream_t.
  * Scratch comes from one static device array of NEMOH_B200_NOALLOC_SCRATCH_BYTES
  * (16 MiB) per device: a call needing more (about
- * nsys*(16 KiB + ceil(n/64)*128 KiB + 16*n*nrhs) bytes) returns
+ * nsys*(48 KiB + ceil(n/64)*128 KiB + 16*n*nrhs) bytes) returns
  * NEMOH_B200_ECAPACITY. The first call on a device does a one-time set-up
  * (symbol lookup, kernel attributes) and should come before any stream
  * capture. All calls on a device share the scratch, so calls that overlap on

@@ -195,7 +195,7 @@ int batch_capacity(nemoh_ctx* c, int nrhs, int want) {
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t N = c->nfa, cls = ncls(c);
   size_t per = (2 * cls * N * N + 2 * cls * N * (size_t)std::max(nrhs, 1)) * sizeof(double2) + sizeof(OmegaParams) +
-               cls * LU_NB * LU_NB * sizeof(double2) + cls * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2);
+               cls * DIAG_SCRATCH * sizeof(double2) + cls * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2);
   if (c->mode == NEMOH_B200_MIXED) per += mixed_bytes_per_system(N) * cls;
   // existing buffers count as available
   size_t have = c->d_D.bytes + c->d_S.bytes + c->d_X.bytes + c->d_Y.bytes + c->d_inv.bytes + c->mixed.bytes();
@@ -212,7 +212,7 @@ void ensure_batch(nemoh_ctx* c, int slots, int nrhs) {
   const size_t rhs = (size_t)slots * cls * N * std::max(nrhs, 1) * sizeof(double2);
   CK(c->d_X.ensure(rhs));
   CK(c->d_Y.ensure(rhs));
-  CK(c->d_diag.ensure((size_t)slots * cls * LU_NB * LU_NB * sizeof(double2)));
+  CK(c->d_diag.ensure((size_t)slots * cls * DIAG_SCRATCH * sizeof(double2)));
   if (c->mode == NEMOH_B200_FP64)
     CK(c->d_inv.ensure((size_t)slots * cls * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
   CK(c->d_oms.ensure((size_t)slots * sizeof(OmegaParams)));
@@ -298,17 +298,12 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
     lu_diag_kernel<double2><<<dim3(1, 1, nsys), 256, 0, c->stream>>>(b, k, c->d_status.as<int>());
     LAUNCHED(c);
-    if (nrb + ncb > 0) {
-      lu_panel_kernel<double2><<<dim3(nrb + ncb, 1, nsys), LU_RB, 0, c->stream>>>(b, k);
+    lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, c->stream>>>(b, k);
+    LAUNCHED(c);
+    if (rest > 0) {
+      zgemm_update<double2>(b, k, nb, Rect{k + nb, N, k + nb, N}, nsys, c->stream);
       LAUNCHED(c);
     }
-    if (rest > 0) {
-      const int t = (rest + GM_T - 1) / GM_T;
-      zgemm_update_kernel<double2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(double2), c->stream>>>(b, k, nb);
-    } else {
-      lu_diag_store_kernel<double2><<<dim3(1, 1, nsys), 256, 0, c->stream>>>(b, k, nb);
-    }
-    LAUNCHED(c);
   }
   static bool attr2 = false;
   if (!attr2) {
@@ -788,8 +783,9 @@ int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5) {
 // Scratch layout (offsets rounded to 256 bytes):
 //   status word (int)                    must be 0 when the factorization starts:
 //                                        the call clears it on its stream first
-//   nsys x 32x32 complex                 factored diagonal block of the current
-//                                        LU step (written before it is read)
+//   nsys x 3 x 32x32 complex             factored diagonal block of the current
+//                                        LU step and the inverses of its two
+//                                        triangles (written before they are read)
 //   nsys x nblk x 2 x 64x64 complex      inverses of the 64x64 diagonal blocks
 //                                        of L and U (written before read)
 //   nsys x n x nrhs complex              intermediate vector of the triangular
@@ -811,7 +807,7 @@ size_t noalloc_align(size_t x) { return (x + 255) & ~size_t(255); }
 // scratch bytes needed for nsys systems of order n with nrhs right-hand sides
 size_t noalloc_bytes(long long n, long long nsys, long long nrhs) {
   const long long nblk = (n + TB - 1) / TB;
-  return noalloc_align(sizeof(int)) + noalloc_align((size_t)nsys * LU_NB * LU_NB * sizeof(double2)) +
+  return noalloc_align(sizeof(int)) + noalloc_align((size_t)nsys * DIAG_SCRATCH * sizeof(double2)) +
          noalloc_align((size_t)(nsys * nblk * 2) * TB * TB * sizeof(double2)) +
          noalloc_align((size_t)(nsys * n * nrhs) * sizeof(double2));
 }
@@ -879,7 +875,7 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
   int* status = reinterpret_cast<int*>(base);
   size_t off = noalloc_align(sizeof(int));
   double2* diag = reinterpret_cast<double2*>(base + off);
-  off += noalloc_align((size_t)nsys * LU_NB * LU_NB * sizeof(double2));
+  off += noalloc_align((size_t)nsys * DIAG_SCRATCH * sizeof(double2));
   double2* inv = reinterpret_cast<double2*>(base + off);
   off += noalloc_align((size_t)(nsys * nblk * 2) * TB * TB * sizeof(double2));
   double2* y = reinterpret_cast<double2*>(base + off);
@@ -893,13 +889,8 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
     const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
     lu_diag_kernel<double2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
-    if (nrb + ncb > 0) lu_panel_kernel<double2><<<dim3(nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k);
-    if (rest > 0) {
-      const int t = (rest + GM_T - 1) / GM_T;
-      zgemm_update_kernel<double2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(double2), st>>>(b, k, nb);
-    } else {
-      lu_diag_store_kernel<double2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, nb);
-    }
+    lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k);
+    if (rest > 0) zgemm_update<double2>(b, k, nb, Rect{k + nb, n, k + nb, n}, nsys, st);
   }
   inv_diag_kernel<double2><<<dim3((unsigned)nblk, 1, nsys), TB, 2 * TB * TB * sizeof(double2), st>>>(b, inv,
                                                                                                       (int)nblk);

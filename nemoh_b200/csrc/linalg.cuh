@@ -5,12 +5,14 @@
 // Here each matrix is factored once as A = L U (L unit lower, U upper) with a
 // blocked right-looking algorithm and the same no-pivot semantics, including
 // the "pivot below 1e-20" stop (M_SOLVER.f90:49-52, 61-64) as a status code.
-// Without pivoting the panel reduces to the small diagonal block plus two
-// triangular solves, so every step is two launches over the whole batch of
-// systems (blockIdx.z = system):
-//   lu_panel_kernel   factor A11 (redundantly per CTA, in shared memory),
-//                     L21 <- A21 U11^-1 and U12 <- L11^-1 A12
-//   zgemm_update      A22 <- A22 - L21 U12
+// Without pivoting a step of width 32 reduces to the small diagonal block and
+// two block products with its inverses (blockIdx.z = system):
+//   lu_diag_kernel    factor A11 once per system, invert L11 and U11
+//   lu_panel_kernel   L21 <- A21 U11^-1, U12 <- L11^-1 A12, store factored A11
+//   zgemm_update      A22 <- A22 - L21 U12 over any rectangle of A22
+// The FP64 path updates the whole trailing matrix after every step; the mixed
+// path (mixed.cuh) defers the update outside a 128-column panel to one
+// tensor-core product per panel.
 #pragma once
 #include "common.cuh"
 
@@ -25,8 +27,9 @@ struct BatchT {
   C2* base;               // system s at base + s * stride
   long long stride;       // elements between systems
   int n;                  // order (leading dimension = n)
-  C2* diag;               // LU_NB*LU_NB scratch per system for the factored diagonal block
+  C2* diag;               // DIAG_SCRATCH elements per system: factored A11, inv(L11), inv(U11)
 };
+constexpr int DIAG_SCRATCH = 3 * LU_NB * LU_NB;
 using Batch = BatchT<double2>;
 
 template <class C2> __device__ __forceinline__ C2 mkc(double x, double y);
@@ -75,8 +78,8 @@ __device__ void factor_block(C2* s, int nb, int* status, bool report) {
 }
 
 // Factor the diagonal block A11 of step k once per system (grid.z = system)
-// into the per-system scratch b.diag; the update kernel of the step stores it
-// back into A (the panel kernel of the same step still reads A11 from there).
+// and invert its triangles. Scratch per system: [LU(A11) | inv(L11) | inv(U11)],
+// column-major nb x nb each (ld = nb). One thread per column inverts.
 template <class C2>
 __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
   __shared__ C2 diag[LU_NB * LU_NB];
@@ -89,46 +92,81 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* 
   }
   __syncthreads();
   factor_block(diag, nb, status, true);
-  C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
+  C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
+  const int t = threadIdx.x;
+  if (t < nb) {
+    // column t of inv(L11): unit lower, forward substitution
+    C2* y = D + LU_NB * LU_NB + nb * t;
+    for (int i = 0; i < nb; ++i) {
+      C2 v = mkc<C2>(i == t ? 1. : 0., 0.);
+      if (i > t)
+        for (int j = t; j < i; ++j) v = cfms(v, diag[i + nb * j], y[j]);
+      else if (i < t)
+        v = mkc<C2>(0., 0.);
+      y[i] = v;
+    }
+  } else if (t >= 32 && t < 32 + nb) {
+    // column c of inv(U11): upper, back substitution
+    const int c = t - 32;
+    C2* y = D + 2 * LU_NB * LU_NB + nb * c;
+    for (int i = nb - 1; i >= 0; --i) {
+      C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
+      if (i <= c) {
+        for (int j = i + 1; j <= c; ++j) v = cfms(v, diag[i + nb * j], y[j]);
+        v = cdv(v, diag[i + nb * i]);
+      } else {
+        v = mkc<C2>(0., 0.);
+      }
+      y[i] = v;
+    }
+  }
 }
 
-// L21 <- A21 U11^-1 (CTAs [0, nrb)) and U12 <- L11^-1 A12 (CTAs [nrb, nrb+ncb))
-// with the factored A11 taken from the scratch written by lu_diag_kernel.
+template <class C2>
+__device__ __forceinline__ void cmac(C2& acc, C2 a, C2 b) {
+  acc.x += a.x * b.x - a.y * b.y;
+  acc.y += a.x * b.y + a.y * b.x;
+}
+
+// L21 <- A21 inv(U11) (CTAs [0, nrb), one thread per row) and
+// U12 <- inv(L11) A12 (CTAs [nrb, nrb+ncb), one thread per column), with the
+// inverses from lu_diag_kernel; CTA 0 also stores the factored A11 into A
+// (no kernel of the step reads A11 from A). Launch with at least one CTA.
 template <class C2>
 __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
-  __shared__ C2 diag[LU_NB * LU_NB];
+  __shared__ C2 inv[LU_NB * LU_NB];
   __shared__ C2 work[LU_NB * LU_CB];
   const int n = b.n;
   const int nb = min(LU_NB, n - k);
   C2* A = b.base + blockIdx.z * b.stride;
-  const C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) diag[q] = D[q];
-  __syncthreads();
+  const C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   const int rest = n - k - nb;
   const int nrb = (rest + LU_RB - 1) / LU_RB;
+  if (blockIdx.x == 0)
+    for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) A[(k + q % nb) + (long long)n * (k + q / nb)] = D[q];
   if (blockIdx.x < nrb) {
-    // L21 rows: x U11 = a, one thread per row
+    for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) inv[q] = D[2 * LU_NB * LU_NB + q];
+    __syncthreads();
     const int r = k + nb + blockIdx.x * LU_RB + threadIdx.x;
     if (r >= n) return;
     C2 x[LU_NB];
 #pragma unroll
     for (int c = 0; c < LU_NB; ++c)
-      if (c < nb) x[c] = A[r + (long long)n * (k + c)];
+      x[c] = (c < nb) ? A[r + (long long)n * (k + c)] : mkc<C2>(0., 0.);
+    // out(c) = sum_{j <= c} x(j) invU(j, c)
 #pragma unroll
     for (int c = 0; c < LU_NB; ++c) {
       if (c < nb) {
-        C2 v = x[c];
+        C2 acc = mkc<C2>(0., 0.);
 #pragma unroll
-        for (int i = 0; i < LU_NB; ++i)
-          if (i < c) v = cfms(v, x[i], diag[i + nb * c]);
-        x[c] = cdv(v, diag[c + nb * c]);
-        A[r + (long long)n * (k + c)] = x[c];
+        for (int j = 0; j <= c; ++j) cmac(acc, x[j], inv[j + nb * c]);
+        A[r + (long long)n * (k + c)] = acc;
       }
     }
     return;
   }
-  // U12 columns: L11 y = a (unit lower), one thread per column
+  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) inv[q] = D[LU_NB * LU_NB + q];
   const int c0 = k + nb + (blockIdx.x - nrb) * LU_CB;
   const int ncol = min(LU_CB, n - c0);
   for (int q = threadIdx.x; q < nb * ncol; q += blockDim.x) {
@@ -137,11 +175,19 @@ __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
   }
   __syncthreads();
   if (threadIdx.x < ncol) {
+    // y(i) = sum_{j <= i} invL(i, j) a(j), in place from the bottom up
     C2* y = work + nb * threadIdx.x;
-    for (int i = 1; i < nb; ++i) {
-      C2 v = y[i];
-      for (int j = 0; j < i; ++j) v = cfms(v, diag[i + nb * j], y[j]);
-      y[i] = v;
+    C2 a[LU_NB];
+#pragma unroll
+    for (int j = 0; j < LU_NB; ++j) a[j] = (j < nb) ? y[j] : mkc<C2>(0., 0.);
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i) {
+      if (i < nb) {
+        C2 acc = a[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) cmac(acc, inv[i + nb * j], a[j]);
+        y[i] = acc;
+      }
     }
   }
   __syncthreads();
@@ -151,60 +197,65 @@ __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
   }
 }
 
-// A22 -= L21 * U12: 64 x 64 output tile per CTA, 16 x 16 threads, 4 x 4 each.
+// A[r0:r1, c0:c1] -= A[r0:r1, k:k+kb] A[k:k+kb, c0:c1]: 64 x 64 output tile
+// per CTA (grid.x over columns, grid.y over rows), 16 x 16 threads, 4 x 4
+// each; the inner dimension is staged through shared memory 32 at a time.
 constexpr int GM_T = 64;
+struct Rect {
+  int r0, r1, c0, c1;
+};
+
 template <class C2>
-__global__ void __launch_bounds__(256) zgemm_update_kernel(BatchT<C2> b, int k, int kb) {
+__global__ void __launch_bounds__(256) zgemm_update_kernel(BatchT<C2> b, int k, int kb, Rect rc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2* As = reinterpret_cast<C2*>(smem_raw);   // [kb][64]
-  C2* Bs = As + LU_NB * GM_T;                 // [kb][64]
+  C2* As = reinterpret_cast<C2*>(smem_raw);   // [32][64]
+  C2* Bs = As + LU_NB * GM_T;                 // [32][64]
   const int n = b.n;
-  const int r0 = k + kb + blockIdx.y * GM_T;
-  const int c0 = k + kb + blockIdx.x * GM_T;
+  const int r0 = rc.r0 + blockIdx.y * GM_T;
+  const int c0 = rc.c0 + blockIdx.x * GM_T;
   C2* A = b.base + blockIdx.z * b.stride;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  if (blockIdx.x == 0 && blockIdx.y == 0) {
-    // store the factored diagonal block of this step (not read by this kernel)
-    const C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
-    for (int q = threadIdx.x; q < kb * kb; q += 256) A[(k + q % kb) + (long long)n * (k + q / kb)] = D[q];
-  }
-  for (int q = threadIdx.x; q < kb * GM_T; q += 256) {
-    const int m = q % GM_T, kk = q / GM_T;
-    const int r = r0 + m;
-    As[kk * GM_T + m] = (r < n) ? A[r + (long long)n * (k + kk)] : mkc<C2>(0., 0.);
-    const int kk2 = q % kb, nn = q / kb;
-    const int c = c0 + nn;
-    Bs[kk2 * GM_T + nn] = (c < n) ? A[(k + kk2) + (long long)n * c] : mkc<C2>(0., 0.);
-  }
-  __syncthreads();
   C2 acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = mkc<C2>(0., 0.);
+  for (int k0 = 0; k0 < kb; k0 += LU_NB) {
+    const int kc = min(LU_NB, kb - k0);
+    if (k0) __syncthreads();
+    for (int q = threadIdx.x; q < kc * GM_T; q += 256) {
+      const int m = q % GM_T, kk = q / GM_T;
+      const int r = r0 + m;
+      As[kk * GM_T + m] = (r < rc.r1) ? A[r + (long long)n * (k + k0 + kk)] : mkc<C2>(0., 0.);
+      const int kk2 = q % kc, nn = q / kc;
+      const int c = c0 + nn;
+      Bs[kk2 * GM_T + nn] = (c < rc.c1) ? A[(k + k0 + kk2) + (long long)n * c] : mkc<C2>(0., 0.);
+    }
+    __syncthreads();
 #pragma unroll 4
-  for (int kk = 0; kk < kb; ++kk) {
-    C2 a[4], bb[4];
+    for (int kk = 0; kk < kc; ++kk) {
+      C2 a[4], bb[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = As[kk * GM_T + ty + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = As[kk * GM_T + ty + 16 * i];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) bb[j] = Bs[kk * GM_T + tx + 16 * j];
+      for (int j = 0; j < 4; ++j) bb[j] = Bs[kk * GM_T + tx + 16 * j];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        acc[i][j].x += a[i].x * bb[j].x - a[i].y * bb[j].y;
-        acc[i][j].y += a[i].x * bb[j].y + a[i].y * bb[j].x;
-      }
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x += a[i].x * bb[j].x - a[i].y * bb[j].y;
+          acc[i][j].y += a[i].x * bb[j].y + a[i].y * bb[j].x;
+        }
+    }
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int c = c0 + tx + 16 * j;
-    if (c >= n) continue;
+    if (c >= rc.c1) continue;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int r = r0 + ty + 16 * i;
-      if (r >= n) continue;
+      if (r >= rc.r1) continue;
       C2* p = A + r + (long long)n * c;
       C2 v = *p;
       v.x -= acc[i][j].x;
@@ -214,12 +265,11 @@ __global__ void __launch_bounds__(256) zgemm_update_kernel(BatchT<C2> b, int k, 
   }
 }
 
-// last step of the factorization has no trailing update: store A11 here
 template <class C2>
-__global__ void lu_diag_store_kernel(BatchT<C2> b, int k, int kb) {
-  C2* A = b.base + blockIdx.z * b.stride;
-  const C2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
-  for (int q = threadIdx.x; q < kb * kb; q += blockDim.x) A[(k + q % kb) + (long long)b.n * (k + q / kb)] = D[q];
+inline void zgemm_update(BatchT<C2> b, int k, int kb, Rect rc, int nsys, cudaStream_t st) {
+  if (rc.r1 <= rc.r0 || rc.c1 <= rc.c0) return;
+  const dim3 grid((rc.c1 - rc.c0 + GM_T - 1) / GM_T, (rc.r1 - rc.r0 + GM_T - 1) / GM_T, nsys);
+  zgemm_update_kernel<C2><<<grid, 256, 2 * LU_NB * GM_T * sizeof(C2), st>>>(b, k, kb, rc);
 }
 
 constexpr int MAX_RHS = 16;

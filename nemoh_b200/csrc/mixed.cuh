@@ -3,9 +3,12 @@
 //
 // x0 = LU32^-1 b;  repeat  r = b - D x (FP64 residual, FP64 matrix D),
 //                          x += LU32^-1 r   until |r|inf <= tol |b|inf.
-// The FP32 factorization reuses the blocked no-pivot LU of linalg.cuh; its
-// trailing updates run on the tensor cores (split-BF16 operands, FP32
-// accumulation) when the tcgen05 path is enabled, else as FP32 SIMT GEMMs.
+// The FP32 factorization is the blocked no-pivot LU of linalg.cuh in two
+// levels: 128-column panels are factored with 32-column steps whose updates
+// stay inside the panel and its row strip (FP32 SIMT), and the rest of the
+// trailing matrix is updated once per panel with K = 128 on the tensor cores
+// (tc_gemm.cuh: split-BF16 operands, FP32 accumulation), or as an FP32 SIMT
+// GEMM when the tcgen05 path is disabled.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -23,7 +26,7 @@ constexpr double REFINE_TOL = 1e-12;
 
 struct MixedWork {
   float2* lu = nullptr;      // FP32 factors, nsys x n x n
-  float2* diag = nullptr;    // panel scratch
+  float2* diag = nullptr;    // diagonal-block scratch (factors and inverses)
   double2* b = nullptr;      // right-hand sides (FP64)
   double2* r = nullptr;      // residual (FP64)
   float2* rf = nullptr;      // residual/correction (FP32)
@@ -51,7 +54,7 @@ struct MixedWork {
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
     cudaError_t e;
     if ((e = cudaMalloc(&lu, nsys * NN * sizeof(float2)))) return e;
-    if ((e = cudaMalloc(&diag, (size_t)nsys * LU_NB * LU_NB * sizeof(float2)))) return e;
+    if ((e = cudaMalloc(&diag, (size_t)nsys * DIAG_SCRATCH * sizeof(float2)))) return e;
     if ((e = cudaMalloc(&b, V * sizeof(double2)))) return e;
     if ((e = cudaMalloc(&r, V * sizeof(double2)))) return e;
     if ((e = cudaMalloc(&rf, V * sizeof(float2)))) return e;
@@ -63,13 +66,15 @@ struct MixedWork {
     cap_sys = nsys;
     cap_n = n;
     cap_rhs = nrhs;
-    total = nsys * NN * sizeof(float2) + V * (2 * sizeof(double2) + 2 * sizeof(float2)) + tc.bytes() + ninv * sizeof(float2);
+    total = nsys * NN * sizeof(float2) + V * (2 * sizeof(double2) + 2 * sizeof(float2)) + tc.bytes() +
+            ninv * sizeof(float2) + (size_t)nsys * DIAG_SCRATCH * sizeof(float2);
     return cudaSuccess;
   }
 };
 
 inline size_t mixed_bytes_per_system(size_t n) {
-  return n * n * sizeof(float2) + tc_bytes_per_system(n) + ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2);
+  return n * n * sizeof(float2) + tc_bytes_per_system(n) + ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2) +
+         DIAG_SCRATCH * sizeof(float2);
 }
 
 __global__ void d2f_kernel(const double2* __restrict__ a, float2* __restrict__ b, long long count) {
@@ -124,23 +129,27 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
   ++launches;
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
-  for (int k = 0; k < n; k += LU_NB) {
-    const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
-    const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-    lu_diag_kernel<float2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
-    ++launches;
-    if (nrb + ncb > 0) {
-      lu_panel_kernel<float2><<<dim3(nrb + ncb, 1, nsys), LU_RB, 0, st>>>(b, k);
+  for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
+    const int kend = std::min(k0 + LU_OUTER, n);
+    for (int k = k0; k < kend; k += LU_NB) {
+      const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
+      const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
+      lu_diag_kernel<float2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
       ++launches;
-    }
-    if (rest > 0) {
-      if (!tc_update(w.tc, b, k, nb, nsys, st, launches, status)) {
-        const int t = (rest + GM_T - 1) / GM_T;
-        zgemm_update_kernel<float2><<<dim3(t, t, nsys), 256, 2 * LU_NB * GM_T * sizeof(float2), st>>>(b, k, nb);
+      lu_panel_kernel<float2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k);
+      ++launches;
+      if (k + nb < kend) {
+        // inside the panel (all rows below) and the panel's row strip right of it
+        zgemm_update<float2>(b, k, nb, Rect{k + nb, n, k + nb, kend}, nsys, st);
         ++launches;
+        if (kend < n) {
+          zgemm_update<float2>(b, k, nb, Rect{k + nb, kend, kend, n}, nsys, st);
+          ++launches;
+        }
       }
-    } else {
-      lu_diag_store_kernel<float2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, nb);
+    }
+    if (kend < n && !tc_update(w.tc, b, k0, nsys, st, launches, status)) {
+      zgemm_update<float2>(b, k0, kend - k0, Rect{kend, n, kend, n}, nsys, st);
       ++launches;
     }
   }

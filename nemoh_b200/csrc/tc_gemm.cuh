@@ -1,23 +1,28 @@
-// Tensor-core trailing update of the FP32 LU (tcgen05, sm_100a).
+// Tensor-core trailing update of the mixed-precision LU (tcgen05, sm_100a).
 //
-// Step k of the blocked LU updates A22 -= L21 * U12 with complex FP32
-// operands and a rank-32 inner dimension. On the tensor cores the complex
-// product is embedded as one real GEMM,
-//     [Re C; Im C] = [[Ar, -Ai], [Ai, Ar]] * [Br; Bi]        (K' = 64),
-// and each operand is split into two BF16 terms x = hi + lo, keeping
-// hi*hi + hi*lo + lo*hi:  A'' = [A_hi, A_hi, A_lo], B'' = [B_hi; B_lo; B_hi]
-// (K'' = 192), which gives ~16-bit operands with FP32 accumulation -- ample
-// for a factorization that only preconditions FP64 iterative refinement.
+// The FP32 LU (mixed.cuh) factors 128-column panels with 32-column steps and
+// then updates the trailing matrix once per panel:
+//     A22 <- A22 - L21 * U12        (complex FP32, inner dimension K = 128).
+// On the tensor cores the complex product becomes real BF16 products with FP32
+// accumulation. A is kept as [Ar | Ai] (K' = 2K real columns) and B as two
+// column blocks, [Br; -Bi] for the real parts and [Bi; Br] for the imaginary
+// parts of the result (N' = 2 x 128), so that
+//     [Re C | Im C] = [Ar | Ai] * [[Br, Bi], [-Bi, Br]].
+// Each operand is split x = hi + lo into two BF16 terms and the product keeps
+// hi*hi + hi*lo + lo*hi (~16-bit operands, FP32 accumulation): the same hi
+// and lo images are reused by three MMAs through their descriptors, so they
+// are stored once.
 //
-// A prep kernel writes A'' and B'' as ready-made shared-memory images
-// (K-major, no swizzle, 8x8 core matrices of 128 bytes), so each CTA moves its
-// operands with two bulk async copies (cp.async.bulk, no tensor map). One CTA
-// computes a 64-complex-row x 128-column tile: one thread issues 12
-// tcgen05.mma (M=128, N=128, K=16, BF16 -> FP32 in TMEM), the accumulator is
-// read back with tcgen05.ld, staged in shared memory as complex values and
-// subtracted from A22 with coalesced read-modify-writes.
+// A prep kernel writes both operands as ready-made shared-memory images
+// (K-major, no swizzle, 8x8 core matrices of 128 bytes) per tile and per
+// chunk of 16 complex k. One CTA computes a 128 x 128 complex tile: thread 0
+// streams the chunks through two shared-memory stages with bulk async copies
+// and issues 6 tcgen05.mma (M=128, N=256, K=16) per chunk into a 256-column
+// TMEM accumulator; afterwards every thread reads its row of the accumulator
+// with tcgen05.ld and subtracts it from A22 with coalesced column accesses.
 // Every wait on an mbarrier is bounded; on timeout the kernel raises a status
-// code, releases its tensor memory and returns.
+// code, waits (bounded) for its copies and MMAs in flight, releases its tensor
+// memory and returns.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -29,18 +34,21 @@
 
 namespace nb200 {
 
-constexpr int TC_ROWS = 64;                     // complex rows per tile (128 real rows)
-constexpr int TC_COLS = 128;                    // columns per tile (MMA N); 2 CTAs per SM
-constexpr int TC_K = 192;                       // K'' = 3 * 2 * LU_NB
-constexpr int TC_SBO = (TC_K / 8) * 128;        // bytes between 8-row core-matrix groups
-constexpr int TC_A_BYTES = 128 * TC_K * 2;      // 48 KB
-constexpr int TC_B_BYTES = TC_COLS * TC_K * 2;  // 48 KB
-constexpr int TC_SMEM = TC_A_BYTES + TC_B_BYTES + 64;
+constexpr int LU_OUTER = 128;                   // panel width of the mixed LU (K of the update)
+constexpr int TC_T = 128;                       // complex rows and columns per tile
+constexpr int TC_KC = 16;                       // complex k per chunk
+constexpr int TC_NCH = LU_OUTER / TC_KC;        // chunks per update
+constexpr int TC_SBO = (2 * TC_KC / 8) * 128;   // 512 bytes between 8-row core-matrix groups
+constexpr int TC_AIMG = TC_T * 2 * TC_KC * 2;   // 8 KB: one A image (hi or lo) of a chunk
+constexpr int TC_BIMG = 2 * TC_T * 2 * TC_KC * 2;   // 16 KB: one B image of a chunk
+constexpr int TC_STAGE = 2 * TC_AIMG + 2 * TC_BIMG;  // 48 KB: A hi, A lo, B hi, B lo
+constexpr int TC_SMEM = 2 * TC_STAGE + 128;
+constexpr int TC_TMEM_COLS = 2 * TC_T;          // accumulator: Re in [0,128), Im in [128,256)
 constexpr int ST_TC_TIMEOUT = 30;
 
 struct TcWork {
-  unsigned char* a = nullptr;   // A'' tiles, nsys x ceil(n/64) x 48 KB
-  unsigned char* b = nullptr;   // B'' tiles, nsys x ceil(n/128) x 48 KB
+  unsigned char* a = nullptr;   // A images: nsys x ceil(n/128) row tiles x TC_NCH chunks x (hi, lo)
+  unsigned char* b = nullptr;   // B images: nsys x ceil(n/128) column tiles x TC_NCH chunks x (hi, lo)
   int cap_sys = 0, cap_n = 0;
   size_t total = 0;
   size_t bytes() const { return total; }
@@ -54,88 +62,100 @@ struct TcWork {
   cudaError_t ensure(int nsys, int n) {
     if (nsys <= cap_sys && n <= cap_n) return cudaSuccess;
     release();
-    const size_t ta = (size_t)(n + TC_ROWS - 1) / TC_ROWS, tb = (size_t)(n + TC_COLS - 1) / TC_COLS;
+    const size_t t = (size_t)(n + TC_T - 1) / TC_T;
     cudaError_t e;
-    if ((e = cudaMalloc(&a, nsys * ta * TC_A_BYTES))) return e;
-    if ((e = cudaMalloc(&b, nsys * tb * TC_B_BYTES))) return e;
+    if ((e = cudaMalloc(&a, nsys * t * TC_NCH * 2 * TC_AIMG))) return e;
+    if ((e = cudaMalloc(&b, nsys * t * TC_NCH * 2 * TC_BIMG))) return e;
     cap_sys = nsys;
     cap_n = n;
-    total = nsys * (ta * TC_A_BYTES + tb * TC_B_BYTES);
+    total = nsys * t * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG);
     return cudaSuccess;
   }
 };
 
 inline size_t tc_bytes_per_system(size_t n) {
-  return ((n + TC_ROWS - 1) / TC_ROWS) * TC_A_BYTES + ((n + TC_COLS - 1) / TC_COLS) * TC_B_BYTES;
+  return ((n + TC_T - 1) / TC_T) * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG);
 }
 
-// byte offset of element (row, kk) in a K-major no-swizzle operand image
-__device__ __forceinline__ int tc_off(int row, int kk) {
-  return (row & 7) * 16 + (row >> 3) * TC_SBO + (kk >> 3) * 128 + (kk & 7) * 2;
+// byte offset of the 16-byte core-matrix row (row, k-group g) in an image
+__device__ __forceinline__ int tc_row_off(int row, int g) { return (row & 7) * 16 + (row >> 3) * TC_SBO + g * 128; }
+
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) {
+  return (uint32_t)__bfloat16_as_ushort(v.x) | ((uint32_t)__bfloat16_as_ushort(v.y) << 16);
 }
 
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(x);
-  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-}
-
-// Build A'' (from L21) and B'' (from U12) for step k; also store the factored
-// diagonal block parked by lu_panel_kernel. grid.z = system.
-__global__ void tc_prep_kernel(BatchT<float2> b, int k, unsigned char* __restrict__ abuf,
-                               unsigned char* __restrict__ bbuf, long long a_sys, long long b_sys) {
-  const int n = b.n, nb = LU_NB, r0 = k + nb, rest = n - r0;
-  float2* A = b.base + blockIdx.z * b.stride;
-  const int ta = (rest + TC_ROWS - 1) / TC_ROWS, tb = (rest + TC_COLS - 1) / TC_COLS;
-  unsigned char* ab = abuf + blockIdx.z * a_sys;
-  unsigned char* bb = bbuf + blockIdx.z * b_sys;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  if (blockIdx.x == 0) {
-    const float2* D = b.diag + (long long)blockIdx.z * LU_NB * LU_NB;
-    for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) A[(k + q % nb) + (long long)n * (k + q / nb)] = D[q];
-  }
-  // A'': one complex element L21(r, j) -> 12 BF16 values
-  const long long na = (long long)ta * TC_ROWS * nb;
-  for (long long q = tid; q < na; q += nth) {
-    const int rr = (int)(q % (ta * TC_ROWS)), j = (int)(q / (ta * TC_ROWS));
-    const int t = rr / TC_ROWS, row = rr % TC_ROWS;
-    float2 v = make_float2(0.f, 0.f);
-    if (rr < rest) v = A[(r0 + rr) + (long long)n * (k + j)];
-    __nv_bfloat16 rh, rl, ih, il, nih, nil;
-    split_bf16(v.x, rh, rl);
-    split_bf16(v.y, ih, il);
-    nih = __hneg(ih);
-    nil = __hneg(il);
-    unsigned char* tile = ab + (long long)t * TC_A_BYTES;
-    // real-part row: [Ar, -Ai]; imaginary-part row (row + 64): [Ai, Ar]
-    const int re = row, im = row + TC_ROWS;
+// eight consecutive values -> BF16 hi terms and BF16 lo = x - hi terms, packed
+// in k order (element 0 in the low half of the first word)
+__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
+  uint32_t h[4], l[4];
 #pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      const bool lo = (s == 2);
-      const int kb = 64 * s;
-      *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(re, kb + j)) = lo ? rl : rh;
-      *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(re, kb + 32 + j)) = lo ? nil : nih;
-      *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(im, kb + j)) = lo ? il : ih;
-      *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(im, kb + 32 + j)) = lo ? rl : rh;
-    }
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+    const float2 hf = __bfloat1622float2(h2);
+    h[i] = bf2_bits(h2);
+    l[i] = bf2_bits(__floats2bfloat162_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y));
   }
-  // B'': one complex element U12(j, c) -> 6 BF16 values in column c's K vector
-  const long long nbv = (long long)tb * TC_COLS * nb;
-  for (long long q = tid; q < nbv; q += nth) {
-    const int j = (int)(q % nb), cc = (int)(q / nb);
-    const int t = cc / TC_COLS, col = cc % TC_COLS;
-    float2 v = make_float2(0.f, 0.f);
-    if (cc < rest) v = A[(k + j) + (long long)n * (r0 + cc)];
-    __nv_bfloat16 rh, rl, ih, il;
-    split_bf16(v.x, rh, rl);
-    split_bf16(v.y, ih, il);
-    unsigned char* tile = bb + (long long)t * TC_B_BYTES;
-    // [B_hi; B_lo; B_hi] with B' = [Br; Bi]
-    *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(col, j)) = rh;
-    *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(col, 32 + j)) = ih;
-    *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(col, 64 + j)) = rl;
-    *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(col, 96 + j)) = il;
-    *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(col, 128 + j)) = rh;
-    *reinterpret_cast<__nv_bfloat16*>(tile + tc_off(col, 160 + j)) = ih;
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// Operand images of the outer update after the panel [k0, k0 + 128):
+// L21 = A[r1:n, k0:k0+128] and U12 = A[k0:k0+128, r1:n] with r1 = k0 + 128.
+// Thread per (row or column of the tile, chunk); blocks [0, na) do A, the rest B.
+__global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, unsigned char* __restrict__ abuf,
+                                                       unsigned char* __restrict__ bbuf, long long sys_bytes_a,
+                                                       long long sys_bytes_b, int na) {
+  const int n = b.n, r1 = k0 + LU_OUTER, rest = n - r1;
+  const int nt = (rest + TC_T - 1) / TC_T;
+  const float2* A = b.base + blockIdx.z * b.stride;
+  const bool isA = (int)blockIdx.x < na;
+  const int q = (isA ? blockIdx.x : blockIdx.x - na) * blockDim.x + threadIdx.x;
+  if (q >= nt * TC_T * TC_NCH) return;
+  const int ch = q / (nt * TC_T), rr = q % (nt * TC_T);   // consecutive threads: consecutive rows/columns
+  const int t = rr / TC_T, row = rr % TC_T;
+  const int kb = k0 + ch * TC_KC;
+  float re[TC_KC], im[TC_KC];
+  if (isA) {
+    const int r = r1 + rr;
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) {
+      const float2 v = (r < n) ? A[r + (long long)n * (kb + j)] : make_float2(0.f, 0.f);
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    unsigned char* img = abuf + blockIdx.z * sys_bytes_a + ((long long)t * TC_NCH + ch) * 2 * TC_AIMG;
+    uint4 h, l;
+    // k-groups: 0,1 = Re(k 0..15), 2,3 = Im(k 0..15)
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      split8((g < 2 ? re : im) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_AIMG + tc_row_off(row, g)) = l;
+    }
+  } else {
+    const int c = r1 + rr;
+    const float2* col = A + (long long)n * c + kb;
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) {
+      const float2 v = (c < n) ? col[j] : make_float2(0.f, 0.f);
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    float nim[TC_KC];
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) nim[j] = -im[j];
+    unsigned char* img = bbuf + blockIdx.z * sys_bytes_b + ((long long)t * TC_NCH + ch) * 2 * TC_BIMG;
+    uint4 h, l;
+    // B row `row` (real parts of the result): [Br; -Bi]; row 128+row (imaginary parts): [Bi; Br]
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      split8((g < 2 ? re : nim) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(row, g)) = l;
+      split8((g < 2 ? im : re) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(TC_T + row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(TC_T + row, g)) = l;
+    }
   }
 }
 
@@ -179,31 +199,53 @@ __host__ __device__ constexpr uint32_t tc_idesc() {
   return (1u << 4)                    // D format F32
          | (1u << 7)                  // A format BF16
          | (1u << 10)                 // B format BF16
-         | ((uint32_t)(TC_COLS >> 3) << 17)
+         | ((uint32_t)((2 * TC_T) >> 3) << 17)
          | ((uint32_t)(128 >> 4) << 24);
 }
 
-__global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int k, const unsigned char* __restrict__ abuf,
-                                                           const unsigned char* __restrict__ bbuf, long long a_sys,
-                                                           long long b_sys, int* status) {
+__device__ __forceinline__ void tc_load_chunk(uint32_t dst, const unsigned char* ga, const unsigned char* gb,
+                                              uint32_t bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TC_STAGE) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(ga), "r"(2 * TC_AIMG), "r"(bar)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst + 2 * TC_AIMG),
+               "l"(gb), "r"(2 * TC_BIMG), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(tc_idesc()), "r"(acc)
+      : "memory");
+}
+
+// A[r1:n, r1:n] -= L21 U12 for the panel [k0, k0+128), r1 = k0 + 128.
+// grid = (column tiles, row tiles, systems), 128 threads, TC_SMEM dynamic smem.
+__global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int k0,
+                                                           const unsigned char* __restrict__ abuf,
+                                                           const unsigned char* __restrict__ bbuf,
+                                                           long long sys_bytes_a, long long sys_bytes_b, int* status) {
   extern __shared__ __align__(128) unsigned char smem[];
-  unsigned char* sA = smem;
-  unsigned char* sB = smem + TC_A_BYTES;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TC_A_BYTES + TC_B_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
-  const int n = b.n, r0 = k + LU_NB, rest = n - r0;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * TC_STAGE);   // full[2], empty[2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
+  __shared__ int s_ok;
+  const int n = b.n, r1 = k0 + LU_OUTER, rest = n - r1;
   const int tcol = blockIdx.x, trow = blockIdx.y;
-  const int warp = threadIdx.x >> 5;
-  const uint32_t bar_load = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
 
   if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_load));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_mma));
+    for (int i = 0; i < 4; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[i])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TC_COLS));
+                 "r"(TC_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -211,159 +253,142 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  bool ok = true;
   if (threadIdx.x == 0) {
-    const unsigned char* ga = abuf + blockIdx.z * a_sys + (long long)trow * TC_A_BYTES;
-    const unsigned char* gb = bbuf + blockIdx.z * b_sys + (long long)tcol * TC_B_BYTES;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_load),
-                 "r"(TC_A_BYTES + TC_B_BYTES)
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(sA)),
-                 "l"(ga), "r"(TC_A_BYTES), "r"(bar_load)
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(sB)),
-                 "l"(gb), "r"(TC_B_BYTES), "r"(bar_load)
-                 : "memory");
-    ok = mbar_wait(bar_load, 0);
-    if (ok) {
+    bool ok = true;
+    const unsigned char* ga = abuf + blockIdx.z * sys_bytes_a + (long long)trow * TC_NCH * 2 * TC_AIMG;
+    const unsigned char* gb = bbuf + blockIdx.z * sys_bytes_b + (long long)tcol * TC_NCH * 2 * TC_BIMG;
+    const uint32_t s0 = smem_u32(smem);
+    tc_load_chunk(s0, ga, gb, full0);
+    tc_load_chunk(s0 + TC_STAGE, ga + 2 * TC_AIMG, gb + 2 * TC_BIMG, full0 + 8);
+    int issued = 2;      // chunks whose loads were issued
+    int committed = 0;   // chunks whose MMAs were committed
+    for (int c = 0; c < TC_NCH && ok; ++c) {
+      const int s = c & 1;
+      const uint32_t par = (uint32_t)((c >> 1) & 1);
+      ok = mbar_wait(full0 + 8 * s, par);
+      if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t idesc = tc_idesc();
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      const uint32_t st = s0 + s * TC_STAGE;
+      const uint32_t ahi = st, alo = st + TC_AIMG, bhi = st + 2 * TC_AIMG, blo = bhi + TC_BIMG;
 #pragma unroll
-      for (int kk = 0; kk < TC_K / 16; ++kk) {
-        const uint64_t da = umma_desc(a0 + kk * 256, 128, TC_SBO);
-        const uint64_t db = umma_desc(b0 + kk * 256, 128, TC_SBO);
-        const uint32_t acc = kk > 0 ? 1u : 0u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-            ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
-            : "memory");
+      for (int kk = 0; kk < 2; ++kk) {
+        const uint32_t o = kk * 256;
+        tc_mma(tmem, umma_desc(ahi + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), (c > 0 || kk > 0) ? 1u : 0u);
+        tc_mma(tmem, umma_desc(ahi + o, 128, TC_SBO), umma_desc(blo + o, 128, TC_SBO), 1u);
+        tc_mma(tmem, umma_desc(alo + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), 1u);
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_mma)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(empty0 + 8 * s)
                    : "memory");
-      ok = mbar_wait(bar_mma, 0);
-    } else {
-      mbar_wait(bar_load, 0);   // give copies still in flight a second bounded chance to land
+      committed = c + 1;
+      // refill the stage of chunk c-1 with chunk c+1 once its MMAs are done
+      if (c >= 1 && c + 1 < TC_NCH && issued == c + 1) {
+        const int sp = (c - 1) & 1;
+        ok = mbar_wait(empty0 + 8 * sp, (uint32_t)(((c - 1) >> 1) & 1));
+        if (!ok) break;
+        tc_load_chunk(s0 + sp * TC_STAGE, ga + (long long)(c + 1) * 2 * TC_AIMG, gb + (long long)(c + 1) * 2 * TC_BIMG,
+                      full0 + 8 * sp);
+        ++issued;
+      }
     }
-    if (!ok) atomicCAS(status, 0, ST_TC_TIMEOUT);
+    if (ok) {
+      // the last commit arrives when every MMA issued before it has completed
+      const int c = TC_NCH - 1;
+      ok = mbar_wait(empty0 + 8 * (c & 1), (uint32_t)((c >> 1) & 1));
+    }
+    if (!ok) {
+      atomicCAS(status, 0, ST_TC_TIMEOUT);
+      // give copies and MMAs still in flight a second bounded chance to finish
+      for (int c = committed; c < issued; ++c) mbar_wait(full0 + 8 * (c & 1), (uint32_t)((c >> 1) & 1));
+      if (committed > 0) {
+        const int c = committed - 1;
+        mbar_wait(empty0 + 8 * (c & 1), (uint32_t)((c >> 1) & 1));
+      }
+    }
+    s_ok = ok ? 1 : 0;
   }
-  // broadcast the outcome of thread 0's waits
-  __shared__ int s_ok;
-  if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
   __syncthreads();
-  ok = s_ok != 0;
-  if (ok) {
+  if (s_ok) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    // TMEM -> registers -> shared memory, real and imaginary parts as separate
-    // [col][row] float planes (reusing the operand area; conflict-free stores)
-    float* sre = reinterpret_cast<float*>(smem);
-    float* sim = sre + TC_COLS * TC_ROWS;
-    const int trow_l = warp * 32 + (threadIdx.x & 31);  // accumulator row of this thread
-    float* plane = trow_l >= TC_ROWS ? sim : sre;
-    const int crow = trow_l & (TC_ROWS - 1);
-    __syncthreads();
+    // row `row` of the tile = TMEM lane; columns [0,128) real, [128,256) imaginary
+    const int row = warp * 32 + lane;
+    const int gr = r1 + trow * TC_T + row;
+    float2* A = b.base + blockIdx.z * b.stride;
+    const int cbase = r1 + tcol * TC_T;
+    const int ncol = min(TC_T, rest - tcol * TC_T);
 #pragma unroll 1
-    for (int chunk = 0; chunk < TC_COLS / 32; ++chunk) {
-      uint32_t v[32];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(chunk * 32);
+    for (int q = 0; q < TC_T / 32; ++q) {
+      if (32 * q >= ncol) break;
+      uint32_t vr[32], vi[32];
+      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(32 * q);
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
           "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
-            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-            "=r"(v[30]), "=r"(v[31])
-          : "r"(taddr));
+          : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]), "=r"(vr[7]),
+            "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]), "=r"(vr[14]),
+            "=r"(vr[15]), "=r"(vr[16]), "=r"(vr[17]), "=r"(vr[18]), "=r"(vr[19]), "=r"(vr[20]), "=r"(vr[21]),
+            "=r"(vr[22]), "=r"(vr[23]), "=r"(vr[24]), "=r"(vr[25]), "=r"(vr[26]), "=r"(vr[27]), "=r"(vr[28]),
+            "=r"(vr[29]), "=r"(vr[30]), "=r"(vr[31])
+          : "r"(ta));
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]), "=r"(vi[7]),
+            "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]), "=r"(vi[14]),
+            "=r"(vi[15]), "=r"(vi[16]), "=r"(vi[17]), "=r"(vi[18]), "=r"(vi[19]), "=r"(vi[20]), "=r"(vi[21]),
+            "=r"(vi[22]), "=r"(vi[23]), "=r"(vi[24]), "=r"(vi[25]), "=r"(vi[26]), "=r"(vi[27]), "=r"(vi[28]),
+            "=r"(vi[29]), "=r"(vi[30]), "=r"(vi[31])
+          : "r"(ta + (uint32_t)TC_T));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (gr < n) {
+        float2 cur[32];
+        float2* p = A + gr + (long long)n * (cbase + 32 * q);
 #pragma unroll
-      for (int j = 0; j < 32; ++j) plane[(chunk * 32 + j) * TC_ROWS + crow] = __uint_as_float(v[j]);
-    }
-    __syncthreads();
-    // read-modify-write of the 64 x 128 tile of A22: warp w takes columns
-    // w, w+4, ...; lane l takes rows 2l, 2l+1 (one 16-byte access when the
-    // order n is even, so that every column starts 16-byte aligned). Sixteen
-    // columns' loads are issued before any is used, to keep memory busy.
-    float2* A = b.base + blockIdx.z * b.stride;
-    const int lane = threadIdx.x & 31;
-    const int gr = trow * TC_ROWS + 2 * lane;
-    const int ncol = min(TC_COLS, rest - tcol * TC_COLS);
-    const bool pair = (gr + 1 < rest) && ((n & 1) == 0);
-    constexpr int UNR = 16;
-    for (int c0 = warp; c0 < ncol; c0 += 4 * UNR) {
-      float4 cur[UNR];
+        for (int j = 0; j < 32; ++j)
+          if (32 * q + j < ncol) cur[j] = p[(long long)n * j];
 #pragma unroll
-      for (int u = 0; u < UNR; ++u) {
-        const int c = c0 + 4 * u;
-        if (c < ncol && gr < rest) {
-          float2* p = A + (r0 + gr) + (long long)n * (r0 + tcol * TC_COLS + c);
-          if (pair) cur[u] = *reinterpret_cast<const float4*>(p);
-          else cur[u] = make_float4(p[0].x, p[0].y, 0.f, 0.f);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < UNR; ++u) {
-        const int c = c0 + 4 * u;
-        if (c < ncol && gr < rest) {
-          float2* p = A + (r0 + gr) + (long long)n * (r0 + tcol * TC_COLS + c);
-          const int q = c * TC_ROWS + 2 * lane;
-          float4 o = cur[u];
-          o.x -= sre[q];
-          o.y -= sim[q];
-          if (pair) {
-            o.z -= sre[q + 1];
-            o.w -= sim[q + 1];
-            *reinterpret_cast<float4*>(p) = o;
-          } else {
-            p[0] = make_float2(o.x, o.y);
-            if (gr + 1 < rest) {
-              float2 t = p[1];
-              t.x -= sre[q + 1];
-              t.y -= sim[q + 1];
-              p[1] = t;
-            }
+        for (int j = 0; j < 32; ++j)
+          if (32 * q + j < ncol) {
+            float2 v = cur[j];
+            v.x -= __uint_as_float(vr[j]);
+            v.y -= __uint_as_float(vi[j]);
+            p[(long long)n * j] = v;
           }
-        }
       }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS));
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
+// NEMOH_B200_TC=0 selects the CUDA-core FP32 update instead (for comparison)
 inline bool tc_enabled() {
-  static int on = -1;
-  if (on < 0) {
+  static const bool on = [] {
     const char* e = std::getenv("NEMOH_B200_TC");
-    on = (e && e[0] == '0') ? 0 : 1;
-  }
-  return on == 1;
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
-// Trailing update of step k on the tensor cores. Returns false when the
-// SIMT update should be used instead (disabled, or no trailing matrix).
-inline bool tc_update(TcWork& w, BatchT<float2> b, int k, int nb, int nsys, cudaStream_t st, long long& launches,
+// outer trailing update after the panel [k0, k0+128); false if disabled
+inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
                       int* status) {
-  const int rest = b.n - k - nb;
-  if (!tc_enabled() || rest <= 0 || nb != LU_NB || !w.a) return false;
+  if (!tc_enabled()) return false;
+  const int n = b.n, rest = n - k0 - LU_OUTER;
+  if (rest <= 0) return true;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) != cudaSuccess)
-      return false;
+    cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
     attr = true;
   }
-  const long long a_sys = (long long)((w.cap_n + TC_ROWS - 1) / TC_ROWS) * TC_A_BYTES;
-  const long long b_sys = (long long)((w.cap_n + TC_COLS - 1) / TC_COLS) * TC_B_BYTES;
-  const int ta = (rest + TC_ROWS - 1) / TC_ROWS, tb = (rest + TC_COLS - 1) / TC_COLS;
-  tc_prep_kernel<<<dim3(std::max(1, std::min(64, ta * 2)), 1, nsys), 256, 0, st>>>(b, k, w.a, w.b, a_sys, b_sys);
+  const int t = (n + TC_T - 1) / TC_T;
+  const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
+  const int nt = (rest + TC_T - 1) / TC_T;
+  const int per = (nt * TC_T * TC_NCH + 127) / 128;
+  tc_prep_kernel<<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
   ++launches;
-  tc_update_kernel<<<dim3(tb, ta, nsys), 128, TC_SMEM, st>>>(b, k, w.a, w.b, a_sys, b_sys, status);
+  tc_update_kernel<<<dim3(nt, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status);
   ++launches;
   return true;
 }
