@@ -198,6 +198,100 @@ def rel_err_families(F, F64, nbeta):
     return float(err.max()), float(np.median(err))
 
 
+def _body_inputs(case):
+    from nemoh_b200 import cases as C
+    nw = len(case.omegas)
+    nv = C.body_conditions(case)
+    npb = len(case.betas_deg) + len(case.rad)
+    nvel = np.asfortranarray(nv.reshape(nv.shape[0], nw, npb).transpose(0, 2, 1))
+    return nvel, np.asfortranarray(C.generalised_normals(case))
+
+
+def run_batched(local, n_bodies, n_omega=20, seed=4):
+    """Batched workload: n_bodies bodies from the seeded generator (cylinder, box
+    or sphere, 200..3000 panels, infinite or 20..200 m depth), 20 frequencies
+    0.1..2.5 rad/s, 6 DOF + heading 0 each; every body's frequencies are one
+    batched call through the host C-ABI (copies included), bodies in order of
+    decreasing panel count so that the workspace is allocated once."""
+    import nemoh_b200 as nb
+    from nemoh_b200 import cases as C
+    rng = np.random.default_rng(seed)
+    omegas = np.linspace(0.1, 2.5, n_omega)
+    bodies = []
+    for _ in range(n_bodies):
+        mesh, depth = C.random_body(rng)
+        case = C.Case(mesh, omegas, np.array([0.0]), C.six_dofs(), C.six_dofs(), depth=depth)
+        bodies.append((case,) + _body_inputs(case))
+    bodies.sort(key=lambda b: -b[0].mesh.npanels)
+    out, F = {}, {}
+    for label, mode in (("fp64", nb.FP64), ("mixed", nb.MIXED)):
+        with nb.Solver(local, mode) as s:
+            s.set_case(bodies[0][0])
+            s.solve_frequencies(omegas[:1], bodies[0][1][:, :, :1], bodies[0][2])   # workspace + warm-up
+            t0 = time.perf_counter()
+            res, fallbacks = [], 0
+            for case, nvel, nds in bodies:
+                s.set_case(case)
+                res.append(s.solve_frequencies(omegas, nvel, nds))
+                fallbacks += mode == nb.MIXED and s.last_refinement()[0] < 0
+            dt = time.perf_counter() - t0
+        F[label] = res
+        out[label + "_solves_per_s"] = n_bodies * n_omega / dt
+        out[label + "_s"] = dt
+        if mode == nb.MIXED:
+            out["mixed_fp64_fallback_bodies"] = int(fallbacks)
+    errs = [rel_err_families(a, b, 1)[0] for a, b in zip(F["mixed"], F["fp64"])]
+    npan = [b[0].mesh.npanels for b in bodies]
+    out.update({"bodies": n_bodies, "omegas_per_body": n_omega, "solves": n_bodies * n_omega,
+                "panels_min": int(min(npan)), "panels_max": int(max(npan)), "panels_median": float(np.median(npan)),
+                "finite_depth_bodies": int(sum(b[0].depth > 0 for b in bodies)),
+                "mixed_speedup": out["fp64_s"] / out["mixed_s"], "mixed_vs_fp64_max_rel_err": float(max(errs)),
+                "timing": "host wall clock around the whole batch, host<->device copies included"})
+    return out
+
+
+def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9), seed=5, n_check=64, workers=4):
+    """Serving workload: Poisson request streams over the batched workload's
+    bodies (one omega U(0.1, 2.5), heading U(0, 180) deg, 6 DOF per request)
+    through the continuous-batching server. The saturation throughput is the
+    rate achieved on a stream offered well above capacity; streams at fractions
+    of it then give the latency percentiles."""
+    import nemoh_b200 as nb
+    from nemoh_b200 import serving as S
+    bodies = S.make_bodies(n_bodies, seed=4)
+    srv = S.SolveServer(bodies, device=local, precision=nb.MIXED, workers=workers)
+    try:
+        srv.run(S.make_requests(min(64, n_req), 0, n_bodies, seed=seed + 100), realtime=False)   # warm-up
+        done, wall = srv.run(S.make_requests(n_req, 5000.0, n_bodies, seed=seed))
+        sat = len(done) / wall
+        out = {"bodies": n_bodies, "requests_per_rate": n_req, "workers": workers, "precision": "mixed",
+               "saturation_solves_per_s": sat, "rates": []}
+        last = None
+        for f in rates:
+            done, wall = srv.run(S.make_requests(n_req, f * sat, n_bodies, seed=seed + int(100 * f)))
+            st = S.latency_stats(done, wall)
+            st.update({"rate_frac": f, "offered_per_s": f * sat})
+            out["rates"].append(st)
+            last = done
+    finally:
+        srv.close()
+    # per-request error against the FP64 path on a sample of the last stream
+    worst = 0.0
+    with nb.Solver(local, nb.FP64) as s:
+        for r in sorted(last, key=lambda r: r.rid)[:n_check]:
+            b = bodies[r.body]
+            s.set_case(b.case)
+            f64 = s.solve_frequencies(np.array([r.omega]), b.rhs(r.omega, r.beta_deg)[:, :, None], b.nds)[:, :, 0]
+            a = np.abs(f64)
+            floor = np.maximum(a, 1e-6 * np.maximum(a[:, :6].max(axis=1, keepdims=True),
+                                                    a[:, 6:].max(axis=1, keepdims=True)))
+            worst = max(worst, float((np.abs(r.force - f64) / floor).max()))
+    out["mixed_vs_fp64_max_rel_err"] = worst
+    out["checked_requests"] = min(n_check, len(last))
+    out["latency"] = "host clock from arrival to result ready"
+    return out
+
+
 def run_ours(args):
     import torch
     import nemoh_b200 as nb
@@ -328,6 +422,16 @@ def run_ours(args):
                                           "steps at N=2400 for one finite-depth and one deep-water omega "
                                           "(%.0f s total), extrapolated by operation counts to 40 omega" %
                                           args.cpu_seconds}
+    for r in results.values():
+        r["solver"].close()
+    results = {}
+    if rank == 0 and not args.no_extras:
+        for key, fn in (("batched", lambda: run_batched(local, args.bodies)),
+                        ("serve", lambda: run_serving(local, args.bodies, args.requests))):
+            try:
+                line[key] = fn()
+            except Exception as e:   # reported in the line; the headline stands on its own
+                line[key] = {"error": "%s: %s" % (type(e).__name__, e)}
     if rank == 0:
         print(json.dumps(line))
     for r in results.values():
@@ -345,6 +449,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=16.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--omegas", type=int, default=N_OMEGA, help="frequency subset (profiling only)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving workloads")
+    ap.add_argument("--bodies", type=int, default=256, help="bodies of the batched and serving workloads")
+    ap.add_argument("--requests", type=int, default=1000, help="requests per serving rate")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

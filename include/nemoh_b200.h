@@ -119,7 +119,10 @@ int nemoh_b200_get_tables(nemoh_ctx* ctx, double* xr, double* xz, double* apd);
 int nemoh_b200_get_geometry(nemoh_ctx* ctx, double* out, double* zer);
 /* timing of the last solve_frequencies call: assembly, factorization, solve+potential+forces (ms) */
 int nemoh_b200_last_timings(nemoh_ctx* ctx, double* assemble_ms, double* factor_ms, double* solve_ms);
-/* mixed precision: refinement iterations and final max relative residual of the last solve */
+/* mixed precision: refinement iterations and final max relative residual of the
+ * last solve; iterations = -1 when the refinement did not reach 1e-12 (FP32
+ * factors too inaccurate, e.g. near an irregular frequency) and that batch was
+ * factored and solved again in FP64 on the device */
 int nemoh_b200_last_refinement(nemoh_ctx* ctx, int* iterations, double* residual);
 /* number of CUDA kernel launches issued by this context since creation */
 long long nemoh_b200_launch_count(const nemoh_ctx* ctx);

@@ -91,11 +91,12 @@ struct nemoh_ctx {
   // per-call workspace
   DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force;
   HostBuf h_oms, h_slots;
-  int cap_slots = 0, cap_nrhs = 0;   // what ensure_batch last provided
+  int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
   int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
   double w_previous = -1.;   // factor cache key of solve_problem
   int cached_fd = 0, cached_nexp = 0;
+  bool lu64 = false;         // d_D holds FP64 LU factors (FP64 mode, or a mixed-mode fallback)
   float t_asm = 0, t_fac = 0, t_sol = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -190,7 +191,8 @@ void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
 
 // capacity: frequencies per device batch
 int batch_capacity(nemoh_ctx* c, int nrhs, int want) {
-  if (want <= c->cap_slots && nrhs <= c->cap_nrhs) return want;   // buffers already fit
+  if (want <= c->cap_slots && nrhs <= c->cap_nrhs && c->nfa == c->cap_nfa && ncls(c) == c->cap_cls)
+    return want;   // buffers already fit (same mesh size as the last batch)
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t N = c->nfa, cls = ncls(c);
@@ -220,6 +222,11 @@ void ensure_batch(nemoh_ctx* c, int slots, int nrhs) {
   CK(c->h_oms.ensure((size_t)slots * sizeof(OmegaParams)));
   CK(c->h_slots.ensure((size_t)slots * sizeof(int)));
   if (c->mode == NEMOH_B200_MIXED) CK(c->mixed.ensure(slots * (int)cls, (int)N, std::max(nrhs, 1)));
+  if ((int)N != c->cap_nfa || (int)cls != c->cap_cls) {   // capacities count slots of this mesh size
+    c->cap_slots = c->cap_nrhs = 0;
+    c->cap_nfa = (int)N;
+    c->cap_cls = (int)cls;
+  }
   c->cap_slots = std::max(c->cap_slots, slots);
   c->cap_nrhs = std::max(c->cap_nrhs, std::max(nrhs, 1));
 }
@@ -324,15 +331,34 @@ void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
   CK(cudaGetLastError());
 }
 
+// Mixed precision: refine the FP32-LU solution; when refinement does not
+// reach the tolerance (the FP32 factors are too inaccurate, as near an
+// irregular frequency where the system is close to singular) the batch is
+// factored again in FP64 on the device and solved from the original
+// right-hand sides, which the refinement kept in mixed.b. d_D then holds the
+// FP64 factors (lu64) instead of the matrix.
+void mixed_solve(nemoh_ctx* c, int nsys, int nrhs) {
+  MixedWork& w = c->mixed;
+  mixed_solve_refine(w, c->d_D.as<double2>(), c->nfa, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(), nrhs,
+                     c->stream, c->launches);
+  CK(cudaGetLastError());
+  if (w.last_residual <= REFINE_TOL) return;
+  const size_t N = c->nfa;
+  CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
+  CK(cudaMemcpyAsync(c->d_X.p, w.b, (size_t)nsys * N * nrhs * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+  factor_fp64(c, nsys);
+  trsm_fp64(c, nsys, nrhs);
+  c->lu64 = true;
+  w.last_iterations = -1;
+  ++w.fallbacks;
+}
+
 void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs) {
+  c->lu64 = c->mode == NEMOH_B200_FP64;
   if (c->mode == NEMOH_B200_MIXED) {
     mixed_factor(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_status.as<int>(), c->stream, c->launches);
     CK(cudaGetLastError());
-    if (have_rhs) {
-      mixed_solve_refine(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(),
-                         nrhs, c->stream, c->launches);
-      CK(cudaGetLastError());
-    }
+    if (have_rhs) mixed_solve(c, nsys, nrhs);
   } else {
     factor_fp64(c, nsys);
     if (have_rhs) trsm_fp64(c, nsys, nrhs);
@@ -344,8 +370,7 @@ void potential(nemoh_ctx* c, int nsys, int nrhs) {
   const long long NN = (long long)N * N, xs = (long long)N * nrhs;
   Batch s{c->d_S.as<double2>(), NN, N, nullptr};
   CK(cudaMemsetAsync(c->d_Y.p, 0, (size_t)nsys * xs * sizeof(double2), c->stream));
-  matvec_acc_kernel<<<dim3((N + 127) / 128, (N + MV_COLS - 1) / MV_COLS, nsys), 128, 0, c->stream>>>(
-      s, c->d_X.as<double2>(), xs, c->d_Y.as<double2>(), xs, nrhs, 1.0);
+  matvec_acc(s, c->d_X.as<double2>(), xs, c->d_Y.as<double2>(), xs, nrhs, nsys, 1.0, c->stream);
   LAUNCHED(c);
 }
 
@@ -636,13 +661,8 @@ int nemoh_b200_solve_problem(nemoh_ctx* c, double period, const double* nvel, do
       for (int i = 0; i < N; ++i) B[(size_t)s * N + i] = c->nsymy ? (v[i] + BX * v[i + N]) * 0.5 : v[i];
     }
     CK(cudaMemcpyAsync(c->d_X.p, B.data(), B.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    if (c->mode == NEMOH_B200_MIXED) {
-      mixed_solve_refine(c->mixed, c->d_D.as<double2>(), N, cls, c->d_X.as<double2>(), c->d_Y.as<double2>(), 1,
-                         c->stream, c->launches);
-      CK(cudaGetLastError());
-    } else {
-      trsm_fp64(c, cls, 1);
-    }
+    if (c->lu64) trsm_fp64(c, cls, 1);
+    else mixed_solve(c, cls, 1);
     std::vector<std::complex<double>> zol((size_t)cls * N), phi((size_t)cls * N);
     CK(cudaMemcpyAsync(zol.data(), c->d_X.p, zol.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     potential(c, cls, 1);

@@ -329,9 +329,6 @@ __global__ void __launch_bounds__(256) force_kernel(const double2* __restrict__ 
   }
 }
 
-}  // namespace nb200
-
-namespace nb200 {
 
 // ---------------------------------------------------------------------------
 // Blocked triangular solves with precomputed inverses of the diagonal blocks.
@@ -505,41 +502,68 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
 
 // Y += sign * M X (FP64) with the columns split over blockIdx.y; partial sums
 // are added with atomics, so Y must hold its initial value (0 or the RHS).
+// The number of right-hand sides is a template parameter so that no
+// predicated-off FMAs are issued (the kernel is balanced between HBM and the
+// FP64 pipe at nine right-hand sides).
 constexpr int MV_COLS = 128;
+template <int NR>
 __global__ void __launch_bounds__(128) matvec_acc_kernel(Batch m, const double2* __restrict__ xbase, long long xstride,
-                                                         double2* ybase, long long ystride, int nrhs, double sign) {
-  __shared__ double2 Xs[MV_COLS * MAX_RHS];
+                                                         double2* ybase, long long ystride, double sign) {
+  __shared__ double2 Xs[MV_COLS * NR];
   const int n = m.n;
   const double2* M = m.base + blockIdx.z * m.stride;
   const double2* X = xbase + blockIdx.z * xstride;
   const int c0 = blockIdx.y * MV_COLS, nc = min(MV_COLS, n - c0);
-  for (int q = threadIdx.x; q < MV_COLS * nrhs; q += blockDim.x) {
+  for (int q = threadIdx.x; q < MV_COLS * NR; q += blockDim.x) {
     const int c = q % MV_COLS, p = q / MV_COLS;
-    Xs[c + MV_COLS * p] = (c < nc) ? X[(c0 + c) + (long long)n * p] : make_double2(0., 0.);
+    Xs[c * NR + p] = (c < nc) ? X[(c0 + c) + (long long)n * p] : make_double2(0., 0.);
   }
   __syncthreads();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
-  double2 acc[MAX_RHS];
+  double2 acc[NR];
 #pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p) acc[p] = make_double2(0., 0.);
+  for (int p = 0; p < NR; ++p) acc[p] = make_double2(0., 0.);
+  const double2* Mr = M + r + (long long)n * c0;
   for (int c8 = 0; c8 < nc; c8 += 8) {
     double2 a[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a[j] = (c8 + j < nc) ? M[r + (long long)n * (c0 + c8 + j)] : make_double2(0., 0.);
+    for (int j = 0; j < 8; ++j) a[j] = (c8 + j < nc) ? __ldg(Mr + (long long)n * (c8 + j)) : make_double2(0., 0.);
 #pragma unroll
     for (int j = 0; j < 8; ++j)
 #pragma unroll
-      for (int p = 0; p < MAX_RHS; ++p)
-        if (p < nrhs) cmad(acc[p], a[j], Xs[c8 + j + MV_COLS * p]);
+      for (int p = 0; p < NR; ++p) cmad(acc[p], a[j], Xs[(c8 + j) * NR + p]);
   }
   double2* Y = ybase + blockIdx.z * ystride;
 #pragma unroll
-  for (int p = 0; p < MAX_RHS; ++p)
-    if (p < nrhs) {
-      atomicAdd(&Y[r + (long long)n * p].x, sign * acc[p].x);
-      atomicAdd(&Y[r + (long long)n * p].y, sign * acc[p].y);
-    }
+  for (int p = 0; p < NR; ++p) {
+    atomicAdd(&Y[r + (long long)n * p].x, sign * acc[p].x);
+    atomicAdd(&Y[r + (long long)n * p].y, sign * acc[p].y);
+  }
+}
+
+template <int NR>
+inline void matvec_acc_nr(Batch m, const double2* x, long long xs, double2* y, long long ys, int nsys, double sign,
+                          cudaStream_t st) {
+  const int n = m.n;
+  matvec_acc_kernel<NR><<<dim3((n + 127) / 128, (n + MV_COLS - 1) / MV_COLS, nsys), 128, 0, st>>>(m, x, xs, y, ys,
+                                                                                                  sign);
+}
+
+// Y += sign * M X for nsys systems with nrhs (1..MAX_RHS) right-hand sides
+inline void matvec_acc(Batch m, const double2* x, long long xs, double2* y, long long ys, int nrhs, int nsys,
+                       double sign, cudaStream_t st) {
+  switch (nrhs) {
+#define NB200_MV(k)                                    \
+  case k:                                              \
+    matvec_acc_nr<k>(m, x, xs, y, ys, nsys, sign, st); \
+    break;
+    NB200_MV(1) NB200_MV(2) NB200_MV(3) NB200_MV(4) NB200_MV(5) NB200_MV(6) NB200_MV(7) NB200_MV(8)
+    NB200_MV(9) NB200_MV(10) NB200_MV(11) NB200_MV(12) NB200_MV(13) NB200_MV(14) NB200_MV(15) NB200_MV(16)
+#undef NB200_MV
+    default:
+      break;
+  }
 }
 
 }  // namespace nb200

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -22,6 +23,14 @@
 namespace nb200 {
 
 constexpr int REFINE_MAX_IT = 30;
+
+// iteration limit: NEMOH_B200_REFINE_MAX_IT overrides the default (tests use a
+// small limit to exercise the FP64 fallback)
+inline int refine_max_it() {
+  const char* e = std::getenv("NEMOH_B200_REFINE_MAX_IT");
+  const int v = e ? std::atoi(e) : 0;
+  return v > 0 ? v : REFINE_MAX_IT;
+}
 constexpr double REFINE_TOL = 1e-12;
 
 struct MixedWork {
@@ -38,6 +47,7 @@ struct MixedWork {
   size_t total = 0;
   int last_iterations = 0;
   double last_residual = 0.;
+  long long fallbacks = 0;   // batches re-solved with FP64 factors
 
   size_t bytes() const { return total; }
   void release() {
@@ -49,7 +59,8 @@ struct MixedWork {
   }
   ~MixedWork() { release(); }
   cudaError_t ensure(int nsys, int n, int nrhs) {
-    if (nsys <= cap_sys && n == cap_n && nrhs <= cap_rhs) return cudaSuccess;
+    if (nsys <= cap_sys && n <= cap_n && nrhs <= cap_rhs)
+      return cudaSuccess;   // strides follow the current n; the buffers are large enough
     release();
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
     cudaError_t e;
@@ -184,14 +195,14 @@ inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double
   std::vector<unsigned long long> h(2 * (size_t)nv);
   Batch dm{D, (long long)n * n, n, nullptr};
   w.last_iterations = 0;
-  for (int it = 0; it < REFINE_MAX_IT; ++it) {
+  const int max_it = refine_max_it();
+  for (int it = 0; it < max_it; ++it) {
     trsm_f32(w, n, nsys, nrhs, st, launches);
     accumulate_kernel<<<1184, 256, 0, st>>>(X, w.rf, V, it == 0);
     ++launches;
     cudaMemsetAsync(w.norms, 0, (size_t)nv * sizeof(unsigned long long), st);
     cudaMemcpyAsync(w.r, w.b, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
-    matvec_acc_kernel<<<dim3((n + 127) / 128, (n + MV_COLS - 1) / MV_COLS, nsys), 128, 0, st>>>(
-        dm, X, (long long)n * nrhs, w.r, (long long)n * nrhs, nrhs, -1.0);
+    matvec_acc(dm, X, (long long)n * nrhs, w.r, (long long)n * nrhs, nrhs, nsys, -1.0, st);
     ++launches;
     residual_finish_kernel<<<dim3(8, nrhs, nsys), 256, 0, st>>>(w.r, w.rf, n, nrhs, w.norms);
     ++launches;

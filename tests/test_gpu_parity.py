@@ -8,6 +8,8 @@ strengths and potentials 1e-10; forces (added
 mass, damping, excitation) 1e-9 relative to the largest force of the same
 integration case. Mixed precision (FP32 LU + FP64 refinement): 1e-6 of FP64.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -173,3 +175,32 @@ def test_mixed_precision_matches_fp64(case):
         # a good low-precision factorization converges in a few refinement steps
         it, res = smx.last_refinement()
         assert it <= 6 and res <= 1e-12, (it, res)
+
+
+def test_mixed_fallback_to_fp64_factors(tmp_path):
+    """Refinement capped at one iteration cannot reach 1e-12: the batch is
+    re-solved with FP64 factors on the device and matches the FP64 path."""
+    import subprocess
+    import sys
+    case = CASES[1]
+    script = tmp_path / "fallback.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        "sys.path[:0] = %r\n"
+        "import gpu_cases as G, nemoh_b200 as nb\n"
+        "case = [c for c in G.small_cases() if c.name == %r][0]\n"
+        "nvel, nds, npb = G.problems(case)\n"
+        "m = case.mesh\n"
+        "out = {}\n"
+        "for mode in (nb.FP64, nb.MIXED):\n"
+        "    with nb.Solver(0, mode) as s:\n"
+        "        s.set_mesh(m.nodes, m.panels, m.isym, case.rho, case.g, case.depth)\n"
+        "        out[mode] = s.solve_frequencies(case.omegas, nvel, nds)\n"
+        "        it = s.last_refinement()[0]\n"
+        "print('ERR', G.rel_err(out[nb.MIXED], out[nb.FP64]), 'IT', it)\n"
+        % ([str(p) for p in (B.HERE + "/..", B.HERE + "/../tests")], case.name))
+    env = dict(os.environ, NEMOH_B200_REFINE_MAX_IT="1")
+    r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [l for l in r.stdout.splitlines() if l.startswith("ERR")][-1].split()
+    assert float(line[1]) < 1e-10 and int(line[3]) == -1, line
