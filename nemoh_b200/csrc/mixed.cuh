@@ -43,7 +43,7 @@ struct MixedWork {
   float2* inv = nullptr;     // inverses of the diagonal blocks of L and U (FP32)
   unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
   TcWork tc;                 // tensor-core GEMM operand buffers
-  int cap_sys = 0, cap_n = 0, cap_rhs = 0;
+  size_t have[8] = {};       // bytes held by lu, diag, b, r, rf, yf, norms, inv
   size_t total = 0;
   int last_iterations = 0;
   double last_residual = 0.;
@@ -54,31 +54,39 @@ struct MixedWork {
     cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms); cudaFree(inv);
     tc.release();
     lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr; inv = nullptr;
-    cap_sys = cap_n = cap_rhs = 0;
+    for (size_t& h : have) h = 0;
     total = 0;
   }
   ~MixedWork() { release(); }
+  // Each buffer grows on its own when the batch needs more bytes than it holds
+  // (strides always follow the current n), so a smaller mesh with more
+  // systems reuses what a larger one left and nothing is freed needlessly:
+  // cudaFree synchronizes the whole device.
   cudaError_t ensure(int nsys, int n, int nrhs) {
-    if (nsys <= cap_sys && n <= cap_n && nrhs <= cap_rhs)
-      return cudaSuccess;   // strides follow the current n; the buffers are large enough
-    release();
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
-    cudaError_t e;
-    if ((e = cudaMalloc(&lu, nsys * NN * sizeof(float2)))) return e;
-    if ((e = cudaMalloc(&diag, (size_t)nsys * DIAG_SCRATCH * sizeof(float2)))) return e;
-    if ((e = cudaMalloc(&b, V * sizeof(double2)))) return e;
-    if ((e = cudaMalloc(&r, V * sizeof(double2)))) return e;
-    if ((e = cudaMalloc(&rf, V * sizeof(float2)))) return e;
-    if ((e = cudaMalloc(&yf, V * sizeof(float2)))) return e;
-    if ((e = cudaMalloc(&norms, (size_t)2 * nsys * nrhs * sizeof(unsigned long long)))) return e;
-    const size_t ninv = (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB;
-    if ((e = cudaMalloc(&inv, ninv * sizeof(float2)))) return e;
-    if ((e = tc.ensure(nsys, n))) return e;
-    cap_sys = nsys;
-    cap_n = n;
-    cap_rhs = nrhs;
-    total = nsys * NN * sizeof(float2) + V * (2 * sizeof(double2) + 2 * sizeof(float2)) + tc.bytes() +
-            ninv * sizeof(float2) + (size_t)nsys * DIAG_SCRATCH * sizeof(float2);
+    const size_t need[8] = {nsys * NN * sizeof(float2),
+                            (size_t)nsys * DIAG_SCRATCH * sizeof(float2),
+                            V * sizeof(double2),
+                            V * sizeof(double2),
+                            V * sizeof(float2),
+                            V * sizeof(float2),
+                            (size_t)2 * nsys * nrhs * sizeof(unsigned long long),
+                            (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2)};
+    void** ptr[8] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
+                     (void**)&inv};
+    for (int i = 0; i < 8; ++i) {
+      if (need[i] <= have[i]) continue;
+      cudaFree(*ptr[i]);
+      *ptr[i] = nullptr;
+      have[i] = 0;
+      cudaError_t e = cudaMalloc(ptr[i], need[i]);
+      if (e) return e;
+      have[i] = need[i];
+    }
+    cudaError_t e = tc.ensure(nsys, n);
+    if (e) return e;
+    total = tc.bytes();
+    for (size_t h : have) total += h;
     return cudaSuccess;
   }
 };

@@ -49,26 +49,32 @@ constexpr int ST_TC_TIMEOUT = 30;
 struct TcWork {
   unsigned char* a = nullptr;   // A images: nsys x ceil(n/128) row tiles x TC_NCH chunks x (hi, lo)
   unsigned char* b = nullptr;   // B images: nsys x ceil(n/128) column tiles x TC_NCH chunks x (hi, lo)
-  int cap_sys = 0, cap_n = 0;
-  size_t total = 0;
-  size_t bytes() const { return total; }
+  size_t have_a = 0, have_b = 0;
+  size_t bytes() const { return have_a + have_b; }
   void release() {
     cudaFree(a);
     cudaFree(b);
     a = b = nullptr;
-    cap_sys = cap_n = 0;
-    total = 0;
+    have_a = have_b = 0;
   }
   cudaError_t ensure(int nsys, int n) {
-    if (nsys <= cap_sys && n <= cap_n) return cudaSuccess;
-    release();
     const size_t t = (size_t)(n + TC_T - 1) / TC_T;
+    const size_t na = nsys * t * TC_NCH * 2 * TC_AIMG, nb = nsys * t * TC_NCH * 2 * TC_BIMG;
     cudaError_t e;
-    if ((e = cudaMalloc(&a, nsys * t * TC_NCH * 2 * TC_AIMG))) return e;
-    if ((e = cudaMalloc(&b, nsys * t * TC_NCH * 2 * TC_BIMG))) return e;
-    cap_sys = nsys;
-    cap_n = n;
-    total = nsys * t * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG);
+    if (na > have_a) {
+      cudaFree(a);
+      a = nullptr;
+      have_a = 0;
+      if ((e = cudaMalloc(&a, na))) return e;
+      have_a = na;
+    }
+    if (nb > have_b) {
+      cudaFree(b);
+      b = nullptr;
+      have_b = 0;
+      if ((e = cudaMalloc(&b, nb))) return e;
+      have_b = nb;
+    }
     return cudaSuccess;
   }
 };

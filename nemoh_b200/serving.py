@@ -13,6 +13,10 @@ Design:
 * admission by HBM footprint: a batch takes at most as many frequencies as
   fit the worker's share of device memory (two complex128 N x N matrices per
   symmetry class plus workspace per frequency);
+* workspace reserved up front: each worker first solves the largest body at
+  `reserve` frequencies, so that later batches of up to that many frequencies
+  find their device buffers in place (growing a buffer frees the old one, and
+  cudaFree waits for every stream on the device, stalling the other workers);
 * continuous batching: whenever a worker is free it takes the body of the
   oldest waiting request and every request of that body that has arrived,
   up to its admission limit; requests that arrive while others run join the
@@ -85,7 +89,7 @@ class SolveServer:
     """Serve a stream of requests on one GPU with `workers` concurrent contexts."""
 
     def __init__(self, bodies: List[Body], device=0, precision=MIXED, workers=2, memory_fraction=0.6,
-                 solver_factory=None, memory_bytes=None):
+                 solver_factory=None, memory_bytes=None, reserve=0):
         self.bodies = bodies
         self.device = device
         self.precision = precision
@@ -104,6 +108,16 @@ class SolveServer:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
         self._budget = free * memory_fraction / workers
+        if reserve > 0 and bodies:
+            big = max(range(len(bodies)), key=lambda b: bodies[b].bytes_per_frequency())
+            body = bodies[big]
+            k = min(reserve, self.admission(body))
+            omegas = np.linspace(0.5, 2.0, k)
+            nvel = np.stack([body.rhs(w, 0.0) for w in omegas], axis=2)
+            for w, s in enumerate(self._solvers):
+                s.set_case(body.case)
+                s.solve_frequencies(omegas, nvel, body.nds)
+                self._current[w] = big
 
     def close(self):
         for s in self._solvers:
