@@ -31,6 +31,11 @@ inline int refine_max_it() {
   const int v = e ? std::atoi(e) : 0;
   return v > 0 ? v : REFINE_MAX_IT;
 }
+// A batch is accepted when its largest relative residual |b - D x|inf/|b|inf
+// is at most REFINE_TOL. The error of x is at most cond(D) times that, below
+// 1e-8 for the conditioning met on hull meshes away from irregular
+// frequencies; near one the FP32 factors stall or diverge and the batch is
+// solved again with FP64 factors.
 constexpr double REFINE_TOL = 1e-12;
 
 struct MixedWork {
@@ -204,6 +209,7 @@ inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double
   Batch dm{D, (long long)n * n, n, nullptr};
   w.last_iterations = 0;
   const int max_it = refine_max_it();
+  double prev = 1e300;
   for (int it = 0; it < max_it; ++it) {
     trsm_f32(w, n, nsys, nrhs, st, launches);
     accumulate_kernel<<<1184, 256, 0, st>>>(X, w.rf, V, it == 0);
@@ -225,7 +231,10 @@ inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double
     }
     w.last_iterations = it + 1;
     w.last_residual = worst;
-    if (worst <= REFINE_TOL || !(worst == worst)) break;
+    // stop at the tolerance, or as soon as the residual no longer halves
+    // (stagnation or divergence: the caller then falls back to FP64 factors)
+    if (worst <= REFINE_TOL || !(worst == worst) || worst > 0.5 * prev) break;
+    prev = worst;
   }
 }
 
