@@ -297,21 +297,14 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
   static bool attr = false;
   if (!attr) {
     CK(cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            2 * LU_NB * GM_T * (int)sizeof(double2)));
+                            zgemm_smem<double2>()));
     attr = true;
   }
-  for (int k = 0; k < N; k += LU_NB) {
-    const int nb = std::min(LU_NB, N - k), rest = N - k - nb;
-    const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-    lu_diag_kernel<double2><<<dim3(1, 1, nsys), 256, 0, c->stream>>>(b, k, c->d_status.as<int>());
-    LAUNCHED(c);
-    lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, c->stream>>>(b, k);
-    LAUNCHED(c);
-    if (rest > 0) {
-      zgemm_update<double2>(b, k, nb, Rect{k + nb, N, k + nb, N}, nsys, c->stream);
-      LAUNCHED(c);
-    }
-  }
+  lu_two_level<double2>(b, nsys, c->d_status.as<int>(), c->stream, c->launches, [&](int k0, int kend) {
+    zgemm_update<double2>(b, k0, kend - k0, Rect{kend, N, kend, N}, nsys, c->stream);
+    ++c->launches;
+  });
+  CK(cudaGetLastError());
   static bool attr2 = false;
   if (!attr2) {
     CK(cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -878,7 +871,7 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
       const int trsm_smem = (2 * TB * MAX_RHS + TB * TB) * (int)sizeof(double2);
       const cudaError_t a[4] = {
           cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               2 * LU_NB * GM_T * (int)sizeof(double2)),
+                               zgemm_smem<double2>()),
           cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                2 * TB * TB * (int)sizeof(double2)),
           cudaFuncSetAttribute(trsm_fused_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -198,63 +198,108 @@ __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
 }
 
 // A[r0:r1, c0:c1] -= A[r0:r1, k:k+kb] A[k:k+kb, c0:c1]: 64 x 64 output tile
-// per CTA (grid.x over columns, grid.y over rows), 16 x 16 threads, 4 x 4
-// each; the inner dimension is staged through shared memory 32 at a time.
+// per CTA (grid.x over columns, grid.y over rows), 128 threads; thread
+// (tr, tc) = (t % 16, t / 16) owns rows tr + 16 i (i < 4) and columns
+// 8 tc + j (j < 8), so 16 consecutive lanes own 16 consecutive rows of a
+// column (coalesced read-modify-write of the result) while each k step reads
+// 4 A values (contiguous across lanes) and 8 B values (broadcast) from shared
+// memory for 32 complex FMAs. The inner dimension streams through two
+// shared-memory stages of 16 with asynchronous copies (cp.async, zero-filled
+// outside the operands), so the next chunk loads while the current one is
+// multiplied; B rows are padded to 65 elements against bank conflicts.
 constexpr int GM_T = 64;
+constexpr int GM_BS = GM_T + 1;
+constexpr int GM_KC = 16;
 struct Rect {
   int r0, r1, c0, c1;
 };
+template <class C2>
+constexpr int zgemm_smem() {
+  return 2 * (GM_KC * GM_T + GM_KC * GM_BS) * (int)sizeof(C2);
+}
+
+// asynchronous global -> shared copy of one complex element; src_bytes = 0
+// zero-fills the destination without reading
+template <class C2>
+__device__ __forceinline__ void cp_async_elem(C2* dst, const C2* src, bool valid) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  const int nbytes = valid ? (int)sizeof(C2) : 0;
+  if (sizeof(C2) == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(nbytes) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(nbytes) : "memory");
+}
 
 template <class C2>
-__global__ void __launch_bounds__(256) zgemm_update_kernel(BatchT<C2> b, int k, int kb, Rect rc) {
+__global__ void __launch_bounds__(128) zgemm_update_kernel(BatchT<C2> b, int k, int kb, Rect rc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2* As = reinterpret_cast<C2*>(smem_raw);   // [32][64]
-  C2* Bs = As + LU_NB * GM_T;                 // [32][64]
+  C2* stage0 = reinterpret_cast<C2*>(smem_raw);
+  constexpr int STAGE = GM_KC * GM_T + GM_KC * GM_BS;   // As [16][64] then Bs [16][65]
   const int n = b.n;
   const int r0 = rc.r0 + blockIdx.y * GM_T;
   const int c0 = rc.c0 + blockIdx.x * GM_T;
   C2* A = b.base + blockIdx.z * b.stride;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  C2 acc[4][4];
+  const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+  auto load = [&](int s, int k0) {
+    C2* As = stage0 + s * STAGE;
+    C2* Bs = As + GM_KC * GM_T;
+    const int kc = min(GM_KC, kb - k0);
+    for (int q = threadIdx.x; q < GM_KC * GM_T; q += 128) {
+      const int m = q % GM_T, kk = q / GM_T;
+      const int r = r0 + m;
+      const bool v = r < rc.r1 && kk < kc;
+      cp_async_elem(As + kk * GM_T + m, v ? A + r + (long long)n * (k + k0 + kk) : A, v);
+    }
+    for (int q = threadIdx.x; q < GM_KC * GM_T; q += 128) {
+      const int kk = q % GM_KC, nn = q / GM_KC;
+      const int c = c0 + nn;
+      const bool v = c < rc.c1 && kk < kc;
+      cp_async_elem(Bs + kk * GM_BS + nn, v ? A + (k + k0 + kk) + (long long)n * c : A, v);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  C2 acc[4][8];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = mkc<C2>(0., 0.);
-  for (int k0 = 0; k0 < kb; k0 += LU_NB) {
-    const int kc = min(LU_NB, kb - k0);
-    if (k0) __syncthreads();
-    for (int q = threadIdx.x; q < kc * GM_T; q += 256) {
-      const int m = q % GM_T, kk = q / GM_T;
-      const int r = r0 + m;
-      As[kk * GM_T + m] = (r < rc.r1) ? A[r + (long long)n * (k + k0 + kk)] : mkc<C2>(0., 0.);
-      const int kk2 = q % kc, nn = q / kc;
-      const int c = c0 + nn;
-      Bs[kk2 * GM_T + nn] = (c < rc.c1) ? A[(k + k0 + kk2) + (long long)n * c] : mkc<C2>(0., 0.);
+    for (int j = 0; j < 8; ++j) acc[i][j] = mkc<C2>(0., 0.);
+  load(0, 0);
+  int s = 0;
+  for (int k0 = 0; k0 < kb; k0 += GM_KC, s ^= 1) {
+    const bool more = k0 + GM_KC < kb;
+    if (more) {
+      load(s ^ 1, k0 + GM_KC);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < kc; ++kk) {
-      C2 a[4], bb[4];
+    const C2* As = stage0 + s * STAGE;
+    const C2* Bs = As + GM_KC * GM_T;
+#pragma unroll 2
+    for (int kk = 0; kk < GM_KC; ++kk) {
+      C2 a[4], bb[8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk * GM_T + ty + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = As[kk * GM_T + tr + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bb[j] = Bs[kk * GM_T + tx + 16 * j];
+      for (int j = 0; j < 8; ++j) bb[j] = Bs[kk * GM_BS + 8 * tc + j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 8; ++j) {
           acc[i][j].x += a[i].x * bb[j].x - a[i].y * bb[j].y;
           acc[i][j].y += a[i].x * bb[j].y + a[i].y * bb[j].x;
         }
     }
+    __syncthreads();   // stage s is refilled two chunks later
   }
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = c0 + tx + 16 * j;
+  for (int j = 0; j < 8; ++j) {
+    const int c = c0 + 8 * tc + j;
     if (c >= rc.c1) continue;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int r = r0 + ty + 16 * i;
+      const int r = r0 + tr + 16 * i;
       if (r >= rc.r1) continue;
       C2* p = A + r + (long long)n * c;
       C2 v = *p;
@@ -269,7 +314,39 @@ template <class C2>
 inline void zgemm_update(BatchT<C2> b, int k, int kb, Rect rc, int nsys, cudaStream_t st) {
   if (rc.r1 <= rc.r0 || rc.c1 <= rc.c0) return;
   const dim3 grid((rc.c1 - rc.c0 + GM_T - 1) / GM_T, (rc.r1 - rc.r0 + GM_T - 1) / GM_T, nsys);
-  zgemm_update_kernel<C2><<<grid, 256, 2 * LU_NB * GM_T * sizeof(C2), st>>>(b, k, kb, rc);
+  zgemm_update_kernel<C2><<<grid, 128, zgemm_smem<C2>(), st>>>(b, k, kb, rc);
+}
+
+// Two-level blocked LU of nsys systems (grid.z = system). Panels of LU_OUTER
+// columns are factored with LU_NB-column steps whose updates stay inside the
+// panel (all rows below) and the panel's row strip (all columns right of it);
+// the rest of the trailing matrix is updated once per panel by `outer(k0,
+// kend)`, A[kend:, kend:] -= A[kend:, k0:kend] A[k0:kend, kend:], which cuts
+// the trailing matrix's read-modify-write traffic by LU_OUTER / LU_NB.
+constexpr int LU_OUTER = 128;
+template <class C2, class Outer>
+inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t st, long long& launches, Outer outer) {
+  const int n = b.n;
+  for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
+    const int kend = std::min(k0 + LU_OUTER, n);
+    for (int k = k0; k < kend; k += LU_NB) {
+      const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
+      const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
+      lu_diag_kernel<C2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
+      ++launches;
+      lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k);
+      ++launches;
+      if (k + nb < kend) {
+        zgemm_update<C2>(b, k, nb, Rect{k + nb, n, k + nb, kend}, nsys, st);
+        ++launches;
+        if (kend < n) {
+          zgemm_update<C2>(b, k, nb, Rect{k + nb, kend, kend, n}, nsys, st);
+          ++launches;
+        }
+      }
+    }
+    if (kend < n) outer(k0, kend);
+  }
 }
 
 constexpr int MAX_RHS = 16;

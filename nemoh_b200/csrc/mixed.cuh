@@ -153,30 +153,12 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
   ++launches;
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
-  for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
-    const int kend = std::min(k0 + LU_OUTER, n);
-    for (int k = k0; k < kend; k += LU_NB) {
-      const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
-      const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-      lu_diag_kernel<float2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
-      ++launches;
-      lu_panel_kernel<float2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k);
-      ++launches;
-      if (k + nb < kend) {
-        // inside the panel (all rows below) and the panel's row strip right of it
-        zgemm_update<float2>(b, k, nb, Rect{k + nb, n, k + nb, kend}, nsys, st);
-        ++launches;
-        if (kend < n) {
-          zgemm_update<float2>(b, k, nb, Rect{k + nb, kend, kend, n}, nsys, st);
-          ++launches;
-        }
-      }
-    }
-    if (kend < n && !tc_update(w.tc, b, k0, nsys, st, launches, status)) {
+  lu_two_level<float2>(b, nsys, status, st, launches, [&](int k0, int kend) {
+    if (!tc_update(w.tc, b, k0, nsys, st, launches, status)) {
       zgemm_update<float2>(b, k0, kend - k0, Rect{kend, n, kend, n}, nsys, st);
       ++launches;
     }
-  }
+  });
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,

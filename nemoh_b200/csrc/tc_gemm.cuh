@@ -34,7 +34,6 @@
 
 namespace nb200 {
 
-constexpr int LU_OUTER = 128;                   // panel width of the mixed LU (K of the update)
 constexpr int TC_T = 128;                       // complex rows and columns per tile
 constexpr int TC_KC = 16;                       // complex k per chunk
 constexpr int TC_NCH = LU_OUTER / TC_KC;        // chunks per update

@@ -127,6 +127,21 @@ def test_cylinder_verification_against_reference_results(solver):
     assert max(errs)[0] < 1e-4
 
 
+def _lu_launches(n, nb=32, outer=128):
+    """Launches of the two-level FP64 LU: per 32-column step the diagonal
+    block and the panel, plus the updates inside the 128-column panel and its
+    row strip; one trailing update per panel."""
+    count = 0
+    for k0 in range(0, n, outer):
+        kend = min(k0 + outer, n)
+        for k in range(k0, kend, nb):
+            count += 2
+            if k + min(nb, n - k) < kend:
+                count += 1 + (kend < n)
+        count += kend < n
+    return count
+
+
 def test_repeated_frequency_reuses_factorization(solver):
     case = CASES[0]
     _mesh(solver, case)
@@ -138,11 +153,9 @@ def test_repeated_frequency_reuses_factorization(solver):
     solver.solve_potential(T, nv[:, 1])
     n2 = solver.launches
     # the second call launches no assembly and no factorization: two assembly
-    # launches (Rankine and wave passes), the LU launches (diagonal block, panel and update per 32-column
-    # step; no panel on the last step) and one diagonal-block inversion fewer
-    steps = (case.mesh.npanels + 31) // 32
-    n_lu = 3 * steps - 1
-    assert (n1 - n0) - (n2 - n1) == 3 + n_lu
+    # launches (Rankine and wave passes), the LU launches and one diagonal-block
+    # inversion fewer
+    assert (n1 - n0) - (n2 - n1) == 3 + _lu_launches(case.mesh.npanels)
 
 
 def test_degenerate_panel_reports_status(solver):
