@@ -602,14 +602,21 @@ __global__ void __launch_bounds__(128) matvec_acc_kernel(Batch m, const double2*
 #pragma unroll
   for (int p = 0; p < NR; ++p) acc[p] = make_double2(0., 0.);
   const double2* Mr = M + r + (long long)n * c0;
-  for (int c8 = 0; c8 < nc; c8 += 8) {
-    double2 a[8];
+  // the next 8 columns are loaded while the current 8 are multiplied
+  double2 a[8], an[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a[j] = (c8 + j < nc) ? __ldg(Mr + (long long)n * (c8 + j)) : make_double2(0., 0.);
+  for (int j = 0; j < 8; ++j) a[j] = (j < nc) ? __ldg(Mr + (long long)n * j) : make_double2(0., 0.);
+#pragma unroll 1
+  for (int c8 = 0; c8 < nc; c8 += 8) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      an[j] = (c8 + 8 + j < nc) ? __ldg(Mr + (long long)n * (c8 + 8 + j)) : make_double2(0., 0.);
 #pragma unroll
     for (int j = 0; j < 8; ++j)
 #pragma unroll
       for (int p = 0; p < NR; ++p) cmad(acc[p], a[j], Xs[(c8 + j) * NR + p]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = an[j];
   }
   double2* Y = ybase + blockIdx.z * ystride;
 #pragma unroll

@@ -258,6 +258,19 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
+  // while thread 0 streams the operands and issues the MMAs, every thread
+  // pulls one column of this CTA's 128 x 128 result tile into L2, so that the
+  // read-modify-write at the end reads from L2 instead of HBM
+  {
+    const int gr0 = r1 + trow * TC_T, nrows = min(TC_T, n - gr0);
+    const int c = r1 + tcol * TC_T + (int)threadIdx.x;
+    if (nrows > 0 && c < n) {
+      const char* p = reinterpret_cast<const char*>(b.base + blockIdx.z * b.stride + gr0 + (long long)n * c);
+      for (int off = 0; off < nrows * (int)sizeof(float2); off += 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
+    }
+  }
+
   if (threadIdx.x == 0) {
     bool ok = true;
     const unsigned char* ga = abuf + blockIdx.z * sys_bytes_a + (long long)trow * TC_NCH * 2 * TC_AIMG;
