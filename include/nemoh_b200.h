@@ -86,6 +86,16 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* ctx, int nomega, const double
                                         const double* nvel_device, int nint, const double* nds_device,
                                         double* force_device, void* stream);
 
+/* Kochin function (COMPUTE_KOCHIN.f90:25-152, as called by SOLVE_BEM.f90:98-102):
+ * for source strengths zigb, zigs (nfa x nprob complex each, as returned by
+ * nemoh_b200_solve_problem; zigs unused without symmetry) of problems at period
+ * `period`, H(theta) at the ntheta directions theta (radians, mesh/Kochin.dat)
+ * about the wave measurement point (xeff, yeff) of Nemoh.cal (yeff is taken
+ * as 0 on symmetric meshes, INITIALIZATION.f90:60). hkochin: ntheta x nprob
+ * complex (theta fastest). */
+int nemoh_b200_kochin(nemoh_ctx* ctx, double period, double xeff, double yeff, int ntheta, const double* theta,
+                      int nprob, const double* zigb, const double* zigs, double* hkochin);
+
 /* No counterpart in the reference: an entry point that allocates nothing, for
  * hosts whose device memory is held by their own allocator (a PyTorch caching
  * allocator, a batching server that admits work by free HBM) and for hosts

@@ -72,6 +72,8 @@ def load_library():
     L.nemoh_b200_last_timings.argtypes = [_vp, _d, _d, _d]
     L.nemoh_b200_last_refinement.argtypes = [_vp, _i, _d]
     L.nemoh_b200_launch_count.argtypes = [_vp]
+    L.nemoh_b200_kochin.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
+                                    ctypes.c_int, _d, _d, _d]
     L.nemoh_b200_launch_count.restype = ctypes.c_longlong
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
     L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
@@ -200,6 +202,21 @@ class Solver:
         it, res = ctypes.c_int(), ctypes.c_double()
         load_library().nemoh_b200_last_refinement(self._h, ctypes.byref(it), ctypes.byref(res))
         return it.value, res.value
+
+    # -- COMPUTE_KOCHIN ---------------------------------------------------------
+    def kochin(self, period, theta, zigb, zigs=None, xeff=0.0, yeff=0.0):
+        """Kochin function H(theta) of problems solved at `period` from their source
+        strengths (nfa,) or (nfa, nprob); returns (ntheta, nprob) complex."""
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        zigb = np.asfortranarray(np.asarray(zigb, dtype=np.complex128).reshape(self.nfa, -1))
+        nprob = zigb.shape[1]
+        zigs = (np.asfortranarray(np.asarray(zigs, dtype=np.complex128).reshape(self.nfa, -1))
+                if zigs is not None else np.zeros_like(zigb))
+        out = np.zeros((len(theta), nprob), dtype=np.complex128, order="F")
+        self._check(load_library().nemoh_b200_kochin(self._h, float(period), float(xeff), float(yeff), len(theta),
+                                                     _p(theta), nprob, zigb.ctypes.data_as(_d),
+                                                     zigs.ctypes.data_as(_d), out.ctypes.data_as(_d)))
+        return out
 
     # -- diagnostics -----------------------------------------------------------
     def assemble(self, omega):

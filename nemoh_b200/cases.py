@@ -102,6 +102,7 @@ class Case:
     xeff: float = 0.0
     yeff: float = 0.0
     name: str = "case"
+    kochin_theta: tuple = ()   # directions (rad) of mesh/Kochin.dat; Kochin switch set for every problem if any
 
     @property
     def nproblems(self) -> int:
@@ -502,12 +503,16 @@ def write_case(case: Case, root: str, case_dir: str = "case") -> str:
         f.write(" ".join(_r(w) for w in case.omegas for _ in range(npb)) + "\n")
         for _ in case.omegas:
             f.write(" ".join([_r(b * math.pi / 180.0) for b in case.betas_deg] + ["-1.0"] * nr) + "\n")
-        for _ in range(3):
+        for _ in range(2):
             f.write(" ".join("0" for _ in range(case.nproblems)) + "\n")
+        sk = "1" if len(case.kochin_theta) else "0"
+        f.write(" ".join(sk for _ in range(case.nproblems)) + "\n")
         for c in range(nvel.shape[0]):
             f.write(" ".join("%s %s" % (_r(v.real), _r(v.imag)) for v in nvel[c]) + "\n")
     with open(os.path.join(d, "mesh", "Kochin.dat"), "w") as f:
-        f.write("0\n")
+        f.write("%d\n" % len(case.kochin_theta))
+        for t in case.kochin_theta:
+            f.write("%s\n" % _r(t))
     with open(os.path.join(d, "mesh", "Freesurface.dat"), "w") as f:
         f.write("0 0\n")
     fk = froude_krylov(case)

@@ -17,6 +17,7 @@
 #include "../../include/nemoh_b200.h"
 #include "assembly.cuh"
 #include "fd_setup.h"
+#include "kochin.cuh"
 #include "linalg.cuh"
 #include "mixed.cuh"
 
@@ -89,7 +90,7 @@ struct nemoh_ctx {
   double ro_eps2 = 0;   // largest x with sqrt(x) <= 1e-4
   DevBuf d_xyz, d_m, d_rec, d_rows;
   // per-call workspace
-  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force;
+  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin;
   HostBuf h_oms, h_slots;
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
@@ -718,6 +719,46 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* c, int nomega, const double* 
     CK(cudaEventRecord(e, c->stream));
     CK(cudaStreamWaitEvent(user, e, 0));
     CK(cudaEventDestroy(e));
+  });
+}
+
+int nemoh_b200_kochin(nemoh_ctx* c, double period, double xeff, double yeff, int ntheta, const double* theta,
+                      int nprob, const double* zigb, const double* zigs, double* hkochin) {
+  if (!c || !c->nfa || !(period > 0) || ntheta < 0 || nprob < 0 || (ntheta > 0 && (!theta || !hkochin)) ||
+      (nprob > 0 && !zigb) || (nprob > 0 && c->nsymy && !zigs))
+    return NEMOH_B200_EINVAL;
+  if (ntheta == 0 || nprob == 0) return NEMOH_B200_OK;
+  return guarded(c, [&] {
+    // wave number of SOLVE_BVP (SOLVE_BEM.f90:62-84): W^2/G, or AMH/Depth from X0
+    const double W = 2. * kPI / period;
+    double kwave = W * W / c->g;
+    if (!((c->depth == 0.) || (kwave * c->depth >= 20))) {
+      double AMH;
+      const int st = finite_depth_root(W * W * c->depth / c->g, &AMH);
+      if (st) throw Fail{st, "ERREUR DANS LA RECHERCHE DE LA RACINE (X0)"};
+      kwave = AMH / c->depth;
+    }
+    const double ye = c->nsymy ? 0. : yeff;   // INITIALIZATION.f90:60
+    const int N = c->nfa;
+    const size_t ns = (size_t)N * nprob, nh = (size_t)ntheta * nprob;
+    std::vector<double2> cs(ntheta);
+    for (int t = 0; t < ntheta; ++t) cs[t] = make_double2(std::cos(theta[t]), std::sin(theta[t]));
+    const size_t bytes = (2 * ns + nh + ntheta) * sizeof(double2);
+    CK(c->d_kochin.ensure(bytes));
+    double2* db = c->d_kochin.as<double2>();
+    double2* ds = db + ns;
+    double2* dh = ds + ns;
+    double2* dc = dh + nh;
+    CK(cudaMemcpyAsync(db, zigb, ns * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (c->nsymy) CK(cudaMemcpyAsync(ds, zigs, ns * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dc, cs.data(), ntheta * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(dh, 0, nh * sizeof(double2), c->stream));
+    kochin_kernel<<<dim3((N + KOCHIN_THREADS - 1) / KOCHIN_THREADS, ntheta), KOCHIN_THREADS, 0, c->stream>>>(
+        c->d_xyz.as<double>(), c->d_m.as<int>(), c->d_rows.as<double>(), N, c->nsymy, kwave, c->depth, xeff, ye, dc,
+        nprob, db, ds, ntheta, dh);
+    LAUNCHED(c);
+    CK(cudaMemcpyAsync(hkochin, dh, nh * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   });
 }
 

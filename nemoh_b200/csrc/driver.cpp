@@ -11,7 +11,10 @@
 // Problems are solved a frequency at a time: consecutive problems that share
 // a frequency go to one nemoh_b200_solve_frequencies call (one assembly and
 // one factorization for all of them, as the reference's w_previous cache).
-// Kochin, free-surface and pressure outputs are not produced.
+// Problems whose Kochin switch is set are also solved through
+// nemoh_b200_solve_problem for their source strengths, and their Kochin
+// functions are written to results/Kochin.<I5>.dat (SOLVE_BEM.f90:98-102,
+// OUTPUT.f90:25-40). Free-surface and pressure outputs are not produced.
 //
 // usage: nemoh_solver_b200 [case-root] [--mixed] [--device N]
 #include <cmath>
@@ -118,8 +121,13 @@ int main(int argc, char** argv) {
     auto vt = bc.read(npb);
     for (int j = 0; j < npb; ++j) stype[j] = std::stod(vt[j]);
     bool extra_outputs = false;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 2; ++k) {
       for (const auto& t : bc.read(npb)) extra_outputs |= std::stoi(t) != 0;
+    }
+    std::vector<int> kochin_switch(npb);
+    {
+      const auto v = bc.read(npb);
+      for (int j = 0; j < npb; ++j) kochin_switch[j] = std::stoi(v[j]);
     }
     std::vector<std::complex<double>> nvel((size_t)nc * npb);
     for (int c = 0; c < nc; ++c) {
@@ -129,6 +137,8 @@ int main(int argc, char** argv) {
     Records cal(dir + "/Nemoh.cal");
     cal.skip();
     const double rho = cal.real(), g = cal.real(), depth = cal.real();
+    const auto xy = cal.read(2);
+    const double xeff = std::stod(xy[0]), yeff = std::stod(xy[1]);
     {
       Records inp(dir + "/input.txt");
       inp.skip();
@@ -140,16 +150,18 @@ int main(int argc, char** argv) {
       const auto v = ig.read(nc);
       for (int c = 0; c < nc; ++c) nds[i + (size_t)nint * c] = std::stod(v[c]);
     }
+    std::vector<double> theta;
     {
       Records kr(dir + "/mesh/Kochin.dat");
-      extra_outputs |= kr.integer() > 0;
+      const int nth = kr.integer();
+      for (int j = 0; j < nth; ++j) theta.push_back(kr.real());
     }
     {
       Records fr(dir + "/mesh/Freesurface.dat");
       extra_outputs |= std::stoi(fr.read(2)[0]) > 0;
     }
     if (extra_outputs)
-      std::fprintf(stderr, "nemoh_solver_b200: Kochin / free-surface / pressure outputs are not produced\n");
+      std::fprintf(stderr, "nemoh_solver_b200: free-surface / pressure outputs are not produced\n");
 
     nemoh_ctx* ctx = nullptr;
     check(nullptr, nemoh_b200_create(&ctx, device, mode), "create");
@@ -169,6 +181,35 @@ int main(int argc, char** argv) {
       for (int p = 0; p < nrhs; ++p)
         for (int i = 0; i < nint; ++i) force[i + (size_t)nint * (j + p)] = f[i + (size_t)nint * p];
       j = e;
+    }
+    // Kochin functions of the problems that ask for them
+    if (!theta.empty()) {
+      std::vector<std::complex<double>> zigb(nfa), zigs(nfa), h(theta.size());
+      const double PI = 4. * std::atan(1.);
+      for (int p = 0; p < npb; ++p) {
+        if (kochin_switch[p] != 1) continue;
+        int nexp = 0;
+        check(ctx,
+              nemoh_b200_solve_problem(ctx, 2. * PI / omega[p], reinterpret_cast<const double*>(&nvel[(size_t)nc * p]),
+                                       reinterpret_cast<double*>(zigb.data()), reinterpret_cast<double*>(zigs.data()),
+                                       nullptr, nullptr, &nexp),
+              "solve_problem");
+        check(ctx,
+              nemoh_b200_kochin(ctx, 2. * PI / omega[p], xeff, yeff, (int)theta.size(), theta.data(), 1,
+                                reinterpret_cast<const double*>(zigb.data()),
+                                reinterpret_cast<const double*>(zigs.data()), reinterpret_cast<double*>(h.data())),
+              "kochin");
+        char name[32];
+        std::snprintf(name, sizeof name, "Kochin.%5d.dat", p + 1);
+        std::ofstream kf(dir + "/results/" + name);
+        if (!kf) throw IoError("cannot write " + dir + "/results/" + name);
+        char line[96];
+        for (size_t t = 0; t < theta.size(); ++t) {
+          std::snprintf(line, sizeof line, " %.17E %.17E %.17E\n", theta[t], std::abs(h[t]),
+                        std::atan2(h[t].imag(), h[t].real()));
+          kf << line;
+        }
+      }
     }
     nemoh_b200_destroy(ctx);
 

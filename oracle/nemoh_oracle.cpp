@@ -1743,6 +1743,67 @@ struct Oracle {
     return NEXP;
   }
 
+  // SOLVE_BEM.f90:62-84: the wave number SOLVE_BVP hands to COMPUTE_KOCHIN
+  // (W^2/G in deep water, AMH/Depth from X0 in finite depth)
+  R kochin_kwave(R Period) {
+    const R PI = 4. * std::atan(1.);
+    R W = 2. * PI / Period;
+    R kwave = W * W / G;
+    if ((Depth == 0.) || (kwave * Depth >= 20)) return W * W / G;
+    R AKH = W * W * Depth / G;
+    R AMH = X0(AKH);
+    return AMH / Depth;
+  }
+
+  // COMPUTE_KOCHIN.f90:25-152, analytical integration over the panels, with
+  // the source strengths ZIGB/ZIGS of the last solve
+  C kochin(R kwave, R Theta, R XEFF, R YEFF) {
+    const R PI = 4. * std::atan(1.);
+    const R CT = std::cos(Theta), ST = std::sin(Theta);
+    std::vector<C> ZS(2 * NFA + 1), CEP(NP + 1), CEM(NP + 1), ZJ(NP + 1);
+    for (int half = 0; half <= NSYMY; ++half) {
+      for (int k = 1; k <= NP; ++k) {
+        R wbar = (X[k] - XEFF) * CT + ((half ? -Y[k] : Y[k]) - YEFF) * ST;
+        ZJ[k] = C(kwave * Z[k], kwave * (-wbar));
+        if (ZJ[k].real() < -18.) CEP[k] = C(0., 0.);
+        else CEP[k] = std::exp(ZJ[k]);
+        C t = -ZJ[k] - 2. * kwave * Depth;
+        if ((t.real() < -18.) || (-kwave * Depth >= 0.)) CEM[k] = C(0., 0.);
+        else CEM[k] = std::exp(t);
+      }
+      for (int i = 1; i <= NFA; ++i) {
+        int KK[6] = {0, M1[i], M2[i], M3[i], M4[i], M1[i]};
+        C ZMS(half ? -YN[i] : YN[i], -(ZN[i] * ST));
+        C ZNS(XN[i], -(ZN[i] * CT));
+        C zs(0., 0.);
+        for (int L = 1; L <= 4; ++L) {
+          R dx = X[KK[L + 1]] - X[KK[L]], dy = Y[KK[L + 1]] - Y[KK[L]];
+          C ZCS = half ? ZMS * dx + ZNS * dy : ZMS * dx - ZNS * dy;
+          C ZC = ZJ[KK[L + 1]] - ZJ[KK[L]];
+          C ZHS, ZHD;
+          if (std::fabs(ZC.imag()) < 1.E-04 && std::fabs(ZC.real()) < 1.E-04) {
+            ZHS = 0.5 * (CEP[KK[L + 1]] + CEP[KK[L]]);
+            ZHD = -0.5 * (CEM[KK[L + 1]] + CEM[KK[L]]);
+          } else {
+            ZHS = (CEP[KK[L + 1]] - CEP[KK[L]]) / ZC;
+            ZHD = (CEM[KK[L + 1]] - CEM[KK[L]]) / ZC;
+          }
+          zs = zs + ZCS * ZHS + std::conj(ZCS * ZHD);
+        }
+        const R sgn = half ? -1. : 1.;
+        if ((kwave * Depth > 18.) || (kwave * Depth <= 0.)) zs = sgn * zs / kwave;
+        else zs = sgn * 0.5 * zs * std::exp(kwave * Depth) / std::sinh(kwave * Depth) * 1. / kwave;
+        ZS[i + half * NFA] = zs;
+      }
+    }
+    C H(0., 0.);
+    for (int i = 1; i <= NFA; ++i) {
+      H = H + ZIGB[i] * ZS[i];
+      if (NSYMY == 1) H = H + ZIGS[i] * ZS[i + NFA];
+    }
+    return 0.25 / PI * H;
+  }
+
   // matrices of one omega (no solve): D+, D-, S+, S- column-major NFA x NFA
   void assemble(R omega, C* dp, C* dm, C* sp, C* sm, int* depth_mode, int* nexp_out) {
     const R PI = 4. * std::atan(1.);
@@ -1925,7 +1986,11 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
   for (int j = 0; j < npb; ++j) omega[j] = std::stod(vo[j]);
   auto vt = bc.read(npb);
   for (int j = 0; j < npb; ++j) stype[j] = std::stod(vt[j]);
-  for (int k = 0; k < 3; ++k) bc.read(npb);
+  bc.read(npb);
+  bc.read(npb);
+  std::vector<int> sk(npb);
+  auto vk = bc.read(npb);
+  for (int j = 0; j < npb; ++j) sk[j] = std::stoi(vk[j]);
   std::vector<C> nvel((size_t)nc * npb);
   for (int c = 0; c < nc; ++c) {
     auto v = bc.read(2 * npb);
@@ -1934,6 +1999,8 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
   ListReader cal(dir + "/Nemoh.cal");
   cal.skip();
   double rho = cal.d(), g = cal.d(), depth = cal.d();
+  auto xy = cal.read(2);
+  double xeff = std::stod(xy[0]), yeff = std::stod(xy[1]);
   { ListReader inp(dir + "/input.txt"); inp.skip(); }
   ListReader ig(dir + "/mesh/Integration.dat");
   int nint = std::stoi(ig.read(1)[0]);
@@ -1942,7 +2009,12 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
     auto v = ig.read(nc);
     for (int c = 0; c < nc; ++c) nds[i + (size_t)nint * c] = std::stod(v[c]);
   }
-  { ListReader kr(dir + "/mesh/Kochin.dat"); kr.read(1); }
+  std::vector<double> theta;
+  {
+    ListReader kr(dir + "/mesh/Kochin.dat");
+    int nth = std::stoi(kr.read(1)[0]);
+    for (int j = 0; j < nth; ++j) theta.push_back(std::stod(kr.read(1)[0]));
+  }
   { ListReader fr(dir + "/mesh/Freesurface.dat"); fr.read(2); }
   Oracle o;
   o.cache_s = cache_s;
@@ -1951,6 +2023,20 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
   std::vector<C> force((size_t)nint * npb, C(0, 0)), pressure(nc);
   for (int j = 0; j < npb; ++j) {
     o.solve_bvp(2. * PI / omega[j], &nvel[(size_t)nc * j], pressure.data(), nullptr);
+    if (sk[j] == 1 && !theta.empty()) {
+      // SOLVE_BEM.f90:98-102 and OUTPUT.f90:25-40 (YEFF = 0 on symmetric meshes,
+      // INITIALIZATION.f90:60); file name with the I5 problem number
+      const double kw = o.kochin_kwave(2. * PI / omega[j]);
+      char name[32];
+      std::snprintf(name, sizeof name, "Kochin.%5d.dat", j + 1);
+      std::ofstream kf(dir + "/results/" + name);
+      for (double th : theta) {
+        C H = o.kochin(kw, th, xeff, isym == 1 ? 0. : yeff);
+        char line[96];
+        std::snprintf(line, sizeof line, " %.17E %.17E %.17E\n", th, std::abs(H), std::atan2(H.imag(), H.real()));
+        kf << line;
+      }
+    }
     for (int i = 0; i < nint; ++i)
       for (int c = 0; c < nc; ++c)
         force[i + (size_t)nint * j] = force[i + (size_t)nint * j] - pressure[c] * nds[i + (size_t)nint * c];
@@ -2072,6 +2158,24 @@ double nemoh_oracle_sample_solve(void* h, double omega, int nprob, double budget
 }
 
 int nemoh_oracle_get_nq(void* h) { return static_cast<Oracle*>(h)->NQ; }
+
+// COMPUTE_KOCHIN for the given source strengths (nfa x nprob complex each;
+// zigs ignored without symmetry): hkochin = ntheta x nprob complex
+int nemoh_oracle_kochin(void* h, double period, double xeff, double yeff, int ntheta, const double* theta,
+                        int nprob, const double* zigb, const double* zigs, double* hkochin) {
+  ORACLE_TRY({
+    Oracle* o = static_cast<Oracle*>(h);
+    const double kw = o->kochin_kwave(period);
+    const double ye = o->NSYMY == 1 ? 0. : yeff;
+    for (int p = 0; p < nprob; ++p) {
+      for (int i = 1; i <= o->NFA; ++i) {
+        o->ZIGB[i] = ((const C*)zigb)[(size_t)p * o->NFA + i - 1];
+        o->ZIGS[i] = (o->NSYMY == 1 && zigs) ? ((const C*)zigs)[(size_t)p * o->NFA + i - 1] : C(0., 0.);
+      }
+      for (int t = 0; t < ntheta; ++t) ((C*)hkochin)[t + (size_t)ntheta * p] = o->kochin(kw, theta[t], xeff, ye);
+    }
+  })
+}
 void nemoh_oracle_set_nq(void* h, int nq) { static_cast<Oracle*>(h)->NQ = nq; }
 
 int nemoh_oracle_run_case(const char* root, int cache_s, double* seconds) {

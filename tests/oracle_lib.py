@@ -51,6 +51,8 @@ def lib():
             L.nemoh_oracle_lisc.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
             L.nemoh_oracle_cint.argtypes = [ctypes.c_double, _d, _d]
             L.nemoh_oracle_gaussz_inverse.argtypes = [ctypes.c_int, _d, _d]
+            L.nemoh_oracle_kochin.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
             _lib = L
     return _lib
 
@@ -119,6 +121,18 @@ class Oracle:
                                                 *[a.ctypes.data_as(_d) for a in (zigb, zigs, zpb, zps, pres)],
                                                 ctypes.byref(nexp), ctypes.byref(fd)))
         return dict(zigb=zigb, zigs=zigs, zpb=zpb, zps=zps, pressure=pres, nexp=nexp.value, fd=fd.value)
+
+    def kochin(self, period, theta, zigb, zigs=None, xeff=0.0, yeff=0.0):
+        """COMPUTE_KOCHIN for given source strengths (n,) or (n, nprob): (ntheta, nprob)."""
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        zigb = np.asfortranarray(np.asarray(zigb, dtype=np.complex128).reshape(self.n, -1))
+        zigs = (np.asfortranarray(np.asarray(zigs, dtype=np.complex128).reshape(self.n, -1))
+                if zigs is not None else np.zeros_like(zigb))
+        out = np.zeros((len(theta), zigb.shape[1]), dtype=np.complex128, order="F")
+        _check(lib().nemoh_oracle_kochin(self.h, period, xeff, yeff, len(theta), theta.ctypes.data_as(_d),
+                                         zigb.shape[1], zigb.ctypes.data_as(_d), zigs.ctypes.data_as(_d),
+                                         out.ctypes.data_as(_d)))
+        return out
 
     @property
     def nq(self):

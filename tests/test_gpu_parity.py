@@ -217,3 +217,28 @@ def test_mixed_fallback_to_fp64_factors(tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     line = [l for l in r.stdout.splitlines() if l.startswith("ERR")][-1].split()
     assert float(line[1]) < 1e-10 and int(line[3]) == -1, line
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_kochin_matches_oracle(solver, case):
+    """COMPUTE_KOCHIN on the GPU vs the oracle, on the same source strengths:
+    every direction within 1e-9 of the problem's largest |H| (the force
+    tolerance; the panel sum cancels, so last-place differences of exp and of
+    the complex divisions grow to ~1e-11)."""
+    _mesh(solver, case)
+    o = G.oracle_for(case)
+    nv = C.body_conditions(case)
+    npb = len(case.betas_deg) + len(case.rad)
+    theta = np.linspace(0.0, 2.0 * np.pi, 37)
+    for w_idx in (0, len(case.omegas) - 1):
+        T = 2 * np.pi / case.omegas[w_idx]
+        cols = range(w_idx * npb, (w_idx + 1) * npb)
+        res = [solver.solve_potential(T, nv[:, j]) for j in cols]
+        zigb = np.stack([r["zigb"] for r in res], axis=1)
+        zigs = np.stack([r["zigs"] for r in res], axis=1)
+        H = solver.kochin(T, theta, zigb, zigs, xeff=1.5, yeff=-0.5)
+        Ho = o.kochin(T, theta, zigb, zigs if case.mesh.isym else None, xeff=1.5, yeff=-0.5)
+        scale = np.abs(Ho).max(axis=0)
+        assert np.all(scale > 0)
+        err = (np.abs(H - Ho) / scale).max()
+        assert err < 1e-9, (case.name, w_idx, err)

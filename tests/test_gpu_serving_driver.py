@@ -46,3 +46,31 @@ def test_dropin_driver_matches_oracle(tmp_path):
     F = np.loadtxt(str(tmp_path / "gpu" / "case" / "results" / "Forces.dat"), ndmin=2)
     got = G.decode_forces(case, F)
     assert G.rel_err(got, ref) < 1e-9
+
+
+def _kochin_files(d, nprob):
+    out = []
+    for p in range(nprob):
+        a = np.loadtxt(os.path.join(d, "case", "results", "Kochin.%5d.dat" % (p + 1)), ndmin=2)
+        out.append(a[:, 1] * np.exp(1j * a[:, 2]))
+    return a[:, 0], np.stack(out, axis=1)
+
+
+def test_dropin_driver_kochin_files_match_oracle(tmp_path):
+    """Kochin.<I5>.dat of every problem (symmetric finite-depth barge, wave
+    measurement point off the origin) against the oracle's reference run."""
+    import dataclasses
+    import oracle_lib as O
+    B.build()
+    case = dataclasses.replace(G.small_cases()[1], kochin_theta=tuple(np.linspace(0.0, np.pi, 13)), xeff=3.0,
+                               yeff=1.0)
+    C.write_case(case, str(tmp_path / "ref"))
+    O.run_case(str(tmp_path / "ref"))
+    C.write_case(case, str(tmp_path / "gpu"))
+    exe = os.path.join(ROOT, "nemoh_b200", "_build", "nemoh_solver_b200")
+    subprocess.run([exe, str(tmp_path / "gpu")], check=True)
+    th_r, Hr = _kochin_files(str(tmp_path / "ref"), case.nproblems)
+    th_g, Hg = _kochin_files(str(tmp_path / "gpu"), case.nproblems)
+    assert np.array_equal(th_r, th_g)
+    err = (np.abs(Hg - Hr) / np.abs(Hr).max(axis=0)).max()
+    assert err < 1e-9, err
