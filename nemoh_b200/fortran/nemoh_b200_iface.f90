@@ -62,6 +62,15 @@ MODULE NEMOH_B200_IFACE
             COMPLEX(C_DOUBLE_COMPLEX), DIMENSION(*) :: nvel, force
             REAL(C_DOUBLE), DIMENSION(*) :: nds
         END FUNCTION
+        INTEGER(C_INT) FUNCTION nemoh_b200_kochin(ctx, period, xeff, yeff, ntheta, theta, nprob, zigb, zigs, &
+                hkochin) BIND(C, NAME='nemoh_b200_kochin')
+            IMPORT :: C_PTR, C_INT, C_DOUBLE, C_DOUBLE_COMPLEX
+            TYPE(C_PTR), VALUE :: ctx
+            REAL(C_DOUBLE), VALUE :: period, xeff, yeff
+            INTEGER(C_INT), VALUE :: ntheta, nprob
+            REAL(C_DOUBLE), DIMENSION(*) :: theta
+            COMPLEX(C_DOUBLE_COMPLEX), DIMENSION(*) :: zigb, zigs, hkochin
+        END FUNCTION
     END INTERFACE
 
     TYPE(C_PTR), SAVE :: B200_CTX = C_NULL_PTR
@@ -135,6 +144,29 @@ CONTAINS
         END DO
         NEXP = NE
         DEALLOCATE(V, ZB, ZS, PB, PS)
+    END SUBROUTINE
+
+    ! Drop-in for COMPUTE_KOCHIN(kwave,Theta,HKochin) (SOLVE_BEM.f90:98-102): the
+    ! library derives kwave from the period T as SOLVE_BVP does and uses the
+    ! source strengths ZIGB, ZIGS of the last SOLVE_POTENTIAL_B200 call.
+    SUBROUTINE COMPUTE_KOCHIN_B200(Theta, HKochin)
+        USE COM_VAR
+        REAL :: Theta
+        COMPLEX :: HKochin
+        REAL(C_DOUBLE) :: TH(1)
+        COMPLEX(C_DOUBLE_COMPLEX), ALLOCATABLE :: ZB(:), ZS(:)
+        COMPLEX(C_DOUBLE_COMPLEX) :: H(1)
+        INTEGER :: I
+        ALLOCATE(ZB(NFA), ZS(NFA))
+        DO I = 1, NFA
+            ZB(I) = CMPLX(ZIGB(I), KIND=C_DOUBLE_COMPLEX)
+            ZS(I) = CMPLX(ZIGS(I), KIND=C_DOUBLE_COMPLEX)
+        END DO
+        TH(1) = REAL(Theta, C_DOUBLE)
+        CALL B200_CHECK(nemoh_b200_kochin(B200_CTX, REAL(T, C_DOUBLE), REAL(XEFF, C_DOUBLE), REAL(YEFF, C_DOUBLE), &
+                        1_C_INT, TH, 1_C_INT, ZB, ZS, H), 'kochin')
+        HKochin = H(1)
+        DEALLOCATE(ZB, ZS)
     END SUBROUTINE
 
     SUBROUTINE B200_FINALIZE
