@@ -96,6 +96,33 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* ctx, int nomega, const double
 int nemoh_b200_kochin(nemoh_ctx* ctx, double period, double xeff, double yeff, int ntheta, const double* theta,
                       int nprob, const double* zigb, const double* zigs, double* hkochin);
 
+/* Pre-processor body conditions on the device for the current mesh
+ * (preProcessor/Main.f90:201-243 with Mesh.f90:197-222, BodyConditions.f90:27-137,
+ * Environment.f90:45-100, Integration.f90:27-86): for nomega frequencies, nbeta
+ * headings (radians) and ndof radiation DOFs (kind 1 translation along dir, 2
+ * rotation about the axis through `axis` with direction dir; 3 doubles each;
+ * dof_body / panel_body select the panels of a body, both may be NULL for one
+ * body) it writes
+ *   nvel  (2^s nfa) x (nbeta + ndof) x nomega complex: NVEL of Normalvelocities.dat
+ *         (per frequency the headings, then the DOFs);
+ *   nds   nforce x (2^s nfa): the generalised normals of Integration.dat (or NULL);
+ *   fk    nforce x nbeta x nomega complex: Froude-Krylov forces (or NULL),
+ * with the wave measurement point (xeff, yeff) and the mesh's rho, g, depth. */
+int nemoh_b200_body_conditions(nemoh_ctx* ctx, const int* panel_body, double xeff, double yeff, int nomega,
+                               const double* omegas, int nbeta, const double* betas, int ndof, const int* dof_kind,
+                               const int* dof_body, const double* dof_dir, const double* dof_axis, int nforce,
+                               const int* force_kind, const int* force_body, const double* force_dir,
+                               const double* force_axis, double* nvel, double* nds, double* fk);
+/* Same with the outputs in device memory of the context's device, ordered
+ * after the work already on `stream` (cudaStream_t) and before what follows;
+ * nvel_device can go straight to nemoh_b200_solve_frequencies_device. */
+int nemoh_b200_body_conditions_device(nemoh_ctx* ctx, const int* panel_body, double xeff, double yeff, int nomega,
+                                      const double* omegas, int nbeta, const double* betas, int ndof,
+                                      const int* dof_kind, const int* dof_body, const double* dof_dir,
+                                      const double* dof_axis, int nforce, const int* force_kind, const int* force_body,
+                                      const double* force_dir, const double* force_axis, double* nvel_device,
+                                      double* nds_device, double* fk_device, void* stream);
+
 /* No counterpart in the reference: an entry point that allocates nothing, for
  * hosts whose device memory is held by their own allocator (a PyTorch caching
  * allocator, a batching server that admits work by free HBM) and for hosts

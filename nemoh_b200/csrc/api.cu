@@ -18,6 +18,7 @@
 #include "assembly.cuh"
 #include "fd_setup.h"
 #include "kochin.cuh"
+#include "preproc.cuh"
 #include "linalg.cuh"
 #include "mixed.cuh"
 
@@ -90,7 +91,7 @@ struct nemoh_ctx {
   double ro_eps2 = 0;   // largest x with sqrt(x) <= 1e-4
   DevBuf d_xyz, d_m, d_rec, d_rows;
   // per-call workspace
-  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin;
+  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin, d_pre;
   HostBuf h_oms, h_slots;
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
@@ -760,6 +761,110 @@ int nemoh_b200_kochin(nemoh_ctx* c, double period, double xeff, double yeff, int
     CK(cudaMemcpyAsync(hkochin, dh, nh * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
+}
+
+static int body_conditions_impl(nemoh_ctx* c, const int* panel_body, double xeff, double yeff, int nomega,
+                                const double* omegas, int nbeta, const double* betas, int ndof, const int* dof_kind,
+                                const int* dof_body, const double* dof_dir, const double* dof_axis, int nforce,
+                                const int* force_kind, const int* force_body, const double* force_dir,
+                                const double* force_axis, double* nvel_d, double* nds_d, double* fk_d,
+                                cudaStream_t user, bool host_out, double* nvel_h, double* nds_h, double* fk_h) {
+  if (!c || !c->nfa || nomega < 0 || nbeta < 0 || ndof < 0 || nforce < 0 || (nomega > 0 && !omegas) ||
+      (nbeta > 0 && !betas) || (ndof > 0 && (!dof_kind || !dof_dir || !dof_axis)) ||
+      (nforce > 0 && (!force_kind || !force_dir || !force_axis)))
+    return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    const int N = c->nfa, nc = N * (c->nsymy + 1), npb = nbeta + ndof;
+    std::vector<PreWave> waves((size_t)nomega * nbeta);
+    for (int w = 0; w < nomega; ++w) {
+      const double k = preproc_wavenumber(omegas[w], c->g, c->depth);
+      for (int b = 0; b < nbeta; ++b) waves[(size_t)w * nbeta + b] = PreWave{omegas[w], k, std::cos(betas[b]), std::sin(betas[b])};
+    }
+    auto spec = [](int n, const int* kind, const int* body, const double* dir, const double* axis) {
+      std::vector<PreDof> v(n);
+      for (int q = 0; q < n; ++q) {
+        if (kind[q] != 1 && kind[q] != 2) throw Fail{NEMOH_B200_EINVAL, "DOF kind must be 1 or 2"};
+        v[q].kind = kind[q];
+        v[q].body = body ? body[q] : 1;
+        for (int d = 0; d < 3; ++d) {
+          v[q].dir[d] = dir[3 * q + d];
+          v[q].axis[d] = axis[3 * q + d];
+        }
+      }
+      return v;
+    };
+    const std::vector<PreDof> dofs = spec(ndof, dof_kind, dof_body, dof_dir, dof_axis);
+    const std::vector<PreDof> frc = spec(nforce, force_kind, force_body, force_dir, force_axis);
+    const size_t n_nvel = (size_t)nc * npb * nomega, n_nds = (size_t)nforce * nc, n_fk = (size_t)nforce * nbeta * nomega;
+    // device staging: specs, waves, panel bodies, and (host outputs) the results
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    const size_t o_w = take(waves.size() * sizeof(PreWave)), o_d = take(dofs.size() * sizeof(PreDof)),
+                 o_f = take(frc.size() * sizeof(PreDof)), o_b = take(panel_body ? N * sizeof(int) : 0),
+                 o_nv = take(host_out ? n_nvel * sizeof(double2) : 0), o_nd = take(host_out ? n_nds * sizeof(double) : 0),
+                 o_fk = take(host_out ? n_fk * sizeof(double2) : 0);
+    CK(c->d_pre.ensure(std::max<size_t>(off, 256)));
+    char* base = c->d_pre.as<char>();
+    cudaStream_t st = c->stream;
+    cudaEvent_t e = nullptr;
+    if (!host_out) {
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      CK(cudaEventRecord(e, user));
+      CK(cudaStreamWaitEvent(st, e, 0));
+    }
+    if (!waves.empty()) CK(cudaMemcpyAsync(base + o_w, waves.data(), waves.size() * sizeof(PreWave), cudaMemcpyHostToDevice, st));
+    if (!dofs.empty()) CK(cudaMemcpyAsync(base + o_d, dofs.data(), dofs.size() * sizeof(PreDof), cudaMemcpyHostToDevice, st));
+    if (!frc.empty()) CK(cudaMemcpyAsync(base + o_f, frc.data(), frc.size() * sizeof(PreDof), cudaMemcpyHostToDevice, st));
+    if (panel_body) CK(cudaMemcpyAsync(base + o_b, panel_body, N * sizeof(int), cudaMemcpyHostToDevice, st));
+    double2* nv = host_out ? reinterpret_cast<double2*>(base + o_nv) : reinterpret_cast<double2*>(nvel_d);
+    double* nd = host_out ? (nds_h ? reinterpret_cast<double*>(base + o_nd) : nullptr) : nds_d;
+    double2* fk = host_out ? (fk_h ? reinterpret_cast<double2*>(base + o_fk) : nullptr) : reinterpret_cast<double2*>(fk_d);
+    if (fk && n_fk) CK(cudaMemsetAsync(fk, 0, n_fk * sizeof(double2), st));
+    if (nv || nd || fk) {
+      preproc_kernel<<<dim3((N + 127) / 128, c->nsymy + 1), 128, 0, st>>>(
+          c->d_xyz.as<double>(), c->d_m.as<int>(), panel_body ? reinterpret_cast<const int*>(base + o_b) : nullptr, N,
+          c->nsymy, c->rho, c->g, c->depth, xeff, yeff, reinterpret_cast<const PreWave*>(base + o_w), nomega, nbeta,
+          reinterpret_cast<const PreDof*>(base + o_d), ndof, reinterpret_cast<const PreDof*>(base + o_f), nforce, nv, nd,
+          fk);
+      LAUNCHED(c);
+    }
+    if (host_out) {
+      if (nvel_h && n_nvel) CK(cudaMemcpyAsync(nvel_h, nv, n_nvel * sizeof(double2), cudaMemcpyDeviceToHost, st));
+      if (nds_h && n_nds) CK(cudaMemcpyAsync(nds_h, nd, n_nds * sizeof(double), cudaMemcpyDeviceToHost, st));
+      if (fk_h && n_fk) CK(cudaMemcpyAsync(fk_h, fk, n_fk * sizeof(double2), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    } else {
+      CK(cudaEventRecord(e, st));
+      CK(cudaStreamWaitEvent(user, e, 0));
+      CK(cudaEventDestroy(e));
+      // the staged specs must outlive the kernel: wait before the next call may overwrite them
+      CK(cudaStreamSynchronize(st));
+    }
+  });
+}
+
+int nemoh_b200_body_conditions(nemoh_ctx* c, const int* panel_body, double xeff, double yeff, int nomega,
+                               const double* omegas, int nbeta, const double* betas, int ndof, const int* dof_kind,
+                               const int* dof_body, const double* dof_dir, const double* dof_axis, int nforce,
+                               const int* force_kind, const int* force_body, const double* force_dir,
+                               const double* force_axis, double* nvel, double* nds, double* fk) {
+  if (!nvel && (nomega * (nbeta + ndof)) > 0) return NEMOH_B200_EINVAL;
+  return body_conditions_impl(c, panel_body, xeff, yeff, nomega, omegas, nbeta, betas, ndof, dof_kind, dof_body,
+                              dof_dir, dof_axis, nforce, force_kind, force_body, force_dir, force_axis, nullptr,
+                              nullptr, nullptr, nullptr, true, nvel, nds, fk);
+}
+
+int nemoh_b200_body_conditions_device(nemoh_ctx* c, const int* panel_body, double xeff, double yeff, int nomega,
+                                      const double* omegas, int nbeta, const double* betas, int ndof,
+                                      const int* dof_kind, const int* dof_body, const double* dof_dir,
+                                      const double* dof_axis, int nforce, const int* force_kind, const int* force_body,
+                                      const double* force_dir, const double* force_axis, double* nvel_device,
+                                      double* nds_device, double* fk_device, void* stream) {
+  if (!nvel_device && (nomega * (nbeta + ndof)) > 0) return NEMOH_B200_EINVAL;
+  return body_conditions_impl(c, panel_body, xeff, yeff, nomega, omegas, nbeta, betas, ndof, dof_kind, dof_body,
+                              dof_dir, dof_axis, nforce, force_kind, force_body, force_dir, force_axis, nvel_device,
+                              nds_device, fk_device, reinterpret_cast<cudaStream_t>(stream), false, nullptr, nullptr,
+                              nullptr);
 }
 
 int nemoh_b200_last_refinement(nemoh_ctx* c, int* iterations, double* residual) {

@@ -380,6 +380,30 @@ void prony_fit(const double* xt, const double* yt, int nj, int& nm, double* lam,
 
 }  // namespace
 
+double preproc_wavenumber(double w, double g, double depth) {
+  double k = w * w / g;
+  const double x0 = k * depth;
+  if (x0 > 0. && x0 <= 20.) {
+    double xg = 0., xd = x0;
+    int nite = 0;
+    while (nite < 10000 && (x0 - xg * std::tanh(xg)) * (x0 - xd * std::tanh(xd)) > 0.) {
+      xg = xd;
+      xd = 2. * xd;
+      ++nite;
+    }
+    nite = 0;
+    double xc = 0.5 * (xd + xg);
+    while (nite < 10000 && std::fabs(xd - xg) / std::fabs(xc) >= 1.0e-6) {
+      xc = 0.5 * (xd + xg);
+      if ((x0 - xg * std::tanh(xg)) * (x0 - xc * std::tanh(xc)) > 0.) xg = xc;
+      else xd = xc;
+      ++nite;
+    }
+    k = xc / depth;
+  }
+  return k;
+}
+
 int finite_depth_root(double ak, double* out) {
   const double EPS = 5.E-6;
   int itour = 0, iiter = 0;

@@ -242,3 +242,23 @@ def test_kochin_matches_oracle(solver, case):
         assert np.all(scale > 0)
         err = (np.abs(H - Ho) / scale).max()
         assert err < 1e-9, (case.name, w_idx, err)
+
+
+@pytest.mark.parametrize("which", ["cylinder300_deep", "barge_half_fd50", "two_bodies_fd"])
+def test_device_body_conditions_match_preprocessor(solver, which):
+    """NVEL, NDS and Froude-Krylov forces computed on the GPU against the
+    pre-processor restatement in nemoh_b200.cases (1e-12 of each array's max)."""
+    import dataclasses
+    if which == "two_bodies_fd":
+        fx = V.load("2Bodies")
+        case = V.case_from_fixture(fx, omegas=fx["omegas"][4:7])
+        case = dataclasses.replace(case, betas_deg=np.array([0.0, 30.0]), xeff=2.0, yeff=-1.0)
+    else:
+        case = [c for c in CASES if c.name == which][0]
+        case = dataclasses.replace(case, betas_deg=np.array([0.0, 45.0, 120.0]), xeff=5.0, yeff=3.0)
+    _mesh(solver, case)
+    nvel, nds, fk = solver.body_conditions(case)
+    nv0, nds0, fk0 = C.body_conditions(case), C.generalised_normals(case), C.froude_krylov(case)
+    for got, ref in ((nvel, nv0), (nds, nds0), (fk, fk0)):
+        assert got.shape == ref.shape
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), which
