@@ -96,6 +96,14 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* ctx, int nomega, const double
 int nemoh_b200_kochin(nemoh_ctx* ctx, double period, double xeff, double yeff, int ntheta, const double* theta,
                       int nprob, const double* zigb, const double* zigs, double* hkochin);
 
+/* Free-surface elevation (COMPUTE_POTENTIAL_DOMAIN.f90:24-82 with
+ * COMPUTE_GREEN_FREESURFACE.f90, as called at SOLVE_BEM.f90:104-109): for source
+ * strengths zigb, zigs (nfa x nprob complex each; zigs unused without symmetry)
+ * of problems at period `period`, ETA = i W / G PHI at the npts points
+ * (x, y, 0) of xy (2 x npts, mesh/Freesurface.dat). eta: npts x nprob complex. */
+int nemoh_b200_free_surface(nemoh_ctx* ctx, double period, int npts, const double* xy, int nprob,
+                            const double* zigb, const double* zigs, double* eta);
+
 /* Pre-processor body conditions on the device for the current mesh
  * (preProcessor/Main.f90:201-243 with Mesh.f90:197-222, BodyConditions.f90:27-137,
  * Environment.f90:45-100, Integration.f90:27-86): for nomega frequencies, nbeta

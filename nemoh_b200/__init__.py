@@ -77,6 +77,7 @@ def load_library():
                                              _d]
     L.nemoh_b200_kochin.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
                                     ctypes.c_int, _d, _d, _d]
+    L.nemoh_b200_free_surface.argtypes = [_vp, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
     L.nemoh_b200_launch_count.restype = ctypes.c_longlong
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
     L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
@@ -249,6 +250,22 @@ class Solver:
         self._check(load_library().nemoh_b200_kochin(self._h, float(period), float(xeff), float(yeff), len(theta),
                                                      _p(theta), nprob, zigb.ctypes.data_as(_d),
                                                      zigs.ctypes.data_as(_d), out.ctypes.data_as(_d)))
+        return out
+
+    # -- COMPUTE_POTENTIAL_DOMAIN on the free surface --------------------------
+    def free_surface(self, period, xy, zigb, zigs=None):
+        """Free-surface elevation ETA = i W/G PHI at the points (x, y, 0) of xy
+        (npts, 2) for problems solved at `period` from their source strengths
+        (nfa,) or (nfa, nprob); returns (npts, nprob) complex."""
+        xy = np.ascontiguousarray(np.asarray(xy, dtype=np.float64).reshape(-1, 2))
+        zigb = np.asfortranarray(np.asarray(zigb, dtype=np.complex128).reshape(self.nfa, -1))
+        nprob = zigb.shape[1]
+        zigs = (np.asfortranarray(np.asarray(zigs, dtype=np.complex128).reshape(self.nfa, -1))
+                if zigs is not None else np.zeros_like(zigb))
+        out = np.zeros((xy.shape[0], nprob), dtype=np.complex128, order="F")
+        self._check(load_library().nemoh_b200_free_surface(self._h, float(period), xy.shape[0], _p(xy), nprob,
+                                                           zigb.ctypes.data_as(_d), zigs.ctypes.data_as(_d),
+                                                           out.ctypes.data_as(_d)))
         return out
 
     # -- diagnostics -----------------------------------------------------------

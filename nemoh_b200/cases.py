@@ -103,6 +103,7 @@ class Case:
     yeff: float = 0.0
     name: str = "case"
     kochin_theta: tuple = ()   # directions (rad) of mesh/Kochin.dat; Kochin switch set for every problem if any
+    fs_grid: tuple = ()        # (Nx, Ny, Lx, Ly) of Nemoh.cal's free-surface line; free-surface switch set if any
 
     @property
     def nproblems(self) -> int:
@@ -438,6 +439,17 @@ def _r(v) -> str:
     return repr(float(v))
 
 
+def freesurface_grid(nx, ny, lx, ly):
+    """Free-surface visualisation grid of the pre-processor (preProcessor/Main.f90:287-300):
+    nx * ny points (x, y) on an lx by ly rectangle centred on the origin, x
+    outer and y inner, and the (nx-1)(ny-1) quadrangles as 1-based point numbers."""
+    nx, ny = int(nx), int(ny)
+    pts = [(-0.5 * lx + lx * i / (nx - 1), -0.5 * ly + ly * j / (ny - 1)) for i in range(nx) for j in range(ny)]
+    quads = [(j + 1 + i * ny, j + 2 + i * ny, j + 2 + (i + 1) * ny, j + 1 + (i + 1) * ny)
+             for i in range(nx - 1) for j in range(ny - 1)]
+    return np.array(pts), np.array(quads, dtype=np.int64).reshape(-1, 4)
+
+
 def write_case(case: Case, root: str, case_dir: str = "case") -> str:
     """Write ID.dat in `root` and the case directory `root/case_dir`."""
     mesh = case.mesh
@@ -471,7 +483,11 @@ def write_case(case: Case, root: str, case_dir: str = "case") -> str:
         f.write("%d %s %s\n" % (len(om), _r(om[0]), _r(om[-1])))
         bt = case.betas_deg
         f.write("%d %s %s\n" % (len(bt), _r(bt[0]) if len(bt) else "0.", _r(bt[-1]) if len(bt) else "0."))
-        f.write("--- Post processing ---\n0 0.1 10.\n0\n0 0. 180.\n0 0 100. 100.\n")
+        kt = np.degrees(np.asarray(case.kochin_theta, dtype=float))
+        fsg = tuple(case.fs_grid) if len(case.fs_grid) else (0, 0, 100.0, 100.0)
+        f.write("--- Post processing ---\n0 0.1 10.\n0\n%d %s %s\n%d %d %s %s\n"
+                % (len(kt), _r(kt[0]) if len(kt) else "0.", _r(kt[-1]) if len(kt) else "180.",
+                   int(fsg[0]), int(fsg[1]), _r(fsg[2]), _r(fsg[3])))
     with open(os.path.join(d, "input.txt"), "w") as f:
         f.write("--- Calculation parameters ---\n0\n")
     # L12: "2 Isym", nodes, 0-line, panels, 0-line (Common/Mesh.f90:102-118)
@@ -503,8 +519,9 @@ def write_case(case: Case, root: str, case_dir: str = "case") -> str:
         f.write(" ".join(_r(w) for w in case.omegas for _ in range(npb)) + "\n")
         for _ in case.omegas:
             f.write(" ".join([_r(b * math.pi / 180.0) for b in case.betas_deg] + ["-1.0"] * nr) + "\n")
-        for _ in range(2):
-            f.write(" ".join("0" for _ in range(case.nproblems)) + "\n")
+        f.write(" ".join("0" for _ in range(case.nproblems)) + "\n")
+        sfs = "1" if len(case.fs_grid) and case.fs_grid[0] > 0 else "0"
+        f.write(" ".join(sfs for _ in range(case.nproblems)) + "\n")
         sk = "1" if len(case.kochin_theta) else "0"
         f.write(" ".join(sk for _ in range(case.nproblems)) + "\n")
         for c in range(nvel.shape[0]):
@@ -514,7 +531,15 @@ def write_case(case: Case, root: str, case_dir: str = "case") -> str:
         for t in case.kochin_theta:
             f.write("%s\n" % _r(t))
     with open(os.path.join(d, "mesh", "Freesurface.dat"), "w") as f:
-        f.write("0 0\n")
+        if len(case.fs_grid) and case.fs_grid[0] > 0:
+            pts, quads = freesurface_grid(*case.fs_grid)
+            f.write("%d %d\n" % (len(pts), len(quads)))
+            for x, y in pts:
+                f.write("%s %s 0.\n" % (_r(x), _r(y)))
+            for q in quads:
+                f.write("%d %d %d %d\n" % tuple(q))
+        else:
+            f.write("0 0\n")
     fk = froude_krylov(case)
     with open(os.path.join(d, "results", "FKForce.dat"), "w") as f:
         for k in range(len(case.force)):

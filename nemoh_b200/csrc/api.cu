@@ -19,6 +19,7 @@
 #include "fd_setup.h"
 #include "kochin.cuh"
 #include "preproc.cuh"
+#include "freesurface.cuh"
 #include "linalg.cuh"
 #include "mixed.cuh"
 
@@ -91,7 +92,7 @@ struct nemoh_ctx {
   double ro_eps2 = 0;   // largest x with sqrt(x) <= 1e-4
   DevBuf d_xyz, d_m, d_rec, d_rows;
   // per-call workspace
-  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin, d_pre;
+  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin, d_pre, d_fs;
   HostBuf h_oms, h_slots;
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
@@ -760,6 +761,66 @@ int nemoh_b200_kochin(nemoh_ctx* c, double period, double xeff, double yeff, int
     LAUNCHED(c);
     CK(cudaMemcpyAsync(hkochin, dh, nh * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int nemoh_b200_free_surface(nemoh_ctx* c, double period, int npts, const double* xy, int nprob, const double* zigb,
+                            const double* zigs, double* eta) {
+  if (!c || !c->nfa || !(period > 0) || npts < 0 || nprob < 0 || (npts > 0 && (!xy || !eta)) ||
+      (nprob > 0 && !zigb) || (nprob > 0 && c->nsymy && !zigs))
+    return NEMOH_B200_EINVAL;
+  if (npts == 0 || nprob == 0) return NEMOH_B200_OK;
+  return guarded(c, [&] {
+    const int N = c->nfa;
+    const double W = 2. * kPI / period;
+    OmegaParams om;
+    omega_params(c, W, om, false);
+    // COMPUTE_POTENTIAL_DOMAIN.f90:46 picks the deep-water forms when Depth = 0
+    // or AMH >= 20, AMH being kwave*Depth on the deep-water path of SOLVE_BVP
+    const double amh = om.fd ? om.amh : om.k0 * c->depth;
+    const bool fd = !((c->depth == 0.) || (amh >= 20));
+    const size_t ns = (size_t)N * FS_MAXP, nphi = (size_t)npts * FS_MAXP;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    const size_t o_om = take(sizeof(OmegaParams)), o_xy = take(npts * sizeof(double2)),
+                 o_b = take(ns * sizeof(double2)), o_s = take(ns * sizeof(double2)), o_p = take(nphi * sizeof(double2));
+    CK(c->d_fs.ensure(off));
+    char* base = c->d_fs.as<char>();
+    cudaStream_t st = c->stream;
+    CK(cudaMemcpyAsync(base + o_om, &om, sizeof om, cudaMemcpyHostToDevice, st));
+    std::vector<double2> pts(npts);
+    for (int q = 0; q < npts; ++q) pts[q] = make_double2(xy[2 * q], xy[2 * q + 1]);
+    CK(cudaMemcpyAsync(base + o_xy, pts.data(), npts * sizeof(double2), cudaMemcpyHostToDevice, st));
+    GreenCtx g = green_ctx(c);
+    std::vector<std::complex<double>> phi(nphi);
+    const std::complex<double> scale(0., W / c->g);   // ETA = i W / G PHI
+    for (int p0 = 0; p0 < nprob; p0 += FS_MAXP) {
+      const int np = std::min(FS_MAXP, nprob - p0);
+      CK(cudaMemcpyAsync(base + o_b, zigb + 2 * (size_t)N * p0, (size_t)N * np * sizeof(double2),
+                         cudaMemcpyHostToDevice, st));
+      if (c->nsymy)
+        CK(cudaMemcpyAsync(base + o_s, zigs + 2 * (size_t)N * p0, (size_t)N * np * sizeof(double2),
+                           cudaMemcpyHostToDevice, st));
+      CK(cudaMemsetAsync(base + o_p, 0, (size_t)npts * np * sizeof(double2), st));
+      const dim3 grid((npts + FS_POINTS - 1) / FS_POINTS, (N + FS_PANELS - 1) / FS_PANELS);
+      auto args = [&](auto kernel) {
+        kernel<<<grid, FS_POINTS, 0, st>>>(g, reinterpret_cast<const OmegaParams*>(base + o_om),
+                                           c->d_rec.as<PanelRec>(), N, reinterpret_cast<const double2*>(base + o_xy),
+                                           npts, np, reinterpret_cast<const double2*>(base + o_b),
+                                           reinterpret_cast<const double2*>(base + o_s),
+                                           reinterpret_cast<double2*>(base + o_p));
+      };
+      if (fd) args(freesurface_kernel<true>);
+      else args(freesurface_kernel<false>);
+      LAUNCHED(c);
+      CK(cudaMemcpyAsync(phi.data(), base + o_p, (size_t)npts * np * sizeof(double2), cudaMemcpyDeviceToHost, st));
+      check_status(c);
+      for (size_t q = 0; q < (size_t)npts * np; ++q) {
+        const std::complex<double> e = scale * phi[q];
+        eta[2 * ((size_t)npts * p0 + q)] = e.real();
+        eta[2 * ((size_t)npts * p0 + q) + 1] = e.imag();
+      }
+    }
   });
 }
 

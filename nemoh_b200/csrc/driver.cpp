@@ -11,10 +11,12 @@
 // Problems are solved a frequency at a time: consecutive problems that share
 // a frequency go to one nemoh_b200_solve_frequencies call (one assembly and
 // one factorization for all of them, as the reference's w_previous cache).
-// Problems whose Kochin switch is set are also solved through
-// nemoh_b200_solve_problem for their source strengths, and their Kochin
-// functions are written to results/Kochin.<I5>.dat (SOLVE_BEM.f90:98-102,
-// OUTPUT.f90:25-40). Free-surface and pressure outputs are not produced.
+// Problems whose Kochin or free-surface switch is set are also solved through
+// nemoh_b200_solve_problem for their source strengths; their Kochin functions
+// go to results/Kochin.<I5>.dat (SOLVE_BEM.f90:98-102, OUTPUT.f90:25-40) and
+// their free-surface elevations at the points of mesh/Freesurface.dat to
+// results/freesurface.<I5>.dat (SOLVE_BEM.f90:104-109, OUTPUT.f90:42-64).
+// Pressure outputs (Switch_Potential) are not produced.
 //
 // usage: nemoh_solver_b200 [case-root] [--mixed] [--device N]
 #include <cmath>
@@ -121,8 +123,11 @@ int main(int argc, char** argv) {
     auto vt = bc.read(npb);
     for (int j = 0; j < npb; ++j) stype[j] = std::stod(vt[j]);
     bool extra_outputs = false;
-    for (int k = 0; k < 2; ++k) {
-      for (const auto& t : bc.read(npb)) extra_outputs |= std::stoi(t) != 0;
+    for (const auto& t : bc.read(npb)) extra_outputs |= std::stoi(t) != 0;   // Switch_Potential
+    std::vector<int> fs_switch(npb);
+    {
+      const auto v = bc.read(npb);
+      for (int j = 0; j < npb; ++j) fs_switch[j] = std::stoi(v[j]);
     }
     std::vector<int> kochin_switch(npb);
     {
@@ -156,12 +161,19 @@ int main(int argc, char** argv) {
       const int nth = kr.integer();
       for (int j = 0; j < nth; ++j) theta.push_back(kr.real());
     }
+    std::vector<double> fs_xy;   // 2 x npts
+    std::vector<int> fs_quads;   // 4 x nquads
     {
       Records fr(dir + "/mesh/Freesurface.dat");
-      extra_outputs |= std::stoi(fr.read(2)[0]) > 0;
+      const auto v = fr.read(2);
+      const int npts = std::stoi(v[0]), nquads = std::stoi(v[1]);
+      for (int q = 0; q < npts; ++q)
+        for (const auto& t : fr.read(2)) fs_xy.push_back(std::stod(t));
+      for (int q = 0; q < nquads; ++q)
+        for (const auto& t : fr.read(4)) fs_quads.push_back(std::stoi(t));
     }
-    if (extra_outputs)
-      std::fprintf(stderr, "nemoh_solver_b200: free-surface / pressure outputs are not produced\n");
+    const int fs_npts = (int)fs_xy.size() / 2;
+    if (extra_outputs) std::fprintf(stderr, "nemoh_solver_b200: pressure outputs are not produced\n");
 
     nemoh_ctx* ctx = nullptr;
     check(nullptr, nemoh_b200_create(&ctx, device, mode), "create");
@@ -182,32 +194,63 @@ int main(int argc, char** argv) {
         for (int i = 0; i < nint; ++i) force[i + (size_t)nint * (j + p)] = f[i + (size_t)nint * p];
       j = e;
     }
-    // Kochin functions of the problems that ask for them
-    if (!theta.empty()) {
-      std::vector<std::complex<double>> zigb(nfa), zigs(nfa), h(theta.size());
+    // Kochin functions and free-surface elevations of the problems that ask for them
+    {
+      std::vector<std::complex<double>> zigb(nfa), zigs(nfa), h(theta.size()), eta(fs_npts);
       const double PI = 4. * std::atan(1.);
       for (int p = 0; p < npb; ++p) {
-        if (kochin_switch[p] != 1) continue;
+        const bool want_fs = fs_switch[p] == 1 && fs_npts > 0, want_k = kochin_switch[p] == 1 && !theta.empty();
+        if (!want_fs && !want_k) continue;
+        const double period = 2. * PI / omega[p];
         int nexp = 0;
         check(ctx,
-              nemoh_b200_solve_problem(ctx, 2. * PI / omega[p], reinterpret_cast<const double*>(&nvel[(size_t)nc * p]),
+              nemoh_b200_solve_problem(ctx, period, reinterpret_cast<const double*>(&nvel[(size_t)nc * p]),
                                        reinterpret_cast<double*>(zigb.data()), reinterpret_cast<double*>(zigs.data()),
                                        nullptr, nullptr, &nexp),
               "solve_problem");
-        check(ctx,
-              nemoh_b200_kochin(ctx, 2. * PI / omega[p], xeff, yeff, (int)theta.size(), theta.data(), 1,
-                                reinterpret_cast<const double*>(zigb.data()),
-                                reinterpret_cast<const double*>(zigs.data()), reinterpret_cast<double*>(h.data())),
-              "kochin");
-        char name[32];
-        std::snprintf(name, sizeof name, "Kochin.%5d.dat", p + 1);
-        std::ofstream kf(dir + "/results/" + name);
-        if (!kf) throw IoError("cannot write " + dir + "/results/" + name);
-        char line[96];
-        for (size_t t = 0; t < theta.size(); ++t) {
-          std::snprintf(line, sizeof line, " %.17E %.17E %.17E\n", theta[t], std::abs(h[t]),
-                        std::atan2(h[t].imag(), h[t].real()));
-          kf << line;
+        char name[40];
+        if (want_fs) {
+          check(ctx,
+                nemoh_b200_free_surface(ctx, period, fs_npts, fs_xy.data(), 1,
+                                        reinterpret_cast<const double*>(zigb.data()),
+                                        reinterpret_cast<const double*>(zigs.data()),
+                                        reinterpret_cast<double*>(eta.data())),
+                "free_surface");
+          std::snprintf(name, sizeof name, "freesurface.%5d.dat", p + 1);
+          std::ofstream ff(dir + "/results/" + name);
+          if (!ff) throw IoError("cannot write " + dir + "/results/" + name);
+          ff << " VARIABLES=\"X\" \"Y\" \"abs(eta) (m)\" \"angle(phi) (rad)\" \"PRE1\" \"PRE2\"\n";
+          char line[160];
+          std::snprintf(line, sizeof line, "ZONE N=%7d ,E = %7d ,F=FEPOINT,ET=QUADRILATERAL\n", fs_npts,
+                        (int)fs_quads.size() / 4);
+          ff << line;
+          for (int q = 0; q < fs_npts; ++q) {
+            const std::complex<double> e = eta[q];
+            std::snprintf(line, sizeof line, " %.17E %.17E %.17E %.17E %.17E %.17E\n", fs_xy[2 * q], fs_xy[2 * q + 1],
+                          std::abs(e), std::atan2(e.imag(), e.real()), e.real(), e.imag());
+            ff << line;
+          }
+          for (size_t q = 0; q < fs_quads.size(); q += 4) {
+            std::snprintf(line, sizeof line, " %d %d %d %d\n", fs_quads[q], fs_quads[q + 1], fs_quads[q + 2],
+                          fs_quads[q + 3]);
+            ff << line;
+          }
+        }
+        if (want_k) {
+          check(ctx,
+                nemoh_b200_kochin(ctx, period, xeff, yeff, (int)theta.size(), theta.data(), 1,
+                                  reinterpret_cast<const double*>(zigb.data()),
+                                  reinterpret_cast<const double*>(zigs.data()), reinterpret_cast<double*>(h.data())),
+                "kochin");
+          std::snprintf(name, sizeof name, "Kochin.%5d.dat", p + 1);
+          std::ofstream kf(dir + "/results/" + name);
+          if (!kf) throw IoError("cannot write " + dir + "/results/" + name);
+          char line[96];
+          for (size_t t = 0; t < theta.size(); ++t) {
+            std::snprintf(line, sizeof line, " %.17E %.17E %.17E\n", theta[t], std::abs(h[t]),
+                          std::atan2(h[t].imag(), h[t].real()));
+            kf << line;
+          }
         }
       }
     }

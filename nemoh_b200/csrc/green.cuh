@@ -236,13 +236,13 @@ __device__ __noinline__ void rankine_near(double XOI, double YOI, double ZOI, co
 // (VAVINFD/VAVFD combination, COMPUTE_GREEN_INFD.f90:176-216).
 template <bool FD>
 __device__ __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI, double YGI, double ZGI, bool self,
-                                        const PanelRec& P, RankineOut& o) {
+                                        const PanelRec& P, RankineOut& o, bool clip = true) {
   const double QPI = 4. * 3.141592653589793;
   const double DPI = 2. * 3.141592653589793;
   const int NJJ = 2 * (g.nsymy + 1);
   const double MK = FD ? -1. : 1.;
   double XOI = XGI, YOI = YGI, ZOI = ZGI;
-  if (ZGI > g.zer) ZOI = FD ? XMUL(20., g.zer) : g.zer;
+  if (clip && ZGI > g.zer) ZOI = FD ? XMUL(20., g.zer) : g.zer;
   const double lim7 = XMUL(7., P.tdis);
   o = RankineOut{0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 1

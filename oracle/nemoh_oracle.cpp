@@ -1804,6 +1804,275 @@ struct Oracle {
     return 0.25 / PI * H;
   }
 
+  // ---- COMPUTE_GREEN_FREESURFACE.f90 + COMPUTE_POTENTIAL_DOMAIN.f90 ---------
+  // Green functions at a field point (XPO, YPO, ZPO) off the mesh; only the
+  // single-layer values SP1, SP2, SM1, SM2 that COMPUTE_POTENTIAL_DOMAIN uses.
+  // VVV (:33-196) is VAV with the field point past the collocation points (no
+  // ZER clip, no self term) and DHSL = 2*Depth for both KKK.
+  void VVV(int KKK, int J, R XOI, R YOI, R ZOI) { VAV(KKK, 2. * Depth, XOI, YOI, ZOI, IMX + 1, J); }
+
+  // VNV (:199-386): tabulated branch of VNSINFD at the unclipped field point
+  void VNV(int J, R XPO, R YPO, R ZPO) {
+    const R PI4 = std::atan(1.), PI = 4. * std::atan(1.), DPI = 2. * PI, DPI2 = 2. * sq(PI);
+    const R EPS = 0.0001;
+    R WH = DPI / T, WR = WH;
+    R AK0 = sq(WR) / G;
+    int NJJ = NSYMY + 1;
+    R FS1[3] = {0, 0, 0}, FS2[3] = {0, 0, 0};
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
+      int BX = (JJ % 2 == 1) ? 1 : -1;
+      R YMJJJ = YG[J] * BX;
+      R RRR = std::sqrt(sq(XPO - XG[J]) + sq(YPO - YMJJJ));
+      R AKR = AK0 * RRR;
+      R ZZZ = ZPO + ZG[J];
+      R AKZ = AK0 * ZZZ;
+      R DD = std::sqrt(sq(RRR) + sq(ZZZ));
+      R PSURR = (DD > EPS) ? PI / cube(AK0 * DD) : 0.;
+      R PD1Z, PD2Z;
+      if (AKZ > -1.5E-6) throw Stop(ST_AKZ_UNDEFINED, "AKZ < -1.5 E-6");
+      if (AKZ > -16.) {
+        if (AKR < 99.7) {
+          int KJ, KI;
+          stencil_kj(AKZ, KJ);
+          stencil_ki(AKR, KI);
+          R XL1 = PL2(XR[KI], XR[KI + 1], XR[KI - 1], AKR);
+          R XL2 = PL2(XR[KI + 1], XR[KI - 1], XR[KI], AKR);
+          R XL3 = PL2(XR[KI - 1], XR[KI], XR[KI + 1], AKR);
+          R ZL1 = PL2(XZ[KJ], XZ[KJ + 1], XZ[KJ - 1], AKZ);
+          R ZL2 = PL2(XZ[KJ + 1], XZ[KJ - 1], XZ[KJ], AKZ);
+          R ZL3 = PL2(XZ[KJ - 1], XZ[KJ], XZ[KJ + 1], AKZ);
+          PD1Z = interp(APD1Z, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+          PD2Z = interp(APD2Z, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+        } else {
+          R EPZ = std::exp(AKZ);
+          R AKP4 = AKR - PI4;
+          R SQ = std::sqrt(DPI / AKR);
+          R CSK = std::cos(AKP4), SIK = std::sin(AKP4);
+          PD1Z = PSURR * AKZ - PI * EPZ * SQ * SIK;
+          PD2Z = EPZ * SQ * CSK;
+        }
+      } else {
+        PD1Z = PSURR * AKZ;
+        PD2Z = 0.;
+      }
+      FS1[JJ] = PD1Z;
+      FS2[JJ] = PD2Z;
+    }
+    R AKAIR = AK0 * AIRE[J];
+    R ADPI2 = AKAIR / DPI2, ADPI = AKAIR / DPI;
+    if (NSYMY == 1) {
+      SM1 = FSM - (FS1[1] - FS1[2]) * ADPI2;
+      SP1 = FSP - (FS1[1] + FS1[2]) * ADPI2;
+      SM2 = -(FS2[1] - FS2[2]) * ADPI;
+      SP2 = -(FS2[1] + FS2[2]) * ADPI;
+    } else {
+      SP1 = FSP - FS1[1] * ADPI2;
+      SM1 = SP1;
+      SP2 = -FS2[1] * ADPI;
+      SM2 = SP2;
+    }
+  }
+
+  // VVG (:911-997): exact panel integral of 1/r at a point, single-layer part
+  R VVG(const R* XLL, const R* YLL, const R* ZLL, int JJ, R PN, R QN, R RN, R ARJ, R TDJ, R XGG, R YGG, R ZGG,
+        R XPO, R YPO, R ZPO) {
+    int MJJ = (JJ % 2 == 1) ? 1 : -1;
+    R RO = std::sqrt(sq(XPO - XGG) + sq(YPO - YGG * MJJ) + sq(ZPO - ZGG));
+    R GZ = (XPO - XGG) * PN + (YPO - YGG * MJJ) * QN * MJJ + (ZPO - ZGG) * RN;
+    if (RO - 7. * TDJ > 0.) return -ARJ / (RO * 12.5663706);
+    R RR[6];
+    for (int L = 1; L <= 5; ++L) RR[L] = std::sqrt(sq(XPO - XLL[L]) + sq(YPO - YLL[L] * MJJ) + sq(ZPO - ZLL[L]));
+    R FS = 0.;
+    for (int L = 1; L <= 4; ++L) {
+      R DK = std::sqrt(sq(XLL[L + 1] - XLL[L]) + sq(YLL[L + 1] - YLL[L]) + sq(ZLL[L + 1] - ZLL[L]));
+      if (DK - 1.E-3 * TDJ <= 0.) continue;
+      R PJ = (XLL[L + 1] - XLL[L]) / DK;
+      R QJ = (YLL[L + 1] - YLL[L]) / DK * MJJ;
+      R RJ = (ZLL[L + 1] - ZLL[L]) / DK;
+      R GYX = MJJ * QN * RJ - RN * QJ;
+      R GYY = RN * PJ - PN * RJ;
+      R GYZ = PN * QJ - QN * MJJ * PJ;
+      R GY = (XPO - XLL[L]) * GYX + (YPO - YLL[L] * MJJ) * GYY + (ZPO - ZLL[L]) * GYZ;
+      R DDK = 2. * DK;
+      R ANT = GY * DDK;
+      R DNT = sq(RR[L + 1] + RR[L]) - DK * DK + 2. * std::fabs(GZ) * (RR[L + 1] + RR[L]);
+      R ARG = ANT / DNT;
+      R ANL = RR[L + 1] + RR[L] + DK;
+      R DNL = RR[L + 1] + RR[L] - DK;
+      R DEN = ANL / DNL;
+      R AT = (std::fabs(GZ) >= 1.E-4 * TDJ) ? std::atan(ARG) : 0.;
+      R ALDEN = std::log(DEN);
+      FS = FS + GY * ALDEN - 2. * std::fabs(GZ) * AT;
+    }
+    R CM = -MJJ / 12.5663706;
+    return FS * CM;
+  }
+
+  // VNVF (:388-908): tabulated branch of VNSFD at the unclipped field point;
+  // the exponential images with, for the last term, the exact panel integral
+  // (VVG) at the field point's mirror image
+  void VNVF(R AM0, R AMH, int NEXP, int J, R XPO, R YPO, R ZPO) {
+    const R PI4 = std::atan(1.), PI = 4. * std::atan(1.), DPI = 2. * PI, QPI = 4. * PI;
+    const R EPS = 0.0001;
+    R H = Depth;
+    R AKH = AMH * std::tanh(AMH);
+    int NJJ = NSYMY + 1;
+    R A = sq(AMH + AKH) / (H * (sq(AMH) - sq(AKH) + AKH));
+    int NEXP1 = NEXP + 1;
+    AMBDA[NEXP1] = 0.;
+    AR[NEXP1] = 2.;
+    R COE3 = -1. / (8. * sq(PI));
+    R COE4 = -A / (8. * PI);
+    R FS1[3] = {0, 0, 0}, FS2[3] = {0, 0, 0};
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
+      int BX = (JJ % 2 == 1) ? 1 : -1;
+      R YMJJJ = BX * YG[J];
+      R COF1 = A * COE3 * AIRE[J];
+      R COF2 = COE4 * AIRE[J];
+      R RRR = std::sqrt(sq(XPO - XG[J]) + sq(YPO - YMJJJ));
+      R AKR = AM0 * RRR;
+      R ZZZ[5] = {0., ZPO + ZG[J], ZG[J] - ZPO - 2 * H, ZPO - ZG[J] - 2 * H, -ZG[J] - ZPO - 4 * H};
+      R XL1 = 0, XL2 = 0, XL3 = 0, PSK = 0, SCK = 0;
+      int KI = 0;
+      R PD1Z[5], PD2Z[5], PSR[5];
+      for (int k = 1; k <= 4; ++k) {
+        R AKZ = AM0 * ZZZ[k];
+        R DD = std::sqrt(sq(RRR) + sq(ZZZ[k]));
+        R PSURR;
+        if (DD > EPS) {
+          R RRk = AM0 * DD;
+          PSR[k] = PI / RRk;
+          PSURR = PI / cube(RRk);
+        } else {
+          PSR[k] = 0.;
+          PSURR = 0.;
+        }
+        if (AKZ > -1.5E-6) throw Stop(ST_AKZ_UNDEFINED, "AKZ < -1.5 E-6");
+        if (AKZ > -16.) {
+          if (AKR < 99.7) {
+            int KJ;
+            stencil_kj(AKZ, KJ);
+            stencil_ki(AKR, KI);
+            XL1 = PL2(XR[KI], XR[KI + 1], XR[KI - 1], AKR);
+            XL2 = PL2(XR[KI + 1], XR[KI - 1], XR[KI], AKR);
+            XL3 = PL2(XR[KI - 1], XR[KI], XR[KI + 1], AKR);
+            R ZL1 = PL2(XZ[KJ], XZ[KJ + 1], XZ[KJ - 1], AKZ);
+            R ZL2 = PL2(XZ[KJ + 1], XZ[KJ - 1], XZ[KJ], AKZ);
+            R ZL3 = PL2(XZ[KJ - 1], XZ[KJ], XZ[KJ + 1], AKZ);
+            PD1Z[k] = interp(APD1Z, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+            PD2Z[k] = interp(APD2Z, KI, KJ, XL1, XL2, XL3, ZL1, ZL2, ZL3);
+          } else {
+            R EPZ = std::exp(AKZ);
+            if (k == 1) {
+              R AKP4 = AKR - PI4;
+              R SQ = std::sqrt(DPI / AKR);
+              R CSK = std::cos(AKP4), SIK = std::sin(AKP4);
+              PSK = PI * SQ * SIK;
+              SCK = SQ * CSK;
+            }
+            PD1Z[k] = PSURR * AKZ - PSK * EPZ;
+            PD2Z[k] = EPZ * SCK;
+          }
+        } else {
+          PD1Z[k] = PSURR * AKZ;
+          PD2Z[k] = 0.;
+        }
+      }
+      R QTQQ = PD1Z[1] + PD1Z[2] + PD1Z[3] + PD1Z[4];
+      FS1[JJ] = COF1 * (QTQQ - PSR[1] - PSR[2] - PSR[3] - PSR[4]);
+      R STSS = PD2Z[1] + PD2Z[2] + PD2Z[3] + PD2Z[4];
+      FS2[JJ] = COF2 * STSS;
+      R ACT = -0.5 * AIRE[J] / QPI;
+      for (int KE = 1; KE <= NEXP1; ++KE) {
+        R AQT = ACT * AR[KE];
+        R ZPG[5] = {0., ZPO - 2. * H + H * AMBDA[KE] - ZG[J], -ZPO - H * AMBDA[KE] - ZG[J],
+                    -ZPO - 4. * H + H * AMBDA[KE] - ZG[J], ZPO + 2. * H - H * AMBDA[KE] - ZG[J]};
+        R FTS[5];
+        for (int k = 1; k <= 4; ++k) {
+          if (k == 2 && KE == NEXP1) {
+            R XL[6], YL[6], ZL[6];
+            int KK[6] = {0, M1[J], M2[J], M3[J], M4[J], M1[J]};
+            for (int L = 1; L <= 5; ++L) { XL[L] = X[KK[L]]; YL[L] = Y[KK[L]]; ZL[L] = Z[KK[L]]; }
+            FTS[2] = VVG(XL, YL, ZL, JJ, XN[J], YN[J], ZN[J], AIRE[J], TDIS[J], XG[J], YG[J], ZG[J], XPO, YPO, -ZPO);
+            continue;
+          }
+          R RRk = sq(RRR) + sq(ZPG[k]);
+          R ROk = std::sqrt(RRk);
+          FTS[k] = (ROk > EPS) ? AQT / ROk : 0.;
+        }
+        FS1[JJ] = FS1[JJ] + FTS[1] + FTS[2] + FTS[3] + FTS[4];
+      }
+    }
+    if (NSYMY == 1) {
+      SM1 = FSM + FS1[1] - FS1[2];
+      SP1 = FSP + FS1[1] + FS1[2];
+      SM2 = FS2[1] - FS2[2];
+      SP2 = FS2[1] + FS2[2];
+    } else {
+      SP1 = FSP + FS1[1];
+      SM1 = SP1;
+      SP2 = FS2[1];
+      SM2 = SP2;
+    }
+  }
+
+  // COMPUTE_POTENTIAL_DOMAIN.f90:24-82, potential at (XC, YC, ZC) from ZIGB/ZIGS
+  C potential_domain(R XC, R YC, R ZC, R AM0, R AMH, int NEXP) {
+    R POT1 = 0., POT2 = 0.;
+    for (int J = 1; J <= IMX; ++J) {
+      SP1 = 0.; SP2 = 0.; SM1 = 0.; SM2 = 0.;
+      if ((Depth == 0.) || (AMH >= 20)) {
+        VVV(1, J, XC, YC, ZC);
+        VNV(J, XC, YC, ZC);
+      } else {
+        VVV(2, J, XC, YC, ZC);
+        VNVF(AM0, AMH, NEXP, J, XC, YC, ZC);
+      }
+      R S1B = ZIGB[J].real(), S1S = ZIGS[J].real(), S2B = ZIGB[J].imag(), S2S = ZIGS[J].imag();
+      R Cc, D;
+      if (NSYMY == 0) {
+        Cc = S1B * SP1; D = S2B * SP2; POT1 = POT1 + Cc - D;
+        Cc = S1B * SP2; D = S2B * SP1; POT2 = POT2 + Cc + D;
+      } else {
+        Cc = S1B * (SP1 + SM1) + S1S * (SP1 - SM1);
+        D = S2B * (SP2 + SM2) + S2S * (SP2 - SM2);
+        POT1 = POT1 + (Cc - D) * 0.5;
+        Cc = S1B * (SP2 + SM2) + S1S * (SP2 - SM2);
+        D = S2B * (SP1 + SM1) + S2S * (SP1 - SM1);
+        POT2 = POT2 + (Cc + D) * 0.5;
+      }
+    }
+    return C(POT1, POT2);
+  }
+
+  // SOLVE_BEM.f90:62-84 and 104-109: the arguments SOLVE_BVP hands to
+  // COMPUTE_POTENTIAL_DOMAIN for period T (sets T, and AMBDA/AR in finite depth)
+  void fs_setup(R Period, R& AM0, R& AMH, int& NEXP) {
+    const R PI = 4. * std::atan(1.);
+    T = Period;
+    R W = 2. * PI / T;
+    R kwave = W * W / G;
+    NEXP = 0;
+    if ((Depth == 0.) || (kwave * Depth >= 20)) {
+      AMH = kwave * Depth;
+      AM0 = kwave;
+    } else {
+      AMH = X0(W * W * Depth / G);
+      AM0 = AMH / Depth;
+      for (int i = 0; i < 32; ++i) { AMBDA[i] = 0.; AR[i] = 0.; }
+      LISC(AMH * std::tanh(AMH), AMH, NEXP, AMBDA, AR);
+    }
+  }
+
+  // free-surface elevation ETA = i W / G PHI at (x, y, 0) (SOLVE_BEM.f90:104-109)
+  C free_surface(R Period, R XC, R YC, R AM0, R AMH, int NEXP) {
+    const R PI = 4. * std::atan(1.);
+    const C II(0., 1.);
+    R W = 2. * PI / Period;
+    C PHI = potential_domain(XC, YC, 0., AM0, AMH, NEXP);
+    return II * W / G * PHI;
+  }
+
   // matrices of one omega (no solve): D+, D-, S+, S- column-major NFA x NFA
   void assemble(R omega, C* dp, C* dm, C* sp, C* sm, int* depth_mode, int* nexp_out) {
     const R PI = 4. * std::atan(1.);
@@ -1987,7 +2256,11 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
   auto vt = bc.read(npb);
   for (int j = 0; j < npb; ++j) stype[j] = std::stod(vt[j]);
   bc.read(npb);
-  bc.read(npb);
+  std::vector<int> sfs(npb);
+  {
+    auto v = bc.read(npb);
+    for (int j = 0; j < npb; ++j) sfs[j] = std::stoi(v[j]);
+  }
   std::vector<int> sk(npb);
   auto vk = bc.read(npb);
   for (int j = 0; j < npb; ++j) sk[j] = std::stoi(vk[j]);
@@ -2015,7 +2288,22 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
     int nth = std::stoi(kr.read(1)[0]);
     for (int j = 0; j < nth; ++j) theta.push_back(std::stod(kr.read(1)[0]));
   }
-  { ListReader fr(dir + "/mesh/Freesurface.dat"); fr.read(2); }
+  std::vector<double> fsx;
+  std::vector<int> fsp;
+  int fs_np = 0, fs_ne = 0;
+  {
+    ListReader fr(dir + "/mesh/Freesurface.dat");
+    auto v = fr.read(2);
+    fs_np = std::stoi(v[0]);
+    fs_ne = std::stoi(v[1]);
+    for (int j = 0; j < fs_np; ++j) {
+      auto p = fr.read(2);
+      fsx.push_back(std::stod(p[0]));
+      fsx.push_back(std::stod(p[1]));
+    }
+    for (int j = 0; j < fs_ne; ++j)
+      for (auto& t : fr.read(4)) fsp.push_back(std::stoi(t));
+  }
   Oracle o;
   o.cache_s = cache_s;
   o.initialize(np, nfa, isym, xyz.data(), m.data(), rho, g, depth);
@@ -2023,6 +2311,32 @@ int run_case(const std::string& root, bool cache_s, double* seconds) {
   std::vector<C> force((size_t)nint * npb, C(0, 0)), pressure(nc);
   for (int j = 0; j < npb; ++j) {
     o.solve_bvp(2. * PI / omega[j], &nvel[(size_t)nc * j], pressure.data(), nullptr);
+    if (sfs[j] == 1 && fs_np > 0) {
+      // SOLVE_BEM.f90:104-109 and OUTPUT.f90:42-64
+      double am0, amh;
+      int ne;
+      o.fs_setup(2. * PI / omega[j], am0, amh, ne);
+      char name[40];
+      std::snprintf(name, sizeof name, "freesurface.%5d.dat", j + 1);
+      std::ofstream ff(dir + "/results/" + name);
+      ff << " VARIABLES=\"X\" \"Y\" \"abs(eta) (m)\" \"angle(phi) (rad)\" \"PRE1\" \"PRE2\"\n";
+      char line[160];
+      std::snprintf(line, sizeof line, "ZONE N=%7d ,E = %7d ,F=FEPOINT,ET=QUADRILATERAL\n", fs_np, fs_ne);
+      ff << line;
+      for (int q = 0; q < fs_np; ++q) {
+        C eta = o.free_surface(2. * PI / omega[j], fsx[2 * q], fsx[2 * q + 1], am0, amh, ne);
+        std::snprintf(line, sizeof line, " %.17E %.17E %.17E %.17E %.17E %.17E\n", fsx[2 * q], fsx[2 * q + 1],
+                      std::abs(eta), std::atan2(eta.imag(), eta.real()), eta.real(), eta.imag());
+        ff << line;
+      }
+      // integers through snprintf: an ostream integer insert compiled into this
+      // library can meet another libstdc++'s locale facets when the host
+      // process (numpy's wheels) loaded one first
+      for (int q = 0; q < fs_ne; ++q) {
+        std::snprintf(line, sizeof line, " %d %d %d %d\n", fsp[4 * q], fsp[4 * q + 1], fsp[4 * q + 2], fsp[4 * q + 3]);
+        ff << line;
+      }
+    }
     if (sk[j] == 1 && !theta.empty()) {
       // SOLVE_BEM.f90:98-102 and OUTPUT.f90:25-40 (YEFF = 0 on symmetric meshes,
       // INITIALIZATION.f90:60); file name with the I5 problem number
@@ -2158,6 +2472,26 @@ double nemoh_oracle_sample_solve(void* h, double omega, int nprob, double budget
 }
 
 int nemoh_oracle_get_nq(void* h) { return static_cast<Oracle*>(h)->NQ; }
+
+// free-surface elevation at the points (x, y, 0) (xy: 2 x npts) for the given
+// source strengths (nfa x nprob each): eta = npts x nprob complex
+int nemoh_oracle_free_surface(void* h, double period, int npts, const double* xy, int nprob, const double* zigb,
+                              const double* zigs, double* eta) {
+  ORACLE_TRY({
+    Oracle* o = static_cast<Oracle*>(h);
+    double am0, amh;
+    int ne;
+    o->fs_setup(period, am0, amh, ne);
+    for (int p = 0; p < nprob; ++p) {
+      for (int i = 1; i <= o->NFA; ++i) {
+        o->ZIGB[i] = ((const C*)zigb)[(size_t)p * o->NFA + i - 1];
+        o->ZIGS[i] = (o->NSYMY == 1 && zigs) ? ((const C*)zigs)[(size_t)p * o->NFA + i - 1] : C(0., 0.);
+      }
+      for (int q = 0; q < npts; ++q)
+        ((C*)eta)[q + (size_t)npts * p] = o->free_surface(period, xy[2 * q], xy[2 * q + 1], am0, amh, ne);
+    }
+  })
+}
 
 // COMPUTE_KOCHIN for the given source strengths (nfa x nprob complex each;
 // zigs ignored without symmetry): hkochin = ntheta x nprob complex

@@ -53,6 +53,8 @@ def lib():
             L.nemoh_oracle_gaussz_inverse.argtypes = [ctypes.c_int, _d, _d]
             L.nemoh_oracle_kochin.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                               ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
+            L.nemoh_oracle_free_surface.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _d,
+                                                    ctypes.c_int, _d, _d, _d]
             _lib = L
     return _lib
 
@@ -132,6 +134,19 @@ class Oracle:
         _check(lib().nemoh_oracle_kochin(self.h, period, xeff, yeff, len(theta), theta.ctypes.data_as(_d),
                                          zigb.shape[1], zigb.ctypes.data_as(_d), zigs.ctypes.data_as(_d),
                                          out.ctypes.data_as(_d)))
+        return out
+
+    def free_surface(self, period, xy, zigb, zigs=None):
+        """ETA at the points (x, y, 0) of xy (npts, 2) for source strengths (n,)
+        or (n, nprob): (npts, nprob) complex."""
+        xy = np.ascontiguousarray(np.asarray(xy, dtype=np.float64).reshape(-1, 2))
+        zigb = np.asfortranarray(np.asarray(zigb, dtype=np.complex128).reshape(self.n, -1))
+        zigs = (np.asfortranarray(np.asarray(zigs, dtype=np.complex128).reshape(self.n, -1))
+                if zigs is not None else np.zeros_like(zigb))
+        out = np.zeros((xy.shape[0], zigb.shape[1]), dtype=np.complex128, order="F")
+        _check(lib().nemoh_oracle_free_surface(self.h, period, xy.shape[0], xy.ctypes.data_as(_d), zigb.shape[1],
+                                               zigb.ctypes.data_as(_d), zigs.ctypes.data_as(_d),
+                                               out.ctypes.data_as(_d)))
         return out
 
     @property

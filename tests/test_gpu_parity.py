@@ -262,3 +262,54 @@ def test_device_body_conditions_match_preprocessor(solver, which):
     for got, ref in ((nvel, nv0), (nds, nds0), (fk, fk0)):
         assert got.shape == ref.shape
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), which
+
+
+def _fs_points(case):
+    """Points (x, y) on z = 0 around the body: a polar grid from just outside
+    the waterline (tabulated wave term) to 30 body radii (asymptotic form)."""
+    nodes = case.mesh.nodes
+    r0 = np.hypot(nodes[:, 0], nodes[:, 1]).max()
+    rr = r0 * np.array([1.15, 1.6, 3.0, 8.0, 30.0])
+    th = np.linspace(0.0, 2.0 * np.pi, 13)[:-1] + 0.1
+    R, TH = np.meshgrid(rr, th)
+    return np.stack([(R * np.cos(TH)).ravel(), (R * np.sin(TH)).ravel()], axis=1)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_free_surface_matches_oracle(solver, case):
+    """Free-surface elevation (COMPUTE_POTENTIAL_DOMAIN on z = 0, ETA = i W/G PHI)
+    on the GPU vs the oracle for the same source strengths: every point within
+    1e-9 of the problem's largest |ETA| (the panel sums cancel like Kochin's)."""
+    _mesh(solver, case)
+    o = G.oracle_for(case)
+    nv = C.body_conditions(case)
+    npb = len(case.betas_deg) + len(case.rad)
+    xy = _fs_points(case)
+    for w_idx in (0, len(case.omegas) - 1):
+        T = 2 * np.pi / case.omegas[w_idx]
+        cols = range(w_idx * npb, (w_idx + 1) * npb)
+        res = [solver.solve_potential(T, nv[:, j]) for j in cols]
+        zigb = np.stack([r["zigb"] for r in res], axis=1)
+        zigs = np.stack([r["zigs"] for r in res], axis=1)
+        eta = solver.free_surface(T, xy, zigb, zigs)
+        eo = o.free_surface(T, xy, zigb, zigs if case.mesh.isym else None)
+        scale = np.abs(eo).max(axis=0)
+        assert np.all(scale > 0)
+        err = (np.abs(eta - eo) / scale).max()
+        assert err < 1e-9, (case.name, w_idx, err)
+
+
+def test_free_surface_more_problems_than_one_launch(solver):
+    """More than 16 problems at once are taken 16 at a time: same values as
+    one problem per call."""
+    case = CASES[0]
+    _mesh(solver, case)
+    nv = C.body_conditions(case)
+    T = 2 * np.pi / case.omegas[1]
+    z = solver.solve_potential(T, nv[:, 0])["zigb"]
+    rng = np.random.default_rng(3)
+    zigb = z[:, None] * (rng.standard_normal(19) + 1j * rng.standard_normal(19))[None, :]
+    xy = _fs_points(case)[:20]
+    eta = solver.free_surface(T, xy, zigb)
+    one = np.concatenate([solver.free_surface(T, xy, zigb[:, p]) for p in range(19)], axis=1)
+    assert np.abs(eta - one).max() <= 1e-13 * np.abs(one).max()

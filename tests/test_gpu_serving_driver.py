@@ -74,3 +74,38 @@ def test_dropin_driver_kochin_files_match_oracle(tmp_path):
     assert np.array_equal(th_r, th_g)
     err = (np.abs(Hg - Hr) / np.abs(Hr).max(axis=0)).max()
     assert err < 1e-9, err
+
+
+def _fs_files(d, nprob):
+    out = []
+    for p in range(nprob):
+        with open(os.path.join(d, "case", "results", "freesurface.%5d.dat" % (p + 1))) as f:
+            head = [f.readline(), f.readline()]
+        a = np.loadtxt(os.path.join(d, "case", "results", "freesurface.%5d.dat" % (p + 1)), skiprows=2,
+                       max_rows=int(head[1].split("=")[1].split()[0]), ndmin=2)
+        out.append(a[:, 4] + 1j * a[:, 5])
+    return head, a[:, :2], np.stack(out, axis=1)
+
+
+def test_dropin_driver_freesurface_files_match_oracle(tmp_path):
+    """freesurface.<I5>.dat of every problem (deep-water cylinder, the
+    pre-processor's 9 x 7 grid over 60 m x 40 m) against the oracle's reference
+    run: same header, points and quadrangles, ETA within 1e-9 of the problem's
+    largest |ETA|."""
+    import dataclasses
+    import oracle_lib as O
+    B.build()
+    case = dataclasses.replace(G.small_cases()[0], fs_grid=(9, 7, 60.0, 40.0))
+    C.write_case(case, str(tmp_path / "ref"))
+    O.run_case(str(tmp_path / "ref"))
+    C.write_case(case, str(tmp_path / "gpu"))
+    exe = os.path.join(ROOT, "nemoh_b200", "_build", "nemoh_solver_b200")
+    subprocess.run([exe, str(tmp_path / "gpu")], check=True)
+    hr, xr, Er = _fs_files(str(tmp_path / "ref"), case.nproblems)
+    hg, xg, Eg = _fs_files(str(tmp_path / "gpu"), case.nproblems)
+    assert hr == hg and np.array_equal(xr, xg) and xr.shape == (63, 2)
+    qr = open(os.path.join(str(tmp_path / "ref"), "case", "results", "freesurface.%5d.dat" % 1)).read().split("\n")
+    qg = open(os.path.join(str(tmp_path / "gpu"), "case", "results", "freesurface.%5d.dat" % 1)).read().split("\n")
+    assert qr[-50:] == qg[-50:]
+    err = (np.abs(Eg - Er) / np.abs(Er).max(axis=0)).max()
+    assert err < 1e-9, err
