@@ -71,6 +71,15 @@ MODULE NEMOH_B200_IFACE
             REAL(C_DOUBLE), DIMENSION(*) :: theta
             COMPLEX(C_DOUBLE_COMPLEX), DIMENSION(*) :: zigb, zigs, hkochin
         END FUNCTION
+        INTEGER(C_INT) FUNCTION nemoh_b200_free_surface(ctx, period, npts, xy, nprob, zigb, zigs, eta) &
+                BIND(C, NAME='nemoh_b200_free_surface')
+            IMPORT :: C_PTR, C_INT, C_DOUBLE, C_DOUBLE_COMPLEX
+            TYPE(C_PTR), VALUE :: ctx
+            REAL(C_DOUBLE), VALUE :: period
+            INTEGER(C_INT), VALUE :: npts, nprob
+            REAL(C_DOUBLE), DIMENSION(*) :: xy
+            COMPLEX(C_DOUBLE_COMPLEX), DIMENSION(*) :: zigb, zigs, eta
+        END FUNCTION
     END INTERFACE
 
     TYPE(C_PTR), SAVE :: B200_CTX = C_NULL_PTR
@@ -167,6 +176,35 @@ CONTAINS
                         1_C_INT, TH, 1_C_INT, ZB, ZS, H), 'kochin')
         HKochin = H(1)
         DEALLOCATE(ZB, ZS)
+    END SUBROUTINE
+
+    ! Drop-in for the free-surface loop of SOLVE_BVP (SOLVE_BEM.f90:104-109):
+    ! ETA(j) = II*W/G*PHI(j) at the points MeshFS%X(1:2, j), from the source
+    ! strengths ZIGB, ZIGS of the last SOLVE_POTENTIAL_B200 call.
+    SUBROUTINE COMPUTE_FS_B200(NPOINTS, XFS, ETA)
+        USE COM_VAR
+        INTEGER :: NPOINTS
+        REAL, DIMENSION(3, *) :: XFS
+        COMPLEX, DIMENSION(*) :: ETA
+        REAL(C_DOUBLE), ALLOCATABLE :: XY(:)
+        COMPLEX(C_DOUBLE_COMPLEX), ALLOCATABLE :: ZB(:), ZS(:), E(:)
+        INTEGER :: I
+        IF (NPOINTS .LE. 0) RETURN
+        ALLOCATE(XY(2 * NPOINTS), E(NPOINTS), ZB(NFA), ZS(NFA))
+        DO I = 1, NPOINTS
+            XY(2 * I - 1) = REAL(XFS(1, I), C_DOUBLE)
+            XY(2 * I) = REAL(XFS(2, I), C_DOUBLE)
+        END DO
+        DO I = 1, NFA
+            ZB(I) = CMPLX(ZIGB(I), KIND=C_DOUBLE_COMPLEX)
+            ZS(I) = CMPLX(ZIGS(I), KIND=C_DOUBLE_COMPLEX)
+        END DO
+        CALL B200_CHECK(nemoh_b200_free_surface(B200_CTX, REAL(T, C_DOUBLE), INT(NPOINTS, C_INT), XY, 1_C_INT, &
+                        ZB, ZS, E), 'free_surface')
+        DO I = 1, NPOINTS
+            ETA(I) = CMPLX(E(I))
+        END DO
+        DEALLOCATE(XY, E, ZB, ZS)
     END SUBROUTINE
 
     SUBROUTINE B200_FINALIZE
