@@ -9,6 +9,14 @@ period). This script reads them from a Nemoh source tree and writes, per case,
 the mesh, environment, DOFs and the reference coefficients at a subset of
 frequencies, so that the tests can run without the source tree.
 
+A fourth case, Verification/Postprocessing (the rotated cube of 2Bodies alone in
+10 m of water, diffraction at omega = 0.8 rad/s, heading 0), ships the
+free-surface elevation on the pre-processor's 50 x 50 grid over 400 m x 400 m
+(Results/Aquaplus/FS.tec, zone "SUR LI": x, y, z, Re, Im, modulus) and the Kochin
+function every 5 degrees (Results/Aquaplus/ZKochin.tec: theta, modulus, phase in
+degrees). Every fifth grid point, the 24 points nearest the body, and every
+direction are kept.
+
 Usage: python tests/golden/make_verification_fixtures.py <nemoh-tree>
 """
 import json
@@ -123,6 +131,31 @@ def main(tree):
         with open(out, "w") as f:
             json.dump(fx, f)
         print("wrote", out, os.path.getsize(out), "bytes")
+    postprocessing(tree, here)
+
+
+def postprocessing(tree, here):
+    d = os.path.join(tree, "Verification", "Postprocessing")
+    fx = parse_cal(d)
+    L = [l.split("!")[0].split() for l in open(os.path.join(d, "Nemoh.cal")).read().split("\n")]
+    i = [n for n, l in enumerate(L) if l and l[0] == "---" and "Load" in " ".join(l)][0]
+    nw, wmin, wmax = int(L[i + 1][0]), float(L[i + 1][1]), float(L[i + 1][2])
+    fx["omegas"] = list(np.linspace(wmin, wmax, nw)) if nw > 1 else [wmin]
+    fx["fs_grid"] = [int(L[i + 7][0]), int(L[i + 7][1]), float(L[i + 7][2]), float(L[i + 7][3])]
+    lines = open(os.path.join(d, "Results", "Aquaplus", "FS.tec")).read().split("\n")
+    z = [n for n, l in enumerate(lines) if "SUR LI" in l][0]
+    npts = int(re.search(r"I=\s*(\d+)", lines[z]).group(1))
+    A = np.array([[float(v) for v in l.split()] for l in lines[z + 1:z + 1 + npts]])
+    r = np.hypot(A[:, 0], A[:, 1])
+    keep = sorted(set(range(0, npts, 5)) | set(np.argsort(r)[:24].tolist()))
+    fx["freesurface"] = {"index": keep, "x": A[keep, 0].tolist(), "y": A[keep, 1].tolist(),
+                         "re": A[keep, 3].tolist(), "im": A[keep, 4].tolist()}
+    K = np.loadtxt(os.path.join(d, "Results", "Aquaplus", "ZKochin.tec"), skiprows=1)
+    fx["kochin"] = {"theta_deg": K[:, 0].tolist(), "abs": K[:, 1].tolist(), "arg_deg": K[:, 2].tolist()}
+    out = os.path.join(here, "verification_Postprocessing.json")
+    with open(out, "w") as f:
+        json.dump(fx, f)
+    print("wrote", out, os.path.getsize(out), "bytes")
 
 
 if __name__ == "__main__":

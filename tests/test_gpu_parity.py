@@ -313,3 +313,26 @@ def test_free_surface_more_problems_than_one_launch(solver):
     eta = solver.free_surface(T, xy, zigb)
     one = np.concatenate([solver.free_surface(T, xy, zigb[:, p]) for p in range(19)], axis=1)
     assert np.abs(eta - one).max() <= 1e-13 * np.abs(one).max()
+
+
+def test_free_surface_and_kochin_match_stored_reference_values(solver):
+    """The GPU path on the reference's Verification/Postprocessing case against
+    its stored single-precision elevation (-i ETA) and Kochin function (i H):
+    the tolerances of the oracle's own pin (2e-5 and 1e-4 of the largest stored
+    modulus; 0.01 degree)."""
+    fx = V.load("Postprocessing")
+    case = V.case_from_fixture(fx)
+    _mesh(solver, case)
+    nv = C.body_conditions(case)
+    T = 2 * np.pi / case.omegas[0]
+    r = solver.solve_potential(T, nv[:, 0])
+    fs = fx["freesurface"]
+    pts, _ = C.freesurface_grid(*fx["fs_grid"])
+    stored = np.array(fs["re"]) + 1j * np.array(fs["im"])
+    eta = solver.free_surface(T, pts[fs["index"]], r["zigb"], r["zigs"])[:, 0]
+    assert np.abs(-1j * eta - stored).max() < 2e-5 * np.abs(stored).max()
+    k = fx["kochin"]
+    Z = 1j * solver.kochin(T, np.radians(k["theta_deg"]), r["zigb"], r["zigs"])[:, 0]
+    assert np.abs(np.abs(Z) - np.array(k["abs"])).max() < 1e-4 * np.max(k["abs"])
+    dphi = (np.degrees(np.angle(Z)) - np.array(k["arg_deg"]) + 180.0) % 360.0 - 180.0
+    assert np.abs(dphi).max() < 1e-2
