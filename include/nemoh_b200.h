@@ -104,6 +104,15 @@ int nemoh_b200_kochin(nemoh_ctx* ctx, double period, double xeff, double yeff, i
 int nemoh_b200_free_surface(nemoh_ctx* ctx, double period, int npts, const double* xy, int nprob,
                             const double* zigb, const double* zigs, double* eta);
 
+/* Radiation impulse response functions of the post-processor (Compute_IRF,
+ * postProcessor/IRF.f90:100-127): from damping and added mass (nw x nrad x
+ * nint, w fastest; w nonzero) the kernels K at t_i = i dt, i < ntime (ntime x
+ * nrad x nint, time fastest) by the trapezoid rule over w, and the
+ * infinite-frequency added mass ainf (nrad x nint) estimated from K. Needs a
+ * context (for its device and stream), not a mesh. */
+int nemoh_b200_irf(nemoh_ctx* ctx, int nw, const double* w, int nrad, int nint, const double* damping,
+                   const double* added_mass, int ntime, double dt, double* K, double* ainf);
+
 /* Pre-processor body conditions on the device for the current mesh
  * (preProcessor/Main.f90:201-243 with Mesh.f90:197-222, BodyConditions.f90:27-137,
  * Environment.f90:45-100, Integration.f90:27-86): for nomega frequencies, nbeta

@@ -78,6 +78,8 @@ def load_library():
     L.nemoh_b200_kochin.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
                                     ctypes.c_int, _d, _d, _d]
     L.nemoh_b200_free_surface.argtypes = [_vp, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
+    L.nemoh_b200_irf.argtypes = [_vp, ctypes.c_int, _d, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int,
+                                 ctypes.c_double, _d, _d]
     L.nemoh_b200_launch_count.restype = ctypes.c_longlong
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
     L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
@@ -267,6 +269,24 @@ class Solver:
                                                            zigb.ctypes.data_as(_d), zigs.ctypes.data_as(_d),
                                                            out.ctypes.data_as(_d)))
         return out
+
+    # -- post-processor: Compute_IRF -------------------------------------------
+    def irf(self, w, damping, added_mass, ntime, dt):
+        """Impulse response functions K (ntime, nrad, nint) at t = i dt and the
+        infinite-frequency added mass (nrad, nint) from damping and added mass
+        (nw, nrad, nint) at the frequencies w (postProcessor/IRF.f90:100-127)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        B = np.asfortranarray(damping, dtype=np.float64)
+        A = np.asfortranarray(added_mass, dtype=np.float64)
+        nw, nrad, nint = B.shape
+        if A.shape != B.shape or len(w) != nw:
+            raise ValueError("damping, added mass and w must agree in shape")
+        K = np.zeros((int(ntime), nrad, nint), order="F")
+        ainf = np.zeros((nrad, nint), order="F")
+        self._check(load_library().nemoh_b200_irf(self._h, nw, _p(w), nrad, nint, B.ctypes.data_as(_d),
+                                                  A.ctypes.data_as(_d), int(ntime), float(dt), K.ctypes.data_as(_d),
+                                                  ainf.ctypes.data_as(_d)))
+        return K, ainf
 
     # -- diagnostics -----------------------------------------------------------
     def assemble(self, omega):

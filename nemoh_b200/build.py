@@ -1,4 +1,4 @@
-"""Build libnemoh_b200.so (sm_100a) and the drop-in Solver driver in-tree.
+"""Build libnemoh_b200.so (sm_100a) and the drop-in Solver and post-processor executables in-tree.
 
     python -m nemoh_b200.build        # or nemoh_b200.build.build()
 
@@ -15,6 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT, "libnemoh_b200.so")
 DRIVER = os.path.join(OUT, "nemoh_solver_b200")
+POSTPROC = os.path.join(OUT, "nemoh_postproc_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -29,7 +30,7 @@ def _sources(names):
 
 LIB_SRC = ["api.cu", "fd_setup.cpp"]
 DEPS = ["api.cu", "fd_setup.cpp", "fd_setup.h", "common.cuh", "green.cuh", "assembly.cuh", "linalg.cuh",
-        "mixed.cuh", "tc_gemm.cuh", "kochin.cuh", "preproc.cuh", "freesurface.cuh", "driver.cpp"]
+        "mixed.cuh", "tc_gemm.cuh", "kochin.cuh", "preproc.cuh", "freesurface.cuh", "postproc.cuh", "case_io.h", "driver.cpp", "postproc.cpp"]
 
 
 def _stale(target, deps):
@@ -49,15 +50,15 @@ def build(force=False, verbose=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-    drv_src = os.path.join(CSRC, "driver.cpp")
-    if os.path.exists(drv_src) and (force or _stale(DRIVER, ["driver.cpp"]) or
-                                    os.path.getmtime(DRIVER) < os.path.getmtime(LIB)):
-        cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-o", DRIVER, drv_src,
-               "-I" + os.path.join(os.path.dirname(HERE), "include"),
-               "-L" + OUT, "-lnemoh_b200", "-Wl,-rpath,$ORIGIN"]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+    for exe, src in ((DRIVER, "driver.cpp"), (POSTPROC, "postproc.cpp")):
+        path = os.path.join(CSRC, src)
+        if force or _stale(exe, [src, "case_io.h"]) or os.path.getmtime(exe) < os.path.getmtime(LIB):
+            cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-Wall", "-o", exe, path,
+                   "-I" + os.path.join(os.path.dirname(HERE), "include"),
+                   "-L" + OUT, "-lnemoh_b200", "-Wl,-rpath,$ORIGIN"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
     return LIB
 
 

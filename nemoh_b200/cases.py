@@ -104,6 +104,7 @@ class Case:
     name: str = "case"
     kochin_theta: tuple = ()   # directions (rad) of mesh/Kochin.dat; Kochin switch set for every problem if any
     fs_grid: tuple = ()        # (Nx, Ny, Lx, Ly) of Nemoh.cal's free-surface line; free-surface switch set if any
+    irf: tuple = ()            # (dt, duration) of Nemoh.cal's IRF line; IRF switch set if given
 
     @property
     def nproblems(self) -> int:
@@ -485,8 +486,9 @@ def write_case(case: Case, root: str, case_dir: str = "case") -> str:
         f.write("%d %s %s\n" % (len(bt), _r(bt[0]) if len(bt) else "0.", _r(bt[-1]) if len(bt) else "0."))
         kt = np.degrees(np.asarray(case.kochin_theta, dtype=float))
         fsg = tuple(case.fs_grid) if len(case.fs_grid) else (0, 0, 100.0, 100.0)
-        f.write("--- Post processing ---\n0 0.1 10.\n0\n%d %s %s\n%d %d %s %s\n"
-                % (len(kt), _r(kt[0]) if len(kt) else "0.", _r(kt[-1]) if len(kt) else "180.",
+        irf = ("1 %s %s" % (_r(case.irf[0]), _r(case.irf[1]))) if len(case.irf) else "0 0.1 10."
+        f.write("--- Post processing ---\n%s\n0\n%d %s %s\n%d %d %s %s\n"
+                % (irf, len(kt), _r(kt[0]) if len(kt) else "0.", _r(kt[-1]) if len(kt) else "180.",
                    int(fsg[0]), int(fsg[1]), _r(fsg[2]), _r(fsg[3])))
     with open(os.path.join(d, "input.txt"), "w") as f:
         f.write("--- Calculation parameters ---\n0\n")
@@ -549,16 +551,40 @@ def write_case(case: Case, root: str, case_dir: str = "case") -> str:
                     vals += [_r(abs(fk[i, c, k])), _r(math.atan2(fk[i, c, k].imag, fk[i, c, k].real))]
                 vals += ["0.0", "0.0"] * nr
             f.write(" ".join(vals) + "\n")
-    with open(os.path.join(d, "results", "index.dat"), "w") as f:
-        f.write("%d %d %d %d %d\n" % (len(case.omegas), len(case.betas_deg), nr, len(case.force), 0))
-        f.write("--- Force ---\n")
+    # FKForce.tec, the post-processor's source of Froude-Krylov forces
+    # (preProcessor/Main.f90:266-276)
+    with open(os.path.join(d, "results", "FKForce.tec"), "w") as f:
+        f.write('VARIABLES="w (rad/s)"\n')
         for k, r in enumerate(case.force):
-            f.write("%d %d %d\n" % (k + 1, r.body, k + 1))
+            f.write('"abs(F%4d%4d)" "angle(F%4d%4d)"\n' % (r.body, k + 1, r.body, k + 1))
+        for c, b in enumerate(case.betas_deg):
+            f.write('Zone t="FKforce - beta = %7.3f",I=%6d,F=POINT\n' % (b, len(case.omegas)))
+            for i, w in enumerate(case.omegas):
+                vals = [_r(w)]
+                for k in range(len(case.force)):
+                    vals += [_r(abs(fk[i, c, k])), _r(math.atan2(fk[i, c, k].imag, fk[i, c, k].real))]
+                f.write(" ".join(vals) + "\n")
+
+    def modes(dofs):   # index of each DOF within its body (Main.f90:160-176)
+        seen = {}
+        out = []
+        for r in dofs:
+            seen[r.body] = seen.get(r.body, 0) + 1
+            out.append(seen[r.body])
+        return out
+
+    with open(os.path.join(d, "results", "index.dat"), "w") as f:
+        f.write("%d %d %d %d %d\n" % (len(case.omegas), len(case.betas_deg), nr, len(case.force),
+                                      len(case.kochin_theta)))
+        f.write("--- Force ---\n")
+        for k, (r, m) in enumerate(zip(case.force, modes(case.force))):
+            f.write("%d %d %d\n" % (k + 1, r.body, m))
         f.write("--- Motion ---\n")
-        for k, r in enumerate(case.rad):
-            f.write("%d %d %d\n" % (k + 1, r.body, k + 1))
+        for k, (r, m) in enumerate(zip(case.rad, modes(case.rad))):
+            f.write("%d %d %d\n" % (k + 1, r.body, m))
         f.write(" ".join(_r(b * math.pi / 180.0) for b in case.betas_deg) + "\n")
-        f.write(" ".join(_r(w) for w in case.omegas) + "\n\n")
+        f.write(" ".join(_r(w) for w in case.omegas) + "\n")
+        f.write(" ".join(_r(t) for t in case.kochin_theta) + "\n")
     return d
 
 

@@ -20,6 +20,7 @@
 #include "kochin.cuh"
 #include "preproc.cuh"
 #include "freesurface.cuh"
+#include "postproc.cuh"
 #include "linalg.cuh"
 #include "mixed.cuh"
 
@@ -92,7 +93,7 @@ struct nemoh_ctx {
   double ro_eps2 = 0;   // largest x with sqrt(x) <= 1e-4
   DevBuf d_xyz, d_m, d_rec, d_rows;
   // per-call workspace
-  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin, d_pre, d_fs;
+  DevBuf d_D, d_S, d_X, d_Y, d_diag, d_inv, d_oms, d_slots, d_nvel, d_nds, d_force, d_kochin, d_pre, d_fs, d_irf;
   HostBuf h_oms, h_slots;
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
@@ -821,6 +822,45 @@ int nemoh_b200_free_surface(nemoh_ctx* c, double period, int npts, const double*
         eta[2 * ((size_t)npts * p0 + q) + 1] = e.imag();
       }
     }
+  });
+}
+
+int nemoh_b200_irf(nemoh_ctx* c, int nw, const double* w, int nrad, int nint, const double* damping,
+                   const double* added_mass, int ntime, double dt, double* K, double* ainf) {
+  if (!c || nw < 1 || nrad < 0 || nint < 0 || ntime < 0 || !(dt > 0) || !w || !K || !ainf ||
+      (nrad * nint > 0 && (!damping || !added_mass)))
+    return NEMOH_B200_EINVAL;
+  const int npair = nrad * nint;
+  if (npair == 0) return NEMOH_B200_OK;
+  for (int l = 0; l < nw; ++l)
+    if (!(w[l] != 0.)) return NEMOH_B200_EINVAL;   // CM(l)/w(l)
+  return guarded(c, [&] {
+    const size_t nc = (size_t)nw * npair, nk = (size_t)std::max(ntime, 1) * npair;
+    CK(c->d_irf.ensure((nw + 3 * nc + nk + npair) * sizeof(double)));
+    double* dw = c->d_irf.as<double>();
+    double* dB = dw + nw;
+    double* dA = dB + nc;
+    double* dcm = dA + nc;
+    double* dK = dcm + nc;
+    double* dai = dK + nk;
+    cudaStream_t st = c->stream;
+    CK(cudaMemcpyAsync(dw, w, nw * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dB, damping, nc * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dA, added_mass, nc * sizeof(double), cudaMemcpyHostToDevice, st));
+    const unsigned chunks = (npair + IRF_CH - 1) / IRF_CH;
+    if (ntime > 0) {
+      irf_kernel<<<dim3((ntime + IRF_THREADS - 1) / IRF_THREADS, chunks), IRF_THREADS, 0, st>>>(nw, dw, npair, dB,
+                                                                                                 ntime, dt, dK);
+      LAUNCHED(c);
+    }
+    irf_added_mass_kernel<<<dim3((nw + IRF_THREADS - 1) / IRF_THREADS, chunks), IRF_THREADS, 0, st>>>(
+        nw, dw, npair, dA, ntime, dt, dK, dcm);
+    LAUNCHED(c);
+    irf_average_kernel<<<(npair + 127) / 128, 128, 0, st>>>(nw, npair, dcm, dai);
+    LAUNCHED(c);
+    if (ntime > 0) CK(cudaMemcpyAsync(K, dK, (size_t)ntime * npair * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ainf, dai, npair * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
   });
 }
 

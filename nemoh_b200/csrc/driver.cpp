@@ -30,47 +30,13 @@
 #include <string>
 #include <vector>
 
+#include "case_io.h"
 #include "nemoh_b200.h"
 
 namespace {
 
-struct IoError : std::runtime_error {
-  using std::runtime_error::runtime_error;
-};
-
-// Fortran list-directed READ: every READ starts a new record; values may span lines
-class Records {
- public:
-  explicit Records(const std::string& path) {
-    std::ifstream f(path);
-    if (!f) throw IoError("cannot open " + path);
-    std::string s;
-    while (std::getline(f, s)) lines_.push_back(s);
-  }
-  void skip() { ++pos_; }
-  std::vector<std::string> read(size_t n) {
-    std::vector<std::string> v;
-    while (v.size() < n) {
-      if (pos_ >= lines_.size()) throw IoError("unexpected end of file");
-      std::string s = lines_[pos_++];
-      const size_t bang = s.find('!');
-      if (bang != std::string::npos) s.resize(bang);
-      for (char& ch : s)
-        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
-      std::istringstream is(s);
-      std::string t;
-      while (is >> t) v.push_back(t);
-    }
-    v.resize(n);
-    return v;
-  }
-  double real() { return std::stod(read(1)[0]); }
-  int integer() { return std::stoi(read(1)[0]); }
-
- private:
-  std::vector<std::string> lines_;
-  size_t pos_ = 0;
-};
+using nb200io::IoError;
+using nb200io::Records;
 
 void check(nemoh_ctx* ctx, int st, const char* what) {
   if (st) {

@@ -34,6 +34,7 @@
 // =============================================================================
 #include <algorithm>
 #include <cmath>
+#include <cstdarg>
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -2384,6 +2385,221 @@ extern "C" {
 
 const char* nemoh_oracle_last_error() { return g_last_error.c_str(); }
 
+
+// ---------------------------------------------------------------------------
+// Post-processor (postProcessor/Main.f90:26-101): ReadTResults and SaveTResults
+// (Common/Results.f90:104-251), Initialize_IRF / Compute_IRF / Save_IRF
+// (postProcessor/IRF.f90:72-143). Compute_RAOs (Compute_RAOs.f90:21-42) only
+// zeroes its array and Plot_WaveElevation never runs (its switch is never set,
+// postProcessor/Plot_WaveElevation.f90:121-135), so neither has an output here.
+// Reals are written with 17 significant digits in place of E14.7 / E13.6.
+
+// Compute_IRF (IRF.f90:100-127): damping/added mass (nw x nrad x nint, w
+// fastest), K (ntime x nrad x nint, time fastest), ainf (nrad x nint)
+void compute_irf(int nw, const double* w, int nrad, int nint, const double* damping, const double* added_mass,
+                 int ntime, double dt, double* K, double* ainf) {
+  const R PI = 4. * std::atan(1.0);
+  std::vector<R> time(ntime), CM(nw);
+  for (int i = 0; i < ntime; ++i) time[i] = i * dt;
+  for (int i = 0; i < ntime; ++i)
+    for (int j = 0; j < nrad; ++j)
+      for (int k = 0; k < nint; ++k) {
+        const R* B = damping + (size_t)nw * (j + (size_t)nrad * k);
+        R acc = 0.;
+        for (int l = 0; l < nw - 1; ++l)
+          acc = acc + 0.5 * (B[l] * std::cos(w[l] * time[i]) + B[l + 1] * std::cos(w[l + 1] * time[i])) *
+                          (w[l + 1] - w[l]);
+        K[i + (size_t)ntime * (j + (size_t)nrad * k)] = acc * 2. / PI;
+      }
+  for (int j = 0; j < nrad; ++j)
+    for (int k = 0; k < nint; ++k) {
+      const R* Kjk = K + (size_t)ntime * (j + (size_t)nrad * k);
+      const R* A = added_mass + (size_t)nw * (j + (size_t)nrad * k);
+      R am = 0.;
+      for (int l = 0; l < nw; ++l) {
+        CM[l] = 0.;
+        for (int i = 0; i < ntime - 1; ++i)
+          CM[l] = CM[l] + 0.5 * (Kjk[i] * std::sin(w[l] * time[i]) + Kjk[i + 1] * std::sin(w[l] * time[i + 1])) *
+                              (time[i + 1] - time[i]);
+        CM[l] = A[l] + CM[l] / w[l];
+        am = am + CM[l];
+      }
+      ainf[j + (size_t)nrad * k] = am / nw;
+    }
+}
+
+struct Text {
+  std::ofstream f;
+  explicit Text(const std::string& path) : f(path) {
+    if (!f) throw Stop(ST_IO, "cannot write " + path);
+  }
+  Text& line(const char* fmt, ...) __attribute__((format(printf, 2, 3))) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    f << buf;
+    return *this;
+  }
+};
+
+int postproc_case(const std::string& root) {
+  const std::string pre = root.empty() ? "" : root + "/";
+  ListReader idr(pre + "ID.dat");
+  const int lid = std::stoi(idr.read(1)[0]);
+  const std::string dir = pre + idr.read(1)[0].substr(0, lid);
+  const R PI = 4. * std::atan(1.0);
+  // ReadTResults (Results.f90:104-165)
+  ListReader ix(dir + "/results/index.dat");
+  auto h = ix.read(5);
+  const int Nw = std::stoi(h[0]), Nbeta = std::stoi(h[1]), Nrad = std::stoi(h[2]), Nint = std::stoi(h[3]),
+            Ntheta = std::stoi(h[4]);
+  ix.skip();
+  std::vector<int> fbody(Nint), fmode(Nint), rbody(Nrad), rmode(Nrad);
+  for (int k = 0; k < Nint; ++k) {
+    auto v = ix.read(3);
+    fbody[k] = std::stoi(v[1]);
+    fmode[k] = std::stoi(v[2]);
+  }
+  ix.skip();
+  for (int k = 0; k < Nrad; ++k) {
+    auto v = ix.read(3);
+    rbody[k] = std::stoi(v[1]);
+    rmode[k] = std::stoi(v[2]);
+  }
+  std::vector<R> beta(Nbeta), w(Nw);
+  {
+    auto v = ix.read(Nbeta);
+    if (Nbeta == 0) ix.skip();
+    for (int k = 0; k < Nbeta; ++k) beta[k] = std::stod(v[k]);
+    auto u = ix.read(Nw);
+    for (int k = 0; k < Nw; ++k) w[k] = std::stod(u[k]);
+  }
+  (void)Ntheta;
+  // arrays (w fastest): diffraction/FK (Nw, Nbeta, Nint), A/B (Nw, Nrad, Nint)
+  std::vector<C> DF((size_t)Nw * Nbeta * Nint), FK((size_t)Nw * Nbeta * Nint);
+  std::vector<R> AM((size_t)Nw * Nrad * Nint), RD((size_t)Nw * Nrad * Nint);
+  auto at = [&](int i, int j, int k, int nj) { return i + (size_t)Nw * (j + (size_t)nj * k); };
+  const C II(0., 1.);
+  {
+    ListReader fr(dir + "/results/Forces.dat");
+    for (int k = 0; k < Nint; ++k) {
+      auto v = fr.read(2 * (size_t)Nw * (Nbeta + Nrad));
+      size_t c = 0;
+      for (int i = 0; i < Nw; ++i) {
+        for (int j = 0; j < Nbeta; ++j, c += 2) DF[at(i, j, k, Nbeta)] = std::stod(v[c]) * std::exp(II * std::stod(v[c + 1]));
+        for (int j = 0; j < Nrad; ++j, c += 2) {
+          AM[at(i, j, k, Nrad)] = std::stod(v[c]);
+          RD[at(i, j, k, Nrad)] = std::stod(v[c + 1]);
+        }
+      }
+    }
+  }
+  {
+    ListReader fk(dir + "/results/FKForce.tec");
+    for (int k = 0; k <= Nint; ++k) fk.skip();
+    for (int j = 0; j < Nbeta; ++j) {
+      fk.skip();
+      for (int i = 0; i < Nw; ++i) {
+        auto v = fk.read(1 + 2 * (size_t)Nint);
+        for (int k = 0; k < Nint; ++k)
+          FK[at(i, j, k, Nbeta)] = std::stod(v[1 + 2 * k]) * std::exp(II * std::stod(v[2 + 2 * k]));
+      }
+    }
+  }
+  // SaveTResults (Results.f90:167-251)
+  const std::string rd = dir + "/results/";
+  {
+    Text t(rd + "RadiationCoefficients.tec");
+    t.line("VARIABLES=\"w (rad/s)\"\n");
+    for (int k = 0; k < Nint; ++k) t.line("\"A%4d%4d\" \"B%4d%4d\"\n", fbody[k], fmode[k], fbody[k], fmode[k]);
+    for (int j = 0; j < Nrad; ++j) {
+      t.line("Zone t=\"Motion of body %4d in DoF%4d\",I=%6d,F=POINT\n", rbody[j], rmode[j], Nw);
+      for (int i = 0; i < Nw; ++i) {
+        t.line(" %.17E", w[i]);
+        for (int k = 0; k < Nint; ++k) t.line(" %.17E %.17E", AM[at(i, j, k, Nrad)], RD[at(i, j, k, Nrad)]);
+        t.line("\n");
+      }
+    }
+  }
+  for (int which = 0; which < 2; ++which) {
+    Text t(rd + (which == 0 ? "DiffractionForce.tec" : "ExcitationForce.tec"));
+    t.line("VARIABLES=\"w (rad/s)\"\n");
+    for (int k = 0; k < Nint; ++k)
+      t.line("\"abs(F%4d%4d)\" \"angle(F%4d%4d)\"\n", fbody[k], fmode[k], fbody[k], fmode[k]);
+    for (int j = 0; j < Nbeta; ++j) {
+      t.line("Zone t=\"Diffraction force - beta = %7.3f deg\",I=%6d,F=POINT\n", beta[j] * 180. / (4. * std::atan(1.0)),
+             Nw);
+      for (int i = 0; i < Nw; ++i) {
+        t.line(" %.17E", w[i]);
+        for (int k = 0; k < Nint; ++k) {
+          const C F = which == 0 ? DF[at(i, j, k, Nbeta)] : DF[at(i, j, k, Nbeta)] + FK[at(i, j, k, Nbeta)];
+          t.line(" %.17E %.17E", std::abs(F), std::atan2(F.imag(), F.real()));
+        }
+        t.line("\n");
+      }
+    }
+  }
+  for (int which = 0; which < 2; ++which) {   // CA.dat (damping), CM.dat (added mass)
+    Text t(rd + (which == 0 ? "CA.dat" : "CM.dat"));
+    t.line("Nb de periode : %5d\n", Nw);
+    const std::vector<R>& X = which == 0 ? RD : AM;
+    for (int l = 0; l < Nw; ++l) {
+      t.line(" %.17E\n", w[l]);
+      for (int j = 0; j < Nrad; ++j) {
+        // (6(X,E13.6)): a new record after every six values
+        for (int k = 0; k < Nrad; ++k) t.line(" %.17E%s", X[at(l, j, k, Nrad)], (k % 6 == 5 || k == Nrad - 1) ? "\n" : "");
+      }
+    }
+  }
+  {
+    Text t(rd + "Fe.dat");
+    t.line("VARIABLES=\"Period (s)\" \"|Fx| (N/m)\" \"|Fy| (N/m)\" \"|Fz| (N/m)\" \"|Cx| (N)\" \"|Cy| (N)\" \"|Cz| (N)\" "
+           "\"ang(Fx) (\xb0)\" \"ang(Fy) (\xb0)\" \"ang(Fz) (\xb0)\" \"ang(Cx) (\xb0)\" \"ang(Cy) (\xb0)\" \"ang(Cz) (\xb0)\"\n");
+    t.line("Zone t=\"Corps %2d\"\n", 1);
+    for (int j = 0; j < Nbeta; ++j) {
+      t.line("Zone t=\"Diffraction force - beta = %7.3f deg\",I=%6d,F=POINT\n", beta[j] * 180. / PI, Nw);
+      for (int l = 0; l < Nw; ++l) {
+        t.line(" %.17E", w[l]);
+        for (int k = 0; k < Nint; ++k) t.line(" %.17E", std::abs(DF[at(l, j, k, Nbeta)] + FK[at(l, j, k, Nbeta)]));
+        for (int k = 0; k < Nint; ++k) {
+          const C F = DF[at(l, j, k, Nbeta)] + FK[at(l, j, k, Nbeta)];
+          t.line(" %.17E", 180. / PI * std::atan2(F.imag(), F.real()));
+        }
+        t.line("\n");
+      }
+    }
+  }
+  // Initialize_IRF (IRF.f90:72-98): the line after "--- Post processing "
+  ListReader cal(dir + "/Nemoh.cal");
+  while (true) {
+    if (cal.pos >= cal.lines.size()) throw Stop(ST_IO, "Nemoh.cal: no post-processing section");
+    if (cal.lines[cal.pos++].compare(0, 20, "--- Post processing ") == 0) break;
+  }
+  auto irf = cal.read(3);
+  if (std::stoi(irf[0]) == 1) {
+    const R dt = std::stod(irf[1]), tf = std::stod(irf[2]);
+    const int Ntime = (int)(tf / dt);
+    std::vector<R> K((size_t)Ntime * Nrad * Nint), ainf((size_t)Nrad * Nint);
+    compute_irf(Nw, w.data(), Nrad, Nint, RD.data(), AM.data(), Ntime, dt, K.data(), ainf.data());
+    // Save_IRF (IRF.f90:129-145)
+    Text t(rd + "IRF.tec");
+    t.line(" VARIABLES=\"Time (s)\"\n");
+    for (int k = 0; k < Nint; ++k) t.line("\"AddedMass %4d\" \"IRF %4d\"\n", k + 1, k + 1);
+    for (int j = 0; j < Nrad; ++j) {
+      t.line("Zone t=\"DoF %4d\",I=%6d,F=POINT\n", j + 1, Ntime);
+      for (int i = 0; i < Ntime; ++i) {
+        t.line(" %.17E", i * dt);
+        for (int k = 0; k < Nint; ++k)
+          t.line(" %.17E %.17E", ainf[j + (size_t)Nrad * k], K[i + (size_t)Ntime * (j + (size_t)Nrad * k)]);
+        t.line("\n");
+      }
+    }
+  }
+  return 0;
+}
+
 #define ORACLE_TRY(...)                                            \
   try {                                                            \
     __VA_ARGS__;                                                          \
@@ -2514,6 +2730,15 @@ void nemoh_oracle_set_nq(void* h, int nq) { static_cast<Oracle*>(h)->NQ = nq; }
 
 int nemoh_oracle_run_case(const char* root, int cache_s, double* seconds) {
   ORACLE_TRY(run_case(root ? root : "", cache_s != 0, seconds))
+}
+
+// post-processor on the case named by <root>/ID.dat (postProcessor/Main.f90)
+int nemoh_oracle_postproc(const char* root) { ORACLE_TRY(postproc_case(root ? root : "")) }
+
+// Compute_IRF on given coefficients (layouts as compute_irf)
+int nemoh_oracle_irf(int nw, const double* w, int nrad, int nint, const double* damping, const double* added_mass,
+                     int ntime, double dt, double* K, double* ainf) {
+  ORACLE_TRY(compute_irf(nw, w, nrad, nint, damping, added_mass, ntime, dt, K, ainf))
 }
 
 void nemoh_oracle_gg(double zr, double zi, double cr, double ci, double* out) {

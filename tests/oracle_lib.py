@@ -188,3 +188,26 @@ def gaussz_inverse(a):
     out = np.zeros_like(a, order="F")
     _check(lib().nemoh_oracle_gaussz_inverse(a.shape[0], a.ctypes.data_as(_d), out.ctypes.data_as(_d)))
     return out
+
+
+def postproc(root):
+    """The post-processor (postProcessor/Main.f90) on the case named by root/ID.dat."""
+    L = lib()
+    L.nemoh_oracle_postproc.argtypes = [ctypes.c_char_p]
+    _check(L.nemoh_oracle_postproc(root.encode()))
+
+
+def irf(w, damping, added_mass, ntime, dt):
+    """Compute_IRF: damping/added mass (nw, nrad, nint) -> K (ntime, nrad, nint), A_inf (nrad, nint)."""
+    L = lib()
+    L.nemoh_oracle_irf.argtypes = [ctypes.c_int, _d, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int,
+                                   ctypes.c_double, _d, _d]
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    B = np.asfortranarray(damping, dtype=np.float64)
+    A = np.asfortranarray(added_mass, dtype=np.float64)
+    nw, nrad, nint = B.shape
+    K = np.zeros((ntime, nrad, nint), order="F")
+    ainf = np.zeros((nrad, nint), order="F")
+    _check(L.nemoh_oracle_irf(nw, w.ctypes.data_as(_d), nrad, nint, B.ctypes.data_as(_d), A.ctypes.data_as(_d),
+                              ntime, dt, K.ctypes.data_as(_d), ainf.ctypes.data_as(_d)))
+    return K, ainf
