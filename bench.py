@@ -253,6 +253,75 @@ def run_batched(local, n_bodies, n_omega=20, seed=4):
     return out
 
 
+def _wall(fn, reps):
+    fn()   # warm-up (workspace growth, first-touch)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    return (time.perf_counter() - t0) / reps
+
+
+def run_outputs(local, omega_index=10):
+    """The solver's output stages beside the solve, on the barge at one
+    finite-depth frequency and its 9 problems, each timed through the C-ABI
+    with host buffers (copies included): Kochin function at 361 directions,
+    free-surface elevation on the pre-processor's 101 x 101 grid over
+    400 m x 400 m, the pre-processor's body conditions for the 40 x 9 problems,
+    and the post-processor's impulse response functions (40 frequencies,
+    6 x 6 coefficients, 1,000 time steps). Beside each, the CPU oracle (one
+    core) on a bounded sample of the same work, scaled to the same unit."""
+    import nemoh_b200 as nb
+    from nemoh_b200 import cases as C
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    case = C.config_barge(n_omega=N_OMEGA)
+    w = float(case.omegas[omega_index])
+    T = 2 * np.pi / w
+    nv = C.body_conditions(case)
+    cols = range(omega_index * NPROB, (omega_index + 1) * NPROB)
+    out = {"omega": w, "problems": NPROB, "n_panels": case.mesh.npanels,
+           "timing": "host wall clock around the C-ABI call, host<->device copies included"}
+    m = case.mesh
+    with nb.Solver(local, nb.FP64) as s:
+        s.set_case(case)
+        res = [s.solve_potential(T, nv[:, j]) for j in cols]
+        zigb = np.stack([r["zigb"] for r in res], axis=1)
+        zigs = np.stack([r["zigs"] for r in res], axis=1)
+        theta = np.linspace(0.0, 2 * np.pi, 361)
+        t = _wall(lambda: s.kochin(T, theta, zigb, zigs), 5)
+        out["kochin"] = {"directions": 361, "ms": t * 1e3, "unit": "directions x problems / s",
+                         "value": 361 * NPROB / t}
+        pts, _ = C.freesurface_grid(101, 101, 400.0, 400.0)
+        t = _wall(lambda: s.free_surface(T, pts, zigb, zigs), 3)
+        out["free_surface"] = {"points": len(pts), "ms": t * 1e3, "unit": "points x problems / s",
+                               "value": len(pts) * NPROB / t,
+                               "green_pairs_per_s": len(pts) * m.npanels / t}
+        t = _wall(lambda: s.body_conditions(case), 5)
+        out["body_conditions"] = {"problems": case.nproblems, "ms": t * 1e3, "unit": "problems / s",
+                                  "value": case.nproblems / t}
+        rng = np.random.default_rng(1)
+        wv = np.linspace(0.05, 2.5, 40)
+        Bc = rng.standard_normal((40, 6, 6)) * np.exp(-wv)[:, None, None]
+        Ac = rng.standard_normal((40, 6, 6))
+        t = _wall(lambda: s.irf(wv, Bc, Ac, 1000, 0.1), 5)
+        out["irf"] = {"nw": 40, "pairs": 36, "ntime": 1000, "ms": t * 1e3}
+    # CPU oracle on bounded samples (one core)
+    o = O.Oracle(m.nodes, m.panels, m.isym, case.rho, case.g, case.depth)
+    th8 = theta[:8]
+    t = _wall(lambda: o.kochin(T, th8, zigb, zigs), 1)
+    out["kochin"]["cpu_oracle_value"] = 8 * NPROB / t
+    t = _wall(lambda: o.free_surface(T, pts[:64], zigb[:, :1], zigs[:, :1]), 1)
+    out["free_surface"]["cpu_oracle_value"] = 64 / t
+    t = _wall(lambda: (C.body_conditions(case), C.generalised_normals(case), C.froude_krylov(case)), 1)
+    out["body_conditions"]["cpu_host_value"] = case.nproblems / t
+    t = _wall(lambda: O.irf(wv, Bc, Ac, 1000, 0.1), 1)
+    out["irf"]["cpu_oracle_ms"] = t * 1e3
+    out["cpu"] = ("oracle (C++, 1 core) on 8 directions x 9 problems / 64 points x 1 problem, scaled; body conditions: "
+                  "the numpy pre-processor restatement in nemoh_b200.cases")
+    del o
+    return out
+
+
 def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9), seed=5, n_check=64, workers=4):
     """Serving workload: Poisson request streams over the batched workload's
     bodies (one omega U(0.1, 2.5), heading U(0, 180) deg, 6 DOF per request)
@@ -447,7 +516,8 @@ def run_ours(args):
         r["solver"].close()
     results = {}
     if rank == 0 and not args.no_extras:
-        for key, fn in (("batched", lambda: run_batched(local, args.bodies)),
+        for key, fn in (("outputs", lambda: run_outputs(local)),
+                        ("batched", lambda: run_batched(local, args.bodies)),
                         ("serve", lambda: run_serving(local, args.bodies, args.requests))):
             try:
                 line[key] = fn()
