@@ -282,6 +282,15 @@ void assemble_range(nemoh_ctx* c, int s0, int s1) {
     LAUNCHED(c);
   }
   if (nfd) {
+    static bool attr = false;
+    if (!attr) {
+      CK(cudaFuncSetAttribute(fd_images_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, IMG_SMEM));
+      attr = true;
+    }
+    const unsigned nt = (N + IMG_T - 1) / IMG_T;
+    fd_images_kernel<<<dim3(nt, nt, (unsigned)nfd), IMG_THREADS, IMG_SMEM, c->stream>>>(g, dom, ds + ninfd, rec, rows,
+                                                                                      N, o);
+    LAUNCHED(c);
     dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
     rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
     LAUNCHED(c);

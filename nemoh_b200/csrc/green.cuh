@@ -635,65 +635,84 @@ __device__ __forceinline__ void wave_fd_pair(const GreenCtx& g, const OmegaParam
 }
 
 // --- VNSFD exponential images (COMPUTE_GREEN_FD.f90:635-706) ----------------
-//   sum_KE AR(KE) (-A/8pi) sum_4 1/rho  and their gradients, per reflection.
+//   sum_KE AR(KE) (-A_J/8pi) sum_4 1/rho  and their gradients, per reflection.
 // The reference adds them to FS1, VSX1, VSY1, VSZ1 of each reflection, and
 // those enter SP1/SM1 and the real parts of D+/- linearly (:830-865). Image
 // depths are shared by both reflections; RO > EPS is decided exactly on RO^2
 // against a precomputed threshold.
-__device__ __forceinline__ void fd_exp_images(const GreenCtx& g, double H, const double* ambda, const double* ar,
-                                              int nexp1, double XGI, double YGI, double ZMIII, const PanelRec& P,
-                                              int NJJ, double* fs, double* vx, double* vy, double* vz) {
-  const double QPI = 4. * 3.141592653589793;
+//
+// The four image depths of collocation I and panel J are
+//   z0 = ZI - 2h + h l - ZJ,  z1 = -ZI - h l - ZJ,  z2 = -ZI - 4h + h l - ZJ,
+//   z3 = ZI + 2h - h l - ZJ,
+// and exchanging I and J maps z0 -> -z3, z3 -> -z0 and keeps z1, z2; the
+// horizontal distance of both reflections is unchanged. So one evaluation of
+// the 4 (NEXP+1) reciprocal distances of an unordered pair serves both
+// ordered pairs. Per reflection b it returns, without the panel factor
+// ACT = -A/8pi,
+//   fs = sum AR sum_k 1/rho_k,        sa = sum AR sum_k 1/rho_k^3,
+//   m1 = sum AR (z0 a0 - z1 a1 - z2 a2 + z3 a3),
+//   m2 = sum AR (z0 a0 + z1 a1 + z2 a2 + z3 a3),   a_k = 1/rho_k^3,
+// from which the pair (I, J) takes fs, -dx sa, -dy sa, -m1 (times ACT_J) and
+// the pair (J, I) takes fs, dx sa, -dy' sa, +m2 (times ACT_I), dy' being the
+// y distance of (J, I) (-dy for the direct reflection, dy for the mirror).
+struct ImageSums {
+  double fs[2], sa[2], m1[2], m2[2], dx[2], dy[2];
+};
+
+__device__ __forceinline__ void fd_image_sums(const GreenCtx& g, double H, const double* ambda, const double* ar,
+                                              int nexp1, double XI, double YI, double ZI, double XJ, double YJ,
+                                              double ZJ, int NJJ, ImageSums& o) {
   const double H2 = XMUL(2., H), H4 = XMUL(4., H);
   const double T2 = g.ro_eps2;
-  double dx[2], dy[2], r2[2];
+  double r2[2];
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
-    fs[b] = vx[b] = vy[b] = vz[b] = 0.;
-    dx[b] = XSUB(XGI, P.xg);
-    dy[b] = XSUB(YGI, P.yg * (b ? -1. : 1.));
-    const double R = XSQRT(XADD(XMUL(dx[b], dx[b]), XMUL(dy[b], dy[b])));
+    o.fs[b] = o.sa[b] = o.m1[b] = o.m2[b] = 0.;
+    o.dx[b] = XSUB(XI, XJ);
+    o.dy[b] = XSUB(YI, YJ * (b ? -1. : 1.));
+    const double R = XSQRT(XADD(XMUL(o.dx[b], o.dx[b]), XMUL(o.dy[b], o.dy[b])));
     r2[b] = XMUL(R, R);
   }
-  const double ACT = -0.5 * P.aire / QPI;
 #pragma unroll 1
   for (int KE = 1; KE <= nexp1; ++KE) {
-    const double AQT = ACT * ar[KE];
+    const double A = ar[KE];
     const double HA = XMUL(H, ambda[KE]);
     double zp[4], z2[4];
-    zp[0] = XSUB(XADD(XSUB(ZMIII, H2), HA), P.zg);
-    zp[1] = XSUB(XSUB(-ZMIII, HA), P.zg);
-    zp[2] = XSUB(XADD(XSUB(-ZMIII, H4), HA), P.zg);
-    zp[3] = XSUB(XSUB(XADD(ZMIII, H2), HA), P.zg);
+    zp[0] = XSUB(XADD(XSUB(ZI, H2), HA), ZJ);
+    zp[1] = XSUB(XSUB(-ZI, HA), ZJ);
+    zp[2] = XSUB(XADD(XSUB(-ZI, H4), HA), ZJ);
+    zp[3] = XSUB(XSUB(XADD(ZI, H2), HA), ZJ);
 #pragma unroll
     for (int k = 0; k < 4; ++k) z2[k] = XMUL(zp[k], zp[k]);
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
       if (b >= NJJ) break;
-      double a[4], sa = 0.;
+      double a[4], f = 0., sa = 0.;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const double RRk = XADD(r2[b], z2[k]);
         if (RRk > T2) {
           const double ri = rsqrt(RRk);
-          const double FT = AQT * ri;
-          fs[b] += FT;
-          a[k] = FT * ri * ri;
+          f += ri;
+          a[k] = ri * ri * ri;
         } else {
           a[k] = 0.;
         }
         sa += a[k];
       }
-      vx[b] -= dx[b] * sa;
-      vy[b] -= dy[b] * sa;
-      vz[b] -= zp[0] * a[0] - zp[1] * a[1] - zp[2] * a[2] + zp[3] * a[3];
+      const double p0 = zp[0] * a[0], p1 = zp[1] * a[1], p2 = zp[2] * a[2], p3 = zp[3] * a[3];
+      o.fs[b] += A * f;
+      o.sa[b] += A * sa;
+      o.m1[b] += A * ((p0 - p1) - (p2 - p3));
+      o.m2[b] += A * ((p0 + p1) + (p2 + p3));
     }
   }
 }
 
 // --- Rankine part of one pair, both symmetry classes -------------------------
-// Real parts of D+/- and S+/- (the wave pass adds the rest). In finite depth
-// this also carries the exponential images of the submerged-panel branch.
+// Real parts of D+/- and S+/- (the wave pass adds the rest). The exponential
+// images of the finite-depth submerged-panel branch come from fd_image_sums,
+// evaluated once per unordered pair by fd_images_kernel.
 struct RealOut {
   double dp, dm, sp, sm;
 };
@@ -704,26 +723,6 @@ __device__ __forceinline__ void pair_rankine(const GreenCtx& g, const OmegaParam
                                              double YNI, double ZNI, bool self, const PanelRec& P, RealOut& out) {
   RankineOut r;
   rankine<FD>(g, FD ? XMUL(2., om.h) : 0., XGI, YGI, ZGI, self, P, r);
-  if (FD && ZGI < g.zer && P.zg < g.zer) {
-    const int NJJ = g.nsymy + 1;
-    double fs[2], vx[2], vy[2], vz[2];
-    fd_exp_images(g, om.h, ambda, ar, om.nexp + 1, XGI, YGI, ZGI, P, NJJ, fs, vx, vy, vz);
-    if (NJJ == 2) {
-      r.FSP += fs[0] + fs[1];
-      r.FSM += fs[0] - fs[1];
-      r.VSXP += vx[0] + vx[1];
-      r.VSXM += vx[0] - vx[1];
-      r.VSYP += vy[0] + vy[1];
-      r.VSYM += vy[0] - vy[1];
-      r.VSZP += vz[0] + vz[1];
-      r.VSZM += vz[0] - vz[1];
-    } else {
-      r.FSP += fs[0];
-      r.VSXP += vx[0];
-      r.VSYP += vy[0];
-      r.VSZP += vz[0];
-    }
-  }
   out.dp = r.VSXP * XNI + r.VSYP * YNI + r.VSZP * ZNI;
   out.dm = r.VSXM * XNI + r.VSYM * YNI + r.VSZM * ZNI;
   out.sp = r.FSP;
