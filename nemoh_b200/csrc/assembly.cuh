@@ -143,7 +143,7 @@ __global__ void crek_kernel(const double* __restrict__ xr, const double* __restr
 constexpr int ASM_ROWS = 128;
 constexpr int ASM_TJ = 32;
 #ifndef ASM_MINB_RANKINE
-#define ASM_MINB_RANKINE 4
+#define ASM_MINB_RANKINE 3
 #endif
 #ifndef ASM_MINB_WAVE_FD
 #define ASM_MINB_WAVE_FD 3

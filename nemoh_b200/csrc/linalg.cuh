@@ -94,32 +94,40 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* 
   factor_block(diag, nb, status, true);
   C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
+  // One thread per column of each inverse, the column held in registers. The
+  // substitutions run over the full index range: entries outside the triangle
+  // are exact zeros, so the extra terms change nothing.
   const int t = threadIdx.x;
   if (t < nb) {
     // column t of inv(L11): unit lower, forward substitution
-    C2* y = D + LU_NB * LU_NB + nb * t;
-    for (int i = 0; i < nb; ++i) {
+    C2 y[LU_NB];
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i) {
       C2 v = mkc<C2>(i == t ? 1. : 0., 0.);
-      if (i > t)
-        for (int j = t; j < i; ++j) v = cfms(v, diag[i + nb * j], y[j]);
-      else if (i < t)
-        v = mkc<C2>(0., 0.);
-      y[i] = v;
+#pragma unroll
+      for (int j = 0; j < i; ++j) v = cfms(v, diag[i + nb * j], y[j]);
+      y[i] = (i < nb) ? v : mkc<C2>(0., 0.);
     }
+    C2* out = D + LU_NB * LU_NB + nb * t;
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i)
+      if (i < nb) out[i] = y[i];
   } else if (t >= 32 && t < 32 + nb) {
     // column c of inv(U11): upper, back substitution
     const int c = t - 32;
-    C2* y = D + 2 * LU_NB * LU_NB + nb * c;
-    for (int i = nb - 1; i >= 0; --i) {
+    C2 y[LU_NB];
+#pragma unroll
+    for (int i = LU_NB - 1; i >= 0; --i) {
       C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
-      if (i <= c) {
-        for (int j = i + 1; j <= c; ++j) v = cfms(v, diag[i + nb * j], y[j]);
-        v = cdv(v, diag[i + nb * i]);
-      } else {
-        v = mkc<C2>(0., 0.);
-      }
-      y[i] = v;
+#pragma unroll
+      for (int j = i + 1; j < LU_NB; ++j)
+        if (j < nb) v = cfms(v, diag[i + nb * j], y[j]);
+      y[i] = (i <= c) ? cdv(v, diag[i + nb * i]) : mkc<C2>(0., 0.);
     }
+    C2* out = D + 2 * LU_NB * LU_NB + nb * c;
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i)
+      if (i < nb) out[i] = y[i];
   }
 }
 
@@ -130,7 +138,7 @@ __device__ __forceinline__ void cmac(C2& acc, C2 a, C2 b) {
 }
 
 // L21 <- A21 inv(U11) (CTAs [0, nrb), one thread per row) and
-// U12 <- inv(L11) A12 (CTAs [nrb, nrb+ncb), one thread per column), with the
+// U12 <- inv(L11) A12 (CTAs [nrb, nrb+ncb), one lane per row of a column), with the
 // inverses from lu_diag_kernel; CTA 0 also stores the factored A11 into A
 // (no kernel of the step reads A11 from A). Launch with at least one CTA.
 template <class C2>
@@ -174,26 +182,15 @@ __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
     work[i + nb * c] = A[(k + i) + (long long)n * (c0 + c)];
   }
   __syncthreads();
-  if (threadIdx.x < ncol) {
-    // y(i) = sum_{j <= i} invL(i, j) a(j), in place from the bottom up
-    C2* y = work + nb * threadIdx.x;
-    C2 a[LU_NB];
-#pragma unroll
-    for (int j = 0; j < LU_NB; ++j) a[j] = (j < nb) ? y[j] : mkc<C2>(0., 0.);
-#pragma unroll
-    for (int i = 0; i < LU_NB; ++i) {
-      if (i < nb) {
-        C2 acc = a[i];
-#pragma unroll
-        for (int j = 0; j < i; ++j) cmac(acc, inv[i + nb * j], a[j]);
-        y[i] = acc;
-      }
-    }
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < nb * ncol; q += blockDim.x) {
-    const int i = q % nb, c = q / nb;
-    A[(k + i) + (long long)n * (c0 + c)] = work[i + nb * c];
+  // y(i, c) = a(i, c) + sum_{j < i} invL(i, j) a(j, c): lane = row i, the
+  // CTA's four warps take every fourth column; results go straight to A
+  const int i = threadIdx.x & 31;
+  if (i >= nb) return;
+  for (int c = threadIdx.x >> 5; c < ncol; c += LU_RB / 32) {
+    const C2* a = work + nb * c;
+    C2 acc = a[i];
+    for (int j = 0; j < i; ++j) cmac(acc, inv[i + nb * j], a[j]);
+    A[(k + i) + (long long)n * (c0 + c)] = acc;
   }
 }
 
@@ -487,9 +484,11 @@ __global__ void __launch_bounds__(128) trsm_fused_kernel(BatchT<C2> b, const C2*
       Sb[i + TB * p] = (i < nb) ? Y[(k + i) + (long long)n * p] : mkc<C2>(0., 0.);
     }
     __syncthreads();
-    // rows of this CTA: forward [k+nb+64c, ...), backward [k-64(c+1), k-64c)
+    // rows of this CTA: forward [k+nb+64c, ...), backward [k-64(c+1), k-64c).
+    // A lane pair shares a row: lane parity picks the half of the 64 columns,
+    // and the two partial sums meet through a shuffle.
     const int r0 = LOWER ? k + nb + (int)blockIdx.x * TB : k - ((int)blockIdx.x + 1) * TB;
-    const int row = threadIdx.x & (TB - 1), part = threadIdx.x >> 6;   // two halves of the 64 columns
+    const int row = threadIdx.x >> 1, part = threadIdx.x & 1;
     const int r = r0 + row;
     const bool live = LOWER ? (r < n) : (r >= 0);
     C2 a[TB / 2];
@@ -498,24 +497,23 @@ __global__ void __launch_bounds__(128) trsm_fused_kernel(BatchT<C2> b, const C2*
       const int c = part * (TB / 2) + j;
       a[j] = (live && c < nb) ? A[r + (long long)n * (k + c)] : mkc<C2>(0., 0.);
     }
-    // partials of the second half go through shared memory (reuse Ti)
+    const C2* Sp = Sb + part * (TB / 2);
     for (int p = 0; p < nrhs; ++p) {
       C2 acc = mkc<C2>(0., 0.);
 #pragma unroll
-      for (int j = 0; j < TB / 2; ++j) cmad(acc, a[j], Sb[part * (TB / 2) + j + TB * p]);
-      if (part == 1) Ti[row + TB * p] = acc;
-      __syncthreads();
+      for (int j = 0; j < TB / 2; ++j) cmad(acc, a[j], Sp[j + TB * p]);
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
       if (part == 0 && live) {
-        const C2 o = Ti[row + TB * p];
         C2* q = X + r + (long long)n * p;
         C2 v = *q;
-        v.x -= acc.x + o.x;
-        v.y -= acc.y + o.y;
+        v.x -= acc.x;
+        v.y -= acc.y;
         *q = v;
         if (blockIdx.x == 0) Xn[row + TB * p] = v;
       }
-      __syncthreads();
     }
+    __syncthreads();
     if (blockIdx.x != 0) return;
     nxt = LOWER ? blk + 1 : blk - 1;
     if (nxt < 0 || nxt >= nblk) return;
