@@ -294,7 +294,9 @@ void assemble_range(nemoh_ctx* c, int s0, int s1) {
     dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
     rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
     LAUNCHED(c);
-    wave_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
+    const unsigned wt = (N + WS_T - 1) / WS_T;
+    wave_fd_sym_kernel<<<dim3(wt * (wt + 1) / 2, 1, (unsigned)nfd), WS_THREADS, 0, c->stream>>>(g, dom, ds + ninfd,
+                                                                                               rec, N, o);
     LAUNCHED(c);
   }
 }

@@ -349,6 +349,100 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(Gre
   }
 }
 
+// ---------------------------------------------------------------------------
+// Finite-depth wave pass over the upper triangle of 16 x 16 tiles: a pair of
+// submerged panels is evaluated once for both orders (wave_fd_sym), any other
+// pair once per order (pair_wave); both the tile and its transpose are added
+// to the real parts and written to the imaginary parts, column by column
+// through shared memory.
+// ---------------------------------------------------------------------------
+constexpr int WS_T = 16;
+constexpr int WS_THREADS = 128;
+
+// linear index t over the upper triangle (a <= b) of a T x T tile grid
+__device__ __forceinline__ void tri_tile(int t, int T, int& a, int& b) {
+  auto start = [T](int r) { return r * T - r * (r - 1) / 2; };
+  const double q = 2. * T + 1.;
+  int r = (int)((q - sqrt(q * q - 8. * t)) * 0.5);
+  r = max(0, min(T - 1, r));
+  while (r > 0 && start(r) > t) --r;
+  while (r < T - 1 && start(r + 1) <= t) ++r;
+  a = r;
+  b = r + (t - start(r));
+}
+
+// one order of a pair with a panel at the free surface (rare; kept out of line)
+__device__ __noinline__ void pair_wave_fd_ordered(const GreenCtx& g, const OmegaParams& om, const PanelRec& PC,
+                                                  const PanelRec& PS, PairOut& out) {
+  pair_wave<true>(g, om, PC.xg, PC.yg, PC.zg, PC.xn, PC.yn, PC.zn, PS, out);
+}
+
+__global__ void __launch_bounds__(WS_THREADS, ASM_MINB_WAVE_FD) wave_fd_sym_kernel(
+    GreenCtx g, const OmegaParams* __restrict__ oms, const int* __restrict__ slots, const PanelRec* __restrict__ rec,
+    int N, AsmOut out) {
+  __shared__ PairOut res[2][WS_T * WS_T];   // [0]: (A_i, B_j) at j*T+i; [1]: (B_j, A_i) at i*T+j
+  __shared__ PanelRec pa[WS_T], pb[WS_T];
+  __shared__ OmegaParams som;
+  const int T = (N + WS_T - 1) / WS_T;
+  int ta, tb;
+  tri_tile(blockIdx.x, T, ta, tb);
+  const int slot = slots[blockIdx.z];
+  stage_params(oms + slot, &som);
+  const int a0 = ta * WS_T, b0 = tb * WS_T;
+  const int na = min(WS_T, N - a0), nb = min(WS_T, N - b0);
+  stage_panels(rec, a0, na, pa);
+  stage_panels(rec, b0, nb, pb);
+  __syncthreads();
+  const bool diag = ta == tb;
+  const int NJJ = g.nsymy + 1;
+  auto live = [&](int i, int j) { return i < na && j < nb && !(diag && i > j); };
+#pragma unroll 1
+  for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {
+    const int i = q % WS_T, j = q / WS_T;
+    if (!live(i, j)) continue;
+    const PanelRec& PI = pa[i];
+    const PanelRec& PJ = pb[j];
+    const bool both = !(diag && i == j);
+    if (PI.zg < g.zer && PJ.zg < g.zer) {
+      PairOut oij, oji;
+      if (!wave_fd_sym(g, som, PI, PJ, NJJ, both, oij, oji)) {
+        set_status(g.status, ST_AKZ_UNDEFINED);
+        oij = oji = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
+      }
+      res[0][j * WS_T + i] = oij;
+      if (both) res[1][i * WS_T + j] = oji;
+    } else {
+      pair_wave_fd_ordered(g, som, PI, PJ, res[0][j * WS_T + i]);
+      if (both) pair_wave_fd_ordered(g, som, PJ, PI, res[1][i * WS_T + j]);
+    }
+  }
+  __syncthreads();
+  const long long NN = (long long)N * N;
+  double2* od = out.d + slot * out.slot_stride;
+  double2* os = out.s + slot * out.slot_stride;
+  auto add = [&](long long o, const PairOut& r) {
+    double2 d = od[o], sv = os[o];
+    od[o] = make_double2(d.x + r.dp_re, r.dp_im);
+    os[o] = make_double2(sv.x + r.sp_re, r.sp_im);
+    if (NJJ == 2) {
+      d = od[NN + o];
+      sv = os[NN + o];
+      od[NN + o] = make_double2(d.x + r.dm_re, r.dm_im);
+      os[NN + o] = make_double2(sv.x + r.sm_re, r.sm_im);
+    }
+  };
+  for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {
+    {   // entry (a0 + i, b0 + j)
+      const int i = q % WS_T, j = q / WS_T;
+      if (live(i, j)) add((a0 + i) + (long long)N * (b0 + j), res[0][j * WS_T + i]);
+    }
+    {   // entry (b0 + j, a0 + i); the diagonal of a diagonal tile is done above
+      const int j = q % WS_T, i = q / WS_T;
+      if (live(i, j) && !(diag && i == j)) add((b0 + j) + (long long)N * (a0 + i), res[1][i * WS_T + j]);
+    }
+  }
+}
+
 template <bool FD>
 __global__ void __launch_bounds__(ASM_ROWS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_WAVE_INFD) wave_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
                                                         const int* __restrict__ slots, const PanelRec* __restrict__ rec,

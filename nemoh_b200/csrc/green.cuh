@@ -634,6 +634,121 @@ __device__ __forceinline__ void wave_fd_pair(const GreenCtx& g, const OmegaParam
   }
 }
 
+// --- VNSFD tabulated branch for both orders of a pair ------------------------
+// With both panels submerged the four image depths of (I, J) are
+//   Z1 = ZI + ZJ, Z2 = (ZJ - ZI) - 2h, Z3 = (ZI - ZJ) - 2h, Z4 = (-ZJ - ZI) - 4h
+// and those of (J, I) are the same numbers with Z2 and Z3 exchanged; the
+// horizontal distances agree as well. So one set of table interpolations
+// serves both orders: the sums over the images are shared, and the z
+// gradient PD1Z1 - PD1Z2 + PD1Z3 - PD1Z4 of (I, J) is PD1Z1 + PD1Z2 - PD1Z3 -
+// PD1Z4 for (J, I). The x and the direct-reflection y distances change sign
+// with the order, the mirror's y distance does not. Each reflection is added
+// to the symmetry classes (+ both, - with the mirror subtracted) of the two
+// orders as it is computed. Returns false (and leaves the outputs) when an
+// image depth is too shallow for the tables (AKZ > -1.5e-6).
+__device__ __forceinline__ void wave_sym_add(const OmegaParams& om, double aire, double XN, double YN, double ZN,
+                                             double sgn, double F1, double F2, double X1, double X2, double ZA1,
+                                             double ZA2, double CVX, double CVY, PairOut& o) {
+  const double COF1 = om.coe3 * aire, COF2 = om.coe4 * aire;
+  const double COF3 = om.k0 * COF1, COF4 = om.k0 * COF2;
+  const double FS1 = COF1 * F1, FS2 = COF2 * F2;
+  const double C1V3 = -COF3 * X1, C2V3 = COF4 * X2;
+  const double D1 = (C1V3 * CVX) * XN + (C1V3 * CVY) * YN + (COF3 * ZA1) * ZN;
+  const double D2 = (C2V3 * CVX) * XN + (C2V3 * CVY) * YN + (COF4 * ZA2) * ZN;
+  o.sp_re += FS1;
+  o.sm_re += sgn * FS1;
+  o.sp_im += FS2;
+  o.sm_im += sgn * FS2;
+  o.dp_re += D1;
+  o.dm_re += sgn * D1;
+  o.dp_im += D2;
+  o.dm_im += sgn * D2;
+}
+
+__device__ __forceinline__ bool wave_fd_sym(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
+                                            const PanelRec& PJ, int NJJ, bool both, PairOut& oij, PairOut& oji) {
+  const double PI_ = 3.141592653589793, PI4 = 0.7853981633974483, DPI = 2. * PI_, EPS = 0.0001;
+  const double AM0 = om.k0, H = om.h;
+  const double H2 = XMUL(2., H), H4 = XMUL(4., H);
+  double Z[4], AKZ[4];
+  Z[0] = XADD(PI.zg, PJ.zg);
+  Z[1] = XSUB(XSUB(PJ.zg, PI.zg), H2);
+  Z[2] = XSUB(XSUB(PI.zg, PJ.zg), H2);
+  Z[3] = XSUB(XSUB(-PJ.zg, PI.zg), H4);
+  bool bad = false;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    AKZ[k] = XMUL(AM0, Z[k]);
+    bad |= AKZ[k] > -1.5E-6;
+  }
+  if (bad) return false;
+  oij = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
+  oji = oij;
+  const bool near = AKZ[0] > -16.;
+  Stencil sz[4];
+  bool have_sz = false;
+#pragma unroll 1
+  for (int b = 0; b < NJJ; ++b) {
+    const double YMJJJ = b ? -PJ.yg : PJ.yg;
+    const double dx = XSUB(PI.xg, PJ.xg), dy = XSUB(PI.yg, YMJJJ);
+    const double RRR = XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy)));
+    const double AKR = XMUL(AM0, RRR);
+    const bool tab = AKR < 99.7;
+    Stencil sx{2, 0., 0., 0.};
+    double PSK = 0., SCK = 0., SCDS = 0., SSDS = 0.;
+    if (near) {
+      if (tab) {
+        stencil_x(g, AKR, sx);
+        if (!have_sz) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (AKZ[k] > -16.) stencil_z(g, AKZ[k], sz[k]);
+          have_sz = true;
+        }
+      } else {
+        const double SQ = sqrt(DPI / AKR);
+        double SIK, CSK;
+        sincos(AKR - PI4, &SIK, &CSK);
+        PSK = PI_ * SQ * SIK;
+        SCK = SQ * CSK;
+        const double DSK = 0.5 / AKR;
+        SCDS = PI_ * SQ * (CSK - DSK * SIK);
+        SSDS = SQ * (SIK + DSK * CSK);
+      }
+    }
+    // image by image into running sums: z gradients with the signs of
+    // (I, J) (+ - + -) and of (J, I) (+ + - -)
+    double s1z = 0., spsr = 0., s2z = 0., s1x = 0., s2r = 0., zp1 = 0., zq1 = 0., zp2 = 0., zq2 = 0.;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      FdImage m;
+      fd_image(g, AM0, AKR, RRR, Z[k], AKZ[k], sx, sz[k], tab, PSK, SCK, SCDS, SSDS, m);
+      const double sp = (k & 1) ? -1. : 1., sq = (k < 2) ? 1. : -1.;
+      s1z += m.PD1Z;
+      spsr += m.PSR;
+      s2z += m.PD2Z;
+      s1x += m.PD1X;
+      s2r += m.VR2;
+      zp1 += sp * m.PD1Z;
+      zq1 += sq * m.PD1Z;
+      zp2 += sp * m.VZ2;
+      zq2 += sq * m.VZ2;
+    }
+    const double F1 = s1z - spsr;
+    const double iR = RRR > EPS ? 1. / RRR : 0.;
+    const double sgn = b ? -1. : 1.;
+    wave_sym_add(om, PJ.aire, PI.xn, PI.yn, PI.zn, sgn, F1, s2z, s1x, s2r, zp1, zp2, dx * iR, dy * iR, oij);
+    if (both)
+      wave_sym_add(om, PI.aire, PJ.xn, PJ.yn, PJ.zn, sgn, F1, s2z, s1x, s2r, zq1, zq2, -dx * iR,
+                   (b ? dy : -dy) * iR, oji);
+  }
+  if (NJJ == 1) {   // one class: the minus entries equal the plus ones
+    oij.sm_re = oij.sp_re; oij.sm_im = oij.sp_im; oij.dm_re = oij.dp_re; oij.dm_im = oij.dp_im;
+    oji.sm_re = oji.sp_re; oji.sm_im = oji.sp_im; oji.dm_re = oji.dp_re; oji.dm_im = oji.dp_im;
+  }
+  return true;
+}
+
 // --- VNSFD exponential images (COMPUTE_GREEN_FD.f90:635-706) ----------------
 //   sum_KE AR(KE) (-A_J/8pi) sum_4 1/rho  and their gradients, per reflection.
 // The reference adds them to FS1, VSX1, VSY1, VSZ1 of each reflection, and
@@ -729,31 +844,18 @@ __device__ __forceinline__ void pair_rankine(const GreenCtx& g, const OmegaParam
   out.sm = r.FSM;
 }
 
-// --- wave part of one pair, both symmetry classes ----------------------------
+// Wave sums of both reflections -> wave parts of D+/-, S+/- of one pair
+// (collocation normal XNI, YNI, ZNI; source panel area `aire`).
 template <bool FD>
-__device__ __forceinline__ void pair_wave(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI, double ZGI,
-                                          double XNI, double YNI, double ZNI, const PanelRec& P, PairOut& out) {
-  const int NJJ = g.nsymy + 1;
-  double ZMIII = ZGI;
-  if (ZGI > g.zer) ZMIII = FD ? XMUL(20., g.zer) : g.zer;
-  WaveJJ w[2];
-  if ((ZGI < g.zer) && (P.zg < g.zer)) {
-    if (FD) wave_fd_pair(g, om, XGI, YGI, ZMIII, P, NJJ, w);
-    else wave_infd_pair(g, om, XGI, YGI, ZMIII, P, NJJ, w);
-  } else {
-#pragma unroll 1
-    for (int JJ = 1; JJ <= NJJ; ++JJ) {
-      if (FD) wave_fd_fs(om, XGI, YGI, ZMIII, JJ, P, w[JJ - 1]);
-      else wave_infd_fs(om, XGI, YGI, ZMIII, JJ == 1 ? 1 : -1, P, w[JJ - 1]);
-    }
-  }
+__device__ __forceinline__ void wave_combine(const OmegaParams& om, double aire, int NJJ, WaveJJ* w, double XNI,
+                                             double YNI, double ZNI, PairOut& out) {
   if (NJJ == 1) w[1] = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
   // VNSINFD (:456-500) scales the wave sums by K A / 2pi^2, K A / 2pi (and K
   // again for gradients) with a minus sign; VNSFD (:830-865) adds them as they are
   double s1 = 1., s2 = 1., v1 = 1., v2 = 1.;
   if (!FD) {
     const double DPI = 2. * 3.141592653589793, DPI2 = 2. * 3.141592653589793 * 3.141592653589793;
-    const double AKAIR = om.k0 * P.aire;
+    const double AKAIR = om.k0 * aire;
     const double ADPI2 = AKAIR / DPI2, ADPI = AKAIR / DPI;
     s1 = -ADPI2;
     s2 = -ADPI;
@@ -777,6 +879,27 @@ __device__ __forceinline__ void pair_wave(const GreenCtx& g, const OmegaParams& 
   out.sp_im = SP2;
   out.sm_re = SM1;
   out.sm_im = SM2;
+}
+
+// --- wave part of one pair, both symmetry classes ----------------------------
+template <bool FD>
+__device__ __forceinline__ void pair_wave(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI, double ZGI,
+                                          double XNI, double YNI, double ZNI, const PanelRec& P, PairOut& out) {
+  const int NJJ = g.nsymy + 1;
+  double ZMIII = ZGI;
+  if (ZGI > g.zer) ZMIII = FD ? XMUL(20., g.zer) : g.zer;
+  WaveJJ w[2];
+  if ((ZGI < g.zer) && (P.zg < g.zer)) {
+    if (FD) wave_fd_pair(g, om, XGI, YGI, ZMIII, P, NJJ, w);
+    else wave_infd_pair(g, om, XGI, YGI, ZMIII, P, NJJ, w);
+  } else {
+#pragma unroll 1
+    for (int JJ = 1; JJ <= NJJ; ++JJ) {
+      if (FD) wave_fd_fs(om, XGI, YGI, ZMIII, JJ, P, w[JJ - 1]);
+      else wave_infd_fs(om, XGI, YGI, ZMIII, JJ == 1 ? 1 : -1, P, w[JJ - 1]);
+    }
+  }
+  wave_combine<FD>(om, P.aire, NJJ, w, XNI, YNI, ZNI, out);
 }
 
 }  // namespace nb200

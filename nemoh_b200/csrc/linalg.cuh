@@ -83,6 +83,7 @@ __device__ void factor_block(C2* s, int nb, int* status, bool report) {
 template <class C2>
 __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
   __shared__ C2 diag[LU_NB * LU_NB];
+  __shared__ C2 ywork[2 * LU_NB * LU_NB];
   const int n = b.n;
   const int nb = min(LU_NB, n - k);
   const C2* A = b.base + blockIdx.z * b.stride;
@@ -94,40 +95,43 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* 
   factor_block(diag, nb, status, true);
   C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
-  // One thread per column of each inverse, the column held in registers. The
-  // substitutions run over the full index range: entries outside the triangle
-  // are exact zeros, so the extra terms change nothing.
+  // One thread per column of each inverse; the columns being built live in
+  // shared memory (column t of a triangle at y[i * LU_NB + t], so the 32
+  // threads of a warp touch 32 consecutive elements), then go out in one
+  // coalesced store.
+  C2* yl = ywork;                    // inv(L11)
+  C2* yu = ywork + LU_NB * LU_NB;    // inv(U11)
   const int t = threadIdx.x;
   if (t < nb) {
     // column t of inv(L11): unit lower, forward substitution
-    C2 y[LU_NB];
-#pragma unroll
-    for (int i = 0; i < LU_NB; ++i) {
+    for (int i = 0; i < nb; ++i) {
       C2 v = mkc<C2>(i == t ? 1. : 0., 0.);
-#pragma unroll
-      for (int j = 0; j < i; ++j) v = cfms(v, diag[i + nb * j], y[j]);
-      y[i] = (i < nb) ? v : mkc<C2>(0., 0.);
+      if (i > t)
+        for (int j = t; j < i; ++j) v = cfms(v, diag[i + nb * j], yl[j * LU_NB + t]);
+      else if (i < t)
+        v = mkc<C2>(0., 0.);
+      yl[i * LU_NB + t] = v;
     }
-    C2* out = D + LU_NB * LU_NB + nb * t;
-#pragma unroll
-    for (int i = 0; i < LU_NB; ++i)
-      if (i < nb) out[i] = y[i];
   } else if (t >= 32 && t < 32 + nb) {
     // column c of inv(U11): upper, back substitution
     const int c = t - 32;
-    C2 y[LU_NB];
-#pragma unroll
-    for (int i = LU_NB - 1; i >= 0; --i) {
+    for (int i = nb - 1; i >= 0; --i) {
       C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
-#pragma unroll
-      for (int j = i + 1; j < LU_NB; ++j)
-        if (j < nb) v = cfms(v, diag[i + nb * j], y[j]);
-      y[i] = (i <= c) ? cdv(v, diag[i + nb * i]) : mkc<C2>(0., 0.);
+      if (i <= c) {
+        for (int j = i + 1; j <= c; ++j) v = cfms(v, diag[i + nb * j], yu[j * LU_NB + c]);
+        v = cdv(v, diag[i + nb * i]);
+      } else {
+        v = mkc<C2>(0., 0.);
+      }
+      yu[i * LU_NB + c] = v;
     }
-    C2* out = D + 2 * LU_NB * LU_NB + nb * c;
-#pragma unroll
-    for (int i = 0; i < LU_NB; ++i)
-      if (i < nb) out[i] = y[i];
+  }
+  __syncthreads();
+  // scratch layout: column-major nb x nb, ld = nb
+  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
+    const int i = q % nb, c = q / nb;
+    D[LU_NB * LU_NB + q] = yl[i * LU_NB + c];
+    D[2 * LU_NB * LU_NB + q] = yu[i * LU_NB + c];
   }
 }
 
