@@ -278,25 +278,18 @@ void assemble_range(nemoh_ctx* c, int s0, int s1) {
     dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)ninfd);
     rankine_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, N, o);
     LAUNCHED(c);
-    wave_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, N, o);
+    const unsigned wt = (N + WS_T - 1) / WS_T;
+    wave_sym_kernel<false><<<dim3(wt * (wt + 1) / 2, 1, (unsigned)ninfd), WS_THREADS, 0, c->stream>>>(g, dom, ds, rec,
+                                                                                                      N, o);
     LAUNCHED(c);
   }
   if (nfd) {
-    static bool attr = false;
-    if (!attr) {
-      CK(cudaFuncSetAttribute(fd_images_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, IMG_SMEM));
-      attr = true;
-    }
-    const unsigned nt = (N + IMG_T - 1) / IMG_T;
-    fd_images_kernel<<<dim3(nt, nt, (unsigned)nfd), IMG_THREADS, IMG_SMEM, c->stream>>>(g, dom, ds + ninfd, rec, rows,
-                                                                                      N, o);
-    LAUNCHED(c);
     dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
     rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
     LAUNCHED(c);
     const unsigned wt = (N + WS_T - 1) / WS_T;
-    wave_fd_sym_kernel<<<dim3(wt * (wt + 1) / 2, 1, (unsigned)nfd), WS_THREADS, 0, c->stream>>>(g, dom, ds + ninfd,
-                                                                                               rec, N, o);
+    wave_sym_kernel<true><<<dim3(wt * (wt + 1) / 2, 1, (unsigned)nfd), WS_THREADS, 0, c->stream>>>(
+        g, dom, ds + ninfd, rec, N, o);
     LAUNCHED(c);
   }
 }

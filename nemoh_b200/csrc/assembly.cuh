@@ -131,11 +131,10 @@ __global__ void crek_kernel(const double* __restrict__ xr, const double* __restr
 // dimension N): D+ then D- in out.d, S+ then S- in out.s (nsymy=0: one D and
 // one S). Column-major writes by consecutive rows are coalesced 16-byte
 // stores.
-//   rankine_kernel: Rankine part (VAVINFD / VAVFD; in finite depth added to the
-//                   exponential images of VNSFD that fd_images_kernel wrote)
-//                   -> real parts, imaginary = 0;
-//   wave_kernel:    wave part (VNSINFD / VNSFD) added to the real parts and
-//                   written to the imaginary parts.
+//   rankine_kernel: Rankine part (VAVINFD / VAVFD) -> real parts, imaginary = 0;
+//   wave_sym_kernel: wave part (VNSINFD / VNSFD; in finite depth with the
+//                   exponential images) added to the real parts and written to
+//                   the imaginary parts.
 // Splitting the pair evaluation keeps each kernel's registers and code small
 // enough for several CTAs per SM; the extra read of the matrices is 64 bytes
 // per pair and symmetry class pair.
@@ -171,141 +170,6 @@ __device__ __forceinline__ void stage_params(const OmegaParams* __restrict__ om,
   for (int i = threadIdx.x; i < (int)(sizeof(OmegaParams) / 8); i += blockDim.x) dst[i] = src[i];
 }
 
-// ---------------------------------------------------------------------------
-// Finite-depth exponential images (VNSFD, COMPUTE_GREEN_FD.f90:635-706) of
-// both ordered pairs of every unordered pair of submerged panels, written as
-// the real parts of D+/-, S+/- ahead of the Rankine pass, which adds its own
-// part to them. CTA = one 32 x 32 tile of the upper triangle (row tile <= column
-// tile); the results of the tile and of its transpose are staged in shared
-// memory so that both are stored column by column.
-// ---------------------------------------------------------------------------
-constexpr int IMG_T = 32;
-constexpr int IMG_THREADS = 256;
-constexpr int IMG_SMEM = 2 * IMG_T * IMG_T * (int)sizeof(double4);
-
-struct ImgTile {
-  double x[IMG_T], y[IMG_T], z[IMG_T], xn[IMG_T], yn[IMG_T], zn[IMG_T], act[IMG_T];
-};
-
-__device__ __forceinline__ void img_stage(const PanelRec* __restrict__ rec, const double* __restrict__ rows, int N,
-                                          int p0, int np, int t, ImgTile& T) {
-  if (t >= np) return;
-  const int J = p0 + t;
-  T.x[t] = rows[J];
-  T.y[t] = rows[N + J];
-  T.z[t] = rows[2 * N + J];
-  T.xn[t] = rows[3 * N + J];
-  T.yn[t] = rows[4 * N + J];
-  T.zn[t] = rows[5 * N + J];
-  T.act[t] = -0.5 * rec[J].aire / (4. * 3.141592653589793);
-}
-
-__global__ void __launch_bounds__(IMG_THREADS, 2) fd_images_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
-                                                                 const int* __restrict__ slots,
-                                                                 const PanelRec* __restrict__ rec,
-                                                                 const double* __restrict__ rows, int N, AsmOut out) {
-  const int ta = blockIdx.y, tb = blockIdx.x;
-  if (ta > tb) return;
-  extern __shared__ __align__(16) unsigned char img_dsm[];
-  double4* res = reinterpret_cast<double4*>(img_dsm);   // [0]: (A_i, B_j) at j*T+i; [1]: (B_j, A_i) at i*T+j
-  __shared__ ImgTile A, B;
-  __shared__ OmegaParams som;
-  const int slot = slots[blockIdx.z];
-  stage_params(oms + slot, &som);
-  const int a0 = ta * IMG_T, b0 = tb * IMG_T;
-  const int na = min(IMG_T, N - a0), nb = min(IMG_T, N - b0);
-  if (threadIdx.x < IMG_T) img_stage(rec, rows, N, a0, na, threadIdx.x, A);
-  else if (threadIdx.x < 2 * IMG_T) img_stage(rec, rows, N, b0, nb, threadIdx.x - IMG_T, B);
-  __syncthreads();
-  const bool diag = ta == tb;
-  const int NJJ = g.nsymy + 1;
-  auto live = [&](int i, int j) {
-    return i < na && j < nb && !(diag && i > j) && A.z[i] < g.zer && B.z[j] < g.zer;
-  };
-#pragma unroll 1
-  for (int q = threadIdx.x; q < IMG_T * IMG_T; q += IMG_THREADS) {
-    const int i = q % IMG_T, j = q / IMG_T;
-    double4 e1 = make_double4(0., 0., 0., 0.), e2 = e1;   // {dp, dm, sp, sm}
-    if (live(i, j)) {
-      ImageSums S;
-      fd_image_sums(g, som.h, som.ambda, som.ar, som.nexp + 1, A.x[i], A.y[i], A.z[i], B.x[j], B.y[j], B.z[j], NJJ,
-                    S);
-      double fs[2], vx[2], vy[2], vz[2];
-      // (I, J): collocation A_i, panel B_j
-      const double cj = B.act[j];
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        fs[b] = cj * S.fs[b];
-        vx[b] = -S.dx[b] * (cj * S.sa[b]);
-        vy[b] = -S.dy[b] * (cj * S.sa[b]);
-        vz[b] = -(cj * S.m1[b]);
-      }
-      if (NJJ == 2) {
-        e1.x = (vx[0] + vx[1]) * A.xn[i] + (vy[0] + vy[1]) * A.yn[i] + (vz[0] + vz[1]) * A.zn[i];
-        e1.y = (vx[0] - vx[1]) * A.xn[i] + (vy[0] - vy[1]) * A.yn[i] + (vz[0] - vz[1]) * A.zn[i];
-        e1.z = fs[0] + fs[1];
-        e1.w = fs[0] - fs[1];
-      } else {
-        e1.x = vx[0] * A.xn[i] + vy[0] * A.yn[i] + vz[0] * A.zn[i];
-        e1.z = fs[0];
-      }
-      // (J, I): collocation B_j, panel A_i; x distance and the direct y
-      // distance change sign, the mirror's y distance does not
-      const double ci = A.act[i];
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        fs[b] = ci * S.fs[b];
-        vx[b] = S.dx[b] * (ci * S.sa[b]);
-        vy[b] = (b ? -S.dy[b] : S.dy[b]) * (ci * S.sa[b]);
-        vz[b] = ci * S.m2[b];
-      }
-      if (NJJ == 2) {
-        e2.x = (vx[0] + vx[1]) * B.xn[j] + (vy[0] + vy[1]) * B.yn[j] + (vz[0] + vz[1]) * B.zn[j];
-        e2.y = (vx[0] - vx[1]) * B.xn[j] + (vy[0] - vy[1]) * B.yn[j] + (vz[0] - vz[1]) * B.zn[j];
-        e2.z = fs[0] + fs[1];
-        e2.w = fs[0] - fs[1];
-      } else {
-        e2.x = vx[0] * B.xn[j] + vy[0] * B.yn[j] + vz[0] * B.zn[j];
-        e2.z = fs[0];
-      }
-    }
-    res[j * IMG_T + i] = e1;
-    res[IMG_T * IMG_T + i * IMG_T + j] = e2;
-  }
-  __syncthreads();
-  const long long NN = (long long)N * N;
-  double2* od = out.d + slot * out.slot_stride;
-  double2* os = out.s + slot * out.slot_stride;
-  for (int q = threadIdx.x; q < IMG_T * IMG_T; q += IMG_THREADS) {
-    {   // entry (a0 + i, b0 + j), consecutive threads down a column
-      const int i = q % IMG_T, j = q / IMG_T;
-      if (live(i, j)) {
-        const double4 e = res[j * IMG_T + i];
-        const long long o = (a0 + i) + (long long)N * (b0 + j);
-        od[o] = make_double2(e.x, 0.);
-        os[o] = make_double2(e.z, 0.);
-        if (NJJ == 2) {
-          od[NN + o] = make_double2(e.y, 0.);
-          os[NN + o] = make_double2(e.w, 0.);
-        }
-      }
-    }
-    {   // entry (b0 + j, a0 + i); the diagonal of a diagonal tile is written above
-      const int j = q % IMG_T, i = q / IMG_T;
-      if (live(i, j) && !(diag && i == j)) {
-        const double4 e = res[IMG_T * IMG_T + i * IMG_T + j];
-        const long long o = (b0 + j) + (long long)N * (a0 + i);
-        od[o] = make_double2(e.x, 0.);
-        os[o] = make_double2(e.z, 0.);
-        if (NJJ == 2) {
-          od[NN + o] = make_double2(e.y, 0.);
-          os[NN + o] = make_double2(e.w, 0.);
-        }
-      }
-    }
-  }
-}
-
 template <bool FD>
 __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
                                                            const int* __restrict__ slots,
@@ -332,14 +196,6 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(Gre
     RealOut r;
     pair_rankine<FD>(g, som, som.ambda, som.ar, XGI, YGI, ZGI, XNI, YNI, ZNI, I == J, sp[jj], r);
     const long long q = I + (long long)N * J;
-    if (FD && ZGI < g.zer && sp[jj].zg < g.zer) {   // exponential images from fd_images_kernel
-      r.dp += od[q].x;
-      r.sp += os[q].x;
-      if (g.nsymy == 1) {
-        r.dm += od[NN + q].x;
-        r.sm += os[NN + q].x;
-      }
-    }
     od[q] = make_double2(r.dp, 0.);
     os[q] = make_double2(r.sp, 0.);
     if (g.nsymy == 1) {
@@ -350,11 +206,12 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(Gre
 }
 
 // ---------------------------------------------------------------------------
-// Finite-depth wave pass over the upper triangle of 16 x 16 tiles: a pair of
-// submerged panels is evaluated once for both orders (wave_fd_sym), any other
-// pair once per order (pair_wave); both the tile and its transpose are added
-// to the real parts and written to the imaginary parts, column by column
-// through shared memory.
+// Wave pass over the upper triangle of 16 x 16 tiles: a pair of submerged
+// panels is evaluated once for both orders (finite depth: wave_fd_sym and the
+// exponential images of the same branch, fd_images_pair; deep water:
+// wave_infd_both), any other pair once per order (pair_wave); both the tile
+// and its transpose are added to the real parts and written to the imaginary
+// parts, column by column through shared memory.
 // ---------------------------------------------------------------------------
 constexpr int WS_T = 16;
 constexpr int WS_THREADS = 128;
@@ -371,13 +228,76 @@ __device__ __forceinline__ void tri_tile(int t, int T, int& a, int& b) {
   b = r + (t - start(r));
 }
 
-// one order of a pair with a panel at the free surface (rare; kept out of line)
-__device__ __noinline__ void pair_wave_fd_ordered(const GreenCtx& g, const OmegaParams& om, const PanelRec& PC,
-                                                  const PanelRec& PS, PairOut& out) {
-  pair_wave<true>(g, om, PC.xg, PC.yg, PC.zg, PC.xn, PC.yn, PC.zn, PS, out);
+// Exponential images (VNSFD, COMPUTE_GREEN_FD.f90:635-706) of both orders of
+// a pair of submerged panels, added to the real parts of D+/-, S+/-.
+__device__ __forceinline__ void fd_images_pair(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
+                                               const PanelRec& PJ, int NJJ, bool both, PairOut& oij, PairOut& oji) {
+  ImageSums S;
+  fd_image_sums(g, om.h, om.ambda, om.ar, om.nexp + 1, PI.xg, PI.yg, PI.zg, PJ.xg, PJ.yg, PJ.zg, NJJ, S);
+  const double QPI = 4. * 3.141592653589793;
+#pragma unroll
+  for (int order = 0; order < 2; ++order) {
+    if (order == 1 && !both) break;
+    const bool tr = order == 1;
+    const PanelRec& C = tr ? PJ : PI;   // collocation panel
+    const double act = -0.5 * (tr ? PI.aire : PJ.aire) / QPI;
+    double fs[2], vx[2], vy[2], vz[2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      fs[b] = act * S.fs[b];
+      const double dx = tr ? -S.dx[b] : S.dx[b];
+      const double dy = (tr && b == 0) ? -S.dy[b] : S.dy[b];
+      vx[b] = -dx * (act * S.sa[b]);
+      vy[b] = -dy * (act * S.sa[b]);
+      vz[b] = tr ? act * S.m2[b] : -(act * S.m1[b]);
+    }
+    PairOut& o = tr ? oji : oij;
+    if (NJJ == 2) {
+      o.dp_re += (vx[0] + vx[1]) * C.xn + (vy[0] + vy[1]) * C.yn + (vz[0] + vz[1]) * C.zn;
+      o.dm_re += (vx[0] - vx[1]) * C.xn + (vy[0] - vy[1]) * C.yn + (vz[0] - vz[1]) * C.zn;
+      o.sp_re += fs[0] + fs[1];
+      o.sm_re += fs[0] - fs[1];
+    } else {
+      const double d = vx[0] * C.xn + vy[0] * C.yn + vz[0] * C.zn;
+      o.dp_re += d;
+      o.dm_re += d;
+      o.sp_re += fs[0];
+      o.sm_re += fs[0];
+    }
+  }
 }
 
-__global__ void __launch_bounds__(WS_THREADS, ASM_MINB_WAVE_FD) wave_fd_sym_kernel(
+// one order of a pair with a panel at the free surface (rare; kept out of line)
+template <bool FD>
+__device__ __noinline__ void pair_wave_ordered(const GreenCtx& g, const OmegaParams& om, const PanelRec& PC,
+                                               const PanelRec& PS, PairOut& out) {
+  pair_wave<FD>(g, om, PC.xg, PC.yg, PC.zg, PC.xn, PC.yn, PC.zn, PS, out);
+}
+
+// Deep water (VNSINFD, one image at ZI + ZJ): every sum is the same for both
+// orders except the horizontal gradient, whose x part and direct-reflection y
+// part change sign.
+__device__ __forceinline__ void wave_infd_both(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
+                                               const PanelRec& PJ, int NJJ, bool both, PairOut& oij, PairOut& oji) {
+  WaveJJ w[2];
+  wave_infd_pair(g, om, PI.xg, PI.yg, PI.zg, PJ, NJJ, w);
+  if (NJJ == 1) w[1] = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
+  wave_combine<false>(om, PJ.aire, NJJ, w, PI.xn, PI.yn, PI.zn, oij);
+  if (!both) return;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    w[b].VSX1 = -w[b].VSX1;
+    w[b].VSX2 = -w[b].VSX2;
+    if (b == 0) {
+      w[b].VSY1 = -w[b].VSY1;
+      w[b].VSY2 = -w[b].VSY2;
+    }
+  }
+  wave_combine<false>(om, PI.aire, NJJ, w, PJ.xn, PJ.yn, PJ.zn, oji);
+}
+
+template <bool FD>
+__global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_WAVE_INFD) wave_sym_kernel(
     GreenCtx g, const OmegaParams* __restrict__ oms, const int* __restrict__ slots, const PanelRec* __restrict__ rec,
     int N, AsmOut out) {
   __shared__ PairOut res[2][WS_T * WS_T];   // [0]: (A_i, B_j) at j*T+i; [1]: (B_j, A_i) at i*T+j
@@ -405,15 +325,20 @@ __global__ void __launch_bounds__(WS_THREADS, ASM_MINB_WAVE_FD) wave_fd_sym_kern
     const bool both = !(diag && i == j);
     if (PI.zg < g.zer && PJ.zg < g.zer) {
       PairOut oij, oji;
-      if (!wave_fd_sym(g, som, PI, PJ, NJJ, both, oij, oji)) {
-        set_status(g.status, ST_AKZ_UNDEFINED);
-        oij = oji = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
+      if (FD) {
+        if (!wave_fd_sym(g, som, PI, PJ, NJJ, both, oij, oji)) {
+          set_status(g.status, ST_AKZ_UNDEFINED);
+          oij = oji = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
+        }
+        fd_images_pair(g, som, PI, PJ, NJJ, both, oij, oji);
+      } else {
+        wave_infd_both(g, som, PI, PJ, NJJ, both, oij, oji);
       }
       res[0][j * WS_T + i] = oij;
       if (both) res[1][i * WS_T + j] = oji;
     } else {
-      pair_wave_fd_ordered(g, som, PI, PJ, res[0][j * WS_T + i]);
-      if (both) pair_wave_fd_ordered(g, som, PJ, PI, res[1][i * WS_T + j]);
+      pair_wave_ordered<FD>(g, som, PI, PJ, res[0][j * WS_T + i]);
+      if (both) pair_wave_ordered<FD>(g, som, PJ, PI, res[1][i * WS_T + j]);
     }
   }
   __syncthreads();
@@ -439,42 +364,6 @@ __global__ void __launch_bounds__(WS_THREADS, ASM_MINB_WAVE_FD) wave_fd_sym_kern
     {   // entry (b0 + j, a0 + i); the diagonal of a diagonal tile is done above
       const int j = q % WS_T, i = q / WS_T;
       if (live(i, j) && !(diag && i == j)) add((b0 + j) + (long long)N * (a0 + i), res[1][i * WS_T + j]);
-    }
-  }
-}
-
-template <bool FD>
-__global__ void __launch_bounds__(ASM_ROWS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_WAVE_INFD) wave_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
-                                                        const int* __restrict__ slots, const PanelRec* __restrict__ rec,
-                                                        const double* __restrict__ rows, int N, AsmOut out) {
-  __shared__ PanelRec sp[ASM_TJ];
-  __shared__ OmegaParams som;
-  const int slot = slots[blockIdx.z];
-  stage_params(oms + slot, &som);
-  const int j0 = blockIdx.y * ASM_TJ;
-  const int nj = min(ASM_TJ, N - j0);
-  stage_panels(rec, j0, nj, sp);
-  __syncthreads();
-  const int I = blockIdx.x * ASM_ROWS + threadIdx.x;
-  if (I >= N) return;
-  const double XGI = rows[I], YGI = rows[N + I], ZGI = rows[2 * N + I];
-  const double XNI = rows[3 * N + I], YNI = rows[4 * N + I], ZNI = rows[5 * N + I];
-  const long long NN = (long long)N * N;
-  double2* od = out.d + slot * out.slot_stride;
-  double2* os = out.s + slot * out.slot_stride;
-#pragma unroll 1
-  for (int jj = 0; jj < nj; ++jj) {
-    PairOut r;
-    pair_wave<FD>(g, som, XGI, YGI, ZGI, XNI, YNI, ZNI, sp[jj], r);
-    const long long q = I + (long long)N * (j0 + jj);
-    double2 d = od[q], s = os[q];
-    od[q] = make_double2(d.x + r.dp_re, r.dp_im);
-    os[q] = make_double2(s.x + r.sp_re, r.sp_im);
-    if (g.nsymy == 1) {
-      d = od[NN + q];
-      s = os[NN + q];
-      od[NN + q] = make_double2(d.x + r.dm_re, r.dm_im);
-      os[NN + q] = make_double2(s.x + r.sm_re, r.sm_im);
     }
   }
 }

@@ -825,9 +825,9 @@ __device__ __forceinline__ void fd_image_sums(const GreenCtx& g, double H, const
 }
 
 // --- Rankine part of one pair, both symmetry classes -------------------------
-// Real parts of D+/- and S+/- (the wave pass adds the rest). The exponential
-// images of the finite-depth submerged-panel branch come from fd_image_sums,
-// evaluated once per unordered pair by fd_images_kernel.
+// Real parts of D+/- and S+/- (the wave pass adds the rest, and in finite
+// depth the exponential images of the submerged-panel branch, fd_image_sums,
+// evaluated once per unordered pair).
 struct RealOut {
   double dp, dm, sp, sm;
 };
