@@ -296,6 +296,7 @@ void assemble_range(nemoh_ctx* c, int s0, int s1) {
 
 Batch dbatch(nemoh_ctx* c) {
   const long long NN = (long long)c->nfa * c->nfa;
+  // FP64 keeps the per-step row-strip updates (FP64 GEMM tiles beat the fused strip solve there)
   return Batch{c->d_D.as<double2>(), NN, c->nfa, c->d_diag.as<double2>()};
 }
 
@@ -1153,7 +1154,7 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
     const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
     lu_diag_kernel<double2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
-    lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k);
+    lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k, n);
     if (rest > 0) zgemm_update<double2>(b, k, nb, Rect{k + nb, n, k + nb, n}, nsys, st);
   }
   inv_diag_kernel<double2><<<dim3((unsigned)nblk, 1, nsys), TB, 2 * TB * TB * sizeof(double2), st>>>(b, inv,

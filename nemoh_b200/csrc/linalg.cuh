@@ -28,8 +28,12 @@ struct BatchT {
   long long stride;       // elements between systems
   int n;                  // order (leading dimension = n)
   C2* diag;               // DIAG_SCRATCH elements per system: factored A11, inv(L11), inv(U11)
+  C2* pinv = nullptr;     // optional, PINV_SCRATCH per system: inv(L) of the LU_OUTER / LU_NB
+                          // diagonal blocks of the current outer panel (two-level LU only)
 };
 constexpr int DIAG_SCRATCH = 3 * LU_NB * LU_NB;
+constexpr int LU_OUTER = 128;
+constexpr int PINV_SCRATCH = (LU_OUTER / LU_NB) * LU_NB * LU_NB;
 using Batch = BatchT<double2>;
 
 template <class C2> __device__ __forceinline__ C2 mkc(double x, double y);
@@ -128,10 +132,12 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* 
   }
   __syncthreads();
   // scratch layout: column-major nb x nb, ld = nb
+  C2* P = b.pinv ? b.pinv + (long long)blockIdx.z * PINV_SCRATCH + ((k % LU_OUTER) / LU_NB) * LU_NB * LU_NB : nullptr;
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
     const int i = q % nb, c = q / nb;
     D[LU_NB * LU_NB + q] = yl[i * LU_NB + c];
     D[2 * LU_NB * LU_NB + q] = yu[i * LU_NB + c];
+    if (P) P[q] = yl[i * LU_NB + c];
   }
 }
 
@@ -142,11 +148,12 @@ __device__ __forceinline__ void cmac(C2& acc, C2 a, C2 b) {
 }
 
 // L21 <- A21 inv(U11) (CTAs [0, nrb), one thread per row) and
-// U12 <- inv(L11) A12 (CTAs [nrb, nrb+ncb), one lane per row of a column), with the
+// U12 <- inv(L11) A12 for the columns [k + nb, ucol_end) (CTAs [nrb, nrb+ncb),
+// one lane per row of a column), with the
 // inverses from lu_diag_kernel; CTA 0 also stores the factored A11 into A
 // (no kernel of the step reads A11 from A). Launch with at least one CTA.
 template <class C2>
-__global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
+__global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k, int ucol_end) {
   __shared__ C2 inv[LU_NB * LU_NB];
   __shared__ C2 work[LU_NB * LU_CB];
   const int n = b.n;
@@ -180,7 +187,7 @@ __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k) {
   }
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) inv[q] = D[LU_NB * LU_NB + q];
   const int c0 = k + nb + (blockIdx.x - nrb) * LU_CB;
-  const int ncol = min(LU_CB, n - c0);
+  const int ncol = min(LU_CB, ucol_end - c0);
   for (int q = threadIdx.x; q < nb * ncol; q += blockDim.x) {
     const int i = q % nb, c = q / nb;
     work[i + nb * c] = A[(k + i) + (long long)n * (c0 + c)];
@@ -324,7 +331,72 @@ inline void zgemm_update(BatchT<C2> b, int k, int kb, Rect rc, int nsys, cudaStr
 // the rest of the trailing matrix is updated once per panel by `outer(k0,
 // kend)`, A[kend:, kend:] -= A[kend:, k0:kend] A[k0:kend, kend:], which cuts
 // the trailing matrix's read-modify-write traffic by LU_OUTER / LU_NB.
-constexpr int LU_OUTER = 128;
+// Row strip of an outer panel: U[k0:kend, kend:n] = inv(L11) A[k0:kend, kend:n]
+// with L11 the unit-lower part of the factored panel's diagonal block, by
+// blocks of LU_NB rows: X_j <- inv(L_jj) X_j (inverses from lu_diag, in
+// b.pinv), then X_i -= L_ij X_j for the blocks below. CTA = one system and
+// ST_C columns of the strip, held in shared memory (column-major, ld
+// LU_OUTER); thread = (row i of a block, every fourth column). Replaces the
+// per-step row-strip updates of the right-looking panel factorization, so the
+// strip is read and written once per outer panel.
+constexpr int ST_C = 32;
+template <class C2>
+constexpr int strip_smem() {
+  return (LU_OUTER * ST_C + LU_NB * LU_NB + LU_NB * ST_C) * (int)sizeof(C2);
+}
+template <class C2>
+__global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
+  extern __shared__ __align__(16) unsigned char strip_sm[];
+  C2* X = reinterpret_cast<C2*>(strip_sm);   // [ST_C][LU_OUTER]
+  C2* T = X + LU_OUTER * ST_C;              // [LU_NB][LU_NB] inv(L_jj) or L_ij, column-major
+  C2* Y = T + LU_NB * LU_NB;                // [ST_C][LU_NB]
+  const int n = b.n, kend = k0 + LU_OUTER;
+  const int c0 = kend + blockIdx.x * ST_C, ncol = min(ST_C, n - c0);
+  C2* A = b.base + blockIdx.z * b.stride;
+  const C2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
+  for (int q = threadIdx.x; q < LU_OUTER * ST_C; q += blockDim.x) {
+    const int r = q % LU_OUTER, c = q / LU_OUTER;
+    X[q] = c < ncol ? A[(k0 + r) + (long long)n * (c0 + c)] : mkc<C2>(0., 0.);
+  }
+  const int i = threadIdx.x & (LU_NB - 1), g = threadIdx.x / LU_NB;
+  constexpr int NBLK = LU_OUTER / LU_NB, GROUPS = 128 / LU_NB;
+  for (int jb = 0; jb < NBLK; ++jb) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) T[q] = P[jb * LU_NB * LU_NB + q];
+    __syncthreads();
+    // Y = inv(L_jj) X_j (unit diagonal)
+    for (int c = g; c < ST_C; c += GROUPS) {
+      const C2* x = X + c * LU_OUTER + jb * LU_NB;
+      C2 acc = x[i];
+      for (int j = 0; j < i; ++j) cmac(acc, T[i + LU_NB * j], x[j]);
+      Y[c * LU_NB + i] = acc;
+    }
+    __syncthreads();
+    for (int c = g; c < ST_C; c += GROUPS) {
+      const C2 v = Y[c * LU_NB + i];
+      X[c * LU_OUTER + jb * LU_NB + i] = v;
+      if (c < ncol) A[(k0 + jb * LU_NB + i) + (long long)n * (c0 + c)] = v;
+    }
+    // X_i -= L_ij X_j for the blocks below
+    for (int ib = jb + 1; ib < NBLK; ++ib) {
+      __syncthreads();
+      for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) {
+        const int r = q % LU_NB, cc = q / LU_NB;
+        T[q] = A[(k0 + ib * LU_NB + r) + (long long)n * (k0 + jb * LU_NB + cc)];
+      }
+      __syncthreads();
+      for (int c = g; c < ST_C; c += GROUPS) {
+        const C2* x = X + c * LU_OUTER + jb * LU_NB;
+        C2 acc = mkc<C2>(0., 0.);
+        for (int j = 0; j < LU_NB; ++j) cmac(acc, T[i + LU_NB * j], x[j]);
+        C2& y = X[c * LU_OUTER + ib * LU_NB + i];
+        y.x -= acc.x;
+        y.y -= acc.y;
+      }
+    }
+  }
+}
+
 template <class C2, class Outer>
 inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t st, long long& launches, Outer outer) {
   const int n = b.n;
@@ -332,19 +404,31 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t st, l
     const int kend = std::min(k0 + LU_OUTER, n);
     for (int k = k0; k < kend; k += LU_NB) {
       const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
-      const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
+      const int nrb = (rest + LU_RB - 1) / LU_RB;
+      // with b.pinv the row strip right of the panel waits for strip_kernel
+      const int ucol = b.pinv ? kend : n;
+      const int ncb_used = (std::max(0, ucol - k - nb) + LU_CB - 1) / LU_CB;
       lu_diag_kernel<C2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
       ++launches;
-      lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k);
+      lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb_used), 1, nsys), LU_RB, 0, st>>>(b, k, ucol);
       ++launches;
       if (k + nb < kend) {
         zgemm_update<C2>(b, k, nb, Rect{k + nb, n, k + nb, kend}, nsys, st);
         ++launches;
-        if (kend < n) {
+        if (kend < n && !b.pinv) {
           zgemm_update<C2>(b, k, nb, Rect{k + nb, kend, kend, n}, nsys, st);
           ++launches;
         }
       }
+    }
+    if (kend < n && b.pinv) {
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(strip_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_smem<C2>());
+        attr = true;
+      }
+      strip_kernel<C2><<<dim3((n - kend + ST_C - 1) / ST_C, 1, nsys), 128, strip_smem<C2>(), st>>>(b, k0);
+      ++launches;
     }
     if (kend < n) outer(k0, kend);
   }

@@ -46,9 +46,10 @@ struct MixedWork {
   float2* rf = nullptr;      // residual/correction (FP32)
   float2* yf = nullptr;      // forward-solve scratch (FP32)
   float2* inv = nullptr;     // inverses of the diagonal blocks of L and U (FP32)
+  float2* pinv = nullptr;    // inv(L) of the diagonal blocks of the current outer panel
   unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
   TcWork tc;                 // tensor-core GEMM operand buffers
-  size_t have[8] = {};       // bytes held by lu, diag, b, r, rf, yf, norms, inv
+  size_t have[9] = {};       // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv
   size_t total = 0;
   int last_iterations = 0;
   double last_residual = 0.;
@@ -57,8 +58,10 @@ struct MixedWork {
   size_t bytes() const { return total; }
   void release() {
     cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms); cudaFree(inv);
+    cudaFree(pinv);
     tc.release();
     lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr; inv = nullptr;
+    pinv = nullptr;
     for (size_t& h : have) h = 0;
     total = 0;
   }
@@ -69,17 +72,18 @@ struct MixedWork {
   // cudaFree synchronizes the whole device.
   cudaError_t ensure(int nsys, int n, int nrhs) {
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
-    const size_t need[8] = {nsys * NN * sizeof(float2),
+    const size_t need[9] = {nsys * NN * sizeof(float2),
                             (size_t)nsys * DIAG_SCRATCH * sizeof(float2),
                             V * sizeof(double2),
                             V * sizeof(double2),
                             V * sizeof(float2),
                             V * sizeof(float2),
                             (size_t)2 * nsys * nrhs * sizeof(unsigned long long),
-                            (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2)};
-    void** ptr[8] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
-                     (void**)&inv};
-    for (int i = 0; i < 8; ++i) {
+                            (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2),
+                            (size_t)nsys * PINV_SCRATCH * sizeof(float2)};
+    void** ptr[9] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
+                     (void**)&inv, (void**)&pinv};
+    for (int i = 0; i < 9; ++i) {
       if (need[i] <= have[i]) continue;
       cudaFree(*ptr[i]);
       *ptr[i] = nullptr;
@@ -98,7 +102,7 @@ struct MixedWork {
 
 inline size_t mixed_bytes_per_system(size_t n) {
   return n * n * sizeof(float2) + tc_bytes_per_system(n) + ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2) +
-         DIAG_SCRATCH * sizeof(float2);
+         (DIAG_SCRATCH + PINV_SCRATCH) * sizeof(float2);
 }
 
 __global__ void d2f_kernel(const double2* __restrict__ a, float2* __restrict__ b, long long count) {
@@ -152,7 +156,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   const long long total = (long long)nsys * n * n;
   d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
   ++launches;
-  BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
+  BatchT<float2> b{w.lu, (long long)n * n, n, w.diag, w.pinv};
   lu_two_level<float2>(b, nsys, status, st, launches, [&](int k0, int kend) {
     if (!tc_update(w.tc, b, k0, nsys, st, launches, status)) {
       zgemm_update<float2>(b, k0, kend - k0, Rect{kend, n, kend, n}, nsys, st);
