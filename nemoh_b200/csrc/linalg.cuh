@@ -62,22 +62,23 @@ __device__ __forceinline__ float2 cdv(float2 a, float2 b) {
 __device__ __forceinline__ double cabs2(double2 a) { return hypot(a.x, a.y); }
 __device__ __forceinline__ double cabs2(float2 a) { return hypotf(a.x, a.y); }
 
-// Factor the nb x nb block held column-major in shared memory (ld = nb).
+// Factor the nb x nb block held column-major in shared memory (ld = nb) with
+// one warp, lane = row: at step j each lane below the pivot forms its
+// multiplier and updates its row from the pivot row (a broadcast read), the
+// steps separated by __syncwarp. Unpivoted Doolittle, the operations of
+// GAUSSZ's elimination on this block.
 template <class C2>
-__device__ void factor_block(C2* s, int nb, int* status, bool report) {
+__device__ void factor_block_warp(C2* s, int nb, int* status) {
+  const int i = threadIdx.x & 31;
   for (int j = 0; j < nb; ++j) {
     const C2 piv = s[j + nb * j];
-    if (report && threadIdx.x == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-    __syncthreads();
-    // multipliers of column j
-    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) s[i + nb * j] = cdv(s[i + nb * j], piv);
-    __syncthreads();
-    const int m = nb - j - 1;
-    for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
-      const int i = j + 1 + q % m, c = j + 1 + q / m;
-      s[i + nb * c] = cfms(s[i + nb * c], s[i + nb * j], s[j + nb * c]);
+    if (i == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+    if (i > j && i < nb) {
+      const C2 m = cdv(s[i + nb * j], piv);
+      s[i + nb * j] = m;
+      for (int c = j + 1; c < nb; ++c) s[i + nb * c] = cfms(s[i + nb * c], m, s[j + nb * c]);
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -85,7 +86,7 @@ __device__ void factor_block(C2* s, int nb, int* status, bool report) {
 // and invert its triangles. Scratch per system: [LU(A11) | inv(L11) | inv(U11)],
 // column-major nb x nb each (ld = nb). One thread per column inverts.
 template <class C2>
-__global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
+__global__ void __launch_bounds__(64) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
   __shared__ C2 diag[LU_NB * LU_NB];
   __shared__ C2 ywork[2 * LU_NB * LU_NB];
   const int n = b.n;
@@ -96,7 +97,8 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(BatchT<C2> b, int k, int* 
     diag[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
   }
   __syncthreads();
-  factor_block(diag, nb, status, true);
+  if (threadIdx.x < 32) factor_block_warp(diag, nb, status);
+  __syncthreads();
   C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
   // One thread per column of each inverse; the columns being built live in
@@ -408,7 +410,7 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t st, l
       // with b.pinv the row strip right of the panel waits for strip_kernel
       const int ucol = b.pinv ? kend : n;
       const int ncb_used = (std::max(0, ucol - k - nb) + LU_CB - 1) / LU_CB;
-      lu_diag_kernel<C2><<<dim3(1, 1, nsys), 256, 0, st>>>(b, k, status);
+      lu_diag_kernel<C2><<<dim3(1, 1, nsys), 64, 0, st>>>(b, k, status);
       ++launches;
       lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb_used), 1, nsys), LU_RB, 0, st>>>(b, k, ucol);
       ++launches;
@@ -565,6 +567,15 @@ __global__ void __launch_bounds__(128) trsm_fused_kernel(BatchT<C2> b, const C2*
   C2* X = xbase + blockIdx.z * xstride;
   C2* Y = ybase + blockIdx.z * xstride;
   int nxt = blk;            // block solved by CTA 0 at the end
+  // CTA 0 starts copying the inverse of the block it will solve while it
+  // still applies the previous block
+  const int solve_blk = apply ? (LOWER ? blk + 1 : blk - 1) : blk;
+  const bool solver = blockIdx.x == 0 && solve_blk >= 0 && solve_blk < nblk;
+  if (solver) {
+    const C2* src = inv + ((long long)(blockIdx.z * nblk + solve_blk) * 2 + (LOWER ? 0 : 1)) * TB * TB;
+    for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) cp_async_elem(Ti + q, src + q, true);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   if (apply) {
     const int k = blk * TB, nb = min(TB, n - k);
     for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
@@ -615,8 +626,7 @@ __global__ void __launch_bounds__(128) trsm_fused_kernel(BatchT<C2> b, const C2*
   }
   // CTA 0: solve block nxt from Xn (rows beyond n are zero)
   const int kn = nxt * TB, nbn = min(TB, n - kn);
-  const C2* src = inv + ((long long)(blockIdx.z * nblk + nxt) * 2 + (LOWER ? 0 : 1)) * TB * TB;
-  for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) Ti[q] = src[q];
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (apply)
     for (int q = threadIdx.x; q < TB * nrhs; q += blockDim.x) {
       const int i = q % TB, p = q / TB;
