@@ -97,6 +97,7 @@ struct nemoh_ctx {
   HostBuf h_oms, h_slots;
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
+  Lanes lanes;               // side streams for groups of systems in the LU and triangular solves
   int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
   double w_previous = -1.;   // factor cache key of solve_problem
   int cached_fd = 0, cached_nexp = 0;
@@ -309,19 +310,22 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
                             zgemm_smem<double2>()));
     attr = true;
   }
-  lu_two_level<double2>(b, nsys, c->d_status.as<int>(), c->stream, c->launches, [&](int k0, int kend) {
-    zgemm_update<double2>(b, k0, kend - k0, Rect{kend, N, kend, N}, nsys, c->stream);
-    ++c->launches;
-  });
+  lu_two_level<double2>(
+      b, nsys, c->d_status.as<int>(), c->stream, c->launches,
+      [&](Batch bg, int ns, cudaStream_t sg, int, int k0, int kend) {
+        zgemm_update<double2>(bg, k0, kend - k0, Rect{kend, N, kend, N}, ns, sg);
+        ++c->launches;
+      },
+      &c->lanes);
   CK(cudaGetLastError());
   static bool attr2 = false;
   if (!attr2) {
     CK(cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            2 * TB * TB * (int)sizeof(double2)));
+                            inv_diag_smem<double2>()));
     attr2 = true;
   }
   const int nblk = (N + TB - 1) / TB;
-  inv_diag_kernel<double2><<<dim3(nblk, 1, nsys), TB, 2 * TB * TB * sizeof(double2), c->stream>>>(
+  inv_diag_kernel<double2><<<dim3(nblk, 1, nsys), INV_THREADS, inv_diag_smem<double2>(), c->stream>>>(
       b, c->d_inv.as<double2>(), nblk);
   LAUNCHED(c);
 }
@@ -329,7 +333,7 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
 // solve the factored systems for the right-hand sides in X (result in X)
 void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
   trsm_launch<double2>(dbatch(c), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys, nrhs,
-                       c->stream, c->launches);
+                       c->stream, c->launches, &c->lanes);
   CK(cudaGetLastError());
 }
 
@@ -342,7 +346,7 @@ void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
 void mixed_solve(nemoh_ctx* c, int nsys, int nrhs) {
   MixedWork& w = c->mixed;
   mixed_solve_refine(w, c->d_D.as<double2>(), c->nfa, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(), nrhs,
-                     c->stream, c->launches);
+                     c->stream, c->launches, &c->lanes);
   CK(cudaGetLastError());
   if (w.last_residual <= REFINE_TOL) return;
   const size_t N = c->nfa;
@@ -358,7 +362,8 @@ void mixed_solve(nemoh_ctx* c, int nsys, int nrhs) {
 void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs) {
   c->lu64 = c->mode == NEMOH_B200_FP64;
   if (c->mode == NEMOH_B200_MIXED) {
-    mixed_factor(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_status.as<int>(), c->stream, c->launches);
+    mixed_factor(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_status.as<int>(), c->stream, c->launches,
+                 &c->lanes);
     CK(cudaGetLastError());
     if (have_rhs) mixed_solve(c, nsys, nrhs);
   } else {
@@ -460,6 +465,11 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
   int st = guarded(c, [&] {
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) CK(cudaEventCreate(&e));
+    for (int g = 0; g < LANES; ++g) {
+      CK(cudaStreamCreateWithFlags(&c->lanes.s[g], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->lanes.join[g], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&c->lanes.fork, cudaEventDisableTiming));
     CK(c->d_status.ensure(sizeof(int)));
     CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
     CK(c->d_gm.ensure(sizeof(unsigned long long)));
@@ -522,8 +532,15 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
   if (!c) return NEMOH_B200_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int g = 0; g < LANES; ++g)
+    if (c->lanes.s[g]) cudaStreamSynchronize(c->lanes.s[g]);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (int g = 0; g < LANES; ++g) {
+    if (c->lanes.join[g]) cudaEventDestroy(c->lanes.join[g]);
+    if (c->lanes.s[g]) cudaStreamDestroy(c->lanes.s[g]);
+  }
+  if (c->lanes.fork) cudaEventDestroy(c->lanes.fork);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NEMOH_B200_OK;
@@ -1125,7 +1142,7 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
           cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                zgemm_smem<double2>()),
           cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               2 * TB * TB * (int)sizeof(double2)),
+                               inv_diag_smem<double2>()),
           cudaFuncSetAttribute(trsm_fused_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                trsm_smem),
           cudaFuncSetAttribute(trsm_fused_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1153,11 +1170,11 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
   for (int k = 0; k < n; k += LU_NB) {
     const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-    lu_diag_kernel<double2><<<dim3(1, 1, nsys), 64, 0, st>>>(b, k, status);
+    lu_diag_kernel<double2><<<dim3(1, 1, nsys), LU_NB * LU_NB, 0, st>>>(b, k, status);
     lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k, n);
     if (rest > 0) zgemm_update<double2>(b, k, nb, Rect{k + nb, n, k + nb, n}, nsys, st);
   }
-  inv_diag_kernel<double2><<<dim3((unsigned)nblk, 1, nsys), TB, 2 * TB * TB * sizeof(double2), st>>>(b, inv,
+  inv_diag_kernel<double2><<<dim3((unsigned)nblk, 1, nsys), INV_THREADS, inv_diag_smem<double2>(), st>>>(b, inv,
                                                                                                       (int)nblk);
   long long launches = 0;
   trsm_launch<double2>(b, inv, reinterpret_cast<double2*>(x_device), y, nsys, nrhs, st, launches);

@@ -62,84 +62,60 @@ __device__ __forceinline__ float2 cdv(float2 a, float2 b) {
 __device__ __forceinline__ double cabs2(double2 a) { return hypot(a.x, a.y); }
 __device__ __forceinline__ double cabs2(float2 a) { return hypotf(a.x, a.y); }
 
-// Factor the nb x nb block held column-major in shared memory (ld = nb) with
-// one warp, lane = row: at step j each lane below the pivot forms its
-// multiplier and updates its row from the pivot row (a broadcast read), the
-// steps separated by __syncwarp. Unpivoted Doolittle, the operations of
-// GAUSSZ's elimination on this block.
-template <class C2>
-__device__ void factor_block_warp(C2* s, int nb, int* status) {
-  const int i = threadIdx.x & 31;
-  for (int j = 0; j < nb; ++j) {
-    const C2 piv = s[j + nb * j];
-    if (i == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-    if (i > j && i < nb) {
-      const C2 m = cdv(s[i + nb * j], piv);
-      s[i + nb * j] = m;
-      for (int c = j + 1; c < nb; ++c) s[i + nb * c] = cfms(s[i + nb * c], m, s[j + nb * c]);
-    }
-    __syncwarp();
-  }
-}
-
 // Factor the diagonal block A11 of step k once per system (grid.z = system)
 // and invert its triangles. Scratch per system: [LU(A11) | inv(L11) | inv(U11)],
-// column-major nb x nb each (ld = nb). One thread per column inverts.
+// column-major nb x nb each (ld = nb). One thread per element of the 32 x 32
+// block, every step of the three eliminations separated by a barrier:
+//  * unpivoted Doolittle (GAUSSZ's elimination on this block): at step j the
+//    column below the pivot is divided by it, then the trailing block takes
+//    the rank-1 update;
+//  * inv(L): X = I, step j (ascending) subtracts L(i, j) X(j, :) from the rows
+//    below, the order of the column-by-column forward substitution;
+//  * inv(U): X = I, step j (descending) divides row j by U(j, j) and
+//    subtracts U(i, j) X(j, :) from the rows above.
+// With b.pinv (two-level LU) inv(L) also goes to the slot of this block in the
+// current outer panel.
 template <class C2>
-__global__ void __launch_bounds__(64) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
-  __shared__ C2 diag[LU_NB * LU_NB];
-  __shared__ C2 ywork[2 * LU_NB * LU_NB];
+__global__ void __launch_bounds__(1024) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
+  __shared__ C2 sb[LU_NB * LU_NB];   // the block, column-major, ld = nb
+  __shared__ C2 xl[LU_NB * LU_NB];   // inv(L11), ld = LU_NB
+  __shared__ C2 xu[LU_NB * LU_NB];   // inv(U11), ld = LU_NB
   const int n = b.n;
   const int nb = min(LU_NB, n - k);
+  const int i = threadIdx.x & (LU_NB - 1), c = threadIdx.x / LU_NB;
+  const bool in = i < nb && c < nb;
   const C2* A = b.base + blockIdx.z * b.stride;
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
-    const int i = q % nb, c = q / nb;
-    diag[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
+  if (in) sb[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    if (threadIdx.x == 0 && !(cabs2(sb[j + nb * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+    if (in && c == j && i > j) sb[i + nb * j] = cdv(sb[i + nb * j], sb[j + nb * j]);
+    __syncthreads();
+    if (in && i > j && c > j) sb[i + nb * c] = cfms(sb[i + nb * c], sb[i + nb * j], sb[j + nb * c]);
+    __syncthreads();
+  }
+  const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
+  if (in) {
+    xl[i + LU_NB * c] = i == c ? one : zero;
+    xu[i + LU_NB * c] = i == c ? one : zero;
   }
   __syncthreads();
-  if (threadIdx.x < 32) factor_block_warp(diag, nb, status);
-  __syncthreads();
+  for (int step = 0; step < nb; ++step) {
+    const int jl = step, ju = nb - 1 - step;
+    if (in && i == ju && c >= ju) xu[ju + LU_NB * c] = cdv(xu[ju + LU_NB * c], sb[ju + nb * ju]);
+    __syncthreads();
+    if (in && i > jl && c <= jl) xl[i + LU_NB * c] = cfms(xl[i + LU_NB * c], sb[i + nb * jl], xl[jl + LU_NB * c]);
+    if (in && i < ju && c >= ju) xu[i + LU_NB * c] = cfms(xu[i + LU_NB * c], sb[i + nb * ju], xu[ju + LU_NB * c]);
+    __syncthreads();
+  }
   C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) D[q] = diag[q];
-  // One thread per column of each inverse; the columns being built live in
-  // shared memory (column t of a triangle at y[i * LU_NB + t], so the 32
-  // threads of a warp touch 32 consecutive elements), then go out in one
-  // coalesced store.
-  C2* yl = ywork;                    // inv(L11)
-  C2* yu = ywork + LU_NB * LU_NB;    // inv(U11)
-  const int t = threadIdx.x;
-  if (t < nb) {
-    // column t of inv(L11): unit lower, forward substitution
-    for (int i = 0; i < nb; ++i) {
-      C2 v = mkc<C2>(i == t ? 1. : 0., 0.);
-      if (i > t)
-        for (int j = t; j < i; ++j) v = cfms(v, diag[i + nb * j], yl[j * LU_NB + t]);
-      else if (i < t)
-        v = mkc<C2>(0., 0.);
-      yl[i * LU_NB + t] = v;
-    }
-  } else if (t >= 32 && t < 32 + nb) {
-    // column c of inv(U11): upper, back substitution
-    const int c = t - 32;
-    for (int i = nb - 1; i >= 0; --i) {
-      C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
-      if (i <= c) {
-        for (int j = i + 1; j <= c; ++j) v = cfms(v, diag[i + nb * j], yu[j * LU_NB + c]);
-        v = cdv(v, diag[i + nb * i]);
-      } else {
-        v = mkc<C2>(0., 0.);
-      }
-      yu[i * LU_NB + c] = v;
-    }
-  }
-  __syncthreads();
-  // scratch layout: column-major nb x nb, ld = nb
   C2* P = b.pinv ? b.pinv + (long long)blockIdx.z * PINV_SCRATCH + ((k % LU_OUTER) / LU_NB) * LU_NB * LU_NB : nullptr;
-  for (int q = threadIdx.x; q < nb * nb; q += blockDim.x) {
-    const int i = q % nb, c = q / nb;
-    D[LU_NB * LU_NB + q] = yl[i * LU_NB + c];
-    D[2 * LU_NB * LU_NB + q] = yu[i * LU_NB + c];
-    if (P) P[q] = yl[i * LU_NB + c];
+  if (in) {
+    const int q = i + nb * c;
+    D[q] = sb[q];
+    D[LU_NB * LU_NB + q] = xl[i + LU_NB * c];
+    D[2 * LU_NB * LU_NB + q] = xu[i + LU_NB * c];
+    if (P) P[q] = xl[i + LU_NB * c];
   }
 }
 
@@ -366,12 +342,21 @@ __global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
     __syncthreads();
     for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) T[q] = P[jb * LU_NB * LU_NB + q];
     __syncthreads();
-    // Y = inv(L_jj) X_j (unit diagonal)
-    for (int c = g; c < ST_C; c += GROUPS) {
-      const C2* x = X + c * LU_OUTER + jb * LU_NB;
-      C2 acc = x[i];
-      for (int j = 0; j < i; ++j) cmac(acc, T[i + LU_NB * j], x[j]);
-      Y[c * LU_NB + i] = acc;
+    // Y = inv(L_jj) X_j (unit diagonal); each inverse entry is read once and
+    // applied to the thread's ST_C / GROUPS columns
+    {
+      constexpr int CPT = ST_C / GROUPS;
+      C2 acc[CPT];
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) acc[m] = X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + i];
+      for (int j = 0; j < LU_NB; ++j) {
+        if (j >= i) break;
+        const C2 t = T[i + LU_NB * j];
+#pragma unroll
+        for (int m = 0; m < CPT; ++m) cmac(acc[m], t, X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + j]);
+      }
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) Y[(g + GROUPS * m) * LU_NB + i] = acc[m];
     }
     __syncthreads();
     for (int c = g; c < ST_C; c += GROUPS) {
@@ -387,21 +372,84 @@ __global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
         T[q] = A[(k0 + ib * LU_NB + r) + (long long)n * (k0 + jb * LU_NB + cc)];
       }
       __syncthreads();
-      for (int c = g; c < ST_C; c += GROUPS) {
-        const C2* x = X + c * LU_OUTER + jb * LU_NB;
-        C2 acc = mkc<C2>(0., 0.);
-        for (int j = 0; j < LU_NB; ++j) cmac(acc, T[i + LU_NB * j], x[j]);
-        C2& y = X[c * LU_OUTER + ib * LU_NB + i];
-        y.x -= acc.x;
-        y.y -= acc.y;
+      constexpr int CPT = ST_C / GROUPS;
+      C2 acc[CPT];
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
+      for (int j = 0; j < LU_NB; ++j) {
+        const C2 t = T[i + LU_NB * j];
+#pragma unroll
+        for (int m = 0; m < CPT; ++m) cmac(acc[m], t, X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + j]);
+      }
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        C2& y = X[(g + GROUPS * m) * LU_OUTER + ib * LU_NB + i];
+        y.x -= acc[m].x;
+        y.y -= acc[m].y;
       }
     }
   }
 }
 
+// Systems split into groups factored side by side on separate streams: the
+// launches of a step are issued group after group, so the latency-bound
+// kernels of one group (diagonal blocks, panels, small updates) overlap the
+// work of the other. Without lanes (or with one system) everything runs on
+// the caller's stream.
+constexpr int LANES = 2;
+struct Lanes {
+  cudaStream_t s[LANES] = {};
+  cudaEvent_t fork = nullptr, join[LANES] = {};
+};
+
+struct LaneSplit {
+  int groups = 1;
+  int first[LANES + 1] = {};
+  cudaStream_t st[LANES] = {};
+};
+
+inline LaneSplit lane_split(int nsys, cudaStream_t main, const Lanes* lanes) {
+  LaneSplit L;
+  if (!lanes || !lanes->s[0] || nsys < 2) {
+    L.groups = 1;
+    L.first[0] = 0;
+    L.first[1] = nsys;
+    L.st[0] = main;
+    return L;
+  }
+  L.groups = LANES;
+  for (int g = 0; g <= LANES; ++g) L.first[g] = (int)((long long)nsys * g / LANES);
+  cudaEventRecord(lanes->fork, main);
+  for (int g = 0; g < LANES; ++g) {
+    L.st[g] = lanes->s[g];
+    cudaStreamWaitEvent(lanes->s[g], lanes->fork, 0);
+  }
+  return L;
+}
+
+inline void lane_join(const LaneSplit& L, cudaStream_t main, const Lanes* lanes) {
+  if (L.groups == 1) return;
+  for (int g = 0; g < L.groups; ++g) {
+    cudaEventRecord(lanes->join[g], L.st[g]);
+    cudaStreamWaitEvent(main, lanes->join[g], 0);
+  }
+}
+
+template <class C2>
+inline BatchT<C2> sub_batch(const BatchT<C2>& b, int s0) {
+  BatchT<C2> r = b;
+  r.base = b.base + s0 * b.stride;
+  r.diag = b.diag + (long long)s0 * DIAG_SCRATCH;
+  if (b.pinv) r.pinv = b.pinv + (long long)s0 * PINV_SCRATCH;
+  return r;
+}
+
+// outer(bsub, nsub, stream, s0, k0, kend): trailing update of one group
 template <class C2, class Outer>
-inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t st, long long& launches, Outer outer) {
+inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main, long long& launches, Outer outer,
+                         const Lanes* lanes = nullptr) {
   const int n = b.n;
+  const LaneSplit L = lane_split(nsys, main, lanes);
   for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
     const int kend = std::min(k0 + LU_OUTER, n);
     for (int k = k0; k < kend; k += LU_NB) {
@@ -410,30 +458,41 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t st, l
       // with b.pinv the row strip right of the panel waits for strip_kernel
       const int ucol = b.pinv ? kend : n;
       const int ncb_used = (std::max(0, ucol - k - nb) + LU_CB - 1) / LU_CB;
-      lu_diag_kernel<C2><<<dim3(1, 1, nsys), 64, 0, st>>>(b, k, status);
-      ++launches;
-      lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb_used), 1, nsys), LU_RB, 0, st>>>(b, k, ucol);
-      ++launches;
-      if (k + nb < kend) {
-        zgemm_update<C2>(b, k, nb, Rect{k + nb, n, k + nb, kend}, nsys, st);
+      for (int g = 0; g < L.groups; ++g) {
+        const int s0 = L.first[g], ns = L.first[g + 1] - s0;
+        const BatchT<C2> bg = sub_batch(b, s0);
+        const cudaStream_t st = L.st[g];
+        lu_diag_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, 0, st>>>(bg, k, status);
         ++launches;
-        if (kend < n && !b.pinv) {
-          zgemm_update<C2>(b, k, nb, Rect{k + nb, kend, kend, n}, nsys, st);
+        lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb_used), 1, ns), LU_RB, 0, st>>>(bg, k, ucol);
+        ++launches;
+        if (k + nb < kend) {
+          zgemm_update<C2>(bg, k, nb, Rect{k + nb, n, k + nb, kend}, ns, st);
           ++launches;
+          if (kend < n && !b.pinv) {
+            zgemm_update<C2>(bg, k, nb, Rect{k + nb, kend, kend, n}, ns, st);
+            ++launches;
+          }
         }
       }
     }
-    if (kend < n && b.pinv) {
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(strip_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_smem<C2>());
-        attr = true;
+    for (int g = 0; g < L.groups; ++g) {
+      const int s0 = L.first[g], ns = L.first[g + 1] - s0;
+      const BatchT<C2> bg = sub_batch(b, s0);
+      const cudaStream_t st = L.st[g];
+      if (kend < n && b.pinv) {
+        static bool attr = false;
+        if (!attr) {
+          cudaFuncSetAttribute(strip_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_smem<C2>());
+          attr = true;
+        }
+        strip_kernel<C2><<<dim3((n - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
+        ++launches;
       }
-      strip_kernel<C2><<<dim3((n - kend + ST_C - 1) / ST_C, 1, nsys), 128, strip_smem<C2>(), st>>>(b, k0);
-      ++launches;
+      if (kend < n) outer(bg, ns, st, s0, k0, kend);
     }
-    if (kend < n) outer(k0, kend);
   }
+  lane_join(L, main, lanes);
 }
 
 constexpr int MAX_RHS = 16;
@@ -509,44 +568,59 @@ __device__ __forceinline__ void cmad(C2& acc, C2 a, C2 b) {
   acc.y += a.x * b.y + a.y * b.x;
 }
 
-// inv layout: ((sys * nblk + blk) * 2 + {0: inv L, 1: inv U}) * TB * TB, column-major
+// inv layout: ((sys * nblk + blk) * 2 + {0: inv L, 1: inv U}) * TB * TB, column-major.
+// Inverses of the unit-lower and upper triangles of the TB x TB diagonal
+// blocks (a partial last block is padded with the identity): 1024 threads, each
+// owning row i of four columns, one barrier per elimination step. inv(L):
+// X = I, step j (ascending) subtracts L(i, j) X(j, :) from the rows below
+// (the order of the column-by-column forward substitution); inv(U): X = I, step
+// j (descending) divides row j by U(j, j), then subtracts U(i, j) X(j, :) from
+// the rows above.
+constexpr int INV_THREADS = 1024;
 template <class C2>
-__global__ void __launch_bounds__(TB) inv_diag_kernel(BatchT<C2> b, C2* __restrict__ inv, int nblk) {
+constexpr int inv_diag_smem() {
+  return 3 * TB * TB * (int)sizeof(C2);
+}
+template <class C2>
+__global__ void __launch_bounds__(INV_THREADS) inv_diag_kernel(BatchT<C2> b, C2* __restrict__ inv, int nblk) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  C2* T = reinterpret_cast<C2*>(dsm);   // [TB][TB]
-  C2* W = T + TB * TB;                  // work columns [TB][TB]
+  C2* T = reinterpret_cast<C2*>(dsm);   // [TB][TB] the block
+  C2* XL = T + TB * TB;                 // inv(L)
+  C2* XU = XL + TB * TB;                // inv(U)
   const int n = b.n, blk = blockIdx.x, k = blk * TB, nb = min(TB, n - k);
   const C2* A = b.base + blockIdx.z * b.stride;
+  const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
   for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) {
     const int i = q % TB, c = q / TB;
-    T[q] = (i < nb && c < nb) ? A[(k + i) + (long long)n * (k + c)] : mkc<C2>(i == c ? 1. : 0., 0.);
+    T[q] = (i < nb && c < nb) ? A[(k + i) + (long long)n * (k + c)] : (i == c ? one : zero);
+    XL[q] = i == c ? one : zero;
+    XU[q] = i == c ? one : zero;
   }
   __syncthreads();
-  const int c = threadIdx.x;
-  C2* out = inv + ((long long)(blockIdx.z * nblk + blk) * 2) * TB * TB;
-  // inv(L): unit lower, column c
-  C2* y = W + TB * c;
-  for (int i = 0; i < TB; ++i) {
-    C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
-    if (i > c)
-      for (int j = c; j < i; ++j) v = cfms(v, T[i + TB * j], y[j]);
-    else if (i < c)
-      v = mkc<C2>(0., 0.);
-    y[i] = v;
-  }
-  for (int i = 0; i < TB; ++i) out[i + TB * c] = y[i];
-  // inv(U): upper, column c
-  for (int i = TB - 1; i >= 0; --i) {
-    C2 v = mkc<C2>(i == c ? 1. : 0., 0.);
-    if (i <= c) {
-      for (int j = i + 1; j <= c; ++j) v = cfms(v, T[i + TB * j], y[j]);
-      v = cdv(v, T[i + TB * i]);
-    } else {
-      v = mkc<C2>(0., 0.);
+  constexpr int CG = INV_THREADS / TB;   // column groups: columns cq + CG m
+  const int i = threadIdx.x % TB, cq = threadIdx.x / TB;
+  for (int step = 0; step < TB; ++step) {
+    const int jl = step, ju = TB - 1 - step;
+    if (i == ju)
+#pragma unroll
+      for (int m = 0; m < TB / CG; ++m) {
+        const int c = cq + CG * m;
+        if (c >= ju) XU[ju + TB * c] = cdv(XU[ju + TB * c], T[ju + TB * ju]);
+      }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < TB / CG; ++m) {
+      const int c = cq + CG * m;
+      if (i > jl && c <= jl) XL[i + TB * c] = cfms(XL[i + TB * c], T[i + TB * jl], XL[jl + TB * c]);
+      if (i < ju && c >= ju) XU[i + TB * c] = cfms(XU[i + TB * c], T[i + TB * ju], XU[ju + TB * c]);
     }
-    y[i] = v;
+    __syncthreads();
   }
-  for (int i = 0; i < TB; ++i) out[TB * TB + i + TB * c] = y[i];
+  C2* out = inv + ((long long)(blockIdx.z * nblk + blk) * 2) * TB * TB;
+  for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) {
+    out[q] = XL[q];
+    out[TB * TB + q] = XU[q];
+  }
 }
 
 // Triangular solves, one launch per diagonal block. X holds the running
@@ -644,7 +718,8 @@ __global__ void __launch_bounds__(128) trsm_fused_kernel(BatchT<C2> b, const C2*
 // Forward then backward solve of the factored systems: X holds the right-hand
 // sides and receives the solution, Y is scratch of the same size.
 template <class C2>
-void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st, long long& launches) {
+void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t main, long long& launches,
+                 const Lanes* lanes = nullptr) {
   const int N = b.n;
   const long long xs = (long long)N * nrhs;
   const int nblk = (N + TB - 1) / TB;
@@ -655,22 +730,40 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
     cudaFuncSetAttribute(trsm_fused_kernel<C2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr = true;
   }
+  const LaneSplit L = lane_split(nsys, main, lanes);
+  auto each = [&](auto launch) {
+    for (int g = 0; g < L.groups; ++g) {
+      const int s0 = L.first[g], ns = L.first[g + 1] - s0;
+      BatchT<C2> bg = b;
+      bg.base = b.base + s0 * b.stride;
+      launch(bg, inv + (long long)s0 * nblk * 2 * TB * TB, X + s0 * xs, Y + s0 * xs, ns, L.st[g]);
+    }
+  };
   // forward: X -> Y
-  trsm_fused_kernel<C2, true><<<dim3(1, 1, nsys), 128, smem, st>>>(b, inv, nblk, X, Y, xs, nrhs, 0, 0);
-  ++launches;
+  each([&](BatchT<C2> bg, const C2* ig, C2* xg, C2* yg, int ns, cudaStream_t st) {
+    trsm_fused_kernel<C2, true><<<dim3(1, 1, ns), 128, smem, st>>>(bg, ig, nblk, xg, yg, xs, nrhs, 0, 0);
+    ++launches;
+  });
   for (int blk = 0; blk + 1 < nblk; ++blk) {
     const int below = N - std::min(N, (blk + 1) * TB);
-    trsm_fused_kernel<C2, true><<<dim3(std::max(1, (below + TB - 1) / TB), 1, nsys), 128, smem, st>>>(
-        b, inv, nblk, X, Y, xs, nrhs, blk, 1);
-    ++launches;
+    each([&](BatchT<C2> bg, const C2* ig, C2* xg, C2* yg, int ns, cudaStream_t st) {
+      trsm_fused_kernel<C2, true><<<dim3(std::max(1, (below + TB - 1) / TB), 1, ns), 128, smem, st>>>(
+          bg, ig, nblk, xg, yg, xs, nrhs, blk, 1);
+      ++launches;
+    });
   }
   // backward: Y -> X
-  trsm_fused_kernel<C2, false><<<dim3(1, 1, nsys), 128, smem, st>>>(b, inv, nblk, Y, X, xs, nrhs, nblk - 1, 0);
-  ++launches;
-  for (int blk = nblk - 1; blk >= 1; --blk) {
-    trsm_fused_kernel<C2, false><<<dim3(blk, 1, nsys), 128, smem, st>>>(b, inv, nblk, Y, X, xs, nrhs, blk, 1);
+  each([&](BatchT<C2> bg, const C2* ig, C2* xg, C2* yg, int ns, cudaStream_t st) {
+    trsm_fused_kernel<C2, false><<<dim3(1, 1, ns), 128, smem, st>>>(bg, ig, nblk, yg, xg, xs, nrhs, nblk - 1, 0);
     ++launches;
+  });
+  for (int blk = nblk - 1; blk >= 1; --blk) {
+    each([&](BatchT<C2> bg, const C2* ig, C2* xg, C2* yg, int ns, cudaStream_t st) {
+      trsm_fused_kernel<C2, false><<<dim3(blk, 1, ns), 128, smem, st>>>(bg, ig, nblk, yg, xg, xs, nrhs, blk, 1);
+      ++launches;
+    });
   }
+  lane_join(L, main, lanes);
 }
 
 // Y += sign * M X (FP64) with the columns split over blockIdx.y; partial sums

@@ -152,37 +152,46 @@ __global__ void residual_finish_kernel(const double2* __restrict__ r, float2* __
   if ((threadIdx.x & 31) == 0) atomicMax(rnorm + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
-inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches) {
+inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches,
+                         const Lanes* lanes = nullptr) {
   const long long total = (long long)nsys * n * n;
   d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
   ++launches;
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag, w.pinv};
-  lu_two_level<float2>(b, nsys, status, st, launches, [&](int k0, int kend) {
-    if (!tc_update(w.tc, b, k0, nsys, st, launches, status)) {
-      zgemm_update<float2>(b, k0, kend - k0, Rect{kend, n, kend, n}, nsys, st);
-      ++launches;
-    }
-  });
+  const size_t tiles = (size_t)(n + TC_T - 1) / TC_T;
+  lu_two_level<float2>(
+      b, nsys, status, st, launches,
+      [&](BatchT<float2> bg, int ns, cudaStream_t sg, int s0, int k0, int kend) {
+        TcWork tg = w.tc;   // the group's slice of the operand images
+        tg.a += (size_t)s0 * tiles * TC_NCH * 2 * TC_AIMG;
+        tg.b += (size_t)s0 * tiles * TC_NCH * 2 * TC_BIMG;
+        if (!tc_update(tg, bg, k0, ns, sg, launches, status)) {
+          zgemm_update<float2>(bg, k0, kend - k0, Rect{kend, n, kend, n}, ns, sg);
+          ++launches;
+        }
+      },
+      lanes);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         2 * TB * TB * (int)sizeof(float2));
+                         inv_diag_smem<float2>());
     attr = true;
   }
   const int nblk = (n + TB - 1) / TB;
-  inv_diag_kernel<float2><<<dim3(nblk, 1, nsys), TB, 2 * TB * TB * sizeof(float2), st>>>(b, w.inv, nblk);
+  inv_diag_kernel<float2><<<dim3(nblk, 1, nsys), INV_THREADS, inv_diag_smem<float2>(), st>>>(b, w.inv, nblk);
   ++launches;
 }
 
-inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches) {
+inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches,
+                     const Lanes* lanes) {
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
-  trsm_launch<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches);
+  trsm_launch<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, lanes);
   // the solution is left in w.rf (forward into yf, backward back into rf)
 }
 
 // X: right-hand sides in, solution out (FP64); Y unused scratch
 inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double2* X, double2* /*Y*/, int nrhs,
-                               cudaStream_t st, long long& launches) {
+                               cudaStream_t st, long long& launches, const Lanes* lanes = nullptr) {
   const long long V = (long long)nsys * n * nrhs;
   const int nv = nsys * nrhs;
   cudaMemcpyAsync(w.b, X, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
@@ -197,7 +206,7 @@ inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double
   const int max_it = refine_max_it();
   double prev = 1e300;
   for (int it = 0; it < max_it; ++it) {
-    trsm_f32(w, n, nsys, nrhs, st, launches);
+    trsm_f32(w, n, nsys, nrhs, st, launches, lanes);
     accumulate_kernel<<<1184, 256, 0, st>>>(X, w.rf, V, it == 0);
     ++launches;
     cudaMemsetAsync(w.norms, 0, (size_t)nv * sizeof(unsigned long long), st);
