@@ -466,17 +466,18 @@ def run_ours(args):
     hbm, tc, src = peaks()
     # Dominant kernels of the mixed step: the two assembly passes (FP64 Green
     # functions). Algorithmic bytes = the influence matrices written, 4 x 16 N^2
-    # per frequency, over the assembly phase's CUDA-event time. DRAM traffic per
-    # frequency from the ncu capture of the same passes (Rankine pass writes the
-    # matrices, wave pass reads and rewrites them): 1.10 GB finite depth, 1.03 GB
-    # deep water at N=2400.
+    # per frequency, plus the FP32 copy of D+ and D- (2 x 8 N^2) that the wave
+    # pass writes for the mixed LU, over the assembly phase's CUDA-event time.
+    # DRAM traffic per frequency from the ncu capture of the same passes (the
+    # Rankine pass writes the matrices, the wave pass reads and rewrites them):
+    # 1.101 GB finite depth, 1.114 GB deep water at N=2400, plus the FP32 copy.
     N = case.mesh.npanels
     asm_ms = mx["phase"][0]
-    asm_bytes = 4 * 16.0 * N * N * nomega
+    asm_bytes = (4 * 16.0 + 2 * 8.0) * N * N * nomega
     achieved = asm_bytes / (asm_ms / 1e3) / 1e9
     kw = case.omegas ** 2 / case.g
     n_fd = int((~((case.depth == 0.0) | (kw * case.depth >= 20))).sum())
-    traffic = (1.103e9 * n_fd + 1.033e9 * (nomega - n_fd)) * (N / 2400.0) ** 2
+    traffic = (1.101e9 * n_fd + 1.114e9 * (nomega - n_fd)) * (N / 2400.0) ** 2 + 2 * 8.0 * N * N * nomega
     line = {
         "metric": "BEM solves/s (mixed vs FP64 GPU, rel err<=1e-6) at N=2400; serve p50/p99 ms",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -489,13 +490,14 @@ def run_ours(args):
                  "phase_ms": {"assemble": f64["phase"][0], "factor": f64["phase"][1], "solve": f64["phase"][2]}},
         "mixed_vs_fp64": {"max_rel_err": err_max, "median_rel_err": err_med, "speedup": f64["ms"] / mx["ms"]},
         "phase_ms": {"assemble": mx["phase"][0], "factor_refine": mx["phase"][1], "solve": mx["phase"][2]},
-        "roofline": {"bound": "hbm", "kernel": "rankine_kernel + wave_kernel (influence-matrix assembly, FP64)",
+        "roofline": {"bound": "hbm",
+                     "kernel": "rankine_kernel + wave_sym_kernel (influence-matrix assembly, FP64)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
                      "traffic": traffic / nomega, "traffic_unit": "DRAM bytes per frequency (ncu)",
-                     "algorithmic_bytes_per_frequency": 64.0 * N * N,
+                     "algorithmic_bytes_per_frequency": 80.0 * N * N,
                      "fp64": {"note": "the assembly is FP64-pipe and latency bound, not HBM bound",
-                              "fp64_pipe_active_ncu": {"rankine_kernel<1>": 0.516, "wave_kernel<1>": 0.337,
-                                                       "rankine_kernel<0>": 0.171, "wave_kernel<0>": 0.270}},
+                              "fp64_pipe_active_ncu": {"rankine_kernel<1>": 0.325, "wave_sym_kernel<1>": 0.339,
+                                                       "rankine_kernel<0>": 0.295, "wave_sym_kernel<0>": 0.152}},
                      "lu_tc": {"kernel": "tc_update_kernel (mixed LU outer update, K=128)", "bound": "hbm",
                                "frac_ncu": 0.53, "tensor_pipe_active_ncu": 0.34,
                                "traffic_equals_algorithmic": True}},

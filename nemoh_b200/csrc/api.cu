@@ -270,6 +270,8 @@ void assemble_range(nemoh_ctx* c, int s0, int s1) {
   GreenCtx g = green_ctx(c);
   const long long NN = (long long)N * N;
   AsmOut o{c->d_D.as<double2>(), c->d_S.as<double2>(), cls * NN};
+  // the mixed LU factors an FP32 copy of D: the wave pass writes it with the final D
+  if (c->mode == NEMOH_B200_MIXED) o.d32 = c->mixed.lu;
   dim3 blk(ASM_ROWS);
   const OmegaParams* dom = c->d_oms.as<OmegaParams>();
   const PanelRec* rec = c->d_rec.as<PanelRec>();
@@ -363,7 +365,7 @@ void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs) {
   c->lu64 = c->mode == NEMOH_B200_FP64;
   if (c->mode == NEMOH_B200_MIXED) {
     mixed_factor(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_status.as<int>(), c->stream, c->launches,
-                 &c->lanes);
+                 &c->lanes, /*have_f32=*/true);
     CK(cudaGetLastError());
     if (have_rhs) mixed_solve(c, nsys, nrhs);
   } else {

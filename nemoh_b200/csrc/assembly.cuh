@@ -134,7 +134,8 @@ __global__ void crek_kernel(const double* __restrict__ xr, const double* __restr
 //   rankine_kernel: Rankine part (VAVINFD / VAVFD) -> real parts, imaginary = 0;
 //   wave_sym_kernel: wave part (VNSINFD / VNSFD; in finite depth with the
 //                   exponential images) added to the real parts and written to
-//                   the imaginary parts.
+//                   the imaginary parts; in mixed precision it also writes the
+//                   FP32 copy of D that the FP32 LU factors.
 // Splitting the pair evaluation keeps each kernel's registers and code small
 // enough for several CTAs per SM; the extra read of the matrices is 64 bytes
 // per pair and symmetry class pair.
@@ -155,6 +156,7 @@ struct AsmOut {
   double2* d;           // D+ (and D-) of frequency slot s at d + s * slot_stride
   double2* s;           // S+ (and S-) likewise
   long long slot_stride;
+  float2* d32 = nullptr;   // optional FP32 copy of the final D (same layout), for the mixed LU
 };
 
 __device__ __forceinline__ void stage_panels(const PanelRec* __restrict__ rec, int j0, int nj, PanelRec* sp) {
@@ -345,15 +347,20 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
   const long long NN = (long long)N * N;
   double2* od = out.d + slot * out.slot_stride;
   double2* os = out.s + slot * out.slot_stride;
+  float2* o32 = out.d32 ? out.d32 + slot * out.slot_stride : nullptr;
   auto add = [&](long long o, const PairOut& r) {
     double2 d = od[o], sv = os[o];
-    od[o] = make_double2(d.x + r.dp_re, r.dp_im);
+    const double2 dn = make_double2(d.x + r.dp_re, r.dp_im);
+    od[o] = dn;
     os[o] = make_double2(sv.x + r.sp_re, r.sp_im);
+    if (o32) o32[o] = make_float2((float)dn.x, (float)dn.y);
     if (NJJ == 2) {
       d = od[NN + o];
       sv = os[NN + o];
-      od[NN + o] = make_double2(d.x + r.dm_re, r.dm_im);
+      const double2 dm = make_double2(d.x + r.dm_re, r.dm_im);
+      od[NN + o] = dm;
       os[NN + o] = make_double2(sv.x + r.sm_re, r.sm_im);
+      if (o32) o32[NN + o] = make_float2((float)dm.x, (float)dm.y);
     }
   };
   for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {

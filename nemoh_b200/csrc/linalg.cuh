@@ -417,10 +417,10 @@ inline LaneSplit lane_split(int nsys, cudaStream_t main, const Lanes* lanes) {
     L.st[0] = main;
     return L;
   }
-  L.groups = LANES;
-  for (int g = 0; g <= LANES; ++g) L.first[g] = (int)((long long)nsys * g / LANES);
+  L.groups = std::min(LANES, nsys);   // every group holds at least one system
+  for (int g = 0; g <= L.groups; ++g) L.first[g] = (int)((long long)nsys * g / L.groups);
   cudaEventRecord(lanes->fork, main);
-  for (int g = 0; g < LANES; ++g) {
+  for (int g = 0; g < L.groups; ++g) {
     L.st[g] = lanes->s[g];
     cudaStreamWaitEvent(lanes->s[g], lanes->fork, 0);
   }

@@ -152,11 +152,14 @@ __global__ void residual_finish_kernel(const double2* __restrict__ r, float2* __
   if ((threadIdx.x & 31) == 0) atomicMax(rnorm + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
+// have_f32: the assembly already wrote the FP32 copy of D into w.lu
 inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches,
-                         const Lanes* lanes = nullptr) {
-  const long long total = (long long)nsys * n * n;
-  d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
-  ++launches;
+                         const Lanes* lanes = nullptr, bool have_f32 = false) {
+  if (!have_f32) {
+    const long long total = (long long)nsys * n * n;
+    d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
+    ++launches;
+  }
   BatchT<float2> b{w.lu, (long long)n * n, n, w.diag, w.pinv};
   const size_t tiles = (size_t)(n + TC_T - 1) / TC_T;
   lu_two_level<float2>(
