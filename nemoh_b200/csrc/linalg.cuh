@@ -396,7 +396,10 @@ __global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
 // kernels of one group (diagonal blocks, panels, small updates) overlap the
 // work of the other. Without lanes (or with one system) everything runs on
 // the caller's stream.
-constexpr int LANES = 2;
+#ifndef NB_LANES
+#define NB_LANES 4
+#endif
+constexpr int LANES = NB_LANES;
 struct Lanes {
   cudaStream_t s[LANES] = {};
   cudaEvent_t fork = nullptr, join[LANES] = {};
