@@ -76,7 +76,8 @@ int nemoh_b200_solve_problem(nemoh_ctx* ctx, double period, const double* nvel, 
  * complex, Force = -sum_c PRESSURE(c) NDS(i,c) with PRESSURE = rho i W phi
  * (NEMOH.f90:137-141, SOLVE_BEM.f90:91-96). Frequencies are processed in the
  * given order (the order matters only for the reference's free-surface-panel
- * quadrature state, see DESIGN). */
+ * quadrature state: in deep water the theta sum runs over the node count NQ
+ * left by the last finite-depth frequency, SOLVE_BEM_INFD_DIRECT.f90:79). */
 int nemoh_b200_solve_frequencies(nemoh_ctx* ctx, int nomega, const double* omegas, int nrhs, const double* nvel,
                                  int nint, const double* nds, double* force);
 

@@ -16,7 +16,9 @@ int nemoh_b200_diag_dispersion_root(double ak, double* root);
 int nemoh_b200_diag_exponential_fit(double akh, double amh, int* nexp, double* ambda, double* ar);
 /* CINT_INFD / CINT_FD: returns the node count; qq, cq hold >= 101 entries */
 int nemoh_b200_diag_theta_quadrature(double akk, double* qq, double* cq);
-/* thresholds of the table-stencil indices, 48 each (see DESIGN) */
+/* thresholds of the table-stencil indices, 48 each: for every index k the
+ * smallest x whose truncated log10 formula gives >= k, found by bisection on the
+ * double bit pattern with the host's log10 */
 int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5);
 
 #ifdef __cplusplus
