@@ -306,12 +306,11 @@ Batch dbatch(nemoh_ctx* c) {
 void factor_fp64(nemoh_ctx* c, int nsys) {
   Batch b = dbatch(c);
   const int N = c->nfa;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  once_per_device(attr, [] {
     CK(cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             zgemm_smem<double2>()));
-    attr = true;
-  }
+  });
   lu_two_level<double2>(
       b, nsys, c->d_status.as<int>(), c->stream, c->launches,
       [&](Batch bg, int ns, cudaStream_t sg, int, int k0, int kend) {
@@ -320,12 +319,11 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
       },
       &c->lanes);
   CK(cudaGetLastError());
-  static bool attr2 = false;
-  if (!attr2) {
+  static std::atomic<unsigned long long> attr2{0};
+  once_per_device(attr2, [] {
     CK(cudaFuncSetAttribute(inv_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             inv_diag_smem<double2>()));
-    attr2 = true;
-  }
+  });
   const int nblk = (N + TB - 1) / TB;
   inv_diag_kernel<double2><<<dim3(nblk, 1, nsys), INV_THREADS, inv_diag_smem<double2>(), c->stream>>>(
       b, c->d_inv.as<double2>(), nblk);

@@ -3,7 +3,24 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace nb200 {
+
+// cudaFuncSetAttribute acts on the current device only, so a kernel that needs
+// more dynamic shared memory than the default is set up once on every device
+// a process uses; `done` holds one bit per device (concurrent first calls on a
+// device may both set it, which is harmless).
+template <class F>
+inline void once_per_device(std::atomic<unsigned long long>& done, F set) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  set();
+  done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
 
 // ---------------------------------------------------------------------------
 // Exactly rounded arithmetic for every quantity that decides a branch.

@@ -484,11 +484,10 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
       const BatchT<C2> bg = sub_batch(b, s0);
       const cudaStream_t st = L.st[g];
       if (kend < n && b.pinv) {
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        once_per_device(attr, [] {
           cudaFuncSetAttribute(strip_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_smem<C2>());
-          attr = true;
-        }
+        });
         strip_kernel<C2><<<dim3((n - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
         ++launches;
       }
@@ -727,12 +726,11 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
   const long long xs = (long long)N * nrhs;
   const int nblk = (N + TB - 1) / TB;
   const int smem = (2 * TB * MAX_RHS + TB * TB) * (int)sizeof(C2);
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  once_per_device(attr, [smem] {
     cudaFuncSetAttribute(trsm_fused_kernel<C2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     cudaFuncSetAttribute(trsm_fused_kernel<C2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  });
   const LaneSplit L = lane_split(nsys, main, lanes);
   auto each = [&](auto launch) {
     for (int g = 0; g < L.groups; ++g) {

@@ -174,12 +174,11 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
         }
       },
       lanes);
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  once_per_device(attr, [] {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          inv_diag_smem<float2>());
-    attr = true;
-  }
+  });
   const int nblk = (n + TB - 1) / TB;
   inv_diag_kernel<float2><<<dim3(nblk, 1, nsys), INV_THREADS, inv_diag_smem<float2>(), st>>>(b, w.inv, nblk);
   ++launches;

@@ -395,11 +395,10 @@ inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_
   if (!tc_enabled()) return false;
   const int n = b.n, rest = n - k0 - LU_OUTER;
   if (rest <= 0) return true;
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<unsigned long long> attr{0};
+  once_per_device(attr, [] {
     cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    attr = true;
-  }
+  });
   const int t = (n + TC_T - 1) / TC_T;
   const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
   const int nt = (rest + TC_T - 1) / TC_T;
