@@ -119,10 +119,17 @@ __global__ void __launch_bounds__(1024) lu_diag_kernel(BatchT<C2> b, int k, int*
   }
 }
 
+// acc += a b as four fused multiply-adds into the accumulator (written out:
+// `acc.x += a.x*b.x - a.y*b.y` compiles to a multiply, an FMA and an add per
+// component, 50% more floating-point instructions in the update loops)
+__device__ __forceinline__ double fmx(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fmx(float a, float b, float c) { return fmaf(a, b, c); }
 template <class C2>
 __device__ __forceinline__ void cmac(C2& acc, C2 a, C2 b) {
-  acc.x += a.x * b.x - a.y * b.y;
-  acc.y += a.x * b.y + a.y * b.x;
+  acc.x = fmx(a.x, b.x, acc.x);
+  acc.x = fmx(-a.y, b.y, acc.x);
+  acc.y = fmx(a.x, b.y, acc.y);
+  acc.y = fmx(a.y, b.x, acc.y);
 }
 
 // L21 <- A21 inv(U11) (CTAs [0, nrb), one thread per row) and
@@ -272,10 +279,7 @@ __global__ void __launch_bounds__(128) zgemm_update_kernel(BatchT<C2> b, int k, 
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          acc[i][j].x += a[i].x * bb[j].x - a[i].y * bb[j].y;
-          acc[i][j].y += a[i].x * bb[j].y + a[i].y * bb[j].x;
-        }
+        for (int j = 0; j < 8; ++j) cmac(acc[i][j], a[i], bb[j]);
     }
     __syncthreads();   // stage s is refilled two chunks later
   }
@@ -566,8 +570,7 @@ constexpr int TRSM_ROWS = 32;   // rows updated per CTA of a solve step
 
 template <class C2>
 __device__ __forceinline__ void cmad(C2& acc, C2 a, C2 b) {
-  acc.x += a.x * b.x - a.y * b.y;
-  acc.y += a.x * b.y + a.y * b.x;
+  cmac(acc, a, b);
 }
 
 // inv layout: ((sys * nblk + blk) * 2 + {0: inv L, 1: inv U}) * TB * TB, column-major.
