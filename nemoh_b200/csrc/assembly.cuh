@@ -146,7 +146,7 @@ constexpr int ASM_TJ = 32;
 #define ASM_MINB_RANKINE 3
 #endif
 #ifndef ASM_MINB_WAVE_FD
-#define ASM_MINB_WAVE_FD 3
+#define ASM_MINB_WAVE_FD 4
 #endif
 #ifndef ASM_MINB_WAVE_INFD
 #define ASM_MINB_WAVE_INFD 4
