@@ -70,7 +70,8 @@ int nemoh_b200_set_mesh(nemoh_ctx* ctx, int np, int nfa, int nsymy, const double
 int nemoh_b200_solve_problem(nemoh_ctx* ctx, double period, const double* nvel, double* zigb, double* zigs,
                              double* zpb, double* zps, int* nexp);
 
-/* Batched fast path: nomega frequencies, each with nrhs problems (nrhs <= 16).
+/* Batched fast path: nomega frequencies, each with nrhs problems (1 <= nrhs <= 16;
+ * NEMOH_B200_EINVAL below, NEMOH_B200_ECAPACITY above, both before any copy).
  * nvel: (2^s nfa) x nrhs x nomega complex; nds: nint x (2^s nfa) real
  * (mesh/Integration.dat, NEMOH.f90:88-94); force: nint x nrhs x nomega
  * complex, Force = -sum_c PRESSURE(c) NDS(i,c) with PRESSURE = rho i W phi

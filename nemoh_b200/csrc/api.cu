@@ -709,8 +709,12 @@ int nemoh_b200_solve_problem(nemoh_ctx* c, double period, const double* nvel, do
 
 int nemoh_b200_solve_frequencies(nemoh_ctx* c, int nomega, const double* omegas, int nrhs, const double* nvel,
                                  int nint, const double* nds, double* force) {
-  if (!c || nomega < 1 || !omegas || !nvel || nint < 0 || (nint > 0 && (!nds || !force))) return NEMOH_B200_EINVAL;
+  if (!c || nomega < 1 || !omegas || !nvel || nrhs < 1 || nint < 0 || (nint > 0 && (!nds || !force)))
+    return NEMOH_B200_EINVAL;
   return guarded(c, [&] {
+    // sizes are checked before any copy reads the caller's buffers
+    if (!c->nfa) throw Fail{NEMOH_B200_EINVAL, "no mesh"};
+    if (nrhs > MAX_RHS) throw Fail{NEMOH_B200_ECAPACITY, "nrhs must be in 1..16"};
     const int N = c->nfa, cls = ncls(c);
     const size_t nv = (size_t)cls * N * nrhs * nomega;
     CK(c->d_nvel.ensure(nv * sizeof(double2)));
@@ -732,7 +736,9 @@ int nemoh_b200_solve_frequencies(nemoh_ctx* c, int nomega, const double* omegas,
 int nemoh_b200_solve_frequencies_device(nemoh_ctx* c, int nomega, const double* omegas, int nrhs,
                                         const double* nvel_device, int nint, const double* nds_device,
                                         double* force_device, void* stream) {
-  if (!c || nomega < 1 || !omegas || !nvel_device) return NEMOH_B200_EINVAL;
+  if (!c || nomega < 1 || !omegas || !nvel_device || nrhs < 1 || nint < 0 ||
+      (nint > 0 && (!nds_device || !force_device)))
+    return NEMOH_B200_EINVAL;
   return guarded(c, [&] {
     cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
     cudaEvent_t e;

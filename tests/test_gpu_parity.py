@@ -176,6 +176,39 @@ def test_tiny_frequency_reports_status(solver):
     assert e.value.code == 4
 
 
+def test_batched_sizes_refused(solver):
+    """nrhs outside 1..16 and missing buffers are refused with the header's
+    status codes, and the context solves as before afterwards. Every buffer
+    passed is large enough for the call it is passed to."""
+    import torch
+    case = CASES[0]
+    _mesh(solver, case)
+    m = case.mesh
+    nc = m.npanels * 2 ** m.isym
+    rng = np.random.default_rng(11)
+    nvel = rng.standard_normal((nc, 7, 1)) + 1j * rng.standard_normal((nc, 7, 1))
+    nds = np.asfortranarray(rng.standard_normal((3, nc)))
+    om = np.array([case.omegas[0]])
+    before = solver.solve_frequencies(om, nvel, nds)
+    lib = nb.load_library()
+    d = lambda a: a.ctypes.data_as(nb._d)
+    h = solver._h
+    big = np.zeros((nc, 17, 1), np.complex128, order="F")
+    force = np.zeros((3, 17, 1), np.complex128, order="F")
+    assert lib.nemoh_b200_solve_frequencies(h, 1, d(om), 0, d(big), 3, d(nds), d(force)) == 1
+    assert lib.nemoh_b200_solve_frequencies(h, 1, d(om), 17, d(big), 3, d(nds), d(force)) == 23
+    assert "1..16" in lib.nemoh_b200_last_error(h).decode()
+    assert lib.nemoh_b200_solve_frequencies(h, 1, d(om), 7, d(big), 3, None, d(force)) == 1
+    dev = torch.zeros(2 * nc * 17, dtype=torch.float64, device="cuda:0")
+    dnds = torch.zeros(3 * nc, dtype=torch.float64, device="cuda:0")
+    dforce = torch.zeros(2 * 3 * 17, dtype=torch.float64, device="cuda:0")
+    assert lib.nemoh_b200_solve_frequencies_device(h, 1, d(om), 0, dev.data_ptr(), 3, dnds.data_ptr(),
+                                                   dforce.data_ptr(), None) == 1
+    torch.cuda.synchronize()
+    after = solver.solve_frequencies(om, nvel, nds)
+    np.testing.assert_allclose(after, before, rtol=0, atol=1e-12 * np.abs(before).max())
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_mixed_precision_matches_fp64(case):
     with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
