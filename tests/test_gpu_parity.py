@@ -209,6 +209,41 @@ def test_batched_sizes_refused(solver):
     np.testing.assert_allclose(after, before, rtol=0, atol=1e-12 * np.abs(before).max())
 
 
+def _first_panels(case, k):
+    """The case restricted to its first k panels (an open surface): orders
+    below, at and just above the tile and panel widths of the kernels."""
+    m = case.mesh
+    sub = C.Mesh(m.nodes, m.panels[:k], m.isym)
+    c = C.Case(sub, case.omegas[:2], case.betas_deg[:1], case.rad, case.force, rho=case.rho, g=case.g,
+               depth=case.depth)
+    c.name = "%s_first%d" % (case.name, k)
+    return c
+
+
+TINY = [(0, 1), (0, 17), (0, 129), (0, 257), (1, 5), (1, 33), (1, 65)]
+
+
+@pytest.mark.parametrize("which,k", TINY, ids=["%s_%d" % (IDS[w], k) for w, k in TINY])
+def test_small_and_ragged_orders_match_oracle(which, k, tmp_path):
+    """FP64 forces against the oracle (1e-9 of the largest force) and mixed
+    precision against FP64 (1e-6) for a single panel and for orders one above
+    a multiple of the 16-row assembly tiles, the 32-column LU steps, the
+    64-row triangular-solve blocks and the 128-column outer panels (129 and
+    257: tensor-core outer updates of one row and column)."""
+    case = _first_panels(CASES[which], k)
+    with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
+        for s in (s64, smx):
+            _mesh(s, case)
+        nvel, nds, npb = G.problems(case)
+        F64 = s64.solve_frequencies(case.omegas, nvel, nds)
+        Fmx = smx.solve_frequencies(case.omegas, nvel, nds)
+    Fo = G.oracle_forces(case, str(tmp_path))
+    scale = np.abs(Fo).max()
+    assert scale > 0
+    assert np.abs(F64 - Fo).max() <= 1e-9 * scale, (case.name, np.abs(F64 - Fo).max() / scale)
+    assert np.abs(Fmx - F64).max() <= 1e-6 * scale, (case.name, np.abs(Fmx - F64).max() / scale)
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_mixed_precision_matches_fp64(case):
     with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
