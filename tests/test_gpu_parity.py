@@ -244,6 +244,26 @@ def test_small_and_ragged_orders_match_oracle(which, k, tmp_path):
     assert np.abs(Fmx - F64).max() <= 1e-6 * scale, (case.name, np.abs(Fmx - F64).max() / scale)
 
 
+@pytest.mark.parametrize("which", [0, 1], ids=[IDS[0], IDS[1]])
+def test_sixteen_problems_per_frequency(which, tmp_path):
+    """The largest batch of right-hand sides (10 headings + 6 DOF = 16 per
+    frequency): FP64 against the oracle, mixed against FP64."""
+    base = CASES[which]
+    case = C.Case(base.mesh, base.omegas[:2], np.linspace(0.0, 162.0, 10), base.rad, base.force, rho=base.rho,
+                  g=base.g, depth=base.depth)
+    case.name = base.name + "_16rhs"
+    with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
+        for s in (s64, smx):
+            _mesh(s, case)
+        nvel, nds, npb = G.problems(case)
+        assert npb == 16
+        F64 = s64.solve_frequencies(case.omegas, nvel, nds)
+        Fmx = smx.solve_frequencies(case.omegas, nvel, nds)
+    Fo = G.oracle_forces(case, str(tmp_path))
+    assert G.rel_err(F64, Fo) < 1e-9
+    assert G.rel_err(Fmx, F64) < 1e-6
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_mixed_precision_matches_fp64(case):
     with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
