@@ -774,10 +774,12 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
 // are added with atomics, so Y must hold its initial value (0 or the RHS).
 // The number of right-hand sides is a template parameter so that no
 // predicated-off FMAs are issued (the kernel is balanced between HBM and the
-// FP64 pipe at nine right-hand sides).
+// FP64 pipe at nine right-hand sides). Four CTAs per SM (128 registers, 16
+// bytes of spills at nine right-hand sides instead of 132 registers and three
+// CTAs) keep a third more column loads in flight: 9% less time per launch.
 constexpr int MV_COLS = 128;
 template <int NR>
-__global__ void __launch_bounds__(128) matvec_acc_kernel(Batch m, const double2* __restrict__ xbase, long long xstride,
+__global__ void __launch_bounds__(128, 4) matvec_acc_kernel(Batch m, const double2* __restrict__ xbase, long long xstride,
                                                          double2* ybase, long long ystride, double sign) {
   __shared__ double2 Xs[MV_COLS * NR];
   const int n = m.n;
