@@ -75,6 +75,9 @@ def load_library():
     L.nemoh_b200_body_conditions.argtypes = [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int,
                                              _d, ctypes.c_int, _i, _i, _d, _d, ctypes.c_int, _i, _i, _d, _d, _d, _d,
                                              _d]
+    L.nemoh_b200_body_conditions_device.argtypes = [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
+                                                    ctypes.c_int, _d, ctypes.c_int, _i, _i, _d, _d, ctypes.c_int, _i,
+                                                    _i, _d, _d, _vp, _vp, _vp, _vp]
     L.nemoh_b200_kochin.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
                                     ctypes.c_int, _d, _d, _d]
     L.nemoh_b200_free_surface.argtypes = [_vp, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
@@ -214,30 +217,46 @@ class Solver:
         """NVEL (2^s N, Nproblems) in the pre-processor's problem order, NDS
         (Nint, 2^s N) and Froude-Krylov forces (Nw, Nbeta, Nint), computed on the
         GPU for `case` (its mesh must be the current one)."""
-        mesh = case.mesh
         nc = self.nfa * 2 ** self.isym
         nw, nb, nr, nf = len(case.omegas), len(case.betas_deg), len(case.rad), len(case.force)
+        nvel = np.zeros((nc, nb + nr, nw), dtype=np.complex128, order="F")
+        nds = np.zeros((nf, nc), dtype=np.float64, order="F")
+        fk = np.zeros((nf, nb, nw), dtype=np.complex128, order="F")
+        args, _keep = self._body_condition_args(case)
+        self._check(load_library().nemoh_b200_body_conditions(
+            self._h, *args, nvel.ctypes.data_as(_d), nds.ctypes.data_as(_d), fk.ctypes.data_as(_d)))
+        return nvel.reshape(nc, (nb + nr) * nw, order="F"), nds, fk.transpose(2, 1, 0)
 
+    def body_conditions_device(self, case, nvel_ptr, nds_ptr, fk_ptr, stream=0):
+        """The same outputs written to device memory of the context's device,
+        column-major: nvel (2^s N, Nbeta + Nrad, Nw) complex, nds (Nint, 2^s N)
+        real, fk (Nint, Nbeta, Nw) complex; ordered after the work on `stream`."""
+        args, _keep = self._body_condition_args(case)
+        self._check(load_library().nemoh_b200_body_conditions_device(
+            self._h, *args, _vp(nvel_ptr), _vp(nds_ptr), _vp(fk_ptr), _vp(stream)))
+
+    @staticmethod
+    def _body_condition_args(case):
+        """Leading C arguments of the body-conditions entry points (and the
+        arrays they point into, which must outlive the call)."""
         def spec(dofs):
             kind = np.array([d.icase for d in dofs] or [1], dtype=np.int32)
             body = np.array([d.body for d in dofs] or [1], dtype=np.int32)
             dr = np.array([d.direction for d in dofs] or [(0, 0, 0)], dtype=np.float64).ravel()
             ax = np.array([d.axis for d in dofs] or [(0, 0, 0)], dtype=np.float64).ravel()
             return kind, body, dr, ax
+        nw, nb, nr, nf = len(case.omegas), len(case.betas_deg), len(case.rad), len(case.force)
         rk, rb, rd, ra = spec(case.rad)
         fk_, fb, fd, fa = spec(case.force)
         om = np.ascontiguousarray(case.omegas, dtype=np.float64)
         beta = np.ascontiguousarray(np.asarray(case.betas_deg, dtype=np.float64) * np.pi / 180.0)
-        pb = np.ascontiguousarray(mesh.body, dtype=np.int32)
-        nvel = np.zeros((nc, nb + nr, nw), dtype=np.complex128, order="F")
-        nds = np.zeros((nf, nc), dtype=np.float64, order="F")
-        fk = np.zeros((nf, nb, nw), dtype=np.complex128, order="F")
+        if not nb:
+            beta = np.zeros(1)
+        pb = np.ascontiguousarray(case.mesh.body, dtype=np.int32)
         ip = lambda a: a.ctypes.data_as(_i)
-        self._check(load_library().nemoh_b200_body_conditions(
-            self._h, ip(pb), float(case.xeff), float(case.yeff), nw, _p(om), nb, _p(beta if nb else np.zeros(1)),
-            nr, ip(rk), ip(rb), _p(rd), _p(ra), nf, ip(fk_), ip(fb), _p(fd), _p(fa),
-            nvel.ctypes.data_as(_d), nds.ctypes.data_as(_d), fk.ctypes.data_as(_d)))
-        return nvel.reshape(nc, (nb + nr) * nw, order="F"), nds, fk.transpose(2, 1, 0)
+        args = (ip(pb), float(case.xeff), float(case.yeff), nw, _p(om), nb, _p(beta), nr, ip(rk), ip(rb), _p(rd),
+                _p(ra), nf, ip(fk_), ip(fb), _p(fd), _p(fa))
+        return args, (rk, rb, rd, ra, fk_, fb, fd, fa, om, beta, pb)
 
     # -- COMPUTE_KOCHIN ---------------------------------------------------------
     def kochin(self, period, theta, zigb, zigs=None, xeff=0.0, yeff=0.0):

@@ -76,6 +76,15 @@ struct Fail {
   std::string msg;
 };
 
+// event that orders the context's stream against a caller's stream; released
+// on every path out of the call, errors included
+struct ScopedEvent {
+  cudaEvent_t e = nullptr;
+  ~ScopedEvent() {
+    if (e) cudaEventDestroy(e);
+  }
+};
+
 }  // namespace
 
 struct nemoh_ctx {
@@ -741,15 +750,14 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* c, int nomega, const double* 
     return NEMOH_B200_EINVAL;
   return guarded(c, [&] {
     cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
-    cudaEvent_t e;
-    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    CK(cudaEventRecord(e, user));
-    CK(cudaStreamWaitEvent(c->stream, e, 0));
+    ScopedEvent ev;
+    CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev.e, user));
+    CK(cudaStreamWaitEvent(c->stream, ev.e, 0));
     solve_frequencies_impl(c, nomega, omegas, nrhs, reinterpret_cast<const double2*>(nvel_device), nint, nds_device,
                            reinterpret_cast<double2*>(force_device));
-    CK(cudaEventRecord(e, c->stream));
-    CK(cudaStreamWaitEvent(user, e, 0));
-    CK(cudaEventDestroy(e));
+    CK(cudaEventRecord(ev.e, c->stream));
+    CK(cudaStreamWaitEvent(user, ev.e, 0));
   });
 }
 
@@ -935,11 +943,11 @@ static int body_conditions_impl(nemoh_ctx* c, const int* panel_body, double xeff
     CK(c->d_pre.ensure(std::max<size_t>(off, 256)));
     char* base = c->d_pre.as<char>();
     cudaStream_t st = c->stream;
-    cudaEvent_t e = nullptr;
+    ScopedEvent ev;
     if (!host_out) {
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventRecord(e, user));
-      CK(cudaStreamWaitEvent(st, e, 0));
+      CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+      CK(cudaEventRecord(ev.e, user));
+      CK(cudaStreamWaitEvent(st, ev.e, 0));
     }
     if (!waves.empty()) CK(cudaMemcpyAsync(base + o_w, waves.data(), waves.size() * sizeof(PreWave), cudaMemcpyHostToDevice, st));
     if (!dofs.empty()) CK(cudaMemcpyAsync(base + o_d, dofs.data(), dofs.size() * sizeof(PreDof), cudaMemcpyHostToDevice, st));
@@ -963,9 +971,8 @@ static int body_conditions_impl(nemoh_ctx* c, const int* panel_body, double xeff
       if (fk_h && n_fk) CK(cudaMemcpyAsync(fk_h, fk, n_fk * sizeof(double2), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
     } else {
-      CK(cudaEventRecord(e, st));
-      CK(cudaStreamWaitEvent(user, e, 0));
-      CK(cudaEventDestroy(e));
+      CK(cudaEventRecord(ev.e, st));
+      CK(cudaStreamWaitEvent(user, ev.e, 0));
       // the staged specs must outlive the kernel: wait before the next call may overwrite them
       CK(cudaStreamSynchronize(st));
     }

@@ -352,6 +352,41 @@ def test_device_body_conditions_match_preprocessor(solver, which):
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), which
 
 
+@pytest.mark.parametrize("which", [0, 1], ids=[IDS[0], IDS[1]])
+def test_device_pointer_entry_points_match_host(solver, which):
+    """Body conditions and the batched solve with device-resident buffers on a
+    caller's stream give the host-buffer results: NVEL and NDS identical,
+    Froude-Krylov forces (atomic sums) and forces (atomic mat-vec sums) within
+    1e-12 of their largest entry."""
+    import dataclasses
+    import torch
+    case = dataclasses.replace(CASES[which], betas_deg=np.array([0.0, 60.0]))
+    _mesh(solver, case)
+    nvel_h, nds_h, fk_h = solver.body_conditions(case)
+    nc = case.mesh.npanels * 2 ** case.mesh.isym
+    nw, nb, nr, nf = len(case.omegas), len(case.betas_deg), len(case.rad), len(case.force)
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.Stream(dev)
+    nvel_d = torch.zeros(2 * nc * (nb + nr) * nw, dtype=torch.float64, device=dev)
+    nds_d = torch.zeros(nf * nc, dtype=torch.float64, device=dev)
+    fk_d = torch.zeros(2 * nf * nb * nw, dtype=torch.float64, device=dev)
+    force_d = torch.zeros(2 * nf * (nb + nr) * nw, dtype=torch.float64, device=dev)
+    stream.wait_stream(torch.cuda.current_stream(dev))
+    solver.body_conditions_device(case, nvel_d.data_ptr(), nds_d.data_ptr(), fk_d.data_ptr(), stream.cuda_stream)
+    solver.solve_frequencies_device(case.omegas, nvel_d.data_ptr(), nb + nr, nf, nds_d.data_ptr(),
+                                    force_d.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    nv = nvel_d.cpu().numpy().view(np.complex128).reshape((nc, nb + nr, nw), order="F")
+    nd = nds_d.cpu().numpy().reshape((nf, nc), order="F")
+    fk = fk_d.cpu().numpy().view(np.complex128).reshape((nf, nb, nw), order="F")
+    assert np.array_equal(nv.reshape(nc, -1, order="F"), nvel_h)
+    assert np.array_equal(nd, nds_h)
+    assert np.abs(fk.transpose(2, 1, 0) - fk_h).max() <= 1e-12 * np.abs(fk_h).max()
+    F_h = solver.solve_frequencies(case.omegas, nv, nd)
+    F_d = force_d.cpu().numpy().view(np.complex128).reshape((nf, nb + nr, nw), order="F")
+    assert np.abs(F_d - F_h).max() <= 1e-12 * np.abs(F_h).max()
+
+
 def _fs_points(case):
     """Points (x, y) on z = 0 around the body: a polar grid from just outside
     the waterline (tabulated wave term) to 30 body radii (asymptotic form)."""
