@@ -156,6 +156,13 @@ def whole_job_rate(world, units_per_rank, ms):
     return world * units_per_rank / (ms / 1e3)
 
 
+def single_gpu_extras(rank, world):
+    """The CPU baseline sample and the single-GPU workloads beside the headline
+    (output stages, batched bodies, serving streams) run once, on rank 0 of a
+    one-GPU job: with more ranks they would only hold the other GPUs idle."""
+    return rank == 0 and world == 1
+
+
 def run_reference(args):
     """--impl reference: the reference CPU algorithm on all host cores."""
     import multiprocessing as mp
@@ -516,7 +523,7 @@ def run_ours(args):
         "gpu_launches": int(mx["launches"]),
         "clocks": mx["clocks"],
     }
-    if rank == 0 and not args.no_cpu:
+    if single_gpu_extras(rank, world) and not args.no_cpu:
         rate, detail = cpu_sample(case, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": 1, "kind": "port",
                                 "sample": "1 core: whole rows of Green evaluations and the first GAUSSZ elimination "
@@ -526,7 +533,7 @@ def run_ours(args):
     for r in results.values():
         r["solver"].close()
     results = {}
-    if rank == 0 and not args.no_extras:
+    if single_gpu_extras(rank, world) and not args.no_extras:
         for key, fn in (("outputs", lambda: run_outputs(local)),
                         ("batched", lambda: run_batched(local, args.bodies)),
                         ("serve", lambda: run_serving(local, args.bodies, args.requests))):

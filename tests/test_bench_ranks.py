@@ -1,7 +1,8 @@
 """The multi-rank plumbing of bench.py on CPU: two `gloo` ranks, launched the
 way torchrun would (RANK / WORLD_SIZE / MASTER_ADDR=127.0.0.1), each time its
 own copy of the workload; the reported time is the slowest rank's, the job
-rate counts every rank's units, and the reference arm runs on rank 0 only."""
+rate counts every rank's units, the reference arm runs on rank 0 only, and the
+CPU baseline and single-GPU extras run only in a one-rank job."""
 import os
 import socket
 import sys
@@ -50,3 +51,12 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     monkeypatch.setenv("RANK", "1")
     assert bench.run_reference(None) is None   # returns before touching the arguments
     assert capsys.readouterr().out == ""
+
+
+def test_cpu_baseline_and_extras_only_in_a_one_rank_job():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.single_gpu_extras(0, 1)
+    assert not bench.single_gpu_extras(0, 2)
+    assert not bench.single_gpu_extras(1, 2)
+    assert not bench.single_gpu_extras(3, 8)
