@@ -61,18 +61,38 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons of one GPU during the timed
+    region: read through NVML every 20 ms, or from `nvidia-smi -lms 200` where
+    the NVML bindings are missing. Reads only; no GPU setting is changed."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event bits of hw_slowdown, hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap
+    BITS = (0x8, 0x40, 0x20, 0x4)
 
-    def __init__(self, index):
+    def __init__(self, index, period=0.02, nvml=None):
         self.index = index
+        self.period = period
         self.rows = []
         self.proc = None
+        self.nv = nvml
+        self.stop = threading.Event()
 
     def __enter__(self):
+        try:
+            if self.nv is None:
+                import pynvml
+                self.nv = pynvml
+            self.nv.nvmlInit()
+            self.h = self.nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.mx = self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+            self.sample()   # one sample before the region starts, so a short region still has one
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -83,11 +103,33 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def sample(self):
+        """One NVML reading in the row layout of the nvidia-smi query."""
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+        self.rows.append([str(self.index), str(sm), str(self.mx), "", ""] +
+                         ["Active" if bits & b else "Not Active" for b in self.BITS])
+
+    def _poll(self):
+        while not self.stop.wait(self.period):
+            try:
+                self.sample()
+            except Exception:
+                return
+
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([v.strip() for v in line.split(",")])
 
     def __exit__(self, *a):
+        if self.nv is not None:
+            self.stop.set()
+            self.t.join(timeout=5)
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
