@@ -264,6 +264,29 @@ def test_sixteen_problems_per_frequency(which, tmp_path):
     assert G.rel_err(Fmx, F64) < 1e-6
 
 
+def test_two_spheres_8000_panels_mixed_matches_fp64():
+    """The precision configuration at full size: two floating spheres of radius
+    4 m, 20 m apart, 8,000 panels, deep water, 12 DOF + 2 headings, at the
+    lowest, a middle and the highest of its 30 frequencies: mixed precision
+    (split-BF16 tensor-core LU + FP64 refinement) within 1e-6 of FP64 per
+    integration case. The oracle is too slow at this order; its parity with
+    the FP64 path is covered at the smaller orders above."""
+    import dataclasses
+    case = C.config_two_spheres()
+    case = dataclasses.replace(case, omegas=case.omegas[[0, 15, 29]])
+    assert case.mesh.npanels == 8000
+    with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
+        for s in (s64, smx):
+            _mesh(s, case)
+        nvel, nds, npb = G.problems(case)
+        assert npb == 14
+        F64 = s64.solve_frequencies(case.omegas, nvel, nds)
+        Fmx = smx.solve_frequencies(case.omegas, nvel, nds)
+        it, res = smx.last_refinement()
+    assert np.isfinite(F64).all() and np.abs(F64).max() > 0
+    assert G.rel_err(Fmx, F64) < 1e-6, (G.rel_err(Fmx, F64), it, res)
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_mixed_precision_matches_fp64(case):
     with nb.Solver(0, nb.FP64) as s64, nb.Solver(0, nb.MIXED) as smx:
