@@ -232,7 +232,7 @@ __device__ __forceinline__ void tri_tile(int t, int T, int& a, int& b) {
 
 // Exponential images (VNSFD, COMPUTE_GREEN_FD.f90:635-706) of both orders of
 // a pair of submerged panels, added to the real parts of D+/-, S+/-.
-__device__ __forceinline__ void fd_images_pair(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
+NB_HD __forceinline__ void fd_images_pair(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
                                                const PanelRec& PJ, int NJJ, bool both, PairOut& oij, PairOut& oji) {
   ImageSums S;
   fd_image_sums(g, om.h, om.ambda, om.ar, om.nexp + 1, PI.xg, PI.yg, PI.zg, PJ.xg, PJ.yg, PJ.zg, NJJ, S);
@@ -271,7 +271,7 @@ __device__ __forceinline__ void fd_images_pair(const GreenCtx& g, const OmegaPar
 
 // one order of a pair with a panel at the free surface (rare; kept out of line)
 template <bool FD>
-__device__ __noinline__ void pair_wave_ordered(const GreenCtx& g, const OmegaParams& om, const PanelRec& PC,
+NB_HD __noinline__ void pair_wave_ordered(const GreenCtx& g, const OmegaParams& om, const PanelRec& PC,
                                                const PanelRec& PS, PairOut& out) {
   pair_wave<FD>(g, om, PC.xg, PC.yg, PC.zg, PC.xn, PC.yn, PC.zn, PS, out);
 }
@@ -279,7 +279,7 @@ __device__ __noinline__ void pair_wave_ordered(const GreenCtx& g, const OmegaPar
 // Deep water (VNSINFD, one image at ZI + ZJ): every sum is the same for both
 // orders except the horizontal gradient, whose x part and direct-reflection y
 // part change sign.
-__device__ __forceinline__ void wave_infd_both(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
+NB_HD __forceinline__ void wave_infd_both(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
                                                const PanelRec& PJ, int NJJ, bool both, PairOut& oij, PairOut& oji) {
   WaveJJ w[2];
   wave_infd_pair(g, om, PI.xg, PI.yg, PI.zg, PJ, NJJ, w);

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <cmath>
 
 namespace nb200 {
 
@@ -33,11 +34,27 @@ inline void once_per_device(std::atomic<unsigned long long>& done, F set) {
 // compiled with -ffp-contract=off. Values that only feed arithmetic use the
 // fast path (FMA, CUDA libm).
 // ---------------------------------------------------------------------------
+#ifdef __CUDA_ARCH__
 #define XADD(a, b) __dadd_rn((a), (b))
 #define XSUB(a, b) __dsub_rn((a), (b))
 #define XMUL(a, b) __dmul_rn((a), (b))
 #define XDIV(a, b) __ddiv_rn((a), (b))
 #define XSQRT(a) __dsqrt_rn((a))
+#define NB_LDG(p) __ldg(p)
+#else
+// Host compilation of the same functions (the CPU check of the pair
+// functions): IEEE double operations, built with -ffp-contract=off so that
+// nothing is contracted into an FMA.
+#define XADD(a, b) ((a) + (b))
+#define XSUB(a, b) ((a) - (b))
+#define XMUL(a, b) ((a) * (b))
+#define XDIV(a, b) ((a) / (b))
+#define XSQRT(a) std::sqrt((a))
+#define NB_LDG(p) (*(p))
+#endif
+// functions of the Green-function family, compiled for the device and, for the
+// CPU check, for the host
+#define NB_HD __host__ __device__
 
 struct cplx {
   double re, im;
@@ -66,13 +83,13 @@ __host__ __device__ __forceinline__ cplx operator/(cplx a, cplx b) {
 }
 __host__ __device__ __forceinline__ cplx operator/(double s, cplx b) { return mk(s, 0.0) / b; }
 __host__ __device__ __forceinline__ cplx operator/(cplx a, double s) { return {a.re / s, a.im / s}; }
-__device__ __forceinline__ double cabs_(cplx a) { return hypot(a.re, a.im); }
-__device__ __forceinline__ cplx cexp_(cplx a) {
+NB_HD __forceinline__ double cabs_(cplx a) { return hypot(a.re, a.im); }
+NB_HD __forceinline__ cplx cexp_(cplx a) {
   double e = exp(a.re), s, c;
   sincos(a.im, &s, &c);
   return {e * c, e * s};
 }
-__device__ __forceinline__ cplx clog_(cplx a) { return {log(hypot(a.re, a.im)), atan2(a.im, a.re)}; }
+NB_HD __forceinline__ cplx clog_(cplx a) { return {log(hypot(a.re, a.im)), atan2(a.im, a.re)}; }
 
 // ---------------------------------------------------------------------------
 // Table geometry (Solver/NEMOH.f90:179-208): 328 radial x 46 vertical nodes.

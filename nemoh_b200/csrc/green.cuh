@@ -35,10 +35,16 @@ struct PairOut {
   double sp_re, sp_im, sm_re, sm_im;  // S+, S-
 };
 
-__device__ __forceinline__ void set_status(int* st, int code) { atomicCAS(st, 0, code); }
+NB_HD __forceinline__ void set_status(int* st, int code) {
+#ifdef __CUDA_ARCH__
+  atomicCAS(st, 0, code);
+#else
+  if (*st == 0) *st = code;
+#endif
+}
 
 // --- GG(Z,CEX): ELEMENTARY_FNS.f90:31-81 ----------------------------------
-__device__ __noinline__ cplx GG(cplx Z, cplx CEX) {
+NB_HD __noinline__ cplx GG(cplx Z, cplx CEX) {
   const cplx IPI = mk(0., 3.14159265);
   if (Z.re + 16. <= 0.) {
     cplx Y = 1. / Z;
@@ -74,17 +80,17 @@ __device__ __noinline__ cplx GG(cplx Z, cplx CEX) {
 }
 
 // integer part of a monotone log10 expression, made exact by thresholds
-__device__ __forceinline__ int stencil_adjust(double x, const double* thr, int k) {
+NB_HD __forceinline__ int stencil_adjust(double x, const double* thr, int k) {
   k = max(0, min(k, 47));
 #pragma unroll 1
-  for (int it = 0; it < 4 && k < 47 && x >= __ldg(thr + k + 1); ++it) ++k;
+  for (int it = 0; it < 4 && k < 47 && x >= NB_LDG(thr + k + 1); ++it) ++k;
 #pragma unroll 1
-  for (int it = 0; it < 4 && k > 0 && x < __ldg(thr + k); ++it) --k;
+  for (int it = 0; it < 4 && k > 0 && x < NB_LDG(thr + k); ++it) --k;
   return k;
 }
 
 // KJ of COMPUTE_GREEN_INFD.f90:292-298 (AKZ in (-16, -1.5e-6])
-__device__ __forceinline__ int stencil_kj(double AKZ, const StencilThresholds* T) {
+NB_HD __forceinline__ int stencil_kj(double AKZ, const StencilThresholds* T) {
   double x = -AKZ;
   int k;
   if (AKZ < -1.E-2) k = stencil_adjust(x, T->kj8, (int)(8. * (log10(x) + 4.5)));
@@ -94,7 +100,7 @@ __device__ __forceinline__ int stencil_kj(double AKZ, const StencilThresholds* T
 }
 
 // KI of COMPUTE_GREEN_INFD.f90:299-305
-__device__ __forceinline__ int stencil_ki(double AKR, const StencilThresholds* T) {
+NB_HD __forceinline__ int stencil_ki(double AKR, const StencilThresholds* T) {
   int k;
   if (AKR < 1.) {
     double y = XADD(AKR, 1.E-20);
@@ -117,13 +123,13 @@ struct Stencil {
   double L1, L2, L3;
 };
 
-__device__ __forceinline__ double4 ldg4(const double4* p) {
+NB_HD __forceinline__ double4 ldg4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);
-  const double2 a = __ldg(q), b = __ldg(q + 1);
+  const double2 a = NB_LDG(q), b = NB_LDG(q + 1);
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
-__device__ __forceinline__ void stencil_coeffs(const double4* lag, int K, double u, Stencil& s) {
+NB_HD __forceinline__ void stencil_coeffs(const double4* lag, int K, double u, Stencil& s) {
   const double4 p = ldg4(lag + 2 * K), q = ldg4(lag + 2 * K + 1);
   s.K = K;
   s.L1 = ((u - p.y) * (u - p.z)) * p.w;
@@ -131,15 +137,15 @@ __device__ __forceinline__ void stencil_coeffs(const double4* lag, int K, double
   s.L3 = ((u - p.x) * (u - p.y)) * q.y;
 }
 
-__device__ __forceinline__ void stencil_x(const GreenCtx& g, double AKR, Stencil& s) {
+NB_HD __forceinline__ void stencil_x(const GreenCtx& g, double AKR, Stencil& s) {
   stencil_coeffs(g.xlag, stencil_ki(AKR, g.thr), AKR, s);
 }
-__device__ __forceinline__ void stencil_z(const GreenCtx& g, double AKZ, Stencil& s) {
+NB_HD __forceinline__ void stencil_z(const GreenCtx& g, double AKZ, Stencil& s) {
   stencil_coeffs(g.zlag, stencil_kj(AKZ, g.thr), AKZ, s);
 }
 
 // 3x3 Lagrange interpolation of the four tables (:306-319, :345-352)
-__device__ __forceinline__ double4 interp4(const GreenCtx& g, const Stencil& sx, const Stencil& sz) {
+NB_HD __forceinline__ double4 interp4(const GreenCtx& g, const Stencil& sx, const Stencil& sz) {
   double4 r = make_double4(0., 0., 0., 0.);
   const double zl[3] = {sz.L1, sz.L2, sz.L3};
 #pragma unroll
@@ -165,7 +171,7 @@ struct RankineOut {
 };
 
 // exact edge-sum panel integral and gradient for one image (:99-174)
-__device__ __noinline__ void rankine_near(double XOI, double YOI, double ZOI, const PanelRec& P, int MY, int MZ,
+NB_HD __noinline__ void rankine_near(double XOI, double YOI, double ZOI, const PanelRec& P, int MY, int MZ,
                                           double DHMH, double& AIJS, double& VXS, double& VYS, double& VZS) {
   double TXN[5], TYN[5], TZN[5], RR[5], DRX[5], DRY[5], DRZ[5];
 #pragma unroll
@@ -235,7 +241,7 @@ __device__ __noinline__ void rankine_near(double XOI, double YOI, double ZOI, co
 // class + takes (1, -MK, -MK, 1), class - takes (1, -MK, MK, -1) of the four
 // (VAVINFD/VAVFD combination, COMPUTE_GREEN_INFD.f90:176-216).
 template <bool FD>
-__device__ __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI, double YGI, double ZGI, bool self,
+NB_HD __forceinline__ void rankine(const GreenCtx& g, double DH, double XGI, double YGI, double ZGI, bool self,
                                         const PanelRec& P, RankineOut& o, bool clip = true) {
   const double QPI = 4. * 3.141592653589793;
   const double DPI = 2. * 3.141592653589793;
@@ -293,7 +299,7 @@ struct WaveJJ {
 };
 
 // --- VNSINFD free-surface-panel branch (COMPUTE_GREEN_INFD.f90:385-453) ---
-__device__ __noinline__ void wave_infd_fs(const OmegaParams& om, double XGI, double YGI, double ZMIII, int BX,
+NB_HD __noinline__ void wave_infd_fs(const OmegaParams& om, double XGI, double YGI, double ZMIII, int BX,
                                           const PanelRec& P, WaveJJ& w) {
   const double EPS = 0.0001;
   const double AK0 = om.k0;
@@ -344,7 +350,7 @@ __device__ __noinline__ void wave_infd_fs(const OmegaParams& om, double XGI, dou
 
 // --- VNSINFD tabulated branch, both reflections (:271-382) ----------------
 // AKZ depends on the depths only, so its stencil is shared by BX = +1 and -1.
-__device__ __forceinline__ void wave_infd_pair(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
+NB_HD __forceinline__ void wave_infd_pair(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
                                                double ZMIII, const PanelRec& P, int NJJ, WaveJJ* w) {
   const double PI = 3.141592653589793, PI4 = 0.7853981633974483, DPI = 2. * PI, EPS = 0.0001;
   const double AK0 = om.k0;
@@ -421,7 +427,7 @@ __device__ __forceinline__ void wave_infd_pair(const GreenCtx& g, const OmegaPar
 
 // --- VSD: exact Rankine panel integral used by the FD free-surface branch --
 // (COMPUTE_GREEN_FD.f90:1514-1609)
-__device__ __noinline__ void vsd(const PanelRec& P, int JJ, double XGI, double YGI, double ZIG, double& FS, double& VX,
+NB_HD __noinline__ void vsd(const PanelRec& P, int JJ, double XGI, double YGI, double ZIG, double& FS, double& VX,
                                  double& VY, double& VZ) {
   const double QPI = 4. * 4. * atan(1.);
   const int MJJ = (JJ & 1) ? 1 : -1;
@@ -490,7 +496,7 @@ __device__ __noinline__ void vsd(const PanelRec& P, int JJ, double XGI, double Y
 // zeroed while CINT_FD filled only its local copies (COMPUTE_GREEN_FD.f90:874),
 // so it contributes exactly zero and is skipped; the exponential images (VSD)
 // carry the whole term.
-__device__ __noinline__ void wave_fd_fs(const OmegaParams& om, double XGI, double YGI, double ZMIII, int JJ,
+NB_HD __noinline__ void wave_fd_fs(const OmegaParams& om, double XGI, double YGI, double ZMIII, int JJ,
                                         const PanelRec& P, WaveJJ& w) {
   const double H = om.h;
   w = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
@@ -516,7 +522,7 @@ struct FdImage {
   double PD1Z, PD2Z, VZ2, PD1X, VR2, PSR;
 };
 
-__device__ __forceinline__ void fd_image(const GreenCtx& g, double AM0, double AKR, double RRR, double ZZZ, double AKZ,
+NB_HD __forceinline__ void fd_image(const GreenCtx& g, double AM0, double AKR, double RRR, double ZZZ, double AKZ,
                                          const Stencil& sx, const Stencil& sz, bool tab, double PSK, double SCK,
                                          double SCDS, double SSDS, FdImage& m) {
   const double PI = 3.141592653589793, EPS = 0.0001;
@@ -556,7 +562,7 @@ __device__ __forceinline__ void fd_image(const GreenCtx& g, double AM0, double A
 // The four image depths Z1..Z4 (and their AKZ stencils) depend on the depths
 // only and are shared by BX = +1 and -1. |Z1| is the smallest of the four,
 // so AKZ1 <= -16 puts every image in the far branch.
-__device__ __forceinline__ void wave_fd_pair(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
+NB_HD __forceinline__ void wave_fd_pair(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI,
                                              double ZMIII, const PanelRec& P, int NJJ, WaveJJ* w) {
   const double PI = 3.141592653589793, PI4 = 0.7853981633974483, DPI = 2. * PI, EPS = 0.0001;
   const double AM0 = om.k0, H = om.h;
@@ -646,7 +652,7 @@ __device__ __forceinline__ void wave_fd_pair(const GreenCtx& g, const OmegaParam
 // to the symmetry classes (+ both, - with the mirror subtracted) of the two
 // orders as it is computed. Returns false (and leaves the outputs) when an
 // image depth is too shallow for the tables (AKZ > -1.5e-6).
-__device__ __forceinline__ void wave_sym_add(const OmegaParams& om, double aire, double XN, double YN, double ZN,
+NB_HD __forceinline__ void wave_sym_add(const OmegaParams& om, double aire, double XN, double YN, double ZN,
                                              double sgn, double F1, double F2, double X1, double X2, double ZA1,
                                              double ZA2, double CVX, double CVY, PairOut& o) {
   const double COF1 = om.coe3 * aire, COF2 = om.coe4 * aire;
@@ -665,7 +671,7 @@ __device__ __forceinline__ void wave_sym_add(const OmegaParams& om, double aire,
   o.dm_im += sgn * D2;
 }
 
-__device__ __forceinline__ bool wave_fd_sym(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
+NB_HD __forceinline__ bool wave_fd_sym(const GreenCtx& g, const OmegaParams& om, const PanelRec& PI,
                                             const PanelRec& PJ, int NJJ, bool both, PairOut& oij, PairOut& oji) {
   const double PI_ = 3.141592653589793, PI4 = 0.7853981633974483, DPI = 2. * PI_, EPS = 0.0001;
   const double AM0 = om.k0, H = om.h;
@@ -774,7 +780,7 @@ struct ImageSums {
   double fs[2], sa[2], m1[2], m2[2], dx[2], dy[2];
 };
 
-__device__ __forceinline__ void fd_image_sums(const GreenCtx& g, double H, const double* ambda, const double* ar,
+NB_HD __forceinline__ void fd_image_sums(const GreenCtx& g, double H, const double* ambda, const double* ar,
                                               int nexp1, double XI, double YI, double ZI, double XJ, double YJ,
                                               double ZJ, int NJJ, ImageSums& o) {
   const double H2 = XMUL(2., H), H4 = XMUL(4., H);
@@ -833,7 +839,7 @@ struct RealOut {
 };
 
 template <bool FD>
-__device__ __forceinline__ void pair_rankine(const GreenCtx& g, const OmegaParams& om, const double* ambda,
+NB_HD __forceinline__ void pair_rankine(const GreenCtx& g, const OmegaParams& om, const double* ambda,
                                              const double* ar, double XGI, double YGI, double ZGI, double XNI,
                                              double YNI, double ZNI, bool self, const PanelRec& P, RealOut& out) {
   RankineOut r;
@@ -847,7 +853,7 @@ __device__ __forceinline__ void pair_rankine(const GreenCtx& g, const OmegaParam
 // Wave sums of both reflections -> wave parts of D+/-, S+/- of one pair
 // (collocation normal XNI, YNI, ZNI; source panel area `aire`).
 template <bool FD>
-__device__ __forceinline__ void wave_combine(const OmegaParams& om, double aire, int NJJ, WaveJJ* w, double XNI,
+NB_HD __forceinline__ void wave_combine(const OmegaParams& om, double aire, int NJJ, WaveJJ* w, double XNI,
                                              double YNI, double ZNI, PairOut& out) {
   if (NJJ == 1) w[1] = WaveJJ{0, 0, 0, 0, 0, 0, 0, 0};
   // VNSINFD (:456-500) scales the wave sums by K A / 2pi^2, K A / 2pi (and K
@@ -883,7 +889,7 @@ __device__ __forceinline__ void wave_combine(const OmegaParams& om, double aire,
 
 // --- wave part of one pair, both symmetry classes ----------------------------
 template <bool FD>
-__device__ __forceinline__ void pair_wave(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI, double ZGI,
+NB_HD __forceinline__ void pair_wave(const GreenCtx& g, const OmegaParams& om, double XGI, double YGI, double ZGI,
                                           double XNI, double YNI, double ZNI, const PanelRec& P, PairOut& out) {
   const int NJJ = g.nsymy + 1;
   double ZMIII = ZGI;

@@ -1,0 +1,216 @@
+// CPU check of the assembly's pair functions (test infrastructure).
+//
+// The Rankine and wave functions that the assembly kernels call for each pair
+// of panels (nemoh_b200/csrc/green.cuh and assembly.cuh) are compiled here for
+// the host and applied to every pair the way the two assembly passes apply
+// them: the Rankine pass writes the real parts of D+/- and S+/- for every
+// ordered pair (collocation I, source J); the wave pass takes each unordered
+// pair I <= J once, evaluates both orders together when both panels are
+// submerged and each order on its own otherwise, adds the results to the real
+// parts and writes the imaginary parts. The per-frequency setup takes the same
+// host functions as the library (fd_setup.cpp: X0, LISC, CINT, table nodes,
+// stencil thresholds) in the order of SOLVE_BEM.f90:62-84; the tabulated wave
+// integrals come from the caller (the oracle's CREK tables), since the
+// library computes them with a kernel. The tests compare the matrices with
+// the oracle's on the same mesh and frequencies.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../nemoh_b200/csrc/assembly.cuh"
+#include "../../nemoh_b200/csrc/fd_setup.h"
+
+using namespace nb200;
+
+namespace {
+
+const double kPI = 4. * std::atan(1.);
+
+// per-frequency parameters (SOLVE_BEM.f90:62-84, SOLVE_BEM_INFD_DIRECT.f90:79,
+// SOLVE_BEM_FD_DIRECT.f90:99, COMPUTE_GREEN_FD.f90:259-268); 0 or a status code
+int frequency_setup(double W, double g, double depth, double gm, int* nq_state, OmegaParams& om) {
+  std::memset(&om, 0, sizeof om);
+  om.w = W;
+  om.h = depth;
+  const double kwave = W * W / g;
+  const bool fd = !((depth == 0.) || (kwave * depth >= 20));
+  if (std::fabs(W) < 1.E-4) return ST_OMEGA;
+  double qq[MAX_NQ + 2], cq[MAX_NQ + 2];
+  if (!fd) {
+    om.k0 = W * W / g;
+    const int n = theta_quadrature(om.k0 * gm, qq, cq);
+    om.nq = std::min(*nq_state, n);
+    for (int i = 1; i <= om.nq; ++i) {
+      om.cq[i] = cq[i];
+      om.ct[i] = std::cos(qq[i]);
+      om.st[i] = std::sin(qq[i]);
+    }
+    return 0;
+  }
+  om.fd = 1;
+  double AMH;
+  int st = finite_depth_root(W * W * depth / g, &AMH);
+  if (st) return st;
+  const double AKH = AMH * std::tanh(AMH), AM0 = AMH / depth;
+  om.k0 = AM0;
+  om.amh = AMH;
+  *nq_state = theta_quadrature(AM0 * gm, qq, cq);
+  int nexp = 0;
+  st = exponential_fit(AKH, AMH, &nexp, om.ambda, om.ar);
+  if (st) return st;
+  om.nexp = nexp;
+  om.ambda[nexp + 1] = 0.;
+  om.ar[nexp + 1] = 2.;
+  const double A = (AMH + AKH) * (AMH + AKH) / (depth * (AMH * AMH - AKH * AKH + AKH));
+  const double ADPI2 = -A / (8. * kPI * kPI), ADPI = -A / (8 * kPI);
+  om.coe1 = ADPI2 / AM0;
+  om.coe2 = ADPI / AM0;
+  om.coe3 = ADPI2;
+  om.coe4 = ADPI;
+  return 0;
+}
+
+// GM: largest horizontal node-pair distance including the y-mirror
+// (SOLVE_BEM_INFD_DIRECT.f90:66-76)
+double largest_distance(int np, int nsymy, const double* xyz) {
+  double best = 0.;
+  for (int i = 0; i < np; ++i)
+    for (int j = i + 1; j < np; ++j) {
+      const double dx = XSUB(xyz[3 * j], xyz[3 * i]);
+      for (int jj = 0; jj <= nsymy; ++jj) {
+        const double dy = XSUB(xyz[3 * i + 1], xyz[3 * j + 1] * (jj ? -1. : 1.));
+        best = std::fmax(best, XSQRT(XADD(XMUL(dx, dx), XMUL(dy, dy))));
+      }
+    }
+  return best;
+}
+
+// 3-node Lagrange stencils of one table axis: nodes and reciprocal denominators
+void stencils(const double* x, int n, double* out) {
+  for (int k = 2; k < n; ++k) {
+    const double a = x[k - 1], b = x[k], c = x[k + 1];
+    double* q = out + 8 * k;
+    q[0] = a;
+    q[1] = b;
+    q[2] = c;
+    q[3] = 1. / ((a - b) * (a - c));
+    q[4] = 1. / ((b - c) * (b - a));
+    q[5] = 1. / ((c - a) * (c - b));
+  }
+}
+
+void put(double* m, long long q, double re, double im) {
+  m[2 * q] = re;
+  m[2 * q + 1] = im;
+}
+
+template <bool FD>
+void assemble(const GreenCtx& g, const OmegaParams& om, const std::vector<PanelRec>& P, double* dp, double* dm,
+              double* sp, double* sm) {
+  const int N = (int)P.size(), NJJ = g.nsymy + 1;
+  for (int J = 0; J < N; ++J)
+    for (int I = 0; I < N; ++I) {
+      RealOut r;
+      pair_rankine<FD>(g, om, om.ambda, om.ar, P[I].xg, P[I].yg, P[I].zg, P[I].xn, P[I].yn, P[I].zn, I == J, P[J], r);
+      const long long q = I + (long long)N * J;
+      put(dp, q, r.dp, 0.);
+      put(sp, q, r.sp, 0.);
+      put(dm, q, r.dm, 0.);
+      put(sm, q, r.sm, 0.);
+    }
+  auto add = [&](long long q, const PairOut& o) {
+    put(dp, q, dp[2 * q] + o.dp_re, o.dp_im);
+    put(sp, q, sp[2 * q] + o.sp_re, o.sp_im);
+    put(dm, q, dm[2 * q] + o.dm_re, o.dm_im);
+    put(sm, q, sm[2 * q] + o.sm_re, o.sm_im);
+  };
+  for (int J = 0; J < N; ++J)
+    for (int I = 0; I <= J; ++I) {
+      const PanelRec &PI = P[I], &PJ = P[J];
+      const bool both = I != J;
+      PairOut oij{}, oji{};
+      if (PI.zg < g.zer && PJ.zg < g.zer) {
+        if (FD) {
+          if (!wave_fd_sym(g, om, PI, PJ, NJJ, both, oij, oji)) {
+            set_status(g.status, ST_AKZ_UNDEFINED);
+            oij = oji = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
+          }
+          fd_images_pair(g, om, PI, PJ, NJJ, both, oij, oji);
+        } else {
+          wave_infd_both(g, om, PI, PJ, NJJ, both, oij, oji);
+        }
+      } else {
+        pair_wave_ordered<FD>(g, om, PI, PJ, oij);
+        if (both) pair_wave_ordered<FD>(g, om, PJ, PI, oji);
+      }
+      add(I + (long long)N * J, oij);
+      if (both) add(J + (long long)N * I, oji);
+    }
+}
+
+}  // namespace
+
+// geo: 8 x nfa (XN, YN, ZN, XG, YG, ZG, AIRE, TDIS); m1234: 4 x nfa, 1-based;
+// apd: {APD1X, APD1Z, APD2X, APD2Z} as 4 x 328 x 46 (column-major per table);
+// nq_state: the reference's NQ, in and out. Outputs: complex n x n,
+// column-major; without symmetry dm = dp and sm = sp. Returns 0 or a status.
+extern "C" int host_pairs_assemble(int np, int nfa, int nsymy, const double* xyz, const int* m1234, const double* geo,
+                                   double zer, const double* apd, double g, double depth, double omega,
+                                   int* nq_state, int* fd_mode, double* dp, double* dm, double* sp, double* sm) {
+  std::vector<PanelRec> P(nfa);
+  for (int i = 0; i < nfa; ++i) {
+    PanelRec& p = P[i];
+    p.xn = geo[0 * nfa + i];
+    p.yn = geo[1 * nfa + i];
+    p.zn = geo[2 * nfa + i];
+    p.xg = geo[3 * nfa + i];
+    p.yg = geo[4 * nfa + i];
+    p.zg = geo[5 * nfa + i];
+    p.aire = geo[6 * nfa + i];
+    p.tdis = geo[7 * nfa + i];
+    for (int v = 0; v < 4; ++v) {
+      const int k = m1234[4 * i + v] - 1;
+      p.vx[v] = xyz[3 * k];
+      p.vy[v] = xyz[3 * k + 1];
+      p.vz[v] = xyz[3 * k + 2];
+    }
+  }
+  std::vector<double> xr(TAB_IR + 2, 0.), xz(TAB_JZ + 2, 0.);
+  table_nodes(xr.data(), xz.data());
+  std::vector<double4> tab((size_t)TAB_IR * TAB_JZ);
+  for (size_t q = 0; q < tab.size(); ++q)
+    tab[q] = make_double4(apd[q], apd[tab.size() + q], apd[2 * tab.size() + q], apd[3 * tab.size() + q]);
+  std::vector<double> lag(8 * (size_t)(TAB_IR + 2 + TAB_JZ + 2), 0.);
+  stencils(xr.data(), TAB_IR, lag.data());
+  stencils(xz.data(), TAB_JZ, lag.data() + 8 * (TAB_IR + 2));
+  StencilThresholds thr;
+  stencil_thresholds(&thr);
+  double t = 1.E-8;   // largest double whose correctly rounded square root is <= 1e-4
+  while (std::sqrt(std::nextafter(t, 1.)) <= 1.E-4) t = std::nextafter(t, 1.);
+  while (std::sqrt(t) > 1.E-4) t = std::nextafter(t, 0.);
+  int status = 0;
+  GreenCtx gc;
+  gc.ro_eps2 = t;
+  gc.xr = xr.data();
+  gc.xz = xz.data();
+  gc.apd = tab.data();
+  gc.xlag = reinterpret_cast<const double4*>(lag.data());
+  gc.zlag = reinterpret_cast<const double4*>(lag.data()) + 2 * (TAB_IR + 2);
+  gc.thr = &thr;
+  gc.zer = zer;
+  gc.nsymy = nsymy;
+  gc.status = &status;
+  OmegaParams om;
+  const double T = 2. * kPI / omega;
+  const int st = frequency_setup(2. * kPI / T, g, depth, largest_distance(np, nsymy, xyz), nq_state, om);
+  if (st) return st;
+  if (om.fd) assemble<true>(gc, om, P, dp, dm, sp, sm);
+  else assemble<false>(gc, om, P, dp, dm, sp, sm);
+  if (!nsymy) {   // one symmetry class: the library keeps D and S only
+    std::memcpy(dm, dp, sizeof(double) * 2 * (size_t)nfa * nfa);
+    std::memcpy(sm, sp, sizeof(double) * 2 * (size_t)nfa * nfa);
+  }
+  if (fd_mode) *fd_mode = om.fd;
+  return status;
+}
