@@ -17,7 +17,7 @@ namespace nb200 {
 // VVG (COMPUTE_GREEN_FREESURFACE.f90:911-997), single-layer part: exact
 // integral over panel P (reflection JJ) at (XPO, YPO, ZPO); the reference's
 // literal 12.5663706 for 4 pi is kept
-__device__ __noinline__ double vvg_fs(const PanelRec& P, int JJ, double XPO, double YPO, double ZPO) {
+NB_HD __noinline__ double vvg_fs(const PanelRec& P, int JJ, double XPO, double YPO, double ZPO) {
   const int MJJ = (JJ & 1) ? 1 : -1;
   const double dx = XSUB(XPO, P.xg), dy = XSUB(YPO, P.yg * MJJ), dz = XSUB(ZPO, P.zg);
   const double RO = XSQRT(XADD(XADD(XMUL(dx, dx), XMUL(dy, dy)), XMUL(dz, dz)));
@@ -52,7 +52,7 @@ __device__ __noinline__ double vvg_fs(const PanelRec& P, int JJ, double XPO, dou
 
 // single-layer values of panel P at a field point (XPO, YPO, ZPO)
 template <bool FD>
-__device__ __forceinline__ void field_green(const GreenCtx& g, const OmegaParams& om, double XPO, double YPO,
+NB_HD __forceinline__ void field_green(const GreenCtx& g, const OmegaParams& om, double XPO, double YPO,
                                             double ZPO, const PanelRec& P, double& SP1, double& SP2, double& SM1,
                                             double& SM2) {
   const int NJJ = g.nsymy + 1;

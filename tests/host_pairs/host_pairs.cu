@@ -2,8 +2,8 @@
 //
 // The Rankine and wave functions that the assembly kernels call for each pair
 // of panels (nemoh_b200/csrc/green.cuh and assembly.cuh) are compiled here for
-// the host and applied to every pair the way the two assembly passes apply
-// them: the Rankine pass writes the real parts of D+/- and S+/- for every
+// the host and applied the way the kernels apply them. Assembly: the Rankine and
+// wave passes: the Rankine pass writes the real parts of D+/- and S+/- for every
 // ordered pair (collocation I, source J); the wave pass takes each unordered
 // pair I <= J once, evaluates both orders together when both panels are
 // submerged and each order on its own otherwise, adds the results to the real
@@ -11,14 +11,17 @@
 // host functions as the library (fd_setup.cpp: X0, LISC, CINT, table nodes,
 // stencil thresholds) in the order of SOLVE_BEM.f90:62-84; the tabulated wave
 // integrals come from the caller (the oracle's CREK tables), since the
-// library computes them with a kernel. The tests compare the matrices with
-// the oracle's on the same mesh and frequencies.
+// library computes them with a kernel. Free surface: the field-point Green
+// functions of every panel at every point, contracted with the source
+// strengths as the free-surface kernel does, ETA = i W / G PHI. The tests
+// compare both with the oracle's on the same mesh and frequencies.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "../../nemoh_b200/csrc/assembly.cuh"
+#include "../../nemoh_b200/csrc/freesurface.cuh"
 #include "../../nemoh_b200/csrc/fd_setup.h"
 
 using namespace nb200;
@@ -149,6 +152,90 @@ void assemble(const GreenCtx& g, const OmegaParams& om, const std::vector<PanelR
     }
 }
 
+// Mesh, tables and Green-function context of one call
+struct HostCtx {
+  std::vector<PanelRec> P;
+  std::vector<double> xr, xz, lag;
+  std::vector<double4> tab;
+  StencilThresholds thr;
+  int status = 0;
+  double gm = 0.;
+  GreenCtx gc;
+
+  HostCtx(int np, int nfa, int nsymy, const double* xyz, const int* m1234, const double* geo, double zer,
+          const double* apd)
+      : P(nfa), xr(TAB_IR + 2, 0.), xz(TAB_JZ + 2, 0.), lag(8 * (size_t)(TAB_IR + 2 + TAB_JZ + 2), 0.),
+        tab((size_t)TAB_IR * TAB_JZ) {
+    for (int i = 0; i < nfa; ++i) {
+      PanelRec& p = P[i];
+      p.xn = geo[0 * nfa + i];
+      p.yn = geo[1 * nfa + i];
+      p.zn = geo[2 * nfa + i];
+      p.xg = geo[3 * nfa + i];
+      p.yg = geo[4 * nfa + i];
+      p.zg = geo[5 * nfa + i];
+      p.aire = geo[6 * nfa + i];
+      p.tdis = geo[7 * nfa + i];
+      for (int v = 0; v < 4; ++v) {
+        const int k = m1234[4 * i + v] - 1;
+        p.vx[v] = xyz[3 * k];
+        p.vy[v] = xyz[3 * k + 1];
+        p.vz[v] = xyz[3 * k + 2];
+      }
+    }
+    table_nodes(xr.data(), xz.data());
+    for (size_t q = 0; q < tab.size(); ++q)
+      tab[q] = make_double4(apd[q], apd[tab.size() + q], apd[2 * tab.size() + q], apd[3 * tab.size() + q]);
+    stencils(xr.data(), TAB_IR, lag.data());
+    stencils(xz.data(), TAB_JZ, lag.data() + 8 * (TAB_IR + 2));
+    stencil_thresholds(&thr);
+    double t = 1.E-8;   // largest double whose correctly rounded square root is <= 1e-4
+    while (std::sqrt(std::nextafter(t, 1.)) <= 1.E-4) t = std::nextafter(t, 1.);
+    while (std::sqrt(t) > 1.E-4) t = std::nextafter(t, 0.);
+    gm = largest_distance(np, nsymy, xyz);
+    gc.ro_eps2 = t;
+    gc.xr = xr.data();
+    gc.xz = xz.data();
+    gc.apd = tab.data();
+    gc.xlag = reinterpret_cast<const double4*>(lag.data());
+    gc.zlag = reinterpret_cast<const double4*>(lag.data()) + 2 * (TAB_IR + 2);
+    gc.thr = &thr;
+    gc.zer = zer;
+    gc.nsymy = nsymy;
+    gc.status = &status;
+  }
+};
+
+// ETA at the points for the source strengths of nprob problems (column-major
+// nfa x nprob complex), as the free-surface kernel sums them
+template <bool FD>
+void free_surface(const GreenCtx& g, const OmegaParams& om, const std::vector<PanelRec>& P, double W, double grav,
+                  int npts, const double* xy, int nprob, const double* zigb, const double* zigs, double* eta) {
+  const int N = (int)P.size();
+  for (int q = 0; q < npts; ++q)
+    for (int p = 0; p < nprob; ++p) {
+      double pot1 = 0., pot2 = 0.;
+      for (int J = 0; J < N; ++J) {
+        double SP1, SP2, SM1, SM2;
+        field_green<FD>(g, om, xy[2 * q], xy[2 * q + 1], 0., P[J], SP1, SP2, SM1, SM2);
+        const double bx = zigb[2 * ((size_t)p * N + J)], by = zigb[2 * ((size_t)p * N + J) + 1];
+        if (g.nsymy == 0) {
+          pot1 += bx * SP1 - by * SP2;
+          pot2 += bx * SP2 + by * SP1;
+        } else {
+          const double sx = zigs[2 * ((size_t)p * N + J)], sy = zigs[2 * ((size_t)p * N + J) + 1];
+          const double C1 = bx * (SP1 + SM1) + sx * (SP1 - SM1), D1 = by * (SP2 + SM2) + sy * (SP2 - SM2);
+          const double C2 = bx * (SP2 + SM2) + sx * (SP2 - SM2), D2 = by * (SP1 + SM1) + sy * (SP1 - SM1);
+          pot1 += (C1 - D1) * 0.5;
+          pot2 += (C2 + D2) * 0.5;
+        }
+      }
+      // ETA = i W / G PHI
+      eta[2 * ((size_t)npts * p + q)] = -(W / grav) * pot2;
+      eta[2 * ((size_t)npts * p + q) + 1] = (W / grav) * pot1;
+    }
+}
+
 }  // namespace
 
 // geo: 8 x nfa (XN, YN, ZN, XG, YG, ZG, AIRE, TDIS); m1234: 4 x nfa, 1-based;
@@ -158,59 +245,39 @@ void assemble(const GreenCtx& g, const OmegaParams& om, const std::vector<PanelR
 extern "C" int host_pairs_assemble(int np, int nfa, int nsymy, const double* xyz, const int* m1234, const double* geo,
                                    double zer, const double* apd, double g, double depth, double omega,
                                    int* nq_state, int* fd_mode, double* dp, double* dm, double* sp, double* sm) {
-  std::vector<PanelRec> P(nfa);
-  for (int i = 0; i < nfa; ++i) {
-    PanelRec& p = P[i];
-    p.xn = geo[0 * nfa + i];
-    p.yn = geo[1 * nfa + i];
-    p.zn = geo[2 * nfa + i];
-    p.xg = geo[3 * nfa + i];
-    p.yg = geo[4 * nfa + i];
-    p.zg = geo[5 * nfa + i];
-    p.aire = geo[6 * nfa + i];
-    p.tdis = geo[7 * nfa + i];
-    for (int v = 0; v < 4; ++v) {
-      const int k = m1234[4 * i + v] - 1;
-      p.vx[v] = xyz[3 * k];
-      p.vy[v] = xyz[3 * k + 1];
-      p.vz[v] = xyz[3 * k + 2];
-    }
-  }
-  std::vector<double> xr(TAB_IR + 2, 0.), xz(TAB_JZ + 2, 0.);
-  table_nodes(xr.data(), xz.data());
-  std::vector<double4> tab((size_t)TAB_IR * TAB_JZ);
-  for (size_t q = 0; q < tab.size(); ++q)
-    tab[q] = make_double4(apd[q], apd[tab.size() + q], apd[2 * tab.size() + q], apd[3 * tab.size() + q]);
-  std::vector<double> lag(8 * (size_t)(TAB_IR + 2 + TAB_JZ + 2), 0.);
-  stencils(xr.data(), TAB_IR, lag.data());
-  stencils(xz.data(), TAB_JZ, lag.data() + 8 * (TAB_IR + 2));
-  StencilThresholds thr;
-  stencil_thresholds(&thr);
-  double t = 1.E-8;   // largest double whose correctly rounded square root is <= 1e-4
-  while (std::sqrt(std::nextafter(t, 1.)) <= 1.E-4) t = std::nextafter(t, 1.);
-  while (std::sqrt(t) > 1.E-4) t = std::nextafter(t, 0.);
-  int status = 0;
-  GreenCtx gc;
-  gc.ro_eps2 = t;
-  gc.xr = xr.data();
-  gc.xz = xz.data();
-  gc.apd = tab.data();
-  gc.xlag = reinterpret_cast<const double4*>(lag.data());
-  gc.zlag = reinterpret_cast<const double4*>(lag.data()) + 2 * (TAB_IR + 2);
-  gc.thr = &thr;
-  gc.zer = zer;
-  gc.nsymy = nsymy;
-  gc.status = &status;
+  HostCtx h(np, nfa, nsymy, xyz, m1234, geo, zer, apd);
   OmegaParams om;
   const double T = 2. * kPI / omega;
-  const int st = frequency_setup(2. * kPI / T, g, depth, largest_distance(np, nsymy, xyz), nq_state, om);
+  const int st = frequency_setup(2. * kPI / T, g, depth, h.gm, nq_state, om);
   if (st) return st;
-  if (om.fd) assemble<true>(gc, om, P, dp, dm, sp, sm);
-  else assemble<false>(gc, om, P, dp, dm, sp, sm);
+  if (om.fd) assemble<true>(h.gc, om, h.P, dp, dm, sp, sm);
+  else assemble<false>(h.gc, om, h.P, dp, dm, sp, sm);
   if (!nsymy) {   // one symmetry class: the library keeps D and S only
     std::memcpy(dm, dp, sizeof(double) * 2 * (size_t)nfa * nfa);
     std::memcpy(sm, sp, sizeof(double) * 2 * (size_t)nfa * nfa);
   }
   if (fd_mode) *fd_mode = om.fd;
-  return status;
+  return h.status;
+}
+
+// Free-surface elevation at npts points (x, y, 0) (xy: npts x 2, row-major) of
+// nprob problems solved at `period` (zigb, zigs: nfa x nprob complex; zigs
+// unused without symmetry); eta: npts x nprob complex. The frequency setup
+// leaves the NQ state as it is (nq_state is read only).
+extern "C" int host_pairs_free_surface(int np, int nfa, int nsymy, const double* xyz, const int* m1234,
+                                       const double* geo, double zer, const double* apd, double g, double depth,
+                                       double period, int nq_state, int npts, const double* xy, int nprob,
+                                       const double* zigb, const double* zigs, double* eta) {
+  HostCtx h(np, nfa, nsymy, xyz, m1234, geo, zer, apd);
+  OmegaParams om;
+  const double W = 2. * kPI / period;
+  int nq = nq_state;
+  const int st = frequency_setup(W, g, depth, h.gm, &nq, om);
+  if (st) return st;
+  // COMPUTE_POTENTIAL_DOMAIN.f90:46: deep-water forms when Depth = 0 or AMH >= 20
+  const double amh = om.fd ? om.amh : om.k0 * depth;
+  const bool fd = !((depth == 0.) || (amh >= 20));
+  if (fd) free_surface<true>(h.gc, om, h.P, W, g, npts, xy, nprob, zigb, zigs, eta);
+  else free_surface<false>(h.gc, om, h.P, W, g, npts, xy, nprob, zigb, zigs, eta);
+  return h.status;
 }

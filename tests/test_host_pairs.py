@@ -1,4 +1,4 @@
-"""CPU check of the assembly's pair functions.
+"""CPU check of the kernels' pair functions.
 
 The Rankine and wave functions that the assembly kernels call per pair of
 panels, compiled for the host (tests/host_pairs/host_pairs.cu) and applied to
@@ -6,8 +6,10 @@ every pair the way the two assembly passes do, against the oracle's influence
 matrices at the GPU parity test's tolerances: 1e-12 of each row's largest entry
 in deep water, 1e-10 in finite depth. Frequencies run in each case's order, so
 the free-surface-panel quadrature state NQ carries over as in the reference.
-This runs without a GPU; the same functions on the device are checked by the
-GPU parity tests."""
+Likewise the field-point Green functions of the free-surface kernel against the
+oracle's elevation for the same source strengths: 1e-9 of each problem's
+largest |ETA|. This runs without a GPU; the same functions on the device are
+checked by the GPU parity tests."""
 import ctypes
 import os
 import subprocess
@@ -22,8 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "nemoh_b200", "csrc")
 SRC = os.path.join(HERE, "host_pairs", "host_pairs.cu")
 LIB = os.path.join(HERE, "host_pairs", "_build", "libhost_pairs.so")
-DEPS = [SRC] + [os.path.join(CSRC, f) for f in ("common.cuh", "green.cuh", "assembly.cuh", "fd_setup.cpp",
-                                                "fd_setup.h")]
+DEPS = [SRC] + [os.path.join(CSRC, f) for f in ("common.cuh", "green.cuh", "assembly.cuh", "freesurface.cuh",
+                                                "fd_setup.cpp", "fd_setup.h")]
 _d = ctypes.POINTER(ctypes.c_double)
 _i = ctypes.POINTER(ctypes.c_int)
 
@@ -37,6 +39,9 @@ def _lib():
     L = ctypes.CDLL(LIB)
     L.host_pairs_assemble.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _i, _d, ctypes.c_double, _d,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, _i, _i, _d, _d, _d, _d]
+    L.host_pairs_free_surface.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _i, _d, ctypes.c_double, _d,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
     return L
 
 
@@ -71,3 +76,46 @@ def test_host_pair_functions_match_oracle(case):
             row = np.abs(b).max(axis=1, keepdims=True)
             err = np.abs(a - b) / row
             assert err.max() < tol, (case.name, w, err.max(), np.unravel_index(err.argmax(), err.shape))
+
+
+def _fs_points(case):
+    """A polar grid on z = 0 from just outside the waterline (tabulated wave
+    term) to 30 body radii (asymptotic form)."""
+    nodes = case.mesh.nodes
+    r0 = np.hypot(nodes[:, 0], nodes[:, 1]).max()
+    R, TH = np.meshgrid(r0 * np.array([1.15, 1.6, 3.0, 8.0, 30.0]), np.linspace(0.0, 2.0 * np.pi, 7)[:-1] + 0.1)
+    return np.ascontiguousarray(np.stack([(R * np.cos(TH)).ravel(), (R * np.sin(TH)).ravel()], axis=1))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_host_free_surface_functions_match_oracle(case):
+    from nemoh_b200 import cases as C
+    L = _lib()
+    m = case.mesh
+    n = m.npanels
+    o = G.oracle_for(case)
+    geo, zer = o.geometry()
+    geo = np.ascontiguousarray(geo)
+    _, _, apd = o.tables()
+    apd = np.ascontiguousarray(apd.transpose(0, 2, 1)).ravel()
+    nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+    panels = np.ascontiguousarray(m.panels, dtype=np.int32)
+    p = lambda a: a.ctypes.data_as(_d)
+    nv = C.body_conditions(case)
+    npb = len(case.betas_deg) + len(case.rad)
+    xy = _fs_points(case)
+    w_idx = len(case.omegas) - 1
+    T = 2 * np.pi / case.omegas[w_idx]
+    cols = [w_idx * npb, w_idx * npb + npb - 1]   # the first heading and the last DOF
+    res = [o.solve_problem(T, nv[:, j]) for j in cols]
+    zigb = np.asfortranarray(np.stack([r["zigb"] for r in res], axis=1))
+    zigs = np.asfortranarray(np.stack([r["zigs"] for r in res], axis=1))
+    eta = np.zeros((len(xy), len(cols)), dtype=np.complex128, order="F")
+    st = L.host_pairs_free_surface(len(nodes), n, m.isym, p(nodes), panels.ctypes.data_as(_i), p(geo), zer, p(apd),
+                                   case.g, case.depth, T, o.nq, len(xy), p(xy), len(cols), p(zigb), p(zigs), p(eta))
+    assert st == 0
+    eo = o.free_surface(T, xy, zigb, zigs if m.isym else None)
+    scale = np.abs(eo).max(axis=0)
+    assert np.all(scale > 0)
+    err = (np.abs(eta - eo) / scale).max()
+    assert err < 1e-9, (case.name, err)
