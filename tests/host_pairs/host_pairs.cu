@@ -13,8 +13,10 @@
 // integrals come from the caller (the oracle's CREK tables), since the
 // library computes them with a kernel. Free surface: the field-point Green
 // functions of every panel at every point, contracted with the source
-// strengths as the free-surface kernel does, ETA = i W / G PHI. The tests
-// compare both with the oracle's on the same mesh and frequencies.
+// strengths as the free-surface kernel does, ETA = i W / G PHI. Kochin: the
+// panel integrals of the Kochin kernel, contracted with the source strengths.
+// The tests compare all three with the oracle's on the same mesh and
+// frequencies.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -22,6 +24,7 @@
 
 #include "../../nemoh_b200/csrc/assembly.cuh"
 #include "../../nemoh_b200/csrc/freesurface.cuh"
+#include "../../nemoh_b200/csrc/kochin.cuh"
 #include "../../nemoh_b200/csrc/fd_setup.h"
 
 using namespace nb200;
@@ -280,4 +283,47 @@ extern "C" int host_pairs_free_surface(int np, int nfa, int nsymy, const double*
   if (fd) free_surface<true>(h.gc, om, h.P, W, g, npts, xy, nprob, zigb, zigs, eta);
   else free_surface<false>(h.gc, om, h.P, W, g, npts, xy, nprob, zigb, zigs, eta);
   return h.status;
+}
+
+// Kochin function H (ntheta x nprob complex) at the directions theta of
+// nprob problems solved at `period` (COMPUTE_KOCHIN.f90:25-152 with the wave
+// number of SOLVE_BEM.f90:62-84); yeff is taken as 0 on symmetric meshes.
+extern "C" int host_pairs_kochin(int nfa, int nsymy, const double* xyz, const int* m1234, const double* geo,
+                                 double g, double depth, double period, double xeff, double yeff, int ntheta,
+                                 const double* theta, int nprob, const double* zigb, const double* zigs, double* h) {
+  const double W = 2. * kPI / period;
+  double kwave = W * W / g;
+  if (!((depth == 0.) || (kwave * depth >= 20))) {
+    double AMH;
+    const int st = finite_depth_root(W * W * depth / g, &AMH);
+    if (st) return st;
+    kwave = AMH / depth;
+  }
+  const double ye = nsymy ? 0. : yeff;
+  std::vector<double> rows(6 * (size_t)nfa);   // XG, YG, ZG, XN, YN, ZN
+  for (int i = 0; i < nfa; ++i)
+    for (int r = 0; r < 3; ++r) {
+      rows[r * nfa + i] = geo[(3 + r) * nfa + i];
+      rows[(3 + r) * nfa + i] = geo[r * nfa + i];
+    }
+  const double q = 0.25 / 3.141592653589793;
+  for (int t = 0; t < ntheta; ++t) {
+    const double ct = std::cos(theta[t]), st = std::sin(theta[t]);
+    std::vector<cplx> zs(2 * (size_t)nfa);
+    for (int i = 0; i < nfa; ++i) {
+      zs[2 * i] = zs[2 * i + 1] = mk(0., 0.);
+      kochin_panel(xyz, m1234, rows.data(), nfa, nsymy, kwave, depth, xeff, ye, ct, st, i, &zs[2 * i]);
+    }
+    for (int p = 0; p < nprob; ++p) {
+      cplx acc = mk(0., 0.);
+      for (int i = 0; i < nfa; ++i) {
+        const size_t k = (size_t)p * nfa + i;
+        acc = acc + mk(zigb[2 * k], zigb[2 * k + 1]) * zs[2 * i];
+        if (nsymy) acc = acc + mk(zigs[2 * k], zigs[2 * k + 1]) * zs[2 * i + 1];
+      }
+      h[2 * ((size_t)ntheta * p + t)] = q * acc.re;
+      h[2 * ((size_t)ntheta * p + t) + 1] = q * acc.im;
+    }
+  }
+  return 0;
 }

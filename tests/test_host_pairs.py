@@ -7,8 +7,9 @@ matrices at the GPU parity test's tolerances: 1e-12 of each row's largest entry
 in deep water, 1e-10 in finite depth. Frequencies run in each case's order, so
 the free-surface-panel quadrature state NQ carries over as in the reference.
 Likewise the field-point Green functions of the free-surface kernel against the
-oracle's elevation for the same source strengths: 1e-9 of each problem's
-largest |ETA|. This runs without a GPU; the same functions on the device are
+oracle's elevation for the same source strengths (1e-9 of each problem's
+largest |ETA|), and the Kochin kernel's panel integrals against the oracle's
+Kochin function (1e-9 of the largest |H|). This runs without a GPU; the same functions on the device are
 checked by the GPU parity tests."""
 import ctypes
 import os
@@ -25,7 +26,7 @@ CSRC = os.path.join(os.path.dirname(HERE), "nemoh_b200", "csrc")
 SRC = os.path.join(HERE, "host_pairs", "host_pairs.cu")
 LIB = os.path.join(HERE, "host_pairs", "_build", "libhost_pairs.so")
 DEPS = [SRC] + [os.path.join(CSRC, f) for f in ("common.cuh", "green.cuh", "assembly.cuh", "freesurface.cuh",
-                                                "fd_setup.cpp", "fd_setup.h")]
+                                                "kochin.cuh", "fd_setup.cpp", "fd_setup.h")]
 _d = ctypes.POINTER(ctypes.c_double)
 _i = ctypes.POINTER(ctypes.c_int)
 
@@ -42,6 +43,9 @@ def _lib():
     L.host_pairs_free_surface.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _i, _d, ctypes.c_double, _d,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           ctypes.c_int, _d, ctypes.c_int, _d, _d, _d]
+    L.host_pairs_kochin.argtypes = [ctypes.c_int, ctypes.c_int, _d, _i, _d, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
+                                    ctypes.c_int, _d, _d, _d]
     return L
 
 
@@ -119,3 +123,34 @@ def test_host_free_surface_functions_match_oracle(case):
     assert np.all(scale > 0)
     err = (np.abs(eta - eo) / scale).max()
     assert err < 1e-9, (case.name, err)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_host_kochin_functions_match_oracle(case):
+    from nemoh_b200 import cases as C
+    L = _lib()
+    m = case.mesh
+    n = m.npanels
+    o = G.oracle_for(case)
+    geo, _ = o.geometry()
+    geo = np.ascontiguousarray(geo)
+    nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+    panels = np.ascontiguousarray(m.panels, dtype=np.int32)
+    p = lambda a: a.ctypes.data_as(_d)
+    nv = C.body_conditions(case)
+    npb = len(case.betas_deg) + len(case.rad)
+    theta = np.linspace(0.0, 2.0 * np.pi, 37)
+    xeff, yeff = 1.5, -0.7
+    for w_idx in (0, len(case.omegas) - 1):
+        T = 2 * np.pi / case.omegas[w_idx]
+        cols = list(range(w_idx * npb, (w_idx + 1) * npb))
+        res = [o.solve_problem(T, nv[:, j]) for j in cols]
+        zigb = np.asfortranarray(np.stack([r["zigb"] for r in res], axis=1))
+        zigs = np.asfortranarray(np.stack([r["zigs"] for r in res], axis=1))
+        H = np.zeros((len(theta), len(cols)), dtype=np.complex128, order="F")
+        st = L.host_pairs_kochin(n, m.isym, p(nodes), panels.ctypes.data_as(_i), p(geo), case.g, case.depth, T,
+                                 xeff, yeff, len(theta), p(theta), len(cols), p(zigb), p(zigs), p(H))
+        assert st == 0
+        Ho = o.kochin(T, theta, zigb, zigs if m.isym else None, xeff, 0.0 if m.isym else yeff)
+        err = np.abs(H - Ho).max() / np.abs(Ho).max()
+        assert err < 1e-9, (case.name, w_idx, err)
