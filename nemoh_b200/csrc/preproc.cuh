@@ -26,8 +26,8 @@ struct PreWave {
   double w, k, cb, sb;   // frequency, pre-processor wave number, cos/sin of the heading
 };
 
-__device__ __forceinline__ void pre_panel(const double* __restrict__ xyz, const int* __restrict__ m, int i, double* xm,
-                                          double* nrm, double& area) {
+NB_HD __forceinline__ void pre_panel(const double* __restrict__ xyz, const int* __restrict__ m, int i, double* xm,
+                                     double* nrm, double& area) {
   double x[4][3];
 #pragma unroll
   for (int l = 0; l < 4; ++l)
@@ -60,7 +60,7 @@ __device__ __forceinline__ void pre_panel(const double* __restrict__ xyz, const 
 }
 
 // radiation velocity . normal for one DOF at (x, n)
-__device__ __forceinline__ double pre_dof(const PreDof& d, const double* x, const double* n) {
+NB_HD __forceinline__ double pre_dof(const PreDof& d, const double* x, const double* n) {
   if (d.kind == 1) return n[0] * d.dir[0] + n[1] * d.dir[1] + n[2] * d.dir[2];
   const double r0 = x[0] - d.axis[0], r1 = x[1] - d.axis[1], r2 = x[2] - d.axis[2];
   const double v0 = d.dir[1] * r2 - d.dir[2] * r1, v1 = d.dir[2] * r0 - d.dir[0] * r2, v2 = d.dir[0] * r1 - d.dir[1] * r0;

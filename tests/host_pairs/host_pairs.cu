@@ -16,7 +16,8 @@
 // strengths as the free-surface kernel does, ETA = i W / G PHI. Kochin: the
 // panel integrals of the Kochin kernel, contracted with the source strengths.
 // The tests compare all three with the oracle's on the same mesh and
-// frequencies.
+// frequencies. Pre-processor: the panel quantities and radiation conditions
+// of the body-conditions kernel, compared with the pre-processor restatement.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -25,6 +26,7 @@
 #include "../../nemoh_b200/csrc/assembly.cuh"
 #include "../../nemoh_b200/csrc/freesurface.cuh"
 #include "../../nemoh_b200/csrc/kochin.cuh"
+#include "../../nemoh_b200/csrc/preproc.cuh"
 #include "../../nemoh_b200/csrc/fd_setup.h"
 
 using namespace nb200;
@@ -326,4 +328,30 @@ extern "C" int host_pairs_kochin(int nfa, int nsymy, const double* xyz, const in
     }
   }
   return 0;
+}
+
+// Pre-processor panel quantities (centroid, normal, area: 7 x nfa) and the
+// radiation condition n . d or n . (d x (x - axis)) of each DOF (ndof x nfa)
+// for DOF specs (kind, dir[3], axis[3]) on a one-body mesh
+extern "C" void host_pairs_preproc(int nfa, const double* xyz, const int* m1234, int ndof, const int* kind,
+                                   const double* dir, const double* axis, double* panel, double* rad) {
+  for (int i = 0; i < nfa; ++i) {
+    double xm[3], n[3], area;
+    pre_panel(xyz, m1234, i, xm, n, area);
+    for (int c = 0; c < 3; ++c) {
+      panel[c * nfa + i] = xm[c];
+      panel[(3 + c) * nfa + i] = n[c];
+    }
+    panel[6 * nfa + i] = area;
+    for (int d = 0; d < ndof; ++d) {
+      PreDof q;
+      q.kind = kind[d];
+      q.body = 1;
+      for (int c = 0; c < 3; ++c) {
+        q.dir[c] = dir[3 * d + c];
+        q.axis[c] = axis[3 * d + c];
+      }
+      rad[d * nfa + i] = pre_dof(q, xm, n);
+    }
+  }
 }

@@ -9,7 +9,9 @@ the free-surface-panel quadrature state NQ carries over as in the reference.
 Likewise the field-point Green functions of the free-surface kernel against the
 oracle's elevation for the same source strengths (1e-9 of each problem's
 largest |ETA|), and the Kochin kernel's panel integrals against the oracle's
-Kochin function (1e-9 of the largest |H|). This runs without a GPU; the same functions on the device are
+Kochin function (1e-9 of the largest |H|), and the body-conditions kernel's
+panel quantities and radiation conditions against the pre-processor
+restatement (1e-12). This runs without a GPU; the same functions on the device are
 checked by the GPU parity tests."""
 import ctypes
 import os
@@ -26,7 +28,7 @@ CSRC = os.path.join(os.path.dirname(HERE), "nemoh_b200", "csrc")
 SRC = os.path.join(HERE, "host_pairs", "host_pairs.cu")
 LIB = os.path.join(HERE, "host_pairs", "_build", "libhost_pairs.so")
 DEPS = [SRC] + [os.path.join(CSRC, f) for f in ("common.cuh", "green.cuh", "assembly.cuh", "freesurface.cuh",
-                                                "kochin.cuh", "fd_setup.cpp", "fd_setup.h")]
+                                                "kochin.cuh", "preproc.cuh", "fd_setup.cpp", "fd_setup.h")]
 _d = ctypes.POINTER(ctypes.c_double)
 _i = ctypes.POINTER(ctypes.c_int)
 
@@ -46,6 +48,8 @@ def _lib():
     L.host_pairs_kochin.argtypes = [ctypes.c_int, ctypes.c_int, _d, _i, _d, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d,
                                     ctypes.c_int, _d, _d, _d]
+    L.host_pairs_preproc.argtypes = [ctypes.c_int, _d, _i, ctypes.c_int, _i, _d, _d, _d, _d]
+    L.host_pairs_preproc.restype = None
     return L
 
 
@@ -154,3 +158,28 @@ def test_host_kochin_functions_match_oracle(case):
         Ho = o.kochin(T, theta, zigb, zigs if m.isym else None, xeff, 0.0 if m.isym else yeff)
         err = np.abs(H - Ho).max() / np.abs(Ho).max()
         assert err < 1e-9, (case.name, w_idx, err)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_host_preprocessor_functions_match_restatement(case):
+    from nemoh_b200 import cases as C
+    L = _lib()
+    m = case.mesh
+    n = m.npanels
+    nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+    panels = np.ascontiguousarray(m.panels, dtype=np.int32)
+    p = lambda a: a.ctypes.data_as(_d)
+    dofs = case.rad
+    kind = np.array([d.icase for d in dofs], dtype=np.int32)
+    dr = np.ascontiguousarray([d.direction for d in dofs], dtype=np.float64)
+    ax = np.ascontiguousarray([d.axis for d in dofs], dtype=np.float64)
+    panel = np.zeros((7, n))
+    rad = np.zeros((len(dofs), n))
+    L.host_pairs_preproc(n, p(nodes), panels.ctypes.data_as(_i), len(dofs), kind.ctypes.data_as(_i), p(dr), p(ax),
+                         p(panel), p(rad))
+    xm, nrm, a = C.panel_quantities(m)
+    for got, ref in ((panel[0:3].T, xm), (panel[3:6].T, nrm), (panel[6], a)):
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    for d, dof in enumerate(dofs):
+        ref = C._dof_vector(m, xm, nrm, a, dof, False)[:n]
+        assert np.abs(rad[d] - ref).max() <= 1e-12 * max(np.abs(ref).max(), 1.0), (case.name, d)
