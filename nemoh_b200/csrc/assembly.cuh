@@ -219,7 +219,7 @@ constexpr int WS_T = 16;
 constexpr int WS_THREADS = 128;
 
 // linear index t over the upper triangle (a <= b) of a T x T tile grid
-__device__ __forceinline__ void tri_tile(int t, int T, int& a, int& b) {
+NB_HD __forceinline__ void tri_tile(int t, int T, int& a, int& b) {
   auto start = [T](int r) { return r * T - r * (r - 1) / 2; };
   const double q = 2. * T + 1.;
   int r = (int)((q - sqrt(q * q - 8. * t)) * 0.5);

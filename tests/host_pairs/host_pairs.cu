@@ -355,3 +355,21 @@ extern "C" void host_pairs_preproc(int nfa, const double* xyz, const int* m1234,
     }
   }
 }
+
+// The wave pass's tile enumeration: for a T x T tile grid, the number of
+// upper-triangle tiles (a <= b) that blocks 0 .. T(T+1)/2 - 1 do not map to
+// exactly once (0 when every tile is taken by exactly one block)
+extern "C" long long host_pairs_tri_tile_misses(int T) {
+  std::vector<int> hits((size_t)T * T, 0);
+  const long long nt = (long long)T * (T + 1) / 2;
+  long long bad = 0;
+  for (long long t = 0; t < nt; ++t) {
+    int a, b;
+    tri_tile((int)t, T, a, b);
+    if (a < 0 || b < a || b >= T) ++bad;
+    else ++hits[(size_t)a * T + b];
+  }
+  for (int a = 0; a < T; ++a)
+    for (int b = a; b < T; ++b) bad += hits[(size_t)a * T + b] != 1;
+  return bad;
+}

@@ -11,7 +11,8 @@ oracle's elevation for the same source strengths (1e-9 of each problem's
 largest |ETA|), and the Kochin kernel's panel integrals against the oracle's
 Kochin function (1e-9 of the largest |H|), and the body-conditions kernel's
 panel quantities and radiation conditions against the pre-processor
-restatement (1e-12). This runs without a GPU; the same functions on the device are
+restatement (1e-12); and the wave pass's enumeration of upper-triangle tiles.
+This runs without a GPU; the same functions on the device are
 checked by the GPU parity tests."""
 import ctypes
 import os
@@ -50,6 +51,8 @@ def _lib():
                                     ctypes.c_int, _d, _d, _d]
     L.host_pairs_preproc.argtypes = [ctypes.c_int, _d, _i, ctypes.c_int, _i, _d, _d, _d, _d]
     L.host_pairs_preproc.restype = None
+    L.host_pairs_tri_tile_misses.argtypes = [ctypes.c_int]
+    L.host_pairs_tri_tile_misses.restype = ctypes.c_longlong
     return L
 
 
@@ -183,3 +186,12 @@ def test_host_preprocessor_functions_match_restatement(case):
     for d, dof in enumerate(dofs):
         ref = C._dof_vector(m, xm, nrm, a, dof, False)[:n]
         assert np.abs(rad[d] - ref).max() <= 1e-12 * max(np.abs(ref).max(), 1.0), (case.name, d)
+
+
+def test_wave_pass_takes_every_upper_triangle_tile_once():
+    """Block t of the wave pass maps to tile (a, b), a <= b, of the T x T grid
+    of 16 x 16 tiles: every tile exactly once, for every grid up to 8,000
+    panels (T = 500) and the orders of the benchmark and tests."""
+    L = _lib()
+    for T in list(range(1, 201)) + [250, 300, 499, 500, 501]:
+        assert L.host_pairs_tri_tile_misses(T) == 0, T
