@@ -407,7 +407,7 @@ def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9), seed=5, n_
         last = None
         for f in rates:
             done, wall = srv.run(S.make_requests(n_req, f * sat, n_bodies, seed=seed + int(100 * f)))
-            st = S.latency_stats(done, wall)
+            st = S.latency_stats(done, wall, expected=n_req)
             st.update({"rate_frac": f, "offered_per_s": f * sat})
             out["rates"].append(st)
             last = done

@@ -142,6 +142,34 @@ int nemoh_b200_body_conditions_device(nemoh_ctx* ctx, const int* panel_body, dou
                                       const double* force_dir, const double* force_axis, double* nvel_device,
                                       double* nds_device, double* fk_device, void* stream);
 
+/* Resident bodies and cross-body batches. The reference solves one body per
+ * run, its problems one after another (Solver/NEMOH.f90:129-143, the boundary
+ * SOLVE_POTENTIAL_*_DIRECT once per problem); these entry points extend that
+ * boundary to many bodies at once:
+ *
+ * nemoh_b200_add_body keeps a body on the device for the life of the context:
+ * its mesh (as nemoh_b200_set_mesh, INITIALIZE + PRE_PROC_MESH), environment
+ * and generalised normals nds (nint x 2^s nfa, Integration.dat), and its own
+ * NQ state. body_id receives its index (0, 1, ...). The context's current mesh
+ * (set_mesh) is not changed.
+ *
+ * nemoh_b200_solve_bodies solves nitem (body[i], omegas[i]) items, each with
+ * nrhs (1..16) right-hand sides, as nemoh_b200_solve_frequencies does for one
+ * body: nvel holds, item after item, (2^s nfa_i) x nrhs complex NVEL columns;
+ * force receives, item after item, nint_i x nrhs complex forces. Items of
+ * different bodies share one launch sequence (systems of different orders in
+ * one batch); the items of one body are set up in the order given (its NQ
+ * state follows them). Batches are sized by free device memory. */
+int nemoh_b200_add_body(nemoh_ctx* ctx, int np, int nfa, int nsymy, const double* xyz, const int* m1234, double rho,
+                        double g, double depth, int nint, const double* nds, int* body_id);
+int nemoh_b200_body_count(const nemoh_ctx* ctx);
+int nemoh_b200_solve_bodies(nemoh_ctx* ctx, int nitem, const int* body, const double* omegas, int nrhs,
+                            const double* nvel, double* force);
+/* Same with nvel and force in device memory of the context's device, ordered
+ * on `stream` (cudaStream_t) like nemoh_b200_solve_frequencies_device. */
+int nemoh_b200_solve_bodies_device(nemoh_ctx* ctx, int nitem, const int* body, const double* omegas, int nrhs,
+                                   const double* nvel_device, double* force_device, void* stream);
+
 /* No counterpart in the reference: an entry point that allocates nothing, for
  * hosts whose device memory is held by their own allocator (a PyTorch caching
  * allocator, a batching server that admits work by free HBM) and for hosts
@@ -157,8 +185,13 @@ int nemoh_b200_body_conditions_device(nemoh_ctx* ctx, const int* panel_body, dou
  * NEMOH_B200_ECAPACITY. The first call on a device does a one-time set-up
  * (symbol lookup, kernel attributes) and should come before any stream
  * capture. All calls on a device share the scratch, so calls that overlap on
- * the GPU race. The call returns after its work on `stream` has finished;
- * msg (may be NULL) receives the error text. */
+ * the GPU race. Both pointers must be device (or managed) memory of `device`:
+ * host memory or another GPU's memory is refused with NEMOH_B200_EINVAL before
+ * any launch. The scratch address found at set-up is kept for the life of the
+ * process; after cudaDeviceReset on that device it is stale, so do not call
+ * this entry point again in a process that reset the device. The call returns
+ * after its work on `stream` has finished; msg (may be NULL) receives the
+ * error text. */
 #define NEMOH_B200_NOALLOC_SCRATCH_BYTES (16u << 20)
 int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsys, double* a_device, int nrhs, double* x_device,
                                            void* stream, char* msg, int msg_len);

@@ -84,6 +84,11 @@ def load_library():
     L.nemoh_b200_irf.argtypes = [_vp, ctypes.c_int, _d, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int,
                                  ctypes.c_double, _d, _d]
     L.nemoh_b200_launch_count.restype = ctypes.c_longlong
+    L.nemoh_b200_add_body.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _i, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_int, _d, _i]
+    L.nemoh_b200_body_count.argtypes = [_vp]
+    L.nemoh_b200_solve_bodies.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _d, _d]
+    L.nemoh_b200_solve_bodies_device.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _vp, _vp, _vp]
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
     L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
     L.nemoh_b200_diag_theta_quadrature.argtypes = [ctypes.c_double, _d, _d]
@@ -201,6 +206,56 @@ class Solver:
         self._check(load_library().nemoh_b200_solve_frequencies_device(
             self._h, len(omegas), _p(omegas), int(nrhs), _vp(nvel_ptr), int(nint), _vp(nds_ptr),
             _vp(force_ptr), _vp(stream)))
+
+    # -- resident bodies and cross-body batches ------------------------------
+    def add_body(self, case, nds=None):
+        """Keep a body (mesh and environment of a cases.Case, generalised
+        normals nds (nint, 2^s N), by default those of the case) resident on
+        the device; returns its id."""
+        from . import cases as C
+        m = case.mesh
+        nodes = np.ascontiguousarray(m.nodes, dtype=np.float64)
+        panels = np.ascontiguousarray(m.panels, dtype=np.int32)
+        if nds is None:
+            nds = C.generalised_normals(case)
+        nds = np.asfortranarray(nds, dtype=np.float64)
+        bid = ctypes.c_int()
+        self._check(load_library().nemoh_b200_add_body(self._h, len(nodes), len(panels), int(m.isym), _p(nodes),
+                                                       panels.ctypes.data_as(_i), case.rho, case.g, case.depth,
+                                                       nds.shape[0], _p(nds), ctypes.byref(bid)))
+        if not hasattr(self, "_bodies"):
+            self._bodies = []
+        self._bodies.append((len(panels) * (2 if m.isym == 1 else 1), nds.shape[0]))
+        return bid.value
+
+    def solve_bodies(self, bodies, omegas, nvels):
+        """(body, omega) items with their right-hand sides nvels[i] ((2^s N_i, nrhs)
+        complex, the same nrhs for all); returns the forces, one (nint_i, nrhs)
+        array per item."""
+        bodies = np.ascontiguousarray(bodies, dtype=np.int32)
+        omegas = np.ascontiguousarray(omegas, dtype=np.float64)
+        nrhs = nvels[0].shape[1]
+        for b, v in zip(bodies, nvels):
+            if v.shape != (self._bodies[b][0], nrhs):
+                raise ValueError("right-hand sides of body %d: expected %s, got %s" % (b, (self._bodies[b][0], nrhs),
+                                                                                    v.shape))
+        flat = np.concatenate([np.asfortranarray(v, dtype=np.complex128).ravel(order="F") for v in nvels])
+        sizes = [self._bodies[b][1] * nrhs for b in bodies]
+        force = np.zeros(sum(sizes), dtype=np.complex128)
+        self._check(load_library().nemoh_b200_solve_bodies(self._h, len(bodies), bodies.ctypes.data_as(_i),
+                                                           _p(omegas), nrhs, _p(flat), _p(force)))
+        out, o = [], 0
+        for b, sz in zip(bodies, sizes):
+            out.append(force[o:o + sz].reshape((self._bodies[b][1], nrhs), order="F"))
+            o += sz
+        return out
+
+    def solve_bodies_device(self, bodies, omegas, nrhs, nvel_ptr, force_ptr, stream=0):
+        bodies = np.ascontiguousarray(bodies, dtype=np.int32)
+        omegas = np.ascontiguousarray(omegas, dtype=np.float64)
+        self._check(load_library().nemoh_b200_solve_bodies_device(
+            self._h, len(bodies), bodies.ctypes.data_as(_i), _p(omegas), int(nrhs), _vp(nvel_ptr), _vp(force_ptr),
+            _vp(stream)))
 
     def last_timings(self):
         a, f, s = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

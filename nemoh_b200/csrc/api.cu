@@ -8,7 +8,11 @@
 #include <complex>
 #include <cstdint>
 #include <functional>
+#include <initializer_list>
+#include <utility>
+#include <memory>
 #include <mutex>
+#include <numeric>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -85,6 +89,16 @@ struct ScopedEvent {
   }
 };
 
+// A body kept resident on the device (nemoh_b200_add_body): its panel
+// geometry, environment, generalised normals and its own NQ state (the
+// reference's NQ, left by the body's last finite-depth solve).
+struct BodyState {
+  int np = 0, nfa = 0, nsymy = 0, nint = 0;
+  double rho = 0, g = 0, depth = 0, zer = 0, gm = 0;
+  int nq_state = 0;
+  DevBuf d_xyz, d_m, d_rec, d_rows, d_nds;
+};
+
 }  // namespace
 
 struct nemoh_ctx {
@@ -113,6 +127,10 @@ struct nemoh_ctx {
   bool lu64 = false;         // d_D holds FP64 LU factors (FP64 mode, or a mixed-mode fallback)
   float t_asm = 0, t_fac = 0, t_sol = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // resident bodies and the descriptions of the current ragged batch
+  std::vector<std::unique_ptr<BodyState>> bodies;
+  DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce;
+  HostBuf h_rag;
 };
 
 #define CK(call)                                                                                 \
@@ -130,6 +148,30 @@ struct nemoh_ctx {
   } while (0)
 
 static int guarded(nemoh_ctx* ctx, const std::function<void()>& f);
+
+// Empty when every non-null pointer is device (or managed) memory that
+// `device` can address; otherwise the reason. Run before any launch, so that a
+// host buffer or another GPU's buffer handed to a *_device entry point is a
+// status code instead of an illegal-address fault.
+static std::string device_pointer_problem(int device, std::initializer_list<std::pair<const void*, const char*>> ptrs) {
+  for (const auto& pn : ptrs) {
+    if (!pn.first) continue;
+    cudaPointerAttributes at{};
+    const cudaError_t e = cudaPointerGetAttributes(&at, pn.first);
+    if (e != cudaSuccess) {
+      cudaGetLastError();   // clear the sticky-free error of the query
+      return std::string(pn.second) + ": not a CUDA pointer (" + cudaGetErrorString(e) + ")";
+    }
+    if (at.type == cudaMemoryTypeManaged) continue;
+    if (at.type != cudaMemoryTypeDevice)
+      return std::string(pn.second) + (at.type == cudaMemoryTypeHost ? ": pinned host memory, device memory expected"
+                                                                      : ": host memory, device memory expected");
+    if (at.device != device)
+      return std::string(pn.second) + ": memory of device " + std::to_string(at.device) + ", not of device " +
+             std::to_string(device);
+  }
+  return std::string();
+}
 
 namespace {
 
@@ -154,22 +196,36 @@ void check_status(nemoh_ctx* c) {
 
 // Host-side setup of one frequency (SOLVE_BEM.f90:62-84 and the preambles of
 // SOLVE_POTENTIAL_*_DIRECT). W is the reference's 2*PI/T.
+// The mesh-dependent inputs of the per-frequency setup: gravity, depth, GM
+// and the NQ state that the finite-depth solves leave (the context's current
+// mesh, or a resident body).
+struct Env {
+  double g, depth, gm;
+  int* nq_state;
+};
+
+void omega_params_env(const Env& e, double W, OmegaParams& om, bool advance_nq);
+
 void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
+  omega_params_env(Env{c->g, c->depth, c->gm, &c->nq_state}, W, om, advance_nq);
+}
+
+void omega_params_env(const Env& env, double W, OmegaParams& om, bool advance_nq) {
   std::memset(&om, 0, sizeof om);
   om.w = W;
-  om.h = c->depth;
-  const double kwave = W * W / c->g;
-  const bool fd = !((c->depth == 0.) || (kwave * c->depth >= 20));
+  om.h = env.depth;
+  const double kwave = W * W / env.g;
+  const bool fd = !((env.depth == 0.) || (kwave * env.depth >= 20));
   if (std::fabs(W) < 1.E-4) throw Fail{NEMOH_B200_EOMEGA, "ABS(WR) < 1.E-4"};
   double qq[MAX_NQ + 2], cq[MAX_NQ + 2];
   if (!fd) {
     om.fd = 0;
-    om.k0 = W * W / c->g;
-    const int n = theta_quadrature(om.k0 * c->gm, qq, cq);
+    om.k0 = W * W / env.g;
+    const int n = theta_quadrature(om.k0 * env.gm, qq, cq);
     // NQ is not set on this path (SOLVE_BEM_INFD_DIRECT.f90:79): the
     // free-surface-panel theta sum runs NQ (left by the last finite-depth
     // solve) times over this path's weights, which are zero past n.
-    om.nq = std::min(c->nq_state, n);
+    om.nq = std::min(*env.nq_state, n);
     for (int i = 1; i <= om.nq; ++i) {
       om.cq[i] = cq[i];
       om.ct[i] = std::cos(qq[i]);
@@ -177,16 +233,16 @@ void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
     }
   } else {
     om.fd = 1;
-    const double AKH0 = W * W * c->depth / c->g;
+    const double AKH0 = W * W * env.depth / env.g;
     double AMH;
     int st = finite_depth_root(AKH0, &AMH);
     if (st) throw Fail{st, "ERREUR DANS LA RECHERCHE DE LA RACINE (X0)"};
     const double AKH = AMH * std::tanh(AMH);
-    const double AM0 = AMH / c->depth;
+    const double AM0 = AMH / env.depth;
     om.k0 = AM0;
     om.amh = AMH;
-    const int n = theta_quadrature(AM0 * c->gm, qq, cq);
-    if (advance_nq) c->nq_state = n;   // NQ=N (SOLVE_BEM_FD_DIRECT.f90:99)
+    const int n = theta_quadrature(AM0 * env.gm, qq, cq);
+    if (advance_nq) *env.nq_state = n;   // NQ=N (SOLVE_BEM_FD_DIRECT.f90:99)
     om.nq = 0;                         // CQ is zero on this path (COMPUTE_GREEN_FD.f90:874)
     int nexp = 0;
     st = exponential_fit(AKH, AMH, &nexp, om.ambda, om.ar);
@@ -194,13 +250,50 @@ void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
     om.nexp = nexp;
     om.ambda[nexp + 1] = 0.;
     om.ar[nexp + 1] = 2.;
-    const double A = (AMH + AKH) * (AMH + AKH) / (c->depth * (AMH * AMH - AKH * AKH + AKH));
+    const double A = (AMH + AKH) * (AMH + AKH) / (env.depth * (AMH * AMH - AKH * AKH + AKH));
     const double ADPI2 = -A / (8. * kPI * kPI), ADPI = -A / (8 * kPI);
     om.coe1 = ADPI2 / AM0;
     om.coe2 = ADPI / AM0;
     om.coe3 = ADPI2;
     om.coe4 = ADPI;
   }
+}
+
+// Mesh upload and panel geometry (INITIALIZE + PRE_PROC_MESH: GOMG, ZER and
+// GM): nodes and connectivity to the device, GOMG there, ZER on the host
+// (PREPARE_MESH.f90:58-69: the largest pairwise |dx| is max - min), GM by a
+// device reduction. Synchronises the context's stream.
+void upload_geometry(nemoh_ctx* c, int np, int nfa, int nsymy, const double* xyz, const int* m1234, DevBuf& d_xyz,
+                     DevBuf& d_m, DevBuf& d_rec, DevBuf& d_rows, double& zer, double& gm) {
+  for (int i = 0; i < 4 * nfa; ++i)
+    if (m1234[i] < 1 || m1234[i] > np) throw Fail{NEMOH_B200_EINVAL, "panel node index out of range"};
+  double xmin = xyz[0], xmax = xyz[0], ymin = xyz[1], ymax = xyz[1], yabs = 0;
+  for (int i = 0; i < np; ++i) {
+    xmin = std::min(xmin, xyz[3 * i]);
+    xmax = std::max(xmax, xyz[3 * i]);
+    ymin = std::min(ymin, xyz[3 * i + 1]);
+    ymax = std::max(ymax, xyz[3 * i + 1]);
+    yabs = std::max(yabs, std::fabs(xyz[3 * i + 1]));
+  }
+  const double GL0 = xmax - xmin;
+  const double BL = nsymy ? 2. * yabs : ymax - ymin;
+  zer = -1.E-5 * std::max(GL0, BL);
+  CK(d_xyz.ensure(sizeof(double) * 3 * np));
+  CK(d_m.ensure(sizeof(int) * 4 * nfa));
+  CK(d_rec.ensure(sizeof(PanelRec) * nfa));
+  CK(d_rows.ensure(sizeof(double) * 6 * nfa));
+  CK(cudaMemcpyAsync(d_xyz.p, xyz, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(d_m.p, m1234, sizeof(int) * 4 * nfa, cudaMemcpyHostToDevice, c->stream));
+  gomg_kernel<<<(nfa + 127) / 128, 128, 0, c->stream>>>(nfa, d_xyz.as<double>(), d_m.as<int>(), d_rec.as<PanelRec>(),
+                                                       d_rows.as<double>(), c->d_status.as<int>());
+  LAUNCHED(c);
+  CK(cudaMemsetAsync(c->d_gm.p, 0, sizeof(unsigned long long), c->stream));
+  gm_kernel<<<592, 256, 0, c->stream>>>(np, nsymy, d_xyz.as<double>(), c->d_gm.as<unsigned long long>());
+  LAUNCHED(c);
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_gm.p, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+  check_status(c);
+  std::memcpy(&gm, &bits, sizeof bits);
 }
 
 // capacity: frequencies per device batch
@@ -261,17 +354,25 @@ GreenCtx green_ctx(nemoh_ctx* c) {
 }
 
 // Upload the parameters of slots [s0, s1) (already in c->h_oms) and assemble
-// those frequencies: deep-water slots first, then finite-depth ones.
-void assemble_range(nemoh_ctx* c, int s0, int s1) {
+// those frequencies: deep-water slots first, then finite-depth ones. Ragged
+// batches pass each slot's mesh on the device (dmesh) and its order on the
+// host (host_n); each launch's grid is then sized by its largest slot.
+void assemble_range(nemoh_ctx* c, int s0, int s1, const SlotMesh* dmesh = nullptr, const int* host_n = nullptr) {
   const int N = c->nfa, cls = ncls(c);
   const OmegaParams* hom = c->h_oms.as<OmegaParams>();
   int* hs = c->h_slots.as<int>() + s0;
-  int ninfd = 0;
+  int ninfd = 0, n_infd = 0, n_fd = 0;
   for (int s = s0; s < s1; ++s)
-    if (!hom[s].fd) hs[ninfd++] = s;
+    if (!hom[s].fd) {
+      hs[ninfd++] = s;
+      n_infd = std::max(n_infd, host_n ? host_n[s] : N);
+    }
   int nfd = 0;
   for (int s = s0; s < s1; ++s)
-    if (hom[s].fd) hs[ninfd + nfd++] = s;
+    if (hom[s].fd) {
+      hs[ninfd + nfd++] = s;
+      n_fd = std::max(n_fd, host_n ? host_n[s] : N);
+    }
   CK(cudaMemcpyAsync(c->d_oms.as<OmegaParams>() + s0, hom + s0, (size_t)(s1 - s0) * sizeof(OmegaParams),
                      cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_slots.as<int>() + s0, hs, (size_t)(s1 - s0) * sizeof(int), cudaMemcpyHostToDevice,
@@ -287,34 +388,43 @@ void assemble_range(nemoh_ctx* c, int s0, int s1) {
   const double* rows = c->d_rows.as<double>();
   const int* ds = c->d_slots.as<int>() + s0;
   if (ninfd) {
-    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)ninfd);
-    rankine_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, N, o);
+    const int n = n_infd;
+    dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ, (unsigned)ninfd);
+    rankine_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, n, o, dmesh);
     LAUNCHED(c);
-    const unsigned wt = (N + WS_T - 1) / WS_T;
+    const unsigned wt = (n + WS_T - 1) / WS_T;
     wave_sym_kernel<false><<<dim3(wt * (wt + 1) / 2, 1, (unsigned)ninfd), WS_THREADS, 0, c->stream>>>(g, dom, ds, rec,
-                                                                                                      N, o);
+                                                                                                      n, o, dmesh);
     LAUNCHED(c);
   }
   if (nfd) {
-    dim3 grid((N + ASM_ROWS - 1) / ASM_ROWS, (N + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
-    rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, N, o);
+    const int n = n_fd;
+    dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
+    rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, n, o, dmesh);
     LAUNCHED(c);
-    const unsigned wt = (N + WS_T - 1) / WS_T;
+    const unsigned wt = (n + WS_T - 1) / WS_T;
     wave_sym_kernel<true><<<dim3(wt * (wt + 1) / 2, 1, (unsigned)nfd), WS_THREADS, 0, c->stream>>>(
-        g, dom, ds + ninfd, rec, N, o);
+        g, dom, ds + ninfd, rec, n, o, dmesh);
     LAUNCHED(c);
   }
 }
 
-Batch dbatch(nemoh_ctx* c) {
-  const long long NN = (long long)c->nfa * c->nfa;
+// The systems of a batch: nsys systems of order n (uniform, the current mesh),
+// or of orders up to n described by rg (ragged, several bodies).
+struct Shape {
+  int n;
+  Ragged rg;
+};
+Shape uniform_shape(const nemoh_ctx* c) { return Shape{c->nfa, Ragged()}; }
+
+Batch dbatch(nemoh_ctx* c, const Shape& sh) {
   // FP64 keeps the per-step row-strip updates (FP64 GEMM tiles beat the fused strip solve there)
-  return Batch{c->d_D.as<double2>(), NN, c->nfa, c->d_diag.as<double2>()};
+  return make_batch<double2>(c->d_D.as<double2>(), sh.n, c->d_diag.as<double2>(), nullptr, sh.rg);
 }
 
-void factor_fp64(nemoh_ctx* c, int nsys) {
-  Batch b = dbatch(c);
-  const int N = c->nfa;
+void factor_fp64(nemoh_ctx* c, int nsys, const Shape& sh) {
+  Batch b = dbatch(c, sh);
+  const int N = sh.n;
   static std::atomic<unsigned long long> attr{0};
   once_per_device(attr, [] {
     CK(cudaFuncSetAttribute(zgemm_update_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -323,10 +433,10 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
   lu_two_level<double2>(
       b, nsys, c->d_status.as<int>(), c->stream, c->launches,
       [&](Batch bg, int ns, cudaStream_t sg, int, int k0, int kend) {
-        zgemm_update<double2>(bg, k0, kend - k0, Rect{kend, N, kend, N}, ns, sg);
+        zgemm_update<double2>(bg, k0, kend - k0, Rect{kend, bg.n, kend, bg.n}, ns, sg);
         ++c->launches;
       },
-      &c->lanes);
+      &c->lanes, sh.rg.host_ord);
   CK(cudaGetLastError());
   static std::atomic<unsigned long long> attr2{0};
   once_per_device(attr2, [] {
@@ -340,9 +450,9 @@ void factor_fp64(nemoh_ctx* c, int nsys) {
 }
 
 // solve the factored systems for the right-hand sides in X (result in X)
-void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
-  trsm_launch<double2>(dbatch(c), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys, nrhs,
-                       c->stream, c->launches, &c->lanes);
+void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
+  CK(trsm_sweep<double2>(dbatch(c, sh), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys,
+                         nrhs, c->stream, c->launches));
   CK(cudaGetLastError());
 }
 
@@ -352,39 +462,44 @@ void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs) {
 // factored again in FP64 on the device and solved from the original
 // right-hand sides, which the refinement kept in mixed.b. d_D then holds the
 // FP64 factors (lu64) instead of the matrix.
-void mixed_solve(nemoh_ctx* c, int nsys, int nrhs) {
+void mixed_fallback(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
   MixedWork& w = c->mixed;
-  mixed_solve_refine(w, c->d_D.as<double2>(), c->nfa, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(), nrhs,
-                     c->stream, c->launches, &c->lanes);
-  CK(cudaGetLastError());
-  if (w.last_residual <= REFINE_TOL) return;
-  const size_t N = c->nfa;
+  const size_t N = sh.n;
   CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
   CK(cudaMemcpyAsync(c->d_X.p, w.b, (size_t)nsys * N * nrhs * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
-  factor_fp64(c, nsys);
-  trsm_fp64(c, nsys, nrhs);
+  factor_fp64(c, nsys, sh);
+  trsm_fp64(c, nsys, nrhs, sh);
   c->lu64 = true;
   w.last_iterations = -1;
   ++w.fallbacks;
 }
 
-void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs) {
+void mixed_solve(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
+  MixedWork& w = c->mixed;
+  mixed_solve_refine(w, c->d_D.as<double2>(), sh.n, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(), nrhs,
+                     c->stream, c->launches, sh.rg);
+  CK(cudaGetLastError());
+  if (w.last_residual <= REFINE_TOL) return;
+  mixed_fallback(c, nsys, nrhs, sh);
+}
+
+void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs, const Shape& sh) {
   c->lu64 = c->mode == NEMOH_B200_FP64;
   if (c->mode == NEMOH_B200_MIXED) {
-    mixed_factor(c->mixed, c->d_D.as<double2>(), c->nfa, nsys, c->d_status.as<int>(), c->stream, c->launches,
-                 &c->lanes, /*have_f32=*/true);
+    mixed_factor(c->mixed, c->d_D.as<double2>(), sh.n, nsys, c->d_status.as<int>(), c->stream, c->launches,
+                 &c->lanes, /*have_f32=*/true, sh.rg);
     CK(cudaGetLastError());
-    if (have_rhs) mixed_solve(c, nsys, nrhs);
+    if (have_rhs) mixed_solve(c, nsys, nrhs, sh);
   } else {
-    factor_fp64(c, nsys);
-    if (have_rhs) trsm_fp64(c, nsys, nrhs);
+    factor_fp64(c, nsys, sh);
+    if (have_rhs) trsm_fp64(c, nsys, nrhs, sh);
   }
 }
 
-void potential(nemoh_ctx* c, int nsys, int nrhs) {
-  const int N = c->nfa;
-  const long long NN = (long long)N * N, xs = (long long)N * nrhs;
-  Batch s{c->d_S.as<double2>(), NN, N, nullptr};
+void potential(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
+  const int N = sh.n;
+  const long long xs = (long long)N * nrhs;
+  const Batch s = make_batch<double2>(c->d_S.as<double2>(), N, nullptr, nullptr, sh.rg);
   CK(cudaMemsetAsync(c->d_Y.p, 0, (size_t)nsys * xs * sizeof(double2), c->stream));
   matvec_acc(s, c->d_X.as<double2>(), xs, c->d_Y.as<double2>(), xs, nrhs, nsys, 1.0, c->stream);
   LAUNCHED(c);
@@ -421,9 +536,9 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
     fold_rhs_kernel<<<dim3((N + 127) / 128, nrhs, nw), 128, 0, c->stream>>>(
         nvel_d + (long long)w0 * nrhs * cls * N, N, c->nsymy, nrhs, c->d_X.as<double2>());
     LAUNCHED(c);
-    factor_and_solve(c, nw * cls, nrhs, true);
+    factor_and_solve(c, nw * cls, nrhs, true, uniform_shape(c));
     CK(cudaEventRecord(c->ev[2], c->stream));
-    potential(c, nw * cls, nrhs);
+    potential(c, nw * cls, nrhs, uniform_shape(c));
     if (nint > 0) {
       force_kernel<<<dim3(nint, nrhs, nw), 256, 0, c->stream>>>(c->d_Y.as<double2>(), c->d_oms.as<OmegaParams>(), N,
                                                                 c->nsymy, nrhs, nint, nds_d, c->rho,
@@ -441,6 +556,176 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
     c->t_sol += s;
   }
   c->w_previous = -1.;  // the batch reused the cached-factor slot
+}
+
+// ---------------------------------------------------------------------------
+// Cross-body batches. The reference solves one body at a time, frequency by
+// frequency (NEMOH.f90:129-143); here (resident body, frequency) items of
+// different bodies share one launch sequence: their systems are sorted by
+// decreasing order and every kernel of the pipeline takes each system's own
+// order and place (ragged batch), so one launch covers the same step of every
+// system of the batch.
+// ---------------------------------------------------------------------------
+
+// device bytes one item adds to a ragged batch whose largest order is nmax
+size_t item_bytes(const nemoh_ctx* c, const BodyState& b, int nmax, int nrhs) {
+  const size_t n = b.nfa, cls = b.nsymy + 1, nm = nmax, nblk = (nm + TB - 1) / TB;
+  size_t per_sys = 2 * nm * nrhs * sizeof(double2) + DIAG_SCRATCH * sizeof(double2) +
+                   nblk * 2 * TB * TB * sizeof(double2) + 64;
+  size_t mats = 2 * n * n * sizeof(double2);
+  if (c->mode == NEMOH_B200_MIXED) {
+    mats += n * n * sizeof(float2);
+    per_sys += nm * nrhs * (2 * sizeof(double2) + 2 * sizeof(float2)) + (DIAG_SCRATCH + PINV_SCRATCH) * sizeof(float2) +
+               nblk * 2 * TB * TB * sizeof(float2) + tc_bytes_per_system(nm);
+  }
+  return cls * (mats + per_sys) + sizeof(OmegaParams) + sizeof(SlotMesh) + sizeof(ItemDesc);
+}
+
+// one ragged batch: items[0..k) index the caller's arrays, already in
+// decreasing order of their body's panel count
+void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const double* omegas, int nrhs,
+                  const std::vector<long long>& nvel_off, const std::vector<long long>& force_off,
+                  const double2* nvel_d, double2* force_d) {
+  std::vector<long long> off;
+  std::vector<int> ord, host_n(k);
+  std::vector<SlotMesh> sm(k);
+  std::vector<ItemDesc> it(k);
+  long long mat = 0;
+  int nint_max = 0;
+  for (int j = 0; j < k; ++j) {
+    const int i = items[j];
+    const BodyState& b = *c->bodies[body[i]];
+    sm[j] = SlotMesh{b.d_rec.as<PanelRec>(), b.d_rows.as<double>(), mat, b.nfa, b.nsymy, b.zer};
+    it[j] = ItemDesc{nvel_off[i], force_off[i], b.d_nds.as<double>(), b.rho, b.nfa, b.nsymy, (int)ord.size(), b.nint};
+    host_n[j] = b.nfa;
+    nint_max = std::max(nint_max, b.nint);
+    for (int cc = 0; cc <= b.nsymy; ++cc) {
+      off.push_back(mat);
+      ord.push_back(b.nfa);
+      mat += (long long)b.nfa * b.nfa;
+    }
+  }
+  const int nsys = (int)ord.size(), nmax = ord[0];
+  const size_t N = nmax, V = (size_t)nsys * N * nrhs;
+  CK(c->d_D.ensure((size_t)mat * sizeof(double2)));
+  CK(c->d_S.ensure((size_t)mat * sizeof(double2)));
+  CK(c->d_X.ensure(V * sizeof(double2)));
+  CK(c->d_Y.ensure(V * sizeof(double2)));
+  CK(c->d_diag.ensure((size_t)nsys * DIAG_SCRATCH * sizeof(double2)));
+  if (c->mode == NEMOH_B200_FP64)
+    CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
+  else
+    CK(c->mixed.ensure(nsys, nmax, nrhs, (size_t)mat));
+  CK(c->d_oms.ensure((size_t)k * sizeof(OmegaParams)));
+  CK(c->d_slots.ensure((size_t)k * sizeof(int)));
+  CK(c->h_oms.ensure((size_t)k * sizeof(OmegaParams)));
+  CK(c->h_slots.ensure((size_t)k * sizeof(int)));
+  // descriptions through one pinned staging buffer (the batch ends with a
+  // synchronisation, so the next batch may rewrite it)
+  const size_t b_off = 0, b_ord = b_off + ((nsys * sizeof(long long) + 255) & ~size_t(255));
+  const size_t b_sm = b_ord + ((nsys * sizeof(int) + 255) & ~size_t(255));
+  const size_t b_it = b_sm + ((k * sizeof(SlotMesh) + 255) & ~size_t(255));
+  const size_t b_end = b_it + k * sizeof(ItemDesc);
+  CK(c->h_rag.ensure(b_end));
+  CK(c->d_roff.ensure(nsys * sizeof(long long)));
+  CK(c->d_rord.ensure(nsys * sizeof(int)));
+  CK(c->d_smesh.ensure(k * sizeof(SlotMesh)));
+  CK(c->d_items.ensure(k * sizeof(ItemDesc)));
+  char* hr = c->h_rag.as<char>();
+  std::memcpy(hr + b_off, off.data(), nsys * sizeof(long long));
+  std::memcpy(hr + b_ord, ord.data(), nsys * sizeof(int));
+  std::memcpy(hr + b_sm, sm.data(), k * sizeof(SlotMesh));
+  std::memcpy(hr + b_it, it.data(), k * sizeof(ItemDesc));
+  CK(cudaMemcpyAsync(c->d_roff.p, hr + b_off, nsys * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_rord.p, hr + b_ord, nsys * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_smesh.p, hr + b_sm, k * sizeof(SlotMesh), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_items.p, hr + b_it, k * sizeof(ItemDesc), cudaMemcpyHostToDevice, c->stream));
+  // the uniform path's buffers and cached factors no longer hold what they did
+  c->cap_nfa = -1;
+  c->w_previous = -1.;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  OmegaParams* hom = c->h_oms.as<OmegaParams>();
+  int done = 0;
+  for (int j = 0; j < k; ++j) {
+    BodyState& b = *c->bodies[body[items[j]]];
+    const double T = 2. * kPI / omegas[items[j]];
+    omega_params_env(Env{b.g, b.depth, b.gm, &b.nq_state}, 2. * kPI / T, hom[j], true);
+    if (j + 1 == k || j + 1 - done >= ASM_GROUP) {
+      assemble_range(c, done, j + 1, c->d_smesh.as<SlotMesh>(), host_n.data());
+      done = j + 1;
+    }
+  }
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  const long long xs = (long long)N * nrhs;
+  fold_rhs_ragged_kernel<<<dim3((nmax + 127) / 128, nrhs, k), 128, 0, c->stream>>>(nvel_d, c->d_items.as<ItemDesc>(),
+                                                                                  nrhs, xs, c->d_X.as<double2>());
+  LAUNCHED(c);
+  const Shape sh{nmax, Ragged{c->d_roff.as<long long>(), c->d_rord.as<int>(), ord.data()}};
+  factor_and_solve(c, nsys, nrhs, true, sh);
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  potential(c, nsys, nrhs, sh);
+  if (nint_max > 0) {
+    force_ragged_kernel<<<dim3(nint_max, nrhs, k), 256, 0, c->stream>>>(c->d_Y.as<double2>(), c->d_items.as<ItemDesc>(),
+                                                                       c->d_oms.as<OmegaParams>(), nrhs, xs, force_d);
+    LAUNCHED(c);
+  }
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  check_status(c);
+  float a, f, s;
+  CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+  CK(cudaEventElapsedTime(&f, c->ev[1], c->ev[2]));
+  CK(cudaEventElapsedTime(&s, c->ev[2], c->ev[3]));
+  c->t_asm += a;
+  c->t_fac += f;
+  c->t_sol += s;
+}
+
+void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* omegas, int nrhs,
+                       const double2* nvel_d, double2* force_d) {
+  if (nrhs < 1 || nrhs > MAX_RHS) throw Fail{NEMOH_B200_ECAPACITY, "nrhs must be in 1..16"};
+  std::vector<long long> nvel_off(nitem), force_off(nitem);
+  long long ov = 0, of = 0;
+  for (int i = 0; i < nitem; ++i) {
+    const BodyState& b = *c->bodies[body[i]];
+    nvel_off[i] = ov;
+    force_off[i] = of;
+    ov += (long long)(b.nsymy + 1) * b.nfa * nrhs;
+    of += (long long)b.nint * nrhs;
+  }
+  // decreasing panel count; stable, so each body's frequencies keep the
+  // caller's order, which the body's NQ state follows
+  std::vector<int> idx(nitem);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(),
+                   [&](int a, int b) { return c->bodies[body[a]]->nfa > c->bodies[body[b]]->nfa; });
+  // admission by HBM footprint: 80% of the free memory, the batch's own
+  // buffers counted as free
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t have = c->d_D.bytes + c->d_S.bytes + c->d_X.bytes + c->d_Y.bytes + c->d_inv.bytes + c->d_diag.bytes +
+                      c->mixed.bytes();
+  size_t budget = (size_t)((fr + have) * 0.8);
+  // NEMOH_B200_BATCH_BYTES lowers the budget (tests use it to split a call
+  // into several batches)
+  if (const char* e = std::getenv("NEMOH_B200_BATCH_BYTES")) {
+    const long long v = std::atoll(e);
+    if (v > 0) budget = std::min(budget, (size_t)v);
+  }
+  c->t_asm = c->t_fac = c->t_sol = 0;
+  int pos = 0;
+  while (pos < nitem) {
+    const int nmax = c->bodies[body[idx[pos]]]->nfa;
+    size_t used = 0;
+    int end = pos;
+    while (end < nitem) {
+      const size_t need = item_bytes(c, *c->bodies[body[idx[end]]], nmax, nrhs);
+      if (end > pos && used + need > budget) break;
+      used += need;
+      ++end;
+    }
+    ragged_batch(c, idx.data() + pos, end - pos, body, omegas, nrhs, nvel_off, force_off, nvel_d, force_d);
+    pos = end;
+  }
 }
 
 }  // namespace
@@ -563,7 +848,7 @@ int nemoh_b200_set_mesh(nemoh_ctx* c, int np, int nfa, int nsymy, const double* 
                         double g, double depth) {
   if (!c || np < 2 || nfa < 1 || !xyz || !m1234 || !(g > 0)) return NEMOH_B200_EINVAL;
   return guarded(c, [&] {
-    for (int i = 0; i < 4 * nfa; ++i)
+    for (int i = 0; i < 4 * nfa; ++i)   // before the context changes
       if (m1234[i] < 1 || m1234[i] > np) throw Fail{NEMOH_B200_EINVAL, "panel node index out of range"};
     c->np = np;
     c->nfa = nfa;
@@ -573,35 +858,83 @@ int nemoh_b200_set_mesh(nemoh_ctx* c, int np, int nfa, int nsymy, const double* 
     c->depth = depth;
     c->w_previous = -1.;
     c->nq_state = 0;
-    // ZER (PREPARE_MESH.f90:58-69): the largest pairwise |dx| is max-min
-    double xmin = xyz[0], xmax = xyz[0], ymin = xyz[1], ymax = xyz[1], yabs = 0;
-    for (int i = 0; i < np; ++i) {
-      xmin = std::min(xmin, xyz[3 * i]);
-      xmax = std::max(xmax, xyz[3 * i]);
-      ymin = std::min(ymin, xyz[3 * i + 1]);
-      ymax = std::max(ymax, xyz[3 * i + 1]);
-      yabs = std::max(yabs, std::fabs(xyz[3 * i + 1]));
-    }
-    const double GL0 = xmax - xmin;
-    const double BL = c->nsymy ? 2. * yabs : ymax - ymin;
-    c->zer = -1.E-5 * std::max(GL0, BL);
-    CK(c->d_xyz.ensure(sizeof(double) * 3 * np));
-    CK(c->d_m.ensure(sizeof(int) * 4 * nfa));
-    CK(c->d_rec.ensure(sizeof(PanelRec) * nfa));
-    CK(c->d_rows.ensure(sizeof(double) * 6 * nfa));
-    CK(cudaMemcpyAsync(c->d_xyz.p, xyz, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->d_m.p, m1234, sizeof(int) * 4 * nfa, cudaMemcpyHostToDevice, c->stream));
-    gomg_kernel<<<(nfa + 127) / 128, 128, 0, c->stream>>>(nfa, c->d_xyz.as<double>(), c->d_m.as<int>(),
-                                                         c->d_rec.as<PanelRec>(), c->d_rows.as<double>(),
-                                                         c->d_status.as<int>());
-    LAUNCHED(c);
-    CK(cudaMemsetAsync(c->d_gm.p, 0, sizeof(unsigned long long), c->stream));
-    gm_kernel<<<592, 256, 0, c->stream>>>(np, c->nsymy, c->d_xyz.as<double>(), c->d_gm.as<unsigned long long>());
-    LAUNCHED(c);
-    unsigned long long bits = 0;
-    CK(cudaMemcpyAsync(&bits, c->d_gm.p, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
-    check_status(c);
-    std::memcpy(&c->gm, &bits, sizeof bits);
+    upload_geometry(c, np, nfa, c->nsymy, xyz, m1234, c->d_xyz, c->d_m, c->d_rec, c->d_rows, c->zer, c->gm);
+  });
+}
+
+int nemoh_b200_add_body(nemoh_ctx* c, int np, int nfa, int nsymy, const double* xyz, const int* m1234, double rho,
+                        double g, double depth, int nint, const double* nds, int* body_id) {
+  if (!c || np < 2 || nfa < 1 || !xyz || !m1234 || !(g > 0) || nint < 0 || (nint > 0 && !nds) || !body_id)
+    return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    auto b = std::make_unique<BodyState>();
+    b->np = np;
+    b->nfa = nfa;
+    b->nsymy = (nsymy == 1) ? 1 : 0;
+    b->rho = rho;
+    b->g = g;
+    b->depth = depth;
+    b->nint = nint;
+    upload_geometry(c, np, nfa, b->nsymy, xyz, m1234, b->d_xyz, b->d_m, b->d_rec, b->d_rows, b->zer, b->gm);
+    const size_t nds_elems = (size_t)nint * nfa * (b->nsymy + 1);
+    CK(b->d_nds.ensure(std::max<size_t>(1, nds_elems) * sizeof(double)));
+    if (nint) CK(cudaMemcpyAsync(b->d_nds.p, nds, nds_elems * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->bodies.push_back(std::move(b));
+    *body_id = (int)c->bodies.size() - 1;
+  });
+}
+
+int nemoh_b200_body_count(const nemoh_ctx* c) { return c ? (int)c->bodies.size() : 0; }
+
+static int bodies_args_ok(const nemoh_ctx* c, int nitem, const int* body, const double* omegas) {
+  if (!c || nitem < 1 || !body || !omegas) return 0;
+  for (int i = 0; i < nitem; ++i)
+    if (body[i] < 0 || body[i] >= (int)c->bodies.size()) return 0;
+  return 1;
+}
+
+static void bodies_sizes(const nemoh_ctx* c, int nitem, const int* body, int nrhs, size_t* nvel, size_t* force) {
+  *nvel = *force = 0;
+  for (int i = 0; i < nitem; ++i) {
+    const BodyState& b = *c->bodies[body[i]];
+    *nvel += (size_t)(b.nsymy + 1) * b.nfa * nrhs;
+    *force += (size_t)b.nint * nrhs;
+  }
+}
+
+int nemoh_b200_solve_bodies(nemoh_ctx* c, int nitem, const int* body, const double* omegas, int nrhs,
+                            const double* nvel, double* force) {
+  if (!bodies_args_ok(c, nitem, body, omegas) || nrhs < 1 || !nvel || !force) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    if (nrhs > MAX_RHS) throw Fail{NEMOH_B200_ECAPACITY, "nrhs must be in 1..16"};
+    size_t nv = 0, nf = 0;
+    bodies_sizes(c, nitem, body, nrhs, &nv, &nf);
+    CK(c->d_bnvel.ensure(nv * sizeof(double2)));
+    CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2)));
+    CK(cudaMemcpyAsync(c->d_bnvel.p, nvel, nv * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    solve_bodies_impl(c, nitem, body, omegas, nrhs, c->d_bnvel.as<double2>(), c->d_bforce.as<double2>());
+    if (nf) CK(cudaMemcpyAsync(force, c->d_bforce.p, nf * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int nemoh_b200_solve_bodies_device(nemoh_ctx* c, int nitem, const int* body, const double* omegas, int nrhs,
+                                   const double* nvel_device, double* force_device, void* stream) {
+  if (!bodies_args_ok(c, nitem, body, omegas) || nrhs < 1 || !nvel_device || !force_device) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    const std::string bad =
+        device_pointer_problem(c->device, {{nvel_device, "nvel_device"}, {force_device, "force_device"}});
+    if (!bad.empty()) throw Fail{NEMOH_B200_EINVAL, bad};
+    cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+    ScopedEvent ev;
+    CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev.e, user));
+    CK(cudaStreamWaitEvent(c->stream, ev.e, 0));
+    solve_bodies_impl(c, nitem, body, omegas, nrhs, reinterpret_cast<const double2*>(nvel_device),
+                      reinterpret_cast<double2*>(force_device));
+    CK(cudaEventRecord(ev.e, c->stream));
+    CK(cudaStreamWaitEvent(user, ev.e, 0));
   });
 }
 
@@ -672,7 +1005,7 @@ int nemoh_b200_solve_problem(nemoh_ctx* c, double period, const double* nvel, do
       OmegaParams& om = c->h_oms.as<OmegaParams>()[0];
       omega_params(c, W, om, true);
       assemble_range(c, 0, 1);
-      factor_and_solve(c, cls, 1, false);
+      factor_and_solve(c, cls, 1, false, uniform_shape(c));
       check_status(c);
       c->w_previous = W;
       c->cached_fd = om.fd;
@@ -689,11 +1022,11 @@ int nemoh_b200_solve_problem(nemoh_ctx* c, double period, const double* nvel, do
       for (int i = 0; i < N; ++i) B[(size_t)s * N + i] = c->nsymy ? (v[i] + BX * v[i + N]) * 0.5 : v[i];
     }
     CK(cudaMemcpyAsync(c->d_X.p, B.data(), B.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    if (c->lu64) trsm_fp64(c, cls, 1);
-    else mixed_solve(c, cls, 1);
+    if (c->lu64) trsm_fp64(c, cls, 1, uniform_shape(c));
+    else mixed_solve(c, cls, 1, uniform_shape(c));
     std::vector<std::complex<double>> zol((size_t)cls * N), phi((size_t)cls * N);
     CK(cudaMemcpyAsync(zol.data(), c->d_X.p, zol.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-    potential(c, cls, 1);
+    potential(c, cls, 1, uniform_shape(c));
     CK(cudaMemcpyAsync(phi.data(), c->d_Y.p, phi.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     check_status(c);
     auto put = [](double* o, int i, std::complex<double> z) {
@@ -749,6 +1082,9 @@ int nemoh_b200_solve_frequencies_device(nemoh_ctx* c, int nomega, const double* 
       (nint > 0 && (!nds_device || !force_device)))
     return NEMOH_B200_EINVAL;
   return guarded(c, [&] {
+    const std::string bad = device_pointer_problem(
+        c->device, {{nvel_device, "nvel_device"}, {nds_device, "nds_device"}, {force_device, "force_device"}});
+    if (!bad.empty()) throw Fail{NEMOH_B200_EINVAL, bad};
     cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
     ScopedEvent ev;
     CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
@@ -945,6 +1281,9 @@ static int body_conditions_impl(nemoh_ctx* c, const int* panel_body, double xeff
     cudaStream_t st = c->stream;
     ScopedEvent ev;
     if (!host_out) {
+      const std::string bad = device_pointer_problem(
+          c->device, {{nvel_d, "nvel_device"}, {nds_d, "nds_device"}, {fk_d, "fk_device"}});
+      if (!bad.empty()) throw Fail{NEMOH_B200_EINVAL, bad};
       CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
       CK(cudaEventRecord(ev.e, user));
       CK(cudaStreamWaitEvent(st, ev.e, 0));
@@ -1141,6 +1480,14 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
   };
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+  {
+    const std::string bad = device_pointer_problem(device, {{a_device, "a_device"}, {x_device, "x_device"}});
+    if (!bad.empty()) {
+      noalloc_message(msg, msg_len, bad);
+      if (prev >= 0) cudaSetDevice(prev);
+      return NEMOH_B200_EINVAL;
+    }
+  }
   unsigned char* base = nullptr;
   {
     // set-up, once per device (the first call on the device): look up the

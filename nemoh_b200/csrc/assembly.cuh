@@ -159,6 +159,18 @@ struct AsmOut {
   float2* d32 = nullptr;   // optional FP32 copy of the final D (same layout), for the mixed LU
 };
 
+// Ragged batches (frequency slots of different bodies in one launch): the
+// mesh and output place of each slot. Without it every slot uses the
+// kernel's own mesh arguments and slot * slot_stride.
+struct SlotMesh {
+  const PanelRec* rec;
+  const double* rows;
+  long long off;   // element offset of the slot's D+ (and S+, FP32 copy); D-/S- follow after n*n
+  int n;
+  int nsymy;
+  double zer;
+};
+
 __device__ __forceinline__ void stage_panels(const PanelRec* __restrict__ rec, int j0, int nj, PanelRec* sp) {
   const double* src = reinterpret_cast<const double*>(rec + j0);
   double* dst = reinterpret_cast<double*>(sp);
@@ -176,12 +188,24 @@ template <bool FD>
 __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(GreenCtx g, const OmegaParams* __restrict__ oms,
                                                            const int* __restrict__ slots,
                                                            const PanelRec* __restrict__ rec,
-                                                           const double* __restrict__ rows, int N, AsmOut out) {
+                                                           const double* __restrict__ rows, int N, AsmOut out,
+                                                           const SlotMesh* __restrict__ meshes) {
   __shared__ PanelRec sp[ASM_TJ];
   __shared__ OmegaParams som;
   const int slot = slots[blockIdx.z];
-  stage_params(oms + slot, &som);
+  long long base = slot * out.slot_stride;
+  if (meshes) {
+    const SlotMesh m = meshes[slot];
+    rec = m.rec;
+    rows = m.rows;
+    N = m.n;
+    g.nsymy = m.nsymy;
+    g.zer = m.zer;
+    base = m.off;
+  }
   const int j0 = blockIdx.y * ASM_TJ;
+  if (j0 >= N || (int)blockIdx.x * ASM_ROWS >= N) return;   // beyond a smaller slot's order (whole CTA)
+  stage_params(oms + slot, &som);
   const int nj = min(ASM_TJ, N - j0);
   stage_panels(rec, j0, nj, sp);
   __syncthreads();
@@ -190,8 +214,8 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(Gre
   const double XGI = rows[I], YGI = rows[N + I], ZGI = rows[2 * N + I];
   const double XNI = rows[3 * N + I], YNI = rows[4 * N + I], ZNI = rows[5 * N + I];
   const long long NN = (long long)N * N;
-  double2* od = out.d + slot * out.slot_stride;
-  double2* os = out.s + slot * out.slot_stride;
+  double2* od = out.d + base;
+  double2* os = out.s + base;
 #pragma unroll 1
   for (int jj = 0; jj < nj; ++jj) {
     const int J = j0 + jj;
@@ -301,14 +325,24 @@ NB_HD __forceinline__ void wave_infd_both(const GreenCtx& g, const OmegaParams& 
 template <bool FD>
 __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_WAVE_INFD) wave_sym_kernel(
     GreenCtx g, const OmegaParams* __restrict__ oms, const int* __restrict__ slots, const PanelRec* __restrict__ rec,
-    int N, AsmOut out) {
+    int N, AsmOut out, const SlotMesh* __restrict__ meshes) {
   __shared__ PairOut res[2][WS_T * WS_T];   // [0]: (A_i, B_j) at j*T+i; [1]: (B_j, A_i) at i*T+j
   __shared__ PanelRec pa[WS_T], pb[WS_T];
   __shared__ OmegaParams som;
+  const int slot = slots[blockIdx.z];
+  long long base = slot * out.slot_stride;
+  if (meshes) {
+    const SlotMesh m = meshes[slot];
+    rec = m.rec;
+    N = m.n;
+    g.nsymy = m.nsymy;
+    g.zer = m.zer;
+    base = m.off;
+  }
   const int T = (N + WS_T - 1) / WS_T;
+  if ((int)blockIdx.x >= T * (T + 1) / 2) return;   // beyond a smaller slot's tiles (whole CTA)
   int ta, tb;
   tri_tile(blockIdx.x, T, ta, tb);
-  const int slot = slots[blockIdx.z];
   stage_params(oms + slot, &som);
   const int a0 = ta * WS_T, b0 = tb * WS_T;
   const int na = min(WS_T, N - a0), nb = min(WS_T, N - b0);
@@ -345,9 +379,9 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
   }
   __syncthreads();
   const long long NN = (long long)N * N;
-  double2* od = out.d + slot * out.slot_stride;
-  double2* os = out.s + slot * out.slot_stride;
-  float2* o32 = out.d32 ? out.d32 + slot * out.slot_stride : nullptr;
+  double2* od = out.d + base;
+  double2* os = out.s + base;
+  float2* o32 = out.d32 ? out.d32 + base : nullptr;
   auto add = [&](long long o, const PairOut& r) {
     double2 d = od[o], sv = os[o];
     const double2 dn = make_double2(d.x + r.dp_re, r.dp_im);

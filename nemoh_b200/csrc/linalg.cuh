@@ -14,6 +14,8 @@
 // path (mixed.cuh) defers the update outside a 128-column panel to one
 // tensor-core product per panel.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace nb200 {
@@ -22,15 +24,41 @@ constexpr int LU_NB = 32;     // panel width
 constexpr int LU_RB = 128;    // rows per L21 CTA
 constexpr int LU_CB = 64;     // columns per U12 CTA
 
+// A batch of systems. Uniform: every system has order n and starts `stride`
+// elements after the previous one. Ragged (systems of different bodies in one
+// launch sequence): `off` and `ord` (device arrays) give each system's offset
+// and order, n is the largest order, and the systems are sorted by decreasing
+// order so that the systems still active at an elimination step are a prefix
+// of the batch; every kernel takes its own system's order and leaves the parts
+// of the launch grid beyond it. Per-system scratch (diag, pinv, inverted
+// diagonal blocks, right-hand sides) keeps uniform strides sized by n.
 template <class C2>
 struct BatchT {
-  C2* base;               // system s at base + s * stride
-  long long stride;       // elements between systems
-  int n;                  // order (leading dimension = n)
+  C2* base;               // system s at base + s * stride (uniform) or base + off[s] (ragged)
+  long long stride;       // elements between systems (uniform)
+  int n;                  // order (uniform), largest order (ragged)
   C2* diag;               // DIAG_SCRATCH elements per system: factored A11, inv(L11), inv(U11)
   C2* pinv = nullptr;     // optional, PINV_SCRATCH per system: inv(L) of the LU_OUTER / LU_NB
                           // diagonal blocks of the current outer panel (two-level LU only)
+  const long long* off = nullptr;   // ragged: element offset of each system
+  const int* ord = nullptr;         // ragged: order (and leading dimension) of each system
+  __device__ __forceinline__ int order(int s) const { return ord ? ord[s] : n; }
+  __device__ __forceinline__ C2* sys(int s) const { return base + (off ? off[s] : (long long)s * stride); }
 };
+// The ragged description of a batch: device arrays for the kernels, and the
+// orders again on the host (decreasing) for the launch loop.
+struct Ragged {
+  const long long* off = nullptr;
+  const int* ord = nullptr;
+  const int* host_ord = nullptr;
+};
+template <class C2>
+inline BatchT<C2> make_batch(C2* base, int n, C2* diag, C2* pinv, const Ragged& rg) {
+  BatchT<C2> b{base, (long long)n * n, n, diag, pinv};
+  b.off = rg.off;
+  b.ord = rg.ord;
+  return b;
+}
 constexpr int DIAG_SCRATCH = 3 * LU_NB * LU_NB;
 constexpr int LU_OUTER = 128;
 constexpr int PINV_SCRATCH = (LU_OUTER / LU_NB) * LU_NB * LU_NB;
@@ -80,11 +108,12 @@ __global__ void __launch_bounds__(1024) lu_diag_kernel(BatchT<C2> b, int k, int*
   __shared__ C2 sb[LU_NB * LU_NB];   // the block, column-major, ld = nb
   __shared__ C2 xl[LU_NB * LU_NB];   // inv(L11), ld = LU_NB
   __shared__ C2 xu[LU_NB * LU_NB];   // inv(U11), ld = LU_NB
-  const int n = b.n;
+  const int n = b.order(blockIdx.z);
+  if (k >= n) return;
   const int nb = min(LU_NB, n - k);
   const int i = threadIdx.x & (LU_NB - 1), c = threadIdx.x / LU_NB;
   const bool in = i < nb && c < nb;
-  const C2* A = b.base + blockIdx.z * b.stride;
+  const C2* A = b.sys(blockIdx.z);
   if (in) sb[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
@@ -141,9 +170,11 @@ template <class C2>
 __global__ void __launch_bounds__(LU_RB) lu_panel_kernel(BatchT<C2> b, int k, int ucol_end) {
   __shared__ C2 inv[LU_NB * LU_NB];
   __shared__ C2 work[LU_NB * LU_CB];
-  const int n = b.n;
+  const int n = b.order(blockIdx.z);
+  if (k >= n) return;
+  ucol_end = min(ucol_end, n);
   const int nb = min(LU_NB, n - k);
-  C2* A = b.base + blockIdx.z * b.stride;
+  C2* A = b.sys(blockIdx.z);
   const C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   const int rest = n - k - nb;
   const int nrb = (rest + LU_RB - 1) / LU_RB;
@@ -228,10 +259,14 @@ __global__ void __launch_bounds__(128) zgemm_update_kernel(BatchT<C2> b, int k, 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2* stage0 = reinterpret_cast<C2*>(smem_raw);
   constexpr int STAGE = GM_KC * GM_T + GM_KC * GM_BS;   // As [16][64] then Bs [16][65]
-  const int n = b.n;
+  const int n = b.order(blockIdx.z);
+  rc.r1 = min(rc.r1, n);
+  rc.c1 = min(rc.c1, n);
+  kb = min(kb, n - k);
   const int r0 = rc.r0 + blockIdx.y * GM_T;
   const int c0 = rc.c0 + blockIdx.x * GM_T;
-  C2* A = b.base + blockIdx.z * b.stride;
+  if (r0 >= rc.r1 || c0 >= rc.c1 || kb <= 0) return;
+  C2* A = b.sys(blockIdx.z);
   const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
   auto load = [&](int s, int k0) {
     C2* As = stage0 + s * STAGE;
@@ -332,9 +367,10 @@ __global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
   C2* X = reinterpret_cast<C2*>(strip_sm);   // [ST_C][LU_OUTER]
   C2* T = X + LU_OUTER * ST_C;              // [LU_NB][LU_NB] inv(L_jj) or L_ij, column-major
   C2* Y = T + LU_NB * LU_NB;                // [ST_C][LU_NB]
-  const int n = b.n, kend = k0 + LU_OUTER;
+  const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
   const int c0 = kend + blockIdx.x * ST_C, ncol = min(ST_C, n - c0);
-  C2* A = b.base + blockIdx.z * b.stride;
+  if (ncol <= 0) return;
+  C2* A = b.sys(blockIdx.z);
   const C2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
   for (int q = threadIdx.x; q < LU_OUTER * ST_C; q += blockDim.x) {
     const int r = q % LU_OUTER, c = q / LU_OUTER;
@@ -445,57 +481,83 @@ inline void lane_join(const LaneSplit& L, cudaStream_t main, const Lanes* lanes)
 template <class C2>
 inline BatchT<C2> sub_batch(const BatchT<C2>& b, int s0) {
   BatchT<C2> r = b;
-  r.base = b.base + s0 * b.stride;
+  if (b.off) {
+    r.off = b.off + s0;
+    r.ord = b.ord + s0;
+  } else {
+    r.base = b.base + s0 * b.stride;
+  }
   r.diag = b.diag + (long long)s0 * DIAG_SCRATCH;
   if (b.pinv) r.pinv = b.pinv + (long long)s0 * PINV_SCRATCH;
   return r;
 }
 
-// outer(bsub, nsub, stream, s0, k0, kend): trailing update of one group
+// outer(bsub, nsub, stream, s0, k0, kend): trailing update of one group.
+// host_ord (ragged batches): the systems' orders on the host, in decreasing
+// order; at every step only the systems still above it are launched (a prefix
+// of each group) and the grids are sized by the group's largest system.
 template <class C2, class Outer>
 inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main, long long& launches, Outer outer,
-                         const Lanes* lanes = nullptr) {
+                         const Lanes* lanes = nullptr, const int* host_ord = nullptr) {
   const int n = b.n;
   const LaneSplit L = lane_split(nsys, main, lanes);
+  // systems of group g whose order exceeds k
+  auto active = [&](int g, int k) {
+    const int s0 = L.first[g], s1 = L.first[g + 1];
+    if (!host_ord) return k < n ? s1 - s0 : 0;
+    int c = 0;
+    while (s0 + c < s1 && host_ord[s0 + c] > k) ++c;
+    return c;
+  };
   for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
-    const int kend = std::min(k0 + LU_OUTER, n);
-    for (int k = k0; k < kend; k += LU_NB) {
-      const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
-      const int nrb = (rest + LU_RB - 1) / LU_RB;
-      // with b.pinv the row strip right of the panel waits for strip_kernel
-      const int ucol = b.pinv ? kend : n;
-      const int ncb_used = (std::max(0, ucol - k - nb) + LU_CB - 1) / LU_CB;
+    for (int k = k0; k < std::min(k0 + LU_OUTER, n); k += LU_NB) {
       for (int g = 0; g < L.groups; ++g) {
-        const int s0 = L.first[g], ns = L.first[g + 1] - s0;
-        const BatchT<C2> bg = sub_batch(b, s0);
+        const int ns = active(g, k);
+        if (ns == 0) continue;
+        const int s0 = L.first[g];
+        const int ng = host_ord ? host_ord[s0] : n;   // largest order in the group
+        const int kend = std::min(k0 + LU_OUTER, ng);
+        const int nb = std::min(LU_NB, ng - k), rest = ng - k - nb;
+        const int nrb = (rest + LU_RB - 1) / LU_RB;
+        // with b.pinv the row strip right of the panel waits for strip_kernel
+        const int ucol = b.pinv ? kend : ng;
+        const int ncb_used = (std::max(0, ucol - k - nb) + LU_CB - 1) / LU_CB;
+        BatchT<C2> bg = sub_batch(b, s0);
+        bg.n = ng;
         const cudaStream_t st = L.st[g];
         lu_diag_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, 0, st>>>(bg, k, status);
         ++launches;
         lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb_used), 1, ns), LU_RB, 0, st>>>(bg, k, ucol);
         ++launches;
         if (k + nb < kend) {
-          zgemm_update<C2>(bg, k, nb, Rect{k + nb, n, k + nb, kend}, ns, st);
+          zgemm_update<C2>(bg, k, nb, Rect{k + nb, ng, k + nb, kend}, ns, st);
           ++launches;
-          if (kend < n && !b.pinv) {
-            zgemm_update<C2>(bg, k, nb, Rect{k + nb, kend, kend, n}, ns, st);
+          if (kend < ng && !b.pinv) {
+            zgemm_update<C2>(bg, k, nb, Rect{k + nb, kend, kend, ng}, ns, st);
             ++launches;
           }
         }
       }
     }
     for (int g = 0; g < L.groups; ++g) {
-      const int s0 = L.first[g], ns = L.first[g + 1] - s0;
-      const BatchT<C2> bg = sub_batch(b, s0);
+      const int ns = active(g, k0);
+      if (ns == 0) continue;
+      const int s0 = L.first[g];
+      const int ng = host_ord ? host_ord[s0] : n;
+      const int kend = std::min(k0 + LU_OUTER, ng);
+      if (kend >= ng) continue;
+      BatchT<C2> bg = sub_batch(b, s0);
+      bg.n = ng;
       const cudaStream_t st = L.st[g];
-      if (kend < n && b.pinv) {
+      if (b.pinv) {
         static std::atomic<unsigned long long> attr{0};
         once_per_device(attr, [] {
           cudaFuncSetAttribute(strip_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_smem<C2>());
         });
-        strip_kernel<C2><<<dim3((n - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
+        strip_kernel<C2><<<dim3((ng - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
         ++launches;
       }
-      if (kend < n) outer(bg, ns, st, s0, k0, kend);
+      outer(bg, ns, st, s0, k0, kend);
     }
   }
   lane_join(L, main, lanes);
@@ -517,6 +579,73 @@ __global__ void fold_rhs_kernel(const double2* __restrict__ nvel, int n, int nsy
     X[((long long)w * 2 + 1) * n * nrhs + (long long)p * n + i] = make_double2((a.x - b.x) * 0.5, (a.y - b.y) * 0.5);
   } else {
     X[(long long)w * n * nrhs + (long long)p * n + i] = v[i];
+  }
+}
+
+// One (body, frequency) item of a ragged batch: where its inputs and outputs
+// are in the caller's arrays (items in the caller's order) and where its
+// systems are in the batch (sorted by decreasing order).
+struct ItemDesc {
+  long long nvel_off;    // complex offset of the item's NVEL, (2^s n) x nrhs column-major
+  long long force_off;   // complex offset of the item's forces, nint x nrhs
+  const double* nds;     // the body's generalised normals, nint x (2^s n)
+  double rho;
+  int n, nsymy, sys0, nint;
+};
+
+// fold_rhs_kernel per item; X: system s at s * xstride, leading dimension n
+__global__ void fold_rhs_ragged_kernel(const double2* __restrict__ nvel, const ItemDesc* __restrict__ items, int nrhs,
+                                       long long xstride, double2* __restrict__ X) {
+  const ItemDesc it = items[blockIdx.z];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, p = blockIdx.y, n = it.n;
+  if (i >= n) return;
+  const int cls = it.nsymy ? 2 : 1;
+  const double2* v = nvel + it.nvel_off + (long long)p * cls * n;
+  double2* x0 = X + it.sys0 * xstride + (long long)p * n;
+  if (it.nsymy) {
+    const double2 a = v[i], b = v[i + n];
+    x0[i] = make_double2((a.x + b.x) * 0.5, (a.y + b.y) * 0.5);
+    x0[xstride + i] = make_double2((a.x - b.x) * 0.5, (a.y - b.y) * 0.5);
+  } else {
+    x0[i] = v[i];
+  }
+}
+
+// force_kernel per item (its frequency's parameters in oms[item])
+__global__ void __launch_bounds__(256) force_ragged_kernel(const double2* __restrict__ phi,
+                                                           const ItemDesc* __restrict__ items,
+                                                           const OmegaParams* __restrict__ oms, int nrhs,
+                                                           long long xstride, double2* __restrict__ force) {
+  const ItemDesc it = items[blockIdx.z];
+  const int i = blockIdx.x, p = blockIdx.y, n = it.n;
+  if (i >= it.nint) return;
+  const int cls = it.nsymy ? 2 : 1;
+  const double2* pp = phi + it.sys0 * xstride + (long long)p * n;
+  const double2* pm = pp + (cls - 1) * xstride;
+  double sr = 0., si = 0.;
+  for (int c = threadIdx.x; c < cls * n; c += blockDim.x) {
+    double2 z;
+    if (!it.nsymy) z = pp[c];
+    else if (c < n) z = make_double2(pp[c].x + pm[c].x, pp[c].y + pm[c].y);
+    else z = make_double2(pp[c - n].x - pm[c - n].x, pp[c - n].y - pm[c - n].y);
+    const double f = it.nds[i + (long long)it.nint * c];
+    sr += z.x * f;
+    si += z.y * f;
+  }
+  __shared__ double red[2][256];
+  red[0][threadIdx.x] = sr;
+  red[1][threadIdx.x] = si;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double rw = it.rho * oms[blockIdx.z].w;
+    force[it.force_off + (long long)p * it.nint + i] = make_double2(rw * red[1][0], -rw * red[0][0]);
   }
 }
 
@@ -592,8 +721,9 @@ __global__ void __launch_bounds__(INV_THREADS) inv_diag_kernel(BatchT<C2> b, C2*
   C2* T = reinterpret_cast<C2*>(dsm);   // [TB][TB] the block
   C2* XL = T + TB * TB;                 // inv(L)
   C2* XU = XL + TB * TB;                // inv(U)
-  const int n = b.n, blk = blockIdx.x, k = blk * TB, nb = min(TB, n - k);
-  const C2* A = b.base + blockIdx.z * b.stride;
+  const int n = b.order(blockIdx.z), blk = blockIdx.x, k = blk * TB, nb = min(TB, n - k);
+  if (nb <= 0) return;
+  const C2* A = b.sys(blockIdx.z);
   const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
   for (int q = threadIdx.x; q < TB * TB; q += blockDim.x) {
     const int i = q % TB, c = q / TB;
@@ -770,6 +900,194 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
   lane_join(L, main, lanes);
 }
 
+// ---------------------------------------------------------------------------
+// Triangular sweep in one launch per direction. A thread-block cluster of
+// `csize` CTAs (1..8, one cluster per system along grid.x) owns the 64-row
+// blocks of one system cyclically (block i belongs to CTA i mod csize). Step s
+// of the forward sweep:
+//   * every CTA copies the solved block y_s from its owner's shared memory
+//     (distributed shared memory) and subtracts L[rows, block s] y_s from the
+//     right-hand sides of its own rows below block s (right-looking, so a row
+//     block only ever receives updates from the CTA that owns it);
+//   * the owner of block s+1, whose rows are then complete, solves
+//     y_{s+1} = inv(L_{s+1,s+1}) r_{s+1} with the inverted diagonal block
+//     (prefetched by cp.async during the update) into one of two shared
+//     buffers, and writes it to Y;
+//   * one cluster barrier (hardware) ends the step. The two y buffers
+//     alternate, so a buffer is rewritten only after the barrier that follows
+//     every read of it.
+// The backward sweep runs the same way from the last block with U. X holds the
+// right-hand sides and is overwritten by partial sums; Y receives the solution.
+// `active` (may be null): the launch does nothing when *active == 0 (a
+// converged refinement), read uniformly by every CTA.
+// ---------------------------------------------------------------------------
+constexpr int SW_THREADS = 256;
+template <class C2, int NR>
+constexpr int sweep_smem() {
+  return (TB * TB + 4 * TB * NR) * (int)sizeof(C2);   // inverse block, y buffers x2, local y, r block
+}
+
+template <class C2, int NR, bool LOWER>
+__global__ void __launch_bounds__(SW_THREADS) trsm_sweep_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk,
+                                                                C2* xbase, C2* ybase, long long xstride,
+                                                                const int* active) {
+  namespace cg = cooperative_groups;
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char sw_sm[];
+  C2* Ti = reinterpret_cast<C2*>(sw_sm);   // [TB][TB] inverse of the block being solved, column-major
+  C2* ybuf = Ti + TB * TB;                 // [2][NR][TB] solved blocks (read by the whole cluster)
+  C2* yloc = ybuf + 2 * TB * NR;           // [NR][TB] local copy of the block applied in this step
+  C2* rb = yloc + TB * NR;                 // [NR][TB] right-hand sides of the block being solved
+  cg::cluster_group cl = cg::this_cluster();
+  const int csize = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int sys = blockIdx.x / csize;
+  const int n = b.order(sys);
+  const C2* A = b.sys(sys);
+  C2* X = xbase + sys * xstride;
+  C2* Y = ybase + sys * xstride;
+  // nblk: the stride of the inverted blocks per system; this system has nbs blocks
+  const C2* invs = inv + (long long)sys * nblk * 2 * TB * TB + (LOWER ? 0 : TB * TB);
+  const int nbs = (n + TB - 1) / TB;
+  const int t = threadIdx.x;
+  const int step = LOWER ? 1 : -1;
+  const int first = LOWER ? 0 : nbs - 1, last = LOWER ? nbs - 1 : 0;
+  auto prefetch_inv = [&](int blk) {
+    const C2* src = invs + (long long)blk * 2 * TB * TB;
+    for (int q = t; q < TB * TB; q += SW_THREADS) cp_async_elem(Ti + q, src + q, true);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // owner: rb <- X rows of blk (zero past n), then y = Ti rb into ybuf[blk & 1] and Y
+  auto solve = [&](int blk) {
+    const int k = blk * TB, nb = min(TB, n - k);
+    for (int q = t; q < TB * NR; q += SW_THREADS) {
+      const int i = q % TB, p = q / TB;
+      rb[q] = i < nb ? X[(k + i) + (long long)n * p] : mkc<C2>(0., 0.);
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    C2* yb = ybuf + (blk & 1) * TB * NR;
+    const int i = t % TB;
+    for (int p = t / TB; p < NR; p += SW_THREADS / TB) {
+      C2 acc = mkc<C2>(0., 0.);
+#pragma unroll 8
+      for (int j = 0; j < TB; ++j) cmac(acc, Ti[i + TB * j], rb[j + TB * p]);
+      yb[i + TB * p] = acc;
+      if (i < nb) Y[(k + i) + (long long)n * p] = acc;
+    }
+  };
+  if (rank == first % csize) {
+    prefetch_inv(first);
+    solve(first);
+  }
+  cl.sync();
+  for (int s = first; s != last; s += step) {
+    const int nxt = s + step;
+    const bool owns_next = rank == nxt % csize;
+    if (owns_next) prefetch_inv(nxt);
+    const C2* src = cl.map_shared_rank(ybuf + (s & 1) * TB * NR, s % csize);
+    for (int q = t; q < TB * NR; q += SW_THREADS) yloc[q] = src[q];
+    __syncthreads();
+    // own row blocks still to come: forward i > s, backward i < s
+    const int k = s * TB, nb = min(TB, n - k);
+    const int i0 = LOWER ? s + 1 : 0, i1 = LOWER ? nbs : s;   // [i0, i1)
+    int mine0 = i0 + ((rank - i0 % csize) % csize + csize) % csize;   // first block >= i0 owned here
+    for (int ib = mine0 + (t / TB) * csize; ib < i1; ib += (SW_THREADS / TB) * csize) {
+      const int r = ib * TB + (t % TB);
+      if (r >= n) continue;
+      const C2* Ar = A + r + (long long)n * k;
+      C2 acc[NR];
+#pragma unroll
+      for (int p = 0; p < NR; ++p) acc[p] = mkc<C2>(0., 0.);
+      C2 a[8];
+#pragma unroll 1
+      for (int c8 = 0; c8 < nb; c8 += 8) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = (c8 + j < nb) ? Ar[(long long)n * (c8 + j)] : mkc<C2>(0., 0.);
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+          for (int p = 0; p < NR; ++p) cmac(acc[p], a[j], yloc[(c8 + j) + TB * p]);
+      }
+#pragma unroll
+      for (int p = 0; p < NR; ++p) {
+        C2* q = X + r + (long long)n * p;
+        C2 v = *q;
+        v.x -= acc[p].x;
+        v.y -= acc[p].y;
+        *q = v;
+      }
+    }
+    __syncthreads();
+    if (owns_next) solve(nxt);
+    cl.sync();
+  }
+}
+
+// cluster size of the sweep: enough CTAs in flight for the device (about two
+// per SM), at most 8 per system (portable cluster size), a power of two
+inline int sweep_cluster(int nsys, int nblk, int sms) {
+  int c = 1;
+  while (c < 8 && c < nblk && (long long)nsys * c < 2LL * sms) c *= 2;
+  return c;
+}
+
+template <class C2, int NR, bool LOWER>
+inline cudaError_t trsm_sweep_nr(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int csize, cudaStream_t st,
+                                 const int* active) {
+  const int n = b.n, nblk = (n + TB - 1) / TB;
+  constexpr int smem = sweep_smem<C2, NR>();
+  static std::atomic<unsigned long long> attr{0};
+  once_per_device(attr, [] {
+    cudaFuncSetAttribute(trsm_sweep_kernel<C2, NR, LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  });
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nsys * csize), 1, 1);
+  cfg.blockDim = dim3(SW_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)csize;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, trsm_sweep_kernel<C2, NR, LOWER>, b, inv, nblk, X, Y, (long long)n * NR, active);
+}
+
+// Forward then backward sweep of nsys factored systems (nrhs right-hand sides
+// in X, solution back in X, Y scratch of the same size): two launches.
+// csize <= 0 picks the cluster size from the device's SM count.
+template <class C2>
+inline cudaError_t trsm_sweep(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st,
+                              long long& launches, const int* active = nullptr, int csize = 0) {
+  if (csize <= 0) {
+    static int sms = 0;
+    if (!sms) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (sms <= 0) sms = 148;
+    }
+    csize = sweep_cluster(nsys, (b.n + TB - 1) / TB, sms);
+  }
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (nrhs) {
+#define NB200_SW(k)                                                                          \
+  case k:                                                                                    \
+    e = trsm_sweep_nr<C2, k, true>(b, inv, X, Y, nsys, csize, st, active);                   \
+    if (e == cudaSuccess) e = trsm_sweep_nr<C2, k, false>(b, inv, Y, X, nsys, csize, st, active); \
+    break;
+    NB200_SW(1) NB200_SW(2) NB200_SW(3) NB200_SW(4) NB200_SW(5) NB200_SW(6) NB200_SW(7) NB200_SW(8)
+    NB200_SW(9) NB200_SW(10) NB200_SW(11) NB200_SW(12) NB200_SW(13) NB200_SW(14) NB200_SW(15) NB200_SW(16)
+#undef NB200_SW
+    default:
+      break;
+  }
+  launches += 2;
+  return e;
+}
+
 // Y += sign * M X (FP64) with the columns split over blockIdx.y; partial sums
 // are added with atomics, so Y must hold its initial value (0 or the RHS).
 // The number of right-hand sides is a template parameter so that no
@@ -780,12 +1098,15 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
 constexpr int MV_COLS = 128;
 template <int NR>
 __global__ void __launch_bounds__(128, 4) matvec_acc_kernel(Batch m, const double2* __restrict__ xbase, long long xstride,
-                                                         double2* ybase, long long ystride, double sign) {
+                                                         double2* ybase, long long ystride, double sign,
+                                                         const int* active) {
+  if (active && *active == 0) return;   // a converged refinement skips its remaining passes
   __shared__ double2 Xs[MV_COLS * NR];
-  const int n = m.n;
-  const double2* M = m.base + blockIdx.z * m.stride;
+  const int n = m.order(blockIdx.z);
+  const double2* M = m.sys(blockIdx.z);
   const double2* X = xbase + blockIdx.z * xstride;
   const int c0 = blockIdx.y * MV_COLS, nc = min(MV_COLS, n - c0);
+  if (nc <= 0 || (int)(blockIdx.x * blockDim.x) >= n) return;
   for (int q = threadIdx.x; q < MV_COLS * NR; q += blockDim.x) {
     const int c = q % MV_COLS, p = q / MV_COLS;
     Xs[c * NR + p] = (c < nc) ? X[(c0 + c) + (long long)n * p] : make_double2(0., 0.);
@@ -823,19 +1144,20 @@ __global__ void __launch_bounds__(128, 4) matvec_acc_kernel(Batch m, const doubl
 
 template <int NR>
 inline void matvec_acc_nr(Batch m, const double2* x, long long xs, double2* y, long long ys, int nsys, double sign,
-                          cudaStream_t st) {
+                          cudaStream_t st, const int* active) {
   const int n = m.n;
   matvec_acc_kernel<NR><<<dim3((n + 127) / 128, (n + MV_COLS - 1) / MV_COLS, nsys), 128, 0, st>>>(m, x, xs, y, ys,
-                                                                                                  sign);
+                                                                                                  sign, active);
 }
 
-// Y += sign * M X for nsys systems with nrhs (1..MAX_RHS) right-hand sides
+// Y += sign * M X for nsys systems with nrhs (1..MAX_RHS) right-hand sides;
+// with `active`, nothing is done when *active == 0 on the device
 inline void matvec_acc(Batch m, const double2* x, long long xs, double2* y, long long ys, int nrhs, int nsys,
-                       double sign, cudaStream_t st) {
+                       double sign, cudaStream_t st, const int* active = nullptr) {
   switch (nrhs) {
-#define NB200_MV(k)                                    \
-  case k:                                              \
-    matvec_acc_nr<k>(m, x, xs, y, ys, nsys, sign, st); \
+#define NB200_MV(k)                                            \
+  case k:                                                      \
+    matvec_acc_nr<k>(m, x, xs, y, ys, nsys, sign, st, active); \
     break;
     NB200_MV(1) NB200_MV(2) NB200_MV(3) NB200_MV(4) NB200_MV(5) NB200_MV(6) NB200_MV(7) NB200_MV(8)
     NB200_MV(9) NB200_MV(10) NB200_MV(11) NB200_MV(12) NB200_MV(13) NB200_MV(14) NB200_MV(15) NB200_MV(16)

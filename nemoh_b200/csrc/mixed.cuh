@@ -38,6 +38,18 @@ inline int refine_max_it() {
 // solved again with FP64 factors.
 constexpr double REFINE_TOL = 1e-12;
 
+// Refinement state on the device: decided by the last CTA of each residual
+// pass, read by every later kernel of the refinement (which do nothing once
+// `active` is 0) and by the host once per batch.
+struct RefineState {
+  int active;          // 1 while another pass is wanted
+  int iterations;      // passes whose residual was measured
+  int done_ctas;       // CTAs of the current residual pass that have finished
+  int max_it;
+  double worst;        // largest |r|inf / |b|inf of the last pass
+  double prev;         // the same, one pass earlier
+};
+
 struct MixedWork {
   float2* lu = nullptr;      // FP32 factors, nsys x n x n
   float2* diag = nullptr;    // diagonal-block scratch (factors and inverses)
@@ -48,8 +60,9 @@ struct MixedWork {
   float2* inv = nullptr;     // inverses of the diagonal blocks of L and U (FP32)
   float2* pinv = nullptr;    // inv(L) of the diagonal blocks of the current outer panel
   unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
+  RefineState* state = nullptr;         // refinement decisions on the device
   TcWork tc;                 // tensor-core GEMM operand buffers
-  size_t have[9] = {};       // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv
+  size_t have[10] = {};      // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv, state
   size_t total = 0;
   int last_iterations = 0;
   double last_residual = 0.;
@@ -58,10 +71,10 @@ struct MixedWork {
   size_t bytes() const { return total; }
   void release() {
     cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms); cudaFree(inv);
-    cudaFree(pinv);
+    cudaFree(pinv); cudaFree(state);
     tc.release();
     lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr; inv = nullptr;
-    pinv = nullptr;
+    pinv = nullptr; state = nullptr;
     for (size_t& h : have) h = 0;
     total = 0;
   }
@@ -70,9 +83,10 @@ struct MixedWork {
   // (strides always follow the current n), so a smaller mesh with more
   // systems reuses what a larger one left and nothing is freed needlessly:
   // cudaFree synchronizes the whole device.
-  cudaError_t ensure(int nsys, int n, int nrhs) {
+  // mat_elems: elements of all matrices of a ragged batch (0: nsys x n x n)
+  cudaError_t ensure(int nsys, int n, int nrhs, size_t mat_elems = 0) {
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
-    const size_t need[9] = {nsys * NN * sizeof(float2),
+    const size_t need[10] = {(mat_elems ? mat_elems : nsys * NN) * sizeof(float2),
                             (size_t)nsys * DIAG_SCRATCH * sizeof(float2),
                             V * sizeof(double2),
                             V * sizeof(double2),
@@ -80,10 +94,11 @@ struct MixedWork {
                             V * sizeof(float2),
                             (size_t)2 * nsys * nrhs * sizeof(unsigned long long),
                             (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2),
-                            (size_t)nsys * PINV_SCRATCH * sizeof(float2)};
-    void** ptr[9] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
-                     (void**)&inv, (void**)&pinv};
-    for (int i = 0; i < 9; ++i) {
+                            (size_t)nsys * PINV_SCRATCH * sizeof(float2),
+                            sizeof(RefineState)};
+    void** ptr[10] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
+                      (void**)&inv, (void**)&pinv, (void**)&state};
+    for (int i = 0; i < 10; ++i) {
       if (need[i] <= have[i]) continue;
       cudaFree(*ptr[i]);
       *ptr[i] = nullptr;
@@ -112,24 +127,14 @@ __global__ void d2f_kernel(const double2* __restrict__ a, float2* __restrict__ b
   }
 }
 
-// x += correction (FP32 -> FP64); on the first pass x = correction
-__global__ void accumulate_kernel(double2* __restrict__ x, const float2* __restrict__ d, long long count, int first) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < count; q += (long long)gridDim.x * blockDim.x) {
-    const float2 v = d[q];
-    if (first) x[q] = make_double2(v.x, v.y);
-    else {
-      double2 o = x[q];
-      o.x += v.x;
-      o.y += v.y;
-      x[q] = o;
-    }
-  }
-}
-
-// |b|inf per (system, rhs)
-__global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsigned long long* out) {
+// |b|inf per (system, rhs). Vectors of system s start at s * nrhs * n (n =
+// the largest order of a ragged batch, `ord` its systems' orders, or null)
+// with leading dimension the system's own order.
+__global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsigned long long* out,
+                            const int* __restrict__ ord) {
   const int p = blockIdx.y, s = blockIdx.z;
-  const double2* x = v + ((long long)s * nrhs + p) * n;
+  const double2* x = v + (long long)s * nrhs * n + (long long)p * (ord ? ord[s] : n);
+  if (ord) n = ord[s];
   double m = 0.;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     m = fmax(m, fmax(fabs(x[i].x), fabs(x[i].y)));
@@ -137,30 +142,19 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
   if ((threadIdx.x & 31) == 0) atomicMax(out + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
-// rf = (float) r and |r|inf per (system, rhs), r = b - D x formed beforehand
-__global__ void residual_finish_kernel(const double2* __restrict__ r, float2* __restrict__ rf, int n, int nrhs,
-                                       unsigned long long* __restrict__ rnorm) {
-  const int p = blockIdx.y, s = blockIdx.z;
-  const long long base = ((long long)s * nrhs + p) * n;
-  double m = 0.;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double2 v = r[base + i];
-    rf[base + i] = make_float2((float)v.x, (float)v.y);
-    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
-  }
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(rnorm + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
-}
-
 // have_f32: the assembly already wrote the FP32 copy of D into w.lu
+// rg: ragged batch (systems sorted by decreasing order, n the largest; the
+// FP32 copy in w.lu has the same element offsets as D); mat_elems: elements
+// of all matrices (for the conversion when the copy is not there yet)
 inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches,
-                         const Lanes* lanes = nullptr, bool have_f32 = false) {
+                         const Lanes* lanes = nullptr, bool have_f32 = false, const Ragged& rg = Ragged(),
+                         long long mat_elems = -1) {
   if (!have_f32) {
-    const long long total = (long long)nsys * n * n;
+    const long long total = mat_elems >= 0 ? mat_elems : (long long)nsys * n * n;
     d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
     ++launches;
   }
-  BatchT<float2> b{w.lu, (long long)n * n, n, w.diag, w.pinv};
+  BatchT<float2> b = make_batch<float2>(w.lu, n, w.diag, w.pinv, rg);
   const size_t tiles = (size_t)(n + TC_T - 1) / TC_T;
   lu_two_level<float2>(
       b, nsys, status, st, launches,
@@ -169,11 +163,11 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
         tg.a += (size_t)s0 * tiles * TC_NCH * 2 * TC_AIMG;
         tg.b += (size_t)s0 * tiles * TC_NCH * 2 * TC_BIMG;
         if (!tc_update(tg, bg, k0, ns, sg, launches, status)) {
-          zgemm_update<float2>(bg, k0, kend - k0, Rect{kend, n, kend, n}, ns, sg);
+          zgemm_update<float2>(bg, k0, kend - k0, Rect{kend, bg.n, kend, bg.n}, ns, sg);
           ++launches;
         }
       },
-      lanes);
+      lanes, rg.host_ord);
   static std::atomic<unsigned long long> attr{0};
   once_per_device(attr, [] {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -185,53 +179,168 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
 }
 
 inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches,
-                     const Lanes* lanes) {
-  BatchT<float2> b{w.lu, (long long)n * n, n, w.diag};
-  trsm_launch<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, lanes);
+                     const int* active, const Ragged& rg) {
+  BatchT<float2> b = make_batch<float2>(w.lu, n, w.diag, nullptr, rg);
+  trsm_sweep<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, active);
   // the solution is left in w.rf (forward into yf, backward back into rf)
 }
 
-// X: right-hand sides in, solution out (FP64); Y unused scratch
-inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double2* X, double2* /*Y*/, int nrhs,
-                               cudaStream_t st, long long& launches, const Lanes* lanes = nullptr) {
-  const long long V = (long long)nsys * n * nrhs;
-  const int nv = nsys * nrhs;
-  cudaMemcpyAsync(w.b, X, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+__global__ void refine_start_kernel(RefineState* st, int max_it) {
+  st->active = 1;
+  st->iterations = 0;
+  st->done_ctas = 0;
+  st->max_it = max_it;
+  st->worst = 1e300;
+  st->prev = 1e300;
+}
+
+// x += correction (x = correction on the first pass), r = b, residual norms
+// cleared for the coming residual pass
+__global__ void refine_update_kernel(double2* __restrict__ x, const float2* __restrict__ d,
+                                     const double2* __restrict__ b, double2* __restrict__ r, long long count,
+                                     unsigned long long* __restrict__ rnorm, int nv, const RefineState* st) {
+  if (!st->active) return;
+  const int first = st->iterations == 0;
+  const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = t0; q < nv; q += stride) rnorm[q] = 0ull;
+  for (long long q = t0; q < count; q += stride) {
+    const float2 v = d[q];
+    if (first) x[q] = make_double2(v.x, v.y);
+    else {
+      double2 o = x[q];
+      o.x += v.x;
+      o.y += v.y;
+      x[q] = o;
+    }
+    r[q] = b[q];
+  }
+}
+
+// rf = (float) r and |r|inf per (system, rhs), r = b - D x formed beforehand;
+// the last CTA to finish compares the largest relative residual with the
+// tolerance and the previous pass (no CTA waits on another: the decision is
+// taken by whichever CTA counts itself last, after a fence)
+__global__ void __launch_bounds__(256) refine_residual_kernel(const double2* __restrict__ r, float2* __restrict__ rf,
+                                                              int n, int nrhs, unsigned long long* __restrict__ norms,
+                                                              int nv, RefineState* st, double tol,
+                                                              const int* __restrict__ ord) {
+  if (!st->active) return;
+  const int p = blockIdx.y, s = blockIdx.z;
+  const long long base = (long long)s * nrhs * n + (long long)p * (ord ? ord[s] : n);
+  if (ord) n = ord[s];
+  double m = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 v = r[base + i];
+    rf[base + i] = make_float2((float)v.x, (float)v.y);
+    // a NaN component counts as infinite (fmax would drop it), so a failed
+    // factorization can never pass for a converged one
+    m = fmax(m, (v.x == v.x && v.y == v.y) ? fmax(fabs(v.x), fabs(v.y)) : HUGE_VAL);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(norms + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
+  __threadfence();
+  __syncthreads();
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    const int total = gridDim.x * gridDim.y * gridDim.z;
+    last = atomicAdd(&st->done_ctas, 1) == total - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double worst = 0.;
+  for (int q = threadIdx.x; q < nv; q += blockDim.x) {
+    const double rn = __longlong_as_double((long long)atomicAdd(norms + q, 0ull));
+    const double bn = __longlong_as_double((long long)norms[nv + q]);
+    worst = fmax(worst, bn > 0 ? rn / bn : rn);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = worst;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double w = red[0];
+    const int it = st->iterations + 1;
+    st->iterations = it;
+    st->worst = w;
+    // stop at the tolerance, or as soon as the residual no longer halves
+    // (stagnation or divergence: the host then falls back to FP64 factors)
+    const bool stop = w <= tol || !(w == w) || w > 0.5 * st->prev || it >= st->max_it;
+    st->prev = w;
+    st->done_ctas = 0;
+    st->active = stop ? 0 : 1;
+  }
+}
+
+// Passes issued per host check: the refinement normally meets the tolerance in
+// two or three, and a pass issued after convergence costs only its launches.
+constexpr int REFINE_CHUNK = 4;
+
+// The refinement in two halves so that a captured launch sequence can hold
+// it: mixed_refine_begin issues the set-up, mixed_refine_passes issues passes
+// without any host synchronisation (each pass's last residual kernel decides
+// on the device whether another is wanted, and the passes after that decision
+// do nothing), mixed_refine_read reads the decision.
+struct RefineArgs {
+  double2* D;      // FP64 matrices (the residual's operator)
+  int n, nsys, nrhs;
+  double2* X;      // right-hand sides in, solution out (FP64)
+  Ragged rg;
+};
+
+inline void mixed_refine_begin(MixedWork& w, const RefineArgs& a, int max_it, cudaStream_t st, long long& launches) {
+  const long long V = (long long)a.nsys * a.n * a.nrhs;
+  const int nv = a.nsys * a.nrhs;
+  cudaMemcpyAsync(w.b, a.X, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
   cudaMemsetAsync(w.norms, 0, 2 * (size_t)nv * sizeof(unsigned long long), st);
-  norm_kernel<<<dim3(4, nrhs, nsys), 256, 0, st>>>(w.b, n, nrhs, w.norms + nv);
+  norm_kernel<<<dim3(4, a.nrhs, a.nsys), 256, 0, st>>>(w.b, a.n, a.nrhs, w.norms + nv, a.rg.ord);
   ++launches;
   d2f_kernel<<<1184, 256, 0, st>>>(w.b, w.rf, V);
   ++launches;
-  std::vector<unsigned long long> h(2 * (size_t)nv);
-  Batch dm{D, (long long)n * n, n, nullptr};
-  w.last_iterations = 0;
+  refine_start_kernel<<<1, 1, 0, st>>>(w.state, max_it);
+  ++launches;
+}
+
+inline void mixed_refine_passes(MixedWork& w, const RefineArgs& a, int passes, cudaStream_t st, long long& launches) {
+  const long long V = (long long)a.nsys * a.n * a.nrhs, xs = (long long)a.n * a.nrhs;
+  const int nv = a.nsys * a.nrhs;
+  const Batch dm = make_batch<double2>(a.D, a.n, nullptr, nullptr, a.rg);
+  const int* active = &w.state->active;
+  for (int it = 0; it < passes; ++it) {
+    trsm_f32(w, a.n, a.nsys, a.nrhs, st, launches, active, a.rg);
+    refine_update_kernel<<<1184, 256, 0, st>>>(a.X, w.rf, w.b, w.r, V, w.norms, nv, w.state);
+    ++launches;
+    matvec_acc(dm, a.X, xs, w.r, xs, a.nrhs, a.nsys, -1.0, st, active);
+    ++launches;
+    refine_residual_kernel<<<dim3(8, a.nrhs, a.nsys), 256, 0, st>>>(w.r, w.rf, a.n, a.nrhs, w.norms, nv, w.state,
+                                                                    REFINE_TOL, a.rg.ord);
+    ++launches;
+  }
+}
+
+// waits for the stream; returns true while the device still wants passes
+inline bool mixed_refine_read(MixedWork& w, cudaStream_t st) {
+  RefineState h{};
+  cudaMemcpyAsync(&h, w.state, sizeof h, cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  w.last_iterations = h.iterations;
+  w.last_residual = h.worst;
+  return h.active != 0;
+}
+
+// X: right-hand sides in, solution out (FP64). Passes are issued
+// REFINE_CHUNK at a time, with one host check per chunk.
+inline void mixed_solve_refine(MixedWork& w, double2* D, int n, int nsys, double2* X, double2* /*Y*/, int nrhs,
+                               cudaStream_t st, long long& launches, const Ragged& rg = Ragged()) {
+  const RefineArgs a{D, n, nsys, nrhs, X, rg};
   const int max_it = refine_max_it();
-  double prev = 1e300;
-  for (int it = 0; it < max_it; ++it) {
-    trsm_f32(w, n, nsys, nrhs, st, launches, lanes);
-    accumulate_kernel<<<1184, 256, 0, st>>>(X, w.rf, V, it == 0);
-    ++launches;
-    cudaMemsetAsync(w.norms, 0, (size_t)nv * sizeof(unsigned long long), st);
-    cudaMemcpyAsync(w.r, w.b, V * sizeof(double2), cudaMemcpyDeviceToDevice, st);
-    matvec_acc(dm, X, (long long)n * nrhs, w.r, (long long)n * nrhs, nrhs, nsys, -1.0, st);
-    ++launches;
-    residual_finish_kernel<<<dim3(8, nrhs, nsys), 256, 0, st>>>(w.r, w.rf, n, nrhs, w.norms);
-    ++launches;
-    cudaMemcpyAsync(h.data(), w.norms, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    double worst = 0.;
-    for (int q = 0; q < nv; ++q) {
-      double rn, bn;
-      std::memcpy(&rn, &h[q], 8);
-      std::memcpy(&bn, &h[nv + q], 8);
-      worst = std::max(worst, bn > 0 ? rn / bn : rn);
-    }
-    w.last_iterations = it + 1;
-    w.last_residual = worst;
-    // stop at the tolerance, or as soon as the residual no longer halves
-    // (stagnation or divergence: the caller then falls back to FP64 factors)
-    if (worst <= REFINE_TOL || !(worst == worst) || worst > 0.5 * prev) break;
-    prev = worst;
+  mixed_refine_begin(w, a, max_it, st, launches);
+  for (int it0 = 0; it0 < max_it; it0 += REFINE_CHUNK) {
+    mixed_refine_passes(w, a, std::min(REFINE_CHUNK, max_it - it0), st, launches);
+    if (!mixed_refine_read(w, st)) break;
   }
 }
 

@@ -110,9 +110,10 @@ __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
 __global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, unsigned char* __restrict__ abuf,
                                                        unsigned char* __restrict__ bbuf, long long sys_bytes_a,
                                                        long long sys_bytes_b, int na) {
-  const int n = b.n, r1 = k0 + LU_OUTER, rest = n - r1;
+  const int n = b.order(blockIdx.z), r1 = k0 + LU_OUTER, rest = n - r1;
+  if (rest <= 0) return;
   const int nt = (rest + TC_T - 1) / TC_T;
-  const float2* A = b.base + blockIdx.z * b.stride;
+  const float2* A = b.sys(blockIdx.z);
   const bool isA = (int)blockIdx.x < na;
   const int q = (isA ? blockIdx.x : blockIdx.x - na) * blockDim.x + threadIdx.x;
   if (q >= nt * TC_T * TC_NCH) return;
@@ -239,8 +240,11 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * TC_STAGE);   // full[2], empty[2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
   __shared__ int s_ok;
-  const int n = b.n, r1 = k0 + LU_OUTER, rest = n - r1;
+  const int n = b.order(blockIdx.z), r1 = k0 + LU_OUTER, rest = n - r1;
   const int tcol = blockIdx.x, trow = blockIdx.y;
+  // a ragged batch's smaller systems leave the tiles beyond their order
+  // (uniform per CTA, before any barrier or tensor-memory allocation)
+  if (rest <= 0 || tcol * TC_T >= rest || trow * TC_T >= rest) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]);
 
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
     const int gr0 = r1 + trow * TC_T, nrows = min(TC_T, n - gr0);
     const int c = r1 + tcol * TC_T + (int)threadIdx.x;
     if (nrows > 0 && c < n) {
-      const char* p = reinterpret_cast<const char*>(b.base + blockIdx.z * b.stride + gr0 + (long long)n * c);
+      const char* p = reinterpret_cast<const char*>(b.sys(blockIdx.z) + gr0 + (long long)n * c);
       for (int off = 0; off < nrows * (int)sizeof(float2); off += 128)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(p + off));
     }
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
     // row `row` of the tile = TMEM lane; columns [0,128) real, [128,256) imaginary
     const int row = warp * 32 + lane;
     const int gr = r1 + trow * TC_T + row;
-    float2* A = b.base + blockIdx.z * b.stride;
+    float2* A = b.sys(blockIdx.z);
     const int cbase = r1 + tcol * TC_T;
     const int ncol = min(TC_T, rest - tcol * TC_T);
 #pragma unroll 1

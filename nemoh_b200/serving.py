@@ -49,6 +49,7 @@ class Request:
     start: float = 0.0
     done: float = 0.0
     force: Optional[np.ndarray] = None   # (nint, 7): 6 radiation DOFs, then diffraction
+    error: Optional[str] = None          # set when the request's batch failed
 
 
 class Body:
@@ -85,6 +86,18 @@ class Body:
         return cls * n * n * 16 * 2 + cls * n * n * 8 + cls * n * 7 * 16 * 6
 
 
+class ServeError(RuntimeError):
+    """Raised by SolveServer.run when batches failed: `failed` holds their
+    requests (each with its `error` text), `done` the requests that were served."""
+
+    def __init__(self, failed, done):
+        first = failed[0]
+        super().__init__("%d of %d requests failed; first (request %d): %s" %
+                         (len(failed), len(failed) + len(done), first.rid, first.error))
+        self.failed = failed
+        self.done = done
+
+
 class SolveServer:
     """Serve a stream of requests on one GPU with `workers` concurrent contexts."""
 
@@ -98,6 +111,7 @@ class SolveServer:
         self._lock = threading.Condition()
         self._pending = collections.deque()
         self._done: List[Request] = []
+        self._failed: List[Request] = []
         self._feeding = False
         make = solver_factory or (lambda: Solver(device, precision))
         self._solvers = [make() for _ in range(workers)]
@@ -157,12 +171,22 @@ class SolveServer:
             tb = time.perf_counter() - t0
             for r in batch:
                 r.start = tb
-            if self._current[w] != b:
-                s.set_case(body.case)
-                self._current[w] = b
-            omegas = np.array([r.omega for r in batch])
-            nvel = np.stack([body.rhs(r.omega, r.beta_deg) for r in batch], axis=2)
-            force = s.solve_frequencies(omegas, nvel, body.nds)
+            try:
+                if self._current[w] != b:
+                    self._current[w] = None
+                    s.set_case(body.case)
+                    self._current[w] = b
+                omegas = np.array([r.omega for r in batch])
+                nvel = np.stack([body.rhs(r.omega, r.beta_deg) for r in batch], axis=2)
+                force = s.solve_frequencies(omegas, nvel, body.nds)
+            except Exception as e:   # the batch fails as a whole; the worker serves on
+                td = time.perf_counter() - t0
+                for r in batch:
+                    r.error = "%s: %s" % (type(e).__name__, e)
+                    r.done = td
+                with self._lock:
+                    self._failed.extend(batch)
+                continue
             td = time.perf_counter() - t0
             for i, r in enumerate(batch):
                 r.force = force[:, :, i]
@@ -174,6 +198,7 @@ class SolveServer:
     def run(self, requests: List[Request], realtime=True):
         """Feed requests at their arrival times (or all at once) and wait for all results."""
         self._done = []
+        self._failed = []
         self.batches = []
         reqs = sorted(requests, key=lambda r: r.arrival)
         self._feeding = True
@@ -195,10 +220,20 @@ class SolveServer:
         for t in threads:
             t.join()
         wall = time.perf_counter() - t0
+        if self._failed:
+            raise ServeError(self._failed, self._done)
+        if len(self._done) != len(reqs):
+            raise RuntimeError("served %d of %d requests" % (len(self._done), len(reqs)))
         return self._done, wall
 
 
-def latency_stats(done: List[Request], wall: float):
+def latency_stats(done: List[Request], wall: float, expected: Optional[int] = None):
+    """p50/p99/mean latency (arrival to result) and throughput; with `expected`
+    the number of served requests must match it."""
+    if expected is not None and len(done) != expected:
+        raise RuntimeError("latency over %d requests, %d expected" % (len(done), expected))
+    if any(r.force is None for r in done):
+        raise RuntimeError("a request without a result")
     lat = np.array([r.done - r.arrival for r in done]) * 1e3
     return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "solves_per_s": len(done) / wall}

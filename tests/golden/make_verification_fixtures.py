@@ -159,4 +159,6 @@ def postprocessing(tree, here):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_verification_fixtures.py <nemoh-source-tree>")
+    main(sys.argv[1])

@@ -63,6 +63,24 @@ def decode_forces(case, F):
     return out
 
 
+def coef_err(a, b, nbeta, floor=1e-6, per_coef=False):
+    """Per-coefficient error of forces a against b, both (nint, nprob, nw):
+    |a - b| / max(|b|, floor * family max), a family being one force component
+    and one problem over all frequencies (force(i, p) over omega); the first
+    nbeta problems are diffraction, the rest radiation. A family whose largest
+    value is at most 1e-9 of the largest coefficient of its kind vanishes by the
+    body's symmetry (both sides hold round-off there) and is measured against
+    `floor` times that kind maximum. Returns the maximum (or the array)."""
+    mag = np.abs(b)
+    fam = mag.max(axis=2, keepdims=True)
+    kind = np.empty_like(fam)
+    kind[:, :nbeta] = mag[:, :nbeta].max() if nbeta else 0.0
+    kind[:, nbeta:] = mag[:, nbeta:].max() if nbeta < mag.shape[1] else 0.0
+    den = np.where(fam <= 1e-9 * kind, floor * kind, np.maximum(mag, floor * fam))
+    err = np.abs(a - b) / np.maximum(den, 1e-300)
+    return err if per_coef else float(err.max())
+
+
 def rel_err(a, b):
     """max |a-b| / max|b| per integration case (row), maximised over rows."""
     num = np.abs(a - b).reshape(a.shape[0], -1).max(axis=1)

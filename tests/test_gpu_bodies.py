@@ -1,0 +1,104 @@
+"""Cross-body (ragged) batches through the C-ABI: nemoh_b200_add_body and
+nemoh_b200_solve_bodies against the single-body path.
+
+Items of bodies with different panel counts (deep and finite depth, with and
+without y-symmetry) and frequencies, in a shuffled order with repeated bodies,
+are solved in one call; every item's forces must equal those of
+nemoh_b200_solve_frequencies on that body alone (itself checked against the
+oracle in test_gpu_parity.py) within 1e-12 of the item's largest force in
+FP64 (the mat-vec sums by atomics, so the last bits may differ), and in mixed
+precision within 1e-10 of the single-body mixed result and 1e-6 (per
+coefficient) of FP64. A device-memory budget small enough to split the call
+into several batches gives the same results.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import gpu_cases as G
+import nemoh_b200 as nb
+from nemoh_b200 import build as B
+from nemoh_b200 import cases as C
+
+pytestmark = pytest.mark.gpu
+
+
+def _bodies():
+    out = [c for c in G.small_cases()]
+    rng = np.random.default_rng(21)
+    for _ in range(3):
+        mesh, depth = C.random_body(rng, 150, 700)
+        out.append(C.Case(mesh, np.array([0.7]), np.array([0.0]), C.six_dofs(), C.six_dofs(), depth=depth))
+    return out
+
+
+def _items(cases, seed=3, n=14):
+    rng = np.random.default_rng(seed)
+    body = rng.integers(0, len(cases), n)
+    body[:len(cases)] = np.arange(len(cases))          # every body at least once
+    rng.shuffle(body)
+    omega = rng.uniform(0.3, 2.2, n)
+    return body, omega
+
+
+def _rhs(case, omega, beta=30.0):
+    c = C.Case(case.mesh, np.array([omega]), np.array([beta]), case.rad, case.force, rho=case.rho, g=case.g,
+               depth=case.depth)
+    return C.body_conditions(c)   # (2^s N, 1 + ndof)
+
+
+def _single(case, mode, omegas, nvels):
+    with nb.Solver(0, mode) as s:
+        s.set_case(case)
+        nds = C.generalised_normals(case)
+        return [s.solve_frequencies(np.array([w]), v[:, :, None], nds)[:, :, 0] for w, v in zip(omegas, nvels)]
+
+
+@pytest.mark.parametrize("budget", [None, 48 << 20], ids=["one_batch", "split_batches"])
+def test_bodies_match_single_body_path(budget):
+    B.build()
+    cases = _bodies()
+    body, omega = _items(cases)
+    nvels = [_rhs(cases[b], w) for b, w in zip(body, omega)]
+    old = os.environ.get("NEMOH_B200_BATCH_BYTES")
+    if budget:
+        os.environ["NEMOH_B200_BATCH_BYTES"] = str(budget)
+    try:
+        got = {}
+        for mode in (nb.FP64, nb.MIXED):
+            with nb.Solver(0, mode) as s:
+                ids = [s.add_body(c) for c in cases]
+                assert ids == list(range(len(cases)))
+                got[mode] = s.solve_bodies(body, omega, nvels)
+    finally:
+        if budget:
+            if old is None:
+                del os.environ["NEMOH_B200_BATCH_BYTES"]
+            else:
+                os.environ["NEMOH_B200_BATCH_BYTES"] = old
+    for b in range(len(cases)):
+        sel = [i for i in range(len(body)) if body[i] == b]
+        ref64 = _single(cases[b], nb.FP64, omega[sel], [nvels[i] for i in sel])
+        refmx = _single(cases[b], nb.MIXED, omega[sel], [nvels[i] for i in sel])
+        for q, i in enumerate(sel):
+            scale = np.abs(ref64[q]).max()
+            assert np.abs(got[nb.FP64][i] - ref64[q]).max() <= 1e-12 * scale, (cases[b].name, i)
+            assert np.abs(got[nb.MIXED][i] - refmx[q]).max() <= 1e-10 * scale, (cases[b].name, i)
+        F = np.stack([got[nb.MIXED][i] for i in sel], axis=2)
+        F64 = np.stack(ref64, axis=2)
+        assert G.coef_err(F, F64, 1) < 1e-6
+
+
+def test_bodies_refuse_unknown_body_and_keep_working():
+    B.build()
+    cases = _bodies()[:2]
+    with nb.Solver(0, nb.FP64) as s:
+        for c in cases:
+            s.add_body(c)
+        nv = _rhs(cases[0], 0.9)
+        with pytest.raises(nb.NemohError):
+            s.solve_bodies(np.array([0, 5]), np.array([0.9, 0.9]), [nv, nv])
+        out = s.solve_bodies(np.array([0]), np.array([0.9]), [nv])
+        ref = _single(cases[0], nb.FP64, [0.9], [nv])[0]
+        assert np.abs(out[0] - ref).max() <= 1e-12 * np.abs(ref).max()

@@ -204,6 +204,15 @@ def test_batched_sizes_refused(solver):
     dforce = torch.zeros(2 * 3 * 17, dtype=torch.float64, device="cuda:0")
     assert lib.nemoh_b200_solve_frequencies_device(h, 1, d(om), 0, dev.data_ptr(), 3, dnds.data_ptr(),
                                                    dforce.data_ptr(), None) == 1
+    # host buffers handed in as device memory: refused before any launch
+    launches = solver.launches
+    assert lib.nemoh_b200_solve_frequencies_device(h, 1, d(om), 7, nvel.ctypes.data, 3, dnds.data_ptr(),
+                                                   dforce.data_ptr(), None) == 1
+    assert "nvel_device: host memory" in lib.nemoh_b200_last_error(h).decode()
+    assert lib.nemoh_b200_solve_frequencies_device(h, 1, d(om), 7, dev.data_ptr(), 3, dnds.data_ptr(),
+                                                   force.ctypes.data, None) == 1
+    assert "force_device" in lib.nemoh_b200_last_error(h).decode()
+    assert solver.launches == launches
     torch.cuda.synchronize()
     after = solver.solve_frequencies(om, nvel, nds)
     np.testing.assert_allclose(after, before, rtol=0, atol=1e-12 * np.abs(before).max())

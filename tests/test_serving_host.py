@@ -65,3 +65,38 @@ def test_admission_limits_batch_by_memory():
     reqs = [S.Request(i, 0, 0.5 + 0.01 * i, 0.0) for i in range(20)]
     done, _ = srv.run(reqs, realtime=False)
     assert len(done) == 20 and max(FakeSolver.calls) <= 3
+
+
+class FailingSolver(FakeSolver):
+    """Raises on every batch that contains the frequency 0.777 (a status-code error)."""
+
+    def solve_frequencies(self, omegas, nvel, nds):
+        if np.any(np.isclose(omegas, 0.777)):
+            raise RuntimeError("nemoh_b200 status 5: EAKZ")
+        return super().solve_frequencies(omegas, nvel, nds)
+
+
+def test_failed_batch_is_reported_not_dropped():
+    bodies = _bodies()
+    srv = S.SolveServer(bodies, workers=2, solver_factory=FailingSolver, memory_bytes=1 << 30)
+    reqs = S.make_requests(30, rate=0, n_bodies=2, seed=3)
+    reqs[11].omega = 0.777
+    try:
+        srv.run(reqs, realtime=False)
+    except S.ServeError as e:
+        failed = {r.rid for r in e.failed}
+        assert 11 in failed and all(r.error and "EAKZ" in r.error for r in e.failed)
+        assert len(e.failed) + len(e.done) == 30          # every request accounted for
+        assert not failed & {r.rid for r in e.done}
+    else:
+        raise AssertionError("a failed batch went unreported")
+    # the server still serves afterwards, and the statistics check the count
+    done, wall = srv.run(reqs[:5] + reqs[12:20], realtime=False)
+    st = S.latency_stats(done, wall, expected=13)
+    assert st["requests"] == 13
+    try:
+        S.latency_stats(done[:-1], wall, expected=13)
+    except RuntimeError:
+        pass
+    else:
+        raise AssertionError("a short result list went unnoticed")

@@ -112,3 +112,17 @@ def test_noalloc_rejects_sizes_beyond_scratch():
     st = f(0, 4096, 2, 256, 16, 512, None, msg, 512)
     assert st == ECAPACITY
     assert b"exceeds the fixed" in msg.value
+
+
+def test_noalloc_refuses_host_buffers():
+    """Host memory handed in as device memory is a status code, not a fault:
+    the pointers are checked before any kernel is launched."""
+    B.build()
+    f = _entry()
+    msg = ctypes.create_string_buffer(512)
+    a = np.zeros(2 * 8 * 8, dtype=np.float64)
+    x = np.zeros(2 * 8, dtype=np.float64)
+    st = f(0, 8, 1, a.ctypes.data, 1, x.ctypes.data, None, msg, 512)
+    assert st == 1, (st, msg.value)   # NEMOH_B200_EINVAL
+    assert b"host memory" in msg.value
+    assert not a.any() and not x.any()
