@@ -276,46 +276,52 @@ def _body_inputs(case):
     return nvel, np.asfortranarray(C.generalised_normals(case))
 
 
-def run_batched(local, n_bodies, n_omega=20, seed=4):
+def run_batched(local, n_bodies, n_omega=20, seed=4, steps=2):
     """Batched workload: n_bodies bodies from the seeded generator (cylinder, box
     or sphere, 200..3000 panels, infinite or 20..200 m depth), 20 frequencies
-    0.1..2.5 rad/s, 6 DOF + heading 0 each; every body's frequencies are one
-    batched call through the host C-ABI (copies included), bodies in order of
-    decreasing panel count so that the workspace is allocated once."""
+    0.1..2.5 rad/s, 6 DOF + heading 0 each. The bodies are resident on the
+    device (nemoh_b200_add_body, not timed); one step is one
+    nemoh_b200_solve_bodies call over all n_bodies x 20 (body, omega) items
+    with host buffers (copies included): items of different bodies share
+    ragged batches sized by free device memory. One untimed warm-up step, then
+    `steps` timed steps (host wall clock)."""
     import nemoh_b200 as nb
     from nemoh_b200 import cases as C
     rng = np.random.default_rng(seed)
     omegas = np.linspace(0.1, 2.5, n_omega)
-    bodies = []
+    cases, nvels = [], []
     for _ in range(n_bodies):
         mesh, depth = C.random_body(rng)
         case = C.Case(mesh, omegas, np.array([0.0]), C.six_dofs(), C.six_dofs(), depth=depth)
-        bodies.append((case,) + _body_inputs(case))
-    bodies.sort(key=lambda b: -b[0].mesh.npanels)
+        nvel, _ = _body_inputs(case)
+        cases.append(case)
+        nvels.append(nvel)
+    items_b = np.repeat(np.arange(n_bodies), n_omega)
+    items_w = np.tile(omegas, n_bodies)
+    items_v = [nvels[b][:, :, w] for b in range(n_bodies) for w in range(n_omega)]
     out, F = {}, {}
     for label, mode in (("fp64", nb.FP64), ("mixed", nb.MIXED)):
         with nb.Solver(local, mode) as s:
-            s.set_case(bodies[0][0])
-            s.solve_frequencies(omegas[:1], bodies[0][1][:, :, :1], bodies[0][2])   # workspace + warm-up
+            for case in cases:
+                s.add_body(case)
+            res = s.solve_bodies(items_b, items_w, items_v)   # warm-up: workspace, kernel attributes
             t0 = time.perf_counter()
-            res, fallbacks = [], 0
-            for case, nvel, nds in bodies:
-                s.set_case(case)
-                res.append(s.solve_frequencies(omegas, nvel, nds))
-                fallbacks += mode == nb.MIXED and s.last_refinement()[0] < 0
-            dt = time.perf_counter() - t0
-        F[label] = res
+            for _ in range(steps):
+                res = s.solve_bodies(items_b, items_w, items_v)
+            dt = (time.perf_counter() - t0) / steps
+            t = s.last_timings()
+        F[label] = [np.stack(res[b * n_omega:(b + 1) * n_omega], axis=2) for b in range(n_bodies)]
         out[label + "_solves_per_s"] = n_bodies * n_omega / dt
         out[label + "_s"] = dt
-        if mode == nb.MIXED:
-            out["mixed_fp64_fallback_bodies"] = int(fallbacks)
+        out[label + "_phase_ms"] = {"assemble": t["assemble_ms"], "factor": t["factor_ms"], "solve": t["solve_ms"]}
     errs = [rel_err_families(a, b, 1)[0] for a, b in zip(F["mixed"], F["fp64"])]
-    npan = [b[0].mesh.npanels for b in bodies]
-    out.update({"bodies": n_bodies, "omegas_per_body": n_omega, "solves": n_bodies * n_omega,
+    npan = [c.mesh.npanels for c in cases]
+    out.update({"bodies": n_bodies, "omegas_per_body": n_omega, "solves": n_bodies * n_omega, "steps": steps,
                 "panels_min": int(min(npan)), "panels_max": int(max(npan)), "panels_median": float(np.median(npan)),
-                "finite_depth_bodies": int(sum(b[0].depth > 0 for b in bodies)),
+                "finite_depth_bodies": int(sum(c.depth > 0 for c in cases)),
                 "mixed_speedup": out["fp64_s"] / out["mixed_s"], "mixed_vs_fp64_max_rel_err": float(max(errs)),
-                "timing": "host wall clock around the whole batch, host<->device copies included"})
+                "path": "nemoh_b200_solve_bodies: all bodies and frequencies in one call, ragged batches",
+                "timing": "host wall clock per call, host<->device copies included"})
     return out
 
 
@@ -388,19 +394,20 @@ def run_outputs(local, omega_index=10):
     return out
 
 
-def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9), seed=5, n_check=64, workers=4):
+def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9, 1.0, 1.2), seed=5, n_check=64, workers=2):
     """Serving workload: Poisson request streams over the batched workload's
     bodies (one omega U(0.1, 2.5), heading U(0, 180) deg, 6 DOF per request)
-    through the continuous-batching server. The saturation throughput is the
-    rate achieved on a stream offered well above capacity; streams at fractions
-    of it then give the latency percentiles."""
+    through the continuous-batching server (resident bodies, right-hand sides
+    built on the device, cross-body batches). The saturation throughput is the
+    rate achieved on a stream offered well above capacity; streams at
+    fractions of it then give the latency percentiles."""
     import nemoh_b200 as nb
     from nemoh_b200 import serving as S
     bodies = S.make_bodies(n_bodies, seed=4)
-    srv = S.SolveServer(bodies, device=local, precision=nb.MIXED, workers=workers, reserve=4)
+    srv = S.SolveServer(bodies, device=local, precision=nb.MIXED, workers=workers)
     try:
-        srv.run(S.make_requests(min(64, n_req), 0, n_bodies, seed=seed + 100), realtime=False)   # warm-up
-        done, wall = srv.run(S.make_requests(n_req, 5000.0, n_bodies, seed=seed))
+        srv.run(S.make_requests(min(256, n_req), 0, n_bodies, seed=seed + 100), realtime=False)   # warm-up
+        done, wall = srv.run(S.make_requests(min(n_req, 4000), 1e6, n_bodies, seed=seed))
         sat = len(done) / wall
         out = {"bodies": n_bodies, "requests_per_rate": n_req, "workers": workers, "precision": "mixed",
                "saturation_solves_per_s": sat, "rates": []}
@@ -408,28 +415,33 @@ def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9), seed=5, n_
         for f in rates:
             done, wall = srv.run(S.make_requests(n_req, f * sat, n_bodies, seed=seed + int(100 * f)))
             st = S.latency_stats(done, wall, expected=n_req)
-            st.update({"rate_frac": f, "offered_per_s": f * sat})
+            st.update({"rate_frac": f, "offered_per_s": f * sat,
+                       "mean_batch": float(np.mean([b[2] for b in srv.batches])),
+                       "mean_bodies_per_batch": float(np.mean([b[1] for b in srv.batches]))})
             out["rates"].append(st)
             last = done
     finally:
         srv.close()
     # per-request error against the FP64 path on a sample of the last stream
     worst = 0.0
+    check = sorted(last, key=lambda r: r.rid)[:n_check]
     with nb.Solver(local, nb.FP64) as s:
-        for r in sorted(last, key=lambda r: r.rid)[:n_check]:
-            b = bodies[r.body]
-            s.set_case(b.case)
-            f64 = s.solve_frequencies(np.array([r.omega]), b.rhs(r.omega, r.beta_deg)[:, :, None], b.nds)[:, :, 0]
-            a = np.abs(f64)
-            # one frequency per request: each coefficient against itself, or
-            # against 1e-6 of its kind's largest value where it vanishes by symmetry
-            floor = np.empty_like(a)
-            for cols in (slice(0, 6), slice(6, 7)):
-                k = a[:, cols].max()
-                floor[:, cols] = np.where(a[:, cols] <= 1e-9 * k, 1e-6 * k, a[:, cols])
-            worst = max(worst, float((np.abs(r.force - f64) / floor).max()))
+        for b in bodies:
+            bid = s.add_body(b.case)
+            s.set_body_dofs(bid, b.case.rad)
+        f64s = s.solve_requests(np.array([r.body for r in check]), np.array([r.omega for r in check]),
+                                np.radians([r.beta_deg for r in check]))
+    for r, f64 in zip(check, f64s):
+        a = np.abs(f64)
+        # one frequency per request: each coefficient against itself, or
+        # against 1e-6 of its kind's largest value where it vanishes by symmetry
+        floor = np.empty_like(a)
+        for cols in (slice(0, 1), slice(1, 7)):
+            k = a[:, cols].max()
+            floor[:, cols] = np.where(a[:, cols] <= 1e-9 * k, 1e-6 * k, a[:, cols])
+        worst = max(worst, float((np.abs(r.force - f64) / floor).max()))
     out["mixed_vs_fp64_max_rel_err"] = worst
-    out["checked_requests"] = min(n_check, len(last))
+    out["checked_requests"] = len(check)
     out["latency"] = "host clock from arrival to result ready"
     return out
 
@@ -602,7 +614,7 @@ def main():
     ap.add_argument("--omegas", type=int, default=N_OMEGA, help="frequency subset (profiling only)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving workloads")
     ap.add_argument("--bodies", type=int, default=256, help="bodies of the batched and serving workloads")
-    ap.add_argument("--requests", type=int, default=1000, help="requests per serving rate")
+    ap.add_argument("--requests", type=int, default=10000, help="requests per serving rate")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -165,6 +165,19 @@ int nemoh_b200_add_body(nemoh_ctx* ctx, int np, int nfa, int nsymy, const double
 int nemoh_b200_body_count(const nemoh_ctx* ctx);
 int nemoh_b200_solve_bodies(nemoh_ctx* ctx, int nitem, const int* body, const double* omegas, int nrhs,
                             const double* nvel, double* force);
+/* Serving requests on resident bodies. nemoh_b200_set_body_dofs gives a body
+ * its ndof radiation DOFs (kind, dir, axis as in nemoh_b200_body_conditions;
+ * 1 + ndof <= 16). nemoh_b200_solve_requests solves nreq (body[i], omegas[i],
+ * betas[i] in radians) requests with right-hand sides built on the device by
+ * the pre-processor's formulas (preProcessor/BodyConditions.f90:27-137,
+ * Environment.f90:86-100; wave measurement point at the origin): per request
+ * the diffraction problem at its heading, then the radiation DOFs; force
+ * receives, request after request, nint_i x (1 + ndof) complex forces. The
+ * bodies of one call must have the same ndof. */
+int nemoh_b200_set_body_dofs(nemoh_ctx* ctx, int body, int ndof, const int* dof_kind, const double* dof_dir,
+                             const double* dof_axis);
+int nemoh_b200_solve_requests(nemoh_ctx* ctx, int nreq, const int* body, const double* omegas, const double* betas,
+                              double* force);
 /* Same with nvel and force in device memory of the context's device, ordered
  * on `stream` (cudaStream_t) like nemoh_b200_solve_frequencies_device. */
 int nemoh_b200_solve_bodies_device(nemoh_ctx* ctx, int nitem, const int* body, const double* omegas, int nrhs,

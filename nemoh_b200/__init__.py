@@ -89,6 +89,8 @@ def load_library():
     L.nemoh_b200_body_count.argtypes = [_vp]
     L.nemoh_b200_solve_bodies.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _d, _d]
     L.nemoh_b200_solve_bodies_device.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _vp, _vp, _vp]
+    L.nemoh_b200_set_body_dofs.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _i, _d, _d]
+    L.nemoh_b200_solve_requests.argtypes = [_vp, ctypes.c_int, _i, _d, _d, _d]
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
     L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
     L.nemoh_b200_diag_theta_quadrature.argtypes = [ctypes.c_double, _d, _d]
@@ -244,6 +246,33 @@ class Solver:
         force = np.zeros(sum(sizes), dtype=np.complex128)
         self._check(load_library().nemoh_b200_solve_bodies(self._h, len(bodies), bodies.ctypes.data_as(_i),
                                                            _p(omegas), nrhs, _p(flat), _p(force)))
+        out, o = [], 0
+        for b, sz in zip(bodies, sizes):
+            out.append(force[o:o + sz].reshape((self._bodies[b][1], nrhs), order="F"))
+            o += sz
+        return out
+
+    def set_body_dofs(self, body, dofs):
+        """Radiation DOFs (cases.Dof list) of a resident body's serving requests."""
+        kind = np.array([d.icase for d in dofs], dtype=np.int32)
+        direc = np.ascontiguousarray([d.direction for d in dofs], dtype=np.float64).reshape(-1)
+        axis = np.ascontiguousarray([d.axis for d in dofs], dtype=np.float64).reshape(-1)
+        self._check(load_library().nemoh_b200_set_body_dofs(self._h, int(body), len(dofs), kind.ctypes.data_as(_i),
+                                                            _p(direc), _p(axis)))
+        self._bodies[body] = self._bodies[body][:2] + (len(dofs),)
+
+    def solve_requests(self, bodies, omegas, betas_rad):
+        """Serving requests (body, omega, heading): right-hand sides built on
+        the device; returns per request the forces (nint, 1 + ndof): the
+        diffraction problem, then the radiation DOFs."""
+        bodies = np.ascontiguousarray(bodies, dtype=np.int32)
+        omegas = np.ascontiguousarray(omegas, dtype=np.float64)
+        betas = np.ascontiguousarray(betas_rad, dtype=np.float64)
+        nrhs = 1 + self._bodies[bodies[0]][2]
+        sizes = [self._bodies[b][1] * nrhs for b in bodies]
+        force = np.zeros(sum(sizes), dtype=np.complex128)
+        self._check(load_library().nemoh_b200_solve_requests(self._h, len(bodies), bodies.ctypes.data_as(_i),
+                                                             _p(omegas), _p(betas), _p(force)))
         out, o = [], 0
         for b, sz in zip(bodies, sizes):
             out.append(force[o:o + sz].reshape((self._bodies[b][1], nrhs), order="F"))

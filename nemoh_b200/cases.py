@@ -34,7 +34,7 @@ import numpy as np
 
 __all__ = [
     "Mesh", "Dof", "Case", "six_dofs",
-    "cylinder_mesh", "box_mesh", "hemisphere_mesh", "merge_meshes",
+    "cylinder_mesh", "box_mesh", "hemisphere_mesh", "icosphere_hull", "merge_meshes",
     "panel_quantities", "wavenumber", "body_conditions", "generalised_normals",
     "froude_krylov", "write_case", "read_case", "CaseArrays",
     "config_cylinder", "config_barge", "config_two_spheres",
@@ -275,6 +275,123 @@ def hemisphere_mesh(radius=4.0, n_lat=40, n_lon=100, center=(0.0, 0.0),
     panels = np.array(quads, dtype=np.int32)
     cen = np.tile([cx, cy, zc], (len(panels), 1))
     return Mesh(nodes, _orient(nodes, panels, cen), isym=1 if half else 0)
+
+
+_ICO_FACES = ((0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+              (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+              (6, 2, 10), (8, 6, 7), (9, 8, 1))
+
+
+def _icosahedron():
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    return v / np.linalg.norm(v, axis=1)[:, None]
+
+
+def icosphere_hull(radius=4.0, freq=12, cut=-0.055, center=(0.0, 0.0), n_target=None, jitter=0.0, rng=None) -> Mesh:
+    """Submerged part of a floating sphere from a geodesic icosphere, in quads.
+
+    The icosahedron's faces are subdivided into freq^2 triangles each and
+    projected on the unit sphere; the triangles whose centroid lies below
+    z = cut (in sphere radii) are kept and their vertices above the plane are
+    levelled onto it (moved down the sphere to the waterline circle). Each
+    triangle is split into three quads (vertex, two edge midpoints and the
+    centroid, projected on the sphere; waterline midpoints stay on the
+    waterline). With `n_target`, the largest quads are halved (across their
+    longer pair of opposite edges) until that count is reached. The sphere is
+    then scaled to `radius` and placed so that the waterline is z = 0 at
+    `center`. `jitter` moves every node off the waterline tangentially by up
+    to that fraction of the local edge length (seeded by `rng`), which changes
+    panel areas by up to about the same fraction.
+    """
+    V = _icosahedron()
+    ns = _NodeSet()
+    zc = math.sqrt(max(0.0, 1.0 - cut * cut))
+
+    def level(p):
+        p = p / np.linalg.norm(p)
+        if p[2] > cut:   # onto the waterline circle, same azimuth
+            r = math.hypot(p[0], p[1])
+            p = np.array([p[0] * zc / r, p[1] * zc / r, cut])
+        return p
+
+    tris = []
+    for a, b, c in _ICO_FACES:
+        A, B, Cc = V[a], V[b], V[c]
+        P = {}
+        for i in range(freq + 1):
+            for j in range(freq + 1 - i):
+                p = A + (B - A) * i / freq + (Cc - A) * j / freq
+                P[(i, j)] = p / np.linalg.norm(p)
+        for i in range(freq):
+            for j in range(freq - i):
+                tris.append((P[(i, j)], P[(i + 1, j)], P[(i, j + 1)]))
+                if i + j + 1 < freq:
+                    tris.append((P[(i + 1, j)], P[(i + 1, j + 1)], P[(i, j + 1)]))
+    kept = [tuple(level(v) for v in t) for t in tris if (t[0][2] + t[1][2] + t[2][2]) / 3.0 < cut]
+
+    def mid(p, q):
+        m = 0.5 * (p + q)
+        if abs(p[2] - cut) < 1e-12 and abs(q[2] - cut) < 1e-12:   # a waterline edge
+            r = math.hypot(m[0], m[1])
+            return np.array([m[0] * zc / r, m[1] * zc / r, cut])
+        return m / np.linalg.norm(m)
+
+    quads = []
+    for v0, v1, v2 in kept:
+        c = (v0 + v1 + v2) / np.linalg.norm(v0 + v1 + v2)
+        m01, m12, m20 = mid(v0, v1), mid(v1, v2), mid(v2, v0)
+        quads += [[v0, m01, c, m20], [v1, m12, c, m01], [v2, m20, c, m12]]
+
+    def quad_area(q):
+        return 0.5 * np.linalg.norm(np.cross(q[2] - q[0], q[3] - q[1]))
+
+    if n_target is not None:
+        if n_target < len(quads):
+            raise ValueError("icosphere_hull: %d quads exceed the target %d" % (len(quads), n_target))
+        while len(quads) < n_target:
+            k = max(range(len(quads)), key=lambda i: quad_area(quads[i]))
+            p0, p1, p2, p3 = quads.pop(k)
+            if np.linalg.norm(p1 - p0) + np.linalg.norm(p3 - p2) >= np.linalg.norm(p2 - p1) + np.linalg.norm(p0 - p3):
+                a, b = mid(p0, p1), mid(p2, p3)       # halve edges p0p1 and p2p3
+                quads += [[p0, a, b, p3], [a, p1, p2, b]]
+            else:
+                a, b = mid(p1, p2), mid(p3, p0)       # halve edges p1p2 and p3p0
+                quads += [[p0, p1, a, b], [b, a, p2, p3]]
+    ids = [[ns.add(tuple(v)) for v in q] for q in quads]
+    nodes = np.array(ns.xyz)
+    if jitter and rng is not None:
+        panels0 = np.array(ids) - 1
+        edge = np.zeros(len(nodes))
+        cnt = np.zeros(len(nodes))
+        for q in panels0:
+            for k in range(4):
+                a, b = q[k], q[(k + 1) % 4]
+                d = np.linalg.norm(nodes[a] - nodes[b])
+                edge[a] += d
+                edge[b] += d
+                cnt[a] += 1
+                cnt[b] += 1
+        h = edge / np.maximum(cnt, 1)
+        for i in range(len(nodes)):
+            p = nodes[i]
+            if abs(p[2] - cut) < 1e-12:
+                continue   # the waterline stays in the plane
+            t1 = np.cross(p, [0.0, 0.0, 1.0] if abs(p[2]) < 0.9 else [1.0, 0.0, 0.0])
+            t1 /= np.linalg.norm(t1)
+            t2 = np.cross(p, t1)
+            d = jitter * h[i] * rng.uniform(-1, 1, 2)
+            q = p + d[0] * t1 + d[1] * t2
+            q /= np.linalg.norm(q)
+            nodes[i] = q if q[2] < cut else p
+    nodes = nodes * radius
+    nodes[:, 2] -= cut * radius
+    nodes[:, 0] += center[0]
+    nodes[:, 1] += center[1]
+    panels = np.array(ids, dtype=np.int32)
+    cen = np.tile([center[0], center[1], -cut * radius], (len(panels), 1))
+    return Mesh(nodes, _orient(nodes, panels, cen), isym=0)
 
 
 def merge_meshes(meshes: Sequence[Mesh]) -> Mesh:
@@ -706,11 +823,20 @@ def config_barge(n_omega=40, nx=50, ny=20, nz=20, nye=10) -> Case:
                 six_dofs(), six_dofs(), rho=1025.0, g=9.81, depth=50.0, name="barge2400")
 
 
-def config_two_spheres(n_omega=30, n_lat=40, n_lon=100, seed=3) -> Case:
-    """Two floating spheres R=4 m, centres (+-10, 0, 0), 8,000 panels total."""
+ICO_JITTER = 0.03   # tangential node jitter: panel areas within +-10% of the unjittered mesh
+
+
+def config_two_spheres(n_omega=30, seed=3) -> Case:
+    """Two floating spheres R=4 m, centres (+-10, 0, 0), 8,000 panels total.
+
+    Each hull is a geodesic icosphere (frequency 12) cut at 0.055 radii below
+    the centre (draft 3.78 m) and levelled onto the waterline, quadrangulated
+    (three quads per triangle, 3,996 quads, the four largest halved: 4,000),
+    with node jitter from `seed` that changes panel areas by up to 10%.
+    """
     rng = np.random.default_rng(seed)
-    a = hemisphere_mesh(4.0, n_lat, n_lon, center=(-10.0, 0.0), jitter=0.2, rng=rng)
-    b = hemisphere_mesh(4.0, n_lat, n_lon, center=(10.0, 0.0), jitter=0.2, rng=rng)
+    a = icosphere_hull(4.0, 12, -0.055, (-10.0, 0.0), n_target=4000, jitter=ICO_JITTER, rng=rng)
+    b = icosphere_hull(4.0, 12, -0.055, (10.0, 0.0), n_target=4000, jitter=ICO_JITTER, rng=rng)
     mesh = merge_meshes([a, b])
     dofs = six_dofs((-10.0, 0.0, 0.0), 1) + six_dofs((10.0, 0.0, 0.0), 2)
     return Case(mesh, np.linspace(0.2, 3.0, n_omega), np.array([0.0, 90.0]),

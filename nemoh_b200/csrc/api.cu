@@ -96,7 +96,8 @@ struct BodyState {
   int np = 0, nfa = 0, nsymy = 0, nint = 0;
   double rho = 0, g = 0, depth = 0, zer = 0, gm = 0;
   int nq_state = 0;
-  DevBuf d_xyz, d_m, d_rec, d_rows, d_nds;
+  int ndof = 0;   // radiation DOFs of serving requests (nemoh_b200_set_body_dofs)
+  DevBuf d_xyz, d_m, d_rec, d_rows, d_nds, d_dofs;
 };
 
 }  // namespace
@@ -129,8 +130,8 @@ struct nemoh_ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   // resident bodies and the descriptions of the current ragged batch
   std::vector<std::unique_ptr<BodyState>> bodies;
-  DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce;
-  HostBuf h_rag;
+  DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce, d_reqs;
+  HostBuf h_rag, h_reqs;
 };
 
 #define CK(call)                                                                                 \
@@ -914,6 +915,66 @@ int nemoh_b200_solve_bodies(nemoh_ctx* c, int nitem, const int* body, const doub
     CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2)));
     CK(cudaMemcpyAsync(c->d_bnvel.p, nvel, nv * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     solve_bodies_impl(c, nitem, body, omegas, nrhs, c->d_bnvel.as<double2>(), c->d_bforce.as<double2>());
+    if (nf) CK(cudaMemcpyAsync(force, c->d_bforce.p, nf * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int nemoh_b200_set_body_dofs(nemoh_ctx* c, int body, int ndof, const int* dof_kind, const double* dof_dir,
+                             const double* dof_axis) {
+  if (!c || body < 0 || body >= (int)c->bodies.size() || ndof < 0 || ndof + 1 > MAX_RHS ||
+      (ndof > 0 && (!dof_kind || !dof_dir || !dof_axis)))
+    return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    std::vector<PreDof> v(ndof);
+    for (int q = 0; q < ndof; ++q) {
+      if (dof_kind[q] != 1 && dof_kind[q] != 2) throw Fail{NEMOH_B200_EINVAL, "DOF kind must be 1 or 2"};
+      v[q].kind = dof_kind[q];
+      v[q].body = 1;
+      for (int d = 0; d < 3; ++d) {
+        v[q].dir[d] = dof_dir[3 * q + d];
+        v[q].axis[d] = dof_axis[3 * q + d];
+      }
+    }
+    BodyState& b = *c->bodies[body];
+    CK(b.d_dofs.ensure(std::max<size_t>(1, v.size()) * sizeof(PreDof)));
+    if (ndof) CK(cudaMemcpyAsync(b.d_dofs.p, v.data(), v.size() * sizeof(PreDof), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    b.ndof = ndof;
+  });
+}
+
+int nemoh_b200_solve_requests(nemoh_ctx* c, int nreq, const int* body, const double* omegas, const double* betas,
+                              double* force) {
+  if (!bodies_args_ok(c, nreq, body, omegas) || !betas || !force) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    const int ndof = c->bodies[body[0]]->ndof, nrhs = 1 + ndof;
+    for (int i = 0; i < nreq; ++i)
+      if (c->bodies[body[i]]->ndof != ndof)
+        throw Fail{NEMOH_B200_EINVAL, "the bodies of one call must have the same number of DOFs"};
+    size_t nv = 0, nf = 0;
+    bodies_sizes(c, nreq, body, nrhs, &nv, &nf);
+    CK(c->d_bnvel.ensure(nv * sizeof(double2)));
+    CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2)));
+    CK(c->h_reqs.ensure((size_t)nreq * sizeof(ReqDesc)));
+    CK(c->d_reqs.ensure((size_t)nreq * sizeof(ReqDesc)));
+    ReqDesc* rq = c->h_reqs.as<ReqDesc>();
+    long long off = 0;
+    int nmax = 0;
+    for (int i = 0; i < nreq; ++i) {
+      const BodyState& b = *c->bodies[body[i]];
+      const double k = preproc_wavenumber(omegas[i], b.g, b.depth);
+      rq[i] = ReqDesc{b.d_xyz.as<double>(), b.d_m.as<int>(), b.d_dofs.as<PreDof>(),
+                      PreWave{omegas[i], k, std::cos(betas[i]), std::sin(betas[i])}, b.g, b.depth, off, b.nfa,
+                      b.nsymy, ndof};
+      off += (long long)(b.nsymy + 1) * b.nfa * nrhs;
+      nmax = std::max(nmax, b.nfa);
+    }
+    CK(cudaMemcpyAsync(c->d_reqs.p, rq, (size_t)nreq * sizeof(ReqDesc), cudaMemcpyHostToDevice, c->stream));
+    request_rhs_kernel<<<dim3((nmax + 127) / 128, 2, nreq), 128, 0, c->stream>>>(c->d_reqs.as<ReqDesc>(),
+                                                                                c->d_bnvel.as<double2>());
+    LAUNCHED(c);
+    solve_bodies_impl(c, nreq, body, omegas, nrhs, c->d_bnvel.as<double2>(), c->d_bforce.as<double2>());
     if (nf) CK(cudaMemcpyAsync(force, c->d_bforce.p, nf * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });

@@ -67,6 +67,30 @@ NB_HD __forceinline__ double pre_dof(const PreDof& d, const double* x, const dou
   return n[0] * v0 + n[1] * v1 + n[2] * v2;
 }
 
+// diffraction condition -v_I . n of the incident wave pw at (xm, n), with the
+// depth factors CIH/SIH that the Froude-Krylov pressure also needs
+NB_HD __forceinline__ void pre_diffraction(const PreWave& pw, double g, double depth, double xeff, double yeff,
+                                           const double* xm, const double* n, double& vr, double& vi, double& cih,
+                                           double& ce, double& se) {
+  const double k = pw.k, kh = k * depth;
+  double sih;
+  if (kh <= 20. && kh > 0.) {
+    cih = cosh(k * (xm[2] + depth)) / cosh(kh);
+    sih = sinh(k * (xm[2] + depth)) / cosh(kh);
+  } else {
+    cih = sih = exp(k * xm[2]);
+  }
+  const double wbar = (xm[0] - xeff) * pw.cb + (xm[1] - yeff) * pw.sb;
+  sincos(k * wbar, &se, &ce);
+  const double gwk = g / pw.w * k;
+  // v = (gwk cb cih e, gwk sb cih e, -i gwk sih e), e = exp(i k wbar)
+  const double vxr = gwk * pw.cb * cih * ce, vxi = gwk * pw.cb * cih * se;
+  const double vyr = gwk * pw.sb * cih * ce, vyi = gwk * pw.sb * cih * se;
+  const double vzr = gwk * sih * se, vzi = -gwk * sih * ce;
+  vr = -(vxr * n[0] + vyr * n[1] + vzr * n[2]);
+  vi = -(vxi * n[0] + vyi * n[1] + vzi * n[2]);
+}
+
 // nvel: per frequency w, (nbeta + ndof) columns of 2^s N complex (headings
 // then DOFs, the pre-processor's problem order); nds: nforce x 2^s N;
 // fk: nforce x nbeta x nomega complex, accumulated with atomics (zeroed first).
@@ -96,24 +120,9 @@ __global__ void __launch_bounds__(128)
     }
     for (int b = 0; b < nbeta; ++b) {
       const PreWave& pw = waves[w * nbeta + b];
-      const double k = pw.k, kh = k * depth;
-      double cih, sih;
-      if (kh <= 20. && kh > 0.) {
-        cih = cosh(k * (xm[2] + depth)) / cosh(kh);
-        sih = sinh(k * (xm[2] + depth)) / cosh(kh);
-      } else {
-        cih = sih = exp(k * xm[2]);
-      }
-      const double wbar = (xm[0] - xeff) * pw.cb + (xm[1] - yeff) * pw.sb;
-      double se, ce;
-      sincos(k * wbar, &se, &ce);
-      const double gwk = g / pw.w * k;
-      // v = (gwk cb cih e, gwk sb cih e, -i gwk sih e), e = exp(i k wbar)
-      const double vxr = gwk * pw.cb * cih * ce, vxi = gwk * pw.cb * cih * se;
-      const double vyr = gwk * pw.sb * cih * ce, vyi = gwk * pw.sb * cih * se;
-      const double vzr = gwk * sih * se, vzi = -gwk * sih * ce;
-      nvel[row + (long long)nc * (b + (long long)npb * w)] =
-          make_double2(-(vxr * n[0] + vyr * n[1] + vzr * n[2]), -(vxi * n[0] + vyi * n[1] + vzi * n[2]));
+      double vr, vi, cih, ce, se;
+      pre_diffraction(pw, g, depth, xeff, yeff, xm, n, vr, vi, cih, ce, se);
+      nvel[row + (long long)nc * (b + (long long)npb * w)] = make_double2(vr, vi);
       if (fk) {
         const double pr = rho * g * cih * ce, pi = rho * g * cih * se;
         for (int q = 0; q < nforce; ++q) {
@@ -125,6 +134,40 @@ __global__ void __launch_bounds__(128)
       }
     }
   }
+}
+
+// Right-hand sides of serving requests: request r is (resident body, omega,
+// heading) with the body's ndof radiation DOFs; its NVEL block (2^s N) x
+// (1 + ndof) at nvel + nvel_off holds the diffraction column at the heading,
+// then the radiation columns, as the pre-processor orders the problems of one
+// frequency (one thread per panel and mesh half; grid.z = request).
+struct ReqDesc {
+  const double* xyz;
+  const int* m1234;
+  const PreDof* dofs;
+  PreWave wave;
+  double g, depth;
+  long long nvel_off;
+  int nfa, nsymy, ndof;
+};
+
+__global__ void __launch_bounds__(128) request_rhs_kernel(const ReqDesc* __restrict__ reqs, double2* __restrict__ nvel) {
+  const ReqDesc rq = reqs[blockIdx.z];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int half = blockIdx.y;
+  if (i >= rq.nfa || half > rq.nsymy) return;
+  double xm[3], n[3], area;
+  pre_panel(rq.xyz, rq.m1234, i, xm, n, area);
+  if (half) {
+    xm[1] = -xm[1];
+    n[1] = -n[1];
+  }
+  const int nc = rq.nfa * (rq.nsymy + 1), row = i + half * rq.nfa;
+  double2* out = nvel + rq.nvel_off;
+  double vr, vi, cih, ce, se;
+  pre_diffraction(rq.wave, rq.g, rq.depth, 0., 0., xm, n, vr, vi, cih, ce, se);
+  out[row] = make_double2(vr, vi);
+  for (int d = 0; d < rq.ndof; ++d) out[row + (long long)nc * (1 + d)] = make_double2(pre_dof(rq.dofs[d], xm, n), 0.);
 }
 
 }  // namespace nb200

@@ -1,34 +1,33 @@
 """Continuous-batching solve server on one GPU.
 
 Requests are (body, omega, heading) solves of Nemoh's per-frequency BEM
-problem: 6 radiation DOFs plus the diffraction problem at one heading, i.e.
-one (mesh, omega) system with 7 right-hand sides, whose result is the force
-matrix (nint x 7) of Solver/NEMOH.f90:137-141.
+problem: the diffraction problem at the request's heading plus the body's 6
+radiation DOFs, i.e. one (mesh, omega) system with 7 right-hand sides, whose
+result is the force matrix (nint x 7) of Solver/NEMOH.f90:137-141. The
+reference has no server: it runs one body's frequencies one after another
+(NEMOH.f90:129-143) with right-hand sides from its pre-processor
+(preProcessor/BodyConditions.f90:27-137).
 
 Design:
-* workers -- each owns one library context (its own CUDA stream and device
-  workspace), so batches of different workers overlap on the device;
-* meshes stay resident: a worker keeps its current mesh and switches with
-  `set_mesh` (panel geometry on the device, no table rebuild);
-* admission by HBM footprint: a batch takes at most as many frequencies as
-  fit the worker's share of device memory (two complex128 N x N matrices per
-  symmetry class plus workspace per frequency);
-* workspace reserved up front: each worker first solves the largest body at
-  `reserve` frequencies, so that later batches of up to that many frequencies
-  find their device buffers in place (growing a buffer frees the old one, and
-  cudaFree waits for every stream on the device, stalling the other workers);
-* continuous batching: whenever a worker is free it takes the body of the
-  oldest waiting request and every request of that body that has arrived,
-  up to its admission limit; requests that arrive while others run join the
-  next batch as soon as a worker frees up.
-
-Radiation right-hand sides do not depend on omega and are built once per
-body; the diffraction right-hand side of each request is built on the host
-(pre-processor formulas, cases.py).
+* resident bodies -- every body's mesh, generalised normals and DOFs are
+  added to every worker's context once (nemoh_b200_add_body,
+  nemoh_b200_set_body_dofs); a batch names bodies by index, nothing is
+  uploaded per request but (omega, heading);
+* right-hand sides on the device -- nemoh_b200_solve_requests builds each
+  request's diffraction and radiation conditions with the pre-processor's
+  formulas in a kernel;
+* cross-body batches -- a batch holds requests of any bodies; their systems
+  (of different orders) share one launch sequence (ragged batch);
+* admission by HBM footprint -- a batch takes waiting requests in arrival
+  order while their matrices and workspace (Body.bytes_per_frequency) fit
+  the worker's share of device memory;
+* continuous batching -- workers (one library context, CUDA stream and
+  workspace each) take the next batch as soon as they are free, so requests
+  that arrive while others are on the GPU join the next batch and batches of
+  different workers overlap on the device.
 """
 import collections
 import dataclasses
-import math
 import threading
 import time
 from typing import List, Optional
@@ -48,39 +47,25 @@ class Request:
     arrival: float = 0.0          # seconds from the start of the run
     start: float = 0.0
     done: float = 0.0
-    force: Optional[np.ndarray] = None   # (nint, 7): 6 radiation DOFs, then diffraction
+    force: Optional[np.ndarray] = None   # (nint, 7): diffraction at the heading, then the 6 radiation DOFs
     error: Optional[str] = None          # set when the request's batch failed
 
 
 class Body:
-    """One resident body: mesh, environment, generalised normals, radiation RHS."""
+    """One body of the stream: mesh, environment, 6 DOFs about the origin."""
 
     def __init__(self, mesh: C.Mesh, depth: float, rho=1025.0, g=9.81):
         self.case = C.Case(mesh, np.array([1.0]), np.array([0.0]), C.six_dofs(), C.six_dofs(), rho=rho, g=g,
                            depth=depth)
         self.mesh = mesh
-        self.nds = np.asfortranarray(C.generalised_normals(self.case))
-        xm, n, a = C.panel_quantities(mesh)
-        self._xm, self._n = xm, n
-        self.rad = np.stack([C._dof_vector(mesh, xm, n, a, d, False) for d in self.case.rad], axis=1)
 
     @property
     def npanels(self):
         return self.mesh.npanels
 
-    def rhs(self, omega, beta_deg):
-        """(2^s N, 7) right-hand sides: 6 radiation DOFs then the diffraction problem."""
-        k = C.wavenumber(omega, self.case.g, self.case.depth)
-        beta = beta_deg * math.pi / 180.0
-        xm, n = self._xm, self._n
-        _, vx, vy, vz = C._wave(self.case, k, omega, beta, xm[:, 0], xm[:, 1], xm[:, 2])
-        diff = -(vx * n[:, 0] + vy * n[:, 1] + vz * n[:, 2])
-        if self.mesh.isym == 1:
-            _, vx, vy, vz = C._wave(self.case, k, omega, beta, xm[:, 0], -xm[:, 1], xm[:, 2])
-            diff = np.concatenate([diff, -(vx * n[:, 0] - vy * n[:, 1] + vz * n[:, 2])])
-        return np.concatenate([self.rad.astype(np.complex128), diff[:, None]], axis=1)
-
     def bytes_per_frequency(self):
+        """Device bytes of one request: D and S in FP64, the FP32 copy of D,
+        and the right-hand-side workspace, per symmetry class."""
         n = self.npanels
         cls = 2 if self.mesh.isym else 1
         return cls * n * n * 16 * 2 + cls * n * n * 8 + cls * n * 7 * 16 * 6
@@ -102,12 +87,13 @@ class SolveServer:
     """Serve a stream of requests on one GPU with `workers` concurrent contexts."""
 
     def __init__(self, bodies: List[Body], device=0, precision=MIXED, workers=2, memory_fraction=0.6,
-                 solver_factory=None, memory_bytes=None, reserve=0):
+                 solver_factory=None, memory_bytes=None, max_batch=64):
         self.bodies = bodies
         self.device = device
         self.precision = precision
         self.nworkers = workers
         self.memory_fraction = memory_fraction
+        self.max_batch = max_batch
         self._lock = threading.Condition()
         self._pending = collections.deque()
         self._done: List[Request] = []
@@ -115,70 +101,53 @@ class SolveServer:
         self._feeding = False
         make = solver_factory or (lambda: Solver(device, precision))
         self._solvers = [make() for _ in range(workers)]
-        self._current = [None] * workers
-        self.batches = []   # (worker, body, nreq, t0, t1)
+        for s in self._solvers:
+            for b in bodies:
+                bid = s.add_body(b.case)
+                s.set_body_dofs(bid, b.case.rad)
+        self.batches = []   # (worker, bodies in the batch, nreq, t0, t1)
         free = memory_bytes
         if free is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
         self._budget = free * memory_fraction / workers
-        if reserve > 0 and bodies:
-            big = max(range(len(bodies)), key=lambda b: bodies[b].bytes_per_frequency())
-            body = bodies[big]
-            k = min(reserve, self.admission(body))
-            omegas = np.linspace(0.5, 2.0, k)
-            nvel = np.stack([body.rhs(w, 0.0) for w in omegas], axis=2)
-            for w, s in enumerate(self._solvers):
-                s.set_case(body.case)
-                s.solve_frequencies(omegas, nvel, body.nds)
-                self._current[w] = big
 
     def close(self):
         for s in self._solvers:
             s.close()
 
     def admission(self, body: Body):
-        """Frequencies per batch that fit this worker's share of HBM."""
+        """Requests of this body alone that fit a worker's share of HBM."""
         return max(1, int(self._budget // body.bytes_per_frequency()))
 
-    def _take_batch(self, w):
+    def _take_batch(self):
+        """Waiting requests in arrival order while they fit the budget (at least one)."""
         with self._lock:
             while not self._pending:
                 if not self._feeding:
                     return None
                 self._lock.wait(timeout=0.005)
-            head = self._pending[0]
-            b = head.body
-            cap = self.admission(self.bodies[b])
-            batch, keep = [], collections.deque()
-            while self._pending:
-                r = self._pending.popleft()
-                if r.body == b and len(batch) < cap:
-                    batch.append(r)
-                else:
-                    keep.append(r)
-            self._pending = keep
+            batch, used = [], 0
+            while self._pending and len(batch) < self.max_batch:
+                need = self.bodies[self._pending[0].body].bytes_per_frequency()
+                if batch and used + need > self._budget:
+                    break
+                batch.append(self._pending.popleft())
+                used += need
             return batch
 
     def _worker(self, w, t0):
         s = self._solvers[w]
         while True:
-            batch = self._take_batch(w)
+            batch = self._take_batch()
             if batch is None:
                 return
-            b = batch[0].body
-            body = self.bodies[b]
             tb = time.perf_counter() - t0
             for r in batch:
                 r.start = tb
             try:
-                if self._current[w] != b:
-                    self._current[w] = None
-                    s.set_case(body.case)
-                    self._current[w] = b
-                omegas = np.array([r.omega for r in batch])
-                nvel = np.stack([body.rhs(r.omega, r.beta_deg) for r in batch], axis=2)
-                force = s.solve_frequencies(omegas, nvel, body.nds)
+                force = s.solve_requests(np.array([r.body for r in batch]), np.array([r.omega for r in batch]),
+                                         np.radians([r.beta_deg for r in batch]))
             except Exception as e:   # the batch fails as a whole; the worker serves on
                 td = time.perf_counter() - t0
                 for r in batch:
@@ -188,12 +157,12 @@ class SolveServer:
                     self._failed.extend(batch)
                 continue
             td = time.perf_counter() - t0
-            for i, r in enumerate(batch):
-                r.force = force[:, :, i]
+            for r, f in zip(batch, force):
+                r.force = f
                 r.done = td
             with self._lock:
                 self._done.extend(batch)
-                self.batches.append((w, b, len(batch), tb, td))
+                self.batches.append((w, len({r.body for r in batch}), len(batch), tb, td))
 
     def run(self, requests: List[Request], realtime=True):
         """Feed requests at their arrival times (or all at once) and wait for all results."""

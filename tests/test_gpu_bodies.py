@@ -102,3 +102,27 @@ def test_bodies_refuse_unknown_body_and_keep_working():
         out = s.solve_bodies(np.array([0]), np.array([0.9]), [nv])
         ref = _single(cases[0], nb.FP64, [0.9], [nv])[0]
         assert np.abs(out[0] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_requests_with_device_rhs_match_host_rhs():
+    """nemoh_b200_solve_requests builds each request's right-hand sides on the
+    device (pre-processor formulas); its forces equal those of
+    nemoh_b200_solve_bodies given the host pre-processor's right-hand sides
+    for the same (body, omega, heading), within 1e-12 of the largest force."""
+    B.build()
+    cases = _bodies()
+    body, omega = _items(cases, seed=8, n=12)
+    beta = np.random.default_rng(9).uniform(0.0, 180.0, len(body))
+    nvels = [_rhs(cases[b], w, be) for b, w, be in zip(body, omega, beta)]
+    for mode in (nb.FP64, nb.MIXED):
+        with nb.Solver(0, mode) as s:
+            for c in cases:
+                bid = s.add_body(c)
+                s.set_body_dofs(bid, c.rad)
+            got = s.solve_requests(body, omega, np.radians(beta))
+            ref = s.solve_bodies(body, omega, nvels)
+        # mixed precision: both sides refined to a 1e-12 residual, not bitwise
+        tol = 1e-12 if mode == nb.FP64 else 1e-10
+        for g, r in zip(got, ref):
+            assert g.shape == r.shape
+            assert np.abs(g - r).max() <= tol * np.abs(r).max()

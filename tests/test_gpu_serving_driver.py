@@ -24,7 +24,8 @@ def test_serving_result_same_alone_and_in_the_mix(precision):
         reqs = S.make_requests(48, rate=0, n_bodies=4, seed=12)
         done, wall = srv.run(reqs, realtime=False)
         assert sorted(r.rid for r in done) == list(range(48))
-        assert max(b[2] for b in srv.batches) > 1
+        assert max(b[2] for b in srv.batches) > 1     # requests were batched
+        assert max(b[1] for b in srv.batches) > 1     # with requests of different bodies together
         by = {r.rid: r for r in done}
         for rid in (0, 17, 33):
             r0 = reqs[rid]

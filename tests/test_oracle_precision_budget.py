@@ -65,3 +65,31 @@ def test_fp32_factors_refined_against_fp64_matrices_meet_it(hemisphere):
     case, mats, nvel, nds, F64 = hemisphere
     err, _ = bench.rel_err_families(_forces(case, mats, nvel, nds, _fp32_lu_refined), F64, len(case.betas_deg))
     assert err < 1e-8, err
+
+
+def _near_field(o, case):
+    """Pairs (I, J) whose Rankine integral the reference evaluates exactly:
+    RO <= 7 TDIS(J) for one of the images the pair is summed over (direct,
+    free-surface image, y-mirrors; COMPUTE_GREEN_INFD.f90:80-98)."""
+    geo, _ = o.geometry()
+    XG, YG, ZG, T = geo[3], geo[4], geo[5], geo[7]
+    ro = []
+    for sy in ((1.0, -1.0) if case.mesh.isym else (1.0,)):
+        for zj in (ZG, -ZG):
+            ro.append(np.sqrt((XG[:, None] - XG[None, :]) ** 2 + (YG[:, None] - sy * YG[None, :]) ** 2 +
+                              (ZG[:, None] - zj[None, :]) ** 2))
+    return np.min(ro, axis=0) <= 7.0 * T[None, :]
+
+
+def test_fp32_far_field_split_misses_the_budget(hemisphere):
+    """The split of near-field pairs in FP64 and far-field pairs in FP32, at
+    its most favourable: near-field entries exact, far-field entries the FP64
+    values rounded to single precision (the least error an FP32 evaluation of
+    them can have). Solved exactly, it still misses 1e-6 on the jittered
+    hemisphere (observed 1.8e-5; 76% of its pairs are near field)."""
+    case, mats, nvel, nds, F64 = hemisphere
+    o = G.oracle_for(case)
+    near = _near_field(o, case)
+    split = [tuple(np.where(near, m, m.astype(np.complex64).astype(np.complex128)) for m in ms) for ms in mats]
+    err, _ = bench.rel_err_families(_forces(case, split, nvel, nds, np.linalg.solve), F64, len(case.betas_deg))
+    assert err > 1e-6, err

@@ -9,22 +9,30 @@ from nemoh_b200 import serving as S
 
 
 class FakeSolver:
-    """Returns force = sum of the RHS columns scaled by omega; records batches."""
+    """Resident bodies; a request's forces are a fixed function of (body,
+    omega, heading), the same alone and in any batch; records batch sizes."""
     calls = []
     lock = threading.Lock()
 
     def __init__(self):
-        self.mesh = None
+        self.cases = []
 
-    def set_case(self, case):
-        self.mesh = case.mesh
+    def add_body(self, case):
+        self.cases.append(case)
+        return len(self.cases) - 1
 
-    def solve_frequencies(self, omegas, nvel, nds):
+    def set_body_dofs(self, body, dofs):
+        assert len(dofs) == 6
+
+    def solve_requests(self, bodies, omegas, betas):
         time.sleep(0.002)
         with FakeSolver.lock:
-            FakeSolver.calls.append(len(omegas))
-        f = np.einsum("cpw,ic->ipw", nvel, nds) * omegas[None, None, :]
-        return f
+            FakeSolver.calls.append(len(bodies))
+        out = []
+        for b, w, be in zip(bodies, omegas, betas):
+            n = self.cases[b].mesh.npanels
+            out.append(np.outer(np.arange(1, 7), np.arange(1, 8)) * (w + 1j * np.cos(be)) * n)
+        return out
 
     def close(self):
         pass
@@ -70,10 +78,10 @@ def test_admission_limits_batch_by_memory():
 class FailingSolver(FakeSolver):
     """Raises on every batch that contains the frequency 0.777 (a status-code error)."""
 
-    def solve_frequencies(self, omegas, nvel, nds):
+    def solve_requests(self, bodies, omegas, betas):
         if np.any(np.isclose(omegas, 0.777)):
             raise RuntimeError("nemoh_b200 status 5: EAKZ")
-        return super().solve_frequencies(omegas, nvel, nds)
+        return super().solve_requests(bodies, omegas, betas)
 
 
 def test_failed_batch_is_reported_not_dropped():
