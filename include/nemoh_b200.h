@@ -165,6 +165,19 @@ int nemoh_b200_add_body(nemoh_ctx* ctx, int np, int nfa, int nsymy, const double
 int nemoh_b200_body_count(const nemoh_ctx* ctx);
 int nemoh_b200_solve_bodies(nemoh_ctx* ctx, int nitem, const int* body, const double* omegas, int nrhs,
                             const double* nvel, double* force);
+/* CUDA graphs for repeated cross-body batches (on = 1; off by default). In
+ * graph mode every batch of nemoh_b200_solve_bodies / _solve_requests does
+ * its host setup and uploads first and then issues its launch sequence, which
+ * reads device buffers only; the second batch with the same sequence (same
+ * bodies' orders and depth regimes in the same order, nrhs, buffers and
+ * pointers) is captured into a graph and later ones replay it. Refinement
+ * passes beyond the REFINE_CHUNK captured ones and the FP64 fallback run as
+ * ordinary launches after the replay. The timings of nemoh_b200_last_timings
+ * then hold the whole batch in solve_ms (assembly and factor 0).
+ * nemoh_b200_graph_stats: graphs captured and replayed so far. */
+int nemoh_b200_set_graphs(nemoh_ctx* ctx, int on);
+int nemoh_b200_graph_stats(const nemoh_ctx* ctx, long long* captures, long long* replays);
+
 /* Serving requests on resident bodies. nemoh_b200_set_body_dofs gives a body
  * its ndof radiation DOFs (kind, dir, axis as in nemoh_b200_body_conditions;
  * 1 + ndof <= 16). nemoh_b200_solve_requests solves nreq (body[i], omegas[i],

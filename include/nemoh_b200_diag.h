@@ -20,6 +20,10 @@ int nemoh_b200_diag_theta_quadrature(double akk, double* qq, double* cq);
  * smallest x whose truncated log10 formula gives >= k, found by bisection on the
  * double bit pattern with the host's log10 */
 int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5);
+/* autotuner of the triangular sweep: keys tuned in this process so far, and
+ * the cluster size chosen for a batch of nsys systems of order n with nrhs
+ * right-hand sides in single (1) or double (0) precision (0 if not tuned) */
+int nemoh_b200_diag_sweep_tuning(long long* keys_tuned, int n, int nsys, int nrhs, int single, int* cluster_size);
 
 #ifdef __cplusplus
 }

@@ -90,6 +90,8 @@ def load_library():
     L.nemoh_b200_solve_bodies.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _d, _d]
     L.nemoh_b200_solve_bodies_device.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _vp, _vp, _vp]
     L.nemoh_b200_set_body_dofs.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _i, _d, _d]
+    L.nemoh_b200_set_graphs.argtypes = [_vp, ctypes.c_int]
+    L.nemoh_b200_graph_stats.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.nemoh_b200_solve_requests.argtypes = [_vp, ctypes.c_int, _i, _d, _d, _d]
     L.nemoh_b200_diag_dispersion_root.argtypes = [ctypes.c_double, _d]
     L.nemoh_b200_diag_exponential_fit.argtypes = [ctypes.c_double, ctypes.c_double, _i, _d, _d]
@@ -251,6 +253,15 @@ class Solver:
             out.append(force[o:o + sz].reshape((self._bodies[b][1], nrhs), order="F"))
             o += sz
         return out
+
+    def set_graphs(self, on=True):
+        """Capture repeated cross-body batches into CUDA graphs and replay them."""
+        self._check(load_library().nemoh_b200_set_graphs(self._h, 1 if on else 0))
+
+    def graph_stats(self):
+        cap, rep = ctypes.c_longlong(), ctypes.c_longlong()
+        load_library().nemoh_b200_graph_stats(self._h, ctypes.byref(cap), ctypes.byref(rep))
+        return cap.value, rep.value
 
     def set_body_dofs(self, body, dofs):
         """Radiation DOFs (cases.Dof list) of a resident body's serving requests."""

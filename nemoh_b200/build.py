@@ -30,7 +30,7 @@ def _sources(names):
 
 LIB_SRC = ["api.cu", "fd_setup.cpp"]
 DEPS = ["api.cu", "fd_setup.cpp", "fd_setup.h", "common.cuh", "green.cuh", "assembly.cuh", "linalg.cuh",
-        "mixed.cuh", "tc_gemm.cuh", "kochin.cuh", "preproc.cuh", "freesurface.cuh", "postproc.cuh", "case_io.h", "driver.cpp", "postproc.cpp"]
+        "mixed.cuh", "tc_gemm.cuh", "tune.cuh", "kochin.cuh", "preproc.cuh", "freesurface.cuh", "postproc.cuh", "case_io.h", "driver.cpp", "postproc.cpp"]
 
 
 def _stale(target, deps):

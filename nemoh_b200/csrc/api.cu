@@ -100,6 +100,13 @@ struct BodyState {
   DevBuf d_xyz, d_m, d_rec, d_rows, d_nds, d_dofs;
 };
 
+// a launch sequence seen before (key of its shapes and buffers) and, from its
+// second sighting on, its captured graph
+struct GraphEntry {
+  unsigned long long key;
+  cudaGraphExec_t exec;
+};
+
 }  // namespace
 
 struct nemoh_ctx {
@@ -132,6 +139,10 @@ struct nemoh_ctx {
   std::vector<std::unique_ptr<BodyState>> bodies;
   DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce, d_reqs;
   HostBuf h_rag, h_reqs;
+  // CUDA graphs of cross-body batches (nemoh_b200_set_graphs)
+  bool graph_mode = false;
+  std::vector<GraphEntry> graphs;
+  long long graph_captures = 0, graph_replays = 0;
 };
 
 #define CK(call)                                                                                 \
@@ -358,26 +369,45 @@ GreenCtx green_ctx(nemoh_ctx* c) {
 // those frequencies: deep-water slots first, then finite-depth ones. Ragged
 // batches pass each slot's mesh on the device (dmesh) and its order on the
 // host (host_n); each launch's grid is then sized by its largest slot.
-void assemble_range(nemoh_ctx* c, int s0, int s1, const SlotMesh* dmesh = nullptr, const int* host_n = nullptr) {
-  const int N = c->nfa, cls = ncls(c);
+// One assembly group: its slots [s0, s1) ordered deep water first, and the
+// launch shape of each depth regime.
+struct AsmGroup {
+  int s0, s1, ninfd, nfd, n_infd, n_fd;
+};
+
+// uploads the parameters and slot order of slots [s0, s1) (already in c->h_oms)
+AsmGroup assemble_upload(nemoh_ctx* c, int s0, int s1, const int* host_n) {
+  const int N = c->nfa;
   const OmegaParams* hom = c->h_oms.as<OmegaParams>();
   int* hs = c->h_slots.as<int>() + s0;
-  int ninfd = 0, n_infd = 0, n_fd = 0;
+  AsmGroup ag{s0, s1, 0, 0, 0, 0};
   for (int s = s0; s < s1; ++s)
     if (!hom[s].fd) {
-      hs[ninfd++] = s;
-      n_infd = std::max(n_infd, host_n ? host_n[s] : N);
+      hs[ag.ninfd++] = s;
+      ag.n_infd = std::max(ag.n_infd, host_n ? host_n[s] : N);
     }
-  int nfd = 0;
   for (int s = s0; s < s1; ++s)
     if (hom[s].fd) {
-      hs[ninfd + nfd++] = s;
-      n_fd = std::max(n_fd, host_n ? host_n[s] : N);
+      hs[ag.ninfd + ag.nfd++] = s;
+      ag.n_fd = std::max(ag.n_fd, host_n ? host_n[s] : N);
     }
   CK(cudaMemcpyAsync(c->d_oms.as<OmegaParams>() + s0, hom + s0, (size_t)(s1 - s0) * sizeof(OmegaParams),
                      cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_slots.as<int>() + s0, hs, (size_t)(s1 - s0) * sizeof(int), cudaMemcpyHostToDevice,
                      c->stream));
+  return ag;
+}
+
+void assemble_launch(nemoh_ctx* c, const AsmGroup& ag, const SlotMesh* dmesh);
+
+void assemble_range(nemoh_ctx* c, int s0, int s1, const SlotMesh* dmesh = nullptr, const int* host_n = nullptr) {
+  assemble_launch(c, assemble_upload(c, s0, s1, host_n), dmesh);
+}
+
+// the Rankine and wave passes of one group (reads only device buffers)
+void assemble_launch(nemoh_ctx* c, const AsmGroup& ag, const SlotMesh* dmesh) {
+  const int N = c->nfa, cls = ncls(c);
+  const int s0 = ag.s0, ninfd = ag.ninfd, nfd = ag.nfd, n_infd = ag.n_infd, n_fd = ag.n_fd;
   GreenCtx g = green_ctx(c);
   const long long NN = (long long)N * N;
   AsmOut o{c->d_D.as<double2>(), c->d_S.as<double2>(), cls * NN};
@@ -452,7 +482,7 @@ void factor_fp64(nemoh_ctx* c, int nsys, const Shape& sh) {
 
 // solve the factored systems for the right-hand sides in X (result in X)
 void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
-  CK(trsm_sweep<double2>(dbatch(c, sh), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys,
+  CK(trsm_sweep_tuned<double2>(dbatch(c, sh), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys,
                          nrhs, c->stream, c->launches));
   CK(cudaGetLastError());
 }
@@ -644,41 +674,151 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   // the uniform path's buffers and cached factors no longer hold what they did
   c->cap_nfa = -1;
   c->w_previous = -1.;
-  CK(cudaEventRecord(c->ev[0], c->stream));
+  const long long xs = (long long)N * nrhs;
+  const Shape sh{nmax, Ragged{c->d_roff.as<long long>(), c->d_rord.as<int>(), ord.data()}};
   OmegaParams* hom = c->h_oms.as<OmegaParams>();
-  int done = 0;
-  for (int j = 0; j < k; ++j) {
+  auto host_setup = [&](int j) {
     BodyState& b = *c->bodies[body[items[j]]];
     const double T = 2. * kPI / omegas[items[j]];
     omega_params_env(Env{b.g, b.depth, b.gm, &b.nq_state}, 2. * kPI / T, hom[j], true);
-    if (j + 1 == k || j + 1 - done >= ASM_GROUP) {
-      assemble_range(c, done, j + 1, c->d_smesh.as<SlotMesh>(), host_n.data());
-      done = j + 1;
-    }
-  }
-  CK(cudaEventRecord(c->ev[1], c->stream));
-  const long long xs = (long long)N * nrhs;
-  fold_rhs_ragged_kernel<<<dim3((nmax + 127) / 128, nrhs, k), 128, 0, c->stream>>>(nvel_d, c->d_items.as<ItemDesc>(),
-                                                                                  nrhs, xs, c->d_X.as<double2>());
-  LAUNCHED(c);
-  const Shape sh{nmax, Ragged{c->d_roff.as<long long>(), c->d_rord.as<int>(), ord.data()}};
-  factor_and_solve(c, nsys, nrhs, true, sh);
-  CK(cudaEventRecord(c->ev[2], c->stream));
-  potential(c, nsys, nrhs, sh);
-  if (nint_max > 0) {
-    force_ragged_kernel<<<dim3(nint_max, nrhs, k), 256, 0, c->stream>>>(c->d_Y.as<double2>(), c->d_items.as<ItemDesc>(),
-                                                                       c->d_oms.as<OmegaParams>(), nrhs, xs, force_d);
+  };
+  auto fold = [&] {
+    fold_rhs_ragged_kernel<<<dim3((nmax + 127) / 128, nrhs, k), 128, 0, c->stream>>>(
+        nvel_d, c->d_items.as<ItemDesc>(), nrhs, xs, c->d_X.as<double2>());
     LAUNCHED(c);
+  };
+  auto potential_forces = [&] {
+    potential(c, nsys, nrhs, sh);
+    if (nint_max > 0) {
+      force_ragged_kernel<<<dim3(nint_max, nrhs, k), 256, 0, c->stream>>>(
+          c->d_Y.as<double2>(), c->d_items.as<ItemDesc>(), c->d_oms.as<OmegaParams>(), nrhs, xs, force_d);
+      LAUNCHED(c);
+    }
+  };
+  if (!c->graph_mode) {
+    // host setup of each item overlapped with the assembly of the groups set up before it
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    int done = 0;
+    for (int j = 0; j < k; ++j) {
+      host_setup(j);
+      if (j + 1 == k || j + 1 - done >= ASM_GROUP) {
+        assemble_range(c, done, j + 1, c->d_smesh.as<SlotMesh>(), host_n.data());
+        done = j + 1;
+      }
+    }
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    fold();
+    factor_and_solve(c, nsys, nrhs, true, sh);
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    potential_forces();
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    check_status(c);
+    float a, f, s;
+    CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+    CK(cudaEventElapsedTime(&f, c->ev[1], c->ev[2]));
+    CK(cudaEventElapsedTime(&s, c->ev[2], c->ev[3]));
+    c->t_asm += a;
+    c->t_fac += f;
+    c->t_sol += s;
+    return;
+  }
+  // Graph mode: every host setup and upload first, then one launch sequence
+  // that reads device buffers only. The second batch with the same launch
+  // sequence (same shapes, buffers and pointers) is captured, later ones
+  // replay the captured graph.
+  std::vector<AsmGroup> groups;
+  for (int j0 = 0; j0 < k; j0 += ASM_GROUP) {
+    const int j1 = std::min(k, j0 + ASM_GROUP);
+    for (int j = j0; j < j1; ++j) host_setup(j);
+    groups.push_back(assemble_upload(c, j0, j1, host_n.data()));
+  }
+  const bool mixed = c->mode == NEMOH_B200_MIXED;
+  const int max_it = refine_max_it(), passes = mixed ? std::min(REFINE_CHUNK, max_it) : 0;
+  std::vector<long long> sig = {c->mode, nrhs, k, nsys, nmax, nint_max, passes, (long long)nvel_d,
+                                (long long)force_d, (long long)c->d_D.p, (long long)c->d_S.p, (long long)c->d_X.p,
+                                (long long)c->d_Y.p, (long long)c->d_diag.p, (long long)c->d_inv.p,
+                                (long long)c->d_oms.p, (long long)c->d_slots.p, (long long)c->d_smesh.p,
+                                (long long)c->d_items.p, (long long)c->d_roff.p, (long long)c->d_rord.p,
+                                (long long)c->mixed.lu, (long long)c->mixed.diag, (long long)c->mixed.b,
+                                (long long)c->mixed.r, (long long)c->mixed.rf, (long long)c->mixed.yf,
+                                (long long)c->mixed.inv, (long long)c->mixed.pinv, (long long)c->mixed.norms,
+                                (long long)c->mixed.state, (long long)c->mixed.tc.a, (long long)c->mixed.tc.b};
+  for (const AsmGroup& g : groups) sig.insert(sig.end(), {g.ninfd, g.nfd, g.n_infd, g.n_fd});
+  sig.insert(sig.end(), ord.begin(), ord.end());
+  unsigned long long key = 1469598103934665603ull;   // FNV-1a over the signature
+  for (long long v : sig)
+    for (int b = 0; b < 8; ++b) key = (key ^ (unsigned long long)((v >> (8 * b)) & 0xff)) * 1099511628211ull;
+  GraphEntry* ge = nullptr;
+  for (GraphEntry& e : c->graphs)
+    if (e.key == key) ge = &e;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  auto issue = [&] {
+    for (const AsmGroup& g : groups) assemble_launch(c, g, c->d_smesh.as<SlotMesh>());
+    fold();
+    c->lu64 = !mixed;
+    if (mixed) {
+      mixed_factor(c->mixed, c->d_D.as<double2>(), nmax, nsys, c->d_status.as<int>(), c->stream, c->launches,
+                   &c->lanes, /*have_f32=*/true, sh.rg);
+      const RefineArgs a{c->d_D.as<double2>(), nmax, nsys, nrhs, c->d_X.as<double2>(), sh.rg};
+      mixed_refine_begin(c->mixed, a, max_it, c->stream, c->launches);
+      mixed_refine_passes(c->mixed, a, passes, c->stream, c->launches);
+    } else {
+      factor_fp64(c, nsys, sh);
+      trsm_fp64(c, nsys, nrhs, sh);
+    }
+    potential_forces();
+  };
+  if (ge && ge->exec) {
+    CK(cudaGraphLaunch(ge->exec, c->stream));
+    ++c->graph_replays;
+  } else if (ge) {   // second sighting: capture, then launch the graph
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      issue();
+    } catch (...) {
+      cudaStreamEndCapture(c->stream, &gr);
+      if (gr) cudaGraphDestroy(gr);
+      throw;
+    }
+    CK(cudaStreamEndCapture(c->stream, &gr));
+    const cudaError_t e = cudaGraphInstantiate(&ge->exec, gr, 0);
+    cudaGraphDestroy(gr);
+    CK(e);
+    CK(cudaGraphLaunch(ge->exec, c->stream));
+    ++c->graph_captures;
+  } else {   // first sighting: run as is and remember the sequence
+    issue();
+    if (c->graphs.size() >= 16) {
+      if (c->graphs.front().exec) cudaGraphExecDestroy(c->graphs.front().exec);
+      c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back(GraphEntry{key, nullptr});
   }
   CK(cudaEventRecord(c->ev[3], c->stream));
   check_status(c);
-  float a, f, s;
-  CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
-  CK(cudaEventElapsedTime(&f, c->ev[1], c->ev[2]));
-  CK(cudaEventElapsedTime(&s, c->ev[2], c->ev[3]));
-  c->t_asm += a;
-  c->t_fac += f;
-  c->t_sol += s;
+  float s = 0;
+  CK(cudaEventElapsedTime(&s, c->ev[0], c->ev[3]));
+  c->t_sol += s;   // graph mode times the batch as a whole
+  if (mixed) {
+    // refinement passes beyond those in the sequence, and the FP64 fallback,
+    // run as ordinary launches; the potential and forces are then redone
+    const RefineArgs a{c->d_D.as<double2>(), nmax, nsys, nrhs, c->d_X.as<double2>(), sh.rg};
+    bool more = mixed_refine_read(c->mixed, c->stream), redo = false;
+    for (int it = passes; more && it < max_it; it += REFINE_CHUNK) {
+      mixed_refine_passes(c->mixed, a, std::min(REFINE_CHUNK, max_it - it), c->stream, c->launches);
+      more = mixed_refine_read(c->mixed, c->stream);
+      redo = true;
+    }
+    if (c->mixed.last_residual > REFINE_TOL) {
+      mixed_fallback(c, nsys, nrhs, sh);
+      redo = true;
+    }
+    if (redo) {
+      potential_forces();
+      check_status(c);
+    }
+  }
 }
 
 void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* omegas, int nrhs,
@@ -829,6 +969,8 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int g = 0; g < LANES; ++g)
     if (c->lanes.s[g]) cudaStreamSynchronize(c->lanes.s[g]);
+  for (GraphEntry& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (int g = 0; g < LANES; ++g) {
@@ -887,6 +1029,24 @@ int nemoh_b200_add_body(nemoh_ctx* c, int np, int nfa, int nsymy, const double* 
 }
 
 int nemoh_b200_body_count(const nemoh_ctx* c) { return c ? (int)c->bodies.size() : 0; }
+
+int nemoh_b200_set_graphs(nemoh_ctx* c, int on) {
+  if (!c) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    CK(cudaStreamSynchronize(c->stream));
+    for (GraphEntry& g : c->graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+    c->graph_mode = on != 0;
+  });
+}
+
+int nemoh_b200_graph_stats(const nemoh_ctx* c, long long* captures, long long* replays) {
+  if (!c) return NEMOH_B200_EINVAL;
+  if (captures) *captures = c->graph_captures;
+  if (replays) *replays = c->graph_replays;
+  return NEMOH_B200_OK;
+}
 
 static int bodies_args_ok(const nemoh_ctx* c, int nitem, const int* body, const double* omegas) {
   if (!c || nitem < 1 || !body || !omegas) return 0;
@@ -1456,6 +1616,19 @@ int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5) {
     kj8[k] = t.kj8[k];
     kj5[k] = t.kj5[k];
     ki5[k] = t.ki5[k];
+  }
+  return 0;
+}
+
+int nemoh_b200_diag_sweep_tuning(long long* keys_tuned, int n, int nsys, int nrhs, int single, int* cluster_size) {
+  SweepTuner& t = sweep_tuner();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(t.mu);
+  if (keys_tuned) *keys_tuned = t.tuned;
+  if (cluster_size) {
+    auto it = t.best.find(sweep_key(dev, single != 0, n, nsys, nrhs));
+    *cluster_size = it == t.best.end() ? 0 : it->second;
   }
   return 0;
 }

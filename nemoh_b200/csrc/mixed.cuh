@@ -19,6 +19,7 @@
 
 #include "linalg.cuh"
 #include "tc_gemm.cuh"
+#include "tune.cuh"
 
 namespace nb200 {
 
@@ -181,7 +182,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
 inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches,
                      const int* active, const Ragged& rg) {
   BatchT<float2> b = make_batch<float2>(w.lu, n, w.diag, nullptr, rg);
-  trsm_sweep<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, active);
+  trsm_sweep_tuned<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, active);
   // the solution is left in w.rf (forward into yf, backward back into rf)
 }
 

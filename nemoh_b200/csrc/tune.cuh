@@ -1,0 +1,120 @@
+// Autotuner of the triangular sweep's tile shape.
+//
+// The sweep (linalg.cuh, trsm_sweep_kernel) spreads the 64-row blocks of one
+// system over a thread-block cluster of csize CTAs (1, 2, 4 or 8): a larger
+// cluster puts more SMs on one system's updates but adds cluster barriers and
+// distributed-shared-memory copies per step. The fastest csize depends on the
+// number of systems in the batch, their order, the precision and the number
+// of right-hand sides. The tuner times every candidate once per key (device,
+// element type, power-of-two buckets of the order, of the system count and
+// of the right-hand sides) on a copy of the batch's right-hand sides, keeps
+// the fastest for the life of the process, and then solves with it. Under
+// stream capture (no timing possible) and before a key has been tuned without
+// scratch, the SM-count heuristic of trsm_sweep decides.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <map>
+#include <mutex>
+
+#include "linalg.cuh"
+
+namespace nb200 {
+
+struct SweepTuner {
+  std::mutex mu;
+  std::map<unsigned long long, int> best;   // key -> cluster size
+  void* scratch[64] = {};                   // per device: right-hand sides kept while candidates run
+  size_t scratch_bytes[64] = {};
+  long long tuned = 0;                      // keys tuned so far (diagnostics)
+};
+
+inline SweepTuner& sweep_tuner() {
+  static SweepTuner t;
+  return t;
+}
+
+inline int log2_bucket(long long v) {
+  int b = 0;
+  while ((1LL << b) < v) ++b;
+  return b;
+}
+
+inline unsigned long long sweep_key(int dev, bool f32, int n, int nsys, int nrhs) {
+  return ((unsigned long long)dev << 40) | ((unsigned long long)f32 << 32) |
+         ((unsigned long long)log2_bucket(n) << 16) | ((unsigned long long)log2_bucket(nsys) << 8) |
+         (unsigned long long)log2_bucket(nrhs);
+}
+
+// cluster size cached for this batch's key, 0 if none yet
+template <class C2>
+inline int sweep_tuned_size(const BatchT<C2>& b, int nsys, int nrhs) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  SweepTuner& t = sweep_tuner();
+  std::lock_guard<std::mutex> lock(t.mu);
+  auto it = t.best.find(sweep_key(dev, sizeof(C2) == sizeof(float2), b.n, nsys, nrhs));
+  return it == t.best.end() ? 0 : it->second;
+}
+
+// trsm_sweep with the tuned cluster size; tunes the key first when it is new
+// and the stream is not being captured. X: right-hand sides in, solution out.
+template <class C2>
+inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st,
+                                    long long& launches, const int* active = nullptr) {
+  int csize = sweep_tuned_size(b, nsys, nrhs);
+  if (csize > 0) return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, csize);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long key = sweep_key(dev, sizeof(C2) == sizeof(float2), b.n, nsys, nrhs);
+  const size_t bytes = (size_t)nsys * b.n * nrhs * sizeof(C2);
+  SweepTuner& t = sweep_tuner();
+  std::lock_guard<std::mutex> lock(t.mu);
+  cudaError_t e;
+  if (dev < 0 || dev >= 64) return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active);
+  void*& scratch = t.scratch[dev];
+  if (t.scratch_bytes[dev] < bytes) {
+    cudaFree(scratch);
+    scratch = nullptr;
+    t.scratch_bytes[dev] = 0;
+    if ((e = cudaMalloc(&scratch, bytes)) != cudaSuccess) return e;
+    t.scratch_bytes[dev] = bytes;
+  }
+  if ((e = cudaMemcpyAsync(scratch, X, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+  cudaEvent_t ev[2];
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
+  const int nblk = (b.n + TB - 1) / TB;
+  float best_ms = FLT_MAX;
+  int best_c = 0;
+  for (int c = 1; c <= 8 && c <= nblk; c *= 2) {
+    cudaMemcpyAsync(X, scratch, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaEventRecord(ev[0], st);
+    long long l = 0;
+    e = trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, l, active, c);
+    cudaEventRecord(ev[1], st);
+    if (e != cudaSuccess) {   // e.g. a cluster that cannot be scheduled: not a candidate
+      cudaGetLastError();
+      continue;
+    }
+    float ms = 0.f;
+    if (cudaEventSynchronize(ev[1]) != cudaSuccess || cudaEventElapsedTime(&ms, ev[0], ev[1]) != cudaSuccess) continue;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_c = c;
+    }
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (!best_c) return cudaErrorLaunchFailure;
+  t.best[key] = best_c;
+  ++t.tuned;
+  if ((e = cudaMemcpyAsync(X, scratch, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+  return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, best_c);
+}
+
+}  // namespace nb200

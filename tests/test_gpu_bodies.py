@@ -126,3 +126,28 @@ def test_requests_with_device_rhs_match_host_rhs():
         for g, r in zip(got, ref):
             assert g.shape == r.shape
             assert np.abs(g - r).max() <= tol * np.abs(r).max()
+
+
+@pytest.mark.parametrize("mode", [nb.FP64, nb.MIXED], ids=["fp64", "mixed"])
+def test_graph_replay_matches_direct_launches(mode):
+    """Graph mode: the first batch runs its launches directly, the second
+    identical batch is captured into a CUDA graph and the later ones replay
+    it; every call gives the direct path's forces (1e-12 of the largest force
+    in FP64, 1e-10 in mixed precision, where the refinement's last bits
+    differ)."""
+    B.build()
+    cases = _bodies()
+    body, omega = _items(cases, seed=5, n=10)
+    nvels = [_rhs(cases[b], w) for b, w in zip(body, omega)]
+    with nb.Solver(0, mode) as s:
+        for c in cases:
+            s.add_body(c)
+        ref = s.solve_bodies(body, omega, nvels)
+        s.set_graphs(True)
+        runs = [s.solve_bodies(body, omega, nvels) for _ in range(4)]
+        cap, rep = s.graph_stats()
+    assert cap >= 1 and rep >= 2, (cap, rep)
+    tol = 1e-12 if mode == nb.FP64 else 1e-10
+    for got in runs:
+        for g, r in zip(got, ref):
+            assert np.abs(g - r).max() <= tol * np.abs(r).max()
