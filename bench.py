@@ -52,6 +52,31 @@ def build_workload(n_omega=None):
     return case, nvel, nds
 
 
+ASM_PROFILE = "profiles/assembly_counters_barge_4omega.md"
+
+
+def assembly_counters():
+    """Per-pair counts of the assembly passes from the committed ncu summary:
+    the line `counters:` holds key=value pairs (FP64 FLOP executed per (I, J)
+    pair and frequency by each pass and depth regime, DRAM bytes per pair of
+    both passes together). None when the summary is absent."""
+    p = os.path.join(ROOT, ASM_PROFILE)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("counters:"):
+            return {k: float(v) for k, v in (kv.split("=") for kv in line.split()[1:])}
+    return None
+
+
+def fp64_peak_tflops(device):
+    import nemoh_b200 as nb
+    L = nb.load_library()
+    L.nemoh_b200_diag_fp64_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    v = ctypes.c_double()
+    return v.value if L.nemoh_b200_diag_fp64_peak(int(device), ctypes.byref(v)) == 0 else None
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -310,10 +335,25 @@ def run_batched(local, n_bodies, n_omega=20, seed=4, steps=2):
                 res = s.solve_bodies(items_b, items_w, items_v)
             dt = (time.perf_counter() - t0) / steps
             t = s.last_timings()
+            # the same calls replayed as CUDA graphs: the first call in graph
+            # mode runs directly, the second is captured, later ones replay
+            s.set_graphs(True)
+            for _ in range(2):
+                s.solve_bodies(items_b, items_w, items_v)
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                rg = s.solve_bodies(items_b, items_w, items_v)
+            dtg = (time.perf_counter() - t0) / steps
+            cap, rep = s.graph_stats()
         F[label] = [np.stack(res[b * n_omega:(b + 1) * n_omega], axis=2) for b in range(n_bodies)]
         out[label + "_solves_per_s"] = n_bodies * n_omega / dt
         out[label + "_s"] = dt
-        out[label + "_phase_ms"] = {"assemble": t["assemble_ms"], "factor": t["factor_ms"], "solve": t["solve_ms"]}
+        out[label + "_phase_ms"] = {"assemble": t["assemble_ms"], "factor_solve": t["factor_ms"], "lu": t["lu_ms"],
+                                    "solve": t["solve_ms"]}
+        out[label + "_graph_solves_per_s"] = n_bodies * n_omega / dtg
+        out[label + "_graph"] = {"captured": cap, "replayed": rep,
+                                 "max_diff_vs_direct": float(max(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+                                                                 for a, b in zip(rg, res)))}
     errs = [rel_err_families(a, b, 1)[0] for a, b in zip(F["mixed"], F["fp64"])]
     npan = [c.mesh.npanels for c in cases]
     out.update({"bodies": n_bodies, "omegas_per_body": n_omega, "solves": n_bodies * n_omega, "steps": steps,
@@ -322,6 +362,59 @@ def run_batched(local, n_bodies, n_omega=20, seed=4, steps=2):
                 "mixed_speedup": out["fp64_s"] / out["mixed_s"], "mixed_vs_fp64_max_rel_err": float(max(errs)),
                 "path": "nemoh_b200_solve_bodies: all bodies and frequencies in one call, ragged batches",
                 "timing": "host wall clock per call, host<->device copies included"})
+    return out
+
+
+def run_two_spheres(local, n_omega=30):
+    """Precision workload: two floating spheres R=4 m, centres 20 m apart, deep
+    water, 8,000 quad panels (quadrangulated icospheres, seed 3), 12 DOF + 2
+    headings, 30 frequencies 0.2..3.0 rad/s: one step = the 30 solves through
+    nemoh_b200_solve_frequencies_device (inputs resident on the device), FP64
+    and mixed precision, CUDA events; the mixed result's error against FP64
+    per coefficient."""
+    import torch
+    import nemoh_b200 as nb
+    from nemoh_b200 import cases as C
+    case = C.config_two_spheres(n_omega=n_omega)
+    nvel_h, nds_h = _body_inputs(case)
+    nc, nrhs, nw = nvel_h.shape
+    nint = nds_h.shape[0]
+    dev = torch.device("cuda", local)
+    nvel_d = torch.from_numpy(np.ascontiguousarray(nvel_h.transpose(2, 1, 0)).view(np.float64)).to(dev)
+    nds_d = torch.from_numpy(np.ascontiguousarray(nds_h.T)).to(dev)
+    force_d = torch.zeros((nw, nrhs, nint, 2), dtype=torch.float64, device=dev)
+    out, F = {"n_panels": case.mesh.npanels, "omegas": nw, "problems_per_omega": nrhs}, {}
+    om = case.omegas.astype(np.float64)
+    for label, mode in (("fp64", nb.FP64), ("mixed", nb.MIXED)):
+        with nb.Solver(local, mode) as s:
+            s.set_case(case)
+            s.solve_frequencies_device(om[:2], nvel_d.data_ptr(), nrhs, nint, nds_d.data_ptr(),
+                                       force_d.data_ptr())   # warm-up: workspace, kernel attributes, tuning
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            s.solve_frequencies_device(om, nvel_d.data_ptr(), nrhs, nint, nds_d.data_ptr(), force_d.data_ptr())
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1)
+            t = s.last_timings()
+            Fh = force_d.cpu().numpy()
+            F[label] = (Fh[..., 0] + 1j * Fh[..., 1]).transpose(2, 1, 0)
+            out[label] = {"solves_per_s": nw / (ms / 1e3), "ms_per_step": ms,
+                          "phase_ms": {"assemble": t["assemble_ms"], "factor_solve": t["factor_ms"],
+                                       "lu": t["lu_ms"], "solve": t["solve_ms"]}}
+            if mode == nb.MIXED:
+                out[label]["refinement"] = dict(zip(("iterations", "residual"), s.last_refinement()))
+    N = case.mesh.npanels
+    err_max, err_med = rel_err_families(F["mixed"], F["fp64"], len(case.betas_deg))
+    lu_flop = 8.0 / 3.0 * N ** 3 * nw
+    out.update({"mixed_speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+                "mixed_vs_fp64_max_rel_err": err_max, "mixed_vs_fp64_median_rel_err": err_med,
+                "lu_effective_tflops": {k: lu_flop / (out[k]["phase_ms"]["lu"] / 1e3) / 1e12
+                                        for k in ("fp64", "mixed") if out[k]["phase_ms"]["lu"] > 0},
+                "mesh": "icosphere frequency 12 cut 0.055 R below the centre, 3 quads per triangle, 4,000 per "
+                        "sphere, node jitter: areas within 10%, seed 3",
+                "timing": "CUDA events around one 30-frequency call, inputs on the device"})
     return out
 
 
@@ -485,7 +578,7 @@ def run_ours(args):
             s.solve_frequencies_device(omegas, nvel_d.data_ptr(), nrhs, nint, nds_d.data_ptr(), force_d.data_ptr())
         barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        phase = np.zeros(3)
+        phase = np.zeros(4)
         l0 = s.launches
         with ClockSampler(local) as clk:
             barrier()
@@ -494,7 +587,7 @@ def run_ours(args):
                 s.solve_frequencies_device(omegas, nvel_d.data_ptr(), nrhs, nint, nds_d.data_ptr(),
                                            force_d.data_ptr())
                 t = s.last_timings()
-                phase += [t["assemble_ms"], t["factor_ms"], t["solve_ms"]]
+                phase += [t["assemble_ms"], t["factor_ms"], t["solve_ms"], t["lu_ms"]]
             ev1.record()
             barrier()
         launches = s.launches - l0
@@ -538,16 +631,29 @@ def run_ours(args):
     # functions). Algorithmic bytes = the influence matrices written, 4 x 16 N^2
     # per frequency, plus the FP32 copy of D+ and D- (2 x 8 N^2) that the wave
     # pass writes for the mixed LU, over the assembly phase's CUDA-event time.
-    # DRAM traffic per frequency from the ncu capture of the same passes (the
-    # Rankine pass writes the matrices, the wave pass reads and rewrites them):
-    # 1.101 GB finite depth, 1.114 GB deep water at N=2400, plus the FP32 copy.
+    # The binding roof is the FP64 pipe: FP64 operations per pair as counted
+    # by ncu on the current kernels (committed summary), over the same time,
+    # against the FP64 FMA throughput measured here.
     N = case.mesh.npanels
     asm_ms = mx["phase"][0]
     asm_bytes = (4 * 16.0 + 2 * 8.0) * N * N * nomega
     achieved = asm_bytes / (asm_ms / 1e3) / 1e9
     kw = case.omegas ** 2 / case.g
     n_fd = int((~((case.depth == 0.0) | (kw * case.depth >= 20))).sum())
-    traffic = (1.101e9 * n_fd + 1.114e9 * (nomega - n_fd)) * (N / 2400.0) ** 2 + 2 * 8.0 * N * N * nomega
+    cnt = assembly_counters()
+    fp64_peak = fp64_peak_tflops(local)
+    fp64 = {"peak_tflops": fp64_peak,
+            "peak_source": "measured in this run (nemoh_b200_diag_fp64_peak: FMA chains on every SM)"}
+    traffic = None
+    if cnt:
+        pairs = N * N
+        flop = pairs * (n_fd * (cnt["rankine_fd_flop"] + cnt["wave_fd_flop"]) +
+                        (nomega - n_fd) * (cnt["rankine_deep_flop"] + cnt["wave_deep_flop"]))
+        traffic = pairs * (n_fd * cnt["fd_dram_bytes"] + (nomega - n_fd) * cnt["deep_dram_bytes"]) / nomega
+        ach = flop / (asm_ms / 1e3) / 1e12
+        fp64.update({"achieved_tflops": ach, "frac": ach / fp64_peak if fp64_peak else None,
+                     "flop_source": "FP64 instructions (DFMA x2, DADD, DMUL) per pair executed by the current "
+                                    "kernels, ncu, " + ASM_PROFILE})
     line = {
         "metric": "BEM solves/s (mixed vs FP64 GPU, rel err<=1e-6) at N=2400; serve p50/p99 ms",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -557,20 +663,20 @@ def run_ours(args):
                    "n_panels": N, "omegas": nomega, "problems_per_omega": NPROB, "precision": "mixed",
                    "l2": "working set 15 GB of matrices per step, larger than L2 (no flush needed)"},
         "fp64": {"value": whole_job_rate(world, nomega, f64["ms"]), "unit": "solves/s", "ms_per_step": f64["ms"],
-                 "phase_ms": {"assemble": f64["phase"][0], "factor": f64["phase"][1], "solve": f64["phase"][2]}},
+                 "phase_ms": {"assemble": f64["phase"][0], "factor_solve": f64["phase"][1], "lu": f64["phase"][3],
+                              "solve": f64["phase"][2]}},
         "mixed_vs_fp64": {"max_rel_err": err_max, "median_rel_err": err_med, "speedup": f64["ms"] / mx["ms"]},
-        "phase_ms": {"assemble": mx["phase"][0], "factor_refine": mx["phase"][1], "solve": mx["phase"][2]},
+        "phase_ms": {"assemble": mx["phase"][0], "factor_refine": mx["phase"][1], "lu": mx["phase"][3],
+                     "solve": mx["phase"][2]},
         "roofline": {"bound": "hbm",
                      "kernel": "rankine_kernel + wave_sym_kernel (influence-matrix assembly, FP64)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": src,
-                     "traffic": traffic / nomega, "traffic_unit": "DRAM bytes per frequency (ncu)",
+                     "traffic": traffic,
+                     "traffic_unit": ("DRAM bytes per frequency (ncu counts per pair, " + ASM_PROFILE + ")")
+                     if traffic else None,
                      "algorithmic_bytes_per_frequency": 80.0 * N * N,
-                     "fp64": {"note": "the assembly is FP64-pipe and latency bound, not HBM bound",
-                              "fp64_pipe_active_ncu": {"rankine_kernel<1>": 0.325, "wave_sym_kernel<1>": 0.339,
-                                                       "rankine_kernel<0>": 0.295, "wave_sym_kernel<0>": 0.152}},
-                     "lu_tc": {"kernel": "tc_update_kernel (mixed LU outer update, K=128)", "bound": "hbm",
-                               "frac_ncu": 0.53, "tensor_pipe_active_ncu": 0.34,
-                               "traffic_equals_algorithmic": True}},
+                     "binding": "FP64 pipe: the HBM fraction is low because the passes are not HBM bound",
+                     "fp64": fp64},
         "e2e": {"value": whole_job_rate(world, nomega, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(pin_nvel.numel() * 8 + pin_nds.numel() * 8),
                 "d2h_bytes_per_step": int(pin_force.numel() * 8)},
@@ -589,8 +695,11 @@ def run_ours(args):
     results = {}
     if single_gpu_extras(rank, world) and not args.no_extras:
         for key, fn in (("outputs", lambda: run_outputs(local)),
+                        ("two_spheres", lambda: run_two_spheres(local)),
                         ("batched", lambda: run_batched(local, args.bodies)),
                         ("serve", lambda: run_serving(local, args.bodies, args.requests))):
+            if key not in args.extras.split(","):
+                continue
             try:
                 line[key] = fn()
             except Exception as e:   # reported in the line; the headline stands on its own
@@ -612,7 +721,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=16.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--omegas", type=int, default=N_OMEGA, help="frequency subset (profiling only)")
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving workloads")
+    ap.add_argument("--no-extras", action="store_true", help="skip the workloads beside the headline")
+    ap.add_argument("--extras", default="outputs,two_spheres,batched,serve",
+                    help="comma list of the workloads beside the headline to run")
     ap.add_argument("--bodies", type=int, default=256, help="bodies of the batched and serving workloads")
     ap.add_argument("--requests", type=int, default=10000, help="requests per serving rate")
     args = ap.parse_args()

@@ -234,6 +234,9 @@ int nemoh_b200_get_tables(nemoh_ctx* ctx, double* xr, double* xz, double* apd);
 int nemoh_b200_get_geometry(nemoh_ctx* ctx, double* out, double* zer);
 /* timing of the last solve_frequencies call: assembly, factorization, solve+potential+forces (ms) */
 int nemoh_b200_last_timings(nemoh_ctx* ctx, double* assemble_ms, double* factor_ms, double* solve_ms);
+/* the factorization alone within factor_ms (the rest of factor_ms is the
+ * triangular solves, and in mixed precision the refinement) */
+int nemoh_b200_last_factor_ms(nemoh_ctx* ctx, double* lu_ms);
 /* mixed precision: refinement iterations and final max relative residual of the
  * last solve; iterations = -1 when the refinement did not reach 1e-12 (FP32
  * factors too inaccurate, e.g. near an irregular frequency) and that batch was

@@ -24,6 +24,9 @@ int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5);
  * the cluster size chosen for a batch of nsys systems of order n with nrhs
  * right-hand sides in single (1) or double (0) precision (0 if not tuned) */
 int nemoh_b200_diag_sweep_tuning(long long* keys_tuned, int n, int nsys, int nrhs, int single, int* cluster_size);
+/* measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
+ * best of four launches of independent FMA chains on every SM */
+int nemoh_b200_diag_fp64_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -70,6 +70,7 @@ def load_library():
     L.nemoh_b200_get_tables.argtypes = [_vp, _d, _d, _d]
     L.nemoh_b200_get_geometry.argtypes = [_vp, _d, _d]
     L.nemoh_b200_last_timings.argtypes = [_vp, _d, _d, _d]
+    L.nemoh_b200_last_factor_ms.argtypes = [_vp, _d]
     L.nemoh_b200_last_refinement.argtypes = [_vp, _i, _d]
     L.nemoh_b200_launch_count.argtypes = [_vp]
     L.nemoh_b200_body_conditions.argtypes = [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int,
@@ -298,9 +299,11 @@ class Solver:
             _vp(stream)))
 
     def last_timings(self):
-        a, f, s = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-        load_library().nemoh_b200_last_timings(self._h, ctypes.byref(a), ctypes.byref(f), ctypes.byref(s))
-        return dict(assemble_ms=a.value, factor_ms=f.value, solve_ms=s.value)
+        a, f, s, lu = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        L = load_library()
+        L.nemoh_b200_last_timings(self._h, ctypes.byref(a), ctypes.byref(f), ctypes.byref(s))
+        L.nemoh_b200_last_factor_ms(self._h, ctypes.byref(lu))
+        return dict(assemble_ms=a.value, factor_ms=f.value, solve_ms=s.value, lu_ms=lu.value)
 
     def last_refinement(self):
         it, res = ctypes.c_int(), ctypes.c_double()

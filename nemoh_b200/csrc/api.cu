@@ -133,8 +133,10 @@ struct nemoh_ctx {
   double w_previous = -1.;   // factor cache key of solve_problem
   int cached_fd = 0, cached_nexp = 0;
   bool lu64 = false;         // d_D holds FP64 LU factors (FP64 mode, or a mixed-mode fallback)
-  float t_asm = 0, t_fac = 0, t_sol = 0;
+  float t_asm = 0, t_fac = 0, t_sol = 0, t_lu = 0;   // t_lu: the factorization alone, within t_fac
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_lu[2] = {nullptr, nullptr};
+  bool lu_timed = false;
   // resident bodies and the descriptions of the current ragged batch
   std::vector<std::unique_ptr<BodyState>> bodies;
   DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce, d_reqs;
@@ -516,15 +518,28 @@ void mixed_solve(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
 
 void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs, const Shape& sh) {
   c->lu64 = c->mode == NEMOH_B200_FP64;
+  CK(cudaEventRecord(c->ev_lu[0], c->stream));
   if (c->mode == NEMOH_B200_MIXED) {
     mixed_factor(c->mixed, c->d_D.as<double2>(), sh.n, nsys, c->d_status.as<int>(), c->stream, c->launches,
                  &c->lanes, /*have_f32=*/true, sh.rg);
     CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev_lu[1], c->stream));
     if (have_rhs) mixed_solve(c, nsys, nrhs, sh);
   } else {
     factor_fp64(c, nsys, sh);
+    CK(cudaEventRecord(c->ev_lu[1], c->stream));
     if (have_rhs) trsm_fp64(c, nsys, nrhs, sh);
   }
+  c->lu_timed = true;
+}
+
+// adds the factorization's share of the last factor_and_solve (after a sync)
+void add_lu_time(nemoh_ctx* c) {
+  if (!c->lu_timed) return;
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev_lu[0], c->ev_lu[1]));
+  c->t_lu += ms;
+  c->lu_timed = false;
 }
 
 void potential(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
@@ -547,7 +562,7 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
   const int N = c->nfa, cls = ncls(c);
   const int cap = batch_capacity(c, nrhs, nomega);
   ensure_batch(c, cap, nrhs);
-  c->t_asm = c->t_fac = c->t_sol = 0;
+  c->t_asm = c->t_fac = c->t_sol = c->t_lu = 0;
   for (int w0 = 0; w0 < nomega; w0 += cap) {
     const int nw = std::min(cap, nomega - w0);
     // host setup of each frequency (in the caller's order, which the NQ state
@@ -585,6 +600,7 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
     c->t_asm += a;
     c->t_fac += f;
     c->t_sol += s;
+    add_lu_time(c);
   }
   c->w_previous = -1.;  // the batch reused the cached-factor slot
 }
@@ -720,6 +736,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
     c->t_asm += a;
     c->t_fac += f;
     c->t_sol += s;
+    add_lu_time(c);
     return;
   }
   // Graph mode: every host setup and upload first, then one launch sequence
@@ -852,7 +869,7 @@ void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* o
     const long long v = std::atoll(e);
     if (v > 0) budget = std::min(budget, (size_t)v);
   }
-  c->t_asm = c->t_fac = c->t_sol = 0;
+  c->t_asm = c->t_fac = c->t_sol = c->t_lu = 0;
   int pos = 0;
   while (pos < nitem) {
     const int nmax = c->bodies[body[idx[pos]]]->nfa;
@@ -900,6 +917,7 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
   int st = guarded(c, [&] {
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) CK(cudaEventCreate(&e));
+    for (auto& e : c->ev_lu) CK(cudaEventCreate(&e));
     for (int g = 0; g < LANES; ++g) {
       CK(cudaStreamCreateWithFlags(&c->lanes.s[g], cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&c->lanes.join[g], cudaEventDisableTiming));
@@ -972,6 +990,8 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
   for (GraphEntry& g : c->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->ev_lu)
     if (e) cudaEventDestroy(e);
   for (int g = 0; g < LANES; ++g) {
     if (c->lanes.join[g]) cudaEventDestroy(c->lanes.join[g]);
@@ -1578,6 +1598,12 @@ int nemoh_b200_last_timings(nemoh_ctx* c, double* a, double* f, double* s) {
   return NEMOH_B200_OK;
 }
 
+int nemoh_b200_last_factor_ms(nemoh_ctx* c, double* lu_ms) {
+  if (!c || !lu_ms) return NEMOH_B200_EINVAL;
+  *lu_ms = c->t_lu;
+  return NEMOH_B200_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1618,6 +1644,68 @@ int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5) {
     ki5[k] = t.ki5[k];
   }
   return 0;
+}
+
+}  // extern "C"
+
+// FP64 FMA throughput of the device: every thread runs eight independent FMA
+// chains (enough to cover the pipe's latency with eight CTAs of 256 threads
+// per SM), iters steps each; 2 FLOP per FMA.
+__global__ void __launch_bounds__(256) dfma_peak_kernel(double* out, int iters, double b, double c) {
+  double a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = (threadIdx.x + j) * 1e-9;
+#pragma unroll 1
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = fma(a[j], b, c);
+  double s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += a[j];
+  if (s == 12345.678) out[0] = s;   // keeps the chains live; never true for these inputs
+}
+
+extern "C" {
+
+int nemoh_b200_diag_fp64_peak(int device, double* tflops) {
+  if (!tflops) return NEMOH_B200_EINVAL;
+  *tflops = 0;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  int sms = 0;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return NEMOH_B200_ECUDA;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double* out = nullptr;
+  int rc = NEMOH_B200_OK;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess || cudaMalloc(&out, sizeof(double)) != cudaSuccess) {
+    rc = NEMOH_B200_ECUDA;
+  } else {
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    double best = 0;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(e0, st);
+      dfma_peak_kernel<<<blocks, threads, 0, st>>>(out, iters, 1.0000001, 1e-7);
+      cudaEventRecord(e1, st);
+      float ms = 0;
+      if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess || ms <= 0) {
+        rc = NEMOH_B200_ECUDA;
+        break;
+      }
+      const double flop = 2.0 * 8.0 * iters * (double)blocks * threads;
+      best = std::max(best, flop / (ms * 1e-3) / 1e12);
+    }
+    *tflops = best;
+  }
+  if (out) cudaFree(out);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  if (prev >= 0) cudaSetDevice(prev);
+  return rc;
 }
 
 int nemoh_b200_diag_sweep_tuning(long long* keys_tuned, int n, int nsys, int nrhs, int single, int* cluster_size) {

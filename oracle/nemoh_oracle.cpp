@@ -2805,8 +2805,11 @@ int nemoh_oracle_gaussz_inverse(int n, const double* a, double* ainv) {
 #ifdef NEMOH_ORACLE_MAIN
 int main(int argc, char** argv) {
   const char* root = argc > 1 ? argv[1] : "";
+  // "faithful": the reference's loop structure (Green functions recomputed
+  // for every problem's potential); otherwise the single-layer matrix is kept
+  const bool faithful = argc > 2 && std::string(argv[2]) == "faithful";
   double secs = 0;
-  int st = nemoh_oracle_run_case(root, 1, &secs);
+  int st = nemoh_oracle_run_case(root, faithful ? 0 : 1, &secs);
   if (st) {
     std::fprintf(stderr, "nemoh_oracle: error %d: %s\n", st, nemoh_oracle_last_error());
     return st;
