@@ -242,6 +242,11 @@ int nemoh_b200_last_factor_ms(nemoh_ctx* ctx, double* lu_ms);
  * factors too inaccurate, e.g. near an irregular frequency) and that batch was
  * factored and solved again in FP64 on the device */
 int nemoh_b200_last_refinement(nemoh_ctx* ctx, int* iterations, double* residual);
+/* mixed precision: batches that needed the FP64 fallback since the context was
+ * created, and the systems re-solved there (a batch of several bodies
+ * re-solves only its systems that missed the tolerance; systems counts only
+ * those partial fallbacks) */
+int nemoh_b200_fallback_count(const nemoh_ctx* ctx, long long* batches, long long* systems);
 /* number of CUDA kernel launches issued by this context since creation */
 long long nemoh_b200_launch_count(const nemoh_ctx* ctx);
 

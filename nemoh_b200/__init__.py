@@ -71,6 +71,7 @@ def load_library():
     L.nemoh_b200_get_geometry.argtypes = [_vp, _d, _d]
     L.nemoh_b200_last_timings.argtypes = [_vp, _d, _d, _d]
     L.nemoh_b200_last_factor_ms.argtypes = [_vp, _d]
+    L.nemoh_b200_fallback_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.nemoh_b200_last_refinement.argtypes = [_vp, _i, _d]
     L.nemoh_b200_launch_count.argtypes = [_vp]
     L.nemoh_b200_body_conditions.argtypes = [_vp, _i, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int,
@@ -241,6 +242,8 @@ class Solver:
         omegas = np.ascontiguousarray(omegas, dtype=np.float64)
         nrhs = nvels[0].shape[1]
         for b, v in zip(bodies, nvels):
+            if not 0 <= b < len(getattr(self, "_bodies", ())):
+                raise NemohError(1, "unknown body %d" % b)
             if v.shape != (self._bodies[b][0], nrhs):
                 raise ValueError("right-hand sides of body %d: expected %s, got %s" % (b, (self._bodies[b][0], nrhs),
                                                                                     v.shape))
@@ -304,6 +307,12 @@ class Solver:
         L.nemoh_b200_last_timings(self._h, ctypes.byref(a), ctypes.byref(f), ctypes.byref(s))
         L.nemoh_b200_last_factor_ms(self._h, ctypes.byref(lu))
         return dict(assemble_ms=a.value, factor_ms=f.value, solve_ms=s.value, lu_ms=lu.value)
+
+    def fallback_count(self):
+        """(batches that fell back to FP64 factors, systems re-solved in partial fallbacks)"""
+        nb_, ns = ctypes.c_longlong(), ctypes.c_longlong()
+        load_library().nemoh_b200_fallback_count(self._h, ctypes.byref(nb_), ctypes.byref(ns))
+        return nb_.value, ns.value
 
     def last_refinement(self):
         it, res = ctypes.c_int(), ctypes.c_double()

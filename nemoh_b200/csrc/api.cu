@@ -140,6 +140,8 @@ struct nemoh_ctx {
   // resident bodies and the descriptions of the current ragged batch
   std::vector<std::unique_ptr<BodyState>> bodies;
   DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce, d_reqs;
+  DevBuf d_froff, d_frord, d_fx, d_fy;   // partial FP64 fallback of a ragged batch
+  long long fallback_systems = 0;         // systems re-solved with FP64 factors so far
   HostBuf h_rag, h_reqs;
   // CUDA graphs of cross-body batches (nemoh_b200_set_graphs)
   bool graph_mode = false;
@@ -507,13 +509,72 @@ void mixed_fallback(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
   ++w.fallbacks;
 }
 
+// Ragged batches (many bodies): only the systems whose refinement missed the
+// tolerance are factored again in FP64 (their matrices are still in d_D; the
+// FP32 LU worked on its copy) and solved from their kept right-hand sides;
+// the others keep their refined solutions.
+void mixed_fallback_ragged(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
+  MixedWork& w = c->mixed;
+  const int nv = nsys * nrhs;
+  std::vector<unsigned long long> h(2 * (size_t)nv);
+  CK(cudaMemcpyAsync(h.data(), w.norms, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<int> bad;
+  for (int s = 0; s < nsys; ++s) {
+    bool fail = false;
+    for (int p = 0; p < nrhs; ++p) {
+      double rn, bn;
+      std::memcpy(&rn, &h[(size_t)s * nrhs + p], 8);
+      std::memcpy(&bn, &h[(size_t)nv + (size_t)s * nrhs + p], 8);
+      const double r = bn > 0 ? rn / bn : rn;
+      fail = fail || !(r <= REFINE_TOL);
+    }
+    if (fail) bad.push_back(s);
+  }
+  if (bad.empty() || (int)bad.size() == nsys) {
+    mixed_fallback(c, nsys, nrhs, sh);
+    return;
+  }
+  const int nf = (int)bad.size();
+  std::vector<long long> off_f(nf);
+  std::vector<int> ord_f(nf);
+  for (int j = 0; j < nf; ++j) {
+    off_f[j] = sh.rg.host_off[bad[j]];
+    ord_f[j] = sh.rg.host_ord[bad[j]];
+  }
+  const size_t N = sh.n, xs = N * nrhs, xf = (size_t)ord_f[0] * nrhs;
+  CK(c->d_froff.ensure(nf * sizeof(long long)));
+  CK(c->d_frord.ensure(nf * sizeof(int)));
+  CK(c->d_fx.ensure((size_t)nf * xf * sizeof(double2)));
+  CK(c->d_fy.ensure((size_t)nf * xf * sizeof(double2)));
+  CK(c->d_inv.ensure((size_t)nf * ((ord_f[0] + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
+  CK(cudaMemcpyAsync(c->d_froff.p, off_f.data(), nf * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_frord.p, ord_f.data(), nf * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  double2* fx = c->d_fx.as<double2>();
+  double2* X = c->d_X.as<double2>();
+  for (int j = 0; j < nf; ++j)   // a system's right-hand sides: ord x nrhs, contiguous
+    CK(cudaMemcpyAsync(fx + j * xf, w.b + bad[j] * xs, (size_t)ord_f[j] * nrhs * sizeof(double2),
+                       cudaMemcpyDeviceToDevice, c->stream));
+  const Shape shf{ord_f[0], Ragged{c->d_froff.as<long long>(), c->d_frord.as<int>(), ord_f.data(), off_f.data()}};
+  factor_fp64(c, nf, shf);
+  CK(trsm_sweep_tuned<double2>(dbatch(c, shf), c->d_inv.as<double2>(), fx, c->d_fy.as<double2>(), nf, nrhs,
+                               c->stream, c->launches));
+  for (int j = 0; j < nf; ++j)
+    CK(cudaMemcpyAsync(X + bad[j] * xs, fx + j * xf, (size_t)ord_f[j] * nrhs * sizeof(double2),
+                       cudaMemcpyDeviceToDevice, c->stream));
+  w.last_iterations = -1;
+  w.fallbacks += 1;
+  c->fallback_systems += nf;
+}
+
 void mixed_solve(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
   MixedWork& w = c->mixed;
   mixed_solve_refine(w, c->d_D.as<double2>(), sh.n, nsys, c->d_X.as<double2>(), c->d_Y.as<double2>(), nrhs,
                      c->stream, c->launches, sh.rg);
   CK(cudaGetLastError());
   if (w.last_residual <= REFINE_TOL) return;
-  mixed_fallback(c, nsys, nrhs, sh);
+  if (sh.rg.host_off) mixed_fallback_ragged(c, nsys, nrhs, sh);
+  else mixed_fallback(c, nsys, nrhs, sh);
 }
 
 void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs, const Shape& sh) {
@@ -691,7 +752,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   c->cap_nfa = -1;
   c->w_previous = -1.;
   const long long xs = (long long)N * nrhs;
-  const Shape sh{nmax, Ragged{c->d_roff.as<long long>(), c->d_rord.as<int>(), ord.data()}};
+  const Shape sh{nmax, Ragged{c->d_roff.as<long long>(), c->d_rord.as<int>(), ord.data(), off.data()}};
   OmegaParams* hom = c->h_oms.as<OmegaParams>();
   auto host_setup = [&](int j) {
     BodyState& b = *c->bodies[body[items[j]]];
@@ -828,7 +889,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
       redo = true;
     }
     if (c->mixed.last_residual > REFINE_TOL) {
-      mixed_fallback(c, nsys, nrhs, sh);
+      mixed_fallback_ragged(c, nsys, nrhs, sh);
       redo = true;
     }
     if (redo) {
@@ -1595,6 +1656,13 @@ int nemoh_b200_last_timings(nemoh_ctx* c, double* a, double* f, double* s) {
   if (a) *a = c->t_asm;
   if (f) *f = c->t_fac;
   if (s) *s = c->t_sol;
+  return NEMOH_B200_OK;
+}
+
+int nemoh_b200_fallback_count(const nemoh_ctx* c, long long* batches, long long* systems) {
+  if (!c) return NEMOH_B200_EINVAL;
+  if (batches) *batches = c->mixed.fallbacks;
+  if (systems) *systems = c->fallback_systems;
   return NEMOH_B200_OK;
 }
 

@@ -51,6 +51,7 @@ struct Ragged {
   const long long* off = nullptr;
   const int* ord = nullptr;
   const int* host_ord = nullptr;
+  const long long* host_off = nullptr;   // host copy of off
 };
 template <class C2>
 inline BatchT<C2> make_batch(C2* base, int n, C2* diag, C2* pinv, const Ragged& rg) {

@@ -63,22 +63,36 @@ def decode_forces(case, F):
     return out
 
 
-def coef_err(a, b, nbeta, floor=1e-6, per_coef=False):
+def coef_err(a, b, nbeta, floor=1e-6, per_coef=False, vanish_floor=None):
     """Per-coefficient error of forces a against b, both (nint, nprob, nw):
     |a - b| / max(|b|, floor * family max), a family being one force component
     and one problem over all frequencies (force(i, p) over omega); the first
     nbeta problems are diffraction, the rest radiation. A family whose largest
     value is at most 1e-9 of the largest coefficient of its kind vanishes by the
     body's symmetry (both sides hold round-off there) and is measured against
-    `floor` times that kind maximum. Returns the maximum (or the array)."""
+    `vanish_floor` (default `floor`) times that kind maximum. Returns the
+    maximum (or the array)."""
     mag = np.abs(b)
     fam = mag.max(axis=2, keepdims=True)
     kind = np.empty_like(fam)
     kind[:, :nbeta] = mag[:, :nbeta].max() if nbeta else 0.0
     kind[:, nbeta:] = mag[:, nbeta:].max() if nbeta < mag.shape[1] else 0.0
-    den = np.where(fam <= 1e-9 * kind, floor * kind, np.maximum(mag, floor * fam))
+    vf = floor if vanish_floor is None else vanish_floor
+    den = np.where(fam <= 1e-9 * kind, vf * kind, np.maximum(mag, floor * fam))
     err = np.abs(a - b) / np.maximum(den, 1e-300)
     return err if per_coef else float(err.max())
+
+
+PARITY_TOL = 1e-9
+
+
+def parity_err(a, b, nbeta):
+    """The FP64 parity metric: coef_err per coefficient with the benchmark's
+    floor of 1e-6 of the family maximum; families that vanish by symmetry hold
+    only round-off on both sides and are measured against 1e-3 of their kind's
+    largest coefficient, so that PARITY_TOL bounds their absolute difference
+    by 1e-12 of that maximum."""
+    return coef_err(a, b, nbeta, floor=1e-6, vanish_floor=1e-3)
 
 
 def rel_err(a, b):

@@ -30,7 +30,7 @@ from nemoh_b200 import cases as C
 pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-COEF_TOL = 1e-9
+COEF_TOL = G.PARITY_TOL
 SIGMA_TOL = 1e-10
 
 
@@ -63,7 +63,7 @@ def test_barge_2400_forces_per_coefficient(solver):
     solver.set_case(case)
     nvel, nds, npb = G.problems(case)
     F = solver.solve_frequencies(case.omegas, nvel, nds)
-    err = G.coef_err(F, Fo, len(case.betas_deg))
+    err = G.parity_err(F, Fo, len(case.betas_deg))
     assert err < COEF_TOL, err
 
 
@@ -89,5 +89,5 @@ def test_cylinder_all_ten_frequencies_per_coefficient(solver, tmp_path):
     nvel, nds, npb = G.problems(case)
     F = solver.solve_frequencies(case.omegas, nvel, nds)
     Fo = G.oracle_forces(case, str(tmp_path))
-    err = G.coef_err(F, Fo, len(case.betas_deg))
+    err = G.parity_err(F, Fo, len(case.betas_deg))
     assert err < COEF_TOL, err

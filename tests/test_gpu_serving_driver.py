@@ -46,7 +46,7 @@ def test_dropin_driver_matches_oracle(tmp_path):
     subprocess.run([exe, str(tmp_path / "gpu")], check=True)
     F = np.loadtxt(str(tmp_path / "gpu" / "case" / "results" / "Forces.dat"), ndmin=2)
     got = G.decode_forces(case, F)
-    assert G.rel_err(got, ref) < 1e-9
+    assert G.parity_err(got, ref, len(case.betas_deg)) < G.PARITY_TOL
 
 
 def _kochin_files(d, nprob):
