@@ -929,7 +929,8 @@ constexpr int sweep_smem() {
 }
 
 template <class C2, int NR, bool LOWER>
-__global__ void __launch_bounds__(SW_THREADS) trsm_sweep_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk,
+__global__ void __launch_bounds__(SW_THREADS, sizeof(C2) == sizeof(float2) ? 2 : 1)
+    trsm_sweep_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk,
                                                                 C2* xbase, C2* ybase, long long xstride,
                                                                 const int* active) {
   namespace cg = cooperative_groups;
@@ -999,15 +1000,19 @@ __global__ void __launch_bounds__(SW_THREADS) trsm_sweep_kernel(BatchT<C2> b, co
       C2 acc[NR];
 #pragma unroll
       for (int p = 0; p < NR; ++p) acc[p] = mkc<C2>(0., 0.);
-      C2 a[8];
+      // the row's columns of block s are loaded 32 (FP32; two CTAs of 256
+      // threads fit an SM) or 16 (FP64) at a time before any is used, so a
+      // thread keeps that many loads in flight
+      constexpr int PF = sizeof(C2) == sizeof(float2) ? 32 : 16;
+      C2 a[PF];
 #pragma unroll 1
-      for (int c8 = 0; c8 < nb; c8 += 8) {
+      for (int c0 = 0; c0 < nb; c0 += PF) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a[j] = (c8 + j < nb) ? Ar[(long long)n * (c8 + j)] : mkc<C2>(0., 0.);
+        for (int j = 0; j < PF; ++j) a[j] = (c0 + j < nb) ? Ar[(long long)n * (c0 + j)] : mkc<C2>(0., 0.);
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
+        for (int j = 0; j < PF; ++j)
 #pragma unroll
-          for (int p = 0; p < NR; ++p) cmac(acc[p], a[j], yloc[(c8 + j) + TB * p]);
+          for (int p = 0; p < NR; ++p) cmac(acc[p], a[j], yloc[(c0 + j) + TB * p]);
       }
 #pragma unroll
       for (int p = 0; p < NR; ++p) {

@@ -384,6 +384,220 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form of the same update: one CTA per SM walks the tiles of the
+// launch (tile t, t + grid, ...) with three roles, so that one tile's
+// read-modify-write of A22 runs while the next tile's MMAs do:
+//   warp 0 (one thread)  streams operand chunks into TCP_STAGES shared-memory
+//                        stages (bulk async copies, full/empty mbarriers);
+//   warp 1 (one thread)  issues the MMAs of a tile into one of two 256-column
+//                        TMEM accumulators (512 columns in all) and commits the
+//                        finished accumulator to acc_full[buf];
+//   warps 2-5            read the accumulator (each warp the TMEM lane quarter
+//                        it may access, warp % 4), release it on acc_empty[buf]
+//                        and subtract it from A22.
+// Every mbarrier wait is bounded; a role that times out raises the status,
+// flags the others through shared memory, and each role waits (bounded) for
+// the copies or MMAs it has in flight before the CTA frees its tensor memory.
+// ---------------------------------------------------------------------------
+constexpr int TCP_STAGES = 4;
+constexpr int TCP_THREADS = 192;
+constexpr int TCP_SMEM = TCP_STAGES * TC_STAGE + 256;
+
+__global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
+    BatchT<float2> b, int k0, const unsigned char* __restrict__ abuf, const unsigned char* __restrict__ bbuf,
+    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TCP_STAGES * TC_STAGE);
+  // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the TMEM address
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * TCP_STAGES + 4);
+  __shared__ volatile int s_err;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[TCP_STAGES]);
+  const uint32_t accf0 = smem_u32(&bars[2 * TCP_STAGES]), acce0 = smem_u32(&bars[2 * TCP_STAGES + 2]);
+  const int r1 = k0 + LU_OUTER;
+  const long long total = (long long)nt * nt * nsys;
+  // tile t: system z, row tile trow, column tile tcol; false beyond a ragged system's order
+  auto tile = [&](long long t, int& z, int& trow, int& tcol) {
+    z = (int)(t / ((long long)nt * nt));
+    const int rem = (int)(t % ((long long)nt * nt));
+    trow = rem / nt;
+    tcol = rem % nt;
+    const int rest = b.order(z) - r1;
+    return rest > 0 && trow * TC_T < rest && tcol * TC_T < rest;
+  };
+  if (threadIdx.x == 0) {
+    s_err = 0;
+    for (int i = 0; i < TCP_STAGES; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * i));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * i));
+    }
+    for (int i = 0; i < 2; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(accf0 + 8 * i));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(acce0 + 8 * i));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  auto fail = [&] {
+    atomicCAS(status, 0, ST_TC_TIMEOUT);
+    s_err = 1;
+  };
+
+  if (warp == 0 && lane == 0) {
+    // producer
+    const uint32_t s0 = smem_u32(smem);
+    long long g = 0;   // chunks issued
+    bool ok = true;
+    for (long long t = blockIdx.x; t < total && ok && !s_err; t += gridDim.x) {
+      int z, trow, tcol;
+      if (!tile(t, z, trow, tcol)) continue;
+      const unsigned char* ga = abuf + z * sys_bytes_a + (long long)trow * TC_NCH * 2 * TC_AIMG;
+      const unsigned char* gb = bbuf + z * sys_bytes_b + (long long)tcol * TC_NCH * 2 * TC_BIMG;
+      for (int c = 0; c < TC_NCH; ++c) {
+        const int q = (int)(g % TCP_STAGES);
+        const long long r = g / TCP_STAGES;
+        if (r > 0 && !(ok = mbar_wait(empty0 + 8 * q, (uint32_t)((r - 1) & 1)))) break;
+        tc_load_chunk(s0 + q * TC_STAGE, ga + (long long)c * 2 * TC_AIMG, gb + (long long)c * 2 * TC_BIMG,
+                      full0 + 8 * q);
+        ++g;
+      }
+    }
+    if (!ok) fail();
+    // copies in flight land before the CTA can leave: the last round of each stage
+    for (long long h = g - 1; h >= 0 && h >= g - TCP_STAGES; --h)
+      mbar_wait(full0 + 8 * (int)(h % TCP_STAGES), (uint32_t)((h / TCP_STAGES) & 1));
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t s0 = smem_u32(smem);
+    long long g = 0, i = 0;   // chunks consumed, tiles done
+    bool ok = true;
+    for (long long t = blockIdx.x; t < total && ok && !s_err; t += gridDim.x) {
+      int z, trow, tcol;
+      if (!tile(t, z, trow, tcol)) continue;
+      const int buf = (int)(i & 1);
+      const long long u = i >> 1;
+      if (u > 0 && !(ok = mbar_wait(acce0 + 8 * buf, (uint32_t)((u - 1) & 1)))) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tm = tmem + (uint32_t)(buf * TC_TMEM_COLS);
+      for (int c = 0; c < TC_NCH; ++c) {
+        const int q = (int)(g % TCP_STAGES);
+        if (!(ok = mbar_wait(full0 + 8 * q, (uint32_t)((g / TCP_STAGES) & 1)))) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = s0 + q * TC_STAGE;
+        const uint32_t ahi = st, alo = st + TC_AIMG, bhi = st + 2 * TC_AIMG, blo = bhi + TC_BIMG;
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+          const uint32_t o = kk * 256;
+          tc_mma(tm, umma_desc(ahi + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), (c > 0 || kk > 0) ? 1u : 0u);
+          tc_mma(tm, umma_desc(ahi + o, 128, TC_SBO), umma_desc(blo + o, 128, TC_SBO), 1u);
+          tc_mma(tm, umma_desc(alo + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         empty0 + 8 * q)
+                     : "memory");
+        ++g;
+      }
+      if (!ok) break;
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(accf0 + 8 * buf)
+                   : "memory");
+      ++i;
+    }
+    if (!ok) fail();
+    // the MMAs issued last have completed before the tensor memory is freed
+    if (g > 0) mbar_wait(empty0 + 8 * (int)((g - 1) % TCP_STAGES), (uint32_t)(((g - 1) / TCP_STAGES) & 1));
+  } else if (warp >= 2) {
+    // epilogue: thread = accumulator row (TMEM lane), warp w reads lanes 32 (w % 4) ..
+    // (every lane waits on the barrier and the warp goes on only if all did:
+    // the tcgen05.ld below must be executed by every lane of a warp)
+    const int lq = warp & 3;
+    const int row = lq * 32 + lane;
+    long long i = 0;
+    bool ok = true;
+    for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+      if (__shfl_sync(0xffffffffu, s_err, 0)) break;
+      int z, trow, tcol;
+      if (!tile(t, z, trow, tcol)) continue;
+      const int buf = (int)(i & 1);
+      const bool got = mbar_wait(accf0 + 8 * buf, (uint32_t)((i >> 1) & 1));
+      if (!(ok = __all_sync(0xffffffffu, got))) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int n = b.order(z), rest = n - r1;
+      const int gr = r1 + trow * TC_T + row;
+      float2* A = b.sys(z);
+      const int cbase = r1 + tcol * TC_T;
+      const int ncol = min(TC_T, rest - tcol * TC_T);
+#pragma unroll 1
+      for (int q = 0; q < TC_T / 32; ++q) {
+        uint32_t vr[32], vi[32];
+        const uint32_t ta = tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(buf * TC_TMEM_COLS + 32 * q);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]), "=r"(vr[7]),
+              "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]), "=r"(vr[14]),
+              "=r"(vr[15]), "=r"(vr[16]), "=r"(vr[17]), "=r"(vr[18]), "=r"(vr[19]), "=r"(vr[20]), "=r"(vr[21]),
+              "=r"(vr[22]), "=r"(vr[23]), "=r"(vr[24]), "=r"(vr[25]), "=r"(vr[26]), "=r"(vr[27]), "=r"(vr[28]),
+              "=r"(vr[29]), "=r"(vr[30]), "=r"(vr[31])
+            : "r"(ta));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]), "=r"(vi[7]),
+              "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]), "=r"(vi[14]),
+              "=r"(vi[15]), "=r"(vi[16]), "=r"(vi[17]), "=r"(vi[18]), "=r"(vi[19]), "=r"(vi[20]), "=r"(vi[21]),
+              "=r"(vi[22]), "=r"(vi[23]), "=r"(vi[24]), "=r"(vi[25]), "=r"(vi[26]), "=r"(vi[27]), "=r"(vi[28]),
+              "=r"(vi[29]), "=r"(vi[30]), "=r"(vi[31])
+            : "r"(ta + (uint32_t)TC_T));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (q == TC_T / 32 - 1) {   // every column of the accumulator is in registers: release it
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce0 + 8 * buf) : "memory");
+        }
+        if (gr < n && 32 * q < ncol) {
+          float2 cur[32];
+          float2* p = A + gr + (long long)n * (cbase + 32 * q);
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (32 * q + j < ncol) cur[j] = p[(long long)n * j];
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (32 * q + j < ncol) {
+              float2 v = cur[j];
+              v.x -= __uint_as_float(vr[j]);
+              v.y -= __uint_as_float(vi[j]);
+              p[(long long)n * j] = v;
+            }
+        }
+      }
+      ++i;
+    }
+    if (!ok) fail();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_TMEM_COLS));
+}
+
+// NEMOH_B200_TC_PERSISTENT=1 selects the persistent form of the update
+inline bool tc_persistent() {
+  static const bool on = [] {
+    const char* e = std::getenv("NEMOH_B200_TC_PERSISTENT");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 // NEMOH_B200_TC=0 selects the CUDA-core FP32 update instead (for comparison)
 inline bool tc_enabled() {
   static const bool on = [] {
@@ -409,7 +623,21 @@ inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_
   const int per = (nt * TC_T * TC_NCH + 127) / 128;
   tc_prep_kernel<<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
   ++launches;
-  tc_update_kernel<<<dim3(nt, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status);
+  if (tc_persistent()) {
+    static std::atomic<unsigned long long> attr2{0};
+    static int sms = 0;
+    once_per_device(attr2, [] {
+      cudaFuncSetAttribute(tc_update_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TCP_SMEM);
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    });
+    const long long tiles = (long long)nt * nt * nsys;
+    const int grid = (int)std::min<long long>(tiles, sms > 0 ? sms : 148);
+    tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, nt, nsys, status);
+  } else {
+    tc_update_kernel<<<dim3(nt, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status);
+  }
   ++launches;
   return true;
 }

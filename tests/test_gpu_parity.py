@@ -344,6 +344,43 @@ def test_mixed_fallback_to_fp64_factors(tmp_path):
     assert float(line[1]) < 1e-10 and int(line[3]) == -1, line
 
 
+def test_persistent_tensor_core_update(tmp_path):
+    """The persistent form of the tensor-core trailing update
+    (NEMOH_B200_TC_PERSISTENT=1, read once per process, hence a child
+    process): the mixed path through it matches FP64 within 1e-6 per
+    coefficient on orders with one and with several outer updates (the
+    cylinder of 300 panels, a hemisphere of 640), single and batched systems,
+    with the refinement converging as with the other form."""
+    import subprocess
+    import sys
+    script = tmp_path / "persistent.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        "sys.path[:0] = %r\n"
+        "import gpu_cases as G, nemoh_b200 as nb\n"
+        "from nemoh_b200 import cases as C\n"
+        "cyl = C.config_cylinder(n_omega=3)\n"
+        "sph = C.Case(C.hemisphere_mesh(3.0, 16, 40, jitter=0.2, rng=np.random.default_rng(7)),\n"
+        "             np.array([0.5, 1.1, 1.7]), np.array([0.0]), C.six_dofs(), C.six_dofs(), depth=0.0)\n"
+        "for case in (cyl, sph):\n"
+        "    nvel, nds, npb = G.problems(case)\n"
+        "    out = {}\n"
+        "    for mode in (nb.FP64, nb.MIXED):\n"
+        "        with nb.Solver(0, mode) as s:\n"
+        "            s.set_case(case)\n"
+        "            out[mode] = s.solve_frequencies(case.omegas, nvel, nds)\n"
+        "            it = s.last_refinement()[0]\n"
+        "    print('ERR', case.mesh.npanels, G.coef_err(out[nb.MIXED], out[nb.FP64], 1), 'IT', it)\n"
+        % [str(p) for p in (B.HERE + "/..", B.HERE + "/../tests")])
+    env = dict(os.environ, NEMOH_B200_TC_PERSISTENT="1")
+    r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l.split() for l in r.stdout.splitlines() if l.startswith("ERR")]
+    assert len(lines) == 2, r.stdout
+    for line in lines:
+        assert float(line[2]) < 1e-6 and 0 < int(line[4]) <= 6, line
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_kochin_matches_oracle(solver, case):
     """COMPUTE_KOCHIN on the GPU vs the oracle, on the same source strengths:
