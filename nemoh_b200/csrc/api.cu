@@ -1920,7 +1920,7 @@ extern "C" int nemoh_b200_factor_solve_device_noalloc(int device, int n, int nsy
   for (int k = 0; k < n; k += LU_NB) {
     const int nb = std::min(LU_NB, n - k), rest = n - k - nb;
     const int nrb = (rest + LU_RB - 1) / LU_RB, ncb = (rest + LU_CB - 1) / LU_CB;
-    lu_diag_kernel<double2><<<dim3(1, 1, nsys), LU_NB * LU_NB, 0, st>>>(b, k, status);
+    lu_diag_kernel<double2><<<dim3(1, 1, nsys), LU_DIAG_THREADS, 0, st>>>(b, k, status);
     lu_panel_kernel<double2><<<dim3(std::max(1, nrb + ncb), 1, nsys), LU_RB, 0, st>>>(b, k, n);
     if (rest > 0) zgemm_update<double2>(b, k, nb, Rect{k + nb, n, k + nb, n}, nsys, st);
   }

@@ -93,60 +93,77 @@ __device__ __forceinline__ double cabs2(float2 a) { return hypotf(a.x, a.y); }
 
 // Factor the diagonal block A11 of step k once per system (grid.z = system)
 // and invert its triangles. Scratch per system: [LU(A11) | inv(L11) | inv(U11)],
-// column-major nb x nb each (ld = nb). One thread per element of the 32 x 32
-// block, every step of the three eliminations separated by a barrier:
+// column-major nb x nb each (ld = nb). 128 threads: lane i holds row i, warp
+// w the columns c = w mod 4, so every column belongs to one warp:
 //  * unpivoted Doolittle (GAUSSZ's elimination on this block): at step j the
-//    column below the pivot is divided by it, then the trailing block takes
-//    the rank-1 update;
+//    owner of column j divides it below the pivot, one block barrier, then
+//    every warp applies the rank-1 update to its columns right of j (the
+//    owner of column j+1 has then finished it, so the next step needs no
+//    second barrier);
 //  * inv(L): X = I, step j (ascending) subtracts L(i, j) X(j, :) from the rows
 //    below, the order of the column-by-column forward substitution;
 //  * inv(U): X = I, step j (descending) divides row j by U(j, j) and
-//    subtracts U(i, j) X(j, :) from the rows above.
-// With b.pinv (two-level LU) inv(L) also goes to the slot of this block in the
-// current outer panel.
+//    subtracts U(i, j) X(j, :) from the rows above;
+//    a column of either inverse depends only on itself and the factored block,
+//    so each warp inverts its columns with warp-level synchronisation only.
+// Every element sees the same operations in the same order as a sequential
+// elimination. With b.pinv (two-level LU) inv(L) also goes to the slot of this
+// block in the current outer panel.
+constexpr int LU_DIAG_THREADS = 128;
 template <class C2>
-__global__ void __launch_bounds__(1024) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
+__global__ void __launch_bounds__(LU_DIAG_THREADS) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
   __shared__ C2 sb[LU_NB * LU_NB];   // the block, column-major, ld = nb
   __shared__ C2 xl[LU_NB * LU_NB];   // inv(L11), ld = LU_NB
   __shared__ C2 xu[LU_NB * LU_NB];   // inv(U11), ld = LU_NB
+  constexpr int NW = LU_DIAG_THREADS / 32;
   const int n = b.order(blockIdx.z);
   if (k >= n) return;
   const int nb = min(LU_NB, n - k);
-  const int i = threadIdx.x & (LU_NB - 1), c = threadIdx.x / LU_NB;
-  const bool in = i < nb && c < nb;
+  const int i = threadIdx.x & 31, w = threadIdx.x >> 5;
   const C2* A = b.sys(blockIdx.z);
-  if (in) sb[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
+  for (int c = w; c < nb; c += NW)
+    if (i < nb) sb[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
-    if (threadIdx.x == 0 && !(cabs2(sb[j + nb * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-    if (in && c == j && i > j) sb[i + nb * j] = cdv(sb[i + nb * j], sb[j + nb * j]);
+    if (w == (j % NW)) {
+      if (i == 0 && !(cabs2(sb[j + nb * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+      if (i > j && i < nb) sb[i + nb * j] = cdv(sb[i + nb * j], sb[j + nb * j]);
+    }
     __syncthreads();
-    if (in && i > j && c > j) sb[i + nb * c] = cfms(sb[i + nb * c], sb[i + nb * j], sb[j + nb * c]);
-    __syncthreads();
-  }
-  const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
-  if (in) {
-    xl[i + LU_NB * c] = i == c ? one : zero;
-    xu[i + LU_NB * c] = i == c ? one : zero;
+    if (i > j && i < nb)
+      for (int c = w; c < nb; c += NW)
+        if (c > j) sb[i + nb * c] = cfms(sb[i + nb * c], sb[i + nb * j], sb[j + nb * c]);
   }
   __syncthreads();
+  const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
+  for (int c = w; c < nb; c += NW)
+    if (i < nb) {
+      xl[i + LU_NB * c] = i == c ? one : zero;
+      xu[i + LU_NB * c] = i == c ? one : zero;
+    }
+  __syncwarp();
   for (int step = 0; step < nb; ++step) {
     const int jl = step, ju = nb - 1 - step;
-    if (in && i == ju && c >= ju) xu[ju + LU_NB * c] = cdv(xu[ju + LU_NB * c], sb[ju + nb * ju]);
-    __syncthreads();
-    if (in && i > jl && c <= jl) xl[i + LU_NB * c] = cfms(xl[i + LU_NB * c], sb[i + nb * jl], xl[jl + LU_NB * c]);
-    if (in && i < ju && c >= ju) xu[i + LU_NB * c] = cfms(xu[i + LU_NB * c], sb[i + nb * ju], xu[ju + LU_NB * c]);
-    __syncthreads();
+    if (i == ju)
+      for (int c = w; c < nb; c += NW)
+        if (c >= ju) xu[ju + LU_NB * c] = cdv(xu[ju + LU_NB * c], sb[ju + nb * ju]);
+    __syncwarp();
+    for (int c = w; c < nb; c += NW) {
+      if (i < nb && i > jl && c <= jl) xl[i + LU_NB * c] = cfms(xl[i + LU_NB * c], sb[i + nb * jl], xl[jl + LU_NB * c]);
+      if (i < ju && c >= ju) xu[i + LU_NB * c] = cfms(xu[i + LU_NB * c], sb[i + nb * ju], xu[ju + LU_NB * c]);
+    }
+    __syncwarp();
   }
   C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   C2* P = b.pinv ? b.pinv + (long long)blockIdx.z * PINV_SCRATCH + ((k % LU_OUTER) / LU_NB) * LU_NB * LU_NB : nullptr;
-  if (in) {
-    const int q = i + nb * c;
-    D[q] = sb[q];
-    D[LU_NB * LU_NB + q] = xl[i + LU_NB * c];
-    D[2 * LU_NB * LU_NB + q] = xu[i + LU_NB * c];
-    if (P) P[q] = xl[i + LU_NB * c];
-  }
+  for (int c = w; c < nb; c += NW)
+    if (i < nb) {
+      const int q = i + nb * c;
+      D[q] = sb[q];
+      D[LU_NB * LU_NB + q] = xl[i + LU_NB * c];
+      D[2 * LU_NB * LU_NB + q] = xu[i + LU_NB * c];
+      if (P) P[q] = xl[i + LU_NB * c];
+    }
 }
 
 // acc += a b as four fused multiply-adds into the accumulator (written out:
@@ -526,7 +543,7 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
         BatchT<C2> bg = sub_batch(b, s0);
         bg.n = ng;
         const cudaStream_t st = L.st[g];
-        lu_diag_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, 0, st>>>(bg, k, status);
+        lu_diag_kernel<C2><<<dim3(1, 1, ns), LU_DIAG_THREADS, 0, st>>>(bg, k, status);
         ++launches;
         lu_panel_kernel<C2><<<dim3(std::max(1, nrb + ncb_used), 1, ns), LU_RB, 0, st>>>(bg, k, ucol);
         ++launches;

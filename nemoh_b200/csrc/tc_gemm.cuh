@@ -589,11 +589,12 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_TMEM_COLS));
 }
 
-// NEMOH_B200_TC_PERSISTENT=1 selects the persistent form of the update
+// the persistent form of the update is the default; NEMOH_B200_TC_PERSISTENT=0
+// selects the one-tile-per-CTA form (for comparison)
 inline bool tc_persistent() {
   static const bool on = [] {
     const char* e = std::getenv("NEMOH_B200_TC_PERSISTENT");
-    return e && e[0] == '1';
+    return !(e && e[0] == '0');
   }();
   return on;
 }

@@ -344,13 +344,13 @@ def test_mixed_fallback_to_fp64_factors(tmp_path):
     assert float(line[1]) < 1e-10 and int(line[3]) == -1, line
 
 
-def test_persistent_tensor_core_update(tmp_path):
-    """The persistent form of the tensor-core trailing update
-    (NEMOH_B200_TC_PERSISTENT=1, read once per process, hence a child
-    process): the mixed path through it matches FP64 within 1e-6 per
-    coefficient on orders with one and with several outer updates (the
-    cylinder of 300 panels, a hemisphere of 640), single and batched systems,
-    with the refinement converging as with the other form."""
+def test_one_tile_per_cta_tensor_core_update(tmp_path):
+    """The one-tile-per-CTA form of the tensor-core trailing update (the other
+    tests run the default persistent form; NEMOH_B200_TC_PERSISTENT=0 is read
+    once per process, hence a child process): the mixed path through it
+    matches FP64 within 1e-6 per coefficient on orders with one and with
+    several outer updates (the cylinder of 300 panels, a hemisphere of 640),
+    with the refinement converging."""
     import subprocess
     import sys
     script = tmp_path / "persistent.py"
@@ -372,7 +372,7 @@ def test_persistent_tensor_core_update(tmp_path):
         "            it = s.last_refinement()[0]\n"
         "    print('ERR', case.mesh.npanels, G.coef_err(out[nb.MIXED], out[nb.FP64], 1), 'IT', it)\n"
         % [str(p) for p in (B.HERE + "/..", B.HERE + "/../tests")])
-    env = dict(os.environ, NEMOH_B200_TC_PERSISTENT="1")
+    env = dict(os.environ, NEMOH_B200_TC_PERSISTENT="0")
     r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l.split() for l in r.stdout.splitlines() if l.startswith("ERR")]
