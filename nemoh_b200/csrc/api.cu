@@ -98,6 +98,10 @@ struct BodyState {
   int nq_state = 0;
   int ndof = 0;   // radiation DOFs of serving requests (nemoh_b200_set_body_dofs)
   DevBuf d_xyz, d_m, d_rec, d_rows, d_nds, d_dofs;
+  // frequency-independent Rankine part per depth regime (0 deep water, 1
+  // finite depth), kept with the resident body once evaluated
+  DevBuf rk[2];
+  bool rk_valid[2] = {false, false};
 };
 
 // a launch sequence seen before (key of its shapes and buffers) and, from its
@@ -132,6 +136,11 @@ struct nemoh_ctx {
   int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
   double w_previous = -1.;   // factor cache key of solve_problem
   int cached_fd = 0, cached_nexp = 0;
+  // Rankine part of the current mesh per depth regime; valid until the mesh
+  // changes, re-evaluated at the start of every multi-frequency call
+  DevBuf d_rk[2];
+  bool rk_valid[2] = {false, false};
+  size_t rk_body_bytes = 0;   // Rankine caches held by resident bodies
   bool lu64 = false;         // d_D holds FP64 LU factors (FP64 mode, or a mixed-mode fallback)
   float t_asm = 0, t_fac = 0, t_sol = 0, t_lu = 0;   // t_lu: the factorization alone, within t_fac
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -222,6 +231,13 @@ struct Env {
 
 void omega_params_env(const Env& e, double W, OmegaParams& om, bool advance_nq);
 
+// depth regime of a frequency: finite depth unless the depth is infinite (0)
+// or K h >= 20 (Solver/Core/SOLVE_BEM.f90:66, the deep-water branch)
+bool finite_depth(const Env& e, double W) {
+  const double kwave = W * W / e.g;
+  return !((e.depth == 0.) || (kwave * e.depth >= 20));
+}
+
 void omega_params(nemoh_ctx* c, double W, OmegaParams& om, bool advance_nq) {
   omega_params_env(Env{c->g, c->depth, c->gm, &c->nq_state}, W, om, advance_nq);
 }
@@ -230,8 +246,7 @@ void omega_params_env(const Env& env, double W, OmegaParams& om, bool advance_nq
   std::memset(&om, 0, sizeof om);
   om.w = W;
   om.h = env.depth;
-  const double kwave = W * W / env.g;
-  const bool fd = !((env.depth == 0.) || (kwave * env.depth >= 20));
+  const bool fd = finite_depth(env, W);
   if (std::fabs(W) < 1.E-4) throw Fail{NEMOH_B200_EOMEGA, "ABS(WR) < 1.E-4"};
   double qq[MAX_NQ + 2], cq[MAX_NQ + 2];
   if (!fd) {
@@ -325,6 +340,11 @@ int batch_capacity(nemoh_ctx* c, int nrhs, int want) {
   // existing buffers count as available
   size_t have = c->d_D.bytes + c->d_S.bytes + c->d_X.bytes + c->d_Y.bytes + c->d_inv.bytes + c->mixed.bytes();
   size_t budget = (size_t)((fr + have) * 0.8);
+  // room for the Rankine caches of both depth regimes that are not allocated yet
+  for (int r = 0; r < 2; ++r) {
+    const size_t need = cls * N * N * sizeof(double2);
+    if (c->d_rk[r].bytes < need) budget -= std::min(budget, need);
+  }
   int cap = (int)std::max<size_t>(1, budget / per);
   return std::min(cap, want);
 }
@@ -377,10 +397,12 @@ GreenCtx green_ctx(nemoh_ctx* c) {
 // launch shape of each depth regime.
 struct AsmGroup {
   int s0, s1, ninfd, nfd, n_infd, n_fd;
+  bool slot_rk_infd = false, slot_rk_fd = false;   // ragged: a slot of the regime has no Rankine cache
 };
 
-// uploads the parameters and slot order of slots [s0, s1) (already in c->h_oms)
-AsmGroup assemble_upload(nemoh_ctx* c, int s0, int s1, const int* host_n) {
+// uploads the parameters and slot order of slots [s0, s1) (already in c->h_oms);
+// host_rk (ragged) flags the slots whose body has a Rankine cache
+AsmGroup assemble_upload(nemoh_ctx* c, int s0, int s1, const int* host_n, const char* host_rk = nullptr) {
   const int N = c->nfa;
   const OmegaParams* hom = c->h_oms.as<OmegaParams>();
   int* hs = c->h_slots.as<int>() + s0;
@@ -389,11 +411,13 @@ AsmGroup assemble_upload(nemoh_ctx* c, int s0, int s1, const int* host_n) {
     if (!hom[s].fd) {
       hs[ag.ninfd++] = s;
       ag.n_infd = std::max(ag.n_infd, host_n ? host_n[s] : N);
+      ag.slot_rk_infd |= !(host_rk && host_rk[s]);
     }
   for (int s = s0; s < s1; ++s)
     if (hom[s].fd) {
       hs[ag.ninfd + ag.nfd++] = s;
       ag.n_fd = std::max(ag.n_fd, host_n ? host_n[s] : N);
+      ag.slot_rk_fd |= !(host_rk && host_rk[s]);
     }
   CK(cudaMemcpyAsync(c->d_oms.as<OmegaParams>() + s0, hom + s0, (size_t)(s1 - s0) * sizeof(OmegaParams),
                      cudaMemcpyHostToDevice, c->stream));
@@ -404,11 +428,39 @@ AsmGroup assemble_upload(nemoh_ctx* c, int s0, int s1, const int* host_n) {
 
 void assemble_launch(nemoh_ctx* c, const AsmGroup& ag, const SlotMesh* dmesh);
 
-void assemble_range(nemoh_ctx* c, int s0, int s1, const SlotMesh* dmesh = nullptr, const int* host_n = nullptr) {
-  assemble_launch(c, assemble_upload(c, s0, s1, host_n), dmesh);
+void assemble_range(nemoh_ctx* c, int s0, int s1, const SlotMesh* dmesh = nullptr, const int* host_n = nullptr,
+                    const char* host_rk = nullptr) {
+  assemble_launch(c, assemble_upload(c, s0, s1, host_n, host_rk), dmesh);
 }
 
-// the Rankine and wave passes of one group (reads only device buffers)
+// The Rankine part of one mesh in one depth regime into buf (evaluated once,
+// then kept while `valid` holds); returns the cache.
+const double2* rankine_cache(nemoh_ctx* c, GreenCtx g, const PanelRec* rec, const double* rows, int n, int nsymy,
+                             double depth, bool fd, DevBuf& buf, bool& valid) {
+  if (valid) return buf.as<double2>();
+  const size_t nn = (size_t)n * n;
+  CK(buf.ensure((nsymy + 1) * nn * sizeof(double2)));
+  g.nsymy = nsymy;
+  const dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ);
+  if (fd)
+    rankine_cache_kernel<true><<<grid, ASM_ROWS, 0, c->stream>>>(g, 2. * depth, rec, rows, n, buf.as<double2>());
+  else
+    rankine_cache_kernel<false><<<grid, ASM_ROWS, 0, c->stream>>>(g, 0., rec, rows, n, buf.as<double2>());
+  LAUNCHED(c);
+  valid = true;
+  return buf.as<double2>();
+}
+
+// the current mesh's cache of one regime
+const double2* mesh_rankine(nemoh_ctx* c, bool fd) {
+  return rankine_cache(c, green_ctx(c), c->d_rec.as<PanelRec>(), c->d_rows.as<double>(), c->nfa, c->nsymy, c->depth,
+                       fd, c->d_rk[fd], c->rk_valid[fd]);
+}
+
+// The Rankine and wave passes of one group (reads only device buffers). The
+// current mesh reads its Rankine caches; a ragged group (dmesh) reads each
+// body's cache through its slot description, and runs the per-slot Rankine
+// pass only when a slot of the regime has none (ag.slot_rk_*).
 void assemble_launch(nemoh_ctx* c, const AsmGroup& ag, const SlotMesh* dmesh) {
   const int N = c->nfa, cls = ncls(c);
   const int s0 = ag.s0, ninfd = ag.ninfd, nfd = ag.nfd, n_infd = ag.n_infd, n_fd = ag.n_fd;
@@ -424,9 +476,13 @@ void assemble_launch(nemoh_ctx* c, const AsmGroup& ag, const SlotMesh* dmesh) {
   const int* ds = c->d_slots.as<int>() + s0;
   if (ninfd) {
     const int n = n_infd;
-    dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ, (unsigned)ninfd);
-    rankine_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, n, o, dmesh);
-    LAUNCHED(c);
+    if (!dmesh) {
+      o.rk = mesh_rankine(c, false);
+    } else if (ag.slot_rk_infd) {
+      dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ, (unsigned)ninfd);
+      rankine_kernel<false><<<grid, blk, 0, c->stream>>>(g, dom, ds, rec, rows, n, o, dmesh);
+      LAUNCHED(c);
+    }
     const unsigned wt = (n + WS_T - 1) / WS_T;
     wave_sym_kernel<false><<<dim3(wt * (wt + 1) / 2, 1, (unsigned)ninfd), WS_THREADS, 0, c->stream>>>(g, dom, ds, rec,
                                                                                                       n, o, dmesh);
@@ -434,9 +490,13 @@ void assemble_launch(nemoh_ctx* c, const AsmGroup& ag, const SlotMesh* dmesh) {
   }
   if (nfd) {
     const int n = n_fd;
-    dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
-    rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, n, o, dmesh);
-    LAUNCHED(c);
+    if (!dmesh) {
+      o.rk = mesh_rankine(c, true);
+    } else if (ag.slot_rk_fd) {
+      dim3 grid((n + ASM_ROWS - 1) / ASM_ROWS, (n + ASM_TJ - 1) / ASM_TJ, (unsigned)nfd);
+      rankine_kernel<true><<<grid, blk, 0, c->stream>>>(g, dom, ds + ninfd, rec, rows, n, o, dmesh);
+      LAUNCHED(c);
+    }
     const unsigned wt = (n + WS_T - 1) / WS_T;
     wave_sym_kernel<true><<<dim3(wt * (wt + 1) / 2, 1, (unsigned)nfd), WS_THREADS, 0, c->stream>>>(
         g, dom, ds + ninfd, rec, n, o, dmesh);
@@ -624,6 +684,8 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
   const int cap = batch_capacity(c, nrhs, nomega);
   ensure_batch(c, cap, nrhs);
   c->t_asm = c->t_fac = c->t_sol = c->t_lu = 0;
+  // a multi-frequency call evaluates the Rankine part once per depth regime it meets
+  c->rk_valid[0] = c->rk_valid[1] = false;
   for (int w0 = 0; w0 < nomega; w0 += cap) {
     const int nw = std::min(cap, nomega - w0);
     // host setup of each frequency (in the caller's order, which the NQ state
@@ -696,6 +758,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
                   const double2* nvel_d, double2* force_d) {
   std::vector<long long> off;
   std::vector<int> ord, host_n(k);
+  std::vector<char> has_rk(k);
   std::vector<SlotMesh> sm(k);
   std::vector<ItemDesc> it(k);
   long long mat = 0;
@@ -703,7 +766,10 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   for (int j = 0; j < k; ++j) {
     const int i = items[j];
     const BodyState& b = *c->bodies[body[i]];
-    sm[j] = SlotMesh{b.d_rec.as<PanelRec>(), b.d_rows.as<double>(), mat, b.nfa, b.nsymy, b.zer};
+    const bool fd = finite_depth(Env{b.g, b.depth, b.gm, nullptr}, 2. * kPI / (2. * kPI / omegas[i]));
+    has_rk[j] = b.rk_valid[fd];
+    sm[j] = SlotMesh{b.d_rec.as<PanelRec>(), b.d_rows.as<double>(), mat, b.nfa, b.nsymy, b.zer,
+                     has_rk[j] ? b.rk[fd].as<double2>() : nullptr};
     it[j] = ItemDesc{nvel_off[i], force_off[i], b.d_nds.as<double>(), b.rho, b.nfa, b.nsymy, (int)ord.size(), b.nint};
     host_n[j] = b.nfa;
     nint_max = std::max(nint_max, b.nint);
@@ -779,7 +845,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
     for (int j = 0; j < k; ++j) {
       host_setup(j);
       if (j + 1 == k || j + 1 - done >= ASM_GROUP) {
-        assemble_range(c, done, j + 1, c->d_smesh.as<SlotMesh>(), host_n.data());
+        assemble_range(c, done, j + 1, c->d_smesh.as<SlotMesh>(), host_n.data(), has_rk.data());
         done = j + 1;
       }
     }
@@ -808,7 +874,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   for (int j0 = 0; j0 < k; j0 += ASM_GROUP) {
     const int j1 = std::min(k, j0 + ASM_GROUP);
     for (int j = j0; j < j1; ++j) host_setup(j);
-    groups.push_back(assemble_upload(c, j0, j1, host_n.data()));
+    groups.push_back(assemble_upload(c, j0, j1, host_n.data(), has_rk.data()));
   }
   const bool mixed = c->mode == NEMOH_B200_MIXED;
   const int max_it = refine_max_it(), passes = mixed ? std::min(REFINE_CHUNK, max_it) : 0;
@@ -821,7 +887,8 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
                                 (long long)c->mixed.r, (long long)c->mixed.rf, (long long)c->mixed.yf,
                                 (long long)c->mixed.inv, (long long)c->mixed.pinv, (long long)c->mixed.norms,
                                 (long long)c->mixed.state, (long long)c->mixed.tc.a, (long long)c->mixed.tc.b};
-  for (const AsmGroup& g : groups) sig.insert(sig.end(), {g.ninfd, g.nfd, g.n_infd, g.n_fd});
+  for (const AsmGroup& g : groups)
+    sig.insert(sig.end(), {g.ninfd, g.nfd, g.n_infd, g.n_fd, (long long)g.slot_rk_infd, (long long)g.slot_rk_fd});
   sig.insert(sig.end(), ord.begin(), ord.end());
   unsigned long long key = 1469598103934665603ull;   // FNV-1a over the signature
   for (long long v : sig)
@@ -899,6 +966,29 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   }
 }
 
+// Rankine caches of the bodies and depth regimes a call needs, evaluated once
+// and kept with the resident body, while the bodies' caches stay within
+// NEMOH_B200_RANKINE_CACHE_BYTES (default: a quarter of the device memory);
+// a body beyond it gets the per-slot Rankine pass in every batch.
+void ensure_body_rankine(nemoh_ctx* c, int nitem, const int* body, const double* omegas) {
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  size_t cap = tot / 4;
+  if (const char* e = std::getenv("NEMOH_B200_RANKINE_CACHE_BYTES")) cap = (size_t)std::max(0LL, std::atoll(e));
+  for (int i = 0; i < nitem; ++i) {
+    BodyState& b = *c->bodies[body[i]];
+    const bool fd = finite_depth(Env{b.g, b.depth, b.gm, nullptr}, 2. * kPI / (2. * kPI / omegas[i]));
+    if (b.rk_valid[fd]) continue;
+    const size_t bytes = (size_t)(b.nsymy + 1) * b.nfa * b.nfa * sizeof(double2);
+    if (c->rk_body_bytes + bytes > cap) continue;
+    GreenCtx g = green_ctx(c);
+    g.zer = b.zer;
+    rankine_cache(c, g, b.d_rec.as<PanelRec>(), b.d_rows.as<double>(), b.nfa, b.nsymy, b.depth, fd, b.rk[fd],
+                  b.rk_valid[fd]);
+    c->rk_body_bytes += bytes;
+  }
+}
+
 void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* omegas, int nrhs,
                        const double2* nvel_d, double2* force_d) {
   if (nrhs < 1 || nrhs > MAX_RHS) throw Fail{NEMOH_B200_ECAPACITY, "nrhs must be in 1..16"};
@@ -931,6 +1021,12 @@ void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* o
     if (v > 0) budget = std::min(budget, (size_t)v);
   }
   c->t_asm = c->t_fac = c->t_sol = c->t_lu = 0;
+  ScopedEvent rk0, rk1;
+  CK(cudaEventCreate(&rk0.e));
+  CK(cudaEventCreate(&rk1.e));
+  CK(cudaEventRecord(rk0.e, c->stream));
+  ensure_body_rankine(c, nitem, body, omegas);
+  CK(cudaEventRecord(rk1.e, c->stream));
   int pos = 0;
   while (pos < nitem) {
     const int nmax = c->bodies[body[idx[pos]]]->nfa;
@@ -945,6 +1041,9 @@ void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* o
     ragged_batch(c, idx.data() + pos, end - pos, body, omegas, nrhs, nvel_off, force_off, nvel_d, force_d);
     pos = end;
   }
+  float ms = 0;   // the batches ended with a synchronisation
+  CK(cudaEventElapsedTime(&ms, rk0.e, rk1.e));
+  c->t_asm += ms;
 }
 
 }  // namespace
@@ -1082,6 +1181,7 @@ int nemoh_b200_set_mesh(nemoh_ctx* c, int np, int nfa, int nsymy, const double* 
     c->depth = depth;
     c->w_previous = -1.;
     c->nq_state = 0;
+    c->rk_valid[0] = c->rk_valid[1] = false;
     upload_geometry(c, np, nfa, c->nsymy, xyz, m1234, c->d_xyz, c->d_m, c->d_rec, c->d_rows, c->zer, c->gm);
   });
 }

@@ -125,20 +125,26 @@ __global__ void crek_kernel(const double* __restrict__ xr, const double* __restr
 }
 
 // ---------------------------------------------------------------------------
-// Influence-matrix assembly, two passes per frequency. Thread = collocation
-// row I, block = 128 rows; the block stages ASM_TJ source panels J in shared
-// memory and walks them. Output per frequency (column-major, leading
-// dimension N): D+ then D- in out.d, S+ then S- in out.s (nsymy=0: one D and
-// one S). Column-major writes by consecutive rows are coalesced 16-byte
-// stores.
-//   rankine_kernel: Rankine part (VAVINFD / VAVFD) -> real parts, imaginary = 0;
+// Influence-matrix assembly. Thread = collocation row I, block = 128 rows;
+// the block stages ASM_TJ source panels J in shared memory and walks them.
+// Output per frequency (column-major, leading dimension N): D+ then D- in
+// out.d, S+ then S- in out.s (nsymy=0: one D and one S). Column-major writes
+// by consecutive rows are coalesced 16-byte stores.
+//   rankine_cache_kernel: Rankine part (VAVINFD / VAVFD) of every pair. It
+//                   depends on the geometry and the depth regime only (the
+//                   seabed image at 2h in finite depth), not on the
+//                   frequency, so it is evaluated once per mesh and regime
+//                   into a real cache: (D+, S+) pairs, then (D-, S-).
+//   rankine_kernel: the same Rankine part per frequency slot, written to the
+//                   real parts (imaginary = 0) of the slot's matrices; used
+//                   for resident bodies whose cache does not fit.
 //   wave_sym_kernel: wave part (VNSINFD / VNSFD; in finite depth with the
-//                   exponential images) added to the real parts and written to
-//                   the imaginary parts; in mixed precision it also writes the
-//                   FP32 copy of D that the FP32 LU factors.
+//                   exponential images) added to the Rankine part (from the
+//                   cache, or from the real parts the per-slot pass wrote) and
+//                   written to both parts of the matrices; in mixed precision
+//                   it also writes the FP32 copy of D that the FP32 LU factors.
 // Splitting the pair evaluation keeps each kernel's registers and code small
-// enough for several CTAs per SM; the extra read of the matrices is 64 bytes
-// per pair and symmetry class pair.
+// enough for several CTAs per SM.
 // ---------------------------------------------------------------------------
 constexpr int ASM_ROWS = 128;
 constexpr int ASM_TJ = 32;
@@ -157,6 +163,7 @@ struct AsmOut {
   double2* s;           // S+ (and S-) likewise
   long long slot_stride;
   float2* d32 = nullptr;   // optional FP32 copy of the final D (same layout), for the mixed LU
+  const double2* rk = nullptr;   // Rankine cache of the launch's depth regime (null: read the real parts)
 };
 
 // Ragged batches (frequency slots of different bodies in one launch): the
@@ -169,6 +176,7 @@ struct SlotMesh {
   int n;
   int nsymy;
   double zer;
+  const double2* rk;   // the body's Rankine cache for the slot's depth regime, or null
 };
 
 __device__ __forceinline__ void stage_panels(const PanelRec* __restrict__ rec, int j0, int nj, PanelRec* sp) {
@@ -202,6 +210,7 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(Gre
     g.nsymy = m.nsymy;
     g.zer = m.zer;
     base = m.off;
+    if (m.rk) return;   // the wave pass reads this slot's Rankine part from its cache (whole CTA)
   }
   const int j0 = blockIdx.y * ASM_TJ;
   if (j0 >= N || (int)blockIdx.x * ASM_ROWS >= N) return;   // beyond a smaller slot's order (whole CTA)
@@ -228,6 +237,35 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_kernel(Gre
       od[NN + q] = make_double2(r.dm, 0.);
       os[NN + q] = make_double2(r.sm, 0.);
     }
+  }
+}
+
+// Rankine part of every pair of one mesh into its cache: rk[I + N J] =
+// (D+, S+) real parts, rk[N N + I + N J] = (D-, S-) when nsymy = 1. DH is
+// twice the depth in finite depth (seabed image), 0 in deep water.
+template <bool FD>
+__global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_cache_kernel(GreenCtx g, double DH,
+                                                                 const PanelRec* __restrict__ rec,
+                                                                 const double* __restrict__ rows, int N,
+                                                                 double2* __restrict__ rk) {
+  __shared__ PanelRec sp[ASM_TJ];
+  const int j0 = blockIdx.y * ASM_TJ;
+  const int nj = min(ASM_TJ, N - j0);
+  stage_panels(rec, j0, nj, sp);
+  __syncthreads();
+  const int I = blockIdx.x * ASM_ROWS + threadIdx.x;
+  if (I >= N) return;
+  const double XGI = rows[I], YGI = rows[N + I], ZGI = rows[2 * N + I];
+  const double XNI = rows[3 * N + I], YNI = rows[4 * N + I], ZNI = rows[5 * N + I];
+  const long long NN = (long long)N * N;
+#pragma unroll 1
+  for (int jj = 0; jj < nj; ++jj) {
+    const int J = j0 + jj;
+    RankineOut r;
+    rankine<FD>(g, DH, XGI, YGI, ZGI, I == J, sp[jj], r);
+    const long long q = I + (long long)N * J;
+    rk[q] = make_double2(r.VSXP * XNI + r.VSYP * YNI + r.VSZP * ZNI, r.FSP);
+    if (g.nsymy == 1) rk[NN + q] = make_double2(r.VSXM * XNI + r.VSYM * YNI + r.VSZM * ZNI, r.FSM);
   }
 }
 
@@ -331,6 +369,7 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
   __shared__ OmegaParams som;
   const int slot = slots[blockIdx.z];
   long long base = slot * out.slot_stride;
+  const double2* rk = out.rk;
   if (meshes) {
     const SlotMesh m = meshes[slot];
     rec = m.rec;
@@ -338,6 +377,7 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
     g.nsymy = m.nsymy;
     g.zer = m.zer;
     base = m.off;
+    rk = m.rk;
   }
   const int T = (N + WS_T - 1) / WS_T;
   if ((int)blockIdx.x >= T * (T + 1) / 2) return;   // beyond a smaller slot's tiles (whole CTA)
@@ -382,18 +422,22 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
   double2* od = out.d + base;
   double2* os = out.s + base;
   float2* o32 = out.d32 ? out.d32 + base : nullptr;
+  // Rankine real parts of entry o (within the slot) of the plus and minus classes
+  auto rankine_at = [&](long long o, int cls) {
+    if (rk) return rk[cls * NN + o];
+    return make_double2(od[cls * NN + o].x, os[cls * NN + o].x);
+  };
   auto add = [&](long long o, const PairOut& r) {
-    double2 d = od[o], sv = os[o];
-    const double2 dn = make_double2(d.x + r.dp_re, r.dp_im);
+    double2 rr = rankine_at(o, 0);
+    const double2 dn = make_double2(rr.x + r.dp_re, r.dp_im);
     od[o] = dn;
-    os[o] = make_double2(sv.x + r.sp_re, r.sp_im);
+    os[o] = make_double2(rr.y + r.sp_re, r.sp_im);
     if (o32) o32[o] = make_float2((float)dn.x, (float)dn.y);
     if (NJJ == 2) {
-      d = od[NN + o];
-      sv = os[NN + o];
-      const double2 dm = make_double2(d.x + r.dm_re, r.dm_im);
+      rr = rankine_at(o, 1);
+      const double2 dm = make_double2(rr.x + r.dm_re, r.dm_im);
       od[NN + o] = dm;
-      os[NN + o] = make_double2(sv.x + r.sm_re, r.sm_im);
+      os[NN + o] = make_double2(rr.y + r.sm_re, r.sm_im);
       if (o32) o32[NN + o] = make_float2((float)dm.x, (float)dm.y);
     }
   };

@@ -55,15 +55,18 @@ def _single(case, mode, omegas, nvels):
         return [s.solve_frequencies(np.array([w]), v[:, :, None], nds)[:, :, 0] for w, v in zip(omegas, nvels)]
 
 
-@pytest.mark.parametrize("budget", [None, 48 << 20], ids=["one_batch", "split_batches"])
-def test_bodies_match_single_body_path(budget):
+@pytest.mark.parametrize("env", [{}, {"NEMOH_B200_BATCH_BYTES": str(48 << 20)},
+                                 {"NEMOH_B200_RANKINE_CACHE_BYTES": "0"}],
+                         ids=["one_batch", "split_batches", "per_slot_rankine"])
+def test_bodies_match_single_body_path(env):
+    """The single-body path reads the mesh's Rankine cache; the bodies read
+    their own caches, or (cache budget 0) evaluate the Rankine part per slot."""
     B.build()
     cases = _bodies()
     body, omega = _items(cases)
     nvels = [_rhs(cases[b], w) for b, w in zip(body, omega)]
-    old = os.environ.get("NEMOH_B200_BATCH_BYTES")
-    if budget:
-        os.environ["NEMOH_B200_BATCH_BYTES"] = str(budget)
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         got = {}
         for mode in (nb.FP64, nb.MIXED):
@@ -72,11 +75,11 @@ def test_bodies_match_single_body_path(budget):
                 assert ids == list(range(len(cases)))
                 got[mode] = s.solve_bodies(body, omega, nvels)
     finally:
-        if budget:
-            if old is None:
-                del os.environ["NEMOH_B200_BATCH_BYTES"]
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
             else:
-                os.environ["NEMOH_B200_BATCH_BYTES"] = old
+                os.environ[k] = v
     for b in range(len(cases)):
         sel = [i for i in range(len(body)) if body[i] == b]
         ref64 = _single(cases[b], nb.FP64, omega[sel], [nvels[i] for i in sel])
