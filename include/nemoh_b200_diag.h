@@ -21,12 +21,18 @@ int nemoh_b200_diag_theta_quadrature(double akk, double* qq, double* cq);
  * double bit pattern with the host's log10 */
 int nemoh_b200_diag_stencil_thresholds(double* kj8, double* kj5, double* ki5);
 /* autotuner of the triangular sweep: keys tuned in this process so far, and
- * the cluster size chosen for a batch of nsys systems of order n with nrhs
- * right-hand sides in single (1) or double (0) precision (0 if not tuned) */
+ * the sweep chosen for a batch of nsys systems of order n with nrhs
+ * right-hand sides in single (1) or double (0) precision: the cluster size
+ * (1, 2, 4, 8) of the cluster sweep, 16 for the dataflow sweep, 0 if not
+ * tuned */
 int nemoh_b200_diag_sweep_tuning(long long* keys_tuned, int n, int nsys, int nrhs, int single, int* cluster_size);
 /* measured FP64 FMA throughput of a device (TFLOP/s, 2 FLOP per FMA): the
  * best of four launches of independent FMA chains on every SM */
 int nemoh_b200_diag_fp64_peak(int device, double* tflops);
+/* bounded-wait check of the dataflow sweep: a launch whose only item waits on
+ * a ready flag that nothing raises; returns the status word the kernel left
+ * (31 = the wait ran out) and the launch's duration */
+int nemoh_b200_diag_sweep_timeout(int device, int* status, double* ms);
 
 #ifdef __cplusplus
 }

@@ -463,3 +463,31 @@ def stencil_thresholds():
     a, b, c = np.zeros(48), np.zeros(48), np.zeros(48)
     load_library().nemoh_b200_diag_stencil_thresholds(_p(a), _p(b), _p(c))
     return a, b, c
+
+
+def sweep_timeout_check(device=0):
+    """Bounded-wait check of the dataflow triangular sweep: one launch whose
+    only item waits on a ready flag that nothing raises. Returns the status
+    word the kernel left (31: the wait ran out) and the launch's duration in
+    ms; the device stays usable."""
+    L = load_library()
+    L.nemoh_b200_diag_sweep_timeout.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_double)]
+    st, ms = ctypes.c_int(), ctypes.c_double()
+    rc = L.nemoh_b200_diag_sweep_timeout(int(device), ctypes.byref(st), ctypes.byref(ms))
+    if rc:
+        raise NemohError(rc, "sweep timeout check")
+    return st.value, ms.value
+
+
+def sweep_choice(n, nsys, nrhs, single):
+    """The sweep the autotuner chose for a batch shape (0: not tuned yet;
+    1, 2, 4, 8: cluster sweep with that cluster size; 16: dataflow sweep) and
+    the number of shapes tuned so far in this process."""
+    L = load_library()
+    L.nemoh_b200_diag_sweep_tuning.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    keys, cs = ctypes.c_longlong(), ctypes.c_int()
+    L.nemoh_b200_diag_sweep_tuning(ctypes.byref(keys), int(n), int(nsys), int(nrhs), int(bool(single)),
+                                   ctypes.byref(cs))
+    return cs.value, keys.value

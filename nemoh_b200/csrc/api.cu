@@ -150,6 +150,7 @@ struct nemoh_ctx {
   std::vector<std::unique_ptr<BodyState>> bodies;
   DevBuf d_roff, d_rord, d_smesh, d_items, d_bnvel, d_bforce, d_reqs;
   DevBuf d_froff, d_frord, d_fx, d_fy;   // partial FP64 fallback of a ragged batch
+  DevBuf d_flow;                         // workspace of the FP64 dataflow sweep
   long long fallback_systems = 0;         // systems re-solved with FP64 factors so far
   HostBuf h_rag, h_reqs;
   // CUDA graphs of cross-body batches (nemoh_b200_set_graphs)
@@ -211,6 +212,7 @@ void check_status(nemoh_ctx* c) {
   if (st) {
     CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
     const char* m = st == ST_TC_TIMEOUT ? "tensor-core update timed out waiting on its operands"
+                    : st == ST_SWEEP_TIMEOUT ? "triangular sweep timed out waiting on a solved block"
                     : st == ST_PIVOT ? "PIVOT INFERIEUR A 1.E-20 (GAUSSZ)"
                     : st == ST_PANEL_AREA ? "area of a panel is too small (GOMG)"
                     : st == ST_AKZ_UNDEFINED ? "AKZ > -1.5E-6: wave term undefined in the reference"
@@ -544,10 +546,17 @@ void factor_fp64(nemoh_ctx* c, int nsys, const Shape& sh) {
   LAUNCHED(c);
 }
 
+// workspace of an FP64 dataflow sweep over nsys systems of order up to n
+SweepSync fp64_sync(nemoh_ctx* c, int nsys, int n) {
+  CK(c->d_flow.ensure(2 * flow_ws_ints(nsys, (n + TB - 1) / TB) * sizeof(int)));
+  return SweepSync{c->d_flow.as<int>(), c->d_status.as<int>()};
+}
+
 // solve the factored systems for the right-hand sides in X (result in X)
 void trsm_fp64(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
+  const SweepSync sync = fp64_sync(c, nsys, sh.n);
   CK(trsm_sweep_tuned<double2>(dbatch(c, sh), c->d_inv.as<double2>(), c->d_X.as<double2>(), c->d_Y.as<double2>(), nsys,
-                         nrhs, c->stream, c->launches));
+                               nrhs, c->stream, c->launches, nullptr, sync));
   CK(cudaGetLastError());
 }
 
@@ -617,8 +626,9 @@ void mixed_fallback_ragged(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
                        cudaMemcpyDeviceToDevice, c->stream));
   const Shape shf{ord_f[0], Ragged{c->d_froff.as<long long>(), c->d_frord.as<int>(), ord_f.data(), off_f.data()}};
   factor_fp64(c, nf, shf);
+  const SweepSync sync = fp64_sync(c, nf, shf.n);
   CK(trsm_sweep_tuned<double2>(dbatch(c, shf), c->d_inv.as<double2>(), fx, c->d_fy.as<double2>(), nf, nrhs,
-                               c->stream, c->launches));
+                               c->stream, c->launches, nullptr, sync));
   for (int j = 0; j < nf; ++j)
     CK(cudaMemcpyAsync(X + bad[j] * xs, fx + j * xf, (size_t)ord_f[j] * nrhs * sizeof(double2),
                        cudaMemcpyDeviceToDevice, c->stream));
@@ -1085,6 +1095,7 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
     CK(cudaEventCreateWithFlags(&c->lanes.fork, cudaEventDisableTiming));
     CK(c->d_status.ensure(sizeof(int)));
     CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
+    c->mixed.status = c->d_status.as<int>();
     CK(c->d_gm.ensure(sizeof(unsigned long long)));
     // Green tables (CREK): nodes on the host, 251-point theta integrals on the device
     table_nodes(c->h_xr, c->h_xz);
@@ -1874,6 +1885,49 @@ int nemoh_b200_diag_fp64_peak(int device, double* tflops) {
   if (st) cudaStreamDestroy(st);
   if (prev >= 0) cudaSetDevice(prev);
   return rc;
+}
+
+// A dataflow sweep whose wait cannot end: one system of order 128 (two row
+// blocks) with the item counter started past level 0, so the level-1 item
+// waits on a ready flag that no item raises. The wait runs out, records
+// ST_SWEEP_TIMEOUT and the launch returns; the device stays usable.
+int nemoh_b200_diag_sweep_timeout(int device, int* status, double* ms) {
+  if (!status || !ms) return NEMOH_B200_EINVAL;
+  return guarded(nullptr, [&] {
+    CK(cudaSetDevice(device));
+    const int n = 128, nblk = 2;
+    DevBuf A, inv, X, Y, ws, st;
+    CK(A.ensure((size_t)n * n * sizeof(double2)));
+    CK(inv.ensure((size_t)nblk * 2 * TB * TB * sizeof(double2)));
+    CK(X.ensure((size_t)n * sizeof(double2)));
+    CK(Y.ensure((size_t)n * sizeof(double2)));
+    CK(ws.ensure(flow_ws_ints(1, nblk) * sizeof(int)));
+    CK(st.ensure(sizeof(int)));
+    CK(cudaMemset(A.p, 0, A.bytes));
+    CK(cudaMemset(inv.p, 0, inv.bytes));
+    CK(cudaMemset(X.p, 0, X.bytes));
+    CK(cudaMemset(Y.p, 0, Y.bytes));
+    CK(cudaMemset(ws.p, 0, ws.bytes));
+    CK(cudaMemset(st.p, 0, sizeof(int)));
+    const int first = 1;   // the item counter skips the level-0 item
+    CK(cudaMemcpy(ws.p, &first, sizeof(int), cudaMemcpyHostToDevice));
+    const BatchT<double2> b = make_batch<double2>(A.as<double2>(), n, nullptr, nullptr, Ragged());
+    const int smem = flow_smem<double2, 1>() + (nblk + 1) * (int)sizeof(int);
+    ScopedEvent e0, e1;
+    CK(cudaEventCreate(&e0.e));
+    CK(cudaEventCreate(&e1.e));
+    CK(cudaEventRecord(e0.e, 0));
+    trsm_flow_kernel<double2, 1, true><<<1, FL_THREADS, smem>>>(b, inv.as<double2>(), nblk, 1, X.as<double2>(),
+                                                                Y.as<double2>(), n, ws.as<int>(), st.as<int>(),
+                                                                nullptr);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(e1.e, 0));
+    CK(cudaEventSynchronize(e1.e));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0.e, e1.e));
+    *ms = t;
+    CK(cudaMemcpy(status, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+  });
 }
 
 int nemoh_b200_diag_sweep_tuning(long long* keys_tuned, int n, int nsys, int nrhs, int single, int* cluster_size) {

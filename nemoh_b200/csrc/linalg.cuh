@@ -1082,12 +1082,227 @@ inline cudaError_t trsm_sweep_nr(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int 
   return cudaLaunchKernelEx(&cfg, trsm_sweep_kernel<C2, NR, LOWER>, b, inv, nblk, X, Y, (long long)n * NR, active);
 }
 
+// ---------------------------------------------------------------------------
+// Dataflow triangular sweep, one launch per direction. The 64-row blocks of
+// every system are work items numbered level by level (forward: level l is
+// block l; backward: block nbs-1-l); the systems still active at a level are a
+// prefix of the batch (orders decrease along it). A persistent grid claims the
+// items in that order with one atomic counter. An item accumulates the
+// products of its row block with every solved block on the other side of the
+// diagonal (left-looking), waiting on each source block's ready flag (the
+// row block's loads are issued before the wait), solves with the inverted
+// diagonal block, stores its block of the solution and raises its own flag.
+// An item waits only on items of lower levels, which carry smaller numbers
+// and were claimed by running CTAs before it, so the sweep always progresses
+// whatever the number of resident CTAs. Every wait is bounded: one that runs
+// out records ST_SWEEP_TIMEOUT in the status word and sets the abort word,
+// which ends every other wait, so the launch always returns.
+// Thread (r, g): row r of the block, column quarter g of each source block;
+// the quarters' partial sums meet in shared memory.
+// Workspace per direction: [0] item counter, [1] abort word,
+// [2 + sys * nblk + blk] ready flags; zeroed before the launch.
+// ---------------------------------------------------------------------------
+constexpr int FL_THREADS = 256;
+constexpr int FL_QUARTER = TB / 4;
+constexpr int ST_SWEEP_TIMEOUT = 31;
+constexpr long long FL_SPIN_LIMIT = 1LL << 21;
+
+inline size_t flow_ws_ints(int nsys, int nblk) { return 2 + (size_t)nsys * nblk; }
+
+template <class C2, int NR>
+constexpr int flow_smem() {   // source block, partial sums of the four quarters, right-hand-side block
+  return (TB * NR + 4 * TB * NR + TB * NR) * (int)sizeof(C2);
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// bounded wait for a ready flag (thread 0 of the CTA)
+__device__ __forceinline__ void flow_wait(const int* flag, int* abort_w, int* status) {
+  long long it = 0;
+  while (ld_acquire(flag) == 0) {
+    if (ld_acquire(abort_w)) return;
+    if (++it > FL_SPIN_LIMIT) {
+      if (status) atomicCAS(status, 0, ST_SWEEP_TIMEOUT);
+      atomicExch(abort_w, 1);
+      return;
+    }
+    __nanosleep(64);
+  }
+}
+
+template <class C2, int NR, bool LOWER>
+__global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, const C2* __restrict__ inv, int nblk,
+                                                               int nsys, const C2* __restrict__ R, C2* Y,
+                                                               long long xstride, int* ws, int* status,
+                                                               const int* active) {
+  if (active && *active == 0) return;   // a converged refinement skips its remaining passes
+  extern __shared__ __align__(16) unsigned char fl_sm[];
+  C2* yb = reinterpret_cast<C2*>(fl_sm);           // [NR][TB] the source block being applied
+  C2* red = yb + TB * NR;                           // [4][NR][TB] partial sums of the column quarters
+  C2* rb = red + 4 * TB * NR;                       // [NR][TB] right-hand sides of the item's block
+  int* pre = reinterpret_cast<int*>(rb + TB * NR);  // [nblk + 1] items before each level
+  __shared__ int s_item;
+  const int t = threadIdx.x, r = t % TB, g = t / TB;
+  // systems active at level l: those with more than l blocks, a prefix
+  for (int l = t; l < nblk; l += FL_THREADS) {
+    int cnt = nsys;
+    if (b.ord) {   // first system with at most l blocks (orders decrease along the batch)
+      int lo = 0, hi = nsys;
+      while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if ((b.ord[mid] + TB - 1) / TB > l) lo = mid + 1;
+        else hi = mid;
+      }
+      cnt = lo;
+    } else if (l >= (b.n + TB - 1) / TB) {
+      cnt = 0;
+    }
+    pre[l + 1] = cnt;
+  }
+  __syncthreads();
+  if (t == 0) {
+    pre[0] = 0;
+    for (int l = 0; l < nblk; ++l) pre[l + 1] += pre[l];
+  }
+  __syncthreads();
+  const int total = pre[nblk];
+  int* flags = ws + 2;
+  for (;;) {
+    if (t == 0) s_item = atomicAdd(ws, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= total) break;
+    int lo = 0, hi = nblk;   // level: the last l with pre[l] <= item
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (pre[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const int sys = item - pre[lo];
+    const int n = b.order(sys), nbs = (n + TB - 1) / TB;
+    const int blk = LOWER ? lo : nbs - 1 - lo;
+    const int k0 = blk * TB, nb = min(TB, n - k0);
+    const C2* A = b.sys(sys);
+    const C2* Rs = R + sys * xstride;
+    C2* Ys = Y + sys * xstride;
+    int* fl = flags + (long long)sys * nblk;
+    C2 acc[NR];
+#pragma unroll
+    for (int p = 0; p < NR; ++p) acc[p] = mkc<C2>(0., 0.);
+    const int nsrc = LOWER ? blk : nbs - 1 - blk;
+#pragma unroll 1
+    for (int q = 0; q < nsrc; ++q) {
+      const int sb = LOWER ? q : nbs - 1 - q;   // sources in the order they are solved
+      const int c0 = sb * TB + g * FL_QUARTER;
+      C2 a[FL_QUARTER];
+#pragma unroll
+      for (int j = 0; j < FL_QUARTER; ++j)
+        a[j] = (r < nb && c0 + j < n) ? A[(k0 + r) + (long long)n * (c0 + j)] : mkc<C2>(0., 0.);
+      if (t == 0) flow_wait(fl + sb, ws + 1, status);
+      __syncthreads();   // the flag is seen, and every thread is done with yb
+      for (int e = t; e < TB * NR; e += FL_THREADS) {
+        const int i = e % TB, p = e / TB, row = sb * TB + i;
+        yb[e] = row < n ? __ldcg(Ys + row + (long long)n * p) : mkc<C2>(0., 0.);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < FL_QUARTER; ++j)
+#pragma unroll
+        for (int p = 0; p < NR; ++p) cmac(acc[p], a[j], yb[(g * FL_QUARTER + j) + TB * p]);
+    }
+#pragma unroll
+    for (int p = 0; p < NR; ++p) red[(g * NR + p) * TB + r] = acc[p];
+    __syncthreads();
+    for (int e = t; e < TB * NR; e += FL_THREADS) {
+      const int i = e % TB, p = e / TB;
+      C2 v = i < nb ? Rs[(k0 + i) + (long long)n * p] : mkc<C2>(0., 0.);
+#pragma unroll
+      for (int gg = 0; gg < 4; ++gg) {
+        const C2 u = red[(gg * NR + p) * TB + i];
+        v.x -= u.x;
+        v.y -= u.y;
+      }
+      rb[e] = i < nb ? v : mkc<C2>(0., 0.);
+    }
+    __syncthreads();
+    // y = inv(T_blk) rb, the inverse's columns split by quarters like the sources
+    const C2* Ti = inv + ((long long)sys * nblk + blk) * 2 * TB * TB + (LOWER ? 0 : TB * TB);
+#pragma unroll
+    for (int p = 0; p < NR; ++p) acc[p] = mkc<C2>(0., 0.);
+#pragma unroll
+    for (int j = 0; j < FL_QUARTER; ++j) {
+      const int c = g * FL_QUARTER + j;
+      const C2 ti = Ti[r + TB * c];
+#pragma unroll
+      for (int p = 0; p < NR; ++p) cmac(acc[p], ti, rb[c + TB * p]);
+    }
+#pragma unroll
+    for (int p = 0; p < NR; ++p) red[(g * NR + p) * TB + r] = acc[p];
+    __syncthreads();
+    for (int e = t; e < TB * NR; e += FL_THREADS) {
+      const int i = e % TB, p = e / TB;
+      if (i < nb) {
+        C2 v = red[p * TB + i];
+#pragma unroll
+        for (int gg = 1; gg < 4; ++gg) {
+          const C2 u = red[(gg * NR + p) * TB + i];
+          v.x += u.x;
+          v.y += u.y;
+        }
+        Ys[(k0 + i) + (long long)n * p] = v;
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) st_release(fl + blk, 1);
+  }
+}
+
+template <class C2, int NR, bool LOWER>
+inline cudaError_t trsm_flow_nr(BatchT<C2> b, const C2* inv, const C2* R, C2* Y, int nsys, int* ws, int* status,
+                                cudaStream_t st, const int* active) {
+  const int nblk = (b.n + TB - 1) / TB;
+  const int smem = flow_smem<C2, NR>() + (nblk + 1) * (int)sizeof(int);
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  auto kern = trsm_flow_kernel<C2, NR, LOWER>;
+  static std::atomic<unsigned long long> attr{0};
+  once_per_device(attr, [kern] { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); });
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FL_THREADS, smem);
+  if (e != cudaSuccess) return e;
+  const long long items = (long long)nsys * nblk;
+  const int grid = (int)std::max(1LL, std::min(items, (long long)std::max(1, sms) * std::max(1, per_sm)));
+  kern<<<grid, FL_THREADS, smem, st>>>(b, inv, nblk, nsys, R, Y, (long long)b.n * NR, ws, status, active);
+  return cudaGetLastError();
+}
+
+// the workspace both directions of one dataflow sweep use
+struct SweepSync {
+  int* ws = nullptr;       // 2 * flow_ws_ints(nsys, nblk) ints, or null: cluster sweep only
+  int* status = nullptr;
+};
+constexpr int SWEEP_FLOW = 16;   // "cluster size" of the dataflow sweep in the tuner's choices
+
 // Forward then backward sweep of nsys factored systems (nrhs right-hand sides
 // in X, solution back in X, Y scratch of the same size): two launches.
-// csize <= 0 picks the cluster size from the device's SM count.
+// csize: the cluster sweep's cluster size (1..8), SWEEP_FLOW for the dataflow
+// sweep (needs sync.ws), <= 0 for the default: the dataflow sweep when a
+// workspace is given, else a cluster size from the device's SM count.
 template <class C2>
 inline cudaError_t trsm_sweep(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st,
-                              long long& launches, const int* active = nullptr, int csize = 0) {
+                              long long& launches, const int* active = nullptr, int csize = 0,
+                              SweepSync sync = SweepSync()) {
+  if (csize <= 0 && sync.ws) csize = SWEEP_FLOW;
+  if (csize == SWEEP_FLOW && !sync.ws) csize = 0;
   if (csize <= 0) {
     static int sms = 0;
     if (!sms) {
@@ -1099,6 +1314,25 @@ inline cudaError_t trsm_sweep(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsy
     csize = sweep_cluster(nsys, (b.n + TB - 1) / TB, sms);
   }
   cudaError_t e = cudaErrorInvalidValue;
+  if (csize == SWEEP_FLOW) {
+    const size_t wsn = flow_ws_ints(nsys, (b.n + TB - 1) / TB);
+    e = cudaMemsetAsync(sync.ws, 0, 2 * wsn * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    switch (nrhs) {
+#define NB200_FL(k)                                                                                     \
+  case k:                                                                                               \
+    e = trsm_flow_nr<C2, k, true>(b, inv, X, Y, nsys, sync.ws, sync.status, st, active);                \
+    if (e == cudaSuccess) e = trsm_flow_nr<C2, k, false>(b, inv, Y, X, nsys, sync.ws + wsn, sync.status, st, active); \
+    break;
+      NB200_FL(1) NB200_FL(2) NB200_FL(3) NB200_FL(4) NB200_FL(5) NB200_FL(6) NB200_FL(7) NB200_FL(8)
+      NB200_FL(9) NB200_FL(10) NB200_FL(11) NB200_FL(12) NB200_FL(13) NB200_FL(14) NB200_FL(15) NB200_FL(16)
+#undef NB200_FL
+      default:
+        break;
+    }
+    launches += 2;
+    return e;
+  }
   switch (nrhs) {
 #define NB200_SW(k)                                                                          \
   case k:                                                                                    \

@@ -62,8 +62,10 @@ struct MixedWork {
   float2* pinv = nullptr;    // inv(L) of the diagonal blocks of the current outer panel
   unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
   RefineState* state = nullptr;         // refinement decisions on the device
+  int* flow = nullptr;       // workspace of the dataflow sweep (both directions)
+  int* status = nullptr;     // the owner's status word (sweep timeouts)
   TcWork tc;                 // tensor-core GEMM operand buffers
-  size_t have[10] = {};      // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv, state
+  size_t have[11] = {};      // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv, state, flow
   size_t total = 0;
   int last_iterations = 0;
   double last_residual = 0.;
@@ -72,10 +74,10 @@ struct MixedWork {
   size_t bytes() const { return total; }
   void release() {
     cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms); cudaFree(inv);
-    cudaFree(pinv); cudaFree(state);
+    cudaFree(pinv); cudaFree(state); cudaFree(flow);
     tc.release();
     lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr; inv = nullptr;
-    pinv = nullptr; state = nullptr;
+    pinv = nullptr; state = nullptr; flow = nullptr;
     for (size_t& h : have) h = 0;
     total = 0;
   }
@@ -87,7 +89,7 @@ struct MixedWork {
   // mat_elems: elements of all matrices of a ragged batch (0: nsys x n x n)
   cudaError_t ensure(int nsys, int n, int nrhs, size_t mat_elems = 0) {
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
-    const size_t need[10] = {(mat_elems ? mat_elems : nsys * NN) * sizeof(float2),
+    const size_t need[11] = {(mat_elems ? mat_elems : nsys * NN) * sizeof(float2),
                             (size_t)nsys * DIAG_SCRATCH * sizeof(float2),
                             V * sizeof(double2),
                             V * sizeof(double2),
@@ -96,10 +98,11 @@ struct MixedWork {
                             (size_t)2 * nsys * nrhs * sizeof(unsigned long long),
                             (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2),
                             (size_t)nsys * PINV_SCRATCH * sizeof(float2),
-                            sizeof(RefineState)};
-    void** ptr[10] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
-                      (void**)&inv, (void**)&pinv, (void**)&state};
-    for (int i = 0; i < 10; ++i) {
+                            sizeof(RefineState),
+                            2 * flow_ws_ints(nsys, (n + TB - 1) / TB) * sizeof(int)};
+    void** ptr[11] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
+                      (void**)&inv, (void**)&pinv, (void**)&state, (void**)&flow};
+    for (int i = 0; i < 11; ++i) {
       if (need[i] <= have[i]) continue;
       cudaFree(*ptr[i]);
       *ptr[i] = nullptr;
@@ -182,7 +185,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
 inline void trsm_f32(MixedWork& w, int n, int nsys, int nrhs, cudaStream_t st, long long& launches,
                      const int* active, const Ragged& rg) {
   BatchT<float2> b = make_batch<float2>(w.lu, n, w.diag, nullptr, rg);
-  trsm_sweep_tuned<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, active);
+  trsm_sweep_tuned<float2>(b, w.inv, w.rf, w.yf, nsys, nrhs, st, launches, active, SweepSync{w.flow, w.status});
   // the solution is left in w.rf (forward into yf, backward back into rf)
 }
 

@@ -1,20 +1,24 @@
 // Autotuner of the triangular sweep's tile shape.
 //
-// The sweep (linalg.cuh, trsm_sweep_kernel) spreads the 64-row blocks of one
-// system over a thread-block cluster of csize CTAs (1, 2, 4 or 8): a larger
-// cluster puts more SMs on one system's updates but adds cluster barriers and
-// distributed-shared-memory copies per step. The fastest csize depends on the
+// Two sweeps solve the same systems (linalg.cuh): the cluster sweep spreads
+// the 64-row blocks of one system over a thread-block cluster of csize CTAs
+// (1, 2, 4 or 8; a larger cluster puts more SMs on one system's updates but
+// adds cluster barriers and distributed-shared-memory copies per step), the
+// dataflow sweep (SWEEP_FLOW) spreads the row blocks of all systems over a
+// persistent grid that follows ready flags. The fastest choice depends on the
 // number of systems in the batch, their order, the precision and the number
 // of right-hand sides. The tuner times every candidate once per key (device,
 // element type, power-of-two buckets of the order, of the system count and
 // of the right-hand sides) on a copy of the batch's right-hand sides, keeps
 // the fastest for the life of the process, and then solves with it. Under
 // stream capture (no timing possible) and before a key has been tuned without
-// scratch, the SM-count heuristic of trsm_sweep decides.
+// scratch, trsm_sweep's default decides.
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 
@@ -60,14 +64,33 @@ inline int sweep_tuned_size(const BatchT<C2>& b, int nsys, int nrhs) {
 
 // trsm_sweep with the tuned cluster size; tunes the key first when it is new
 // and the stream is not being captured. X: right-hand sides in, solution out.
+// NEMOH_B200_SWEEP=flow or =cluster fixes the choice (tests, diagnosis):
+// the dataflow sweep where a workspace is given, or the cluster sweep with
+// its SM-count cluster size.
+inline int sweep_forced() {
+  static const int f = [] {
+    const char* e = std::getenv("NEMOH_B200_SWEEP");
+    if (!e) return 0;
+    if (std::strcmp(e, "flow") == 0) return SWEEP_FLOW;
+    if (std::strcmp(e, "cluster") == 0) return -1;
+    return 0;
+  }();
+  return f;
+}
+
 template <class C2>
 inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st,
-                                    long long& launches, const int* active = nullptr) {
+                                    long long& launches, const int* active = nullptr, SweepSync sync = SweepSync()) {
+  const int forced = sweep_forced();
+  if (forced == -1) return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, 0, SweepSync());
+  if (forced == SWEEP_FLOW && sync.ws)
+    return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, SWEEP_FLOW, sync);
   int csize = sweep_tuned_size(b, nsys, nrhs);
-  if (csize > 0) return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, csize);
+  if (csize > 0 && (csize != SWEEP_FLOW || sync.ws))
+    return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, csize, sync);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
-    return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active);
+    return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, 0, sync);
   int dev = 0;
   cudaGetDevice(&dev);
   const unsigned long long key = sweep_key(dev, sizeof(C2) == sizeof(float2), b.n, nsys, nrhs);
@@ -75,7 +98,7 @@ inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, i
   SweepTuner& t = sweep_tuner();
   std::lock_guard<std::mutex> lock(t.mu);
   cudaError_t e;
-  if (dev < 0 || dev >= 64) return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active);
+  if (dev < 0 || dev >= 64) return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, 0, sync);
   void*& scratch = t.scratch[dev];
   if (t.scratch_bytes[dev] < bytes) {
     cudaFree(scratch);
@@ -91,11 +114,15 @@ inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, i
   const int nblk = (b.n + TB - 1) / TB;
   float best_ms = FLT_MAX;
   int best_c = 0;
-  for (int c = 1; c <= 8 && c <= nblk; c *= 2) {
+  int cands[5], nc = 0;
+  for (int c = 1; c <= 8 && c <= nblk; c *= 2) cands[nc++] = c;
+  if (sync.ws) cands[nc++] = SWEEP_FLOW;
+  for (int ci = 0; ci < nc; ++ci) {
+    const int c = cands[ci];
     cudaMemcpyAsync(X, scratch, bytes, cudaMemcpyDeviceToDevice, st);
     cudaEventRecord(ev[0], st);
     long long l = 0;
-    e = trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, l, active, c);
+    e = trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, l, active, c, sync);
     cudaEventRecord(ev[1], st);
     if (e != cudaSuccess) {   // e.g. a cluster that cannot be scheduled: not a candidate
       cudaGetLastError();
@@ -114,7 +141,7 @@ inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, i
   t.best[key] = best_c;
   ++t.tuned;
   if ((e = cudaMemcpyAsync(X, scratch, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
-  return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, best_c);
+  return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, best_c, sync);
 }
 
 }  // namespace nb200

@@ -381,6 +381,90 @@ def test_one_tile_per_cta_tensor_core_update(tmp_path):
         assert float(line[2]) < 1e-6 and 0 < int(line[4]) <= 6, line
 
 
+def test_dataflow_and_cluster_sweeps_agree(tmp_path):
+    """The two triangular sweeps, each forced in a child process
+    (NEMOH_B200_SWEEP is read once per process): FP64 forces agree within
+    1e-12 of the largest force, the mixed ones match FP64 within 1e-6 per
+    coefficient with the refinement converging, on a cylinder of 300 panels
+    (5 row blocks, 2 with symmetry classes) and a hemisphere of 640 (10 row
+    blocks, one partial), and a cross-body batch of both (a ragged sweep)."""
+    import subprocess
+    import sys
+    script = tmp_path / "sweeps.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        "sys.path[:0] = %r\n"
+        "import gpu_cases as G, nemoh_b200 as nb\n"
+        "from nemoh_b200 import cases as C\n"
+        "cyl = C.config_cylinder(n_omega=3)\n"
+        "sph = C.Case(C.hemisphere_mesh(3.0, 16, 40, jitter=0.2, rng=np.random.default_rng(7)),\n"
+        "             np.array([0.5, 1.1, 1.7]), np.array([0.0]), C.six_dofs(), C.six_dofs(), depth=0.0)\n"
+        "res = {}\n"
+        "for case in (cyl, sph):\n"
+        "    nvel, nds, npb = G.problems(case)\n"
+        "    for mode in (nb.FP64, nb.MIXED):\n"
+        "        with nb.Solver(0, mode) as s:\n"
+        "            s.set_case(case)\n"
+        "            res['%%s_%%d' %% (case.name, mode)] = s.solve_frequencies(case.omegas, nvel, nds)\n"
+        "            res['it_%%s_%%d' %% (case.name, mode)] = np.array(s.last_refinement()[0])\n"
+        "body = np.array([0, 1, 0, 1]); om = np.array([0.6, 0.9, 1.3, 1.9])\n"
+        "nv = []\n"
+        "for b, w in zip(body, om):\n"
+        "    c = (cyl, sph)[b]\n"
+        "    nv.append(C.body_conditions(C.Case(c.mesh, np.array([w]), np.array([20.0]), c.rad, c.force,\n"
+        "                                       rho=c.rho, g=c.g, depth=c.depth)))\n"
+        "for mode in (nb.FP64, nb.MIXED):\n"
+        "    with nb.Solver(0, mode) as s:\n"
+        "        for c in (cyl, sph):\n"
+        "            s.add_body(c)\n"
+        "        out = s.solve_bodies(body, om, nv)\n"
+        "        for i, f in enumerate(out):\n"
+        "            res['bodies_%%d_%%d' %% (i, mode)] = f\n"
+        "np.savez(sys.argv[1], **res)\n"
+        % [str(p) for p in (B.HERE + "/..", B.HERE + "/../tests")])
+    got = {}
+    for form in ("flow", "cluster"):
+        env = dict(os.environ, NEMOH_B200_SWEEP=form)
+        out = tmp_path / (form + ".npz")
+        r = subprocess.run([sys.executable, str(script), str(out)], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        got[form] = dict(np.load(out))
+    a, b = got["flow"], got["cluster"]
+    assert set(a) == set(b)
+    for k in a:
+        if k.startswith("it_"):
+            assert 0 < int(a[k]) <= 6 or k.endswith("_%d" % nb.FP64), (k, a[k])
+            continue
+        scale = np.abs(b[k]).max()
+        tol = 1e-12 if k.endswith("_%d" % nb.FP64) else 1e-6
+        assert np.abs(a[k] - b[k]).max() <= tol * scale, (k, np.abs(a[k] - b[k]).max() / scale)
+    for k in a:
+        if k.endswith("_%d" % nb.MIXED) and not k.startswith("it_"):
+            ref = a[k[:-len(str(nb.MIXED))] + str(nb.FP64)]
+            if ref.ndim == 3:
+                assert G.coef_err(a[k], ref, 1) < 1e-6, k
+                assert G.coef_err(b[k], ref, 1) < 1e-6, k
+
+
+def test_dataflow_sweep_wait_runs_out_and_device_stays_usable(solver):
+    """A dataflow sweep whose only item waits on a ready flag that nothing
+    raises: the bounded wait ends with the sweep-timeout status (31) in well
+    under the test's time, and a solve on the same device afterwards still
+    matches the oracle."""
+    st, ms = nb.sweep_timeout_check(0)
+    assert st == 31, st
+    assert ms < 30000.0, ms
+    case = CASES[0]
+    _mesh(solver, case)
+    o = G.oracle_for(case)
+    nv = C.body_conditions(case)
+    T = 2 * np.pi / case.omegas[0]
+    g = solver.solve_potential(T, nv[:, 0])
+    r = o.solve_problem(T, nv[:, 0])
+    assert np.abs(g["zpb"] - r["zpb"]).max() <= 1e-10 * np.abs(r["zpb"]).max()
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_kochin_matches_oracle(solver, case):
     """COMPUTE_KOCHIN on the GPU vs the oracle, on the same source strengths:
