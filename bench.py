@@ -508,6 +508,11 @@ def run_outputs(local, omega_index=10):
     return out
 
 
+def tc_split():
+    """Operand split of the mixed LU's tensor-core updates (NEMOH_B200_TC_SPLIT)."""
+    return "bf16" if os.environ.get("NEMOH_B200_TC_SPLIT") == "bf16" else "f16"
+
+
 def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9, 1.0, 1.2), seed=5, n_check=64, workers=2):
     """Serving workload: Poisson request streams over the batched workload's
     bodies (one omega U(0.1, 2.5), heading U(0, 180) deg, 6 DOF per request)
@@ -616,7 +621,7 @@ def run_ours(args):
         F = force_d.cpu().numpy()
         F = (F[..., 0] + 1j * F[..., 1]).transpose(2, 1, 0)
         results[label] = dict(ms=ms / args.steps, phase=phase / args.steps, launches=launches, F=F,
-                              clocks=clk.summary(), solver=s)
+                              clocks=clk.summary(), solver=s, refinement=s.last_refinement())
     # end-to-end through the C-ABI with pinned host buffers
     s = results["mixed"]["solver"]
     pin_nvel = torch.from_numpy(np.ascontiguousarray(nvel_h.transpose(2, 1, 0)).view(np.float64)).pin_memory()
@@ -679,7 +684,8 @@ def run_ours(args):
         "metric": "BEM solves/s (mixed vs FP64 GPU, rel err<=1e-6) at N=2400; serve p50/p99 ms",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": mx["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 assembly / f32+bf16 LU / f64 refinement", "data": "synthetic",
+        "dtype": "f64 assembly / f32 LU, tensor-core updates on split-%s operands / f64 refinement" % tc_split(),
+        "data": "synthetic",
         "config": {"workload": "barge 100x20x10 m, depth 50 m, half mesh N=2400 (y-symmetric), 40 omega x 9 problems",
                    "n_panels": N, "omegas": nomega, "problems_per_omega": NPROB, "precision": "mixed",
                    "l2": "working set 15 GB of matrices per step, larger than L2 (no flush needed)"},
@@ -689,6 +695,7 @@ def run_ours(args):
         "mixed_vs_fp64": {"max_rel_err": err_max, "median_rel_err": err_med, "speedup": f64["ms"] / mx["ms"]},
         "phase_ms": {"assemble": mx["phase"][0], "factor_refine": mx["phase"][1], "lu": mx["phase"][3],
                      "solve": mx["phase"][2]},
+        "refinement": dict(zip(("iterations", "residual"), mx["refinement"])),
         "roofline": roofline_line(achieved, hbm, src, traffic, 80.0 * N * N, fp64),
         "e2e": {"value": whole_job_rate(world, nomega, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(pin_nvel.numel() * 8 + pin_nds.numel() * 8),

@@ -93,81 +93,65 @@ __device__ __forceinline__ double cabs2(float2 a) { return hypotf(a.x, a.y); }
 
 // Factor the diagonal block A11 of step k once per system (grid.z = system)
 // and invert its triangles. Scratch per system: [LU(A11) | inv(L11) | inv(U11)],
-// column-major nb x nb each (ld = nb). 128 threads:
-//  * unpivoted Doolittle (GAUSSZ's elimination on this block), lane i on row
-//    i and warp w on the columns c = w mod 4: at step j the owner of column j
-//    divides it below the pivot, one block barrier, then every warp applies
-//    the rank-1 update to its columns right of j (the owner of column j+1 has
-//    then finished it, so the next step needs no second barrier);
-//  * the inverses, one column per lane held in registers (a column of either
-//    inverse depends only on itself and the factored block, so no barrier):
-//    warp 0 inv(L) (X = I, step j ascending subtracts L(i, j) X(j, c) from
-//    the rows below), warp 1 inv(U) (X = I, step j descending divides X(j, c)
-//    by U(j, j) and subtracts U(i, j) X(j, c) from the rows above), while
-//    warps 2 and 3 store the factored block.
-// Every element sees the same operations in the same order as a sequential
-// elimination. With b.pinv (two-level LU) inv(L) also goes to the slot of this
-// block in the current outer panel.
-constexpr int LU_DIAG_THREADS = 128;
+// column-major nb x nb each (ld = nb). One thread per element of the 32 x 32
+// block, every step of the three eliminations separated by a barrier:
+//  * unpivoted Doolittle (GAUSSZ's elimination on this block): at step j the
+//    column below the pivot is divided by it, then the trailing block takes
+//    the rank-1 update;
+//  * inv(L): X = I, step j (ascending) subtracts L(i, j) X(j, :) from the rows
+//    below, the order of the column-by-column forward substitution;
+//  * inv(U): X = I, step j (descending) divides row j by U(j, j) and
+//    subtracts U(i, j) X(j, :) from the rows above.
+// With b.pinv (two-level LU) inv(L) also goes to the slot of this block in the
+// current outer panel. (Measured against two 128-thread forms, warp-owned
+// columns with the inverses either by warp-owned columns or one column per
+// lane in registers: 28.6 us per launch here against 78.5 and 65 us; the
+// register form's long unrolled instruction stream stalls on instruction
+// fetch.)
+constexpr int LU_DIAG_THREADS = LU_NB * LU_NB;
 template <class C2>
 __global__ void __launch_bounds__(LU_DIAG_THREADS) lu_diag_kernel(BatchT<C2> b, int k, int* status) {
   __shared__ C2 sb[LU_NB * LU_NB];   // the block, column-major, ld = nb
-  constexpr int NW = LU_DIAG_THREADS / 32;
+  __shared__ C2 xl[LU_NB * LU_NB];   // inv(L11), ld = LU_NB
+  __shared__ C2 xu[LU_NB * LU_NB];   // inv(U11), ld = LU_NB
   const int n = b.order(blockIdx.z);
   if (k >= n) return;
   const int nb = min(LU_NB, n - k);
-  const int i = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = threadIdx.x & (LU_NB - 1), c = threadIdx.x / LU_NB;
+  const bool in = i < nb && c < nb;
   const C2* A = b.sys(blockIdx.z);
-  for (int c = w; c < nb; c += NW)
-    if (i < nb) sb[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
+  if (in) sb[i + nb * c] = A[(k + i) + (long long)n * (k + c)];
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
-    if (w == (j % NW)) {
-      if (i == 0 && !(cabs2(sb[j + nb * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-      if (i > j && i < nb) sb[i + nb * j] = cdv(sb[i + nb * j], sb[j + nb * j]);
-    }
+    if (threadIdx.x == 0 && !(cabs2(sb[j + nb * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+    if (in && c == j && i > j) sb[i + nb * j] = cdv(sb[i + nb * j], sb[j + nb * j]);
     __syncthreads();
-    if (i > j && i < nb)
-      for (int c = w; c < nb; c += NW)
-        if (c > j) sb[i + nb * c] = cfms(sb[i + nb * c], sb[i + nb * j], sb[j + nb * c]);
+    if (in && i > j && c > j) sb[i + nb * c] = cfms(sb[i + nb * c], sb[i + nb * j], sb[j + nb * c]);
+    __syncthreads();
+  }
+  const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
+  if (in) {
+    xl[i + LU_NB * c] = i == c ? one : zero;
+    xu[i + LU_NB * c] = i == c ? one : zero;
   }
   __syncthreads();
+  for (int step = 0; step < nb; ++step) {
+    const int jl = step, ju = nb - 1 - step;
+    if (in && i == ju && c >= ju) xu[ju + LU_NB * c] = cdv(xu[ju + LU_NB * c], sb[ju + nb * ju]);
+    __syncthreads();
+    if (in && i > jl && c <= jl) xl[i + LU_NB * c] = cfms(xl[i + LU_NB * c], sb[i + nb * jl], xl[jl + LU_NB * c]);
+    if (in && i < ju && c >= ju) xu[i + LU_NB * c] = cfms(xu[i + LU_NB * c], sb[i + nb * ju], xu[ju + LU_NB * c]);
+    __syncthreads();
+  }
   C2* D = b.diag + (long long)blockIdx.z * DIAG_SCRATCH;
   C2* P = b.pinv ? b.pinv + (long long)blockIdx.z * PINV_SCRATCH + ((k % LU_OUTER) / LU_NB) * LU_NB * LU_NB : nullptr;
-  if (w >= 2) {
-    for (int q = threadIdx.x - 64; q < nb * nb; q += 64) D[q] = sb[q];
-    return;
+  if (in) {
+    const int q = i + nb * c;
+    D[q] = sb[q];
+    D[LU_NB * LU_NB + q] = xl[i + LU_NB * c];
+    D[2 * LU_NB * LU_NB + q] = xu[i + LU_NB * c];
+    if (P) P[q] = xl[i + LU_NB * c];
   }
-  const int c = i;   // the column of the inverse this lane computes
-  if (c >= nb) return;
-  const C2 one = mkc<C2>(1., 0.), zero = mkc<C2>(0., 0.);
-  C2 x[LU_NB];
-#pragma unroll
-  for (int r = 0; r < LU_NB; ++r) x[r] = r == c ? one : zero;
-  if (w == 0) {
-#pragma unroll
-    for (int jl = 0; jl < LU_NB - 1; ++jl) {
-      if (jl < c || jl >= nb) continue;
-#pragma unroll
-      for (int r = jl + 1; r < LU_NB; ++r)
-        if (r < nb) x[r] = cfms(x[r], sb[r + nb * jl], x[jl]);
-    }
-  } else {
-#pragma unroll
-    for (int ju = LU_NB - 1; ju >= 0; --ju) {
-      if (ju > c || ju >= nb) continue;
-      x[ju] = cdv(x[ju], sb[ju + nb * ju]);
-#pragma unroll
-      for (int r = 0; r < ju; ++r) x[r] = cfms(x[r], sb[r + nb * ju], x[ju]);
-    }
-  }
-  C2* out = D + (w == 0 ? 1 : 2) * LU_NB * LU_NB;
-#pragma unroll
-  for (int r = 0; r < LU_NB; ++r)
-    if (r < nb) {
-      out[r + nb * c] = x[r];
-      if (w == 0 && P) P[r + nb * c] = x[r];
-    }
 }
 
 // acc += a b as four fused multiply-adds into the accumulator (written out:

@@ -3,15 +3,15 @@
 // The FP32 LU (mixed.cuh) factors 128-column panels with 32-column steps and
 // then updates the trailing matrix once per panel:
 //     A22 <- A22 - L21 * U12        (complex FP32, inner dimension K = 128).
-// On the tensor cores the complex product becomes real BF16 products with FP32
-// accumulation. A is kept as [Ar | Ai] (K' = 2K real columns) and B as two
+// On the tensor cores the complex product becomes real 16-bit products with
+// FP32 accumulation. A is kept as [Ar | Ai] (K' = 2K real columns) and B as two
 // column blocks, [Br; -Bi] for the real parts and [Bi; Br] for the imaginary
 // parts of the result (N' = 2 x 128), so that
 //     [Re C | Im C] = [Ar | Ai] * [[Br, Bi], [-Bi, Br]].
-// Each operand is split x = hi + lo into two BF16 terms and the product keeps
-// hi*hi + hi*lo + lo*hi (~16-bit operands, FP32 accumulation): the same hi
-// and lo images are reused by three MMAs through their descriptors, so they
-// are stored once.
+// Each operand is split x = hi + lo into two FP16 terms (22 significant bits;
+// BF16 terms, 16 bits, with NEMOH_B200_TC_SPLIT=bf16) and the product keeps
+// hi*hi + hi*lo + lo*hi (FP32 accumulation): the same hi and lo images are
+// reused by three MMAs through their descriptors, so they are stored once.
 //
 // A prep kernel writes both operands as ready-made shared-memory images
 // (K-major, no swizzle, 8x8 core matrices of 128 bytes) per tile and per
@@ -25,10 +25,12 @@
 // memory and returns.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 #include "linalg.cuh"
 
@@ -89,16 +91,32 @@ __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) {
   return (uint32_t)__bfloat16_as_ushort(v.x) | ((uint32_t)__bfloat16_as_ushort(v.y) << 16);
 }
 
-// eight consecutive values -> BF16 hi terms and BF16 lo = x - hi terms, packed
-// in k order (element 0 in the low half of the first word)
+__device__ __forceinline__ uint32_t h2_bits(__half2 v) {
+  return (uint32_t)__half_as_ushort(v.x) | ((uint32_t)__half_as_ushort(v.y) << 16);
+}
+
+// eight consecutive values -> hi terms and lo = x - hi terms, packed in k
+// order (element 0 in the low half of the first word); BF16 terms, or FP16
+// terms (F16: 11-bit significands, so hi + lo keeps 22 bits against 16 with
+// BF16; the LU factors the dimensionless matrix D, whose entries are far
+// inside FP16's range, and a lo term below FP16's normal range loses only
+// what is already below 2^-24 of the largest entries)
+template <bool F16>
 __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const __nv_bfloat162 h2 = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
-    const float2 hf = __bfloat1622float2(h2);
-    h[i] = bf2_bits(h2);
-    l[i] = bf2_bits(__floats2bfloat162_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y));
+    if (F16) {
+      const __half2 h2 = __floats2half2_rn(x[2 * i], x[2 * i + 1]);
+      const float2 hf = __half22float2(h2);
+      h[i] = h2_bits(h2);
+      l[i] = h2_bits(__floats2half2_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y));
+    } else {
+      const __nv_bfloat162 h2 = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+      const float2 hf = __bfloat1622float2(h2);
+      h[i] = bf2_bits(h2);
+      l[i] = bf2_bits(__floats2bfloat162_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y));
+    }
   }
   hi = make_uint4(h[0], h[1], h[2], h[3]);
   lo = make_uint4(l[0], l[1], l[2], l[3]);
@@ -107,6 +125,7 @@ __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
 // Operand images of the outer update after the panel [k0, k0 + 128):
 // L21 = A[r1:n, k0:k0+128] and U12 = A[k0:k0+128, r1:n] with r1 = k0 + 128.
 // Thread per (row or column of the tile, chunk); blocks [0, na) do A, the rest B.
+template <bool F16>
 __global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, unsigned char* __restrict__ abuf,
                                                        unsigned char* __restrict__ bbuf, long long sys_bytes_a,
                                                        long long sys_bytes_b, int na) {
@@ -134,7 +153,7 @@ __global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, 
     // k-groups: 0,1 = Re(k 0..15), 2,3 = Im(k 0..15)
 #pragma unroll
     for (int g = 0; g < 4; ++g) {
-      split8((g < 2 ? re : im) + 8 * (g & 1), h, l);
+      split8<F16>((g < 2 ? re : im) + 8 * (g & 1), h, l);
       *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
       *reinterpret_cast<uint4*>(img + TC_AIMG + tc_row_off(row, g)) = l;
     }
@@ -155,10 +174,10 @@ __global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, 
     // B row `row` (real parts of the result): [Br; -Bi]; row 128+row (imaginary parts): [Bi; Br]
 #pragma unroll
     for (int g = 0; g < 4; ++g) {
-      split8((g < 2 ? re : nim) + 8 * (g & 1), h, l);
+      split8<F16>((g < 2 ? re : nim) + 8 * (g & 1), h, l);
       *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
       *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(row, g)) = l;
-      split8((g < 2 ? im : re) + 8 * (g & 1), h, l);
+      split8<F16>((g < 2 ? im : re) + 8 * (g & 1), h, l);
       *reinterpret_cast<uint4*>(img + tc_row_off(TC_T + row, g)) = h;
       *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(TC_T + row, g)) = l;
     }
@@ -200,11 +219,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
   return d;                 // base offset 0, layout type 0 (no swizzle)
 }
 
-// instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M=128, N=256
-__host__ __device__ constexpr uint32_t tc_idesc() {
+// instruction descriptor: BF16 x BF16 (or F16 x F16: A and B always share
+// the type) -> F32, K-major A and B, M=128, N=256
+__host__ __device__ constexpr uint32_t tc_idesc(bool f16 = false) {
   return (1u << 4)                    // D format F32
-         | (1u << 7)                  // A format BF16
-         | (1u << 10)                 // B format BF16
+         | (f16 ? 0u : 1u << 7)       // A format: F16 (0) or BF16 (1)
+         | (f16 ? 0u : 1u << 10)      // B format: the same as A
          | ((uint32_t)((2 * TC_T) >> 3) << 17)
          | ((uint32_t)(128 >> 4) << 24);
 }
@@ -221,12 +241,12 @@ __device__ __forceinline__ void tc_load_chunk(uint32_t dst, const unsigned char*
                : "memory");
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc, uint32_t idesc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-      "l"(da), "l"(db), "r"(tc_idesc()), "r"(acc)
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
       : "memory");
 }
 
@@ -235,7 +255,8 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, 
 __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int k0,
                                                            const unsigned char* __restrict__ abuf,
                                                            const unsigned char* __restrict__ bbuf,
-                                                           long long sys_bytes_a, long long sys_bytes_b, int* status) {
+                                                           long long sys_bytes_a, long long sys_bytes_b, int* status,
+                                                           uint32_t idesc) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * TC_STAGE);   // full[2], empty[2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
@@ -295,9 +316,10 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk) {
         const uint32_t o = kk * 256;
-        tc_mma(tmem, umma_desc(ahi + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), (c > 0 || kk > 0) ? 1u : 0u);
-        tc_mma(tmem, umma_desc(ahi + o, 128, TC_SBO), umma_desc(blo + o, 128, TC_SBO), 1u);
-        tc_mma(tmem, umma_desc(alo + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), 1u);
+        tc_mma(tmem, umma_desc(ahi + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), (c > 0 || kk > 0) ? 1u : 0u,
+               idesc);
+        tc_mma(tmem, umma_desc(ahi + o, 128, TC_SBO), umma_desc(blo + o, 128, TC_SBO), 1u, idesc);
+        tc_mma(tmem, umma_desc(alo + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), 1u, idesc);
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(empty0 + 8 * s)
                    : "memory");
@@ -406,7 +428,7 @@ constexpr int TCP_SMEM = TCP_STAGES * TC_STAGE + 256;
 
 __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     BatchT<float2> b, int k0, const unsigned char* __restrict__ abuf, const unsigned char* __restrict__ bbuf,
-    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status) {
+    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TCP_STAGES * TC_STAGE);
   // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the TMEM address
@@ -497,9 +519,10 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
 #pragma unroll
         for (int kk = 0; kk < 2; ++kk) {
           const uint32_t o = kk * 256;
-          tc_mma(tm, umma_desc(ahi + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), (c > 0 || kk > 0) ? 1u : 0u);
-          tc_mma(tm, umma_desc(ahi + o, 128, TC_SBO), umma_desc(blo + o, 128, TC_SBO), 1u);
-          tc_mma(tm, umma_desc(alo + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), 1u);
+          tc_mma(tm, umma_desc(ahi + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), (c > 0 || kk > 0) ? 1u : 0u,
+                 idesc);
+          tc_mma(tm, umma_desc(ahi + o, 128, TC_SBO), umma_desc(blo + o, 128, TC_SBO), 1u, idesc);
+          tc_mma(tm, umma_desc(alo + o, 128, TC_SBO), umma_desc(bhi + o, 128, TC_SBO), 1u, idesc);
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                          empty0 + 8 * q)
@@ -599,6 +622,15 @@ inline bool tc_persistent() {
   return on;
 }
 
+// operand split: FP16 terms unless NEMOH_B200_TC_SPLIT=bf16 (BF16 terms)
+inline bool tc_split_f16() {
+  static const bool on = [] {
+    const char* e = std::getenv("NEMOH_B200_TC_SPLIT");
+    return !(e && std::strcmp(e, "bf16") == 0);
+  }();
+  return on;
+}
+
 // NEMOH_B200_TC=0 selects the CUDA-core FP32 update instead (for comparison)
 inline bool tc_enabled() {
   static const bool on = [] {
@@ -622,8 +654,11 @@ inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_
   const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
   const int nt = (rest + TC_T - 1) / TC_T;
   const int per = (nt * TC_T * TC_NCH + 127) / 128;
-  tc_prep_kernel<<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
+  const bool f16 = tc_split_f16();
+  if (f16) tc_prep_kernel<true><<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
+  else tc_prep_kernel<false><<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
   ++launches;
+  const uint32_t idesc = tc_idesc(f16);
   if (tc_persistent()) {
     static std::atomic<unsigned long long> attr2{0};
     static int sms = 0;
@@ -635,9 +670,10 @@ inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_
     });
     const long long tiles = (long long)nt * nt * nsys;
     const int grid = (int)std::min<long long>(tiles, sms > 0 ? sms : 148);
-    tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, nt, nsys, status);
+    tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, nt, nsys, status,
+                                                                     idesc);
   } else {
-    tc_update_kernel<<<dim3(nt, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status);
+    tc_update_kernel<<<dim3(nt, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status, idesc);
   }
   ++launches;
   return true;
