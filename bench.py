@@ -510,7 +510,7 @@ def run_outputs(local, omega_index=10):
 
 def tc_split():
     """Operand split of the mixed LU's tensor-core updates (NEMOH_B200_TC_SPLIT)."""
-    return "bf16" if os.environ.get("NEMOH_B200_TC_SPLIT") == "bf16" else "f16"
+    return "f16" if os.environ.get("NEMOH_B200_TC_SPLIT") == "f16" else "bf16"
 
 
 def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9, 1.0, 1.2), seed=5, n_check=64, workers=2):

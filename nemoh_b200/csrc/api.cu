@@ -133,6 +133,11 @@ struct nemoh_ctx {
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
   Lanes lanes;               // side streams for groups of systems in the LU and triangular solves
+  // pipelined batches: the first frequencies' FP32 LU on stream2 (with its own
+  // lanes) while the main stream assembles the rest
+  cudaStream_t stream2 = nullptr;
+  Lanes lanes2;
+  cudaEvent_t ev_pipe[2] = {nullptr, nullptr};
   int nq_state = 0;          // the reference's NQ, left by the last finite-depth solve
   double w_previous = -1.;   // factor cache key of solve_problem
   int cached_fd = 0, cached_nexp = 0;
@@ -647,12 +652,15 @@ void mixed_solve(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
   else mixed_fallback(c, nsys, nrhs, sh);
 }
 
-void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs, const Shape& sh) {
+// pre (mixed precision, uniform batches): systems [0, pre) were factored on
+// stream2, whose event ev_pipe[1] the refinement waits for
+void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs, const Shape& sh, int pre = 0) {
   c->lu64 = c->mode == NEMOH_B200_FP64;
   CK(cudaEventRecord(c->ev_lu[0], c->stream));
   if (c->mode == NEMOH_B200_MIXED) {
-    mixed_factor(c->mixed, c->d_D.as<double2>(), sh.n, nsys, c->d_status.as<int>(), c->stream, c->launches,
-                 &c->lanes, /*have_f32=*/true, sh.rg);
+    mixed_factor(c->mixed, c->d_D.as<double2>(), sh.n, nsys - pre, c->d_status.as<int>(), c->stream, c->launches,
+                 &c->lanes, /*have_f32=*/true, sh.rg, -1, pre);
+    if (pre) CK(cudaStreamWaitEvent(c->stream, c->ev_pipe[1], 0));
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev_lu[1], c->stream));
     if (have_rhs) mixed_solve(c, nsys, nrhs, sh);
@@ -685,6 +693,22 @@ void potential(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
 // frequencies whose host setup is done before their assembly is launched
 constexpr int ASM_GROUP = 8;
 
+// Pipelined batch (mixed precision): the FP32 LU of the first frequencies of
+// a batch runs on stream2 while the main stream assembles the rest, so the
+// LU's latency-bound launches fill the SMs the FP64-bound assembly leaves
+// between its CTAs. Returns the number of frequencies factored early (0: no
+// pipeline). NEMOH_B200_PIPELINE = percentage of the batch (default 50, 0
+// turns it off).
+int pipeline_split(const nemoh_ctx* c, int nw) {
+  static const int pct = [] {
+    const char* e = std::getenv("NEMOH_B200_PIPELINE");
+    const int v = e ? std::atoi(e) : 50;
+    return std::max(0, std::min(90, v));
+  }();
+  if (c->mode != NEMOH_B200_MIXED || nw < 2 || pct == 0) return 0;
+  return std::max(1, std::min(nw - 1, nw * pct / 100));
+}
+
 // shared by the host and device-pointer batched entry points
 void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int nrhs, const double2* nvel_d, int nint,
                             const double* nds_d, double2* force_d) {
@@ -701,21 +725,30 @@ void solve_frequencies_impl(nemoh_ctx* c, int nomega, const double* omegas, int 
     // host setup of each frequency (in the caller's order, which the NQ state
     // follows) overlapped with the assembly of the groups set up before it
     OmegaParams* hom = c->h_oms.as<OmegaParams>();
+    const int split = pipeline_split(c, nw);
     CK(cudaEventRecord(c->ev[0], c->stream));
     int done = 0;
     for (int i = 0; i < nw; ++i) {
       const double T = 2. * kPI / omegas[w0 + i];
       omega_params(c, 2. * kPI / T, hom[i], true);
-      if (i + 1 == nw || i + 1 - done >= ASM_GROUP) {
+      if (i + 1 == nw || i + 1 - done >= ASM_GROUP || i + 1 == split) {
         assemble_range(c, done, i + 1);
         done = i + 1;
+        if (done == split) {   // the first frequencies are assembled: factor them beside the rest
+          CK(cudaEventRecord(c->ev_pipe[0], c->stream));
+          CK(cudaStreamWaitEvent(c->stream2, c->ev_pipe[0], 0));
+          mixed_factor(c->mixed, c->d_D.as<double2>(), N, split * cls, c->d_status.as<int>(), c->stream2,
+                       c->launches, &c->lanes2, /*have_f32=*/true);
+          CK(cudaGetLastError());
+          CK(cudaEventRecord(c->ev_pipe[1], c->stream2));
+        }
       }
     }
     CK(cudaEventRecord(c->ev[1], c->stream));
     fold_rhs_kernel<<<dim3((N + 127) / 128, nrhs, nw), 128, 0, c->stream>>>(
         nvel_d + (long long)w0 * nrhs * cls * N, N, c->nsymy, nrhs, c->d_X.as<double2>());
     LAUNCHED(c);
-    factor_and_solve(c, nw * cls, nrhs, true, uniform_shape(c));
+    factor_and_solve(c, nw * cls, nrhs, true, uniform_shape(c), split * cls);
     CK(cudaEventRecord(c->ev[2], c->stream));
     potential(c, nw * cls, nrhs, uniform_shape(c));
     if (nint > 0) {
@@ -1093,6 +1126,13 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
       CK(cudaEventCreateWithFlags(&c->lanes.join[g], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&c->lanes.fork, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+    for (int g = 0; g < LANES; ++g) {
+      CK(cudaStreamCreateWithFlags(&c->lanes2.s[g], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->lanes2.join[g], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&c->lanes2.fork, cudaEventDisableTiming));
+    for (auto& e : c->ev_pipe) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CK(c->d_status.ensure(sizeof(int)));
     CK(cudaMemsetAsync(c->d_status.p, 0, sizeof(int), c->stream));
     c->mixed.status = c->d_status.as<int>();
@@ -1156,8 +1196,11 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
   if (!c) return NEMOH_B200_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (int g = 0; g < LANES; ++g)
+  for (int g = 0; g < LANES; ++g) {
     if (c->lanes.s[g]) cudaStreamSynchronize(c->lanes.s[g]);
+    if (c->lanes2.s[g]) cudaStreamSynchronize(c->lanes2.s[g]);
+  }
+  if (c->stream2) cudaStreamSynchronize(c->stream2);
   for (GraphEntry& g : c->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& e : c->ev)
@@ -1169,6 +1212,14 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
     if (c->lanes.s[g]) cudaStreamDestroy(c->lanes.s[g]);
   }
   if (c->lanes.fork) cudaEventDestroy(c->lanes.fork);
+  for (int g = 0; g < LANES; ++g) {
+    if (c->lanes2.join[g]) cudaEventDestroy(c->lanes2.join[g]);
+    if (c->lanes2.s[g]) cudaStreamDestroy(c->lanes2.s[g]);
+  }
+  if (c->lanes2.fork) cudaEventDestroy(c->lanes2.fork);
+  for (auto& e : c->ev_pipe)
+    if (e) cudaEventDestroy(e);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NEMOH_B200_OK;

@@ -1093,9 +1093,12 @@ constexpr long long FL_SPIN_LIMIT = 1LL << 21;
 
 inline size_t flow_ws_ints(int nsys, int nblk) { return 2 + (size_t)nsys * nblk; }
 
+// source blocks staged per wait (their solved blocks are loaded together)
+constexpr int FL_CHUNK = 4;
+
 template <class C2, int NR>
-constexpr int flow_smem() {   // source block, partial sums of the four quarters, right-hand-side block
-  return (TB * NR + 4 * TB * NR + TB * NR) * (int)sizeof(C2);
+constexpr int flow_smem() {   // staged source blocks (later the quarters' partial sums), rhs block, inverse block
+  return (FL_CHUNK * TB * NR + TB * NR + TB * TB) * (int)sizeof(C2);
 }
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -1126,12 +1129,14 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
                                                                int nsys, const C2* __restrict__ R, C2* Y,
                                                                long long xstride, int* ws, int* status,
                                                                const int* active) {
+  static_assert(FL_CHUNK >= 4, "the staging buffer also holds the four quarters' partial sums");
   if (active && *active == 0) return;   // a converged refinement skips its remaining passes
   extern __shared__ __align__(16) unsigned char fl_sm[];
-  C2* yb = reinterpret_cast<C2*>(fl_sm);           // [NR][TB] the source block being applied
-  C2* red = yb + TB * NR;                           // [4][NR][TB] partial sums of the column quarters
-  C2* rb = red + 4 * TB * NR;                       // [NR][TB] right-hand sides of the item's block
-  int* pre = reinterpret_cast<int*>(rb + TB * NR);  // [nblk + 1] items before each level
+  C2* yb = reinterpret_cast<C2*>(fl_sm);             // [FL_CHUNK][NR][TB] staged source blocks
+  C2* red = yb;                                       // [4][NR][TB] partial sums, after the sources
+  C2* rb = yb + FL_CHUNK * TB * NR;                   // [NR][TB] right-hand sides of the item's block
+  C2* Ts = rb + TB * NR;                              // [TB][TB] inverse of its diagonal block
+  int* pre = reinterpret_cast<int*>(Ts + TB * TB);    // [nblk + 1] items before each level
   __shared__ int s_item;
   const int t = threadIdx.x, r = t % TB, g = t / TB;
   // systems active at level l: those with more than l blocks, a prefix
@@ -1177,36 +1182,60 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
     const C2* Rs = R + sys * xstride;
     C2* Ys = Y + sys * xstride;
     int* fl = flags + (long long)sys * nblk;
+    // the item's right-hand sides and inverse block arrive while the sources are applied
+    const C2* Ti = inv + ((long long)sys * nblk + blk) * 2 * TB * TB + (LOWER ? 0 : TB * TB);
+    for (int e = t; e < TB * NR; e += FL_THREADS) {
+      const int i = e % TB, p = e / TB;
+      cp_async_elem(rb + e, i < nb ? Rs + (k0 + i) + (long long)n * p : Rs, i < nb);
+    }
+    for (int e = t; e < TB * TB; e += FL_THREADS) cp_async_elem(Ts + e, Ti + e, true);
+    asm volatile("cp.async.commit_group;" ::: "memory");
     C2 acc[NR];
 #pragma unroll
     for (int p = 0; p < NR; ++p) acc[p] = mkc<C2>(0., 0.);
     const int nsrc = LOWER ? blk : nbs - 1 - blk;
-#pragma unroll 1
-    for (int q = 0; q < nsrc; ++q) {
-      const int sb = LOWER ? q : nbs - 1 - q;   // sources in the order they are solved
-      const int c0 = sb * TB + g * FL_QUARTER;
-      C2 a[FL_QUARTER];
+    auto src = [&](int q) { return LOWER ? q : nbs - 1 - q; };   // sources in the order they are solved
+    auto load_row = [&](int q, C2* a) {   // this thread's 16 entries of the row block against source q
+      const int c0 = src(q) * TB + g * FL_QUARTER;
 #pragma unroll
       for (int j = 0; j < FL_QUARTER; ++j)
         a[j] = (r < nb && c0 + j < n) ? A[(k0 + r) + (long long)n * (c0 + j)] : mkc<C2>(0., 0.);
-      if (t == 0) flow_wait(fl + sb, ws + 1, status);
-      __syncthreads();   // the flag is seen, and every thread is done with yb
-      for (int e = t; e < TB * NR; e += FL_THREADS) {
-        const int i = e % TB, p = e / TB, row = sb * TB + i;
+    };
+    C2 an[FL_QUARTER];
+    if (nsrc > 0) load_row(0, an);
+#pragma unroll 1
+    for (int q0 = 0; q0 < nsrc; q0 += FL_CHUNK) {
+      const int nq = min(FL_CHUNK, nsrc - q0);
+      if (t == 0)
+        for (int qq = 0; qq < nq; ++qq) flow_wait(fl + src(q0 + qq), ws + 1, status);
+      __syncthreads();   // the flags are seen, and every thread is done with the previous chunk
+      for (int e = t; e < nq * TB * NR; e += FL_THREADS) {
+        const int qq = e / (TB * NR), m = e % (TB * NR), i = m % TB, p = m / TB;
+        const int row = src(q0 + qq) * TB + i;
         yb[e] = row < n ? __ldcg(Ys + row + (long long)n * p) : mkc<C2>(0., 0.);
       }
       __syncthreads();
+#pragma unroll 1
+      for (int qq = 0; qq < nq; ++qq) {
+        C2 a[FL_QUARTER];
 #pragma unroll
-      for (int j = 0; j < FL_QUARTER; ++j)
+        for (int j = 0; j < FL_QUARTER; ++j) a[j] = an[j];
+        if (q0 + qq + 1 < nsrc) load_row(q0 + qq + 1, an);   // the next source's entries in flight
+        const C2* y = yb + qq * TB * NR + g * FL_QUARTER;
 #pragma unroll
-        for (int p = 0; p < NR; ++p) cmac(acc[p], a[j], yb[(g * FL_QUARTER + j) + TB * p]);
+        for (int j = 0; j < FL_QUARTER; ++j)
+#pragma unroll
+          for (int p = 0; p < NR; ++p) cmac(acc[p], a[j], y[j + TB * p]);
+      }
     }
+    __syncthreads();   // the staged sources are no longer read: the buffer takes the partial sums
 #pragma unroll
     for (int p = 0; p < NR; ++p) red[(g * NR + p) * TB + r] = acc[p];
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     for (int e = t; e < TB * NR; e += FL_THREADS) {
       const int i = e % TB, p = e / TB;
-      C2 v = i < nb ? Rs[(k0 + i) + (long long)n * p] : mkc<C2>(0., 0.);
+      C2 v = rb[e];
 #pragma unroll
       for (int gg = 0; gg < 4; ++gg) {
         const C2 u = red[(gg * NR + p) * TB + i];
@@ -1217,16 +1246,16 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
     }
     __syncthreads();
     // y = inv(T_blk) rb, the inverse's columns split by quarters like the sources
-    const C2* Ti = inv + ((long long)sys * nblk + blk) * 2 * TB * TB + (LOWER ? 0 : TB * TB);
 #pragma unroll
     for (int p = 0; p < NR; ++p) acc[p] = mkc<C2>(0., 0.);
 #pragma unroll
     for (int j = 0; j < FL_QUARTER; ++j) {
       const int c = g * FL_QUARTER + j;
-      const C2 ti = Ti[r + TB * c];
+      const C2 ti = Ts[r + TB * c];
 #pragma unroll
       for (int p = 0; p < NR; ++p) cmac(acc[p], ti, rb[c + TB * p]);
     }
+    __syncthreads();   // every thread has read the partial sums it needed
 #pragma unroll
     for (int p = 0; p < NR; ++p) red[(g * NR + p) * TB + r] = acc[p];
     __syncthreads();
@@ -1254,10 +1283,10 @@ inline cudaError_t trsm_flow_nr(BatchT<C2> b, const C2* inv, const C2* R, C2* Y,
                                 cudaStream_t st, const int* active) {
   const int nblk = (b.n + TB - 1) / TB;
   const int smem = flow_smem<C2, NR>() + (nblk + 1) * (int)sizeof(int);
-  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  if (smem > 220 * 1024) return cudaErrorInvalidValue;
   auto kern = trsm_flow_kernel<C2, NR, LOWER>;
   static std::atomic<unsigned long long> attr{0};
-  once_per_device(attr, [kern] { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); });
+  once_per_device(attr, [kern] { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024); });
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -150,22 +150,29 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
 // rg: ragged batch (systems sorted by decreasing order, n the largest; the
 // FP32 copy in w.lu has the same element offsets as D); mat_elems: elements
 // of all matrices (for the conversion when the copy is not there yet)
+// sys0 (uniform batches): factor systems [sys0, sys0 + nsys) of the batch, in
+// their own slices of every per-system buffer, so that two ranges of one
+// batch can be factored on two streams at once
 inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches,
                          const Lanes* lanes = nullptr, bool have_f32 = false, const Ragged& rg = Ragged(),
-                         long long mat_elems = -1) {
+                         long long mat_elems = -1, int sys0 = 0) {
+  const size_t NN = (size_t)n * n, tiles = (size_t)(n + TC_T - 1) / TC_T;
+  const int nblk = (n + TB - 1) / TB;
+  float2* lu = w.lu + sys0 * NN;
   if (!have_f32) {
     const long long total = mat_elems >= 0 ? mat_elems : (long long)nsys * n * n;
-    d2f_kernel<<<1184, 256, 0, st>>>(D, w.lu, total);
+    d2f_kernel<<<1184, 256, 0, st>>>(D + sys0 * NN, lu, total);
     ++launches;
   }
-  BatchT<float2> b = make_batch<float2>(w.lu, n, w.diag, w.pinv, rg);
-  const size_t tiles = (size_t)(n + TC_T - 1) / TC_T;
+  BatchT<float2> b = make_batch<float2>(lu, n, w.diag + (size_t)sys0 * DIAG_SCRATCH,
+                                        w.pinv + (size_t)sys0 * PINV_SCRATCH, rg);
+  float2* inv = w.inv + (size_t)sys0 * nblk * 2 * TB * TB;
   lu_two_level<float2>(
       b, nsys, status, st, launches,
       [&](BatchT<float2> bg, int ns, cudaStream_t sg, int s0, int k0, int kend) {
         TcWork tg = w.tc;   // the group's slice of the operand images
-        tg.a += (size_t)s0 * tiles * TC_NCH * 2 * TC_AIMG;
-        tg.b += (size_t)s0 * tiles * TC_NCH * 2 * TC_BIMG;
+        tg.a += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_AIMG;
+        tg.b += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_BIMG;
         if (!tc_update(tg, bg, k0, ns, sg, launches, status)) {
           zgemm_update<float2>(bg, k0, kend - k0, Rect{kend, bg.n, kend, bg.n}, ns, sg);
           ++launches;
@@ -177,8 +184,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          inv_diag_smem<float2>());
   });
-  const int nblk = (n + TB - 1) / TB;
-  inv_diag_kernel<float2><<<dim3(nblk, 1, nsys), INV_THREADS, inv_diag_smem<float2>(), st>>>(b, w.inv, nblk);
+  inv_diag_kernel<float2><<<dim3(nblk, 1, nsys), INV_THREADS, inv_diag_smem<float2>(), st>>>(b, inv, nblk);
   ++launches;
 }
 
