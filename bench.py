@@ -696,6 +696,10 @@ def run_ours(args):
         "phase_ms": {"assemble": mx["phase"][0], "factor_refine": mx["phase"][1], "lu": mx["phase"][3],
                      "solve": mx["phase"][2]},
         "refinement": dict(zip(("iterations", "residual"), mx["refinement"])),
+        "sweep_choice": {"mixed": nb.sweep_choice(N, nomega * 2, NPROB, True)[0],
+                         "fp64": nb.sweep_choice(N, nomega * 2, NPROB, False)[0],
+                         "codes": "1-8: cluster sweep of that cluster size, 16: dataflow sweep"},
+        "pipeline": os.environ.get("NEMOH_B200_PIPELINE", "default"),
         "roofline": roofline_line(achieved, hbm, src, traffic, 80.0 * N * N, fp64),
         "e2e": {"value": whole_job_rate(world, nomega, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(pin_nvel.numel() * 8 + pin_nds.numel() * 8),

@@ -1126,9 +1126,13 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
       CK(cudaEventCreateWithFlags(&c->lanes.join[g], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&c->lanes.fork, cudaEventDisableTiming));
-    CK(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+    // the early LU of a pipelined batch runs at the highest stream priority:
+    // its latency-bound launches take SMs as the assembly's CTAs retire
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CK(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
     for (int g = 0; g < LANES; ++g) {
-      CK(cudaStreamCreateWithFlags(&c->lanes2.s[g], cudaStreamNonBlocking));
+      CK(cudaStreamCreateWithPriority(&c->lanes2.s[g], cudaStreamNonBlocking, prio_hi));
       CK(cudaEventCreateWithFlags(&c->lanes2.join[g], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&c->lanes2.fork, cudaEventDisableTiming));

@@ -16,6 +16,9 @@
 #pragma once
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace nb200 {
@@ -1137,7 +1140,7 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
   C2* rb = yb + FL_CHUNK * TB * NR;                   // [NR][TB] right-hand sides of the item's block
   C2* Ts = rb + TB * NR;                              // [TB][TB] inverse of its diagonal block
   int* pre = reinterpret_cast<int*>(Ts + TB * TB);    // [nblk + 1] items before each level
-  __shared__ int s_item;
+  __shared__ int s_item, s_nq;
   const int t = threadIdx.x, r = t % TB, g = t / TB;
   // systems active at level l: those with more than l blocks, a prefix
   for (int l = t; l < nblk; l += FL_THREADS) {
@@ -1204,11 +1207,18 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
     C2 an[FL_QUARTER];
     if (nsrc > 0) load_row(0, an);
 #pragma unroll 1
-    for (int q0 = 0; q0 < nsrc; q0 += FL_CHUNK) {
-      const int nq = min(FL_CHUNK, nsrc - q0);
-      if (t == 0)
-        for (int qq = 0; qq < nq; ++qq) flow_wait(fl + src(q0 + qq), ws + 1, status);
+    for (int q0 = 0, nq = 0; q0 < nsrc; q0 += nq) {
+      // a chunk: the next source (waited for), then the sources after it
+      // that are already solved, up to FL_CHUNK; the source an item waits on
+      // last is thus applied as soon as it is ready, with nothing held back
+      if (t == 0) {
+        flow_wait(fl + src(q0), ws + 1, status);
+        int m = 1;
+        while (m < FL_CHUNK && q0 + m < nsrc && ld_acquire(fl + src(q0 + m))) ++m;
+        s_nq = m;
+      }
       __syncthreads();   // the flags are seen, and every thread is done with the previous chunk
+      nq = s_nq;
       for (int e = t; e < nq * TB * NR; e += FL_THREADS) {
         const int qq = e / (TB * NR), m = e % (TB * NR), i = m % TB, p = m / TB;
         const int row = src(q0 + qq) * TB + i;
@@ -1287,11 +1297,25 @@ inline cudaError_t trsm_flow_nr(BatchT<C2> b, const C2* inv, const C2* R, C2* Y,
   auto kern = trsm_flow_kernel<C2, NR, LOWER>;
   static std::atomic<unsigned long long> attr{0};
   once_per_device(attr, [kern] { cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024); });
-  int dev = 0, sms = 0, per_sm = 0;
+  int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FL_THREADS, smem);
-  if (e != cudaSuccess) return e;
+  // resident CTAs per SM for this shared-memory size (one query per size and device)
+  static std::mutex mu;
+  static std::map<long long, int> occ;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const long long key = ((long long)dev << 32) | smem;
+    auto it = occ.find(key);
+    if (it != occ.end()) {
+      per_sm = it->second;
+    } else {
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FL_THREADS, smem);
+      if (e != cudaSuccess) return e;
+      occ[key] = per_sm;
+    }
+  }
   const long long items = (long long)nsys * nblk;
   const int grid = (int)std::max(1LL, std::min(items, (long long)std::max(1, sms) * std::max(1, per_sm)));
   kern<<<grid, FL_THREADS, smem, st>>>(b, inv, nblk, nsys, R, Y, (long long)b.n * NR, ws, status, active);

@@ -9,7 +9,8 @@
 // number of systems in the batch, their order, the precision and the number
 // of right-hand sides. The tuner times every candidate once per key (device,
 // element type, power-of-two buckets of the order, of the system count and
-// of the right-hand sides) on a copy of the batch's right-hand sides, keeps
+// of the right-hand sides), after one untimed run of it, on a copy of the
+// batch's right-hand sides, keeps
 // the fastest for the life of the process, and then solves with it. Under
 // stream capture (no timing possible) and before a key has been tuned without
 // scratch, trsm_sweep's default decides.
@@ -119,9 +120,16 @@ inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, i
   if (sync.ws) cands[nc++] = SWEEP_FLOW;
   for (int ci = 0; ci < nc; ++ci) {
     const int c = cands[ci];
+    long long l = 0;
+    // one untimed run first (first-launch setup on the host, cold caches),
+    // then the timed one
+    cudaMemcpyAsync(X, scratch, bytes, cudaMemcpyDeviceToDevice, st);
+    if (trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, l, active, c, sync) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
     cudaMemcpyAsync(X, scratch, bytes, cudaMemcpyDeviceToDevice, st);
     cudaEventRecord(ev[0], st);
-    long long l = 0;
     e = trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, l, active, c, sync);
     cudaEventRecord(ev[1], st);
     if (e != cudaSuccess) {   // e.g. a cluster that cannot be scheduled: not a candidate
