@@ -58,8 +58,9 @@ ASM_PROFILE = "profiles/assembly_counters_barge_4omega.md"
 def assembly_counters():
     """Per-pair counts of the assembly passes from the committed ncu summary:
     the line `counters:` holds key=value pairs (FP64 FLOP executed per (I, J)
-    pair and frequency by each pass and depth regime, DRAM bytes per pair of
-    both passes together). None when the summary is absent."""
+    pair by the Rankine pass of each depth regime, which runs once per call,
+    and by the wave pass of each regime per frequency; DRAM bytes per pair of
+    each). None when the summary is absent."""
     p = os.path.join(ROOT, ASM_PROFILE)
     if not os.path.exists(p):
         return None
@@ -73,7 +74,8 @@ def roofline_line(hbm_achieved, hbm_peak, hbm_src, traffic, alg_bytes, fp64):
     """The assembly passes' roofline: the binding roof is the FP64 pipe (their
     executed FP64 FLOP over the phase's time against the measured FMA peak);
     the HBM view beside it. Without the counters summary, the HBM view only."""
-    kernel = "rankine_kernel + wave_sym_kernel (influence-matrix assembly, FP64)"
+    kernel = ("rankine_cache_kernel (once per depth regime) + wave_sym_kernel (per frequency): "
+              "influence-matrix assembly, FP64")
     hbm_view = {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
                 "peak_source": hbm_src, "algorithmic_bytes_per_frequency": alg_bytes,
                 "traffic": traffic, "traffic_unit": "DRAM bytes per frequency (ncu counts per pair, " + ASM_PROFILE + ")"}
@@ -249,37 +251,93 @@ def single_gpu_extras(rank, world):
 
 
 def run_reference(args):
-    """--impl reference: the reference CPU algorithm on all host cores."""
+    """--impl reference: the reference CPU algorithm on all host cores.
+
+    Every timed step runs whole solves: one single-frequency case of the
+    workload per host thread (the frequencies of the 40-omega set in turn, so
+    the finite-depth / deep-water mix follows the workload's), each through
+    the oracle executable in the reference's own loop structure (`faithful`:
+    Green functions recomputed per problem, GAUSSZ inverse), all threads at
+    once. The step's rate is the sum over threads of 1 / (that thread's solve
+    time): every thread solving frequencies back to back. Warm-up steps run the
+    bounded per-core sample instead (a few seconds), which also gives the
+    extrapolated rate as a cross-check."""
     import multiprocessing as mp
+    import tempfile
+    import shutil
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from nemoh_b200 import cases as C
     case = C.config_barge(n_omega=N_OMEGA)
     cores = os.cpu_count() or 1
-    per_step = float(os.environ.get("NEMOH_REF_SAMPLE_S", "8"))
-    ctx = mp.get_context("spawn")
-    times = []
-    with ctx.Pool(cores) as pool:
-        for step in range(args.warmup + args.steps):
+    exe = os.path.join(ROOT, "oracle", "_build", "nemoh_oracle")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    tmp = tempfile.mkdtemp(prefix="nemoh_ref_")
+    try:
+        dirs = []
+        for i in range(cores):
+            c = C.config_barge(n_omega=N_OMEGA)
+            c.omegas = case.omegas[[i % N_OMEGA]]
+            d = os.path.join(tmp, "t%03d" % i)
+            C.write_case(c, d)
+            dirs.append((d, float(c.omegas[0])))
+        per_warm = float(os.environ.get("NEMOH_REF_SAMPLE_S", "4"))
+        ctx = mp.get_context("spawn")
+        est = []
+        with ctx.Pool(cores) as pool:
+            for _ in range(args.warmup):
+                res = pool.map(_ref_worker, [per_warm] * cores)
+                est.append(sum(r[0] for r in res))   # per-thread extrapolated solves/s, summed
+        steps = []
+        for _ in range(args.steps):
             t0 = time.time()
-            res = pool.map(_ref_worker, [per_step] * cores)
-            dt = time.time() - t0
-            if step >= args.warmup:
-                times.append((dt, res))
-    rates = [sum(r[0] for r in res) for _, res in times]   # cores run independent frequencies
+            done = [None] * cores
+            procs = [subprocess.Popen([exe, d, "faithful"], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+                     for d, _ in dirs]
+
+            def wait(i):
+                procs[i].wait()
+                done[i] = time.time() - t0
+
+            ths = [threading.Thread(target=wait, args=(i,)) for i in range(cores)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+            bad = [i for i, p in enumerate(procs) if p.returncode != 0]
+            if bad:
+                raise RuntimeError("oracle solve failed on thread %d: %s" % (bad[0], procs[bad[0]].stderr.read()))
+            steps.append(done)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    rates = [sum(1.0 / t for t in done) for done in steps]
     value = float(np.mean(rates))
+    kw = case.omegas ** 2 / case.g
+    fd = ~((case.depth == 0.0) | (kw * case.depth >= 20))
+    t_fd = [t for done in steps for i, t in enumerate(done) if fd[i % N_OMEGA]]
+    t_deep = [t for done in steps for i, t in enumerate(done) if not fd[i % N_OMEGA]]
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            model = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), "")
+    except OSError:
+        pass
+    sample = ("timed whole solves: per step one single-frequency case of the workload per host thread "
+              "(%d threads, %s), each the full faithful oracle solve at N=2400 with its 9 problems; "
+              "finite depth %.1f s and deep water %.1f s per solve (mean)"
+              % (cores, model or "cpu", float(np.mean(t_fd)) if t_fd else float("nan"),
+                 float(np.mean(t_deep)) if t_deep else float("nan")))
     line = {
         "impl": "reference", "metric": "BEM solves/s (mixed vs FP64 GPU, rel err<=1e-6) at N=2400; serve p50/p99 ms",
         "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": float(np.mean([t for t, _ in times])) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": float(np.mean([max(d) for d in steps])) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "barge 100x20x10 m, depth 50 m, half mesh N=2400 (y-symmetric), 40 omega x 9 problems",
                    "n_panels": 2400, "omegas": N_OMEGA, "problems_per_omega": NPROB},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": "per core per step: whole rows of Green evaluations and the first GAUSSZ "
-                                   "elimination steps at N=2400 for one finite-depth and one deep-water omega "
-                                   "(%.0f s), extrapolated by operation counts to the 40-omega workload" % per_step},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample,
+                         "extrapolated_cross_check": float(np.mean(est)) if est else None},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -671,11 +729,15 @@ def run_ours(args):
     fp64 = {"peak_tflops": fp64_peak,
             "peak_source": "measured in this run (nemoh_b200_diag_fp64_peak: FMA chains on every SM)"}
     traffic = None
-    if cnt:
-        pairs = N * N
-        flop = pairs * (n_fd * (cnt["rankine_fd_flop"] + cnt["wave_fd_flop"]) +
-                        (nomega - n_fd) * (cnt["rankine_deep_flop"] + cnt["wave_deep_flop"]))
-        traffic = pairs * (n_fd * cnt["fd_dram_bytes"] + (nomega - n_fd) * cnt["deep_dram_bytes"]) / nomega
+    keys = ("rankine_fd_flop", "rankine_deep_flop", "wave_fd_flop", "wave_deep_flop", "rankine_dram_bytes",
+            "wave_fd_dram_bytes", "wave_deep_dram_bytes")
+    if cnt and all(k in cnt for k in keys):
+        # per step: the Rankine part once per depth regime met, the wave pass per frequency
+        pairs, n_deep = N * N, nomega - n_fd
+        flop = pairs * ((n_fd > 0) * cnt["rankine_fd_flop"] + (n_deep > 0) * cnt["rankine_deep_flop"] +
+                        n_fd * cnt["wave_fd_flop"] + n_deep * cnt["wave_deep_flop"])
+        traffic = pairs * (((n_fd > 0) + (n_deep > 0)) * cnt["rankine_dram_bytes"] + n_fd * cnt["wave_fd_dram_bytes"]
+                           + n_deep * cnt["wave_deep_dram_bytes"]) / nomega
         ach = flop / (asm_ms / 1e3) / 1e12
         fp64.update({"achieved_tflops": ach, "frac": ach / fp64_peak if fp64_peak else None,
                      "flop_source": "FP64 instructions (DFMA x2, DADD, DMUL) per pair executed by the current "
@@ -699,7 +761,7 @@ def run_ours(args):
         "sweep_choice": {"mixed": nb.sweep_choice(N, nomega * 2, NPROB, True)[0],
                          "fp64": nb.sweep_choice(N, nomega * 2, NPROB, False)[0],
                          "codes": "1-8: cluster sweep of that cluster size, 16: dataflow sweep"},
-        "pipeline": os.environ.get("NEMOH_B200_PIPELINE", "default"),
+        "pipeline_pct": int(os.environ.get("NEMOH_B200_PIPELINE", "0")),
         "roofline": roofline_line(achieved, hbm, src, traffic, 80.0 * N * N, fp64),
         "e2e": {"value": whole_job_rate(world, nomega, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(pin_nvel.numel() * 8 + pin_nds.numel() * 8),

@@ -693,16 +693,18 @@ void potential(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
 // frequencies whose host setup is done before their assembly is launched
 constexpr int ASM_GROUP = 8;
 
-// Pipelined batch (mixed precision): the FP32 LU of the first frequencies of
-// a batch runs on stream2 while the main stream assembles the rest, so the
-// LU's latency-bound launches fill the SMs the FP64-bound assembly leaves
-// between its CTAs. Returns the number of frequencies factored early (0: no
-// pipeline). NEMOH_B200_PIPELINE = percentage of the batch (default 50, 0
-// turns it off).
+// Pipelined batch (mixed precision, off unless NEMOH_B200_PIPELINE gives the
+// percentage of the batch): the FP32 LU of the first frequencies runs on
+// stream2 (highest priority) while the main stream assembles the rest.
+// Returns the number of frequencies factored early (0: no pipeline).
+// Measured on the barge workload it is slower (76.3 against 74.0 ms per
+// 40-frequency step at 50%; the two-sphere step 389 against 386 ms): the
+// assembly keeps every SM's FP64 pipe busy, so the LU's CTAs only take time
+// from it, and the LU of each half alone is as latency-bound as the whole.
 int pipeline_split(const nemoh_ctx* c, int nw) {
   static const int pct = [] {
     const char* e = std::getenv("NEMOH_B200_PIPELINE");
-    const int v = e ? std::atoi(e) : 50;
+    const int v = e ? std::atoi(e) : 0;
     return std::max(0, std::min(90, v));
   }();
   if (c->mode != NEMOH_B200_MIXED || nw < 2 || pct == 0) return 0;
