@@ -251,57 +251,108 @@ def single_gpu_extras(rank, world):
 
 
 def run_reference(args):
-    """--impl reference: the reference CPU algorithm on all host cores.
+    """--impl reference: the reference CPU algorithm on all host threads.
 
-    Every timed step runs whole solves: one single-frequency case of the
-    workload per host thread (the frequencies of the 40-omega set in turn, so
-    the finite-depth / deep-water mix follows the workload's), each through
-    the oracle executable in the reference's own loop structure (`faithful`:
-    Green functions recomputed per problem, GAUSSZ inverse), all threads at
-    once. The step's rate is the sum over threads of 1 / (that thread's solve
-    time): every thread solving frequencies back to back. Warm-up steps run the
-    bounded per-core sample instead (a few seconds), which also gives the
-    extrapolated rate as a cross-check."""
+    Default (a run of a few minutes): every step runs on every host thread
+    the bounded per-core sample of `cpu_sample` (whole rows of Green
+    evaluations and the first GAUSSZ elimination steps for one finite-depth and
+    one deep-water frequency, timed, and extrapolated by operation counts to
+    the 40-frequency workload); the step's rate is the sum over threads.
+
+    --whole-solves: every timed step runs whole solves instead, one
+    single-frequency case of the workload per host thread (the frequencies
+    spread over the 40-frequency set, so the finite-depth / deep-water mix
+    follows the workload's), each through the oracle executable in the
+    reference's own loop structure (`faithful`), all threads at once; the
+    step's rate is the sum over threads of 1 / (that thread's solve time).
+    A whole solve takes minutes per thread, so this form is for a measurement
+    run, not for the default."""
     import multiprocessing as mp
-    import tempfile
-    import shutil
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from nemoh_b200 import cases as C
     case = C.config_barge(n_omega=N_OMEGA)
     cores = os.cpu_count() or 1
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            model = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), "")
+    except OSError:
+        pass
+    per_step = float(os.environ.get("NEMOH_REF_SAMPLE_S", "8"))
+    ctx = mp.get_context("spawn")
+    times = []
+    whole = None
+    with ctx.Pool(cores) as pool:
+        for step in range(args.warmup + (0 if args.whole_solves else args.steps)):
+            t0 = time.time()
+            res = pool.map(_ref_worker, [per_step] * cores)
+            if step >= args.warmup:
+                times.append((time.time() - t0, sum(r[0] for r in res)))
+    if args.whole_solves:
+        whole = whole_solves(case, cores, args.steps)
+        times = [(max(d), sum(1.0 / t for t in d)) for d in whole["steps"]]
+    value = float(np.mean([r for _, r in times]))
+    if whole:
+        sample = ("timed whole solves: per step one single-frequency case of the workload per host thread "
+                  "(%d threads, %s), each the full faithful oracle solve at N=2400 with its 9 problems; "
+                  "finite depth %.1f s and deep water %.1f s per solve (mean over threads)"
+                  % (cores, model or "cpu", whole["t_fd"], whole["t_deep"]))
+    else:
+        sample = ("per thread per step (%d threads, %s): whole rows of Green evaluations and the first GAUSSZ "
+                  "elimination steps at N=2400 for one finite-depth and one deep-water omega (%.0f s), timed and "
+                  "extrapolated by operation counts to the 40-omega workload; --whole-solves times whole "
+                  "solves instead" % (cores, model or "cpu", per_step))
+    line = {
+        "impl": "reference", "metric": "BEM solves/s (mixed vs FP64 GPU, rel err<=1e-6) at N=2400; serve p50/p99 ms",
+        "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.mean([t for t, _ in times])) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "barge 100x20x10 m, depth 50 m, half mesh N=2400 (y-symmetric), 40 omega x 9 problems",
+                   "n_panels": 2400, "omegas": N_OMEGA, "problems_per_omega": NPROB},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def whole_solves(case, threads, steps):
+    """`steps` rounds of whole faithful oracle solves, one single-frequency
+    case per host thread at once (frequency i * 40 / threads for thread i);
+    returns each round's per-thread solve times and the mean finite-depth and
+    deep-water times."""
+    import tempfile
+    import shutil
+    from nemoh_b200 import cases as C
     exe = os.path.join(ROOT, "oracle", "_build", "nemoh_oracle")
     if not os.path.exists(exe):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    kw = case.omegas ** 2 / case.g
+    fd = ~((case.depth == 0.0) | (kw * case.depth >= 20))
+    pick = [i * N_OMEGA // threads for i in range(threads)] if threads < N_OMEGA else \
+        [i % N_OMEGA for i in range(threads)]
     tmp = tempfile.mkdtemp(prefix="nemoh_ref_")
+    rounds = []
     try:
         dirs = []
-        for i in range(cores):
+        for i, w in enumerate(pick):
             c = C.config_barge(n_omega=N_OMEGA)
-            c.omegas = case.omegas[[i % N_OMEGA]]
+            c.omegas = case.omegas[[w]]
             d = os.path.join(tmp, "t%03d" % i)
             C.write_case(c, d)
-            dirs.append((d, float(c.omegas[0])))
-        per_warm = float(os.environ.get("NEMOH_REF_SAMPLE_S", "4"))
-        ctx = mp.get_context("spawn")
-        est = []
-        with ctx.Pool(cores) as pool:
-            for _ in range(args.warmup):
-                res = pool.map(_ref_worker, [per_warm] * cores)
-                est.append(sum(r[0] for r in res))   # per-thread extrapolated solves/s, summed
-        steps = []
-        for _ in range(args.steps):
+            dirs.append(d)
+        for _ in range(steps):
             t0 = time.time()
-            done = [None] * cores
+            done = [None] * threads
             procs = [subprocess.Popen([exe, d, "faithful"], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
-                     for d, _ in dirs]
+                     for d in dirs]
 
             def wait(i):
                 procs[i].wait()
                 done[i] = time.time() - t0
 
-            ths = [threading.Thread(target=wait, args=(i,)) for i in range(cores)]
+            ths = [threading.Thread(target=wait, args=(i,)) for i in range(threads)]
             for t in ths:
                 t.start()
             for t in ths:
@@ -309,38 +360,13 @@ def run_reference(args):
             bad = [i for i, p in enumerate(procs) if p.returncode != 0]
             if bad:
                 raise RuntimeError("oracle solve failed on thread %d: %s" % (bad[0], procs[bad[0]].stderr.read()))
-            steps.append(done)
+            rounds.append(done)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
-    rates = [sum(1.0 / t for t in done) for done in steps]
-    value = float(np.mean(rates))
-    kw = case.omegas ** 2 / case.g
-    fd = ~((case.depth == 0.0) | (kw * case.depth >= 20))
-    t_fd = [t for done in steps for i, t in enumerate(done) if fd[i % N_OMEGA]]
-    t_deep = [t for done in steps for i, t in enumerate(done) if not fd[i % N_OMEGA]]
-    model = ""
-    try:
-        with open("/proc/cpuinfo") as f:
-            model = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), "")
-    except OSError:
-        pass
-    sample = ("timed whole solves: per step one single-frequency case of the workload per host thread "
-              "(%d threads, %s), each the full faithful oracle solve at N=2400 with its 9 problems; "
-              "finite depth %.1f s and deep water %.1f s per solve (mean)"
-              % (cores, model or "cpu", float(np.mean(t_fd)) if t_fd else float("nan"),
-                 float(np.mean(t_deep)) if t_deep else float("nan")))
-    line = {
-        "impl": "reference", "metric": "BEM solves/s (mixed vs FP64 GPU, rel err<=1e-6) at N=2400; serve p50/p99 ms",
-        "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": float(np.mean([max(d) for d in steps])) * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "barge 100x20x10 m, depth 50 m, half mesh N=2400 (y-symmetric), 40 omega x 9 problems",
-                   "n_panels": 2400, "omegas": N_OMEGA, "problems_per_omega": NPROB},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample,
-                         "extrapolated_cross_check": float(np.mean(est)) if est else None},
-        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line))
+    t_fd = [t for d in rounds for i, t in enumerate(d) if fd[pick[i]]]
+    t_deep = [t for d in rounds for i, t in enumerate(d) if not fd[pick[i]]]
+    return {"steps": rounds, "t_fd": float(np.mean(t_fd)) if t_fd else float("nan"),
+            "t_deep": float(np.mean(t_deep)) if t_deep else float("nan")}
 
 
 def _ref_worker(seconds):
@@ -814,6 +840,8 @@ def main():
                     help="comma list of the workloads beside the headline to run")
     ap.add_argument("--bodies", type=int, default=256, help="bodies of the batched and serving workloads")
     ap.add_argument("--requests", type=int, default=10000, help="requests per serving rate")
+    ap.add_argument("--whole-solves", action="store_true",
+                    help="--impl reference: time whole faithful oracle solves (minutes per step)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
