@@ -153,9 +153,20 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
 // sys0 (uniform batches): factor systems [sys0, sys0 + nsys) of the batch, in
 // their own slices of every per-system buffer, so that two ranges of one
 // batch can be factored on two streams at once
+// ahead: look-ahead streams (lu_two_level): the outer update of the next
+// panel's columns stays on the group's stream, the rest goes to ahead.s as
+// one-tile-per-CTA launches (NEMOH_B200_LOOKAHEAD=2: the persistent form)
+inline int lookahead_mode() {
+  static const int m = [] {
+    const char* e = std::getenv("NEMOH_B200_LOOKAHEAD");
+    return e ? std::atoi(e) : 1;
+  }();
+  return m;
+}
+
 inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches,
                          const Lanes* lanes = nullptr, bool have_f32 = false, const Ragged& rg = Ragged(),
-                         long long mat_elems = -1, int sys0 = 0) {
+                         long long mat_elems = -1, int sys0 = 0, const AheadLanes* ahead = nullptr) {
   const size_t NN = (size_t)n * n, tiles = (size_t)(n + TC_T - 1) / TC_T;
   const int nblk = (n + TB - 1) / TB;
   float2* lu = w.lu + sys0 * NN;
@@ -169,16 +180,26 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   float2* inv = w.inv + (size_t)sys0 * nblk * 2 * TB * TB;
   lu_two_level<float2>(
       b, nsys, status, st, launches,
-      [&](BatchT<float2> bg, int ns, cudaStream_t sg, int s0, int k0, int kend) {
+      [&](BatchT<float2> bg, int ns, cudaStream_t sg, int s0, int k0, int kend, const Ahead& ah) {
         TcWork tg = w.tc;   // the group's slice of the operand images
         tg.a += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_AIMG;
         tg.b += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_BIMG;
-        if (!tc_update(tg, bg, k0, ns, sg, launches, status)) {
+        if (!tc_enabled()) {
           zgemm_update<float2>(bg, k0, kend - k0, Rect{kend, bg.n, kend, bg.n}, ns, sg);
           ++launches;
+        } else if (!ah.s) {
+          tc_update(tg, bg, k0, ns, sg, launches, status);
+        } else {
+          // the next panel's columns now, the rest beside the next panel's steps
+          tc_prep(tg, bg, k0, ns, sg, launches);
+          tc_apply(tg, bg, k0, ns, sg, launches, status, 0, 1, tc_persistent());
+          cudaEventRecord(ah.start, sg);
+          cudaStreamWaitEvent(ah.s, ah.start, 0);
+          tc_apply(tg, bg, k0, ns, ah.s, launches, status, 1, -1, lookahead_mode() == 2);
+          cudaEventRecord(ah.done, ah.s);
         }
       },
-      lanes, rg.host_ord);
+      lanes, rg.host_ord, (ahead && lookahead_mode() > 0 && tc_enabled()) ? ahead : nullptr);
   static std::atomic<unsigned long long> attr{0};
   once_per_device(attr, [] {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,

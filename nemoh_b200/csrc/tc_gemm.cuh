@@ -256,13 +256,13 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
                                                            const unsigned char* __restrict__ abuf,
                                                            const unsigned char* __restrict__ bbuf,
                                                            long long sys_bytes_a, long long sys_bytes_b, int* status,
-                                                           uint32_t idesc) {
+                                                           uint32_t idesc, int tj0) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * TC_STAGE);   // full[2], empty[2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
   __shared__ int s_ok;
   const int n = b.order(blockIdx.z), r1 = k0 + LU_OUTER, rest = n - r1;
-  const int tcol = blockIdx.x, trow = blockIdx.y;
+  const int tcol = blockIdx.x + tj0, trow = blockIdx.y;   // column tiles [tj0, tj0 + gridDim.x)
   // a ragged batch's smaller systems leave the tiles beyond their order
   // (uniform per CTA, before any barrier or tensor-memory allocation)
   if (rest <= 0 || tcol * TC_T >= rest || trow * TC_T >= rest) return;
@@ -428,7 +428,7 @@ constexpr int TCP_SMEM = TCP_STAGES * TC_STAGE + 256;
 
 __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     BatchT<float2> b, int k0, const unsigned char* __restrict__ abuf, const unsigned char* __restrict__ bbuf,
-    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc) {
+    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc, int tj0, int ntc) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TCP_STAGES * TC_STAGE);
   // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the TMEM address
@@ -438,13 +438,14 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[TCP_STAGES]);
   const uint32_t accf0 = smem_u32(&bars[2 * TCP_STAGES]), acce0 = smem_u32(&bars[2 * TCP_STAGES + 2]);
   const int r1 = k0 + LU_OUTER;
-  const long long total = (long long)nt * nt * nsys;
-  // tile t: system z, row tile trow, column tile tcol; false beyond a ragged system's order
+  const long long total = (long long)nt * ntc * nsys;
+  // tile t: system z, row tile trow, column tile tcol in [tj0, tj0 + ntc);
+  // false beyond a ragged system's order
   auto tile = [&](long long t, int& z, int& trow, int& tcol) {
-    z = (int)(t / ((long long)nt * nt));
-    const int rem = (int)(t % ((long long)nt * nt));
-    trow = rem / nt;
-    tcol = rem % nt;
+    z = (int)(t / ((long long)nt * ntc));
+    const int rem = (int)(t % ((long long)nt * ntc));
+    trow = rem / ntc;
+    tcol = tj0 + rem % ntc;
     const int rest = b.order(z) - r1;
     return rest > 0 && trow * TC_T < rest && tcol * TC_T < rest;
   };
@@ -644,26 +645,36 @@ inline bool tc_enabled() {
   return on;
 }
 
-// outer trailing update after the panel [k0, k0+128); false if disabled
-inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
-                      int* status) {
-  if (!tc_enabled()) return false;
+// operand images of the outer update after the panel [k0, k0+128)
+inline void tc_prep(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches) {
   const int n = b.n, rest = n - k0 - LU_OUTER;
-  if (rest <= 0) return true;
-  static std::atomic<unsigned long long> attr{0};
-  once_per_device(attr, [] {
-    cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-  });
+  if (rest <= 0) return;
   const int t = (n + TC_T - 1) / TC_T;
   const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
   const int nt = (rest + TC_T - 1) / TC_T;
   const int per = (nt * TC_T * TC_NCH + 127) / 128;
-  const bool f16 = tc_split_f16();
-  if (f16) tc_prep_kernel<true><<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
+  if (tc_split_f16()) tc_prep_kernel<true><<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
   else tc_prep_kernel<false><<<dim3(2 * per, 1, nsys), 128, 0, st>>>(b, k0, w.a, w.b, sa, sb, per);
   ++launches;
-  const uint32_t idesc = tc_idesc(f16);
-  if (tc_persistent()) {
+}
+
+// The update of the column tiles [tj0, tj0 + ntc) (ntc < 0: to the last) of
+// the trailing matrix from the images tc_prep wrote; persistent: one CTA per
+// SM walking the tiles (the default form), else one tile per CTA (CTAs that
+// retire tile by tile, so launches of higher-priority streams get SMs
+// between them).
+inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
+                     int* status, int tj0, int ntc, bool persistent) {
+  const int n = b.n, rest = n - k0 - LU_OUTER;
+  if (rest <= 0) return;
+  const int t = (n + TC_T - 1) / TC_T;
+  const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
+  const int nt = (rest + TC_T - 1) / TC_T;
+  if (ntc < 0) ntc = nt - tj0;
+  ntc = std::min(ntc, nt - tj0);
+  if (ntc <= 0) return;
+  const uint32_t idesc = tc_idesc(tc_split_f16());
+  if (persistent) {
     static std::atomic<unsigned long long> attr2{0};
     static int sms = 0;
     once_per_device(attr2, [] {
@@ -672,14 +683,26 @@ inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     });
-    const long long tiles = (long long)nt * nt * nsys;
+    const long long tiles = (long long)nt * ntc * nsys;
     const int grid = (int)std::min<long long>(tiles, sms > 0 ? sms : 148);
     tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, nt, nsys, status,
-                                                                     idesc);
+                                                                     idesc, tj0, ntc);
   } else {
-    tc_update_kernel<<<dim3(nt, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status, idesc);
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+      cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    });
+    tc_update_kernel<<<dim3(ntc, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status, idesc, tj0);
   }
   ++launches;
+}
+
+// outer trailing update after the panel [k0, k0+128); false if disabled
+inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
+                      int* status) {
+  if (!tc_enabled()) return false;
+  tc_prep(w, b, k0, nsys, st, launches);
+  tc_apply(w, b, k0, nsys, st, launches, status, 0, -1, tc_persistent());
   return true;
 }
 
