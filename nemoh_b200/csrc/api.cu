@@ -133,7 +133,6 @@ struct nemoh_ctx {
   int cap_slots = 0, cap_nrhs = 0, cap_nfa = 0, cap_cls = 0;   // what ensure_batch last provided
   MixedWork mixed;
   Lanes lanes;               // side streams for groups of systems in the LU and triangular solves
-  AheadLanes ahead;          // lower-priority streams of the FP32 LU's look-ahead (bulk trailing updates)
   // pipelined batches: the first frequencies' FP32 LU on stream2 (with its own
   // lanes) while the main stream assembles the rest
   cudaStream_t stream2 = nullptr;
@@ -535,7 +534,7 @@ void factor_fp64(nemoh_ctx* c, int nsys, const Shape& sh) {
   });
   lu_two_level<double2>(
       b, nsys, c->d_status.as<int>(), c->stream, c->launches,
-      [&](Batch bg, int ns, cudaStream_t sg, int, int k0, int kend, const Ahead&) {
+      [&](Batch bg, int ns, cudaStream_t sg, int, int k0, int kend) {
         zgemm_update<double2>(bg, k0, kend - k0, Rect{kend, bg.n, kend, bg.n}, ns, sg);
         ++c->launches;
       },
@@ -660,7 +659,7 @@ void factor_and_solve(nemoh_ctx* c, int nsys, int nrhs, bool have_rhs, const Sha
   CK(cudaEventRecord(c->ev_lu[0], c->stream));
   if (c->mode == NEMOH_B200_MIXED) {
     mixed_factor(c->mixed, c->d_D.as<double2>(), sh.n, nsys - pre, c->d_status.as<int>(), c->stream, c->launches,
-                 &c->lanes, /*have_f32=*/true, sh.rg, -1, pre, &c->ahead);
+                 &c->lanes, /*have_f32=*/true, sh.rg, -1, pre);
     if (pre) CK(cudaStreamWaitEvent(c->stream, c->ev_pipe[1], 0));
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev_lu[1], c->stream));
@@ -949,7 +948,7 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
     c->lu64 = !mixed;
     if (mixed) {
       mixed_factor(c->mixed, c->d_D.as<double2>(), nmax, nsys, c->d_status.as<int>(), c->stream, c->launches,
-                   &c->lanes, /*have_f32=*/true, sh.rg, -1, 0, &c->ahead);
+                   &c->lanes, /*have_f32=*/true, sh.rg);
       const RefineArgs a{c->d_D.as<double2>(), nmax, nsys, nrhs, c->d_X.as<double2>(), sh.rg};
       mixed_refine_begin(c->mixed, a, max_it, c->stream, c->launches);
       mixed_refine_passes(c->mixed, a, passes, c->stream, c->launches);
@@ -1124,19 +1123,15 @@ int nemoh_b200_create(nemoh_ctx** out, int device, int precision_mode) {
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) CK(cudaEventCreate(&e));
     for (auto& e : c->ev_lu) CK(cudaEventCreate(&e));
-    // The LU's groups run at the highest stream priority and its look-ahead
-    // bulk updates at the lowest: as the bulk's CTAs retire, the panels'
-    // latency-bound launches take the SMs first.
-    int prio_lo = 0, prio_hi = 0;
-    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     for (int g = 0; g < LANES; ++g) {
-      CK(cudaStreamCreateWithPriority(&c->lanes.s[g], cudaStreamNonBlocking, prio_hi));
+      CK(cudaStreamCreateWithFlags(&c->lanes.s[g], cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&c->lanes.join[g], cudaEventDisableTiming));
-      CK(cudaStreamCreateWithPriority(&c->ahead.s[g], cudaStreamNonBlocking, prio_lo));
-      CK(cudaEventCreateWithFlags(&c->ahead.start[g], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&c->ahead.done[g], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&c->lanes.fork, cudaEventDisableTiming));
+    // the early LU of a pipelined batch runs at the highest stream priority:
+    // its latency-bound launches take SMs as the assembly's CTAs retire
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     CK(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
     for (int g = 0; g < LANES; ++g) {
       CK(cudaStreamCreateWithPriority(&c->lanes2.s[g], cudaStreamNonBlocking, prio_hi));
@@ -1210,7 +1205,6 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
   for (int g = 0; g < LANES; ++g) {
     if (c->lanes.s[g]) cudaStreamSynchronize(c->lanes.s[g]);
     if (c->lanes2.s[g]) cudaStreamSynchronize(c->lanes2.s[g]);
-    if (c->ahead.s[g]) cudaStreamSynchronize(c->ahead.s[g]);
   }
   if (c->stream2) cudaStreamSynchronize(c->stream2);
   for (GraphEntry& g : c->graphs)
@@ -1229,11 +1223,6 @@ int nemoh_b200_destroy(nemoh_ctx* c) {
     if (c->lanes2.s[g]) cudaStreamDestroy(c->lanes2.s[g]);
   }
   if (c->lanes2.fork) cudaEventDestroy(c->lanes2.fork);
-  for (int g = 0; g < LANES; ++g) {
-    if (c->ahead.start[g]) cudaEventDestroy(c->ahead.start[g]);
-    if (c->ahead.done[g]) cudaEventDestroy(c->ahead.done[g]);
-    if (c->ahead.s[g]) cudaStreamDestroy(c->ahead.s[g]);
-  }
   for (auto& e : c->ev_pipe)
     if (e) cudaEventDestroy(e);
   if (c->stream2) cudaStreamDestroy(c->stream2);

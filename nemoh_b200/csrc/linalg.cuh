@@ -454,20 +454,6 @@ struct Lanes {
   cudaEvent_t fork = nullptr, join[LANES] = {};
 };
 
-// Look-ahead of the FP32 LU: per group, a lower-priority stream that takes
-// the bulk of each outer trailing update while the group's own stream
-// factors the next panel, and the events that order the two.
-struct Ahead {
-  cudaStream_t s = nullptr;        // null: no look-ahead
-  cudaEvent_t start = nullptr;     // recorded on the group's stream when the bulk may start
-  cudaEvent_t done = nullptr;      // recorded on s when the bulk has finished
-};
-struct AheadLanes {
-  cudaStream_t s[LANES] = {};
-  cudaEvent_t start[LANES] = {}, done[LANES] = {};
-  Ahead at(int g) const { return s[g] ? Ahead{s[g], start[g], done[g]} : Ahead(); }
-};
-
 struct LaneSplit {
   int groups = 1;
   int first[LANES + 1] = {};
@@ -515,24 +501,15 @@ inline BatchT<C2> sub_batch(const BatchT<C2>& b, int s0) {
   return r;
 }
 
-// outer(bsub, nsub, stream, s0, k0, kend, ahead): trailing update of one
-// group. host_ord (ragged batches): the systems' orders on the host, in
-// decreasing order; at every step only the systems still above it are
-// launched (a prefix of each group) and the grids are sized by the group's
-// largest system.
-// ahead (row-strip form only, b.pinv): look-ahead streams. outer() may then
-// leave the update of the columns right of the next panel to ahead.s, with
-// ahead.done recorded after it; this loop makes the group's stream wait for
-// it before the next row strip (the first use of those columns), so the next
-// panel's own steps run beside it.
+// outer(bsub, nsub, stream, s0, k0, kend): trailing update of one group.
+// host_ord (ragged batches): the systems' orders on the host, in decreasing
+// order; at every step only the systems still above it are launched (a prefix
+// of each group) and the grids are sized by the group's largest system.
 template <class C2, class Outer>
 inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main, long long& launches, Outer outer,
-                         const Lanes* lanes = nullptr, const int* host_ord = nullptr,
-                         const AheadLanes* ahead = nullptr) {
+                         const Lanes* lanes = nullptr, const int* host_ord = nullptr) {
   const int n = b.n;
   const LaneSplit L = lane_split(nsys, main, lanes);
-  if (!b.pinv) ahead = nullptr;
-  bool pending[LANES] = {};
   // systems of group g whose order exceeds k
   auto active = [&](int g, int k) {
     const int s0 = L.first[g], s1 = L.first[g + 1];
@@ -581,7 +558,6 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
       BatchT<C2> bg = sub_batch(b, s0);
       bg.n = ng;
       const cudaStream_t st = L.st[g];
-      if (pending[g]) cudaStreamWaitEvent(st, ahead->done[g], 0);   // the previous bulk update is done
       if (b.pinv) {
         static std::atomic<unsigned long long> attr{0};
         once_per_device(attr, [] {
@@ -590,13 +566,9 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
         strip_kernel<C2><<<dim3((ng - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
         ++launches;
       }
-      const Ahead ah = ahead ? ahead->at(g) : Ahead();
-      outer(bg, ns, st, s0, k0, kend, ah);
-      if (ah.s) pending[g] = true;
+      outer(bg, ns, st, s0, k0, kend);
     }
   }
-  for (int g = 0; g < L.groups; ++g)
-    if (pending[g]) cudaStreamWaitEvent(L.st[g], ahead->done[g], 0);
   lane_join(L, main, lanes);
 }
 

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "linalg.cuh"
@@ -146,6 +147,15 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
   if ((threadIdx.x & 31) == 0) atomicMax(out + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
+// merged outer updates of panel pairs (NEMOH_B200_TC_MERGE=0 turns them off)
+inline bool tc_merge() {
+  static const bool on = [] {
+    const char* e = std::getenv("NEMOH_B200_TC_MERGE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // have_f32: the assembly already wrote the FP32 copy of D into w.lu
 // rg: ragged batch (systems sorted by decreasing order, n the largest; the
 // FP32 copy in w.lu has the same element offsets as D); mat_elems: elements
@@ -153,20 +163,9 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
 // sys0 (uniform batches): factor systems [sys0, sys0 + nsys) of the batch, in
 // their own slices of every per-system buffer, so that two ranges of one
 // batch can be factored on two streams at once
-// ahead: look-ahead streams (lu_two_level): the outer update of the next
-// panel's columns stays on the group's stream, the rest goes to ahead.s as
-// one-tile-per-CTA launches (NEMOH_B200_LOOKAHEAD=2: the persistent form)
-inline int lookahead_mode() {
-  static const int m = [] {
-    const char* e = std::getenv("NEMOH_B200_LOOKAHEAD");
-    return e ? std::atoi(e) : 1;
-  }();
-  return m;
-}
-
 inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status, cudaStream_t st, long long& launches,
                          const Lanes* lanes = nullptr, bool have_f32 = false, const Ragged& rg = Ragged(),
-                         long long mat_elems = -1, int sys0 = 0, const AheadLanes* ahead = nullptr) {
+                         long long mat_elems = -1, int sys0 = 0) {
   const size_t NN = (size_t)n * n, tiles = (size_t)(n + TC_T - 1) / TC_T;
   const int nblk = (n + TB - 1) / TB;
   float2* lu = w.lu + sys0 * NN;
@@ -178,28 +177,51 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   BatchT<float2> b = make_batch<float2>(lu, n, w.diag + (size_t)sys0 * DIAG_SCRATCH,
                                         w.pinv + (size_t)sys0 * PINV_SCRATCH, rg);
   float2* inv = w.inv + (size_t)sys0 * nblk * 2 * TB * TB;
+  // Merged outer updates (persistent tensor-core form): after an even panel
+  // whose next panel still has columns beyond it, only the next panel's
+  // columns (all rows) and the next panel's rows (the columns beyond) are
+  // updated; the rest of the trailing matrix takes both panels' products in
+  // the next panel's update (K = 256), so each pair of panels reads and
+  // writes the bulk of A22 once. deferred: per group (by its first system),
+  // the image set holding the deferred panel's images, or -1.
+  const bool merge = tc_enabled() && tc_persistent() && tc_merge();
+  std::map<int, int> deferred;
   lu_two_level<float2>(
       b, nsys, status, st, launches,
-      [&](BatchT<float2> bg, int ns, cudaStream_t sg, int s0, int k0, int kend, const Ahead& ah) {
-        TcWork tg = w.tc;   // the group's slice of the operand images
-        tg.a += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_AIMG;
-        tg.b += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_BIMG;
+      [&](BatchT<float2> bg, int ns, cudaStream_t sg, int s0, int k0, int kend) {
+        // the group's slice of each image set
+        auto slice = [&](int set) {
+          TcWork tg = w.tc.set(set);
+          tg.a += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_AIMG;
+          tg.b += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_BIMG;
+          return tg;
+        };
         if (!tc_enabled()) {
           zgemm_update<float2>(bg, k0, kend - k0, Rect{kend, bg.n, kend, bg.n}, ns, sg);
           ++launches;
-        } else if (!ah.s) {
+          return;
+        }
+        const int set = (k0 / LU_OUTER) & 1;
+        TcWork tg = slice(set);
+        if (!merge) {
           tc_update(tg, bg, k0, ns, sg, launches, status);
+          return;
+        }
+        auto it = deferred.find(s0);
+        tc_prep(tg, bg, k0, ns, sg, launches);
+        if (it != deferred.end() && it->second >= 0) {   // this panel's update and the deferred one
+          const TcWork prev = slice(it->second);
+          tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles(), true, &prev);
+          it->second = -1;
+        } else if (kend + LU_OUTER < bg.n) {   // the next panel has columns beyond it: defer the bulk
+          tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles{0, -1, 0, 1}, true);
+          tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles{0, 1, 1, -1}, true);
+          deferred[s0] = set;
         } else {
-          // the next panel's columns now, the rest beside the next panel's steps
-          tc_prep(tg, bg, k0, ns, sg, launches);
-          tc_apply(tg, bg, k0, ns, sg, launches, status, 0, 1, tc_persistent());
-          cudaEventRecord(ah.start, sg);
-          cudaStreamWaitEvent(ah.s, ah.start, 0);
-          tc_apply(tg, bg, k0, ns, ah.s, launches, status, 1, -1, lookahead_mode() == 2);
-          cudaEventRecord(ah.done, ah.s);
+          tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles(), true);
         }
       },
-      lanes, rg.host_ord, (ahead && lookahead_mode() > 0 && tc_enabled()) ? ahead : nullptr);
+      lanes, rg.host_ord);
   static std::atomic<unsigned long long> attr{0};
   once_per_device(attr, [] {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -47,11 +47,20 @@ constexpr int TC_SMEM = 2 * TC_STAGE + 128;
 constexpr int TC_TMEM_COLS = 2 * TC_T;          // accumulator: Re in [0,128), Im in [128,256)
 constexpr int ST_TC_TIMEOUT = 30;
 
+// Operand images of two outer updates (two sets: the update of one panel may
+// be merged into the next panel's, and both panels' images are then read).
 struct TcWork {
-  unsigned char* a = nullptr;   // A images: nsys x ceil(n/128) row tiles x TC_NCH chunks x (hi, lo)
-  unsigned char* b = nullptr;   // B images: nsys x ceil(n/128) column tiles x TC_NCH chunks x (hi, lo)
+  unsigned char* a = nullptr;   // A images: 2 sets x nsys x ceil(n/128) row tiles x TC_NCH chunks x (hi, lo)
+  unsigned char* b = nullptr;   // B images: 2 sets x nsys x ceil(n/128) column tiles x TC_NCH chunks x (hi, lo)
   size_t have_a = 0, have_b = 0;
   size_t bytes() const { return have_a + have_b; }
+  // the images of set s (0 or 1), each set half of the allocation
+  TcWork set(int s) const {
+    TcWork w = *this;
+    w.a += s * (have_a / 2);
+    w.b += s * (have_b / 2);
+    return w;
+  }
   void release() {
     cudaFree(a);
     cudaFree(b);
@@ -60,7 +69,7 @@ struct TcWork {
   }
   cudaError_t ensure(int nsys, int n) {
     const size_t t = (size_t)(n + TC_T - 1) / TC_T;
-    const size_t na = nsys * t * TC_NCH * 2 * TC_AIMG, nb = nsys * t * TC_NCH * 2 * TC_BIMG;
+    const size_t na = 2 * nsys * t * TC_NCH * 2 * TC_AIMG, nb = 2 * nsys * t * TC_NCH * 2 * TC_BIMG;
     cudaError_t e;
     if (na > have_a) {
       cudaFree(a);
@@ -81,7 +90,7 @@ struct TcWork {
 };
 
 inline size_t tc_bytes_per_system(size_t n) {
-  return ((n + TC_T - 1) / TC_T) * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG);
+  return 2 * ((n + TC_T - 1) / TC_T) * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG);
 }
 
 // byte offset of the 16-byte core-matrix row (row, k-group g) in an image
@@ -256,13 +265,14 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
                                                            const unsigned char* __restrict__ abuf,
                                                            const unsigned char* __restrict__ bbuf,
                                                            long long sys_bytes_a, long long sys_bytes_b, int* status,
-                                                           uint32_t idesc, int tj0) {
+                                                           uint32_t idesc, int ti0, int tj0) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * TC_STAGE);   // full[2], empty[2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
   __shared__ int s_ok;
   const int n = b.order(blockIdx.z), r1 = k0 + LU_OUTER, rest = n - r1;
-  const int tcol = blockIdx.x + tj0, trow = blockIdx.y;   // column tiles [tj0, tj0 + gridDim.x)
+  // column tiles [tj0, tj0 + gridDim.x), row tiles [ti0, ti0 + gridDim.y)
+  const int tcol = blockIdx.x + tj0, trow = blockIdx.y + ti0;
   // a ragged batch's smaller systems leave the tiles beyond their order
   // (uniform per CTA, before any barrier or tensor-memory allocation)
   if (rest <= 0 || tcol * TC_T >= rest || trow * TC_T >= rest) return;
@@ -428,7 +438,8 @@ constexpr int TCP_SMEM = TCP_STAGES * TC_STAGE + 256;
 
 __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     BatchT<float2> b, int k0, const unsigned char* __restrict__ abuf, const unsigned char* __restrict__ bbuf,
-    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc, int tj0, int ntc) {
+    long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc, int ti0, int nti,
+    int tj0, int ntc, const unsigned char* __restrict__ pabuf, const unsigned char* __restrict__ pbbuf) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TCP_STAGES * TC_STAGE);
   // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the TMEM address
@@ -438,13 +449,15 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[TCP_STAGES]);
   const uint32_t accf0 = smem_u32(&bars[2 * TCP_STAGES]), acce0 = smem_u32(&bars[2 * TCP_STAGES + 2]);
   const int r1 = k0 + LU_OUTER;
-  const long long total = (long long)nt * ntc * nsys;
-  // tile t: system z, row tile trow, column tile tcol in [tj0, tj0 + ntc);
-  // false beyond a ragged system's order
+  const long long total = (long long)nti * ntc * nsys;
+  // chunks per tile: the previous panel's images first (a merged update), then this panel's
+  const int nch = pabuf ? 2 * TC_NCH : TC_NCH;
+  // tile t: system z, row tile trow in [ti0, ti0 + nti), column tile tcol in
+  // [tj0, tj0 + ntc); false beyond a ragged system's order
   auto tile = [&](long long t, int& z, int& trow, int& tcol) {
-    z = (int)(t / ((long long)nt * ntc));
-    const int rem = (int)(t % ((long long)nt * ntc));
-    trow = rem / ntc;
+    z = (int)(t / ((long long)nti * ntc));
+    const int rem = (int)(t % ((long long)nti * ntc));
+    trow = ti0 + rem / ntc;
     tcol = tj0 + rem % ntc;
     const int rest = b.order(z) - r1;
     return rest > 0 && trow * TC_T < rest && tcol * TC_T < rest;
@@ -483,14 +496,18 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     for (long long t = blockIdx.x; t < total && ok && !s_err; t += gridDim.x) {
       int z, trow, tcol;
       if (!tile(t, z, trow, tcol)) continue;
-      const unsigned char* ga = abuf + z * sys_bytes_a + (long long)trow * TC_NCH * 2 * TC_AIMG;
-      const unsigned char* gb = bbuf + z * sys_bytes_b + (long long)tcol * TC_NCH * 2 * TC_BIMG;
-      for (int c = 0; c < TC_NCH; ++c) {
+      for (int c = 0; c < nch; ++c) {
+        // the previous panel's tiles are one tile further: its trailing block starts 128 earlier
+        const bool prev = pabuf && c < TC_NCH;
+        const int cc = c % TC_NCH, off = prev ? 1 : 0;
+        const unsigned char* ga = (prev ? pabuf : abuf) + z * sys_bytes_a +
+                                  ((long long)(trow + off) * TC_NCH + cc) * 2 * TC_AIMG;
+        const unsigned char* gb = (prev ? pbbuf : bbuf) + z * sys_bytes_b +
+                                  ((long long)(tcol + off) * TC_NCH + cc) * 2 * TC_BIMG;
         const int q = (int)(g % TCP_STAGES);
         const long long r = g / TCP_STAGES;
         if (r > 0 && !(ok = mbar_wait(empty0 + 8 * q, (uint32_t)((r - 1) & 1)))) break;
-        tc_load_chunk(s0 + q * TC_STAGE, ga + (long long)c * 2 * TC_AIMG, gb + (long long)c * 2 * TC_BIMG,
-                      full0 + 8 * q);
+        tc_load_chunk(s0 + q * TC_STAGE, ga, gb, full0 + 8 * q);
         ++g;
       }
     }
@@ -511,7 +528,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
       if (u > 0 && !(ok = mbar_wait(acce0 + 8 * buf, (uint32_t)((u - 1) & 1)))) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t tm = tmem + (uint32_t)(buf * TC_TMEM_COLS);
-      for (int c = 0; c < TC_NCH; ++c) {
+      for (int c = 0; c < nch; ++c) {
         const int q = (int)(g % TCP_STAGES);
         if (!(ok = mbar_wait(full0 + 8 * q, (uint32_t)((g / TCP_STAGES) & 1)))) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -658,23 +675,30 @@ inline void tc_prep(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t 
   ++launches;
 }
 
-// The update of the column tiles [tj0, tj0 + ntc) (ntc < 0: to the last) of
-// the trailing matrix from the images tc_prep wrote; persistent: one CTA per
-// SM walking the tiles (the default form), else one tile per CTA (CTAs that
-// retire tile by tile, so launches of higher-priority streams get SMs
-// between them).
+// A rectangle of tiles of the trailing matrix: row tiles [ti0, ti0 + nti),
+// column tiles [tj0, tj0 + ntc) (a count < 0: to the last tile)
+struct TcTiles {
+  int ti0 = 0, nti = -1, tj0 = 0, ntc = -1;
+};
+
+// The update of a rectangle of tiles of the trailing matrix from the images
+// tc_prep wrote; persistent: one CTA per SM walking the tiles (the default
+// form), else one tile per CTA. prev (persistent form only): the images of
+// the previous panel, whose update of these tiles was deferred and is merged
+// here (K = 256 in one accumulation: one read-modify-write of the tiles for
+// two panels).
 inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
-                     int* status, int tj0, int ntc, bool persistent) {
+                     int* status, TcTiles tl, bool persistent, const TcWork* prev = nullptr) {
   const int n = b.n, rest = n - k0 - LU_OUTER;
   if (rest <= 0) return;
   const int t = (n + TC_T - 1) / TC_T;
   const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
   const int nt = (rest + TC_T - 1) / TC_T;
-  if (ntc < 0) ntc = nt - tj0;
-  ntc = std::min(ntc, nt - tj0);
-  if (ntc <= 0) return;
+  const int nti = std::min(tl.nti < 0 ? nt - tl.ti0 : tl.nti, nt - tl.ti0);
+  const int ntc = std::min(tl.ntc < 0 ? nt - tl.tj0 : tl.ntc, nt - tl.tj0);
+  if (nti <= 0 || ntc <= 0) return;
   const uint32_t idesc = tc_idesc(tc_split_f16());
-  if (persistent) {
+  if (persistent || prev) {
     static std::atomic<unsigned long long> attr2{0};
     static int sms = 0;
     once_per_device(attr2, [] {
@@ -683,16 +707,18 @@ inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     });
-    const long long tiles = (long long)nt * ntc * nsys;
+    const long long tiles = (long long)nti * ntc * nsys;
     const int grid = (int)std::min<long long>(tiles, sms > 0 ? sms : 148);
-    tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, nt, nsys, status,
-                                                                     idesc, tj0, ntc);
+    tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(
+        b, k0, w.a, w.b, sa, sb, nt, nsys, status, idesc, tl.ti0, nti, tl.tj0, ntc, prev ? prev->a : nullptr,
+        prev ? prev->b : nullptr);
   } else {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
       cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
     });
-    tc_update_kernel<<<dim3(ntc, nt, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status, idesc, tj0);
+    tc_update_kernel<<<dim3(ntc, nti, nsys), 128, TC_SMEM, st>>>(b, k0, w.a, w.b, sa, sb, status, idesc, tl.ti0,
+                                                                 tl.tj0);
   }
   ++launches;
 }
@@ -702,7 +728,7 @@ inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_
                       int* status) {
   if (!tc_enabled()) return false;
   tc_prep(w, b, k0, nsys, st, launches);
-  tc_apply(w, b, k0, nsys, st, launches, status, 0, -1, tc_persistent());
+  tc_apply(w, b, k0, nsys, st, launches, status, TcTiles(), tc_persistent());
   return true;
 }
 

@@ -381,6 +381,62 @@ def test_one_tile_per_cta_tensor_core_update(tmp_path):
         assert float(line[2]) < 1e-6 and 0 < int(line[4]) <= 6, line
 
 
+def test_merged_outer_updates_match_separate_ones(tmp_path):
+    """Mixed-precision LU with the outer updates of panel pairs merged (the
+    default) and with one update per panel (NEMOH_B200_TC_MERGE=0, a child
+    process: the switch is read once per process), on orders with 3 and 5
+    outer panels and a ragged batch of both: the refinement converges in the
+    same few passes without any FP64 fallback (a wrong factor would still give
+    right answers through the fallback, so its count is checked), and the
+    forces agree within 1e-10 of the largest force."""
+    import subprocess
+    import sys
+    script = tmp_path / "merge.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        "sys.path[:0] = %r\n"
+        "import gpu_cases as G, nemoh_b200 as nb\n"
+        "from nemoh_b200 import cases as C\n"
+        "cyl = C.config_cylinder(n_omega=3)\n"
+        "sph = C.Case(C.hemisphere_mesh(3.0, 16, 40, jitter=0.2, rng=np.random.default_rng(7)),\n"
+        "             np.array([0.5, 1.1, 1.7]), np.array([0.0]), C.six_dofs(), C.six_dofs(), depth=0.0)\n"
+        "res = {}\n"
+        "for case in (cyl, sph):\n"
+        "    nvel, nds, npb = G.problems(case)\n"
+        "    with nb.Solver(0, nb.MIXED) as s:\n"
+        "        s.set_case(case)\n"
+        "        res[case.name] = s.solve_frequencies(case.omegas, nvel, nds)\n"
+        "        res['it_' + case.name] = np.array(s.last_refinement()[0])\n"
+        "        res['fb_' + case.name] = np.array(s.fallback_count())\n"
+        "body = np.array([0, 1, 1, 0]); om = np.array([0.6, 0.9, 1.3, 1.9])\n"
+        "nv = [C.body_conditions(C.Case((cyl, sph)[b].mesh, np.array([w]), np.array([20.0]), (cyl, sph)[b].rad,\n"
+        "                               (cyl, sph)[b].force, depth=(cyl, sph)[b].depth)) for b, w in zip(body, om)]\n"
+        "with nb.Solver(0, nb.MIXED) as s:\n"
+        "    for c in (cyl, sph):\n"
+        "        s.add_body(c)\n"
+        "    for i, f in enumerate(s.solve_bodies(body, om, nv)):\n"
+        "        res['bodies_%%d' %% i] = f\n"
+        "    res['fb_bodies'] = np.array(s.fallback_count())\n"
+        "np.savez(sys.argv[1], **res)\n"
+        % [str(p) for p in (B.HERE + "/..", B.HERE + "/../tests")])
+    got = {}
+    for form, env in (("merged", {}), ("separate", {"NEMOH_B200_TC_MERGE": "0"})):
+        out = tmp_path / (form + ".npz")
+        r = subprocess.run([sys.executable, str(script), str(out)], env=dict(os.environ, **env),
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        got[form] = dict(np.load(out))
+    a, b = got["merged"], got["separate"]
+    for k in a:
+        if k.startswith("fb_"):
+            assert tuple(a[k]) == (0, 0) and tuple(b[k]) == (0, 0), (k, a[k], b[k])
+        elif k.startswith("it_"):
+            assert 0 < int(a[k]) <= 4 and abs(int(a[k]) - int(b[k])) <= 1, (k, a[k], b[k])
+        else:
+            scale = np.abs(b[k]).max()
+            assert np.abs(a[k] - b[k]).max() <= 1e-10 * scale, (k, np.abs(a[k] - b[k]).max() / scale)
+
+
 def test_dataflow_and_cluster_sweeps_agree(tmp_path):
     """The two triangular sweeps, each forced in a child process
     (NEMOH_B200_SWEEP is read once per process): FP64 forces agree within
