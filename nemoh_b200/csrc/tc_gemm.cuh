@@ -640,6 +640,18 @@ inline bool tc_persistent() {
   return on;
 }
 
+// CTAs of the persistent update (one per SM): NEMOH_B200_TC_SMS caps them
+// below the SM count, leaving SMs to the LU's latency-bound launches of the
+// other stream groups (the update is HBM-bound, so fewer SMs may stream A22
+// as fast)
+inline int tc_grid_cap(int sms) {
+  static const int cap = [] {
+    const char* e = std::getenv("NEMOH_B200_TC_SMS");
+    return e ? std::atoi(e) : 0;
+  }();
+  return cap > 0 ? std::min(cap, sms) : sms;
+}
+
 // operand split: BF16 terms unless NEMOH_B200_TC_SPLIT=f16 (FP16 terms).
 // Measured on the barge workload (40 frequencies, N=2400): the FP16 split did
 // not make the refinement converge sooner (4 passes to a relative residual of
@@ -708,7 +720,7 @@ inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     });
     const long long tiles = (long long)nti * ntc * nsys;
-    const int grid = (int)std::min<long long>(tiles, sms > 0 ? sms : 148);
+    const int grid = (int)std::min<long long>(tiles, tc_grid_cap(sms > 0 ? sms : 148));
     tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(
         b, k0, w.a, w.b, sa, sb, nt, nsys, status, idesc, tl.ti0, nti, tl.tj0, ntc, prev ? prev->a : nullptr,
         prev ? prev->b : nullptr);
