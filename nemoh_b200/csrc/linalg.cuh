@@ -16,6 +16,7 @@
 #pragma once
 #include <cooperative_groups.h>
 
+#include <cstdlib>
 #include <map>
 #include <mutex>
 
@@ -460,6 +461,16 @@ struct LaneSplit {
   cudaStream_t st[LANES] = {};
 };
 
+// stream groups in use: LANES, or fewer with NEMOH_B200_LANES (1..LANES)
+inline int lane_count() {
+  static const int n = [] {
+    const char* e = std::getenv("NEMOH_B200_LANES");
+    const int v = e ? std::atoi(e) : LANES;
+    return std::max(1, std::min(LANES, v));
+  }();
+  return n;
+}
+
 inline LaneSplit lane_split(int nsys, cudaStream_t main, const Lanes* lanes) {
   LaneSplit L;
   if (!lanes || !lanes->s[0] || nsys < 2) {
@@ -469,7 +480,7 @@ inline LaneSplit lane_split(int nsys, cudaStream_t main, const Lanes* lanes) {
     L.st[0] = main;
     return L;
   }
-  L.groups = std::min(LANES, nsys);   // every group holds at least one system
+  L.groups = std::min(lane_count(), nsys);   // every group holds at least one system
   for (int g = 0; g <= L.groups; ++g) L.first[g] = (int)((long long)nsys * g / L.groups);
   cudaEventRecord(lanes->fork, main);
   for (int g = 0; g < L.groups; ++g) {
@@ -510,6 +521,13 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
                          const Lanes* lanes = nullptr, const int* host_ord = nullptr) {
   const int n = b.n;
   const LaneSplit L = lane_split(nsys, main, lanes);
+  // NEMOH_B200_OUTER_JOIN=1: the groups join for each outer update, which
+  // then covers every system in one launch
+  static const bool join_env = [] {
+    const char* e = std::getenv("NEMOH_B200_OUTER_JOIN");
+    return e && e[0] == '1';
+  }();
+  const bool join_outer = join_env && L.groups > 1;
   // systems of group g whose order exceeds k
   auto active = [&](int g, int k) {
     const int s0 = L.first[g], s1 = L.first[g + 1];
@@ -566,7 +584,21 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
         strip_kernel<C2><<<dim3((ng - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
         ++launches;
       }
-      outer(bg, ns, st, s0, k0, kend);
+      if (!join_outer) outer(bg, ns, st, s0, k0, kend);
+    }
+    if (join_outer) {   // one trailing update for every group, then the groups go on
+      const int ng = host_ord ? host_ord[0] : n;
+      const int kend = std::min(k0 + LU_OUTER, ng);
+      int ns = 0;
+      for (int g = 0; g < L.groups; ++g) ns = std::max(ns, L.first[g] + active(g, k0));
+      if (kend < ng && ns > 0) {
+        lane_join(L, main, lanes);
+        BatchT<C2> bw = b;
+        bw.n = ng;
+        outer(bw, ns, main, 0, k0, kend);
+        cudaEventRecord(lanes->fork, main);
+        for (int g = 0; g < L.groups; ++g) cudaStreamWaitEvent(L.st[g], lanes->fork, 0);
+      }
     }
   }
   lane_join(L, main, lanes);
