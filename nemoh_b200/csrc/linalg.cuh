@@ -17,6 +17,7 @@
 #include <cooperative_groups.h>
 
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 
@@ -66,7 +67,10 @@ inline BatchT<C2> make_batch(C2* base, int n, C2* diag, C2* pinv, const Ragged& 
 }
 constexpr int DIAG_SCRATCH = 3 * LU_NB * LU_NB;
 constexpr int LU_OUTER = 128;
-constexpr int PINV_SCRATCH = (LU_OUTER / LU_NB) * LU_NB * LU_NB;
+// per system: inv(L) of the current outer panel's LU_OUTER / LU_NB diagonal
+// blocks, then inv(L11) of the whole panel (LU_OUTER x LU_OUTER, column-major)
+constexpr int PINV_DIAG = (LU_OUTER / LU_NB) * LU_NB * LU_NB;
+constexpr int PINV_SCRATCH = PINV_DIAG + LU_OUTER * LU_OUTER;
 using Batch = BatchT<double2>;
 
 template <class C2> __device__ __forceinline__ C2 mkc(double x, double y);
@@ -441,6 +445,124 @@ __global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
   }
 }
 
+// The row strip as a product, U[k0:kend, kend:n] = W A[k0:kend, kend:n] with
+// W = inv(L11) formed once per panel and system (strip_winv_kernel): the
+// strip's blocks no longer wait on one another, so every block of W a CTA
+// needs can be in flight at once.
+//
+// strip_winv_kernel: one CTA per system, thread = element (r, c) of a 32 x 32
+// block. Column block j of W: W_jj = inv(L_jj) (from lu_diag), then for the
+// blocks below W_ij = -inv(L_ii) sum_{k=j}^{i-1} L_ik W_kj.
+constexpr int SW_BLK = LU_OUTER / LU_NB;
+template <class C2>
+constexpr int strip_winv_smem() {
+  return (SW_BLK * LU_NB * LU_NB + LU_NB * LU_NB) * (int)sizeof(C2);   // one column block of W, the sum S
+}
+template <class C2>
+__global__ void __launch_bounds__(LU_NB * LU_NB) strip_winv_kernel(BatchT<C2> b, int k0) {
+  extern __shared__ __align__(16) unsigned char sw_sm[];
+  C2* Wc = reinterpret_cast<C2*>(sw_sm);   // [SW_BLK][LU_NB][LU_NB] column block j of W, column-major blocks
+  C2* S = Wc + SW_BLK * LU_NB * LU_NB;     // [LU_NB][LU_NB]
+  const int n = b.order(blockIdx.z);
+  if (k0 + LU_OUTER >= n) return;
+  const C2* A = b.sys(blockIdx.z);
+  const C2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
+  C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_DIAG;
+  const int r = threadIdx.x % LU_NB, c = threadIdx.x / LU_NB, e = r + LU_NB * c;
+  for (int j = 0; j < SW_BLK; ++j) {
+    Wc[j * LU_NB * LU_NB + e] = P[j * LU_NB * LU_NB + e];
+    for (int i = j + 1; i < SW_BLK; ++i) {
+      __syncthreads();   // W_kj for k < i are in shared memory
+      C2 acc = mkc<C2>(0., 0.);
+      for (int k = j; k < i; ++k) {
+        const C2* L = A + (k0 + i * LU_NB + r) + (long long)n * (k0 + k * LU_NB);
+        const C2* Wk = Wc + k * LU_NB * LU_NB + LU_NB * c;
+#pragma unroll 8
+        for (int m = 0; m < LU_NB; ++m) cmac(acc, L[(long long)n * m], Wk[m]);
+      }
+      S[e] = acc;
+      __syncthreads();
+      const C2* Pi = P + i * LU_NB * LU_NB;
+      C2 w = mkc<C2>(0., 0.);
+#pragma unroll 8
+      for (int m = 0; m < LU_NB; ++m) cmac(w, Pi[r + LU_NB * m], S[m + LU_NB * c]);
+      Wc[i * LU_NB * LU_NB + e] = mkc<C2>(-w.x, -w.y);
+    }
+    __syncthreads();
+    for (int i = j; i < SW_BLK; ++i) W[(i * LU_NB + r) + LU_OUTER * (j * LU_NB + c)] = Wc[i * LU_NB * LU_NB + e];
+    __syncthreads();
+  }
+}
+
+// strip_gemm_kernel: CTA = one system and ST_C columns of the strip (held in
+// shared memory, column-major, ld LU_OUTER); thread = (row i of a block, every
+// fourth column). The ten nonzero 32 x 32 blocks of W stream through two
+// shared buffers (cp.async, the next one in flight while the current one is
+// applied); output block ib = sum_{jb <= ib} W_ib,jb X_jb goes straight to A.
+template <class C2>
+constexpr int strip_gemm_smem() {
+  return (LU_OUTER * ST_C + 2 * LU_NB * LU_NB) * (int)sizeof(C2);
+}
+template <class C2>
+__global__ void __launch_bounds__(128) strip_gemm_kernel(BatchT<C2> b, int k0) {
+  extern __shared__ __align__(16) unsigned char sg_sm[];
+  C2* X = reinterpret_cast<C2*>(sg_sm);   // [ST_C][LU_OUTER] the strip before the solve
+  C2* Wb = X + LU_OUTER * ST_C;           // [2][LU_NB][LU_NB] blocks of W, column-major
+  const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
+  const int c0 = kend + blockIdx.x * ST_C, ncol = min(ST_C, n - c0);
+  if (ncol <= 0) return;
+  C2* A = b.sys(blockIdx.z);
+  const C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_DIAG;
+  // block step s -> (ib, jb): (0,0), (1,0), (1,1), (2,0), ...
+  auto blk = [](int s, int& ib, int& jb) {
+    ib = 0;
+    while ((ib + 1) * (ib + 2) / 2 <= s) ++ib;
+    jb = s - ib * (ib + 1) / 2;
+  };
+  auto fetch = [&](int s) {
+    int ib, jb;
+    blk(s, ib, jb);
+    C2* dst = Wb + (s & 1) * LU_NB * LU_NB;
+    for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) {
+      const int rr = q % LU_NB, cc = q / LU_NB;
+      cp_async_elem(dst + q, W + (ib * LU_NB + rr) + LU_OUTER * (jb * LU_NB + cc), true);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  fetch(0);
+  for (int q = threadIdx.x; q < LU_OUTER * ST_C; q += blockDim.x) {
+    const int rr = q % LU_OUTER, cc = q / LU_OUTER;
+    X[q] = cc < ncol ? A[(k0 + rr) + (long long)n * (c0 + cc)] : mkc<C2>(0., 0.);
+  }
+  const int i = threadIdx.x & (LU_NB - 1), g = threadIdx.x / LU_NB;
+  constexpr int GROUPS = 128 / LU_NB, CPT = ST_C / GROUPS, NSTEP = SW_BLK * (SW_BLK + 1) / 2;
+  C2 acc[CPT];
+  for (int s = 0; s < NSTEP; ++s) {
+    int ib, jb;
+    blk(s, ib, jb);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();   // block s has landed; every thread is done with block s - 1
+    if (s + 1 < NSTEP) fetch(s + 1);
+    if (jb == 0) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
+    }
+    const C2* T = Wb + (s & 1) * LU_NB * LU_NB;
+    for (int j = 0; j < LU_NB; ++j) {
+      const C2 t = T[i + LU_NB * j];
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) cmac(acc[m], t, X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + j]);
+    }
+    if (jb == ib) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) {
+        const int c = g + GROUPS * m;
+        if (c < ncol) A[(k0 + ib * LU_NB + i) + (long long)n * (c0 + c)] = acc[m];
+      }
+    }
+  }
+}
+
 // Systems split into groups factored side by side on separate streams: the
 // launches of a step are issued group after group, so the latency-bound
 // kernels of one group (diagonal blocks, panels, small updates) overlap the
@@ -461,6 +583,16 @@ struct LaneSplit {
   cudaStream_t st[LANES] = {};
 };
 
+// row strips as W = inv(L11) times the strip (default), or by the blocked
+// forward solve with NEMOH_B200_STRIP=solve
+inline bool strip_as_product() {
+  static const bool on = [] {
+    const char* e = std::getenv("NEMOH_B200_STRIP");
+    return !(e && std::strcmp(e, "solve") == 0);
+  }();
+  return on;
+}
+
 // stream groups in use: LANES, or fewer with NEMOH_B200_LANES (1..LANES)
 inline int lane_count() {
   static const int n = [] {
@@ -473,7 +605,7 @@ inline int lane_count() {
 
 inline LaneSplit lane_split(int nsys, cudaStream_t main, const Lanes* lanes) {
   LaneSplit L;
-  if (!lanes || !lanes->s[0] || nsys < 2) {
+  if (!lanes || !lanes->s[0] || nsys < 2 || lane_count() < 2) {   // one group: the caller's stream
     L.groups = 1;
     L.first[0] = 0;
     L.first[1] = nsys;
@@ -580,9 +712,20 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
         static std::atomic<unsigned long long> attr{0};
         once_per_device(attr, [] {
           cudaFuncSetAttribute(strip_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_smem<C2>());
+          cudaFuncSetAttribute(strip_winv_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               strip_winv_smem<C2>());
+          cudaFuncSetAttribute(strip_gemm_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               strip_gemm_smem<C2>());
         });
-        strip_kernel<C2><<<dim3((ng - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_smem<C2>(), st>>>(bg, k0);
-        ++launches;
+        const dim3 sgrid((ng - kend + ST_C - 1) / ST_C, 1, ns);
+        if (strip_as_product()) {
+          strip_winv_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
+          strip_gemm_kernel<C2><<<sgrid, 128, strip_gemm_smem<C2>(), st>>>(bg, k0);
+          launches += 2;
+        } else {
+          strip_kernel<C2><<<sgrid, 128, strip_smem<C2>(), st>>>(bg, k0);
+          ++launches;
+        }
       }
       if (!join_outer) outer(bg, ns, st, s0, k0, kend);
     }
