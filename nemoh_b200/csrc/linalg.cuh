@@ -455,42 +455,51 @@ __global__ void __launch_bounds__(128) strip_kernel(BatchT<C2> b, int k0) {
 // blocks below W_ij = -inv(L_ii) sum_{k=j}^{i-1} L_ik W_kj.
 constexpr int SW_BLK = LU_OUTER / LU_NB;
 template <class C2>
-constexpr int strip_winv_smem() {
-  return (SW_BLK * LU_NB * LU_NB + LU_NB * LU_NB) * (int)sizeof(C2);   // one column block of W, the sum S
+constexpr int strip_winv_smem() {   // a column block of W, the sum S, the L11 blocks below the diagonal, inv(L_ii)
+  return (SW_BLK * LU_NB * LU_NB + LU_NB * LU_NB + (SW_BLK * (SW_BLK - 1) / 2) * LU_NB * LU_NB +
+          SW_BLK * LU_NB * LU_NB) * (int)sizeof(C2);
 }
 template <class C2>
 __global__ void __launch_bounds__(LU_NB * LU_NB) strip_winv_kernel(BatchT<C2> b, int k0) {
   extern __shared__ __align__(16) unsigned char sw_sm[];
-  C2* Wc = reinterpret_cast<C2*>(sw_sm);   // [SW_BLK][LU_NB][LU_NB] column block j of W, column-major blocks
-  C2* S = Wc + SW_BLK * LU_NB * LU_NB;     // [LU_NB][LU_NB]
+  constexpr int BB = LU_NB * LU_NB;
+  C2* Wc = reinterpret_cast<C2*>(sw_sm);   // [SW_BLK][BB] column block j of W, column-major blocks
+  C2* S = Wc + SW_BLK * BB;                // [BB]
+  C2* Ls = S + BB;                         // L_ik (i > k) at ((i (i - 1)) / 2 + k) * BB
+  C2* Ps = Ls + (SW_BLK * (SW_BLK - 1) / 2) * BB;   // inv(L_ii) at i * BB
   const int n = b.order(blockIdx.z);
   if (k0 + LU_OUTER >= n) return;
   const C2* A = b.sys(blockIdx.z);
   const C2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
   C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_DIAG;
   const int r = threadIdx.x % LU_NB, c = threadIdx.x / LU_NB, e = r + LU_NB * c;
+  // every block this system needs, loaded once (coalesced along the rows)
+  for (int i = 1; i < SW_BLK; ++i)
+    for (int k = 0; k < i; ++k)
+      Ls[((i * (i - 1)) / 2 + k) * BB + e] = A[(k0 + i * LU_NB + r) + (long long)n * (k0 + k * LU_NB + c)];
+  for (int i = 0; i < SW_BLK; ++i) Ps[i * BB + e] = P[i * BB + e];
   for (int j = 0; j < SW_BLK; ++j) {
-    Wc[j * LU_NB * LU_NB + e] = P[j * LU_NB * LU_NB + e];
+    __syncthreads();   // the staged blocks (first pass) and the previous column block's stores are done
+    Wc[j * BB + e] = Ps[j * BB + e];
     for (int i = j + 1; i < SW_BLK; ++i) {
       __syncthreads();   // W_kj for k < i are in shared memory
       C2 acc = mkc<C2>(0., 0.);
       for (int k = j; k < i; ++k) {
-        const C2* L = A + (k0 + i * LU_NB + r) + (long long)n * (k0 + k * LU_NB);
-        const C2* Wk = Wc + k * LU_NB * LU_NB + LU_NB * c;
+        const C2* L = Ls + ((i * (i - 1)) / 2 + k) * BB + r;
+        const C2* Wk = Wc + k * BB + LU_NB * c;
 #pragma unroll 8
-        for (int m = 0; m < LU_NB; ++m) cmac(acc, L[(long long)n * m], Wk[m]);
+        for (int m = 0; m < LU_NB; ++m) cmac(acc, L[LU_NB * m], Wk[m]);
       }
       S[e] = acc;
       __syncthreads();
-      const C2* Pi = P + i * LU_NB * LU_NB;
+      const C2* Pi = Ps + i * BB + r;
       C2 w = mkc<C2>(0., 0.);
 #pragma unroll 8
-      for (int m = 0; m < LU_NB; ++m) cmac(w, Pi[r + LU_NB * m], S[m + LU_NB * c]);
-      Wc[i * LU_NB * LU_NB + e] = mkc<C2>(-w.x, -w.y);
+      for (int m = 0; m < LU_NB; ++m) cmac(w, Pi[LU_NB * m], S[m + LU_NB * c]);
+      Wc[i * BB + e] = mkc<C2>(-w.x, -w.y);
     }
     __syncthreads();
-    for (int i = j; i < SW_BLK; ++i) W[(i * LU_NB + r) + LU_OUTER * (j * LU_NB + c)] = Wc[i * LU_NB * LU_NB + e];
-    __syncthreads();
+    for (int i = j; i < SW_BLK; ++i) W[(i * LU_NB + r) + LU_OUTER * (j * LU_NB + c)] = Wc[i * BB + e];
   }
 }
 
