@@ -67,10 +67,14 @@ inline BatchT<C2> make_batch(C2* base, int n, C2* diag, C2* pinv, const Ragged& 
 }
 constexpr int DIAG_SCRATCH = 3 * LU_NB * LU_NB;
 constexpr int LU_OUTER = 128;
-// per system: inv(L) of the current outer panel's LU_OUTER / LU_NB diagonal
-// blocks, then inv(L11) of the whole panel (LU_OUTER x LU_OUTER, column-major)
+// per system, for the current outer panel: inv(L) of its LU_OUTER / LU_NB
+// diagonal blocks (P), inv(U) of the same blocks (Q), then inv(L11) (W) and
+// inv(U11) (V) of the whole panel (LU_OUTER x LU_OUTER, column-major)
 constexpr int PINV_DIAG = (LU_OUTER / LU_NB) * LU_NB * LU_NB;
-constexpr int PINV_SCRATCH = PINV_DIAG + LU_OUTER * LU_OUTER;
+constexpr int PINV_Q_OFF = PINV_DIAG;
+constexpr int PINV_W_OFF = 2 * PINV_DIAG;
+constexpr int PINV_V_OFF = PINV_W_OFF + LU_OUTER * LU_OUTER;
+constexpr int PINV_SCRATCH = PINV_V_OFF + LU_OUTER * LU_OUTER;
 using Batch = BatchT<double2>;
 
 template <class C2> __device__ __forceinline__ C2 mkc(double x, double y);
@@ -471,7 +475,7 @@ __global__ void __launch_bounds__(LU_NB * LU_NB) strip_winv_kernel(BatchT<C2> b,
   if (k0 + LU_OUTER >= n) return;
   const C2* A = b.sys(blockIdx.z);
   const C2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
-  C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_DIAG;
+  C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_W_OFF;
   const int r = threadIdx.x % LU_NB, c = threadIdx.x / LU_NB, e = r + LU_NB * c;
   // every block this system needs, loaded once (coalesced along the rows)
   for (int i = 1; i < SW_BLK; ++i)
@@ -521,7 +525,7 @@ __global__ void __launch_bounds__(128) strip_gemm_kernel(BatchT<C2> b, int k0) {
   const int c0 = kend + blockIdx.x * ST_C, ncol = min(ST_C, n - c0);
   if (ncol <= 0) return;
   C2* A = b.sys(blockIdx.z);
-  const C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_DIAG;
+  const C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_W_OFF;
   // block step s -> (ib, jb): (0,0), (1,0), (1,1), (2,0), ...
   auto blk = [](int s, int& ib, int& jb) {
     ib = 0;
@@ -572,6 +576,197 @@ __global__ void __launch_bounds__(128) strip_gemm_kernel(BatchT<C2> b, int k0) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Panel of the FP32 LU as one block (mixed path): instead of LU_OUTER / LU_NB
+// steps of (diagonal block, panel, in-panel update) launches,
+//   panel_block_kernel  factors the panel's LU_OUTER x LU_OUTER diagonal block
+//                       A11 in shared memory (GAUSSZ's unpivoted elimination)
+//                       and inverts the triangles of its 32 x 32 diagonal
+//                       blocks (P = inv(L_ii), Q = inv(U_ii));
+//   strip_winv_kernel   W = inv(L11) (and panel_vinv_kernel V = inv(U11));
+//   panel_l21_kernel    L21 = A21 V for every row below the panel;
+//   strip_gemm_kernel   U12 = W A12 for the row strip;
+// then the outer update as before.
+// ---------------------------------------------------------------------------
+template <class C2>
+constexpr int panel_block_smem() {   // the block, then one 32 x 32 scratch per triangle inversion
+  return (LU_OUTER * LU_OUTER + 2 * SW_BLK * LU_NB * LU_NB) * (int)sizeof(C2);
+}
+template <class C2>
+__global__ void __launch_bounds__(1024) panel_block_kernel(BatchT<C2> b, int k0, int* status) {
+  extern __shared__ __align__(16) unsigned char pb_sm[];
+  C2* T = reinterpret_cast<C2*>(pb_sm);   // [LU_OUTER][LU_OUTER] column-major
+  C2* X = T + LU_OUTER * LU_OUTER;        // [2 * SW_BLK][LU_NB][LU_NB] inversion scratch
+  const int n = b.order(blockIdx.z);
+  if (k0 >= n) return;
+  const int nb = min(LU_OUTER, n - k0), t = threadIdx.x;
+  C2* A = b.sys(blockIdx.z);
+  for (int q = t; q < LU_OUTER * LU_OUTER; q += blockDim.x) {
+    const int r = q % LU_OUTER, c = q / LU_OUTER;
+    T[q] = (r < nb && c < nb) ? A[(k0 + r) + (long long)n * (k0 + c)] : mkc<C2>(0., 0.);
+  }
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    if (t == 0 && !(cabs2(T[j + LU_OUTER * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+    if (t > j && t < nb) T[t + LU_OUTER * j] = cdv(T[t + LU_OUTER * j], T[j + LU_OUTER * j]);
+    __syncthreads();
+    const int m = nb - j - 1;
+    for (int q = t; q < m * m; q += blockDim.x) {
+      const int r = j + 1 + q % m, c = j + 1 + q / m;
+      T[r + LU_OUTER * c] = cfms(T[r + LU_OUTER * c], T[r + LU_OUTER * j], T[j + LU_OUTER * c]);
+    }
+    __syncthreads();
+  }
+  for (int q = t; q < LU_OUTER * LU_OUTER; q += blockDim.x) {
+    const int r = q % LU_OUTER, c = q / LU_OUTER;
+    if (r < nb && c < nb) A[(k0 + r) + (long long)n * (k0 + c)] = T[q];
+  }
+  // inverses of the diagonal blocks' triangles: task = (triangle, block), one
+  // thread per column of the inverse; a partial last block keeps the
+  // identity beyond nb (those rows and columns are never used)
+  C2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
+  const int task = t / 128, col = t % 128;
+  if (col < LU_NB) {
+    const bool upper = task >= SW_BLK;
+    const int bi = task % SW_BLK, o = bi * LU_NB;
+    C2* x = X + task * LU_NB * LU_NB + LU_NB * col;   // this column, in shared memory
+    const int nbb = max(0, min(LU_NB, nb - o));
+    for (int i = 0; i < LU_NB; ++i) x[i] = mkc<C2>(i == col ? 1. : 0., 0.);
+    if (col < nbb) {
+      if (!upper) {   // unit lower: x_i = -sum_{k=col}^{i-1} L_ik x_k
+        for (int i = col + 1; i < nbb; ++i) {
+          C2 v = mkc<C2>(0., 0.);
+          for (int k = col; k < i; ++k) cmac(v, T[(o + i) + LU_OUTER * (o + k)], x[k]);
+          x[i] = mkc<C2>(-v.x, -v.y);
+        }
+      } else {        // upper: x_col = 1 / U_cc, x_i = -(sum_{k=i+1}^{col} U_ik x_k) / U_ii
+        x[col] = cdv(mkc<C2>(1., 0.), T[(o + col) + LU_OUTER * (o + col)]);
+        for (int i = col - 1; i >= 0; --i) {
+          C2 v = mkc<C2>(0., 0.);
+          for (int k = i + 1; k <= col; ++k) cmac(v, T[(o + i) + LU_OUTER * (o + k)], x[k]);
+          const C2 d = cdv(v, T[(o + i) + LU_OUTER * (o + i)]);
+          x[i] = mkc<C2>(-d.x, -d.y);
+        }
+      }
+    }
+    C2* dst = P + (upper ? PINV_Q_OFF : 0) + bi * LU_NB * LU_NB + LU_NB * col;
+    for (int i = 0; i < LU_NB; ++i) dst[i] = x[i];
+  }
+}
+
+// V = inv(U11) of the panel from the blocks of U11 (in A) and Q: column block
+// j of V: V_jj = Q_jj, then for the blocks above, i = j-1 .. 0,
+// V_ij = -Q_ii sum_{k=i+1}^{j} U_ik V_kj. Same layout as strip_winv_kernel.
+template <class C2>
+__global__ void __launch_bounds__(LU_NB * LU_NB) panel_vinv_kernel(BatchT<C2> b, int k0) {
+  extern __shared__ __align__(16) unsigned char pv_sm[];
+  constexpr int BB = LU_NB * LU_NB;
+  C2* Vc = reinterpret_cast<C2*>(pv_sm);   // [SW_BLK][BB] column block j of V
+  C2* S = Vc + SW_BLK * BB;
+  C2* Us = S + BB;                         // U_ik (i < k) at ((k (k - 1)) / 2 + i) * BB
+  C2* Qs = Us + (SW_BLK * (SW_BLK - 1) / 2) * BB;
+  const int n = b.order(blockIdx.z);
+  if (k0 + LU_OUTER >= n) return;
+  const C2* A = b.sys(blockIdx.z);
+  const C2* Q = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_Q_OFF;
+  C2* V = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_V_OFF;
+  const int r = threadIdx.x % LU_NB, c = threadIdx.x / LU_NB, e = r + LU_NB * c;
+  for (int k = 1; k < SW_BLK; ++k)
+    for (int i = 0; i < k; ++i)
+      Us[((k * (k - 1)) / 2 + i) * BB + e] = A[(k0 + i * LU_NB + r) + (long long)n * (k0 + k * LU_NB + c)];
+  for (int i = 0; i < SW_BLK; ++i) Qs[i * BB + e] = Q[i * BB + e];
+  for (int j = 0; j < SW_BLK; ++j) {
+    __syncthreads();
+    Vc[j * BB + e] = Qs[j * BB + e];
+    for (int i = j - 1; i >= 0; --i) {
+      __syncthreads();   // V_kj for k > i are in shared memory
+      C2 acc = mkc<C2>(0., 0.);
+      for (int k = i + 1; k <= j; ++k) {
+        const C2* U = Us + ((k * (k - 1)) / 2 + i) * BB + r;
+        const C2* Vk = Vc + k * BB + LU_NB * c;
+#pragma unroll 8
+        for (int m = 0; m < LU_NB; ++m) cmac(acc, U[LU_NB * m], Vk[m]);
+      }
+      S[e] = acc;
+      __syncthreads();
+      const C2* Qi = Qs + i * BB + r;
+      C2 w = mkc<C2>(0., 0.);
+#pragma unroll 8
+      for (int m = 0; m < LU_NB; ++m) cmac(w, Qi[LU_NB * m], S[m + LU_NB * c]);
+      Vc[i * BB + e] = mkc<C2>(-w.x, -w.y);
+    }
+    __syncthreads();
+    for (int i = 0; i <= j; ++i) V[(i * LU_NB + r) + LU_OUTER * (j * LU_NB + c)] = Vc[i * BB + e];
+  }
+}
+
+// L21 = A21 V for the rows below the panel: CTA = one system and PL_R rows
+// (held in shared memory, column-major, ld PL_R); thread = (row r, every
+// fourth column of each 32-column block). The ten nonzero blocks of V stream
+// through two shared buffers as in strip_gemm_kernel; output column block cb
+// = sum_{kb <= cb} X_kb V_kb,cb.
+constexpr int PL_R = 32;
+template <class C2>
+constexpr int panel_l21_smem() {
+  return (PL_R * LU_OUTER + 2 * LU_NB * LU_NB) * (int)sizeof(C2);
+}
+template <class C2>
+__global__ void __launch_bounds__(128) panel_l21_kernel(BatchT<C2> b, int k0) {
+  extern __shared__ __align__(16) unsigned char pl_sm[];
+  C2* X = reinterpret_cast<C2*>(pl_sm);   // [LU_OUTER][PL_R] the rows before the solve
+  C2* Vb = X + PL_R * LU_OUTER;           // [2][LU_NB][LU_NB]
+  const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
+  const int r0 = kend + blockIdx.x * PL_R, nrow = min(PL_R, n - r0);
+  if (nrow <= 0) return;
+  C2* A = b.sys(blockIdx.z);
+  const C2* V = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_V_OFF;
+  // block step s -> (kb, cb) with kb <= cb: (0,0), (0,1), (1,1), (0,2), ...
+  auto blk = [](int s, int& kb, int& cb) {
+    cb = 0;
+    while ((cb + 1) * (cb + 2) / 2 <= s) ++cb;
+    kb = s - cb * (cb + 1) / 2;
+  };
+  auto fetch = [&](int s) {
+    int kb, cb;
+    blk(s, kb, cb);
+    C2* dst = Vb + (s & 1) * LU_NB * LU_NB;
+    for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) {
+      const int rr = q % LU_NB, cc = q / LU_NB;
+      cp_async_elem(dst + q, V + (kb * LU_NB + rr) + LU_OUTER * (cb * LU_NB + cc), true);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  fetch(0);
+  for (int q = threadIdx.x; q < PL_R * LU_OUTER; q += blockDim.x) {
+    const int rr = q % PL_R, cc = q / PL_R;
+    X[q] = rr < nrow ? A[(r0 + rr) + (long long)n * (k0 + cc)] : mkc<C2>(0., 0.);
+  }
+  const int r = threadIdx.x % PL_R, g = threadIdx.x / PL_R;
+  constexpr int GROUPS = 128 / PL_R, CPT = LU_NB / GROUPS, NSTEP = SW_BLK * (SW_BLK + 1) / 2;
+  C2 acc[CPT];
+  for (int s = 0; s < NSTEP; ++s) {
+    int kb, cb;
+    blk(s, kb, cb);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    if (s + 1 < NSTEP) fetch(s + 1);
+    if (kb == 0) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
+    }
+    const C2* Vt = Vb + (s & 1) * LU_NB * LU_NB;
+    for (int j = 0; j < LU_NB; ++j) {
+      const C2 x = X[(kb * LU_NB + j) * PL_R + r];
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) cmac(acc[m], x, Vt[j + LU_NB * (g + GROUPS * m)]);
+    }
+    if (kb == cb && r < nrow) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) A[(r0 + r) + (long long)n * (k0 + cb * LU_NB + g + GROUPS * m)] = acc[m];
+    }
+  }
+}
+
 // Systems split into groups factored side by side on separate streams: the
 // launches of a step are issued group after group, so the latency-bound
 // kernels of one group (diagonal blocks, panels, small updates) overlap the
@@ -591,6 +786,16 @@ struct LaneSplit {
   int first[LANES + 1] = {};
   cudaStream_t st[LANES] = {};
 };
+
+// FP32 panels factored as one block per system (default), or by LU_NB-column
+// steps with NEMOH_B200_PANEL=steps
+inline bool panel_as_block() {
+  static const bool on = [] {
+    const char* e = std::getenv("NEMOH_B200_PANEL");
+    return !(e && std::strcmp(e, "steps") == 0);
+  }();
+  return on;
+}
 
 // row strips as W = inv(L11) times the strip (default), or by the blocked
 // forward solve with NEMOH_B200_STRIP=solve
@@ -677,7 +882,57 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
     while (s0 + c < s1 && host_ord[s0 + c] > k) ++c;
     return c;
   };
+  // the FP32 row-strip form factors each panel as one block (panel_block_kernel)
+  const bool block = b.pinv && sizeof(C2) == sizeof(float2) && panel_as_block();
+  if (block) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+      cudaFuncSetAttribute(panel_block_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           panel_block_smem<C2>());
+      cudaFuncSetAttribute(strip_winv_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_winv_smem<C2>());
+      cudaFuncSetAttribute(panel_vinv_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_winv_smem<C2>());
+      cudaFuncSetAttribute(panel_l21_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_l21_smem<C2>());
+      cudaFuncSetAttribute(strip_gemm_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_gemm_smem<C2>());
+    });
+  }
   for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
+    if (block) {
+      for (int g = 0; g < L.groups; ++g) {
+        const int ns = active(g, k0);
+        if (ns == 0) continue;
+        const int s0 = L.first[g];
+        const int ng = host_ord ? host_ord[s0] : n;
+        const int kend = std::min(k0 + LU_OUTER, ng);
+        BatchT<C2> bg = sub_batch(b, s0);
+        bg.n = ng;
+        const cudaStream_t st = L.st[g];
+        panel_block_kernel<C2><<<dim3(1, 1, ns), 1024, panel_block_smem<C2>(), st>>>(bg, k0, status);
+        ++launches;
+        if (kend >= ng) continue;
+        strip_winv_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
+        panel_vinv_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
+        panel_l21_kernel<C2><<<dim3((ng - kend + PL_R - 1) / PL_R, 1, ns), 128, panel_l21_smem<C2>(), st>>>(bg, k0);
+        strip_gemm_kernel<C2><<<dim3((ng - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_gemm_smem<C2>(), st>>>(bg,
+                                                                                                            k0);
+        launches += 4;
+        if (!join_outer) outer(bg, ns, st, s0, k0, kend);
+      }
+      if (join_outer) {
+        const int ng = host_ord ? host_ord[0] : n;
+        const int kend = std::min(k0 + LU_OUTER, ng);
+        int ns = 0;
+        for (int g = 0; g < L.groups; ++g) ns = std::max(ns, L.first[g] + active(g, k0));
+        if (kend < ng && ns > 0) {
+          lane_join(L, main, lanes);
+          BatchT<C2> bw = b;
+          bw.n = ng;
+          outer(bw, ns, main, 0, k0, kend);
+          cudaEventRecord(lanes->fork, main);
+          for (int g = 0; g < L.groups; ++g) cudaStreamWaitEvent(L.st[g], lanes->fork, 0);
+        }
+      }
+      continue;
+    }
     for (int k = k0; k < std::min(k0 + LU_OUTER, n); k += LU_NB) {
       for (int g = 0; g < L.groups; ++g) {
         const int ns = active(g, k);
