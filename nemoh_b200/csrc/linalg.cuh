@@ -464,7 +464,7 @@ constexpr int strip_winv_smem() {   // a column block of W, the sum S, the L11 b
           SW_BLK * LU_NB * LU_NB) * (int)sizeof(C2);
 }
 template <class C2>
-__global__ void __launch_bounds__(LU_NB * LU_NB) strip_winv_kernel(BatchT<C2> b, int k0) {
+__device__ __forceinline__ void strip_winv_body(const BatchT<C2>& b, int k0) {
   extern __shared__ __align__(16) unsigned char sw_sm[];
   constexpr int BB = LU_NB * LU_NB;
   C2* Wc = reinterpret_cast<C2*>(sw_sm);   // [SW_BLK][BB] column block j of W, column-major blocks
@@ -517,12 +517,12 @@ constexpr int strip_gemm_smem() {
   return (LU_OUTER * ST_C + 2 * LU_NB * LU_NB) * (int)sizeof(C2);
 }
 template <class C2>
-__global__ void __launch_bounds__(128) strip_gemm_kernel(BatchT<C2> b, int k0) {
+__device__ __forceinline__ void strip_gemm_body(const BatchT<C2>& b, int k0, int bx) {
   extern __shared__ __align__(16) unsigned char sg_sm[];
   C2* X = reinterpret_cast<C2*>(sg_sm);   // [ST_C][LU_OUTER] the strip before the solve
   C2* Wb = X + LU_OUTER * ST_C;           // [2][LU_NB][LU_NB] blocks of W, column-major
   const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
-  const int c0 = kend + blockIdx.x * ST_C, ncol = min(ST_C, n - c0);
+  const int c0 = kend + bx * ST_C, ncol = min(ST_C, n - c0);
   if (ncol <= 0) return;
   C2* A = b.sys(blockIdx.z);
   const C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_W_OFF;
@@ -579,13 +579,13 @@ __global__ void __launch_bounds__(128) strip_gemm_kernel(BatchT<C2> b, int k0) {
 // ---------------------------------------------------------------------------
 // Panel of the FP32 LU as one block (mixed path): instead of LU_OUTER / LU_NB
 // steps of (diagonal block, panel, in-panel update) launches,
-//   panel_block_kernel  factors the panel's LU_OUTER x LU_OUTER diagonal block
-//                       A11 in shared memory (GAUSSZ's unpivoted elimination)
-//                       and inverts the triangles of its 32 x 32 diagonal
-//                       blocks (P = inv(L_ii), Q = inv(U_ii));
-//   strip_winv_kernel   W = inv(L11) (and panel_vinv_kernel V = inv(U11));
-//   panel_l21_kernel    L21 = A21 V for every row below the panel;
-//   strip_gemm_kernel   U12 = W A12 for the row strip;
+//   panel_block_kernel    factors the panel's LU_OUTER x LU_OUTER diagonal
+//                         block A11 in shared memory (GAUSSZ's unpivoted
+//                         elimination) and inverts the triangles of its 32 x 32
+//                         diagonal blocks (P = inv(L_ii), Q = inv(U_ii));
+//   panel_inv_kernel      W = inv(L11) and V = inv(U11), one CTA each per system;
+//   panel_products_kernel L21 = A21 V for every row below the panel and
+//                         U12 = W A12 for the row strip, in one launch;
 // then the outer update as before.
 // ---------------------------------------------------------------------------
 template <class C2>
@@ -606,14 +606,18 @@ __global__ void __launch_bounds__(1024) panel_block_kernel(BatchT<C2> b, int k0,
     T[q] = (r < nb && c < nb) ? A[(k0 + r) + (long long)n * (k0 + c)] : mkc<C2>(0., 0.);
   }
   __syncthreads();
+  // thread = (row tr, every eighth column from tc0): the row's multiplier is
+  // read once per step, the pivot row's entries are broadcast within a warp
+  const int tr = t % LU_OUTER, tc0 = t / LU_OUTER;
+  constexpr int CSTEP = 1024 / LU_OUTER;
   for (int j = 0; j < nb; ++j) {
     if (t == 0 && !(cabs2(T[j + LU_OUTER * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
     if (t > j && t < nb) T[t + LU_OUTER * j] = cdv(T[t + LU_OUTER * j], T[j + LU_OUTER * j]);
     __syncthreads();
-    const int m = nb - j - 1;
-    for (int q = t; q < m * m; q += blockDim.x) {
-      const int r = j + 1 + q % m, c = j + 1 + q / m;
-      T[r + LU_OUTER * c] = cfms(T[r + LU_OUTER * c], T[r + LU_OUTER * j], T[j + LU_OUTER * c]);
+    if (tr > j && tr < nb) {
+      const C2 l = T[tr + LU_OUTER * j];
+      for (int c = j + 1 + tc0; c < nb; c += CSTEP)
+        T[tr + LU_OUTER * c] = cfms(T[tr + LU_OUTER * c], l, T[j + LU_OUTER * c]);
     }
     __syncthreads();
   }
@@ -658,7 +662,7 @@ __global__ void __launch_bounds__(1024) panel_block_kernel(BatchT<C2> b, int k0,
 // j of V: V_jj = Q_jj, then for the blocks above, i = j-1 .. 0,
 // V_ij = -Q_ii sum_{k=i+1}^{j} U_ik V_kj. Same layout as strip_winv_kernel.
 template <class C2>
-__global__ void __launch_bounds__(LU_NB * LU_NB) panel_vinv_kernel(BatchT<C2> b, int k0) {
+__device__ __forceinline__ void panel_vinv_body(const BatchT<C2>& b, int k0) {
   extern __shared__ __align__(16) unsigned char pv_sm[];
   constexpr int BB = LU_NB * LU_NB;
   C2* Vc = reinterpret_cast<C2*>(pv_sm);   // [SW_BLK][BB] column block j of V
@@ -711,12 +715,12 @@ constexpr int panel_l21_smem() {
   return (PL_R * LU_OUTER + 2 * LU_NB * LU_NB) * (int)sizeof(C2);
 }
 template <class C2>
-__global__ void __launch_bounds__(128) panel_l21_kernel(BatchT<C2> b, int k0) {
+__device__ __forceinline__ void panel_l21_body(const BatchT<C2>& b, int k0, int bx) {
   extern __shared__ __align__(16) unsigned char pl_sm[];
   C2* X = reinterpret_cast<C2*>(pl_sm);   // [LU_OUTER][PL_R] the rows before the solve
   C2* Vb = X + PL_R * LU_OUTER;           // [2][LU_NB][LU_NB]
   const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
-  const int r0 = kend + blockIdx.x * PL_R, nrow = min(PL_R, n - r0);
+  const int r0 = kend + bx * PL_R, nrow = min(PL_R, n - r0);
   if (nrow <= 0) return;
   C2* A = b.sys(blockIdx.z);
   const C2* V = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_V_OFF;
@@ -765,6 +769,32 @@ __global__ void __launch_bounds__(128) panel_l21_kernel(BatchT<C2> b, int k0) {
       for (int m = 0; m < CPT; ++m) A[(r0 + r) + (long long)n * (k0 + cb * LU_NB + g + GROUPS * m)] = acc[m];
     }
   }
+}
+
+template <class C2>
+__global__ void __launch_bounds__(LU_NB * LU_NB) strip_winv_kernel(BatchT<C2> b, int k0) {
+  strip_winv_body(b, k0);
+}
+template <class C2>
+__global__ void __launch_bounds__(128) strip_gemm_kernel(BatchT<C2> b, int k0) {
+  strip_gemm_body(b, k0, blockIdx.x);
+}
+// both triangle inverses of the panel's diagonal block: blockIdx.x 0 W, 1 V
+template <class C2>
+__global__ void __launch_bounds__(LU_NB * LU_NB) panel_inv_kernel(BatchT<C2> b, int k0) {
+  if (blockIdx.x == 0) strip_winv_body(b, k0);
+  else panel_vinv_body(b, k0);
+}
+// both block products of the panel: blockIdx.y 0 L21 = A21 V (row chunks),
+// 1 U12 = W A12 (column chunks)
+template <class C2>
+constexpr int panel_products_smem() {
+  return panel_l21_smem<C2>() > strip_gemm_smem<C2>() ? panel_l21_smem<C2>() : strip_gemm_smem<C2>();
+}
+template <class C2>
+__global__ void __launch_bounds__(128) panel_products_kernel(BatchT<C2> b, int k0) {
+  if (blockIdx.y == 0) panel_l21_body(b, k0, blockIdx.x);
+  else strip_gemm_body(b, k0, blockIdx.x);
 }
 
 // Systems split into groups factored side by side on separate streams: the
@@ -889,10 +919,9 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
     once_per_device(attr, [] {
       cudaFuncSetAttribute(panel_block_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            panel_block_smem<C2>());
-      cudaFuncSetAttribute(strip_winv_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_winv_smem<C2>());
-      cudaFuncSetAttribute(panel_vinv_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_winv_smem<C2>());
-      cudaFuncSetAttribute(panel_l21_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_l21_smem<C2>());
-      cudaFuncSetAttribute(strip_gemm_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_gemm_smem<C2>());
+      cudaFuncSetAttribute(panel_inv_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip_winv_smem<C2>());
+      cudaFuncSetAttribute(panel_products_kernel<C2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           panel_products_smem<C2>());
     });
   }
   for (int k0 = 0; k0 < n; k0 += LU_OUTER) {
@@ -909,12 +938,10 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
         panel_block_kernel<C2><<<dim3(1, 1, ns), 1024, panel_block_smem<C2>(), st>>>(bg, k0, status);
         ++launches;
         if (kend >= ng) continue;
-        strip_winv_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
-        panel_vinv_kernel<C2><<<dim3(1, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
-        panel_l21_kernel<C2><<<dim3((ng - kend + PL_R - 1) / PL_R, 1, ns), 128, panel_l21_smem<C2>(), st>>>(bg, k0);
-        strip_gemm_kernel<C2><<<dim3((ng - kend + ST_C - 1) / ST_C, 1, ns), 128, strip_gemm_smem<C2>(), st>>>(bg,
-                                                                                                            k0);
-        launches += 4;
+        panel_inv_kernel<C2><<<dim3(2, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
+        const int nx = std::max((ng - kend + PL_R - 1) / PL_R, (ng - kend + ST_C - 1) / ST_C);
+        panel_products_kernel<C2><<<dim3(nx, 2, ns), 128, panel_products_smem<C2>(), st>>>(bg, k0);
+        launches += 2;
         if (!join_outer) outer(bg, ns, st, s0, k0, kend);
       }
       if (join_outer) {
