@@ -507,33 +507,38 @@ __device__ __forceinline__ void strip_winv_body(const BatchT<C2>& b, int k0) {
   }
 }
 
-// strip product: CTA = one system and ST_C columns of the strip (held in
-// shared memory, column-major, ld LU_OUTER); thread = one row in each of the
-// four 32-row blocks and every fourth column (a 4 x 8 register tile, so each
-// W entry read is applied to 8 columns and each strip entry to 4 rows). W's
-// column blocks (its blocks on and below the diagonal) stream through two
-// shared buffers by cp.async, the next in flight while one is applied; output
-// row block ib = sum_{jb <= ib} W_ib,jb X_jb goes straight to A.
+// strip_gemm_kernel: CTA = one system and ST_C columns of the strip (held in
+// shared memory, column-major, ld LU_OUTER); thread = (row i of a block, every
+// fourth column). The ten nonzero 32 x 32 blocks of W stream through two
+// shared buffers (cp.async, the next one in flight while the current one is
+// applied); output block ib = sum_{jb <= ib} W_ib,jb X_jb goes straight to A.
 template <class C2>
 constexpr int strip_gemm_smem() {
-  return (LU_OUTER * ST_C + 2 * SW_BLK * LU_NB * LU_NB) * (int)sizeof(C2);
+  return (LU_OUTER * ST_C + 2 * LU_NB * LU_NB) * (int)sizeof(C2);
 }
 template <class C2>
 __device__ __forceinline__ void strip_gemm_body(const BatchT<C2>& b, int k0, int bx) {
   extern __shared__ __align__(16) unsigned char sg_sm[];
-  constexpr int BB = LU_NB * LU_NB;
   C2* X = reinterpret_cast<C2*>(sg_sm);   // [ST_C][LU_OUTER] the strip before the solve
-  C2* Ws = X + LU_OUTER * ST_C;           // [2][SW_BLK][BB] column block jb of W, column-major blocks
+  C2* Wb = X + LU_OUTER * ST_C;           // [2][LU_NB][LU_NB] blocks of W, column-major
   const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
   const int c0 = kend + bx * ST_C, ncol = min(ST_C, n - c0);
   if (ncol <= 0) return;
   C2* A = b.sys(blockIdx.z);
   const C2* W = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_W_OFF;
-  auto fetch = [&](int jb) {   // blocks (ib, jb), ib >= jb
-    C2* dst = Ws + (jb & 1) * SW_BLK * BB;
-    for (int q = threadIdx.x; q < (SW_BLK - jb) * BB; q += blockDim.x) {
-      const int ib = jb + q / BB, e = q % BB, rr = e % LU_NB, cc = e / LU_NB;
-      cp_async_elem(dst + ib * BB + e, W + (ib * LU_NB + rr) + LU_OUTER * (jb * LU_NB + cc), true);
+  // block step s -> (ib, jb): (0,0), (1,0), (1,1), (2,0), ...
+  auto blk = [](int s, int& ib, int& jb) {
+    ib = 0;
+    while ((ib + 1) * (ib + 2) / 2 <= s) ++ib;
+    jb = s - ib * (ib + 1) / 2;
+  };
+  auto fetch = [&](int s) {
+    int ib, jb;
+    blk(s, ib, jb);
+    C2* dst = Wb + (s & 1) * LU_NB * LU_NB;
+    for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) {
+      const int rr = q % LU_NB, cc = q / LU_NB;
+      cp_async_elem(dst + q, W + (ib * LU_NB + rr) + LU_OUTER * (jb * LU_NB + cc), true);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
@@ -543,37 +548,32 @@ __device__ __forceinline__ void strip_gemm_body(const BatchT<C2>& b, int k0, int
     X[q] = cc < ncol ? A[(k0 + rr) + (long long)n * (c0 + cc)] : mkc<C2>(0., 0.);
   }
   const int i = threadIdx.x & (LU_NB - 1), g = threadIdx.x / LU_NB;
-  constexpr int GROUPS = 128 / LU_NB, CPT = ST_C / GROUPS;
-  C2 acc[SW_BLK][CPT];
-#pragma unroll
-  for (int ib = 0; ib < SW_BLK; ++ib)
-#pragma unroll
-    for (int m = 0; m < CPT; ++m) acc[ib][m] = mkc<C2>(0., 0.);
-  for (int jb = 0; jb < SW_BLK; ++jb) {
+  constexpr int GROUPS = 128 / LU_NB, CPT = ST_C / GROUPS, NSTEP = SW_BLK * (SW_BLK + 1) / 2;
+  C2 acc[CPT];
+  for (int s = 0; s < NSTEP; ++s) {
+    int ib, jb;
+    blk(s, ib, jb);
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-    __syncthreads();   // column block jb has landed; every thread is done with jb - 1
-    if (jb + 1 < SW_BLK) fetch(jb + 1);
-    const C2* T = Ws + (jb & 1) * SW_BLK * BB;
+    __syncthreads();   // block s has landed; every thread is done with block s - 1
+    if (s + 1 < NSTEP) fetch(s + 1);
+    if (jb == 0) {
+#pragma unroll
+      for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
+    }
+    const C2* T = Wb + (s & 1) * LU_NB * LU_NB;
     for (int j = 0; j < LU_NB; ++j) {
-      C2 xv[CPT];
+      const C2 t = T[i + LU_NB * j];
 #pragma unroll
-      for (int m = 0; m < CPT; ++m) xv[m] = X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + j];
+      for (int m = 0; m < CPT; ++m) cmac(acc[m], t, X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + j]);
+    }
+    if (jb == ib) {
 #pragma unroll
-      for (int ib = 0; ib < SW_BLK; ++ib) {
-        if (ib < jb) continue;
-        const C2 w = T[ib * BB + i + LU_NB * j];
-#pragma unroll
-        for (int m = 0; m < CPT; ++m) cmac(acc[ib][m], w, xv[m]);
+      for (int m = 0; m < CPT; ++m) {
+        const int c = g + GROUPS * m;
+        if (c < ncol) A[(k0 + ib * LU_NB + i) + (long long)n * (c0 + c)] = acc[m];
       }
     }
   }
-#pragma unroll
-  for (int ib = 0; ib < SW_BLK; ++ib)
-#pragma unroll
-    for (int m = 0; m < CPT; ++m) {
-      const int c = g + GROUPS * m;
-      if (c < ncol) A[(k0 + ib * LU_NB + i) + (long long)n * (c0 + c)] = acc[ib][m];
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -705,34 +705,38 @@ __device__ __forceinline__ void panel_vinv_body(const BatchT<C2>& b, int k0) {
 }
 
 // L21 = A21 V for the rows below the panel: CTA = one system and PL_R rows
-// (held in shared memory, ld PL_R); thread = 8 consecutive rows and one column
-// in each 32-column block (an 8 x 4 register tile). V's row blocks (its blocks
-// on and right of the diagonal) stream through two shared buffers (rows
-// padded to 33 entries, so the columns a warp reads fall in distinct banks);
-// output column block cb = sum_{kb <= cb} X_kb V_kb,cb, staged through shared
-// memory for coalesced stores.
+// (held in shared memory, column-major, ld PL_R); thread = (row r, every
+// fourth column of each 32-column block). The ten nonzero blocks of V stream
+// through two shared buffers as in strip_gemm_kernel; output column block cb
+// = sum_{kb <= cb} X_kb V_kb,cb.
 constexpr int PL_R = 32;
-constexpr int PL_LD = LU_NB + 1;
 template <class C2>
 constexpr int panel_l21_smem() {
-  return (PL_R * LU_OUTER + 2 * SW_BLK * LU_NB * PL_LD) * (int)sizeof(C2);
+  return (PL_R * LU_OUTER + 2 * LU_NB * LU_NB) * (int)sizeof(C2);
 }
 template <class C2>
 __device__ __forceinline__ void panel_l21_body(const BatchT<C2>& b, int k0, int bx) {
   extern __shared__ __align__(16) unsigned char pl_sm[];
-  constexpr int VB = LU_NB * PL_LD;
   C2* X = reinterpret_cast<C2*>(pl_sm);   // [LU_OUTER][PL_R] the rows before the solve
-  C2* Vs = X + PL_R * LU_OUTER;           // [2][SW_BLK][LU_NB columns][PL_LD] row block kb of V
+  C2* Vb = X + PL_R * LU_OUTER;           // [2][LU_NB][LU_NB]
   const int n = b.order(blockIdx.z), kend = k0 + LU_OUTER;
   const int r0 = kend + bx * PL_R, nrow = min(PL_R, n - r0);
   if (nrow <= 0) return;
   C2* A = b.sys(blockIdx.z);
   const C2* V = b.pinv + (long long)blockIdx.z * PINV_SCRATCH + PINV_V_OFF;
-  auto fetch = [&](int kb) {   // blocks (kb, cb), cb >= kb; entry (j, c) at c * PL_LD + j
-    C2* dst = Vs + (kb & 1) * SW_BLK * VB;
-    for (int q = threadIdx.x; q < (SW_BLK - kb) * LU_NB * LU_NB; q += blockDim.x) {
-      const int cb = kb + q / (LU_NB * LU_NB), e = q % (LU_NB * LU_NB), j = e % LU_NB, c = e / LU_NB;
-      cp_async_elem(dst + cb * VB + c * PL_LD + j, V + (kb * LU_NB + j) + LU_OUTER * (cb * LU_NB + c), true);
+  // block step s -> (kb, cb) with kb <= cb: (0,0), (0,1), (1,1), (0,2), ...
+  auto blk = [](int s, int& kb, int& cb) {
+    cb = 0;
+    while ((cb + 1) * (cb + 2) / 2 <= s) ++cb;
+    kb = s - cb * (cb + 1) / 2;
+  };
+  auto fetch = [&](int s) {
+    int kb, cb;
+    blk(s, kb, cb);
+    C2* dst = Vb + (s & 1) * LU_NB * LU_NB;
+    for (int q = threadIdx.x; q < LU_NB * LU_NB; q += blockDim.x) {
+      const int rr = q % LU_NB, cc = q / LU_NB;
+      cp_async_elem(dst + q, V + (kb * LU_NB + rr) + LU_OUTER * (cb * LU_NB + cc), true);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
@@ -741,40 +745,29 @@ __device__ __forceinline__ void panel_l21_body(const BatchT<C2>& b, int k0, int 
     const int rr = q % PL_R, cc = q / PL_R;
     X[q] = rr < nrow ? A[(r0 + rr) + (long long)n * (k0 + cc)] : mkc<C2>(0., 0.);
   }
-  constexpr int RPT = 8;                           // rows per thread
-  const int rg = threadIdx.x % (PL_R / RPT), cg = threadIdx.x / (PL_R / RPT);   // cg: 0..31
-  C2 acc[RPT][SW_BLK];
-#pragma unroll
-  for (int rr = 0; rr < RPT; ++rr)
-#pragma unroll
-    for (int cb = 0; cb < SW_BLK; ++cb) acc[rr][cb] = mkc<C2>(0., 0.);
-  for (int kb = 0; kb < SW_BLK; ++kb) {
+  const int r = threadIdx.x % PL_R, g = threadIdx.x / PL_R;
+  constexpr int GROUPS = 128 / PL_R, CPT = LU_NB / GROUPS, NSTEP = SW_BLK * (SW_BLK + 1) / 2;
+  C2 acc[CPT];
+  for (int s = 0; s < NSTEP; ++s) {
+    int kb, cb;
+    blk(s, kb, cb);
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
-    if (kb + 1 < SW_BLK) fetch(kb + 1);
-    const C2* T = Vs + (kb & 1) * SW_BLK * VB;
-    for (int j = 0; j < LU_NB; ++j) {
-      C2 xr[RPT];
+    if (s + 1 < NSTEP) fetch(s + 1);
+    if (kb == 0) {
 #pragma unroll
-      for (int rr = 0; rr < RPT; ++rr) xr[rr] = X[(kb * LU_NB + j) * PL_R + rg * RPT + rr];
-#pragma unroll
-      for (int cb = 0; cb < SW_BLK; ++cb) {
-        if (cb < kb) continue;
-        const C2 v = T[cb * VB + cg * PL_LD + j];
-#pragma unroll
-        for (int rr = 0; rr < RPT; ++rr) cmac(acc[rr][cb], xr[rr], v);
-      }
+      for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
     }
-  }
-  __syncthreads();   // X no longer read: it takes the result
+    const C2* Vt = Vb + (s & 1) * LU_NB * LU_NB;
+    for (int j = 0; j < LU_NB; ++j) {
+      const C2 x = X[(kb * LU_NB + j) * PL_R + r];
 #pragma unroll
-  for (int rr = 0; rr < RPT; ++rr)
+      for (int m = 0; m < CPT; ++m) cmac(acc[m], x, Vt[j + LU_NB * (g + GROUPS * m)]);
+    }
+    if (kb == cb && r < nrow) {
 #pragma unroll
-    for (int cb = 0; cb < SW_BLK; ++cb) X[(cb * LU_NB + cg) * PL_R + rg * RPT + rr] = acc[rr][cb];
-  __syncthreads();
-  for (int q = threadIdx.x; q < PL_R * LU_OUTER; q += blockDim.x) {
-    const int rr = q % PL_R, cc = q / PL_R;
-    if (rr < nrow) A[(r0 + rr) + (long long)n * (k0 + cc)] = X[q];
+      for (int m = 0; m < CPT; ++m) A[(r0 + r) + (long long)n * (k0 + cb * LU_NB + g + GROUPS * m)] = acc[m];
+    }
   }
 }
 
