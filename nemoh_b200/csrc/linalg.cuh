@@ -606,21 +606,36 @@ __global__ void __launch_bounds__(1024) panel_block_kernel(BatchT<C2> b, int k0,
     T[q] = (r < nb && c < nb) ? A[(k0 + r) + (long long)n * (k0 + c)] : mkc<C2>(0., 0.);
   }
   __syncthreads();
-  // thread = (row tr, every eighth column from tc0): the row's multiplier is
-  // read once per step, the pivot row's entries are broadcast within a warp
-  const int tr = t % LU_OUTER, tc0 = t / LU_OUTER;
-  constexpr int CSTEP = 1024 / LU_OUTER;
+  // warp w owns the columns w, w + 32, w + 64, w + 96; lane l the rows l,
+  // l + 32, l + 64, l + 96. Step j: the owner of column j divides it below the
+  // pivot, one barrier, then every warp applies the rank-1 update to its own
+  // columns right of j. Column j + 1 is then final in its owner's view, which
+  // divides it next without a second barrier.
+  const int lane = t & 31, w = t >> 5;
   for (int j = 0; j < nb; ++j) {
-    if (t == 0 && !(cabs2(T[j + LU_OUTER * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-    if (t > j && t < nb) T[t + LU_OUTER * j] = cdv(T[t + LU_OUTER * j], T[j + LU_OUTER * j]);
-    __syncthreads();
-    if (tr > j && tr < nb) {
-      const C2 l = T[tr + LU_OUTER * j];
-      for (int c = j + 1 + tc0; c < nb; c += CSTEP)
-        T[tr + LU_OUTER * c] = cfms(T[tr + LU_OUTER * c], l, T[j + LU_OUTER * c]);
+    if (w == (j & 31)) {
+      const C2 piv = T[j + LU_OUTER * j];
+      if (lane == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+#pragma unroll
+      for (int q = 0; q < LU_OUTER / 32; ++q) {
+        const int r = lane + 32 * q;
+        if (r > j && r < nb) T[r + LU_OUTER * j] = cdv(T[r + LU_OUTER * j], piv);
+      }
     }
     __syncthreads();
+#pragma unroll
+    for (int cc = 0; cc < LU_OUTER / 32; ++cc) {
+      const int c = w + 32 * cc;
+      if (c <= j || c >= nb) continue;
+      const C2 u = T[j + LU_OUTER * c];
+#pragma unroll
+      for (int q = 0; q < LU_OUTER / 32; ++q) {
+        const int r = lane + 32 * q;
+        if (r > j && r < nb) T[r + LU_OUTER * c] = cfms(T[r + LU_OUTER * c], T[r + LU_OUTER * j], u);
+      }
+    }
   }
+  __syncthreads();
   for (int q = t; q < LU_OUTER * LU_OUTER; q += blockDim.x) {
     const int r = q % LU_OUTER, c = q / LU_OUTER;
     if (r < nb && c < nb) A[(k0 + r) + (long long)n * (k0 + c)] = T[q];
