@@ -606,33 +606,26 @@ __global__ void __launch_bounds__(1024) panel_block_kernel(BatchT<C2> b, int k0,
     T[q] = (r < nb && c < nb) ? A[(k0 + r) + (long long)n * (k0 + c)] : mkc<C2>(0., 0.);
   }
   __syncthreads();
-  // warp w owns the columns w, w + 32, w + 64, w + 96; lane l the rows l,
-  // l + 32, l + 64, l + 96. Step j: the owner of column j divides it below the
-  // pivot, one barrier, then every warp applies the rank-1 update to its own
-  // columns right of j. Column j + 1 is then final in its owner's view, which
-  // divides it next without a second barrier.
+  // Step j works on the active block (rows and columns j+1 .. nb-1) only:
+  // lane l takes its rows j+1+l, j+1+l+32, ..., warp w its columns j+1+w,
+  // j+1+w+32, ... (every lane busy, however small the block). Column j+1 is
+  // then updated by warp 0 alone, which also divides it at the next step, so
+  // one barrier per step suffices: the next step's division needs only warp
+  // 0's own updates, and the barrier after it orders the pivot row's entries
+  // (updated by every warp) before they are read.
   const int lane = t & 31, w = t >> 5;
   for (int j = 0; j < nb; ++j) {
-    if (w == (j & 31)) {
+    if (w == 0) {
+      __syncwarp();   // column j was updated by other lanes of this warp at the last step
       const C2 piv = T[j + LU_OUTER * j];
       if (lane == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-#pragma unroll
-      for (int q = 0; q < LU_OUTER / 32; ++q) {
-        const int r = lane + 32 * q;
-        if (r > j && r < nb) T[r + LU_OUTER * j] = cdv(T[r + LU_OUTER * j], piv);
-      }
+      for (int r = j + 1 + lane; r < nb; r += 32) T[r + LU_OUTER * j] = cdv(T[r + LU_OUTER * j], piv);
     }
     __syncthreads();
-#pragma unroll
-    for (int cc = 0; cc < LU_OUTER / 32; ++cc) {
-      const int c = w + 32 * cc;
-      if (c <= j || c >= nb) continue;
+    for (int c = j + 1 + w; c < nb; c += 32) {
       const C2 u = T[j + LU_OUTER * c];
-#pragma unroll
-      for (int q = 0; q < LU_OUTER / 32; ++q) {
-        const int r = lane + 32 * q;
-        if (r > j && r < nb) T[r + LU_OUTER * c] = cfms(T[r + LU_OUTER * c], T[r + LU_OUTER * j], u);
-      }
+      for (int r = j + 1 + lane; r < nb; r += 32)
+        T[r + LU_OUTER * c] = cfms(T[r + LU_OUTER * c], T[r + LU_OUTER * j], u);
     }
   }
   __syncthreads();
