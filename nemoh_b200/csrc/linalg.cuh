@@ -606,29 +606,21 @@ __global__ void __launch_bounds__(1024) panel_block_kernel(BatchT<C2> b, int k0,
     T[q] = (r < nb && c < nb) ? A[(k0 + r) + (long long)n * (k0 + c)] : mkc<C2>(0., 0.);
   }
   __syncthreads();
-  // Step j works on the active block (rows and columns j+1 .. nb-1) only:
-  // lane l takes its rows j+1+l, j+1+l+32, ..., warp w its columns j+1+w,
-  // j+1+w+32, ... (every lane busy, however small the block). Column j+1 is
-  // then updated by warp 0 alone, which also divides it at the next step, so
-  // one barrier per step suffices: the next step's division needs only warp
-  // 0's own updates, and the barrier after it orders the pivot row's entries
-  // (updated by every warp) before they are read.
-  const int lane = t & 31, w = t >> 5;
+  // thread = (row tr, every eighth column from tc0): the row's multiplier is
+  // read once per step, the pivot row's entries are broadcast within a warp
+  const int tr = t % LU_OUTER, tc0 = t / LU_OUTER;
+  constexpr int CSTEP = 1024 / LU_OUTER;
   for (int j = 0; j < nb; ++j) {
-    if (w == 0) {
-      __syncwarp();   // column j was updated by other lanes of this warp at the last step
-      const C2 piv = T[j + LU_OUTER * j];
-      if (lane == 0 && !(cabs2(piv) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
-      for (int r = j + 1 + lane; r < nb; r += 32) T[r + LU_OUTER * j] = cdv(T[r + LU_OUTER * j], piv);
+    if (t == 0 && !(cabs2(T[j + LU_OUTER * j]) > 1.E-20)) atomicCAS(status, 0, ST_PIVOT);
+    if (t > j && t < nb) T[t + LU_OUTER * j] = cdv(T[t + LU_OUTER * j], T[j + LU_OUTER * j]);
+    __syncthreads();
+    if (tr > j && tr < nb) {
+      const C2 l = T[tr + LU_OUTER * j];
+      for (int c = j + 1 + tc0; c < nb; c += CSTEP)
+        T[tr + LU_OUTER * c] = cfms(T[tr + LU_OUTER * c], l, T[j + LU_OUTER * c]);
     }
     __syncthreads();
-    for (int c = j + 1 + w; c < nb; c += 32) {
-      const C2 u = T[j + LU_OUTER * c];
-      for (int r = j + 1 + lane; r < nb; r += 32)
-        T[r + LU_OUTER * c] = cfms(T[r + LU_OUTER * c], T[r + LU_OUTER * j], u);
-    }
   }
-  __syncthreads();
   for (int q = t; q < LU_OUTER * LU_OUTER; q += blockDim.x) {
     const int r = q % LU_OUTER, c = q / LU_OUTER;
     if (r < nb && c < nb) A[(k0 + r) + (long long)n * (k0 + c)] = T[q];
