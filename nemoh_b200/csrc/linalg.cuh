@@ -1393,8 +1393,9 @@ void trsm_launch(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, 
 //     every read of it.
 // The backward sweep runs the same way from the last block with U. X holds the
 // right-hand sides and is overwritten by partial sums; Y receives the solution.
-// `active` (may be null): the launch does nothing when *active == 0 (a
-// converged refinement), read uniformly by every CTA.
+// `active` (may be null): refinement flags, [0] for the whole launch (it
+// does nothing when 0: a converged refinement) and [1 + s] for system s
+// (its cluster leaves at once when 0: that system has converged).
 // ---------------------------------------------------------------------------
 constexpr int SW_THREADS = 256;
 template <class C2, int NR>
@@ -1417,6 +1418,7 @@ __global__ void __launch_bounds__(SW_THREADS, sizeof(C2) == sizeof(float2) ? 2 :
   cg::cluster_group cl = cg::this_cluster();
   const int csize = (int)cl.num_blocks(), rank = (int)cl.block_rank();
   const int sys = blockIdx.x / csize;
+  if (active && active[1 + sys] == 0) return;   // this system has converged (whole cluster)
   const int n = b.order(sys);
   const C2* A = b.sys(sys);
   C2* X = xbase + sys * xstride;
@@ -1644,6 +1646,7 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
       else hi = mid;
     }
     const int sys = item - pre[lo];
+    if (active && active[1 + sys] == 0) continue;   // a converged system: none of its items runs
     const int n = b.order(sys), nbs = (n + TB - 1) / TB;
     const int blk = LOWER ? lo : nbs - 1 - lo;
     const int k0 = blk * TB, nb = min(TB, n - k0);
@@ -1865,6 +1868,7 @@ __global__ void __launch_bounds__(128, 4) matvec_acc_kernel(Batch m, const doubl
                                                          double2* ybase, long long ystride, double sign,
                                                          const int* active) {
   if (active && *active == 0) return;   // a converged refinement skips its remaining passes
+  if (active && active[1 + blockIdx.z] == 0) return;   // and a converged system its own work
   __shared__ double2 Xs[MV_COLS * NR];
   const int n = m.order(blockIdx.z);
   const double2* M = m.sys(blockIdx.z);
@@ -1915,7 +1919,8 @@ inline void matvec_acc_nr(Batch m, const double2* x, long long xs, double2* y, l
 }
 
 // Y += sign * M X for nsys systems with nrhs (1..MAX_RHS) right-hand sides;
-// with `active`, nothing is done when *active == 0 on the device
+// with `active` (refinement flags: [0] the launch, [1 + s] system s), nothing
+// is done for a flag that is 0 on the device
 inline void matvec_acc(Batch m, const double2* x, long long xs, double2* y, long long ys, int nrhs, int nsys,
                        double sign, cudaStream_t st, const int* active = nullptr) {
   switch (nrhs) {

@@ -64,9 +64,10 @@ struct MixedWork {
   unsigned long long* norms = nullptr;  // |r|inf bits per system and rhs, then |b|inf
   RefineState* state = nullptr;         // refinement decisions on the device
   int* flow = nullptr;       // workspace of the dataflow sweep (both directions)
+  int* act = nullptr;        // refinement activity: [0] another pass wanted, [1 + s] system s not converged yet
   int* status = nullptr;     // the owner's status word (sweep timeouts)
   TcWork tc;                 // tensor-core GEMM operand buffers
-  size_t have[11] = {};      // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv, state, flow
+  size_t have[12] = {};      // bytes held by lu, diag, b, r, rf, yf, norms, inv, pinv, state, flow, act
   size_t total = 0;
   int last_iterations = 0;
   double last_residual = 0.;
@@ -75,10 +76,10 @@ struct MixedWork {
   size_t bytes() const { return total; }
   void release() {
     cudaFree(lu); cudaFree(diag); cudaFree(b); cudaFree(r); cudaFree(rf); cudaFree(yf); cudaFree(norms); cudaFree(inv);
-    cudaFree(pinv); cudaFree(state); cudaFree(flow);
+    cudaFree(pinv); cudaFree(state); cudaFree(flow); cudaFree(act);
     tc.release();
     lu = nullptr; diag = nullptr; b = nullptr; r = nullptr; rf = nullptr; yf = nullptr; norms = nullptr; inv = nullptr;
-    pinv = nullptr; state = nullptr; flow = nullptr;
+    pinv = nullptr; state = nullptr; flow = nullptr; act = nullptr;
     for (size_t& h : have) h = 0;
     total = 0;
   }
@@ -90,7 +91,7 @@ struct MixedWork {
   // mat_elems: elements of all matrices of a ragged batch (0: nsys x n x n)
   cudaError_t ensure(int nsys, int n, int nrhs, size_t mat_elems = 0) {
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
-    const size_t need[11] = {(mat_elems ? mat_elems : nsys * NN) * sizeof(float2),
+    const size_t need[12] = {(mat_elems ? mat_elems : nsys * NN) * sizeof(float2),
                             (size_t)nsys * DIAG_SCRATCH * sizeof(float2),
                             V * sizeof(double2),
                             V * sizeof(double2),
@@ -100,10 +101,11 @@ struct MixedWork {
                             (size_t)nsys * ((n + TB - 1) / TB) * 2 * TB * TB * sizeof(float2),
                             (size_t)nsys * PINV_SCRATCH * sizeof(float2),
                             sizeof(RefineState),
-                            2 * flow_ws_ints(nsys, (n + TB - 1) / TB) * sizeof(int)};
-    void** ptr[11] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
-                      (void**)&inv, (void**)&pinv, (void**)&state, (void**)&flow};
-    for (int i = 0; i < 11; ++i) {
+                            2 * flow_ws_ints(nsys, (n + TB - 1) / TB) * sizeof(int),
+                            (size_t)(1 + nsys) * sizeof(int)};
+    void** ptr[12] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
+                      (void**)&inv, (void**)&pinv, (void**)&state, (void**)&flow, (void**)&act};
+    for (int i = 0; i < 12; ++i) {
       if (need[i] <= have[i]) continue;
       cudaFree(*ptr[i]);
       *ptr[i] = nullptr;
@@ -248,15 +250,18 @@ __global__ void refine_start_kernel(RefineState* st, int max_it) {
 }
 
 // x += correction (x = correction on the first pass), r = b, residual norms
-// cleared for the coming residual pass
+// cleared for the coming residual pass; systems that have converged (act[1 +
+// s] == 0, s = q / xs) keep their solution and leave their norms at 0
 __global__ void refine_update_kernel(double2* __restrict__ x, const float2* __restrict__ d,
                                      const double2* __restrict__ b, double2* __restrict__ r, long long count,
-                                     unsigned long long* __restrict__ rnorm, int nv, const RefineState* st) {
+                                     long long xs, unsigned long long* __restrict__ rnorm, int nv,
+                                     const RefineState* st, const int* __restrict__ act) {
   if (!st->active) return;
   const int first = st->iterations == 0;
   const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
   for (long long q = t0; q < nv; q += stride) rnorm[q] = 0ull;
   for (long long q = t0; q < count; q += stride) {
+    if (act[1 + q / xs] == 0) continue;
     const float2 v = d[q];
     if (first) x[q] = make_double2(v.x, v.y);
     else {
@@ -276,13 +281,14 @@ __global__ void refine_update_kernel(double2* __restrict__ x, const float2* __re
 __global__ void __launch_bounds__(256) refine_residual_kernel(const double2* __restrict__ r, float2* __restrict__ rf,
                                                               int n, int nrhs, unsigned long long* __restrict__ norms,
                                                               int nv, RefineState* st, double tol,
-                                                              const int* __restrict__ ord) {
+                                                              const int* __restrict__ ord, int* act) {
   if (!st->active) return;
   const int p = blockIdx.y, s = blockIdx.z;
   const long long base = (long long)s * nrhs * n + (long long)p * (ord ? ord[s] : n);
+  const bool mine = act[1 + s] != 0;   // a converged system's CTAs only count themselves
   if (ord) n = ord[s];
   double m = 0.;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; mine && i < n; i += gridDim.x * blockDim.x) {
     const double2 v = r[base + i];
     rf[base + i] = make_float2((float)v.x, (float)v.y);
     // a NaN component counts as infinite (fmax would drop it), so a failed
@@ -314,6 +320,7 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(const double2* __r
     if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
     __syncthreads();
   }
+  __shared__ int s_stop;
   if (threadIdx.x == 0) {
     const double w = red[0];
     const int it = st->iterations + 1;
@@ -325,6 +332,20 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(const double2* __r
     st->prev = w;
     st->done_ctas = 0;
     st->active = stop ? 0 : 1;
+    act[0] = stop ? 0 : 1;
+    s_stop = stop;
+  }
+  __syncthreads();
+  // the next pass works only on the systems still above the tolerance
+  const int nsys = gridDim.z;
+  for (int sy = threadIdx.x; sy < nsys; sy += blockDim.x) {
+    double ws = 0.;
+    for (int q = sy * nrhs; q < (sy + 1) * nrhs; ++q) {
+      const double rn = __longlong_as_double((long long)atomicAdd(norms + q, 0ull));
+      const double bn = __longlong_as_double((long long)norms[nv + q]);
+      ws = fmax(ws, bn > 0 ? rn / bn : rn);
+    }
+    act[1 + sy] = (!s_stop && !(ws <= tol)) ? 1 : 0;
   }
 }
 
@@ -355,21 +376,23 @@ inline void mixed_refine_begin(MixedWork& w, const RefineArgs& a, int max_it, cu
   ++launches;
   refine_start_kernel<<<1, 1, 0, st>>>(w.state, max_it);
   ++launches;
+  cudaMemsetAsync(w.act, 1, (size_t)(1 + a.nsys) * sizeof(int), st);   // nonzero: every system active
 }
 
 inline void mixed_refine_passes(MixedWork& w, const RefineArgs& a, int passes, cudaStream_t st, long long& launches) {
   const long long V = (long long)a.nsys * a.n * a.nrhs, xs = (long long)a.n * a.nrhs;
   const int nv = a.nsys * a.nrhs;
   const Batch dm = make_batch<double2>(a.D, a.n, nullptr, nullptr, a.rg);
-  const int* active = &w.state->active;
+  // act: [0] another pass wanted, [1 + s] system s still above the tolerance
+  const int* active = w.act;
   for (int it = 0; it < passes; ++it) {
     trsm_f32(w, a.n, a.nsys, a.nrhs, st, launches, active, a.rg);
-    refine_update_kernel<<<1184, 256, 0, st>>>(a.X, w.rf, w.b, w.r, V, w.norms, nv, w.state);
+    refine_update_kernel<<<1184, 256, 0, st>>>(a.X, w.rf, w.b, w.r, V, xs, w.norms, nv, w.state, w.act);
     ++launches;
     matvec_acc(dm, a.X, xs, w.r, xs, a.nrhs, a.nsys, -1.0, st, active);
     ++launches;
     refine_residual_kernel<<<dim3(8, a.nrhs, a.nsys), 256, 0, st>>>(w.r, w.rf, a.n, a.nrhs, w.norms, nv, w.state,
-                                                                    REFINE_TOL, a.rg.ord);
+                                                                    REFINE_TOL, a.rg.ord, w.act);
     ++launches;
   }
 }
