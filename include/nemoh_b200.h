@@ -178,6 +178,18 @@ int nemoh_b200_solve_bodies(nemoh_ctx* ctx, int nitem, const int* body, const do
 int nemoh_b200_set_graphs(nemoh_ctx* ctx, int on);
 int nemoh_b200_graph_stats(const nemoh_ctx* ctx, long long* captures, long long* replays);
 
+/* Evaluates now, for every resident body, the frequency-independent Rankine
+ * part of each depth regime it can meet (deep water; finite depth when its
+ * depth is finite), which a solve otherwise evaluates at the body's first
+ * frequency of that regime (kept within the resident bodies' cache budget).
+ * A server calls it once after adding its bodies, so that no request pays
+ * for it. */
+int nemoh_b200_prepare_bodies(nemoh_ctx* ctx);
+/* Autotuning of the triangular sweep (process-wide; on by default). Off, a
+ * batch shape not tuned yet is solved with the default sweep instead of
+ * timing the candidates first. */
+int nemoh_b200_set_autotune(int on);
+
 /* Serving requests on resident bodies. nemoh_b200_set_body_dofs gives a body
  * its ndof radiation DOFs (kind, dir, axis as in nemoh_b200_body_conditions;
  * 1 + ndof <= 16). nemoh_b200_solve_requests solves nreq (body[i], omegas[i],

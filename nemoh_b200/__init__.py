@@ -89,6 +89,8 @@ def load_library():
     L.nemoh_b200_add_body.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _i, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_int, _d, _i]
     L.nemoh_b200_body_count.argtypes = [_vp]
+    L.nemoh_b200_prepare_bodies.argtypes = [_vp]
+    L.nemoh_b200_set_autotune.argtypes = [ctypes.c_int]
     L.nemoh_b200_solve_bodies.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _d, _d]
     L.nemoh_b200_solve_bodies_device.argtypes = [_vp, ctypes.c_int, _i, _d, ctypes.c_int, _vp, _vp, _vp]
     L.nemoh_b200_set_body_dofs.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _i, _d, _d]
@@ -308,6 +310,11 @@ class Solver:
         L.nemoh_b200_last_factor_ms(self._h, ctypes.byref(lu))
         return dict(assemble_ms=a.value, factor_ms=f.value, solve_ms=s.value, lu_ms=lu.value)
 
+    def prepare_bodies(self):
+        """Evaluate the resident bodies' Rankine parts now (each depth regime
+        they can meet), so that no later solve pays for them."""
+        self._check(load_library().nemoh_b200_prepare_bodies(self._h))
+
     def fallback_count(self):
         """(batches that fell back to FP64 factors, systems re-solved in partial fallbacks)"""
         nb_, ns = ctypes.c_longlong(), ctypes.c_longlong()
@@ -491,3 +498,9 @@ def sweep_choice(n, nsys, nrhs, single):
     L.nemoh_b200_diag_sweep_tuning(ctypes.byref(keys), int(n), int(nsys), int(nrhs), int(bool(single)),
                                    ctypes.byref(cs))
     return cs.value, keys.value
+
+
+def set_autotune(on):
+    """Autotuning of the triangular sweep, process-wide (on by default): off, a
+    batch shape not tuned yet is solved with the default sweep."""
+    load_library().nemoh_b200_set_autotune(int(bool(on)))

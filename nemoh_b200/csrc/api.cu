@@ -1015,22 +1015,31 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
 // and kept with the resident body, while the bodies' caches stay within
 // NEMOH_B200_RANKINE_CACHE_BYTES (default: a quarter of the device memory);
 // a body beyond it gets the per-slot Rankine pass in every batch.
-void ensure_body_rankine(nemoh_ctx* c, int nitem, const int* body, const double* omegas) {
+size_t body_rankine_cap() {
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   size_t cap = tot / 4;
   if (const char* e = std::getenv("NEMOH_B200_RANKINE_CACHE_BYTES")) cap = (size_t)std::max(0LL, std::atoll(e));
+  return cap;
+}
+
+// one body's cache of one depth regime, if it fits the budget
+void body_rankine(nemoh_ctx* c, BodyState& b, bool fd, size_t cap) {
+  if (b.rk_valid[fd]) return;
+  const size_t bytes = (size_t)(b.nsymy + 1) * b.nfa * b.nfa * sizeof(double2);
+  if (c->rk_body_bytes + bytes > cap) return;
+  GreenCtx g = green_ctx(c);
+  g.zer = b.zer;
+  rankine_cache(c, g, b.d_rec.as<PanelRec>(), b.d_rows.as<double>(), b.nfa, b.nsymy, b.depth, fd, b.rk[fd],
+                b.rk_valid[fd]);
+  c->rk_body_bytes += bytes;
+}
+
+void ensure_body_rankine(nemoh_ctx* c, int nitem, const int* body, const double* omegas) {
+  const size_t cap = body_rankine_cap();
   for (int i = 0; i < nitem; ++i) {
     BodyState& b = *c->bodies[body[i]];
-    const bool fd = finite_depth(Env{b.g, b.depth, b.gm, nullptr}, 2. * kPI / (2. * kPI / omegas[i]));
-    if (b.rk_valid[fd]) continue;
-    const size_t bytes = (size_t)(b.nsymy + 1) * b.nfa * b.nfa * sizeof(double2);
-    if (c->rk_body_bytes + bytes > cap) continue;
-    GreenCtx g = green_ctx(c);
-    g.zer = b.zer;
-    rankine_cache(c, g, b.d_rec.as<PanelRec>(), b.d_rows.as<double>(), b.nfa, b.nsymy, b.depth, fd, b.rk[fd],
-                  b.rk_valid[fd]);
-    c->rk_body_bytes += bytes;
+    body_rankine(c, b, finite_depth(Env{b.g, b.depth, b.gm, nullptr}, 2. * kPI / (2. * kPI / omegas[i])), cap);
   }
 }
 
@@ -1278,6 +1287,23 @@ int nemoh_b200_add_body(nemoh_ctx* c, int np, int nfa, int nsymy, const double* 
 }
 
 int nemoh_b200_body_count(const nemoh_ctx* c) { return c ? (int)c->bodies.size() : 0; }
+
+int nemoh_b200_prepare_bodies(nemoh_ctx* c) {
+  if (!c) return NEMOH_B200_EINVAL;
+  return guarded(c, [&] {
+    const size_t cap = body_rankine_cap();
+    for (auto& bp : c->bodies) {
+      body_rankine(c, *bp, false, cap);   // deep water: any body at high enough frequencies
+      if (bp->depth != 0.) body_rankine(c, *bp, true, cap);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int nemoh_b200_set_autotune(int on) {
+  set_sweep_autotune(on != 0);
+  return NEMOH_B200_OK;
+}
 
 int nemoh_b200_set_graphs(nemoh_ctx* c, int on) {
   if (!c) return NEMOH_B200_EINVAL;

@@ -17,6 +17,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cfloat>
 #include <cstdlib>
 #include <cstring>
@@ -79,6 +80,15 @@ inline int sweep_forced() {
   return f;
 }
 
+// autotuning on (default) or off (nemoh_b200_set_autotune): off, a shape not
+// tuned yet takes trsm_sweep's default instead of timing the candidates (a
+// server keeps timing runs, and the lock they hold, off its requests' path)
+inline std::atomic<bool>& sweep_autotune_flag() {
+  static std::atomic<bool> on{true};
+  return on;
+}
+inline void set_sweep_autotune(bool on) { sweep_autotune_flag().store(on); }
+
 template <class C2>
 inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, int nsys, int nrhs, cudaStream_t st,
                                     long long& launches, const int* active = nullptr, SweepSync sync = SweepSync()) {
@@ -90,7 +100,8 @@ inline cudaError_t trsm_sweep_tuned(BatchT<C2> b, const C2* inv, C2* X, C2* Y, i
   if (csize > 0 && (csize != SWEEP_FLOW || sync.ws))
     return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, csize, sync);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+  if (!sweep_autotune_flag().load() || cudaStreamIsCapturing(st, &cap) != cudaSuccess ||
+      cap != cudaStreamCaptureStatusNone)
     return trsm_sweep<C2>(b, inv, X, Y, nsys, nrhs, st, launches, active, 0, sync);
   int dev = 0;
   cudaGetDevice(&dev);

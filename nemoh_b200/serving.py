@@ -34,7 +34,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from . import FP64, MIXED, Solver  # noqa: F401
+from . import FP64, MIXED, Solver, set_autotune  # noqa: F401
 from . import cases as C
 
 
@@ -87,7 +87,11 @@ class SolveServer:
     """Serve a stream of requests on one GPU with `workers` concurrent contexts."""
 
     def __init__(self, bodies: List[Body], device=0, precision=MIXED, workers=2, memory_fraction=0.6,
-                 solver_factory=None, memory_bytes=None, max_batch=64):
+                 solver_factory=None, memory_bytes=None, max_batch=64, autotune=False):
+        """Every worker's context holds every body, with the bodies' Rankine
+        parts evaluated up front (Solver.prepare_bodies). autotune=False turns
+        the triangular sweep's autotuning off for the process, so that no
+        request waits on timing runs of a batch shape it meets first."""
         self.bodies = bodies
         self.device = device
         self.precision = precision
@@ -105,6 +109,10 @@ class SolveServer:
             for b in bodies:
                 bid = s.add_body(b.case)
                 s.set_body_dofs(bid, b.case.rad)
+            if hasattr(s, "prepare_bodies"):
+                s.prepare_bodies()
+        if not autotune and solver_factory is None:
+            set_autotune(False)
         self.batches = []   # (worker, bodies in the batch, nreq, t0, t1)
         free = memory_bytes
         if free is None:

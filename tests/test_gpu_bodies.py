@@ -187,3 +187,28 @@ def test_fallback_in_a_ragged_batch():
         F = np.stack([got[i] for i in sel], axis=2)
         F64 = np.stack([ref[i] for i in sel], axis=2)
         assert G.coef_err(F, F64, 1) < 1e-6, cases[b].name
+
+
+def test_prepared_bodies_match_lazy_caches():
+    """nemoh_b200_prepare_bodies evaluates every body's Rankine parts up front;
+    the solves afterwards (with autotuning off, the default sweep) equal those
+    of a context that evaluates them at first use, within 1e-12 of the largest
+    force."""
+    B.build()
+    cases = _bodies()
+    body, omega = _items(cases, seed=12, n=10)
+    nvels = [_rhs(cases[b], w) for b, w in zip(body, omega)]
+    out = {}
+    for prepared in (False, True):
+        with nb.Solver(0, nb.FP64) as s:
+            for c in cases:
+                s.add_body(c)
+            if prepared:
+                s.prepare_bodies()
+                nb.set_autotune(False)
+            try:
+                out[prepared] = s.solve_bodies(body, omega, nvels)
+            finally:
+                nb.set_autotune(True)
+    for a, b in zip(out[True], out[False]):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
