@@ -171,6 +171,18 @@ __global__ void __launch_bounds__(LU_DIAG_THREADS) lu_diag_kernel(BatchT<C2> b, 
 // component, 50% more floating-point instructions in the update loops)
 __device__ __forceinline__ double fmx(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fmx(float a, float b, float c) { return fmaf(a, b, c); }
+// two consecutive complex values of shared memory (the first at an even
+// index: one 16-byte load in single precision)
+__device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  a = make_float2(v.x, v.y);
+  b = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b) {
+  a = p[0];
+  b = p[1];
+}
+
 template <class C2>
 __device__ __forceinline__ void cmac(C2& acc, C2 a, C2 b) {
   acc.x = fmx(a.x, b.x, acc.x);
@@ -561,10 +573,15 @@ __device__ __forceinline__ void strip_gemm_body(const BatchT<C2>& b, int k0, int
       for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
     }
     const C2* T = Wb + (s & 1) * LU_NB * LU_NB;
-    for (int j = 0; j < LU_NB; ++j) {
-      const C2 t = T[i + LU_NB * j];
+    for (int j = 0; j < LU_NB; j += 2) {   // two k at a time: one 16-byte load gives both strip entries
+      const C2 t0 = T[i + LU_NB * j], t1 = T[i + LU_NB * (j + 1)];
 #pragma unroll
-      for (int m = 0; m < CPT; ++m) cmac(acc[m], t, X[(g + GROUPS * m) * LU_OUTER + jb * LU_NB + j]);
+      for (int m = 0; m < CPT; ++m) {
+        C2 x0, x1;
+        ld_pair(X + (g + GROUPS * m) * LU_OUTER + jb * LU_NB + j, x0, x1);
+        cmac(acc[m], t0, x0);
+        cmac(acc[m], t1, x1);
+      }
     }
     if (jb == ib) {
 #pragma unroll
@@ -759,10 +776,15 @@ __device__ __forceinline__ void panel_l21_body(const BatchT<C2>& b, int k0, int 
       for (int m = 0; m < CPT; ++m) acc[m] = mkc<C2>(0., 0.);
     }
     const C2* Vt = Vb + (s & 1) * LU_NB * LU_NB;
-    for (int j = 0; j < LU_NB; ++j) {
-      const C2 x = X[(kb * LU_NB + j) * PL_R + r];
+    for (int j = 0; j < LU_NB; j += 2) {   // two k at a time: one 16-byte load gives both V entries
+      const C2 x0 = X[(kb * LU_NB + j) * PL_R + r], x1 = X[(kb * LU_NB + j + 1) * PL_R + r];
 #pragma unroll
-      for (int m = 0; m < CPT; ++m) cmac(acc[m], x, Vt[j + LU_NB * (g + GROUPS * m)]);
+      for (int m = 0; m < CPT; ++m) {
+        C2 v0, v1;
+        ld_pair(Vt + j + LU_NB * (g + GROUPS * m), v0, v1);
+        cmac(acc[m], x0, v0);
+        cmac(acc[m], x1, v1);
+      }
     }
     if (kb == cb && r < nrow) {
 #pragma unroll
