@@ -41,14 +41,7 @@ struct DevBuf {
     p = nullptr;
     bytes = 0;
   }
-  cudaError_t ensure(size_t n) {
-    if (n <= bytes) return cudaSuccess;
-    release();
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e == cudaSuccess) bytes = n;
-    else p = nullptr;
-    return e;
-  }
+  cudaError_t ensure(size_t n, bool headroom = false) { return grow_alloc(&p, &bytes, n, headroom); }
   template <class T>
   T* as() const { return reinterpret_cast<T*>(p); }
 };
@@ -553,7 +546,7 @@ void factor_fp64(nemoh_ctx* c, int nsys, const Shape& sh) {
 
 // workspace of an FP64 dataflow sweep over nsys systems of order up to n
 SweepSync fp64_sync(nemoh_ctx* c, int nsys, int n) {
-  CK(c->d_flow.ensure(2 * flow_ws_ints(nsys, (n + TB - 1) / TB) * sizeof(int)));
+  CK(c->d_flow.ensure(2 * flow_ws_ints(nsys, (n + TB - 1) / TB) * sizeof(int), true));
   return SweepSync{c->d_flow.as<int>(), c->d_status.as<int>()};
 }
 
@@ -619,8 +612,8 @@ void mixed_fallback_ragged(nemoh_ctx* c, int nsys, int nrhs, const Shape& sh) {
   const size_t N = sh.n, xs = N * nrhs, xf = (size_t)ord_f[0] * nrhs;
   CK(c->d_froff.ensure(nf * sizeof(long long)));
   CK(c->d_frord.ensure(nf * sizeof(int)));
-  CK(c->d_fx.ensure((size_t)nf * xf * sizeof(double2)));
-  CK(c->d_fy.ensure((size_t)nf * xf * sizeof(double2)));
+  CK(c->d_fx.ensure((size_t)nf * xf * sizeof(double2), true));
+  CK(c->d_fy.ensure((size_t)nf * xf * sizeof(double2), true));
   CK(c->d_inv.ensure((size_t)nf * ((ord_f[0] + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
   CK(cudaMemcpyAsync(c->d_froff.p, off_f.data(), nf * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_frord.p, ord_f.data(), nf * sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -826,15 +819,16 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   }
   const int nsys = (int)ord.size(), nmax = ord[0];
   const size_t N = nmax, V = (size_t)nsys * N * nrhs;
-  CK(c->d_D.ensure((size_t)mat * sizeof(double2)));
-  CK(c->d_S.ensure((size_t)mat * sizeof(double2)));
-  CK(c->d_X.ensure(V * sizeof(double2)));
-  CK(c->d_Y.ensure(V * sizeof(double2)));
-  CK(c->d_diag.ensure((size_t)nsys * DIAG_SCRATCH * sizeof(double2)));
+  // batches of different bodies keep setting new footprints: grow with headroom
+  CK(c->d_D.ensure((size_t)mat * sizeof(double2), true));
+  CK(c->d_S.ensure((size_t)mat * sizeof(double2), true));
+  CK(c->d_X.ensure(V * sizeof(double2), true));
+  CK(c->d_Y.ensure(V * sizeof(double2), true));
+  CK(c->d_diag.ensure((size_t)nsys * DIAG_SCRATCH * sizeof(double2), true));
   if (c->mode == NEMOH_B200_FP64)
-    CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2)));
+    CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2), true));
   else
-    CK(c->mixed.ensure(nsys, nmax, nrhs, (size_t)mat));
+    CK(c->mixed.ensure(nsys, nmax, nrhs, (size_t)mat, true));
   CK(c->d_oms.ensure((size_t)k * sizeof(OmegaParams)));
   CK(c->d_slots.ensure((size_t)k * sizeof(int)));
   CK(c->h_oms.ensure((size_t)k * sizeof(OmegaParams)));
@@ -1346,8 +1340,8 @@ int nemoh_b200_solve_bodies(nemoh_ctx* c, int nitem, const int* body, const doub
     if (nrhs > MAX_RHS) throw Fail{NEMOH_B200_ECAPACITY, "nrhs must be in 1..16"};
     size_t nv = 0, nf = 0;
     bodies_sizes(c, nitem, body, nrhs, &nv, &nf);
-    CK(c->d_bnvel.ensure(nv * sizeof(double2)));
-    CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2)));
+    CK(c->d_bnvel.ensure(nv * sizeof(double2), true));
+    CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2), true));
     CK(cudaMemcpyAsync(c->d_bnvel.p, nvel, nv * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     solve_bodies_impl(c, nitem, body, omegas, nrhs, c->d_bnvel.as<double2>(), c->d_bforce.as<double2>());
     if (nf) CK(cudaMemcpyAsync(force, c->d_bforce.p, nf * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
@@ -1389,8 +1383,8 @@ int nemoh_b200_solve_requests(nemoh_ctx* c, int nreq, const int* body, const dou
         throw Fail{NEMOH_B200_EINVAL, "the bodies of one call must have the same number of DOFs"};
     size_t nv = 0, nf = 0;
     bodies_sizes(c, nreq, body, nrhs, &nv, &nf);
-    CK(c->d_bnvel.ensure(nv * sizeof(double2)));
-    CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2)));
+    CK(c->d_bnvel.ensure(nv * sizeof(double2), true));
+    CK(c->d_bforce.ensure(std::max<size_t>(1, nf) * sizeof(double2), true));
     CK(c->h_reqs.ensure((size_t)nreq * sizeof(ReqDesc)));
     CK(c->d_reqs.ensure((size_t)nreq * sizeof(ReqDesc)));
     ReqDesc* rq = c->h_reqs.as<ReqDesc>();

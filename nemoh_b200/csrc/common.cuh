@@ -12,6 +12,28 @@ namespace nb200 {
 // more dynamic shared memory than the default is set up once on every device
 // a process uses; `done` holds one bit per device (concurrent first calls on a
 // device may both set it, which is harmless).
+// Grows a device allocation to at least n bytes. With headroom a quarter more
+// is taken (n exactly if that does not fit): batches whose footprint keeps
+// setting new maxima (cross-body batches of a request stream) then reallocate
+// a few times instead of at every new maximum, each time a device-wide
+// synchronisation (cudaFree) and a multi-GB cudaMalloc.
+inline cudaError_t grow_alloc(void** p, size_t* have, size_t n, bool headroom) {
+  if (n <= *have) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  size_t want = headroom ? n + n / 4 : n;
+  cudaError_t e = cudaMalloc(p, want);
+  if (e != cudaSuccess && want != n) {
+    cudaGetLastError();
+    want = n;
+    e = cudaMalloc(p, want);
+  }
+  if (e == cudaSuccess) *have = want;
+  else *p = nullptr;
+  return e;
+}
+
 template <class F>
 inline void once_per_device(std::atomic<unsigned long long>& done, F set) {
   int dev = 0;

@@ -89,7 +89,8 @@ struct MixedWork {
   // systems reuses what a larger one left and nothing is freed needlessly:
   // cudaFree synchronizes the whole device.
   // mat_elems: elements of all matrices of a ragged batch (0: nsys x n x n)
-  cudaError_t ensure(int nsys, int n, int nrhs, size_t mat_elems = 0) {
+  // headroom: see grow_alloc (cross-body batches)
+  cudaError_t ensure(int nsys, int n, int nrhs, size_t mat_elems = 0, bool headroom = false) {
     const size_t NN = (size_t)n * n, V = (size_t)nsys * n * nrhs;
     const size_t need[12] = {(mat_elems ? mat_elems : nsys * NN) * sizeof(float2),
                             (size_t)nsys * DIAG_SCRATCH * sizeof(float2),
@@ -106,15 +107,10 @@ struct MixedWork {
     void** ptr[12] = {(void**)&lu, (void**)&diag, (void**)&b, (void**)&r, (void**)&rf, (void**)&yf, (void**)&norms,
                       (void**)&inv, (void**)&pinv, (void**)&state, (void**)&flow, (void**)&act};
     for (int i = 0; i < 12; ++i) {
-      if (need[i] <= have[i]) continue;
-      cudaFree(*ptr[i]);
-      *ptr[i] = nullptr;
-      have[i] = 0;
-      cudaError_t e = cudaMalloc(ptr[i], need[i]);
+      cudaError_t e = grow_alloc(ptr[i], &have[i], need[i], headroom);
       if (e) return e;
-      have[i] = need[i];
     }
-    cudaError_t e = tc.ensure(nsys, n);
+    cudaError_t e = tc.ensure(nsys, n, headroom);
     if (e) return e;
     total = tc.bytes();
     for (size_t h : have) total += h;

@@ -67,25 +67,12 @@ struct TcWork {
     a = b = nullptr;
     have_a = have_b = 0;
   }
-  cudaError_t ensure(int nsys, int n) {
+  cudaError_t ensure(int nsys, int n, bool headroom = false) {
     const size_t t = (size_t)(n + TC_T - 1) / TC_T;
     const size_t na = 2 * nsys * t * TC_NCH * 2 * TC_AIMG, nb = 2 * nsys * t * TC_NCH * 2 * TC_BIMG;
-    cudaError_t e;
-    if (na > have_a) {
-      cudaFree(a);
-      a = nullptr;
-      have_a = 0;
-      if ((e = cudaMalloc(&a, na))) return e;
-      have_a = na;
-    }
-    if (nb > have_b) {
-      cudaFree(b);
-      b = nullptr;
-      have_b = 0;
-      if ((e = cudaMalloc(&b, nb))) return e;
-      have_b = nb;
-    }
-    return cudaSuccess;
+    cudaError_t e = grow_alloc(reinterpret_cast<void**>(&a), &have_a, na, headroom);
+    if (e) return e;
+    return grow_alloc(reinterpret_cast<void**>(&b), &have_b, nb, headroom);
   }
 };
 
