@@ -41,7 +41,10 @@ struct DevBuf {
     p = nullptr;
     bytes = 0;
   }
-  cudaError_t ensure(size_t n, bool headroom = false) { return grow_alloc(&p, &bytes, n, headroom); }
+  // small buffers (descriptors, scratch) always grow with headroom
+  cudaError_t ensure(size_t n, bool headroom = false) {
+    return grow_alloc(&p, &bytes, n, headroom || n < (size_t(64) << 20));
+  }
   template <class T>
   T* as() const { return reinterpret_cast<T*>(p); }
 };
@@ -56,11 +59,14 @@ struct HostBuf {
     p = nullptr;
     bytes = 0;
   }
+  // grows to twice the request: freeing pinned memory synchronizes the device,
+  // so staging buffers of growing batches should grow rarely
   cudaError_t ensure(size_t n) {
     if (n <= bytes) return cudaSuccess;
     release();
-    cudaError_t e = cudaMallocHost(&p, n);
-    if (e == cudaSuccess) bytes = n;
+    const size_t want = std::max<size_t>(2 * n, 4096);
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e == cudaSuccess) bytes = want;
     else p = nullptr;
     return e;
   }
