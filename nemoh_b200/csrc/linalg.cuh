@@ -916,7 +916,7 @@ inline BatchT<C2> sub_batch(const BatchT<C2>& b, int s0) {
 // of each group) and the grids are sized by the group's largest system.
 template <class C2, class Outer>
 inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main, long long& launches, Outer outer,
-                         const Lanes* lanes = nullptr, const int* host_ord = nullptr) {
+                         const Lanes* lanes = nullptr, const int* host_ord = nullptr, bool outer_products = false) {
   const int n = b.n;
   const LaneSplit L = lane_split(nsys, main, lanes);
   // NEMOH_B200_OUTER_JOIN=1: the groups join for each outer update, which
@@ -961,9 +961,12 @@ inline void lu_two_level(BatchT<C2> b, int nsys, int* status, cudaStream_t main,
         ++launches;
         if (kend >= ng) continue;
         panel_inv_kernel<C2><<<dim3(2, 1, ns), LU_NB * LU_NB, strip_winv_smem<C2>(), st>>>(bg, k0);
-        const int nx = std::max((ng - kend + PL_R - 1) / PL_R, (ng - kend + ST_C - 1) / ST_C);
-        panel_products_kernel<C2><<<dim3(nx, 2, ns), 128, panel_products_smem<C2>(), st>>>(bg, k0);
-        launches += 2;
+        ++launches;
+        if (!outer_products) {   // else outer() forms L21 and U12 (on the tensor cores) before its update
+          const int nx = std::max((ng - kend + PL_R - 1) / PL_R, (ng - kend + ST_C - 1) / ST_C);
+          panel_products_kernel<C2><<<dim3(nx, 2, ns), 128, panel_products_smem<C2>(), st>>>(bg, k0);
+          ++launches;
+        }
         if (!join_outer) outer(bg, ns, st, s0, k0, kend);
       }
       if (join_outer) {

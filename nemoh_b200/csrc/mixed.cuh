@@ -145,6 +145,16 @@ __global__ void norm_kernel(const double2* __restrict__ v, int n, int nrhs, unsi
   if ((threadIdx.x & 31) == 0) atomicMax(out + (long long)s * nrhs + p, (unsigned long long)__double_as_longlong(m));
 }
 
+// the block panel's products L21 = A21 inv(U11) and U12 = inv(L11) A12 on the
+// tensor cores (NEMOH_B200_TC_PRODUCTS=0: on the CUDA cores)
+inline bool tc_products_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("NEMOH_B200_TC_PRODUCTS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // merged outer updates of panel pairs (NEMOH_B200_TC_MERGE=0 turns them off)
 inline bool tc_merge() {
   static const bool on = [] {
@@ -183,6 +193,8 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
   // writes the bulk of A22 once. deferred: per group (by its first system),
   // the image set holding the deferred panel's images, or -1.
   const bool merge = tc_enabled() && tc_persistent() && tc_merge();
+  // the block path's L21 and U12 products on the tensor cores too
+  const bool tc_prod = tc_enabled() && tc_persistent() && tc_products_on() && panel_as_block() && w.pinv;
   std::map<int, int> deferred;
   lu_two_level<float2>(
       b, nsys, status, st, launches,
@@ -192,6 +204,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
           TcWork tg = w.tc.set(set);
           tg.a += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_AIMG;
           tg.b += (size_t)(sys0 + s0) * tiles * TC_NCH * 2 * TC_BIMG;
+          tg.wv += (size_t)(sys0 + s0) * TC_WV_BYTES;
           return tg;
         };
         if (!tc_enabled()) {
@@ -201,6 +214,10 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
         }
         const int set = (k0 / LU_OUTER) & 1;
         TcWork tg = slice(set);
+        if (tc_prod) {   // L21 = A21 V and U12 = W A12 from images of the operands
+          tc_prep(tg, bg, k0, ns, sg, launches);
+          tc_products(tg, bg, k0, ns, sg, launches, status);
+        }
         if (!merge) {
           tc_update(tg, bg, k0, ns, sg, launches, status);
           return;
@@ -219,7 +236,7 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
           tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles(), true);
         }
       },
-      lanes, rg.host_ord);
+      lanes, rg.host_ord, tc_prod);
   static std::atomic<unsigned long long> attr{0};
   once_per_device(attr, [] {
     cudaFuncSetAttribute(inv_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,

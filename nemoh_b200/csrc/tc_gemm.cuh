@@ -49,11 +49,18 @@ constexpr int ST_TC_TIMEOUT = 30;
 
 // Operand images of two outer updates (two sets: the update of one panel may
 // be merged into the next panel's, and both panels' images are then read).
+constexpr long long TC_W_BYTES = (long long)TC_NCH * 2 * TC_AIMG;   // one A tile of K = 128
+constexpr long long TC_V_BYTES = (long long)TC_NCH * 2 * TC_BIMG;   // one B tile of K = 128
+constexpr long long TC_WV_BYTES = TC_W_BYTES + TC_V_BYTES;
+
 struct TcWork {
   unsigned char* a = nullptr;   // A images: 2 sets x nsys x ceil(n/128) row tiles x TC_NCH chunks x (hi, lo)
   unsigned char* b = nullptr;   // B images: 2 sets x nsys x ceil(n/128) column tiles x TC_NCH chunks x (hi, lo)
-  size_t have_a = 0, have_b = 0;
-  size_t bytes() const { return have_a + have_b; }
+  // per system: the A image of W = inv(L11), then the B image of V = inv(U11)
+  // (the panel's block products on the tensor cores)
+  unsigned char* wv = nullptr;
+  size_t have_a = 0, have_b = 0, have_wv = 0;
+  size_t bytes() const { return have_a + have_b + have_wv; }
   // the images of set s (0 or 1), each set half of the allocation
   TcWork set(int s) const {
     TcWork w = *this;
@@ -64,20 +71,23 @@ struct TcWork {
   void release() {
     cudaFree(a);
     cudaFree(b);
-    a = b = nullptr;
-    have_a = have_b = 0;
+    cudaFree(wv);
+    a = b = wv = nullptr;
+    have_a = have_b = have_wv = 0;
   }
   cudaError_t ensure(int nsys, int n, bool headroom = false) {
     const size_t t = (size_t)(n + TC_T - 1) / TC_T;
     const size_t na = 2 * nsys * t * TC_NCH * 2 * TC_AIMG, nb = 2 * nsys * t * TC_NCH * 2 * TC_BIMG;
     cudaError_t e = grow_alloc(reinterpret_cast<void**>(&a), &have_a, na, headroom);
     if (e) return e;
+    e = grow_alloc(reinterpret_cast<void**>(&wv), &have_wv, (size_t)nsys * TC_WV_BYTES, headroom);
+    if (e) return e;
     return grow_alloc(reinterpret_cast<void**>(&b), &have_b, nb, headroom);
   }
 };
 
 inline size_t tc_bytes_per_system(size_t n) {
-  return 2 * ((n + TC_T - 1) / TC_T) * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG);
+  return 2 * ((n + TC_T - 1) / TC_T) * TC_NCH * 2 * (size_t)(TC_AIMG + TC_BIMG) + TC_WV_BYTES;
 }
 
 // byte offset of the 16-byte core-matrix row (row, k-group g) in an image
@@ -168,6 +178,60 @@ __global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, 
     unsigned char* img = bbuf + blockIdx.z * sys_bytes_b + ((long long)t * TC_NCH + ch) * 2 * TC_BIMG;
     uint4 h, l;
     // B row `row` (real parts of the result): [Br; -Bi]; row 128+row (imaginary parts): [Bi; Br]
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      split8<F16>((g < 2 ? re : nim) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(row, g)) = l;
+      split8<F16>((g < 2 ? im : re) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(TC_T + row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(TC_T + row, g)) = l;
+    }
+  }
+}
+
+// Images of the panel's W = inv(L11) (an A tile) and V = inv(U11) (a B tile),
+// K = 128, in the layout of tc_prep_kernel's, for the block products
+// L21 = A21 V and U12 = W A12 on the tensor cores. Blocks [0, 8): W, [8, 16): V.
+template <bool F16>
+__global__ void __launch_bounds__(128) tc_prep_wv_kernel(BatchT<float2> b, int k0, unsigned char* __restrict__ wv) {
+  const int n = b.order(blockIdx.z);
+  if (k0 + LU_OUTER >= n) return;
+  const float2* P = b.pinv + (long long)blockIdx.z * PINV_SCRATCH;
+  constexpr int PER = TC_T * TC_NCH / 128;
+  const bool isW = (int)blockIdx.x < PER;
+  const int q = (isW ? blockIdx.x : blockIdx.x - PER) * 128 + threadIdx.x;   // < TC_T * TC_NCH
+  const int ch = q / TC_T, row = q % TC_T, kb = ch * TC_KC;
+  unsigned char* base = wv + blockIdx.z * TC_WV_BYTES;
+  float re[TC_KC], im[TC_KC];
+  uint4 h, l;
+  if (isW) {   // A row `row` of W: W[row, kb + j]
+    const float2* W = P + PINV_W_OFF;
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) {
+      const float2 v = W[row + LU_OUTER * (kb + j)];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    unsigned char* img = base + (long long)ch * 2 * TC_AIMG;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      split8<F16>((g < 2 ? re : im) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_AIMG + tc_row_off(row, g)) = l;
+    }
+  } else {     // B column `row` of V: V[kb + j, row]
+    const float2* V = P + PINV_V_OFF;
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) {
+      const float2 v = V[(kb + j) + LU_OUTER * row];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    float nim[TC_KC];
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) nim[j] = -im[j];
+    unsigned char* img = base + TC_W_BYTES + (long long)ch * 2 * TC_BIMG;
 #pragma unroll
     for (int g = 0; g < 4; ++g) {
       split8<F16>((g < 2 ? re : nim) + 8 * (g & 1), h, l);
@@ -426,7 +490,7 @@ constexpr int TCP_SMEM = TCP_STAGES * TC_STAGE + 256;
 __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     BatchT<float2> b, int k0, const unsigned char* __restrict__ abuf, const unsigned char* __restrict__ bbuf,
     long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc, int ti0, int nti,
-    int tj0, int ntc, const unsigned char* __restrict__ pabuf, const unsigned char* __restrict__ pbbuf) {
+    int tj0, int ntc, const unsigned char* __restrict__ pabuf, const unsigned char* __restrict__ pbbuf, int mode) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TCP_STAGES * TC_STAGE);
   // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the TMEM address
@@ -558,11 +622,13 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
       const bool got = mbar_wait(accf0 + 8 * buf, (uint32_t)((i >> 1) & 1));
       if (!(ok = __all_sync(0xffffffffu, got))) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // mode 0: A22 tile (r1 + ..., r1 + ...) -= product; mode 1: L21 tile
+      // (r1 + ..., k0 + ...) = product; mode 2: U12 tile (k0 + ..., r1 + ...) = product
       const int n = b.order(z), rest = n - r1;
-      const int gr = r1 + trow * TC_T + row;
+      const int gr = (mode == 2 ? k0 : r1 + trow * TC_T) + row;
       float2* A = b.sys(z);
-      const int cbase = r1 + tcol * TC_T;
-      const int ncol = min(TC_T, rest - tcol * TC_T);
+      const int cbase = mode == 1 ? k0 : r1 + tcol * TC_T;
+      const int ncol = mode == 1 ? TC_T : min(TC_T, rest - tcol * TC_T);
 #pragma unroll 1
       for (int q = 0; q < TC_T / 32; ++q) {
         uint32_t vr[32], vi[32];
@@ -591,19 +657,25 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
           asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce0 + 8 * buf) : "memory");
         }
         if (gr < n && 32 * q < ncol) {
-          float2 cur[32];
           float2* p = A + gr + (long long)n * (cbase + 32 * q);
+          if (mode == 0) {
+            float2 cur[32];
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (32 * q + j < ncol) cur[j] = p[(long long)n * j];
+            for (int j = 0; j < 32; ++j)
+              if (32 * q + j < ncol) cur[j] = p[(long long)n * j];
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (32 * q + j < ncol) {
-              float2 v = cur[j];
-              v.x -= __uint_as_float(vr[j]);
-              v.y -= __uint_as_float(vi[j]);
-              p[(long long)n * j] = v;
-            }
+            for (int j = 0; j < 32; ++j)
+              if (32 * q + j < ncol) {
+                float2 v = cur[j];
+                v.x -= __uint_as_float(vr[j]);
+                v.y -= __uint_as_float(vi[j]);
+                p[(long long)n * j] = v;
+              }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (32 * q + j < ncol) p[(long long)n * j] = make_float2(__uint_as_float(vr[j]), __uint_as_float(vi[j]));
+          }
         }
       }
       ++i;
@@ -710,7 +782,7 @@ inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t
     const int grid = (int)std::min<long long>(tiles, tc_grid_cap(sms > 0 ? sms : 148));
     tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(
         b, k0, w.a, w.b, sa, sb, nt, nsys, status, idesc, tl.ti0, nti, tl.tj0, ntc, prev ? prev->a : nullptr,
-        prev ? prev->b : nullptr);
+        prev ? prev->b : nullptr, 0);
   } else {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
@@ -720,6 +792,41 @@ inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t
                                                                  tl.tj0);
   }
   ++launches;
+}
+
+// The panel's block products on the tensor cores (persistent form), from
+// the images tc_prep wrote of A21 and A12 before them: L21 = A21 V (every row
+// tile, one column tile) and U12 = W A12 (one row tile, every column tile),
+// each written over its operand; W and V from the panel's inverses
+// (panel_inv_kernel). The images of the trailing update are prepared after.
+inline void tc_products(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
+                        int* status) {
+  const int n = b.n, rest = n - k0 - LU_OUTER;
+  if (rest <= 0) return;
+  const int t = (n + TC_T - 1) / TC_T;
+  const long long sa = (long long)t * TC_NCH * 2 * TC_AIMG, sb = (long long)t * TC_NCH * 2 * TC_BIMG;
+  const int nt = (rest + TC_T - 1) / TC_T;
+  constexpr int PER = TC_T * TC_NCH / 128;
+  if (tc_split_f16()) tc_prep_wv_kernel<true><<<dim3(2 * PER, 1, nsys), 128, 0, st>>>(b, k0, w.wv);
+  else tc_prep_wv_kernel<false><<<dim3(2 * PER, 1, nsys), 128, 0, st>>>(b, k0, w.wv);
+  ++launches;
+  const uint32_t idesc = tc_idesc(tc_split_f16());
+  static std::atomic<unsigned long long> attr{0};
+  static int sms = 0;
+  once_per_device(attr, [] {
+    cudaFuncSetAttribute(tc_update_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TCP_SMEM);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  });
+  const int cap = tc_grid_cap(sms > 0 ? sms : 148);
+  // L21 = A21 V: A images of A21 (row tiles), the B image of V (tile 0)
+  tc_update_persistent_kernel<<<(int)std::min<long long>((long long)nt * nsys, cap), TCP_THREADS, TCP_SMEM, st>>>(
+      b, k0, w.a, w.wv + TC_W_BYTES, sa, TC_WV_BYTES, nt, nsys, status, idesc, 0, nt, 0, 1, nullptr, nullptr, 1);
+  // U12 = W A12: the A image of W (tile 0), B images of A12 (column tiles)
+  tc_update_persistent_kernel<<<(int)std::min<long long>((long long)nt * nsys, cap), TCP_THREADS, TCP_SMEM, st>>>(
+      b, k0, w.wv, w.b, TC_WV_BYTES, sb, nt, nsys, status, idesc, 0, 1, 0, nt, nullptr, nullptr, 2);
+  launches += 2;
 }
 
 // outer trailing update after the panel [k0, k0+128); false if disabled
