@@ -394,6 +394,43 @@ def rel_err_families(F, F64, nbeta):
     return float(err.max()), float(np.median(err))
 
 
+def _dof_name(d):
+    axis = int(np.argmax(np.abs(np.asarray(d.direction, dtype=float))))
+    return (("surge", "sway", "heave"), ("roll", "pitch", "yaw"))[d.icase - 1][axis] + (
+        "" if d.body == 1 else "%d" % d.body)
+
+
+def _part_err(x, x64):
+    """|x - x64| / max(|x64|, 1e-6 * family max), families over the last axis,
+    vanishing families (at most 1e-9 of the block's largest value) against
+    1e-6 of the block maximum; the largest over the frequencies."""
+    a = np.abs(x64)
+    fam = a.max(axis=-1, keepdims=True)
+    top = a.max()
+    floor = np.where(fam <= 1e-9 * top, 1e-6 * top, np.maximum(a, 1e-6 * fam))
+    return (np.abs(x - x64) / floor).max(axis=-1)
+
+
+def coefficient_errors(F, F64, case):
+    """Mixed against FP64 per coefficient: for every force component the
+    largest relative error over the frequencies of the excitation force per
+    heading, of the added mass (real part of the radiation force) and of the
+    damping (imaginary part) per radiating degree of freedom. F[force,
+    problem, omega], the diffraction problems first."""
+    nb = len(case.betas_deg)
+    forces = [_dof_name(d) for d in case.force]
+    rad = [_dof_name(d) for d in case.rad]
+    r2 = lambda v: float("%.2g" % v)
+    exc = _part_err(F[:, :nb], F64[:, :nb])
+    am = _part_err(F[:, nb:].real, F64[:, nb:].real)
+    dmp = _part_err(F[:, nb:].imag, F64[:, nb:].imag)
+    return {"forces": forces,
+            "excitation": {"beta=%g" % b: [r2(exc[i, k]) for i in range(len(forces))]
+                           for k, b in enumerate(case.betas_deg)},
+            "added_mass": {r: [r2(am[i, k]) for i in range(len(forces))] for k, r in enumerate(rad)},
+            "damping": {r: [r2(dmp[i, k]) for i in range(len(forces))] for k, r in enumerate(rad)}}
+
+
 def _body_inputs(case):
     from nemoh_b200 import cases as C
     nw = len(case.omegas)
@@ -780,7 +817,8 @@ def run_ours(args):
         "fp64": {"value": whole_job_rate(world, nomega, f64["ms"]), "unit": "solves/s", "ms_per_step": f64["ms"],
                  "phase_ms": {"assemble": f64["phase"][0], "factor_solve": f64["phase"][1], "lu": f64["phase"][3],
                               "solve": f64["phase"][2]}},
-        "mixed_vs_fp64": {"max_rel_err": err_max, "median_rel_err": err_med, "speedup": f64["ms"] / mx["ms"]},
+        "mixed_vs_fp64": {"max_rel_err": err_max, "median_rel_err": err_med, "speedup": f64["ms"] / mx["ms"],
+                          "per_coefficient": coefficient_errors(mx["F"], f64["F"], case)},
         "phase_ms": {"assemble": mx["phase"][0], "factor_refine": mx["phase"][1], "lu": mx["phase"][3],
                      "solve": mx["phase"][2]},
         "refinement": dict(zip(("iterations", "residual"), mx["refinement"])),

@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(ASM_ROWS, ASM_MINB_RANKINE) rankine_cache_kern
 // exponential images of the same branch, fd_images_pair; deep water:
 // wave_infd_both), any other pair once per order (pair_wave); both the tile
 // and its transpose are added to the real parts and written to the imaginary
-// parts, column by column through shared memory.
+// parts, the tile straight from the evaluating threads, its transpose column
+// by column through shared memory.
 // ---------------------------------------------------------------------------
 constexpr int WS_T = 16;
 constexpr int WS_THREADS = 128;
@@ -360,11 +361,31 @@ NB_HD __forceinline__ void wave_infd_both(const GreenCtx& g, const OmegaParams& 
   wave_combine<false>(om, PI.aire, NJJ, w, PJ.xn, PJ.yn, PJ.zn, oji);
 }
 
+// Transposed results of a tile, one array per PairOut field, rows padded to
+// T + 1 so that both the store (thread = row i) and the load (thread = column
+// j) touch distinct banks.
+struct TileT {
+  double v[8][WS_T * (WS_T + 1)];
+  NB_HD __forceinline__ void put(int i, int j, const PairOut& r) {
+    const int o = i * (WS_T + 1) + j;
+    v[0][o] = r.dp_re; v[1][o] = r.dp_im; v[2][o] = r.dm_re; v[3][o] = r.dm_im;
+    v[4][o] = r.sp_re; v[5][o] = r.sp_im; v[6][o] = r.sm_re; v[7][o] = r.sm_im;
+  }
+  NB_HD __forceinline__ PairOut get(int i, int j) const {
+    const int o = i * (WS_T + 1) + j;
+    return PairOut{v[0][o], v[1][o], v[2][o], v[3][o], v[4][o], v[5][o], v[6][o], v[7][o]};
+  }
+};
+
 template <bool FD>
 __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_WAVE_INFD) wave_sym_kernel(
     GreenCtx g, const OmegaParams* __restrict__ oms, const int* __restrict__ slots, const PanelRec* __restrict__ rec,
     int N, AsmOut out, const SlotMesh* __restrict__ meshes) {
-  __shared__ PairOut res[2][WS_T * WS_T];   // [0]: (A_i, B_j) at j*T+i; [1]: (B_j, A_i) at i*T+j
+  // (A_i, B_j) goes out from the thread that evaluates it (consecutive
+  // threads hold consecutive rows i); (B_j, A_i) is staged here and written
+  // after the tile, row j by consecutive threads. Keeping only the transposed
+  // half in shared memory leaves more of the SM's L1 to the table gathers.
+  __shared__ TileT res;
   __shared__ PanelRec pa[WS_T], pb[WS_T];
   __shared__ OmegaParams som;
   const int slot = slots[blockIdx.z];
@@ -391,33 +412,6 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
   __syncthreads();
   const bool diag = ta == tb;
   const int NJJ = g.nsymy + 1;
-  auto live = [&](int i, int j) { return i < na && j < nb && !(diag && i > j); };
-#pragma unroll 1
-  for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {
-    const int i = q % WS_T, j = q / WS_T;
-    if (!live(i, j)) continue;
-    const PanelRec& PI = pa[i];
-    const PanelRec& PJ = pb[j];
-    const bool both = !(diag && i == j);
-    if (PI.zg < g.zer && PJ.zg < g.zer) {
-      PairOut oij, oji;
-      if (FD) {
-        if (!wave_fd_sym(g, som, PI, PJ, NJJ, both, oij, oji)) {
-          set_status(g.status, ST_AKZ_UNDEFINED);
-          oij = oji = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
-        }
-        fd_images_pair(g, som, PI, PJ, NJJ, both, oij, oji);
-      } else {
-        wave_infd_both(g, som, PI, PJ, NJJ, both, oij, oji);
-      }
-      res[0][j * WS_T + i] = oij;
-      if (both) res[1][i * WS_T + j] = oji;
-    } else {
-      pair_wave_ordered<FD>(g, som, PI, PJ, res[0][j * WS_T + i]);
-      if (both) pair_wave_ordered<FD>(g, som, PJ, PI, res[1][i * WS_T + j]);
-    }
-  }
-  __syncthreads();
   const long long NN = (long long)N * N;
   double2* od = out.d + base;
   double2* os = out.s + base;
@@ -441,15 +435,37 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
       if (o32) o32[NN + o] = make_float2((float)dm.x, (float)dm.y);
     }
   };
+  auto live = [&](int i, int j) { return i < na && j < nb && !(diag && i > j); };
+#pragma unroll 1
   for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {
-    {   // entry (a0 + i, b0 + j)
-      const int i = q % WS_T, j = q / WS_T;
-      if (live(i, j)) add((a0 + i) + (long long)N * (b0 + j), res[0][j * WS_T + i]);
+    const int i = q % WS_T, j = q / WS_T;
+    if (!live(i, j)) continue;
+    const PanelRec& PI = pa[i];
+    const PanelRec& PJ = pb[j];
+    const bool both = !(diag && i == j);
+    PairOut oij, oji;
+    if (PI.zg < g.zer && PJ.zg < g.zer) {
+      if (FD) {
+        if (!wave_fd_sym(g, som, PI, PJ, NJJ, both, oij, oji)) {
+          set_status(g.status, ST_AKZ_UNDEFINED);
+          oij = oji = PairOut{0, 0, 0, 0, 0, 0, 0, 0};
+        }
+        fd_images_pair(g, som, PI, PJ, NJJ, both, oij, oji);
+      } else {
+        wave_infd_both(g, som, PI, PJ, NJJ, both, oij, oji);
+      }
+    } else {
+      pair_wave_ordered<FD>(g, som, PI, PJ, oij);
+      if (both) pair_wave_ordered<FD>(g, som, PJ, PI, oji);
     }
-    {   // entry (b0 + j, a0 + i); the diagonal of a diagonal tile is done above
-      const int j = q % WS_T, i = q / WS_T;
-      if (live(i, j) && !(diag && i == j)) add((b0 + j) + (long long)N * (a0 + i), res[1][i * WS_T + j]);
-    }
+    add((a0 + i) + (long long)N * (b0 + j), oij);
+    if (both) res.put(i, j, oji);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {
+    // entry (b0 + j, a0 + i); the diagonal of a diagonal tile went out above
+    const int j = q % WS_T, i = q / WS_T;
+    if (live(i, j) && !(diag && i == j)) add((b0 + j) + (long long)N * (a0 + i), res.get(i, j));
   }
 }
 

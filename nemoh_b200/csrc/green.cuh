@@ -811,14 +811,13 @@ NB_HD __forceinline__ void fd_image_sums(const GreenCtx& g, double H, const doub
       double a[4], f = 0., sa = 0.;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
+        // a select, not a branch: images closer than EPS contribute zero (the
+        // reciprocal of a zero distance is computed and dropped)
         const double RRk = XADD(r2[b], z2[k]);
-        if (RRk > T2) {
-          const double ri = rsqrt(RRk);
-          f += ri;
-          a[k] = ri * ri * ri;
-        } else {
-          a[k] = 0.;
-        }
+        const double ri0 = rsqrt(RRk);
+        const double ri = RRk > T2 ? ri0 : 0.;
+        f += ri;
+        a[k] = ri * ri * ri;
         sa += a[k];
       }
       const double p0 = zp[0] * a[0], p1 = zp[1] * a[1], p2 = zp[2] * a[2], p3 = zp[3] * a[3];
