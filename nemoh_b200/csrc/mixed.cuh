@@ -214,16 +214,17 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
         }
         const int set = (k0 / LU_OUTER) & 1;
         TcWork tg = slice(set);
-        if (tc_prod) {   // L21 = A21 V and U12 = W A12 from images of the operands
+        if (tc_prod) {   // L21 = A21 V and U12 = W A12 from images of the operands, and their images
           tc_prep(tg, bg, k0, ns, sg, launches);
           tc_products(tg, bg, k0, ns, sg, launches, status);
+        } else {         // the images of L21 and U12
+          tc_prep(tg, bg, k0, ns, sg, launches);
         }
         if (!merge) {
-          tc_update(tg, bg, k0, ns, sg, launches, status);
+          tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles(), tc_persistent());
           return;
         }
         auto it = deferred.find(s0);
-        tc_prep(tg, bg, k0, ns, sg, launches);
         if (it != deferred.end() && it->second >= 0) {   // this panel's update and the deferred one
           const TcWork prev = slice(it->second);
           tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles(), true, &prev);

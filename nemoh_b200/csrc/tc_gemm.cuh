@@ -49,7 +49,7 @@ constexpr int ST_TC_TIMEOUT = 30;
 
 // Operand images of two outer updates (two sets: the update of one panel may
 // be merged into the next panel's, and both panels' images are then read).
-constexpr long long TC_W_BYTES = (long long)TC_NCH * 2 * TC_AIMG;   // one A tile of K = 128
+constexpr long long TC_W_BYTES = (long long)TC_NCH * 2 * TC_BIMG;   // one B tile of K = 128 (conj(W^T))
 constexpr long long TC_V_BYTES = (long long)TC_NCH * 2 * TC_BIMG;   // one B tile of K = 128
 constexpr long long TC_WV_BYTES = TC_W_BYTES + TC_V_BYTES;
 
@@ -190,9 +190,12 @@ __global__ void __launch_bounds__(128) tc_prep_kernel(BatchT<float2> b, int k0, 
   }
 }
 
-// Images of the panel's W = inv(L11) (an A tile) and V = inv(U11) (a B tile),
-// K = 128, in the layout of tc_prep_kernel's, for the block products
-// L21 = A21 V and U12 = W A12 on the tensor cores. Blocks [0, 8): W, [8, 16): V.
+// Images of the panel's W = inv(L11) and V = inv(U11), K = 128, in the
+// layout of tc_prep_kernel's, for the block products on the tensor cores:
+// V as the B tile of L21 = A21 V, and conj(W^T) as the B tile of
+// conj(U12^T) = conj(A12^T) conj(W^T), the transposed form of U12 = W A12
+// (its A operand, conj(A12^T), is the first half of A12's B image, and each
+// accumulator row is then one column of U12). Blocks [0, 8): W, [8, 16): V.
 template <bool F16>
 __global__ void __launch_bounds__(128) tc_prep_wv_kernel(BatchT<float2> b, int k0, unsigned char* __restrict__ wv) {
   const int n = b.order(blockIdx.z);
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(128) tc_prep_wv_kernel(BatchT<float2> b, int k
   unsigned char* base = wv + blockIdx.z * TC_WV_BYTES;
   float re[TC_KC], im[TC_KC];
   uint4 h, l;
-  if (isW) {   // A row `row` of W: W[row, kb + j]
+  if (isW) {   // B column `row` of conj(W^T): conj(W[row, kb + j])
     const float2* W = P + PINV_W_OFF;
 #pragma unroll
     for (int j = 0; j < TC_KC; ++j) {
@@ -213,12 +216,19 @@ __global__ void __launch_bounds__(128) tc_prep_wv_kernel(BatchT<float2> b, int k
       re[j] = v.x;
       im[j] = v.y;
     }
-    unsigned char* img = base + (long long)ch * 2 * TC_AIMG;
+    float nim[TC_KC];
+#pragma unroll
+    for (int j = 0; j < TC_KC; ++j) nim[j] = -im[j];
+    unsigned char* img = base + (long long)ch * 2 * TC_BIMG;
+    // B column of Y = conj(W^T): [Re Y; -Im Y] = [Re W; Im W], [Im Y; Re Y] = [-Im W; Re W]
 #pragma unroll
     for (int g = 0; g < 4; ++g) {
       split8<F16>((g < 2 ? re : im) + 8 * (g & 1), h, l);
       *reinterpret_cast<uint4*>(img + tc_row_off(row, g)) = h;
-      *reinterpret_cast<uint4*>(img + TC_AIMG + tc_row_off(row, g)) = l;
+      *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(row, g)) = l;
+      split8<F16>((g < 2 ? nim : re) + 8 * (g & 1), h, l);
+      *reinterpret_cast<uint4*>(img + tc_row_off(TC_T + row, g)) = h;
+      *reinterpret_cast<uint4*>(img + TC_BIMG + tc_row_off(TC_T + row, g)) = l;
     }
   } else {     // B column `row` of V: V[kb + j, row]
     const float2* V = P + PINV_V_OFF;
@@ -294,6 +304,25 @@ __device__ __forceinline__ void tc_load_chunk(uint32_t dst, const unsigned char*
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TC_STAGE) : "memory");
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(ga), "r"(2 * TC_AIMG), "r"(bar)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst + 2 * TC_AIMG),
+               "l"(gb), "r"(2 * TC_BIMG), "r"(bar)
+               : "memory");
+}
+
+// the same stage with the A chunk's hi and lo halves from two places (the
+// first 128 rows of a B image's hi and lo terms)
+__device__ __forceinline__ void tc_load_chunk_split(uint32_t dst, const unsigned char* ga_hi,
+                                                    const unsigned char* ga_lo, const unsigned char* gb,
+                                                    uint32_t bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TC_STAGE) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(ga_hi), "r"(TC_AIMG), "r"(bar)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst + TC_AIMG),
+               "l"(ga_lo), "r"(TC_AIMG), "r"(bar)
                : "memory");
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    dst + 2 * TC_AIMG),
@@ -467,6 +496,68 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
+// Operand images of the trailing update written by the block products'
+// epilogue, for two chunks (32 complex k) of one accumulator row: vr, vi the
+// row's 32 real and imaginary parts (FP32 bits), img the first chunk's image.
+// An A row (L21): k-groups Re(k 0..7), Re(k 8..15), Im(k 0..7), Im(k 8..15).
+__device__ __forceinline__ void tc_store_a_row(unsigned char* img, int row, const uint32_t* vr, const uint32_t* vi,
+                                               int f16) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float x[4][8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      x[0][j] = __uint_as_float(vr[16 * h + j]);
+      x[1][j] = __uint_as_float(vr[16 * h + 8 + j]);
+      x[2][j] = __uint_as_float(vi[16 * h + j]);
+      x[3][j] = __uint_as_float(vi[16 * h + 8 + j]);
+    }
+    unsigned char* c = img + h * 2 * TC_AIMG;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      uint4 hi, lo;
+      if (f16) split8<true>(x[g], hi, lo);
+      else split8<false>(x[g], hi, lo);
+      *reinterpret_cast<uint4*>(c + tc_row_off(row, g)) = hi;
+      *reinterpret_cast<uint4*>(c + TC_AIMG + tc_row_off(row, g)) = lo;
+    }
+  }
+}
+
+// The two B rows of one column of U12 (mode 2's accumulator row: vr = Re,
+// vi = -Im of the column's entries): [Br; -Bi] = [vr; vi] and [Bi; Br] =
+// [-vi; vr], as tc_prep_kernel lays them out.
+__device__ __forceinline__ void tc_store_b_rows(unsigned char* img, int row, const uint32_t* vr, const uint32_t* vi,
+                                                int f16) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float re[2][8], ni[2][8], im[2][8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        re[e][j] = __uint_as_float(vr[16 * h + 8 * e + j]);
+        ni[e][j] = __uint_as_float(vi[16 * h + 8 * e + j]);
+        im[e][j] = -ni[e][j];
+      }
+    unsigned char* c = img + h * 2 * TC_BIMG;
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      uint4 hi, lo;
+      const float* xr = g < 2 ? re[g & 1] : ni[g & 1];
+      const float* xi = g < 2 ? im[g & 1] : re[g & 1];
+      if (f16) split8<true>(xr, hi, lo);
+      else split8<false>(xr, hi, lo);
+      *reinterpret_cast<uint4*>(c + tc_row_off(row, g)) = hi;
+      *reinterpret_cast<uint4*>(c + TC_BIMG + tc_row_off(row, g)) = lo;
+      if (f16) split8<true>(xi, hi, lo);
+      else split8<false>(xi, hi, lo);
+      *reinterpret_cast<uint4*>(c + tc_row_off(TC_T + row, g)) = hi;
+      *reinterpret_cast<uint4*>(c + TC_BIMG + tc_row_off(TC_T + row, g)) = lo;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Persistent form of the same update: one CTA per SM walks the tiles of the
 // launch (tile t, t + grid, ...) with three roles, so that one tile's
@@ -479,6 +570,14 @@ __global__ void __launch_bounds__(128, 2) tc_update_kernel(BatchT<float2> b, int
 //   warps 2-5            read the accumulator (each warp the TMEM lane quarter
 //                        it may access, warp % 4), release it on acc_empty[buf]
 //                        and subtract it from A22.
+// Modes 1 and 2 are the panel's block products, written over their operand
+// (each tile is the only reader of its operand's tile) together with the
+// operand images of the trailing update, into iout:
+//   mode 1: L21 = A21 V, a row tile per tile (A: A21's images, B: V's);
+//   mode 2: conj(U12^T) = conj(A12^T) conj(W^T), a column tile of U12 per
+//           tile: accumulator row = column of U12, so each thread writes its
+//           column's B-image rows (A: the first half of A12's B images, B:
+//           conj(W^T)'s image).
 // Every mbarrier wait is bounded; a role that times out raises the status,
 // flags the others through shared memory, and each role waits (bounded) for
 // the copies or MMAs it has in flight before the CTA frees its tensor memory.
@@ -490,7 +589,8 @@ constexpr int TCP_SMEM = TCP_STAGES * TC_STAGE + 256;
 __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
     BatchT<float2> b, int k0, const unsigned char* __restrict__ abuf, const unsigned char* __restrict__ bbuf,
     long long sys_bytes_a, long long sys_bytes_b, int nt, int nsys, int* status, uint32_t idesc, int ti0, int nti,
-    int tj0, int ntc, const unsigned char* __restrict__ pabuf, const unsigned char* __restrict__ pbbuf, int mode) {
+    int tj0, int ntc, const unsigned char* __restrict__ pabuf, const unsigned char* __restrict__ pbbuf, int mode,
+    unsigned char* iout, int f16) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TCP_STAGES * TC_STAGE);
   // bars: full[S], empty[S], acc_full[2], acc_empty[2]; then the TMEM address
@@ -558,7 +658,13 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
         const int q = (int)(g % TCP_STAGES);
         const long long r = g / TCP_STAGES;
         if (r > 0 && !(ok = mbar_wait(empty0 + 8 * q, (uint32_t)((r - 1) & 1)))) break;
-        tc_load_chunk(s0 + q * TC_STAGE, ga, gb, full0 + 8 * q);
+        if (mode == 2) {   // A: rows of A12's B image (column tile tcol), B: conj(W^T) (one tile)
+          const unsigned char* gt = abuf + z * sys_bytes_a + ((long long)tcol * TC_NCH + cc) * 2 * TC_BIMG;
+          tc_load_chunk_split(s0 + q * TC_STAGE, gt, gt + TC_BIMG, bbuf + z * sys_bytes_b + (long long)cc * 2 * TC_BIMG,
+                              full0 + 8 * q);
+        } else {
+          tc_load_chunk(s0 + q * TC_STAGE, ga, gb, full0 + 8 * q);
+        }
         ++g;
       }
     }
@@ -625,7 +731,8 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
       // mode 0: A22 tile (r1 + ..., r1 + ...) -= product; mode 1: L21 tile
       // (r1 + ..., k0 + ...) = product; mode 2: U12 tile (k0 + ..., r1 + ...) = product
       const int n = b.order(z), rest = n - r1;
-      const int gr = (mode == 2 ? k0 : r1 + trow * TC_T) + row;
+      // this thread's row of A22 or L21, or (mode 2) column of U12
+      const int gr = r1 + (mode == 2 ? tcol : trow) * TC_T + row;
       float2* A = b.sys(z);
       const int cbase = mode == 1 ? k0 : r1 + tcol * TC_T;
       const int ncol = mode == 1 ? TC_T : min(TC_T, rest - tcol * TC_T);
@@ -656,7 +763,14 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
           asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce0 + 8 * buf) : "memory");
         }
-        if (gr < n && 32 * q < ncol) {
+        if (mode == 2) {   // accumulator: Re U12(k0 + k, gr) at column k, -Im U12 at 128 + k
+          if (gr < n) {
+            float2* p = A + (k0 + 32 * q) + (long long)n * gr;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) p[j] = make_float2(__uint_as_float(vr[j]), -__uint_as_float(vi[j]));
+          }
+          tc_store_b_rows(iout + z * sys_bytes_a + ((long long)tcol * TC_NCH + 2 * q) * 2 * TC_BIMG, row, vr, vi, f16);
+        } else if (gr < n && 32 * q < ncol) {
           float2* p = A + gr + (long long)n * (cbase + 32 * q);
           if (mode == 0) {
             float2 cur[32];
@@ -677,6 +791,8 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) tc_update_persistent_kernel(
               if (32 * q + j < ncol) p[(long long)n * j] = make_float2(__uint_as_float(vr[j]), __uint_as_float(vi[j]));
           }
         }
+        if (mode == 1)   // rows beyond the order are zero, as tc_prep_kernel writes them
+          tc_store_a_row(iout + z * sys_bytes_a + ((long long)trow * TC_NCH + 2 * q) * 2 * TC_AIMG, row, vr, vi, f16);
       }
       ++i;
     }
@@ -782,7 +898,7 @@ inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t
     const int grid = (int)std::min<long long>(tiles, tc_grid_cap(sms > 0 ? sms : 148));
     tc_update_persistent_kernel<<<grid, TCP_THREADS, TCP_SMEM, st>>>(
         b, k0, w.a, w.b, sa, sb, nt, nsys, status, idesc, tl.ti0, nti, tl.tj0, ntc, prev ? prev->a : nullptr,
-        prev ? prev->b : nullptr, 0);
+        prev ? prev->b : nullptr, 0, nullptr, 0);
   } else {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
@@ -798,7 +914,8 @@ inline void tc_apply(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t
 // the images tc_prep wrote of A21 and A12 before them: L21 = A21 V (every row
 // tile, one column tile) and U12 = W A12 (one row tile, every column tile),
 // each written over its operand; W and V from the panel's inverses
-// (panel_inv_kernel). The images of the trailing update are prepared after.
+// (panel_inv_kernel). Both write the trailing update's operand images of the
+// products over the operands' images (the update needs no tc_prep after).
 inline void tc_products(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
                         int* status) {
   const int n = b.n, rest = n - k0 - LU_OUTER;
@@ -820,22 +937,16 @@ inline void tc_products(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStrea
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   });
   const int cap = tc_grid_cap(sms > 0 ? sms : 148);
+  const int f16 = tc_split_f16() ? 1 : 0;
   // L21 = A21 V: A images of A21 (row tiles), the B image of V (tile 0)
   tc_update_persistent_kernel<<<(int)std::min<long long>((long long)nt * nsys, cap), TCP_THREADS, TCP_SMEM, st>>>(
-      b, k0, w.a, w.wv + TC_W_BYTES, sa, TC_WV_BYTES, nt, nsys, status, idesc, 0, nt, 0, 1, nullptr, nullptr, 1);
-  // U12 = W A12: the A image of W (tile 0), B images of A12 (column tiles)
+      b, k0, w.a, w.wv + TC_W_BYTES, sa, TC_WV_BYTES, nt, nsys, status, idesc, 0, nt, 0, 1, nullptr, nullptr, 1, w.a,
+      f16);
+  // conj(U12^T) = conj(A12^T) conj(W^T): A from the B images of A12 (column
+  // tiles), B the image of conj(W^T) (tile 0)
   tc_update_persistent_kernel<<<(int)std::min<long long>((long long)nt * nsys, cap), TCP_THREADS, TCP_SMEM, st>>>(
-      b, k0, w.wv, w.b, TC_WV_BYTES, sb, nt, nsys, status, idesc, 0, 1, 0, nt, nullptr, nullptr, 2);
+      b, k0, w.b, w.wv, sb, TC_WV_BYTES, nt, nsys, status, idesc, 0, 1, 0, nt, nullptr, nullptr, 2, w.b, f16);
   launches += 2;
-}
-
-// outer trailing update after the panel [k0, k0+128); false if disabled
-inline bool tc_update(TcWork& w, BatchT<float2> b, int k0, int nsys, cudaStream_t st, long long& launches,
-                      int* status) {
-  if (!tc_enabled()) return false;
-  tc_prep(w, b, k0, nsys, st, launches);
-  tc_apply(w, b, k0, nsys, st, launches, status, TcTiles(), tc_persistent());
-  return true;
 }
 
 }  // namespace nb200
