@@ -79,7 +79,9 @@ NB_HD __noinline__ cplx GG(cplx Z, cplx CEX) {
   return (T < 0.) ? num / den - IPI * CEX : num / den + IPI * CEX;
 }
 
-// integer part of a monotone log10 expression, made exact by thresholds
+// integer part of a monotone log10 expression, made exact by thresholds: the
+// estimate k may be off by up to four (it comes from an FP32 log10, within one
+// of the exact value), the thresholds settle it
 NB_HD __forceinline__ int stencil_adjust(double x, const double* thr, int k) {
   k = max(0, min(k, 47));
 #pragma unroll 1
@@ -93,8 +95,9 @@ NB_HD __forceinline__ int stencil_adjust(double x, const double* thr, int k) {
 NB_HD __forceinline__ int stencil_kj(double AKZ, const StencilThresholds* T) {
   double x = -AKZ;
   int k;
-  if (AKZ < -1.E-2) k = stencil_adjust(x, T->kj8, (int)(8. * (log10(x) + 4.5)));
-  else k = stencil_adjust(x, T->kj5, (int)(5. * (log10(x) + 6.)));
+  const float lx = log10f((float)x);
+  if (AKZ < -1.E-2) k = stencil_adjust(x, T->kj8, (int)(8.f * (lx + 4.5f)));
+  else k = stencil_adjust(x, T->kj5, (int)(5.f * (lx + 6.f)));
   k = max(k, 2);
   return min(k, 45);
 }
@@ -104,7 +107,7 @@ NB_HD __forceinline__ int stencil_ki(double AKR, const StencilThresholds* T) {
   int k;
   if (AKR < 1.) {
     double y = XADD(AKR, 1.E-20);
-    k = stencil_adjust(y, T->ki5, (int)(5. * (log10(y) + 6.) + 1.));
+    k = stencil_adjust(y, T->ki5, (int)(5.f * (log10f((float)y) + 6.f) + 1.f));
   } else {
     k = (int)XADD(XMUL(3., AKR), 28.);
   }
