@@ -151,11 +151,16 @@ constexpr int ASM_TJ = 32;
 #ifndef ASM_MINB_RANKINE
 #define ASM_MINB_RANKINE 3
 #endif
+// CTAs per SM of the wave pass (128 and 102 registers at most): measured on the barge
+// step, the finite-depth pass is fastest at 4 (at 5 its spills double and the
+// assembly takes 1.8 ms more); the deep-water pass spills the same at 96
+// registers as at 128 (its stack holds local arrays), and 5 CTAs save about
+// 0.5 ms of the step's assembly
 #ifndef ASM_MINB_WAVE_FD
 #define ASM_MINB_WAVE_FD 4
 #endif
 #ifndef ASM_MINB_WAVE_INFD
-#define ASM_MINB_WAVE_INFD 4
+#define ASM_MINB_WAVE_INFD 5
 #endif
 
 struct AsmOut {
