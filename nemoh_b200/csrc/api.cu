@@ -66,8 +66,12 @@ struct HostBuf {
     release();
     const size_t want = std::max<size_t>(2 * n, 4096);
     cudaError_t e = cudaMallocHost(&p, want);
-    if (e == cudaSuccess) bytes = want;
-    else p = nullptr;
+    if (e == cudaSuccess) {
+      bytes = want;
+    } else {
+      p = nullptr;
+      cudaGetLastError();   // returned; not left for a later launch check
+    }
     return e;
   }
   template <class T>
@@ -799,7 +803,7 @@ size_t item_bytes(const nemoh_ctx* c, const BodyState& b, int nmax, int nrhs) {
 // decreasing order of their body's panel count
 void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const double* omegas, int nrhs,
                   const std::vector<long long>& nvel_off, const std::vector<long long>& force_off,
-                  const double2* nvel_d, double2* force_d) {
+                  const double2* nvel_d, double2* force_d, bool headroom) {
   std::vector<long long> off;
   std::vector<int> ord, host_n(k);
   std::vector<char> has_rk(k);
@@ -825,16 +829,17 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   }
   const int nsys = (int)ord.size(), nmax = ord[0];
   const size_t N = nmax, V = (size_t)nsys * N * nrhs;
-  // batches of different bodies keep setting new footprints: grow with headroom
-  CK(c->d_D.ensure((size_t)mat * sizeof(double2), true));
-  CK(c->d_S.ensure((size_t)mat * sizeof(double2), true));
-  CK(c->d_X.ensure(V * sizeof(double2), true));
-  CK(c->d_Y.ensure(V * sizeof(double2), true));
-  CK(c->d_diag.ensure((size_t)nsys * DIAG_SCRATCH * sizeof(double2), true));
+  // batches of different bodies keep setting new footprints: grow with
+  // headroom, when the batch leaves room for it
+  CK(c->d_D.ensure((size_t)mat * sizeof(double2), headroom));
+  CK(c->d_S.ensure((size_t)mat * sizeof(double2), headroom));
+  CK(c->d_X.ensure(V * sizeof(double2), headroom));
+  CK(c->d_Y.ensure(V * sizeof(double2), headroom));
+  CK(c->d_diag.ensure((size_t)nsys * DIAG_SCRATCH * sizeof(double2), headroom));
   if (c->mode == NEMOH_B200_FP64)
-    CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2), true));
+    CK(c->d_inv.ensure((size_t)nsys * ((N + TB - 1) / TB) * 2 * TB * TB * sizeof(double2), headroom));
   else
-    CK(c->mixed.ensure(nsys, nmax, nrhs, (size_t)mat, true));
+    CK(c->mixed.ensure(nsys, nmax, nrhs, (size_t)mat, headroom));
   CK(c->d_oms.ensure((size_t)k * sizeof(OmegaParams)));
   CK(c->d_slots.ensure((size_t)k * sizeof(int)));
   CK(c->h_oms.ensure((size_t)k * sizeof(OmegaParams)));
@@ -1061,6 +1066,14 @@ void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* o
   std::iota(idx.begin(), idx.end(), 0);
   std::stable_sort(idx.begin(), idx.end(),
                    [&](int a, int b) { return c->bodies[body[a]]->nfa > c->bodies[body[b]]->nfa; });
+  c->t_asm = c->t_fac = c->t_sol = c->t_lu = 0;
+  // the resident bodies' Rankine caches first, so that the budget below sees them
+  ScopedEvent rk0, rk1;
+  CK(cudaEventCreate(&rk0.e));
+  CK(cudaEventCreate(&rk1.e));
+  CK(cudaEventRecord(rk0.e, c->stream));
+  ensure_body_rankine(c, nitem, body, omegas);
+  CK(cudaEventRecord(rk1.e, c->stream));
   // admission by HBM footprint: 80% of the free memory, the batch's own
   // buffers counted as free
   size_t fr = 0, tot = 0;
@@ -1074,13 +1087,6 @@ void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* o
     const long long v = std::atoll(e);
     if (v > 0) budget = std::min(budget, (size_t)v);
   }
-  c->t_asm = c->t_fac = c->t_sol = c->t_lu = 0;
-  ScopedEvent rk0, rk1;
-  CK(cudaEventCreate(&rk0.e));
-  CK(cudaEventCreate(&rk1.e));
-  CK(cudaEventRecord(rk0.e, c->stream));
-  ensure_body_rankine(c, nitem, body, omegas);
-  CK(cudaEventRecord(rk1.e, c->stream));
   int pos = 0;
   while (pos < nitem) {
     const int nmax = c->bodies[body[idx[pos]]]->nfa;
@@ -1092,7 +1098,9 @@ void solve_bodies_impl(nemoh_ctx* c, int nitem, const int* body, const double* o
       used += need;
       ++end;
     }
-    ragged_batch(c, idx.data() + pos, end - pos, body, omegas, nrhs, nvel_off, force_off, nvel_d, force_d);
+    // the buffers' growth headroom (a quarter) only where the batch leaves room
+    ragged_batch(c, idx.data() + pos, end - pos, body, omegas, nrhs, nvel_off, force_off, nvel_d, force_d,
+                 used + used / 4 <= budget);
     pos = end;
   }
   float ms = 0;   // the batches ended with a synchronisation
@@ -1109,6 +1117,10 @@ static int guarded(nemoh_ctx* ctx, const std::function<void()>& f) {
     return NEMOH_B200_OK;
   } catch (const Fail& e) {
     if (ctx) ctx->err = e.msg;
+    // a failed runtime call leaves its error as the thread's last error; it is
+    // reported here, so the next entry point's launch checks must not see it
+    // again (an error that the context keeps comes back on its next call)
+    cudaGetLastError();
     return e.code;
   } catch (const std::exception& e) {
     if (ctx) ctx->err = e.what();

@@ -29,8 +29,14 @@ inline cudaError_t grow_alloc(void** p, size_t* have, size_t n, bool headroom) {
     want = n;
     e = cudaMalloc(p, want);
   }
-  if (e == cudaSuccess) *have = want;
-  else *p = nullptr;
+  if (e == cudaSuccess) {
+    *have = want;
+  } else {
+    *p = nullptr;
+    // the failure goes back as the return value; consume it, so that a later
+    // cudaGetLastError (a launch check) does not report it again
+    cudaGetLastError();
+  }
   return e;
 }
 
