@@ -928,6 +928,10 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
   }
   const bool mixed = c->mode == NEMOH_B200_MIXED;
   const int max_it = refine_max_it(), passes = mixed ? std::min(REFINE_CHUNK, max_it) : 0;
+  // the FP64 sweeps' workspace grows here, never inside a captured sequence
+  if (!mixed) fp64_sync(c, nsys, nmax);
+  // a captured sequence holds every buffer address it was captured with: the
+  // key covers them all, so a buffer that moved since is captured again
   std::vector<long long> sig = {c->mode, nrhs, k, nsys, nmax, nint_max, passes, (long long)nvel_d,
                                 (long long)force_d, (long long)c->d_D.p, (long long)c->d_S.p, (long long)c->d_X.p,
                                 (long long)c->d_Y.p, (long long)c->d_diag.p, (long long)c->d_inv.p,
@@ -936,7 +940,9 @@ void ragged_batch(nemoh_ctx* c, const int* items, int k, const int* body, const 
                                 (long long)c->mixed.lu, (long long)c->mixed.diag, (long long)c->mixed.b,
                                 (long long)c->mixed.r, (long long)c->mixed.rf, (long long)c->mixed.yf,
                                 (long long)c->mixed.inv, (long long)c->mixed.pinv, (long long)c->mixed.norms,
-                                (long long)c->mixed.state, (long long)c->mixed.tc.a, (long long)c->mixed.tc.b};
+                                (long long)c->mixed.state, (long long)c->mixed.tc.a, (long long)c->mixed.tc.b,
+                                (long long)c->mixed.tc.wv, (long long)c->mixed.flow, (long long)c->mixed.act,
+                                (long long)c->d_flow.p};
   for (const AsmGroup& g : groups)
     sig.insert(sig.end(), {g.ninfd, g.nfd, g.n_infd, g.n_fd, (long long)g.slot_rk_infd, (long long)g.slot_rk_fd});
   sig.insert(sig.end(), ord.begin(), ord.end());

@@ -1660,6 +1660,9 @@ __global__ void __launch_bounds__(FL_THREADS) trsm_flow_kernel(BatchT<C2> b, con
   const int total = pre[nblk];
   int* flags = ws + 2;
   for (;;) {
+    // every thread has read the previous item before thread 0 claims the next
+    // (an item of a converged system is skipped straight back to here)
+    __syncthreads();
     if (t == 0) s_item = atomicAdd(ws, 1);
     __syncthreads();
     const int item = s_item;
