@@ -444,12 +444,13 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
 #pragma unroll 1
   for (int q = threadIdx.x; q < WS_T * WS_T; q += WS_THREADS) {
     const int i = q % WS_T, j = q / WS_T;
-    if (!live(i, j)) continue;
+    const bool lv = live(i, j);
     const PanelRec& PI = pa[i];
     const PanelRec& PJ = pb[j];
     const bool both = !(diag && i == j);
     PairOut oij, oji;
-    if (PI.zg < g.zer && PJ.zg < g.zer) {
+    if (!lv) {
+    } else if (PI.zg < g.zer && PJ.zg < g.zer) {
       if (FD) {
         if (!wave_fd_sym(g, som, PI, PJ, NJJ, both, oij, oji)) {
           set_status(g.status, ST_AKZ_UNDEFINED);
@@ -463,6 +464,9 @@ __global__ void __launch_bounds__(WS_THREADS, FD ? ASM_MINB_WAVE_FD : ASM_MINB_W
       pair_wave_ordered<FD>(g, som, PI, PJ, oij);
       if (both) pair_wave_ordered<FD>(g, som, PJ, PI, oji);
     }
+    // the warp stores its rows together: each column segment goes out whole
+    __syncwarp();
+    if (!lv) continue;
     add((a0 + i) + (long long)N * (b0 + j), oij);
     if (both) res.put(i, j, oji);
   }
