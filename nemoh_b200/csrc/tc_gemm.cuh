@@ -56,7 +56,7 @@ constexpr long long TC_WV_BYTES = TC_W_BYTES + TC_V_BYTES;
 struct TcWork {
   unsigned char* a = nullptr;   // A images: 2 sets x nsys x ceil(n/128) row tiles x TC_NCH chunks x (hi, lo)
   unsigned char* b = nullptr;   // B images: 2 sets x nsys x ceil(n/128) column tiles x TC_NCH chunks x (hi, lo)
-  // per system: the A image of W = inv(L11), then the B image of V = inv(U11)
+  // per system: the B images of conj(W^T), W = inv(L11), and of V = inv(U11)
   // (the panel's block products on the tensor cores)
   unsigned char* wv = nullptr;
   size_t have_a = 0, have_b = 0, have_wv = 0;
