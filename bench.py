@@ -639,18 +639,23 @@ def run_serving(local, n_bodies, n_req, rates=(0.25, 0.5, 0.75, 0.9, 1.0, 1.2), 
     bodies (one omega U(0.1, 2.5), heading U(0, 180) deg, 6 DOF per request)
     through the continuous-batching server (resident bodies, right-hand sides
     built on the device, cross-body batches). The saturation throughput is the
-    rate achieved on a stream offered well above capacity; streams at
-    fractions of it then give the latency percentiles."""
+    median of the rates achieved on three streams offered well above capacity
+    (one such stream's rate varies by tens of percent between runs with the
+    batches the workers happen to take); streams at fractions of it then give
+    the latency percentiles."""
     import nemoh_b200 as nb
     from nemoh_b200 import serving as S
     bodies = S.make_bodies(n_bodies, seed=4)
     srv = S.SolveServer(bodies, device=local, precision=nb.MIXED, workers=workers)
     try:
         srv.run(S.make_requests(min(256, n_req), 0, n_bodies, seed=seed + 100), realtime=False)   # warm-up
-        done, wall = srv.run(S.make_requests(min(n_req, 4000), 1e6, n_bodies, seed=seed))
-        sat = len(done) / wall
+        sats = []
+        for k in range(3):
+            done, wall = srv.run(S.make_requests(min(n_req, 4000), 1e6, n_bodies, seed=seed + 1000 * k))
+            sats.append(len(done) / wall)
+        sat = float(np.median(sats))
         out = {"bodies": n_bodies, "requests_per_rate": n_req, "workers": workers, "precision": "mixed",
-               "saturation_solves_per_s": sat, "rates": []}
+               "saturation_solves_per_s": sat, "saturation_streams_solves_per_s": sats, "rates": []}
         last = None
         for f in rates:
             done, wall = srv.run(S.make_requests(n_req, f * sat, n_bodies, seed=seed + int(100 * f)))
