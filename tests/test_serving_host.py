@@ -108,3 +108,46 @@ def test_failed_batch_is_reported_not_dropped():
         pass
     else:
         raise AssertionError("a short result list went unnoticed")
+
+
+def test_collector_off_during_a_stream_and_restored():
+    """The cyclic garbage collector is off while a stream runs (its pauses were
+    the latency tails) and back to the caller's setting afterwards, also when a
+    batch fails."""
+    import gc
+
+    seen = []
+
+    class Probe(FakeSolver):
+        def solve_requests(self, bodies, omegas, betas):
+            seen.append(gc.isenabled())
+            return super().solve_requests(bodies, omegas, betas)
+
+    srv = S.SolveServer(_bodies(), workers=1, solver_factory=Probe, memory_bytes=1 << 30)
+    was = gc.isenabled()
+    try:
+        gc.enable()
+        srv.run(S.make_requests(8, rate=0, n_bodies=2, seed=3), realtime=False)
+        assert seen and not any(seen)
+        assert gc.isenabled()
+        gc.disable()
+        srv.run(S.make_requests(4, rate=0, n_bodies=2, seed=4), realtime=False)
+        assert not gc.isenabled()
+
+        class Failing(FakeSolver):
+            def solve_requests(self, bodies, omegas, betas):
+                raise RuntimeError("planted failure")
+
+        gc.enable()
+        bad = S.SolveServer(_bodies(), workers=1, solver_factory=Failing, memory_bytes=1 << 30)
+        try:
+            bad.run(S.make_requests(3, rate=0, n_bodies=2, seed=5), realtime=False)
+            raise AssertionError("a failed batch must raise")
+        except S.ServeError:
+            pass
+        assert gc.isenabled()
+    finally:
+        if was:
+            gc.enable()
+        else:
+            gc.disable()
