@@ -214,12 +214,11 @@ inline void mixed_factor(MixedWork& w, double2* D, int n, int nsys, int* status,
         }
         const int set = (k0 / LU_OUTER) & 1;
         TcWork tg = slice(set);
-        if (tc_prod) {   // L21 = A21 V and U12 = W A12 from images of the operands, and their images
-          tc_prep(tg, bg, k0, ns, sg, launches);
-          tc_products(tg, bg, k0, ns, sg, launches, status);
-        } else {         // the images of L21 and U12
-          tc_prep(tg, bg, k0, ns, sg, launches);
-        }
+        // operand images of the panel's columns and rows: with tc_prod those of
+        // A21 and A12, from which the block products form L21 = A21 V and
+        // U12 = W A12 together with their images; else those of L21 and U12
+        tc_prep(tg, bg, k0, ns, sg, launches);
+        if (tc_prod) tc_products(tg, bg, k0, ns, sg, launches, status);
         if (!merge) {
           tc_apply(tg, bg, k0, ns, sg, launches, status, TcTiles(), tc_persistent());
           return;
